@@ -1,0 +1,182 @@
+/*
+ * omega_b200.h -- C-ABI of the B200 (sm_100a) matrix-free tomographic projectors.
+ *
+ * This library replaces OMEGA's per-call kernel launch path for the
+ * forward projector A*x and the backprojector A^T*y (projector types 1, 4
+ * and 5) and the OSEM / PDHG subset updates they drive.  Reference
+ * interfaces each entry point replaces are cited beside it (paths inside the
+ * OMEGA source tree).
+ *
+ * Conventions
+ *  - Every function returns an int status: OMB_OK (0) or a negative omb_status.
+ *    Nothing aborts, traps or exits; the message of the last failure on the
+ *    calling thread is returned by omb_last_error().
+ *  - Device pointers are plain CUDA device addresses of float32 buffers owned
+ *    by the caller (e.g. torch tensors' data_ptr()).  Host pointers are only
+ *    read during the call.
+ *  - `stream` is a cudaStream_t passed as void*; NULL means the legacy default
+ *    stream.  All work is stream-ordered; nothing synchronises the device
+ *    except the functions that return a host scalar (documented below).
+ *  - Images are Fortran order (x fastest), length Nx*Ny*Nz.  Measurements are
+ *    sinogram/projection order (detector row fastest, then column, then
+ *    sinogram/projection in subset order); with TOF the bins are outermost per
+ *    call: [bin0 of all rays, bin1 of all rays, ...].
+ *  - A handle binds one device (the current device at omb_create) and is not
+ *    reentrant: do not call into one handle from two threads at once.
+ *    Distinct handles are independent.
+ */
+#ifndef OMEGA_B200_H
+#define OMEGA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OMB_ABI_VERSION 1
+
+typedef enum omb_status {
+    OMB_OK = 0,
+    OMB_ERR_INVALID = -1,     /* bad argument or geometry */
+    OMB_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+    OMB_ERR_ALLOC = -3,       /* device allocation failed */
+    OMB_ERR_UNSUPPORTED = -4, /* valid request outside what this build implements */
+    OMB_ERR_TIMEOUT = -5      /* a bounded device wait gave up */
+} omb_status;
+
+typedef enum omb_modality {
+    OMB_PET_SINOGRAM = 0, /* PET sinogram: xy = (Ndist*Nang) x [xs, ys, xd, yd]; z = nProj x [zs, zd] */
+    OMB_CT_PANEL = 1      /* CT flat panel: xy = nProj x [sx, sy, sz, dx, dy, dz]; z = nProj x [ux*pitchX, uy*pitchX] */
+} omb_modality;
+
+typedef enum omb_bp_mode {
+    OMB_BP_FLOAT_ATOMIC = 0, /* float32 atomics (the reference's CUDA path) */
+    OMB_BP_FIXED64 = 1       /* int64 fixed point, bit-identical run to run (the reference's OpenCL -DATOMIC path) */
+} omb_bp_mode;
+
+/*
+ * Geometry and projector options.  Mirrors the scalars and arrays OMEGA's
+ * Python layer uploads before the first launch
+ * (omegatomo/projector/init.py:468-703, kernel-argument prefixes kIndF/kIndB)
+ * in an explicit, versioned layout: `struct_size` must equal
+ * sizeof(omb_geometry_desc) and `abi_version` OMB_ABI_VERSION.
+ * All arrays are host pointers, copied to the device by omb_create.
+ */
+typedef struct omb_geometry_desc {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    int32_t modality;        /* omb_modality */
+    int32_t fp_type;         /* forward projector: 1 (improved Siddon), 4 (interpolation), 5 (branchless distance-driven) */
+    int32_t bp_type;         /* backprojector: 1, 4 or 5 */
+    uint32_t nx, ny, nz;     /* image size */
+    float dx, dy, dz;        /* voxel size (mm) */
+    float bx, by, bz;        /* FOV corner (mm), the lower edge of voxel 0 */
+    uint32_t n_rows_d;       /* Ndist (PET) / detector rows (CT) */
+    uint32_t n_cols_d;       /* Nang (PET) / detector columns (CT) */
+    int64_t n_proj;          /* sinograms / projections in total */
+    int32_t n_subsets;
+    int32_t subset_type;     /* OMEGA subsetType: 8-11 whole sinograms/projections; 1, 2, 4, 5 measurement-level (PET) */
+    const int64_t *n_meas;   /* n_subsets+1 cumulative sinogram/projection counts (proj.py nMeas) */
+    const float *xy;         /* see omb_modality; CT rows in subset order */
+    int64_t n_xy;            /* number of floats in xy */
+    const float *z;          /* see omb_modality; in subset order for subset types >= 8 */
+    int64_t n_z;             /* number of floats in z */
+    float dpitch_x, dpitch_y;/* detector pitch (proj.py dPitchX/dPitchY) */
+    float global_factor;     /* proj.py global_factor */
+    float epps;              /* proj.py epps */
+    int32_t tof_bins;        /* 1 = no TOF */
+    float sigma_x;           /* TOF Gaussian sigma (mm) */
+    const float *tof_centers;/* tof_bins centres (mm) (proj.py TOFCenter) */
+    float dL;                /* type 4 step length (mm), coordinates.py:242-262 */
+    float d_scale4[3];       /* type 4 1/(d*N) per axis */
+    float d_size5[2];        /* type 5 dSizeX, dSizeY */
+    float d_scale5[3];       /* type 5 dScaleX/Y/Z */
+    float kerroin;           /* type 4 CT backprojection weight */
+    int32_t fixed64_workspace; /* nonzero: allocate the int64 accumulators omb_backward needs for OMB_BP_FIXED64 */
+} omb_geometry_desc;
+
+typedef struct omb_handle omb_handle;
+
+/* Library ABI version (OMB_ABI_VERSION of the build). */
+int omb_abi_version(void);
+
+/* Message of the last failure on the calling thread ("" if none). Valid until the next call on this thread. */
+const char *omb_last_error(void);
+
+/*
+ * Validate the geometry, upload it to the current device and return a handle.
+ * Replaces omegatomo/projector/init.py:39-703 (initProjector: option
+ * assembly, device uploads, kernel JIT) and ProjectorClass.h:1780
+ * (addProjector) / 3055 (createBuffers) / 3117 (initializeKernel).
+ */
+int omb_create(const omb_geometry_desc *desc, omb_handle **out);
+
+/* Free all device memory of the handle. Replaces nothing: OMEGA frees on garbage collection. */
+int omb_destroy(omb_handle *h);
+
+/* Measurement count of one subset (all TOF bins), or of all subsets when subset == -1. */
+int64_t omb_measurement_count(const omb_handle *h, int32_t subset);
+
+/* Image voxel count Nx*Ny*Nz. */
+int64_t omb_image_count(const omb_handle *h);
+
+/*
+ * y = A_s * image.  subset in [0, n_subsets) or -1 for all subsets in one
+ * launch (output concatenated in subset order).  `y` is overwritten.
+ * Replaces omegatomo/projector/projfunctions.py:86-436 (forwardProjection,
+ * CuPy branch) and ProjectorClass.h:3478 (forwardProjection); kernels
+ * restate projectorType123.cl:81-1374 (-DFP -DSIDDON), projectorType4.cl:84
+ * (projectorType4Forward) and projectorType5.cl:64 (projectorType5Forward).
+ */
+int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, void *stream);
+
+/*
+ * image = A_s^T * y, and sens = A_s^T * 1 when `sens` is not NULL (the
+ * reference's no_norm == 0 pass).  Both outputs are overwritten.
+ * mode: omb_bp_mode; OMB_BP_FIXED64 needs a handle created with
+ * fixed64_workspace != 0.
+ * Replaces projfunctions.py:735-1095 (backwardProjection) and
+ * ProjectorClass.h:3893 (backwardProjection); kernels restate
+ * projectorType123.cl (-DBP, rhs() general_opencl_functions.h:1212-1275),
+ * projectorType4.cl:718 (projectorType4Backward) and projectorType5.cl:381.
+ */
+int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, float *sens,
+                 int32_t mode, void *stream);
+
+/*
+ * One OSEM sub-iteration for PET, fused on the device:
+ *   fp = A_s x + epps;  r = y_s / fp (NaN/Inf -> epps);  rhs = A_s^T r;
+ *   x = x / sens_s * (rhs + epps)
+ * `sens` is the subset's sensitivity image already clamped to >= epps
+ * (see omb_sensitivity).  `work_meas` is caller scratch of
+ * omb_measurement_count(h, subset) floats; `work_img` of Nx*Ny*Nz floats.
+ * Restates computeForwardProject.h:20-21, 92-95, 400-401 (ratio),
+ * algorithms.h:12-15 with subiterStep.h:110-121 (EM update).
+ */
+int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset,
+                    const float *sens, float *work_meas, float *work_img, void *stream);
+
+/*
+ * sens = max(A_s^T 1, epps): the per-subset sensitivity image of the first
+ * iteration (reconstructionAF.h:303-328 with the clamp of functions.hpp:2980-2996).
+ */
+int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream);
+
+/*
+ * Poisson log-likelihood sum_i [ y_i * log(fp_i + epps) - (fp_i + epps) ],
+ * accumulated in FP64 on the device, written to *out_host.  Synchronises
+ * `stream`.  `work` is caller scratch of at least omb_reduce_workspace_bytes(n)
+ * bytes.  The reference computes no likelihood; this is the measurement the
+ * OSEM comparisons use.
+ */
+int omb_loglik(const float *y, const float *fp, int64_t n, float epps, double *out_host,
+               void *work, void *stream);
+size_t omb_reduce_workspace_bytes(int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OMEGA_B200_H */

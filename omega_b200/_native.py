@@ -1,0 +1,140 @@
+"""ctypes binding of ``libomega_b200.so`` (the C-ABI of include/omega_b200.h).
+
+The library is loaded from ``omega_b200/lib``; there is no fallback: if it is
+missing or fails to load, every projector call raises.  Build it with
+``python -m omega_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libomega_b200.so")
+
+OMB_ABI_VERSION = 1
+OMB_PET_SINOGRAM = 0
+OMB_CT_PANEL = 1
+OMB_BP_FLOAT_ATOMIC = 0
+OMB_BP_FIXED64 = 1
+
+_c_float_p = ctypes.POINTER(ctypes.c_float)
+_c_i64_p = ctypes.POINTER(ctypes.c_int64)
+
+
+class GeometryDesc(ctypes.Structure):
+    """Mirror of ``omb_geometry_desc`` (explicit natural layout, no packing)."""
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("abi_version", ctypes.c_uint32),
+        ("modality", ctypes.c_int32),
+        ("fp_type", ctypes.c_int32),
+        ("bp_type", ctypes.c_int32),
+        ("nx", ctypes.c_uint32),
+        ("ny", ctypes.c_uint32),
+        ("nz", ctypes.c_uint32),
+        ("dx", ctypes.c_float),
+        ("dy", ctypes.c_float),
+        ("dz", ctypes.c_float),
+        ("bx", ctypes.c_float),
+        ("by", ctypes.c_float),
+        ("bz", ctypes.c_float),
+        ("n_rows_d", ctypes.c_uint32),
+        ("n_cols_d", ctypes.c_uint32),
+        ("n_proj", ctypes.c_int64),
+        ("n_subsets", ctypes.c_int32),
+        ("subset_type", ctypes.c_int32),
+        ("n_meas", _c_i64_p),
+        ("xy", _c_float_p),
+        ("n_xy", ctypes.c_int64),
+        ("z", _c_float_p),
+        ("n_z", ctypes.c_int64),
+        ("dpitch_x", ctypes.c_float),
+        ("dpitch_y", ctypes.c_float),
+        ("global_factor", ctypes.c_float),
+        ("epps", ctypes.c_float),
+        ("tof_bins", ctypes.c_int32),
+        ("sigma_x", ctypes.c_float),
+        ("tof_centers", _c_float_p),
+        ("dL", ctypes.c_float),
+        ("d_scale4", ctypes.c_float * 3),
+        ("d_size5", ctypes.c_float * 2),
+        ("d_scale5", ctypes.c_float * 3),
+        ("kerroin", ctypes.c_float),
+        ("fixed64_workspace", ctypes.c_int32),
+    ]
+
+
+# (name, restype, argtypes) of every exported entry point of include/omega_b200.h
+EXPORTS = [
+    ("omb_abi_version", ctypes.c_int, []),
+    ("omb_last_error", ctypes.c_char_p, []),
+    ("omb_create", ctypes.c_int, [ctypes.POINTER(GeometryDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    ("omb_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("omb_measurement_count", ctypes.c_int64, [ctypes.c_void_p, ctypes.c_int32]),
+    ("omb_image_count", ctypes.c_int64, [ctypes.c_void_p]),
+    ("omb_forward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_backward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    ("omb_osem_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_sensitivity", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_loglik", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_reduce_workspace_bytes", ctypes.c_size_t, [ctypes.c_int64]),
+]
+
+_lib = None
+_lock = threading.Lock()
+
+
+class NativeError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, fn, status, msg):
+        super().__init__(f"{fn} failed with status {status}: {msg}")
+        self.status = status
+
+
+def lib():
+    """The loaded library (raises if it cannot be loaded: no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"omega_b200 native library not found at {LIB_PATH}; "
+                                   "build it with `python -m omega_b200.build`")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, res, args in EXPORTS:
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            if L.omb_abi_version() != OMB_ABI_VERSION:
+                raise RuntimeError("omega_b200 native library ABI version mismatch")
+            _lib = L
+    return _lib
+
+
+def check(fn_name, status):
+    if status != 0:
+        msg = lib().omb_last_error().decode(errors="replace")
+        raise NativeError(fn_name, status, msg)
+
+
+def call(fn_name, *args):
+    """Calls an int-returning entry point and raises NativeError on failure."""
+    st = getattr(lib(), fn_name)(*args)
+    check(fn_name, st)
+    return st
+
+
+def f32_ptr(a: np.ndarray):
+    return a.ctypes.data_as(_c_float_p)
+
+
+def i64_ptr(a: np.ndarray):
+    return a.ctypes.data_as(_c_i64_p)

@@ -1,0 +1,282 @@
+// C-ABI entry points (include/omega_b200.h): handle life cycle, argument
+// validation and dispatch to the projector kernels.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace omb {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return set_error(OMB_ERR_CUDA, m);
+}
+
+}  // namespace omb
+
+using namespace omb;
+
+struct omb_handle {
+    int device = 0;
+    omb_geometry_desc desc{};
+    std::vector<int64_t> n_meas;  // cumulative sinograms/projections per subset
+    Grid grid{};
+    Tof tof{};
+    float *d_xy = nullptr;
+    float *d_z = nullptr;
+    float *d_tofc = nullptr;
+    unsigned long long *d_acc = nullptr;  // 2 * N int64 accumulators (fixed-point BP)
+    int64_t n_img = 0;
+};
+
+static int validate(const omb_geometry_desc *d) {
+    if (!d) return set_error(OMB_ERR_INVALID, "geometry descriptor is NULL");
+    if (d->struct_size != sizeof(omb_geometry_desc))
+        return set_error(OMB_ERR_INVALID, "omb_geometry_desc.struct_size does not match this library (" +
+                                              std::to_string(sizeof(omb_geometry_desc)) + " bytes)");
+    if (d->abi_version != OMB_ABI_VERSION) return set_error(OMB_ERR_INVALID, "unsupported abi_version");
+    if (d->modality != OMB_PET_SINOGRAM && d->modality != OMB_CT_PANEL)
+        return set_error(OMB_ERR_INVALID, "modality must be OMB_PET_SINOGRAM or OMB_CT_PANEL");
+    if (d->fp_type != 1) return set_error(OMB_ERR_UNSUPPORTED, "forward projector type " + std::to_string(d->fp_type) + " is not built");
+    if (d->bp_type != 1) return set_error(OMB_ERR_UNSUPPORTED, "backprojector type " + std::to_string(d->bp_type) + " is not built");
+    if (d->nx == 0 || d->ny == 0 || d->nz == 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (!(d->dx > 0.f) || !(d->dy > 0.f) || !(d->dz > 0.f)) return set_error(OMB_ERR_INVALID, "voxel size must be positive");
+    if (d->n_rows_d == 0 || d->n_cols_d == 0) return set_error(OMB_ERR_INVALID, "detector size must be positive");
+    if (d->n_proj <= 0) return set_error(OMB_ERR_INVALID, "n_proj must be positive");
+    if (d->n_subsets < 1) return set_error(OMB_ERR_INVALID, "n_subsets must be >= 1");
+    if (!d->n_meas) return set_error(OMB_ERR_INVALID, "n_meas is NULL");
+    if (!d->xy || !d->z) return set_error(OMB_ERR_INVALID, "xy/z coordinate arrays are NULL");
+    const bool meas_level = d->n_subsets > 1 && d->subset_type < 8;
+    if (meas_level) {
+        if (d->modality != OMB_PET_SINOGRAM)
+            return set_error(OMB_ERR_UNSUPPORTED, "measurement-level subset types are PET-only");
+        if (d->subset_type != 1 && d->subset_type != 2 && d->subset_type != 4 && d->subset_type != 5)
+            return set_error(OMB_ERR_UNSUPPORTED, "subset type " + std::to_string(d->subset_type) + " is not built");
+    }
+    const int64_t nbin = (int64_t)d->n_rows_d * d->n_cols_d;
+    if (d->modality == OMB_PET_SINOGRAM) {
+        if (d->n_xy != nbin * 4) return set_error(OMB_ERR_INVALID, "PET xy must hold 4 floats per sinogram bin");
+        if (d->n_z != d->n_proj * 2) return set_error(OMB_ERR_INVALID, "PET z must hold 2 floats per sinogram");
+    } else {
+        if (d->n_xy != d->n_proj * 6) return set_error(OMB_ERR_INVALID, "CT xy must hold 6 floats per projection");
+        if (d->n_z != d->n_proj * 2) return set_error(OMB_ERR_INVALID, "CT z must hold 2 floats per projection");
+    }
+    if (d->tof_bins < 1) return set_error(OMB_ERR_INVALID, "tof_bins must be >= 1");
+    if (d->tof_bins > kMaxTofBins) return set_error(OMB_ERR_UNSUPPORTED, "TOF bin count above 16 is not built");
+    if (d->tof_bins > 1) {
+        if (!d->tof_centers) return set_error(OMB_ERR_INVALID, "tof_centers is NULL");
+        if (!(d->sigma_x > 0.f)) return set_error(OMB_ERR_INVALID, "TOF sigma must be positive");
+        if (d->modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_INVALID, "TOF is PET-only");
+    }
+    const int64_t *nm = d->n_meas;
+    if (nm[0] != 0) return set_error(OMB_ERR_INVALID, "n_meas[0] must be 0");
+    for (int s = 0; s < d->n_subsets; ++s)
+        if (nm[s + 1] < nm[s]) return set_error(OMB_ERR_INVALID, "n_meas must be non-decreasing");
+    if (!meas_level && nm[d->n_subsets] != d->n_proj)
+        return set_error(OMB_ERR_INVALID, "n_meas[n_subsets] must equal n_proj");
+    return OMB_OK;
+}
+
+// Rays of one call: a subset, or every subset when subset == -1.
+static int ray_set(const omb_handle *h, int32_t subset, RaySet &rs) {
+    const omb_geometry_desc &d = h->desc;
+    if (subset < -1 || subset >= d.n_subsets)
+        return set_error(OMB_ERR_INVALID, "subset " + std::to_string(subset) + " out of range");
+    rs.xy = h->d_xy;
+    rs.z = h->d_z;
+    rs.modality = d.modality;
+    rs.n_rows = (int)d.n_rows_d;
+    rs.n_cols = (int)d.n_cols_d;
+    rs.pitch_x = d.dpitch_x;
+    rs.pitch_y = d.dpitch_y;
+    rs.n_subsets = d.n_subsets;
+    const int64_t nbin = (int64_t)d.n_rows_d * d.n_cols_d;
+    const bool meas_level = d.n_subsets > 1 && d.subset_type < 8;
+    if (meas_level) {
+        if (subset < 0) return set_error(OMB_ERR_UNSUPPORTED, "subset -1 needs a whole-sinogram subset type");
+        rs.stype = d.subset_type;
+        rs.cur_subset = subset;
+        rs.proj0 = 0;
+        rs.n_proj = d.n_proj;
+        rs.m_size = h->n_meas[subset + 1] - h->n_meas[subset];
+    } else {
+        rs.stype = 0;
+        rs.cur_subset = subset < 0 ? 0 : subset;
+        rs.proj0 = subset < 0 ? 0 : h->n_meas[subset];
+        rs.n_proj = subset < 0 ? d.n_proj : h->n_meas[subset + 1] - h->n_meas[subset];
+        rs.m_size = rs.n_proj * nbin;
+    }
+    return OMB_OK;
+}
+
+extern "C" {
+
+int omb_abi_version(void) { return OMB_ABI_VERSION; }
+
+const char *omb_last_error(void) { return g_last_error.c_str(); }
+
+int omb_create(const omb_geometry_desc *desc, omb_handle **out) {
+    if (!out) return set_error(OMB_ERR_INVALID, "output handle pointer is NULL");
+    *out = nullptr;
+    int st = validate(desc);
+    if (st != OMB_OK) return st;
+    omb_handle *h = new omb_handle();
+    h->desc = *desc;
+    h->desc.xy = nullptr;
+    h->desc.z = nullptr;
+    h->desc.tof_centers = nullptr;
+    h->desc.n_meas = nullptr;
+    h->n_meas.assign(desc->n_meas, desc->n_meas + desc->n_subsets + 1);
+    cudaGetDevice(&h->device);
+    Grid &g = h->grid;
+    g.nx = (int)desc->nx; g.ny = (int)desc->ny; g.nz = (int)desc->nz;
+    g.dx = desc->dx; g.dy = desc->dy; g.dz = desc->dz;
+    g.bx = desc->bx; g.by = desc->by; g.bz = desc->bz;
+    // bmax = b + N*d in float32, as the reference's host code forms it (projfunctions.py:397-399)
+    g.mx = desc->bx + (float)desc->nx * desc->dx;
+    g.my = desc->by + (float)desc->ny * desc->dy;
+    g.mz = desc->bz + (float)desc->nz * desc->dz;
+    h->n_img = (int64_t)desc->nx * desc->ny * desc->nz;
+    Tof &t = h->tof;
+    t.nbins = desc->tof_bins;
+    t.epps = desc->epps;
+    t.sigma_inv = desc->tof_bins > 1 ? 1.f / desc->sigma_x : 0.f;
+    t.sigma_coef = 0.3989423f * t.sigma_inv;
+    auto fail = [&](int code) {
+        omb_destroy(h);
+        return code;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&h->d_xy, desc->n_xy * sizeof(float))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc xy"));
+    if ((e = cudaMalloc(&h->d_z, desc->n_z * sizeof(float))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc z"));
+    if ((e = cudaMemcpy(h->d_xy, desc->xy, desc->n_xy * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(cuda_fail(e, "upload xy"));
+    if ((e = cudaMemcpy(h->d_z, desc->z, desc->n_z * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(cuda_fail(e, "upload z"));
+    if ((e = cudaMalloc(&h->d_tofc, kMaxTofBins * sizeof(float))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc tof"));
+    if ((e = cudaMemset(h->d_tofc, 0, kMaxTofBins * sizeof(float))) != cudaSuccess) return fail(cuda_fail(e, "clear tof"));
+    if (desc->tof_bins > 1 &&
+        (e = cudaMemcpy(h->d_tofc, desc->tof_centers, desc->tof_bins * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(cuda_fail(e, "upload tof centres"));
+    t.centers = h->d_tofc;
+    if (desc->fixed64_workspace) {
+        if ((e = cudaMalloc(&h->d_acc, 2 * h->n_img * sizeof(unsigned long long))) != cudaSuccess)
+            return fail(cuda_fail(e, "cudaMalloc fixed-point accumulators"));
+    }
+    *out = h;
+    return OMB_OK;
+}
+
+int omb_destroy(omb_handle *h) {
+    if (!h) return OMB_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != h->device) cudaSetDevice(h->device);
+    cudaFree(h->d_xy);
+    cudaFree(h->d_z);
+    cudaFree(h->d_tofc);
+    cudaFree(h->d_acc);
+    if (prev != h->device) cudaSetDevice(prev);
+    delete h;
+    return OMB_OK;
+}
+
+int64_t omb_measurement_count(const omb_handle *h, int32_t subset) {
+    if (!h) return -1;
+    RaySet rs{};
+    if (ray_set(h, subset, rs) != OMB_OK) return -1;
+    return rs.m_size * h->desc.tof_bins;
+}
+
+int64_t omb_image_count(const omb_handle *h) { return h ? h->n_img : -1; }
+
+int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!image || !y) return set_error(OMB_ERR_INVALID, "image/y pointer is NULL");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, image, y, (cudaStream_t)stream);
+}
+
+int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, float *sens, int32_t mode,
+                 void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!image || !y) return set_error(OMB_ERR_INVALID, "image/y pointer is NULL");
+    if (mode != OMB_BP_FLOAT_ATOMIC && mode != OMB_BP_FIXED64) return set_error(OMB_ERR_INVALID, "unknown backprojection mode");
+    if (mode == OMB_BP_FIXED64 && !h->d_acc)
+        return set_error(OMB_ERR_INVALID, "fixed-point backprojection needs a handle created with fixed64_workspace");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nb = h->n_img * sizeof(float);
+    if (mode == OMB_BP_FIXED64) {
+        unsigned long long *acc = h->d_acc, *acc_s = sens ? h->d_acc + h->n_img : nullptr;
+        OMB_CUDA_TRY(cudaMemsetAsync(h->d_acc, 0, (sens ? 2 : 1) * h->n_img * sizeof(unsigned long long), s));
+        st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, y, nullptr, nullptr, acc, acc_s, mode, s);
+        if (st != OMB_OK) return st;
+        st = fixed_to_float(acc, image, h->n_img, s);
+        if (st == OMB_OK && sens) st = fixed_to_float(acc_s, sens, h->n_img, s);
+        return st;
+    }
+    OMB_CUDA_TRY(cudaMemsetAsync(image, 0, nb, s));
+    if (sens) OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, nb, s));
+    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, y, image, sens, nullptr, nullptr, mode, s);
+}
+
+int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!sens) return set_error(OMB_ERR_INVALID, "sens pointer is NULL");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    // A^T 1 through the BP kernel's fused sensitivity accumulator, y = NULL.
+    OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, h->n_img * sizeof(float), s));
+    st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, nullptr, nullptr, sens, nullptr, nullptr,
+                         OMB_BP_FLOAT_ATOMIC, s);
+    if (st != OMB_OK) return st;
+    return clamp_min(sens, h->n_img, h->desc.epps, s);
+}
+
+int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
+                    float *work_meas, float *work_img, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!image || !y_subset || !sens || !work_meas || !work_img)
+        return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osem_subset");
+    if (h->desc.modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const float eps = h->desc.epps;
+    st = siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, image, work_meas, s);
+    if (st != OMB_OK) return st;
+    st = osem_ratio(y_subset, work_meas, rs.m_size * h->desc.tof_bins, eps, s);
+    if (st != OMB_OK) return st;
+    OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
+    st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, work_meas, work_img, nullptr, nullptr, nullptr,
+                         OMB_BP_FLOAT_ATOMIC, s);
+    if (st != OMB_OK) return st;
+    return em_update(image, sens, work_img, h->n_img, eps, s);
+}
+
+int omb_loglik(const float *y, const float *fp, int64_t n, float epps, double *out_host, void *work, void *stream) {
+    if (!y || !fp) return set_error(OMB_ERR_INVALID, "y/fp pointer is NULL");
+    if (n < 0) return set_error(OMB_ERR_INVALID, "n must be >= 0");
+    return loglik(y, fp, n, epps, out_host, work, (cudaStream_t)stream);
+}
+
+size_t omb_reduce_workspace_bytes(int64_t n) { return reduce_workspace_bytes(n); }
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// Shared host/device definitions of the omega_b200 projector library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/omega_b200.h"
+
+namespace omb {
+
+// Records `msg` as the calling thread's last error and returns `code`.
+int set_error(int code, const std::string &msg);
+// Turns a CUDA error into OMB_ERR_CUDA with a message naming `what`.
+int cuda_fail(cudaError_t e, const char *what);
+
+#define OMB_CUDA_TRY(call)                                   \
+    do {                                                     \
+        cudaError_t _e = (call);                             \
+        if (_e != cudaSuccess) return ::omb::cuda_fail(_e, #call); \
+    } while (0)
+
+#define OMB_LAUNCH_CHECK(what)                                  \
+    do {                                                        \
+        cudaError_t _e = cudaGetLastError();                    \
+        if (_e != cudaSuccess) return ::omb::cuda_fail(_e, what); \
+    } while (0)
+
+// Voxel grid of one image volume.
+struct Grid {
+    int nx, ny, nz;
+    float dx, dy, dz;
+    float bx, by, bz;     // lower FOV corner
+    float mx, my, mz;     // upper FOV corner b + N*d
+};
+
+// Where one launch's rays come from.  A launch covers `n_proj` consecutive
+// sinograms/projections starting at global position `proj0` (subset order),
+// or, for measurement-level PET subsets (types 1, 2, 4, 5), `m_size`
+// measurements of subset `cur_subset` spread over the whole sinogram.
+struct RaySet {
+    const float *xy;
+    const float *z;
+    int modality;       // omb_modality
+    int n_rows;         // Ndist / detector rows
+    int n_cols;         // Nang / detector columns
+    int64_t proj0;
+    int64_t n_proj;
+    int64_t m_size;     // rays in this launch (TOF bin stride)
+    int stype;          // 0: whole sinograms; 1, 2, 4, 5: measurement-level
+    int n_subsets;
+    int cur_subset;
+    float pitch_x, pitch_y;
+};
+
+struct Tof {
+    int nbins;
+    float sigma_inv;
+    float sigma_coef;   // 1/sqrt(2 pi) / sigma
+    float epps;
+    const float *centers;
+};
+
+constexpr int kMaxTofBins = 16;
+constexpr int kBlock = 256;
+
+inline int num_sms() {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+// Grid size for a grid-stride kernel over `n` items: at most `per_sm`
+// resident blocks on every SM.
+inline unsigned grid_for(int64_t n, int per_sm = 8, int block = kBlock) {
+    int64_t need = (n + block - 1) / block;
+    int64_t cap = (int64_t)num_sms() * per_sm;
+    if (need < 1) need = 1;
+    return (unsigned)(need < cap ? need : cap);
+}
+
+}  // namespace omb

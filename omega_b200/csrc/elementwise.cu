@@ -1,0 +1,134 @@
+// Elementwise and reduction steps of the OSEM subset update.
+//
+// ratio:  computeForwardProject.h:20-21 (input += epps), 92-95 (y / input),
+//         400-401 (NaN/Inf -> epps)
+// EM:     algorithms.h:12-15 via subiterStep.h:118-121 (im / Summ * (rhs + epps))
+// clamp:  functions.hpp:2980-2996 (Summ < epps -> epps)
+// All are HBM-bound streams: float4 loads/stores where the pointers allow.
+#include "kernels.h"
+
+namespace omb {
+
+__device__ __forceinline__ float ratio1(float y, float f, float epps) {
+    float r = y / (f + epps);
+    if (isnan(r) || isinf(r)) r = epps;
+    return r;
+}
+
+__global__ void k_osem_ratio(const float *__restrict__ y, float *__restrict__ fp, int64_t n, float epps) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t n4 = n / 4;
+    const float4 *y4 = reinterpret_cast<const float4 *>(y);
+    float4 *f4 = reinterpret_cast<float4 *>(fp);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        const float4 a = __ldg(y4 + i);
+        float4 b = f4[i];
+        b.x = ratio1(a.x, b.x, epps);
+        b.y = ratio1(a.y, b.y, epps);
+        b.z = ratio1(a.z, b.z, epps);
+        b.w = ratio1(a.w, b.w, epps);
+        f4[i] = b;
+    }
+    for (int64_t i = n4 * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        fp[i] = ratio1(y[i], fp[i], epps);
+}
+
+__global__ void k_em_update(float *__restrict__ img, const float *__restrict__ sens, const float *__restrict__ rhs,
+                            int64_t n, float epps) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        img[i] = img[i] / __ldg(sens + i) * (__ldg(rhs + i) + epps);
+}
+
+__global__ void k_clamp_min(float *__restrict__ x, int64_t n, float lo) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (x[i] < lo) x[i] = lo;
+}
+
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+int osem_ratio(const float *y, float *fp, int64_t n, float epps, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    if (!aligned16(y) || !aligned16(fp)) return set_error(OMB_ERR_INVALID, "osem ratio buffers must be 16-byte aligned");
+    k_osem_ratio<<<grid_for(n / 4 + 1, 4), kBlock, 0, st>>>(y, fp, n, epps);
+    OMB_LAUNCH_CHECK("osem ratio launch");
+    return OMB_OK;
+}
+
+int em_update(float *img, const float *sens, const float *rhs, int64_t n, float epps, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_em_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, sens, rhs, n, epps);
+    OMB_LAUNCH_CHECK("EM update launch");
+    return OMB_OK;
+}
+
+int clamp_min(float *x, int64_t n, float lo, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_clamp_min<<<grid_for(n, 4), kBlock, 0, st>>>(x, n, lo);
+    OMB_LAUNCH_CHECK("clamp launch");
+    return OMB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Poisson log-likelihood in FP64: two-pass block reduction (partials in the
+// caller's workspace, then one block folds them), no atomics, so the result
+// is identical run to run.
+// ---------------------------------------------------------------------------
+
+constexpr int kRedBlocks = 1184;  // 8 x 148 SMs
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[kBlock / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    v = threadIdx.x < kBlock / 32 ? sh[threadIdx.x] : 0.0;
+    if (wid == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kBlock) k_loglik_partial(const float *__restrict__ y, const float *__restrict__ fp,
+                                                           int64_t n, float epps, double *__restrict__ part) {
+    double acc = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double f = (double)__ldg(fp + i) + (double)epps;
+        const double yy = (double)__ldg(y + i);
+        acc += (yy != 0.0 ? yy * log(f) : 0.0) - f;
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(kBlock) k_sum_partials(const double *__restrict__ part, int n,
+                                                         double *__restrict__ out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+
+size_t reduce_workspace_bytes(int64_t) { return (size_t)(kRedBlocks + 1) * sizeof(double); }
+
+int loglik(const float *y, const float *fp, int64_t n, float epps, double *out_host, void *work, cudaStream_t st) {
+    if (!work) return set_error(OMB_ERR_INVALID, "loglik workspace is NULL");
+    if (!out_host) return set_error(OMB_ERR_INVALID, "loglik output pointer is NULL");
+    double *part = static_cast<double *>(work);
+    int blocks = (int)grid_for(n, 8);
+    if (blocks > kRedBlocks) blocks = kRedBlocks;
+    k_loglik_partial<<<blocks, kBlock, 0, st>>>(y, fp, n, epps, part);
+    OMB_LAUNCH_CHECK("loglik partial launch");
+    k_sum_partials<<<1, kBlock, 0, st>>>(part, blocks, part + kRedBlocks);
+    OMB_LAUNCH_CHECK("loglik fold launch");
+    OMB_CUDA_TRY(cudaMemcpyAsync(out_host, part + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, st));
+    OMB_CUDA_TRY(cudaStreamSynchronize(st));
+    return OMB_OK;
+}
+
+}  // namespace omb

@@ -1,0 +1,584 @@
+"""Drop-in ``projectorClass`` for OMEGA's matrix-free projector path.
+
+Mirrors ``omegatomo.projector.proj.projectorClass`` (omegatomo/projector/proj.py:36)
+for the projector path: users set the same attributes, call ``addProjector()``
+(proj.py:520) and ``initProj()`` (proj.py:1913), then project with
+``forwardProject(f, subset)`` / ``backwardProject(y, subset)``
+(proj.py:1923-1933) or the operator sugar ``A * f`` and ``A.T() * y``
+(proj.py:1936-1951).  Inputs and outputs are flat float32 CUDA torch tensors
+(image Fortran order, length Nx*Ny*Nz; measurements of one subset in
+sinogram order, length nRowsD*nColsD*nProjSubset[k] times the TOF bins).
+
+Differences from the reference surface:
+ * every call is stream-ordered on ``torch.cuda.current_stream()``; nothing
+   synchronises (the reference synchronises after each call,
+   projfunctions.py:435-436) -- ``.cpu()`` or ``torch.cuda.synchronize()`` is
+   the caller's sync point;
+ * ``use_64bit_atomics = True`` selects the bit-deterministic int64
+   fixed-point backprojection on CUDA (the reference only offers it on
+   OpenCL and forces it off on CUDA, init.py:251-254);
+ * with TOF the forward projection returns all bins of the subset
+   ([bin0 rays, bin1 rays, ...]); the reference's Python path sizes the output
+   for one bin only.
+The kernels run in the native library (``omega_b200/lib/libomega_b200.so``);
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from .. import _native
+from . import geometry as geo
+
+
+class projectorClass:
+    # Image and FOV
+    x = np.empty(0, dtype=np.float32)
+    y = np.empty(0, dtype=np.float32)
+    z = np.empty(0, dtype=np.float32)
+    x0 = np.empty(0, dtype=np.float32)
+    Nx = 1
+    Ny = 1
+    Nz = 1
+    FOVa_x = 0.
+    FOVa_y = 0.
+    axial_fov = 0.
+    oOffsetX = 0.
+    oOffsetY = 0.
+    oOffsetZ = 0.
+    flip_image = False
+    offangle = 0.
+    # PET scanner
+    cryst_per_block = np.empty(0, dtype=np.uint32)
+    cryst_per_block_axial = cryst_per_block
+    transaxial_multip = 1
+    blocks_per_ring = 1
+    linear_multip = 0
+    diameter = 0.
+    cr_p = 0.
+    cr_pz = 0.
+    DOI = 0.
+    rings = 0
+    det_per_ring = 0
+    det_w_pseudo = 0
+    detectors = 0
+    pseudot = np.empty(0, dtype=np.uint32)
+    ringGaps = np.empty(0, dtype=np.int32)
+    nLayers = 1
+    # Sinogram
+    span = 3
+    ring_difference = 0
+    Ndist = 400
+    Nang = 1
+    NSinos = 1      # proj.py declares NSinos twice; the later default (1) wins
+    TotSinos = 0
+    segment_table = np.empty(0, dtype=np.float32)
+    ndist_side = 1
+    sampling = 1
+    use_raw_data = 0
+    arc_correction = False
+    # CT / panel
+    CT = False
+    PET = False
+    SPECT = False
+    nProjections = 1
+    nRowsD = 0
+    nColsD = 0
+    dPitchX = 0.
+    dPitchY = 0.
+    angles = np.empty(0, dtype=np.float32)
+    sourceToCRot = 1.
+    sourceToDetector = 1.
+    sourceOffsetCol = np.zeros(1, dtype=np.float32)
+    sourceOffsetRow = np.zeros(1, dtype=np.float32)
+    detOffsetRow = np.zeros(1, dtype=np.float32)
+    detOffsetCol = np.zeros(1, dtype=np.float32)
+    bedOffset = np.empty(0, dtype=np.float32)
+    pitchRoll = np.empty(0, dtype=np.float32)
+    uV = np.empty(0, dtype=np.float32)
+    nBed = 1
+    flat = 0.
+    pitch = False
+    useHelical = False
+    # TOF
+    TOF = False
+    TOF_bins = 1
+    TOF_bins_used = 1
+    TOF_FWHM = 0.
+    TOF_width = 0.
+    TOF_offset = 0.
+    TOFCenter = np.empty(0, dtype=np.float32)
+    sigma_x = 0.
+    # Projector
+    projector_type = 11
+    n_rays_transaxial = 1
+    n_rays_axial = 1
+    dL = 0
+    useTotLength = True
+    useImages = True
+    useMAD = True
+    meanFP = False
+    meanBP = False
+    use_psf = False
+    use_64bit_atomics = False
+    use_32bit_atomics = False
+    global_factor = 1.
+    epps = 1e-5
+    # Subsets / reconstruction
+    subsets = 1
+    subsetType = 8
+    subset = 0
+    seed = -1
+    Niter = 4
+    partitions = 1
+    Nt = 1
+    listmode = 0
+    useIndexBasedReconstruction = False
+    SinM = np.empty(0, dtype=np.float32)
+    verbose = 1
+    # Corrections (not on this path; must stay off)
+    attenuation_correction = 0
+    normalization_correction = 0
+    randoms_correction = 0
+    scatter_correction = 0
+    additionalCorrection = 0
+    maskFP = np.empty(0, dtype=np.uint8)
+    maskBP = np.empty(0, dtype=np.uint8)
+    # Execution flags of the reference surface (accepted for compatibility)
+    useTorch = True
+    useCUDA = True
+    useCuPy = False
+    useAF = False
+    useCPU = False
+    deviceNum = 0
+    largeDim = False
+    nMultiVolumes = 0
+    trans = False
+    projectorAdded = False
+    projectorInitialized = False
+
+    def __init__(self):
+        self._handle = None
+        self._device = None
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None:
+            try:
+                _native.lib().omb_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+    # ------------------------------------------------------------------
+    # Geometry (proj.py:520-1066)
+    # ------------------------------------------------------------------
+    def addProjector(self):
+        """Validates the options and computes the detector coordinates,
+        subset indices, voxel grid and projector scales (proj.py:520-1066)."""
+        self.projectorAdded = True
+        if hasattr(self, 'dPitch') and self.dPitch > 0 and self.dPitchX == 0.:
+            self.dPitchX = self.dPitch
+        if hasattr(self, 'dPitch') and self.dPitch > 0 and self.dPitchY == 0.:
+            self.dPitchY = self.dPitch
+        if self.CT:
+            self._ct_setup()
+        cpb_empty = isinstance(self.cryst_per_block_axial, np.ndarray) and self.cryst_per_block_axial.size == 0
+        cpb_set = (isinstance(self.cryst_per_block, np.ndarray) and self.cryst_per_block.size > 0) or (
+            not isinstance(self.cryst_per_block, np.ndarray) and self.cryst_per_block > 0)
+        if cpb_empty and cpb_set:
+            self.cryst_per_block_axial = self.cryst_per_block
+        if self.rings == 0 and not isinstance(self.cryst_per_block_axial, np.ndarray) and \
+                self.cryst_per_block_axial >= 1 and self.linear_multip >= 1:
+            self.rings = self.cryst_per_block_axial * self.linear_multip
+        if self.dPitchX > 0. and self.dPitchY == 0.:
+            self.dPitchY = self.dPitchX
+        if self.cr_p > 0. and self.cr_pz == 0.:
+            self.cr_pz = self.cr_p
+        if self.cr_p == 0. and self.dPitchX > 0.:
+            self.cr_p = self.dPitchX
+        if self.cr_pz == 0. and self.dPitchY > 0.:
+            self.cr_pz = self.dPitchY
+        if self.axial_fov == 0. and (self.cr_pz > 0. or self.dPitchY > 0.):
+            self.axial_fov = self.dPitchY if self.dPitchY > 0. else self.cr_pz
+        if self.det_per_ring == 0 and self.blocks_per_ring >= 1 and not isinstance(self.cryst_per_block, np.ndarray) \
+                and self.cryst_per_block >= 1:
+            self.det_per_ring = self.blocks_per_ring * self.cryst_per_block
+        if self.det_w_pseudo == 0:
+            self.det_w_pseudo = self.det_per_ring
+        if self.detectors == 0:
+            self.detectors = self.det_w_pseudo * self.rings
+        if self.ring_difference == 0 and self.rings > 0:
+            self.ring_difference = self.rings - 1
+        if self.segment_table.size == 0 and self.span > 0 and self.rings > 0:
+            self.segment_table = geo.default_segment_table(self.rings, self.span, self.ring_difference, self._n(self.Nz))
+        if self.Nang == 1 and self.det_per_ring > 1:
+            self.Nang = self.det_per_ring // 2
+        if self.span == 1:
+            self.TotSinos = self.rings ** 2
+            self.NSinos = self.TotSinos
+        elif self.NSinos == 0:
+            self.NSinos = int(np.sum(self.segment_table))
+        if self.TotSinos == 0:
+            self.TotSinos = self.NSinos
+        self.OMEGAErrorCheck()
+        self.TOF = self.TOF_bins > 1 and self.projector_type in (1, 11, 3, 33, 13, 31, 4, 14, 41, 44, 34, 43)
+        if self.TOF:
+            if self.TOF_bins_used == 0 and self.TOF_bins > 0:
+                self.TOF_bins_used = self.TOF_bins
+            if self.TOF_bins_used != self.TOF_bins:
+                self.sigma_x = 0.
+            elif self.TOFCenter.size == 0:
+                self.sigma_x = geo.tof_sigma(self.TOF_FWHM)
+                self.TOFCenter = geo.tof_centers(self.TOF_width, self.TOF_bins, self.TOF_offset)
+            else:
+                self.TOFCenter = np.float32(self.TOFCenter)
+        else:
+            self.sigma_x = 0.
+        if self.maskFP.size > 1 or self.maskBP.size > 1:
+            raise ValueError('Forward/backward projection masks are not supported by this projector build')
+        if isinstance(self.partitions, np.ndarray):
+            if self.partitions.size >= 1:
+                self.Nt = self.partitions.size
+        else:
+            self.Nt = self.partitions
+        if self.Nt > 1 and self.subsetType == 3:
+            raise ValueError('Subset type 3 is not supported with dynamic data!')
+        self.listmode = 0
+        if (not self.CT and not self.SPECT) and (((self.subsetType > 7 or (self.subsetType == 0 and self.listmode == 0))
+                                                   and self.subsets > 1) or self.subsets == 1):
+            self.nProjections = self.NSinos
+            self.PET = True
+        else:
+            self.PET = False
+            self.nProjections = self.NSinos
+        self.index, self.nMeas = geo.subset_indices(self)
+        self.x0 = np.asarray(self.x0).ravel('F')
+        if self.CT and self.projector_type == 11 and not self.useCPU:
+            self.projector_type = 4
+        if self.CT:
+            x_det, z_det = self.x, self.z
+        else:
+            x_det, z_det = geo.pet_sinogram_coordinates(self)
+            self.dPitch = self.cr_p
+            self.dPitchY = self.cr_p
+            self.dPitchX = self.cr_pz
+            self.nProjections = self.NSinos
+            self.nRowsD = self.Ndist
+            self.nColsD = self.Nang
+        self.nMeas = np.insert(np.cumsum(self.nMeas), 0, 0)
+        for nm in ('Nx', 'Ny', 'Nz'):
+            if not isinstance(getattr(self, nm), np.ndarray):
+                setattr(self, nm, np.array(getattr(self, nm), dtype=np.uint32, ndmin=1))
+        self.dx, self.dy, self.dz, self.bx, self.by, self.bz = geo.voxel_grid(self)
+        if self.subsetType >= 8 and self.subsets > 1:
+            if self.CT:
+                x_det = np.reshape(x_det, (self.nProjections, 6))[self.index, :].ravel('C')
+                z_det = np.reshape(z_det, (self.nProjections, 2))[self.index, :].ravel('C')
+                self.uV = self.uV[self.index, :]
+            else:
+                z_det = np.reshape(z_det, (self.nProjections, -1))[self.index, :].ravel('C')
+        self.x = x_det
+        self.z = z_det
+        self.x_center = np.array(self.bx[0].item(), ndmin=1).astype(np.float32)
+        self.y_center = np.array(self.by[0].item(), ndmin=1).astype(np.float32)
+        self.z_center = np.array(self.bz[0].item(), ndmin=1).astype(np.float32)
+        if self.projector_type in (4, 5, 14, 41, 15, 45, 54, 51, 42, 43, 24, 34):
+            geo.projector_scaling(self)
+        if self.nMeas.size == 1:
+            self.nMeas = np.insert(self.nMeas, 0, 0)
+        if self.subsets > 1:
+            self.subset = 0
+        kerroin = self.nColsD * self.nRowsD if (self.subsetType >= 8 or self.subsets == 1) else 1
+        self.nMeasSubset = np.zeros((self.subsets, 1), dtype=np.int64)
+        self.nProjSubset = np.zeros((self.subsets, 1), dtype=np.int64)
+        self.nTotMeas = self.nMeas * kerroin
+        for kk in range(self.subsets):
+            self.nMeasSubset[kk] = self.nMeas[kk + 1] * kerroin - self.nMeas[kk] * kerroin
+            self.nProjSubset[kk] = self.nMeas[kk + 1] - self.nMeas[kk]
+        self.N = self.Nx.astype(np.uint64) * self.Ny.astype(np.uint64) * self.Nz.astype(np.uint64)
+        for nm in ('FOVa_x', 'FOVa_y', 'axial_fov'):
+            if not isinstance(getattr(self, nm), np.ndarray):
+                setattr(self, nm, np.array(getattr(self, nm), dtype=np.float32, ndmin=1))
+        if self.use_32bit_atomics and self.use_64bit_atomics:
+            self.use_64bit_atomics = False
+        self.x0 = self.x0.astype(dtype=np.float32)
+        self.x = np.asarray(self.x).astype(dtype=np.float32)
+        self.z = np.asarray(self.z).astype(dtype=np.float32)
+
+    @staticmethod
+    def _n(v):
+        return int(np.asarray(v).ravel()[0])
+
+    def _ct_setup(self):
+        """CT branch of addProjector (proj.py:528-568) and setCTCoordinates."""
+        if not hasattr(self, 'nProjections') or self.nProjections == 0:
+            self.nProjections = self.NSinos
+        else:
+            self.NSinos = self.nProjections
+        self.NSinos = self.nProjections
+        self.TotSinos = self.nProjections
+        self.span = 3
+        if self.nRowsD == 0:
+            self.nRowsD = self.Ndist
+        else:
+            self.Ndist = self.nRowsD
+        if self.nColsD == 0:
+            self.nColsD = self.Nang
+        else:
+            self.Nang = self.nColsD
+        self.use_raw_data = 0
+        self.attenuation_correction = 0
+        self.normalization_correction = 0
+        self.rings = self.nColsD * self.nBed
+        self.det_per_ring = self.nRowsD * self.nProjections
+        self.arc_correction = False
+        self.det_w_pseudo = self.det_per_ring
+        self.cryst_per_block = self.nColsD * self.nRowsD
+        if hasattr(self, 'dPitch') and self.dPitch > 0:
+            self.cr_pz = self.dPitch
+            self.cr_p = self.dPitch
+        else:
+            self.cr_pz = self.dPitchY
+            self.cr_p = self.dPitchX
+        self.angles = np.asarray(self.angles)
+        if np.max(np.abs(self.angles.flatten())) > 6. * np.pi:
+            self.angles = self.angles * (np.pi / 180.)
+        if self.offangle > 0:
+            self.angles = self.angles + self.offangle
+        if self.subsets > 1 and 0 < self.subsetType < 8:
+            raise ValueError('Subset types < 8 with CT data are not yet supported in Python! Use custom detector '
+                             'coordinates instead or subset types >= 8.')
+        if self.pitchRoll.size > 0 or self.useHelical or self.bedOffset.size > 0:
+            raise ValueError('pitch/roll, helical and multi-bed CT geometries are not supported by this build')
+        self.x, self.z, self.uV = geo.ct_source_detector(self)
+
+    def OMEGAErrorCheck(self):
+        """Option checks of the projector path (proj.py:1068-1283); the same
+        conditions raise ValueError with the reference's messages."""
+        if self.FOVa_x > 0 and self.FOVa_y == 0:
+            self.FOVa_y = self.FOVa_x
+        if not self.CT and not self.SPECT and self.span > self.ring_difference and self.NSinos > 1 and not self.use_raw_data:
+            raise ValueError(f"Span value cannot be larger than ring difference ({self.ring_difference})!")
+        if not self.CT and not self.SPECT and (self.span % 2 == 0 or self.span <= 0) and not self.use_raw_data:
+            raise ValueError("Span value has to be odd and positive!")
+        if not self.CT and not self.SPECT and self.ring_difference >= self.rings and not self.use_raw_data and self.rings > 0:
+            self.ring_difference = self.rings - 1
+        if not self.CT and not self.SPECT and self.ring_difference < 0 and not self.use_raw_data:
+            raise ValueError("Ring difference has to be at least 0!")
+        if not self.CT and not self.SPECT and self.Nang > self.det_w_pseudo / 2 and not self.use_raw_data and self.Nang > 1:
+            raise ValueError(f"Number of sinogram angles can be at most the number of detectors per ring divided by two ({self.det_w_pseudo / 2})!")
+        if not self.CT and not self.SPECT and self.TotSinos < self.NSinos and not self.use_raw_data and self.TotSinos > 0:
+            self.TotSinos = self.NSinos
+        if not self.CT and not self.SPECT and (self.ndist_side > 1 and self.Ndist % 2 == 0 or self.ndist_side < -1 and self.Ndist % 2 == 0) and not self.use_raw_data:
+            raise ValueError("ndist_side can be either 1 or -1!")
+        if not self.CT and not self.SPECT and self.ndist_side == 0 and self.Ndist % 2 == 0 and not self.use_raw_data:
+            raise ValueError("ndist_side cannot be 0 when Ndist is even!")
+        if self.Niter < 1:
+            self.Niter = 1
+        if self.subsets < 1:
+            self.subsets = 1
+        if self.projector_type not in [1, 2, 3, 4, 5, 6, 11, 14, 12, 13, 21, 22, 23, 24, 31, 32, 33, 34, 41, 42, 43,
+                                       44, 45, 51, 15, 54, 55]:
+            raise ValueError('The selected projector type is not supported!')
+        if self.epps <= 0:
+            self.epps = 1e-6
+        if self.projector_type in [5, 15, 51, 45, 54] and not self.CT:
+            raise ValueError('Projector type 5 is only supported with CT data!')
+        if self.useCUDA and self.useCPU:
+            raise ValueError('Both CUDA and CPU selected! Select only one!')
+        if self.TOF_bins_used > 1 and (self.projector_type not in [1, 11, 3, 33, 31, 13, 4, 41, 14, 43, 34]) and not self.CT and not self.SPECT:
+            raise ValueError('TOF is currently only supported with improved Siddon (projector_type = 1), interpolation-based projector (projector_type = 4) and volume of intersection (projector_type = 3)')
+        if self.TOF_bins_used > 1 and self.TOF_width <= 0 and not self.CT and not self.SPECT:
+            raise ValueError('TOF width (self.TOF_width) must be greater than zero.')
+        if self.TOF_bins_used > 1 and self.TOF_FWHM == 0 and not self.CT and not self.SPECT:
+            raise ValueError('TOF enabled, but the TOF FWHM (self.TOF_FWHM) is zero. FWHM must be nonzero.')
+        if not self.largeDim and not np.asarray(self.x0).any():
+            fill = 1e-4 if self.CT else 1.
+            self.x0 = np.ones((self._n(self.Nx), self._n(self.Ny), self._n(self.Nz)), dtype=np.float32, order='F') * fill
+        if not self.largeDim and np.asarray(self.x0).size < self._n(self.Nx) * self._n(self.Ny) * self._n(self.Nz):
+            raise ValueError(f"Initial value has a matrix size smaller ({np.prod(np.shape(self.x0))}) than the actual image size ({self._n(self.Nx)*self._n(self.Ny)*self._n(self.Nz)})!")
+
+    # ------------------------------------------------------------------
+    # Device set-up (init.py:39-703)
+    # ------------------------------------------------------------------
+    def _fp_bp_types(self):
+        pt = self.projector_type
+        fp = {1: 1, 11: 1, 14: 1, 15: 1, 12: 1, 13: 1, 4: 4, 41: 4, 42: 4, 43: 4, 44: 4, 45: 4,
+              5: 5, 51: 5, 52: 5, 53: 5, 54: 5, 55: 5}.get(pt)
+        bp = {1: 1, 11: 1, 21: 1, 31: 1, 41: 1, 51: 1, 4: 4, 14: 4, 24: 4, 34: 4, 44: 4, 54: 4,
+              5: 5, 15: 5, 25: 5, 35: 5, 45: 5, 55: 5}.get(pt)
+        if fp is None or bp is None:
+            raise ValueError(f'Projector type {pt} is not supported by this build')
+        return fp, bp
+
+    def _descriptor(self):
+        fpt, bpt = self._fp_bp_types()
+        self.FPType, self.BPType = fpt, bpt
+        d = _native.GeometryDesc()
+        d.struct_size = ctypes.sizeof(_native.GeometryDesc)
+        d.abi_version = _native.OMB_ABI_VERSION
+        d.modality = _native.OMB_CT_PANEL if self.CT else _native.OMB_PET_SINOGRAM
+        d.fp_type, d.bp_type = fpt, bpt
+        d.nx, d.ny, d.nz = self._n(self.Nx), self._n(self.Ny), self._n(self.Nz)
+        d.dx, d.dy, d.dz = float(self.dx[0]), float(self.dy[0]), float(self.dz[0])
+        d.bx, d.by, d.bz = float(self.bx[0]), float(self.by[0]), float(self.bz[0])
+        d.n_rows_d, d.n_cols_d = int(self.nRowsD), int(self.nColsD)
+        d.n_proj = int(self.nProjections)
+        d.n_subsets = int(self.subsets)
+        d.subset_type = int(self.subsetType)
+        keep = {}
+        keep['n_meas'] = np.ascontiguousarray(np.asarray(self.nMeas, dtype=np.int64).ravel())
+        keep['xy'] = np.ascontiguousarray(np.asarray(self.x, dtype=np.float32).ravel())
+        keep['z'] = np.ascontiguousarray(np.asarray(self.z, dtype=np.float32).ravel())
+        d.n_meas = _native.i64_ptr(keep['n_meas'])
+        d.xy = _native.f32_ptr(keep['xy'])
+        d.n_xy = keep['xy'].size
+        d.z = _native.f32_ptr(keep['z'])
+        d.n_z = keep['z'].size
+        d.dpitch_x, d.dpitch_y = float(self.dPitchX), float(self.dPitchY)
+        d.global_factor = float(self.global_factor)
+        d.epps = float(self.epps)
+        nb = int(self.TOF_bins_used) if self.TOF else 1
+        d.tof_bins = nb
+        d.sigma_x = float(self.sigma_x)
+        if self.TOF:
+            keep['tof'] = np.ascontiguousarray(np.asarray(self.TOFCenter, dtype=np.float32).ravel())
+            d.tof_centers = _native.f32_ptr(keep['tof'])
+        d.dL = float(self.dL)
+        d.fixed64_workspace = 1 if self.use_64bit_atomics else 0
+        return d, keep
+
+    def initProj(self):
+        """Uploads the geometry to the current CUDA device and reorders the
+        measurement data into subset order (init.py:39-703; parseInputs
+        prepass.py:256-355)."""
+        if not self.projectorAdded:
+            self.addProjector()
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError('omega_b200 projectors need a CUDA device')
+        self.projectorInitialized = True
+        if self.TOF_bins_used == 0:
+            self.TOF_bins_used = 1
+        self._parse_inputs()
+        desc, keep = self._descriptor()
+        h = ctypes.c_void_p()
+        _native.call("omb_create", ctypes.byref(desc), ctypes.byref(h))
+        if self._handle is not None:
+            _native.lib().omb_destroy(self._handle)
+        self._handle = h
+        self._device = torch.cuda.current_device()
+        del keep
+
+    def _parse_inputs(self):
+        """Reorders SinM into subset order (prepass.py:282-355, static data)."""
+        if not (self.subsets > 1 and self.subsetType > 0) or self.SinM.size == 0:
+            return
+        if self.Nt > 1:
+            raise ValueError('dynamic data: reorder each frame with subsetMeasurements()')
+        nb = int(self.TOF_bins_used) if self.TOF else 1
+        if self.subsetType >= 8:
+            s = np.reshape(self.SinM, (self.nRowsD, self.nColsD, self.nProjections, nb), order='F')
+            s = s[:, :, self.index, :]
+            self.SinM = s if self.TOF else s[:, :, :, 0]
+        else:
+            if self.TOF:
+                s = np.reshape(self.SinM, (self.SinM.size // nb, nb), order='F')
+                self.SinM = s[self.index, :]
+            else:
+                self.SinM = self.SinM.ravel(order='F')[self.index]
+
+    def subsetMeasurements(self, m, subset):
+        """Measurements of one subset from the subset-ordered flat vector
+        ``m = SinM.ravel('F')`` in the layout the projector expects
+        (all TOF bins of the subset: [bin0 rays, bin1 rays, ...])."""
+        lo, hi = int(self.nTotMeas[subset]), int(self.nTotMeas[subset + 1])
+        if not self.TOF:
+            return m[lo:hi]
+        per_bin = int(self.nTotMeas[-1])
+        parts = [m[b * per_bin + lo:b * per_bin + hi] for b in range(int(self.TOF_bins_used))]
+        import torch
+        return torch.cat(parts) if isinstance(m, torch.Tensor) else np.concatenate(parts)
+
+    # ------------------------------------------------------------------
+    # Projections (projfunctions.py:86-1407)
+    # ------------------------------------------------------------------
+    def _check_ready(self):
+        if not self.projectorInitialized or self._handle is None:
+            self.initProj()
+
+    def _as_device(self, a, n, what):
+        import torch
+        if isinstance(a, np.ndarray):
+            a = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32).ravel()).cuda(self._device)
+        if not isinstance(a, torch.Tensor):
+            raise TypeError(f'{what} must be a torch tensor or a NumPy array')
+        if not a.is_cuda:
+            a = a.cuda(self._device)
+        if a.dtype != torch.float32:
+            a = a.float()
+        a = a.reshape(-1)
+        if not a.is_contiguous():
+            a = a.contiguous()
+        if a.numel() != n:
+            raise ValueError(f'{what} has {a.numel()} elements, expected {n}')
+        return a
+
+    def measurementCount(self, subset):
+        return int(_native.lib().omb_measurement_count(self._handle, int(subset)))
+
+    def forwardProject(self, f, subset=-1):
+        """y = A_subset f (projfunctions.py:86)."""
+        self._check_ready()
+        import torch
+        if subset == -1:
+            subset = self.subset
+        f = self._as_device(f, int(self.N[0]), 'image')
+        m = self.measurementCount(subset)
+        y = torch.empty(m, dtype=torch.float32, device=f.device)
+        stream = torch.cuda.current_stream(f.device).cuda_stream
+        _native.call("omb_forward", self._handle, int(subset), ctypes.c_void_p(f.data_ptr()),
+                     ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(stream))
+        return y
+
+    def backwardProject(self, y, subset=-1, sens=False):
+        """f = A_subset^T y (projfunctions.py:735).  With ``sens=True`` also
+        returns A_subset^T 1 (the reference's no_norm == 0 pass)."""
+        self._check_ready()
+        import torch
+        if subset == -1:
+            subset = self.subset
+        m = self.measurementCount(subset)
+        y = self._as_device(y, m, 'measurement')
+        n = int(self.N[0])
+        f = torch.empty(n, dtype=torch.float32, device=y.device)
+        s = torch.empty(n, dtype=torch.float32, device=y.device) if sens else None
+        stream = torch.cuda.current_stream(y.device).cuda_stream
+        mode = _native.OMB_BP_FIXED64 if self.use_64bit_atomics else _native.OMB_BP_FLOAT_ATOMIC
+        _native.call("omb_backward", self._handle, int(subset), ctypes.c_void_p(y.data_ptr()),
+                     ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(s.data_ptr() if s is not None else 0),
+                     int(mode), ctypes.c_void_p(stream))
+        return (f, s) if sens else f
+
+    def T(self):
+        self.trans = True
+        return self
+
+    def __mul__(self, B):
+        if self.trans:
+            self.trans = False
+            return self.backwardProject(B, self.subset)
+        return self.forwardProject(B, self.subset)
+
+    def __imul__(self, B):
+        return self.__mul__(B)
+
+    def __rmul__(self, B):
+        return self
+
+    def __truediv__(self, B):
+        return self

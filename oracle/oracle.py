@@ -1,0 +1,247 @@
+"""TEST INFRASTRUCTURE ONLY: the CPU oracle of the projector path.
+
+Loads ``oracle/liboracle.so`` (the FP64 restatement in siddon_oracle.c) and,
+when built, ``oracle/_ref/libref_siddon.so`` (the reference's own OpenMP CPU
+projector, projector_functions.h:1312), and restates the OSEM loop in numpy.
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg
+import this module; the product never does.
+
+OSEM restatement (the reference's compiled loop, CS-2):
+  fp = A_s x + epps                      computeForwardProject.h:20-21
+  r  = y_s / fp, NaN/Inf -> epps          computeForwardProject.h:92-95, 400-401
+  rhs = A_s^T r
+  sens_s = max(A_s^T 1, epps)             reconstructionAF.h:303-328, functions.hpp:2980-2996
+  x = x / sens_s * (rhs + epps)           algorithms.h:12-15, subiterStep.h:118-121
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref_siddon.so")
+
+
+class OracleGeom(ctypes.Structure):
+    _fields_ = [
+        ("modality", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("bx", ctypes.c_double), ("by", ctypes.c_double), ("bz", ctypes.c_double),
+        ("n_rows", ctypes.c_int), ("n_cols", ctypes.c_int),
+        ("proj0", ctypes.c_int64), ("n_proj", ctypes.c_int64), ("m_size", ctypes.c_int64),
+        ("stype", ctypes.c_int), ("n_subsets", ctypes.c_int), ("cur_subset", ctypes.c_int),
+        ("pitch_x", ctypes.c_double), ("pitch_y", ctypes.c_double),
+        ("global_factor", ctypes.c_double), ("epps", ctypes.c_double),
+        ("nbins", ctypes.c_int),
+        ("sigma_x", ctypes.c_double),
+        ("tof_centers", ctypes.POINTER(ctypes.c_double)),
+        ("xy", ctypes.POINTER(ctypes.c_float)),
+        ("z", ctypes.POINTER(ctypes.c_float)),
+    ]
+
+
+_lib = None
+_ref = None
+
+
+def build():
+    """Builds the oracle libraries (oracle/Makefile)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        P = ctypes.POINTER(ctypes.c_double)
+        G = ctypes.POINTER(OracleGeom)
+        L.oracle_siddon_fp.argtypes = [G, P, P]
+        L.oracle_siddon_bp.argtypes = [G, P, P, P]
+        L.oracle_siddon_count.argtypes = [G]
+        L.oracle_siddon_count.restype = ctypes.c_int64
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference's own CPU projector, or None when it was not built."""
+    global _ref
+    if _ref is None and os.path.exists(REF_LIB):
+        L = ctypes.CDLL(REF_LIB)
+        for name, T in (("ref_siddon_d", ctypes.c_double), ("ref_siddon_f", ctypes.c_float)):
+            P = ctypes.POINTER(T)
+            u = ctypes.c_uint32
+            getattr(L, name).argtypes = [ctypes.c_int, u, u, u, T, T, T, T, T, T, u, u, u, P, P, P, P, P, u, T, P, T,
+                                         T, u]
+        _ref = L
+    return _ref
+
+
+class Geometry:
+    """Everything the oracle needs from an addProjector()-ed options object."""
+
+    def __init__(self, o):
+        self.ct = bool(o.CT)
+        self.nx, self.ny, self.nz = (int(np.asarray(v).ravel()[0]) for v in (o.Nx, o.Ny, o.Nz))
+        self.d = tuple(float(np.asarray(v).ravel()[0]) for v in (o.dx, o.dy, o.dz))
+        self.b = tuple(float(np.asarray(v).ravel()[0]) for v in (o.bx, o.by, o.bz))
+        self.n_rows, self.n_cols = int(o.nRowsD), int(o.nColsD)
+        self.n_proj = int(o.nProjections)
+        self.n_subsets = int(o.subsets)
+        self.stype = int(o.subsetType)
+        self.n_meas = np.asarray(o.nMeas, dtype=np.int64).ravel()
+        self.xy = np.ascontiguousarray(np.asarray(o.x, dtype=np.float32).ravel())
+        self.z = np.ascontiguousarray(np.asarray(o.z, dtype=np.float32).ravel())
+        self.pitch = (float(o.dPitchX), float(o.dPitchY))
+        self.global_factor = float(o.global_factor)
+        self.epps = float(o.epps)
+        self.nbins = int(o.TOF_bins_used) if o.TOF else 1
+        self.sigma_x = float(o.sigma_x)
+        self.tofc = np.ascontiguousarray(np.asarray(o.TOFCenter, dtype=np.float64).ravel()) if o.TOF else \
+            np.zeros(1, dtype=np.float64)
+
+    @property
+    def n_img(self):
+        return self.nx * self.ny * self.nz
+
+    def meas_level(self):
+        return self.n_subsets > 1 and self.stype < 8
+
+    def rays(self, subset):
+        nbin = self.n_rows * self.n_cols
+        if self.meas_level():
+            return int(self.n_meas[subset + 1] - self.n_meas[subset])
+        if subset < 0:
+            return self.n_proj * nbin
+        return int(self.n_meas[subset + 1] - self.n_meas[subset]) * nbin
+
+    def struct(self, subset):
+        g = OracleGeom()
+        g.modality = 1 if self.ct else 0
+        g.nx, g.ny, g.nz = self.nx, self.ny, self.nz
+        g.dx, g.dy, g.dz = self.d
+        g.bx, g.by, g.bz = self.b
+        g.n_rows, g.n_cols = self.n_rows, self.n_cols
+        if self.meas_level():
+            g.stype = self.stype
+            g.proj0 = 0
+            g.n_proj = self.n_proj
+        else:
+            g.stype = 0
+            g.proj0 = 0 if subset < 0 else int(self.n_meas[subset])
+            g.n_proj = self.n_proj if subset < 0 else int(self.n_meas[subset + 1] - self.n_meas[subset])
+        g.m_size = self.rays(subset)
+        g.n_subsets = self.n_subsets
+        g.cur_subset = max(subset, 0)
+        g.pitch_x, g.pitch_y = self.pitch
+        g.global_factor = self.global_factor
+        g.epps = self.epps
+        g.nbins = self.nbins
+        g.sigma_x = self.sigma_x
+        g.tof_centers = self.tofc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        g.xy = self.xy.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        g.z = self.z.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        return g
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None
+
+
+def forward(geom: Geometry, image, subset):
+    """FP64 y = A_s image (all TOF bins, [bin0 rays, bin1 rays, ...])."""
+    img = np.ascontiguousarray(image, dtype=np.float64).ravel()
+    g = geom.struct(subset)
+    y = np.zeros(g.m_size * geom.nbins, dtype=np.float64)
+    lib().oracle_siddon_fp(ctypes.byref(g), _dp(img), _dp(y))
+    return y
+
+
+def backward(geom: Geometry, y, subset, sens=False):
+    """FP64 A_s^T y (and A_s^T 1 when sens).  y may be None (sensitivity only)."""
+    g = geom.struct(subset)
+    yy = None if y is None else np.ascontiguousarray(y, dtype=np.float64).ravel()
+    img = np.zeros(geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    lib().oracle_siddon_bp(ctypes.byref(g), _dp(yy), _dp(img), _dp(s))
+    return (img, s) if sens else img
+
+
+def intersections(geom: Geometry, subset):
+    """Total voxel-intersection count sum_rays Np of one call."""
+    g = geom.struct(subset)
+    return int(lib().oracle_siddon_count(ctypes.byref(g)))
+
+
+def osem(geom: Geometry, y_subsets, x0, n_iter):
+    """Restated OSEM loop in FP64; returns the image after n_iter iterations."""
+    x = np.asarray(x0, dtype=np.float64).copy()
+    eps = geom.epps
+    sens = []
+    for s in range(geom.n_subsets):
+        _, sv = backward(geom, None, s, sens=True)
+        sens.append(np.maximum(sv, eps))
+    for _ in range(n_iter):
+        for s in range(geom.n_subsets):
+            fp = forward(geom, x, s) + eps
+            with np.errstate(divide="ignore", invalid="ignore"):
+                r = np.asarray(y_subsets[s], dtype=np.float64) / fp
+            r[~np.isfinite(r)] = eps
+            rhs = backward(geom, r, s)
+            x = x / sens[s] * (rhs + eps)
+    return x
+
+
+def loglik(y, fp, eps):
+    """Poisson log-likelihood sum[y log(fp + eps) - (fp + eps)] in FP64."""
+    f = np.asarray(fp, dtype=np.float64) + eps
+    yy = np.asarray(y, dtype=np.float64)
+    return float(np.sum(np.where(yy != 0, yy * np.log(f), 0.0) - f))
+
+
+def ref_forward(geom: Geometry, image, subset, precision="double", threads=0):
+    """The reference's own CPU projector (whole-sinogram subsets, PET)."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libref_siddon.so is not built")
+    return _ref_call(L, geom, image, subset, True, precision, threads)
+
+
+def ref_backward(geom: Geometry, y, subset, precision="double", threads=0, sens=False):
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libref_siddon.so is not built")
+    return _ref_call(L, geom, y, subset, False, precision, threads, sens)
+
+
+def _ref_call(L, geom, inp, subset, fp, precision, threads, sens=False):
+    T = np.float64 if precision == "double" else np.float32
+    fn = L.ref_siddon_d if precision == "double" else L.ref_siddon_f
+    CT = ctypes.c_double if precision == "double" else ctypes.c_float
+    P = ctypes.POINTER(CT)
+    p = (lambda a: a.ctypes.data_as(P) if a is not None else None)
+    n0, n1 = (0, geom.n_proj) if subset < 0 else (int(geom.n_meas[subset]), int(geom.n_meas[subset + 1]))
+    xy = geom.xy.astype(T)
+    z = np.ascontiguousarray(geom.z.astype(T)[n0 * 2:n1 * 2])
+    inp = np.ascontiguousarray(inp, dtype=T).ravel()
+    nmeas = geom.n_rows * geom.n_cols * (n1 - n0)
+    out = np.zeros(nmeas * geom.nbins if fp else geom.n_img, dtype=T)
+    s = np.zeros(geom.n_img, dtype=T) if sens else None
+    tofc = geom.tofc.astype(T)
+    fn(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, geom.n_rows, geom.n_cols, n1 - n0, p(xy), p(z),
+       p(inp), p(out), p(s), geom.nbins, geom.sigma_x, p(tofc), geom.global_factor, geom.epps, int(threads))
+    return (out, s) if sens else out
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))

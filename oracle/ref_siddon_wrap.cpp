@@ -1,0 +1,61 @@
+/*
+ * TEST INFRASTRUCTURE ONLY.  Thin C entry points around OMEGA's own OpenMP
+ * CPU projector, projectorType123Implementation4<T>
+ * (source/cpp/projector_functions.h:1312), compiled from the reference
+ * sources where they lie (oracle/Makefile passes -I to them); nothing of the
+ * reference is copied here.  Output goes to oracle/_ref/libref_siddon.so.
+ * Used to pin the FP64 restatement (oracle/siddon_oracle.c) against the
+ * reference itself, and as the timed CPU baseline of bench.py.
+ *
+ * PET sinogram data, whole-sinogram subsets: the caller passes the z pairs of
+ * the sinograms to project, so the function runs with subsets = 1.
+ */
+#include <cstdint>
+
+#include "projector_functions.h"
+
+template <typename T>
+static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, T bx, T by, T bz, uint32_t n_rows,
+               uint32_t n_cols, uint32_t n_proj, const T *xy, const T *z, T *input, T *output, T *sens, uint32_t nbins,
+               T sigma_x, T *tof_centers, T global_factor, T epps, uint32_t n_threads) {
+    paramStruct<T> p;
+    p.subsetType = 8;
+    p.subsets = 1;
+    p.currentSubset = 0;
+    p.size_x = n_rows;
+    p.size_y = n_cols;
+    p.dx = dx; p.dy = dy; p.dz = dz;
+    p.Nx = nx; p.Ny = ny; p.Nz = nz;
+    p.bx = bx; p.by = by; p.bz = bz;
+    p.projType = 1;
+    p.nProjections = n_proj;
+    p.globalFactor = global_factor;
+    p.epps = epps;
+    p.TOF = nbins > 1;
+    p.nBins = nbins;
+    p.sigma_x = sigma_x;
+    p.TOFCenters = tof_centers;
+    p.noSensImage = sens == nullptr;
+    p.nMeas = 0;
+    const int64_t n_meas = (int64_t)n_rows * n_cols * n_proj;
+    projectorType123Implementation4<T>(p, n_meas, output, xy, z, input, false, false, (uint8_t)(fp ? 1 : 2), sens,
+                                       nullptr, n_threads);
+    return 0;
+}
+
+extern "C" {
+int ref_siddon_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx, double by,
+                 double bz, uint32_t n_rows, uint32_t n_cols, uint32_t n_proj, const double *xy, const double *z,
+                 double *input, double *output, double *sens, uint32_t nbins, double sigma_x, double *tof_centers,
+                 double global_factor, double epps, uint32_t n_threads) {
+    return run<double>(fp, nx, ny, nz, dx, dy, dz, bx, by, bz, n_rows, n_cols, n_proj, xy, z, input, output, sens,
+                       nbins, sigma_x, tof_centers, global_factor, epps, n_threads);
+}
+int ref_siddon_f(int fp, uint32_t nx, uint32_t ny, uint32_t nz, float dx, float dy, float dz, float bx, float by,
+                 float bz, uint32_t n_rows, uint32_t n_cols, uint32_t n_proj, const float *xy, const float *z,
+                 float *input, float *output, float *sens, uint32_t nbins, float sigma_x, float *tof_centers,
+                 float global_factor, float epps, uint32_t n_threads) {
+    return run<float>(fp, nx, ny, nz, dx, dy, dz, bx, by, bz, n_rows, n_cols, n_proj, xy, z, input, output, sens,
+                      nbins, sigma_x, tof_centers, global_factor, epps, n_threads);
+}
+}

@@ -1,0 +1,125 @@
+"""Generates the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a container that holds the OMEGA sources (default /root/reference, or
+$OMEGA_REFERENCE):
+
+    python tests/golden/make_golden.py
+
+For every option set in configs.py it imports the reference's own Python
+projector surface (omegatomo.projector.proj.projectorClass), runs its
+addProjector(), and stores the geometry arrays it produces (detector
+coordinates, subset indices, measurement counts, voxel grid) in
+``geom_<name>.npz``.  For the small PET sets it also runs the reference's own
+OpenMP CPU projector (projectorType123Implementation4<double>, compiled by
+oracle/Makefile into oracle/_ref/libref_siddon.so) on a seeded image and a
+seeded measurement vector and stores the results in ``proj_<name>.npz``.
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("OMEGA_REFERENCE", "/root/reference")
+sys.path.insert(0, HERE)
+from configs import CONFIGS, GEOMETRY_KEYS, SCALAR_KEYS, _pet, apply  # noqa: E402
+
+PROJ_SETS = ["pet_mini", "pet_tof_small"]
+# small TOF set for projector fixtures (kept separate to keep the files small)
+CONFIGS_EXTRA = {
+    "pet_tof_small": _pet(8, 8, 6, 300, 24, 32, 24, 11, 180, 26, subsets=4, TOF_bins=7, TOF_bins_used=7,
+                          TOF_FWHM=200e-12, TOF_width=CONFIGS["pet_mini_tof"]["TOF_width"]),
+}
+
+
+def reference_projector():
+    sys.path.insert(0, os.path.join(REF, "source", "Python"))
+    from omegatomo.projector import proj
+    return proj
+
+
+def geometry(proj, cfg):
+    o = apply(proj.projectorClass(), cfg)
+    o.addProjector()
+    out = {}
+    for k in GEOMETRY_KEYS:
+        out[k] = np.asarray(getattr(o, k))
+    for k in SCALAR_KEYS:
+        out["s_" + k] = np.asarray(getattr(o, k))
+    if o.TOF:
+        out["TOFCenter"] = np.asarray(o.TOFCenter)
+    if o.CT:
+        out["uV"] = np.asarray(o.uV)
+    return o, out
+
+
+def ref_cpu_lib():
+    path = os.path.join(REPO, "oracle", "_ref", "libref_siddon.so")
+    if not os.path.exists(path):
+        raise SystemExit("build the reference CPU projector first: make -C oracle")
+    L = ctypes.CDLL(path)
+    D = ctypes.c_double
+    P = ctypes.POINTER(ctypes.c_double)
+    u = ctypes.c_uint32
+    L.ref_siddon_d.argtypes = [ctypes.c_int, u, u, u, D, D, D, D, D, D, u, u, u, P, P, P, P, P, u, D, P, D, D, u]
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None
+
+
+def ref_project(L, o, subset, fp, inp, sens=False):
+    """Runs the reference CPU projector on one whole-sinogram subset."""
+    nb = int(o.TOF_bins_used) if o.TOF else 1
+    n0, n1 = int(o.nMeas[subset]), int(o.nMeas[subset + 1])
+    nproj = n1 - n0
+    xy = np.ascontiguousarray(o.x.astype(np.float64).ravel())
+    z = np.ascontiguousarray(o.z.astype(np.float64).ravel()[n0 * 2:n1 * 2])
+    N = int(o.Nx[0]) * int(o.Ny[0]) * int(o.Nz[0])
+    nmeas = int(o.nRowsD) * int(o.nColsD) * nproj
+    inp = np.ascontiguousarray(inp, dtype=np.float64)
+    out = np.zeros(nmeas * nb if fp else N, dtype=np.float64)
+    s = np.zeros(N, dtype=np.float64) if sens else None
+    tofc = np.ascontiguousarray(np.asarray(o.TOFCenter, dtype=np.float64)) if o.TOF else None
+    L.ref_siddon_d(1 if fp else 0, int(o.Nx[0]), int(o.Ny[0]), int(o.Nz[0]), float(o.dx[0]), float(o.dy[0]),
+                   float(o.dz[0]), float(o.bx[0]), float(o.by[0]), float(o.bz[0]), int(o.nRowsD), int(o.nColsD),
+                   nproj, _p(xy), _p(z), _p(inp), _p(out), _p(s), nb, float(o.sigma_x), _p(tofc),
+                   float(o.global_factor), float(o.epps), 0)
+    return out, s
+
+
+def main():
+    proj = reference_projector()
+    allc = dict(CONFIGS)
+    allc.update(CONFIGS_EXTRA)
+    L = None
+    for name, cfg in allc.items():
+        o, g = geometry(proj, cfg)
+        np.savez_compressed(os.path.join(HERE, f"geom_{name}.npz"), **g)
+        print(name, {k: np.shape(v) for k, v in g.items() if np.ndim(v) > 0})
+        if name in PROJ_SETS:
+            L = L or ref_cpu_lib()
+            rng = np.random.default_rng(1234)
+            N = int(o.N[0])
+            img = rng.uniform(0.5, 1.5, N)
+            fixtures = {"image": img.astype(np.float32)}
+            nb = int(o.TOF_bins_used) if o.TOF else 1
+            subsets = [0, int(o.subsets) - 1] if nb == 1 else [0]
+            for s in subsets:
+                y, _ = ref_project(L, o, s, True, img.astype(np.float32).astype(np.float64))
+                fixtures[f"fp_{s}"] = y.astype(np.float32)
+            m = int(o.nMeasSubset[0, 0]) * nb
+            yin = rng.uniform(0.0, 2.0, m)
+            fixtures["bp_in_0"] = yin.astype(np.float32)
+            bp, sens = ref_project(L, o, 0, False, yin.astype(np.float32).astype(np.float64), sens=True)
+            fixtures["bp_0"] = bp.astype(np.float32)
+            fixtures["sens_0"] = sens.astype(np.float32)
+            np.savez_compressed(os.path.join(HERE, f"proj_{name}.npz"), **fixtures)
+            print("  projector fixtures:", list(fixtures))
+
+
+if __name__ == "__main__":
+    main()
