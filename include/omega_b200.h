@@ -133,6 +133,16 @@ int64_t omb_image_count(const omb_handle *h);
 int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, void *stream);
 
 /*
+ * Forward projection of n_frames images in one launch (frames of a dynamic
+ * study share the geometry): y[f*y_stride ...] = A_s images[f*image_stride ...].
+ * Each ray is traced once for up to eight frames.  TOF handles take
+ * n_frames == 1.  Replaces the per-timestep FP launches of the reference's
+ * loop (reconstructionAF.h:1089-1190, one launch per frame).
+ */
+int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const float *images, int64_t image_stride,
+                       float *y, int64_t y_stride, void *stream);
+
+/*
  * image = A_s^T * y, and sens = A_s^T * 1 when `sens` is not NULL (the
  * reference's no_norm == 0 pass).  Both outputs are overwritten.
  * mode: omb_bp_mode; OMB_BP_FIXED64 needs a handle created with
@@ -144,6 +154,14 @@ int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, voi
  */
 int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, float *sens,
                  int32_t mode, void *stream);
+
+/*
+ * Backprojection of n_frames measurement vectors into n_frames images (float
+ * atomics; images overwritten).  Replaces the per-timestep BP launches of
+ * reconstructionAF.h:1265.
+ */
+int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const float *y, int64_t y_stride,
+                        float *images, int64_t image_stride, void *stream);
 
 /*
  * One OSEM sub-iteration for PET, fused on the device:
@@ -163,6 +181,15 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
  * iteration (reconstructionAF.h:303-328 with the clamp of functions.hpp:2980-2996).
  */
 int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream);
+
+/*
+ * Total voxel intersections (sum over the subset's rays of the Siddon walk
+ * length Np) written to *out_host; synchronises `stream`.  The
+ * algorithmic-byte model of the projector roofline counts bytes per
+ * intersection.  The reference has no counterpart (its pre-loop computes Np
+ * per ray inside the kernel, general_opencl_functions.h:1873, 1942).
+ */
+int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, void *stream);
 
 /*
  * Poisson log-likelihood sum_i [ y_i * log(fp_i + epps) - (fp_i + epps) ],

@@ -118,6 +118,26 @@ static int ray_set(const omb_handle *h, int32_t subset, RaySet &rs) {
     return OMB_OK;
 }
 
+static Frames one_frame_fp(const omb_handle *h, const float *img, float *y, int64_t m) {
+    Frames f{};
+    f.n = 1;
+    f.img_in = img;
+    f.img_stride = h->n_img;
+    f.meas_out = y;
+    f.meas_stride = m;
+    return f;
+}
+
+static Frames one_frame_bp(const omb_handle *h, const float *y, float *img, int64_t m) {
+    Frames f{};
+    f.n = 1;
+    f.meas = y;
+    f.meas_stride = m;
+    f.img = img;
+    f.img_stride = h->n_img;
+    return f;
+}
+
 extern "C" {
 
 int omb_abi_version(void) { return OMB_ABI_VERSION; }
@@ -205,7 +225,27 @@ int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, voi
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
-    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, image, y, (cudaStream_t)stream);
+    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, y, rs.m_size),
+                          (cudaStream_t)stream);
+}
+
+int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const float *images, int64_t image_stride,
+                       float *y, int64_t y_stride, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!images || !y) return set_error(OMB_ERR_INVALID, "images/y pointer is NULL");
+    if (n_frames < 0) return set_error(OMB_ERR_INVALID, "n_frames must be >= 0");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    if (image_stride < h->n_img || y_stride < rs.m_size * h->desc.tof_bins)
+        return set_error(OMB_ERR_INVALID, "frame strides smaller than one image / one measurement vector");
+    Frames f{};
+    f.n = n_frames;
+    f.img_in = images;
+    f.img_stride = image_stride;
+    f.meas_out = y;
+    f.meas_stride = y_stride;
+    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, f, (cudaStream_t)stream);
 }
 
 int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, float *sens, int32_t mode,
@@ -223,7 +263,7 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
     if (mode == OMB_BP_FIXED64) {
         unsigned long long *acc = h->d_acc, *acc_s = sens ? h->d_acc + h->n_img : nullptr;
         OMB_CUDA_TRY(cudaMemsetAsync(h->d_acc, 0, (sens ? 2 : 1) * h->n_img * sizeof(unsigned long long), s));
-        st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, y, nullptr, nullptr, acc, acc_s, mode, s);
+        st = siddon_backward_fixed(h->grid, rs, h->tof, h->desc.global_factor, y, acc, acc_s, s);
         if (st != OMB_OK) return st;
         st = fixed_to_float(acc, image, h->n_img, s);
         if (st == OMB_OK && sens) st = fixed_to_float(acc_s, sens, h->n_img, s);
@@ -231,7 +271,32 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
     }
     OMB_CUDA_TRY(cudaMemsetAsync(image, 0, nb, s));
     if (sens) OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, nb, s));
-    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, y, image, sens, nullptr, nullptr, mode, s);
+    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, y, image, rs.m_size), sens, s);
+}
+
+int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const float *y, int64_t y_stride,
+                        float *images, int64_t image_stride, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!images || !y) return set_error(OMB_ERR_INVALID, "images/y pointer is NULL");
+    if (n_frames < 0) return set_error(OMB_ERR_INVALID, "n_frames must be >= 0");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    if (image_stride < h->n_img || y_stride < rs.m_size * h->desc.tof_bins)
+        return set_error(OMB_ERR_INVALID, "frame strides smaller than one image / one measurement vector");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (image_stride == h->n_img) {
+        OMB_CUDA_TRY(cudaMemsetAsync(images, 0, (size_t)n_frames * h->n_img * sizeof(float), s));
+    } else {
+        OMB_CUDA_TRY(cudaMemset2DAsync(images, image_stride * sizeof(float), 0, h->n_img * sizeof(float), n_frames, s));
+    }
+    Frames f{};
+    f.n = n_frames;
+    f.meas = y;
+    f.meas_stride = y_stride;
+    f.img = images;
+    f.img_stride = image_stride;
+    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, nullptr, s);
 }
 
 int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
@@ -243,8 +308,8 @@ int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     // A^T 1 through the BP kernel's fused sensitivity accumulator, y = NULL.
     OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, h->n_img * sizeof(float), s));
-    st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, nullptr, nullptr, sens, nullptr, nullptr,
-                         OMB_BP_FLOAT_ATOMIC, s);
+    st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, nullptr, nullptr, rs.m_size),
+                         sens, s);
     if (st != OMB_OK) return st;
     return clamp_min(sens, h->n_img, h->desc.epps, s);
 }
@@ -260,15 +325,37 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     if (st != OMB_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     const float eps = h->desc.epps;
-    st = siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, image, work_meas, s);
+    const int64_t m = rs.m_size * h->desc.tof_bins;
+    st = siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, work_meas, rs.m_size), s);
     if (st != OMB_OK) return st;
-    st = osem_ratio(y_subset, work_meas, rs.m_size * h->desc.tof_bins, eps, s);
+    st = osem_ratio(y_subset, work_meas, m, eps, s);
     if (st != OMB_OK) return st;
     OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
-    st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, work_meas, work_img, nullptr, nullptr, nullptr,
-                         OMB_BP_FLOAT_ATOMIC, s);
+    st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, work_meas, work_img, rs.m_size),
+                         nullptr, s);
     if (st != OMB_OK) return st;
     return em_update(image, sens, work_img, h->n_img, eps, s);
+}
+
+int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!out_host) return set_error(OMB_ERR_INVALID, "output pointer is NULL");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long *d = nullptr;
+    OMB_CUDA_TRY(cudaMallocAsync(&d, sizeof(unsigned long long), s));
+    cudaError_t e = cudaMemsetAsync(d, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) st = siddon_count(h->grid, rs, h->tof, d, s);
+    unsigned long long v = 0;
+    if (e == cudaSuccess && st == OMB_OK) e = cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(d, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "intersection count");
+    if (st != OMB_OK) return st;
+    *out_host = (int64_t)v;
+    return OMB_OK;
 }
 
 int omb_loglik(const float *y, const float *fp, int64_t n, float epps, double *out_host, void *work, void *stream) {

@@ -54,6 +54,19 @@ struct RaySet {
     float pitch_x, pitch_y;
 };
 
+// A batch of frames (images and their measurement vectors) processed by one
+// launch; frame f's image starts at img + f*img_stride and its measurements
+// at meas + f*meas_stride.
+struct Frames {
+    int n;
+    const float *img_in;   // forward: input images
+    float *img;            // backward: output images
+    int64_t img_stride;
+    const float *meas;     // backward: input measurements
+    float *meas_out;       // forward: output measurements
+    int64_t meas_stride;
+};
+
 struct Tof {
     int nbins;
     float sigma_inv;

@@ -5,10 +5,12 @@
 
 namespace omb {
 
-int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *img, float *y,
-                   cudaStream_t st);
-int siddon_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *y, float *img,
-                    float *sens, unsigned long long *acc, unsigned long long *acc_sens, int mode, cudaStream_t st);
+int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, cudaStream_t st);
+int siddon_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, float *sens,
+                    cudaStream_t st);
+int siddon_backward_fixed(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *y,
+                          unsigned long long *acc, unsigned long long *acc_sens, cudaStream_t st);
+int siddon_count(const Grid &g, const RaySet &rs, const Tof &tof, unsigned long long *total, cudaStream_t st);
 int fixed_to_float(const unsigned long long *acc, float *out, int64_t n, cudaStream_t st);
 
 // Elementwise steps of the subset updates.

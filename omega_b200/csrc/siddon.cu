@@ -14,71 +14,103 @@ namespace omb {
 // TH = 1e11 (omegatomo/projector/init.py:105).
 constexpr double kFixedScale = 1e11;
 
-template <int NB>
+// Forward projection.  Each thread walks one ray once and accumulates it for
+// FB frames of a dynamic study (blockIdx.y selects the group of frames), so
+// the traversal cost is shared by up to FB images.
+template <int NB, int FB>
 __global__ void __launch_bounds__(kBlock) k_siddon_fp(Grid g, RaySet rs, Tof tof, float gf,
-                                                      const float *__restrict__ img, float *__restrict__ y) {
+                                                      const float *__restrict__ img, int64_t img_stride,
+                                                      float *__restrict__ y, int64_t y_stride, int n_frames) {
     const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const int f0 = blockIdx.y * FB;
+    const int nf = min(FB, n_frames - f0);
+    img += f0 * img_stride;
+    y += f0 * y_stride;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
         const Ray ray = load_ray(rs, r);
-        float ax[NB];
+        float ax[NB * FB];
 #pragma unroll
-        for (int to = 0; to < NB; ++to) ax[to] = 0.f;
+        for (int to = 0; to < NB * FB; ++to) ax[to] = 0.f;
         float temp = 0.f;
         const bool ok = siddon_walk<NB>(g, ray, pet, gf, tof, temp,
                                         [&](int64_t ind, float ele, const float *w, float tsum) {
-                                            const float v = ele * __ldg(img + ind);
                                             if (NB == 1) {
-                                                ax[0] += v;
+#pragma unroll
+                                                for (int f = 0; f < FB; ++f)
+                                                    if (f < nf) ax[f] += ele * __ldg(img + f * img_stride + ind);
                                             } else {
-                                                const float dX = v / tsum;
+                                                const float dX = ele * __ldg(img + ind) / tsum;
 #pragma unroll
                                                 for (int to = 0; to < NB; ++to) ax[to] += w[to] * dX;
                                             }
                                         });
+        if (NB == 1) {
 #pragma unroll
-        for (int to = 0; to < NB; ++to) y[r + to * rs.m_size] = ok ? ax[to] * temp : 0.f;
+            for (int f = 0; f < FB; ++f)
+                if (f < nf) y[f * y_stride + r] = ok ? ax[f] * temp : 0.f;
+        } else {
+#pragma unroll
+            for (int to = 0; to < NB; ++to) y[r + to * rs.m_size] = ok ? ax[to] * temp : 0.f;
+        }
     }
 }
 
 // Backprojection with float atomics (rhs(), general_opencl_functions.h:1212-1275).
-template <int NB, bool SENS>
+// Frame batching as in the forward kernel: one walk, FB images updated.
+template <int NB, int FB, bool SENS>
 __global__ void __launch_bounds__(kBlock) k_siddon_bp(Grid g, RaySet rs, Tof tof, float gf,
-                                                      const float *__restrict__ y, float *__restrict__ img,
-                                                      float *__restrict__ sens) {
+                                                      const float *__restrict__ y, int64_t y_stride,
+                                                      float *__restrict__ img, int64_t img_stride,
+                                                      float *__restrict__ sens, int n_frames) {
     const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const int f0 = blockIdx.y * FB;
+    const int nf = min(FB, n_frames - f0);
+    if (y) y += f0 * y_stride;
+    if (img) img += f0 * img_stride;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
-        float ax[NB];
+        float ax[NB * FB];
         bool any = SENS;
+        if (NB == 1) {
 #pragma unroll
-        for (int to = 0; to < NB; ++to) {
-            ax[to] = y ? __ldg(y + r + to * rs.m_size) : 0.f;  // y == NULL: sensitivity only
-            any |= ax[to] != 0.f;
+            for (int f = 0; f < FB; ++f) {
+                ax[f] = (y && f < nf) ? __ldg(y + f * y_stride + r) : 0.f;  // y == NULL: sensitivity only
+                any |= ax[f] != 0.f;
+            }
+        } else {
+#pragma unroll
+            for (int to = 0; to < NB; ++to) {
+                ax[to] = y ? __ldg(y + r + to * rs.m_size) : 0.f;
+                any |= ax[to] != 0.f;
+            }
         }
         if (!any) continue;  // adds only zeros
         const Ray ray = load_ray(rs, r);
         float temp = 0.f;
         siddon_walk<NB>(g, ray, pet, gf, tof, temp, [&](int64_t ind, float ele, const float *w, float tsum) {
             const float le = ele * temp;
-            float yax, val;
             if (NB == 1) {
-                yax = ax[0] * le;
-                val = le;
-                if (isnan(le)) yax = 0.f;
+                if (!isnan(le)) {
+#pragma unroll
+                    for (int f = 0; f < FB; ++f) {
+                        const float yax = ax[f] * le;
+                        if (f < nf && yax != 0.f) atomicAdd(img + f * img_stride + ind, yax);
+                    }
+                }
+                if (SENS && le != 0.f) atomicAdd(sens + ind, le);
             } else {
                 const float dX = le / tsum;
-                yax = 0.f;
-                val = 0.f;
+                float yax = 0.f, val = 0.f;
 #pragma unroll
                 for (int to = 0; to < NB; ++to) {
                     const float a = dX * w[to];
                     val += a;
                     yax += a * ax[to];
                 }
+                if (yax != 0.f) atomicAdd(img + ind, yax);
+                if (SENS && val != 0.f) atomicAdd(sens + ind, val);
             }
-            if (yax != 0.f) atomicAdd(img + ind, yax);
-            if (SENS && val != 0.f) atomicAdd(sens + ind, val);
         });
     }
 }
@@ -133,64 +165,137 @@ __global__ void __launch_bounds__(kBlock) k_siddon_bp_fixed(Grid g, RaySet rs, T
     }
 }
 
+// Voxel intersections Np summed over the launch's rays (the walk lengths of
+// the algorithmic-byte model); one int64 atomic per block.
+__global__ void __launch_bounds__(kBlock) k_siddon_count(Grid g, RaySet rs, Tof tof,
+                                                         unsigned long long *__restrict__ total) {
+    const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long n = 0;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
+        const Ray ray = load_ray(rs, r);
+        float temp;
+        siddon_walk<1>(g, ray, pet, 1.f, tof, temp, [&](int64_t, float, const float *, float) { ++n; });
+    }
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+    __shared__ unsigned long long sh[kBlock / 32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < kBlock / 32; ++i) t += sh[i];
+        atomicAdd(total, t);
+    }
+}
+
+int siddon_count(const Grid &g, const RaySet &rs, const Tof &tof, unsigned long long *total, cudaStream_t st) {
+    if (rs.m_size <= 0) return OMB_OK;
+    Tof t1 = tof;
+    t1.nbins = 1;
+    k_siddon_count<<<grid_for(rs.m_size), kBlock, 0, st>>>(g, rs, t1, total);
+    OMB_LAUNCH_CHECK("siddon count launch");
+    return OMB_OK;
+}
+
 __global__ void k_fixed_to_float(const unsigned long long *__restrict__ acc, float *__restrict__ out, int64_t n) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
         out[i] = (float)((double)(long long)acc[i] * (1.0 / kFixedScale));
 }
 
-template <int NB>
-static void fp_nb(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *img, float *y,
-                  cudaStream_t st) {
-    k_siddon_fp<NB><<<grid_for(rs.m_size), kBlock, 0, st>>>(g, rs, tof, gf, img, y);
+template <int NB, int FB>
+static void fp_launch(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, cudaStream_t st) {
+    dim3 grid(grid_for(rs.m_size), (fr.n + FB - 1) / FB);
+    k_siddon_fp<NB, FB><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, fr.img_in, fr.img_stride, fr.meas_out,
+                                                  fr.meas_stride, fr.n);
+}
+
+template <int NB, int FB>
+static void bp_launch(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, float *sens,
+                      cudaStream_t st) {
+    dim3 grid(grid_for(rs.m_size), (fr.n + FB - 1) / FB);
+    if (sens)
+        k_siddon_bp<NB, FB, true><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, fr.meas, fr.meas_stride, fr.img,
+                                                             fr.img_stride, sens, fr.n);
+    else
+        k_siddon_bp<NB, FB, false><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, fr.meas, fr.meas_stride, fr.img,
+                                                              fr.img_stride, nullptr, fr.n);
 }
 
 template <int NB>
-static void bp_nb(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *y, float *img,
-                  float *sens, unsigned long long *acc, unsigned long long *acc_sens, int mode, cudaStream_t st) {
+static void bp_fixed_launch(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *y,
+                            unsigned long long *acc, unsigned long long *acc_sens, cudaStream_t st) {
     const unsigned grid = grid_for(rs.m_size);
-    if (mode == OMB_BP_FIXED64) {
-        if (acc_sens)
-            k_siddon_bp_fixed<NB, true><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, y, acc, acc_sens);
-        else
-            k_siddon_bp_fixed<NB, false><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, y, acc, nullptr);
-    } else {
-        if (sens)
-            k_siddon_bp<NB, true><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, y, img, sens);
-        else
-            k_siddon_bp<NB, false><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, y, img, nullptr);
-    }
+    if (acc_sens)
+        k_siddon_bp_fixed<NB, true><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, y, acc, acc_sens);
+    else
+        k_siddon_bp_fixed<NB, false><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, y, acc, nullptr);
 }
 
 #define OMB_NB_CASES(X) \
     X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 
-int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *img, float *y,
-                   cudaStream_t st) {
-    if (rs.m_size <= 0) return OMB_OK;
-    switch (tof.nbins) {
-#define X(n) case n: fp_nb<n>(g, rs, tof, gf, img, y, st); break;
-        OMB_NB_CASES(X)
+// Frames per walk for non-TOF batches.
+static int frames_per_walk(int n) { return n >= 8 ? 8 : (n >= 4 ? 4 : (n >= 2 ? 2 : 1)); }
+
+int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, cudaStream_t st) {
+    if (rs.m_size <= 0 || fr.n <= 0) return OMB_OK;
+    if (tof.nbins > 1 && fr.n != 1) return set_error(OMB_ERR_UNSUPPORTED, "TOF projections take one frame per call");
+    if (tof.nbins == 1) {
+        switch (frames_per_walk(fr.n)) {
+            case 8: fp_launch<1, 8>(g, rs, tof, gf, fr, st); break;
+            case 4: fp_launch<1, 4>(g, rs, tof, gf, fr, st); break;
+            case 2: fp_launch<1, 2>(g, rs, tof, gf, fr, st); break;
+            default: fp_launch<1, 1>(g, rs, tof, gf, fr, st); break;
+        }
+    } else {
+        switch (tof.nbins) {
+#define X(n) case n: fp_launch<n, 1>(g, rs, tof, gf, fr, st); break;
+            OMB_NB_CASES(X)
 #undef X
-        default:
-            return set_error(OMB_ERR_UNSUPPORTED, "TOF bin count above 16 is not built");
+            default:
+                return set_error(OMB_ERR_UNSUPPORTED, "TOF bin count above 16 is not built");
+        }
     }
     OMB_LAUNCH_CHECK("siddon forward launch");
     return OMB_OK;
 }
 
-int siddon_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *y, float *img,
-                    float *sens, unsigned long long *acc, unsigned long long *acc_sens, int mode,
+int siddon_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, float *sens,
                     cudaStream_t st) {
+    if (rs.m_size <= 0 || fr.n <= 0) return OMB_OK;
+    if (tof.nbins > 1 && fr.n != 1) return set_error(OMB_ERR_UNSUPPORTED, "TOF projections take one frame per call");
+    if (tof.nbins == 1) {
+        switch (frames_per_walk(fr.n)) {
+            case 8: bp_launch<1, 8>(g, rs, tof, gf, fr, sens, st); break;
+            case 4: bp_launch<1, 4>(g, rs, tof, gf, fr, sens, st); break;
+            case 2: bp_launch<1, 2>(g, rs, tof, gf, fr, sens, st); break;
+            default: bp_launch<1, 1>(g, rs, tof, gf, fr, sens, st); break;
+        }
+    } else {
+        switch (tof.nbins) {
+#define X(n) case n: bp_launch<n, 1>(g, rs, tof, gf, fr, sens, st); break;
+            OMB_NB_CASES(X)
+#undef X
+            default:
+                return set_error(OMB_ERR_UNSUPPORTED, "TOF bin count above 16 is not built");
+        }
+    }
+    OMB_LAUNCH_CHECK("siddon backward launch");
+    return OMB_OK;
+}
+
+int siddon_backward_fixed(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *y,
+                          unsigned long long *acc, unsigned long long *acc_sens, cudaStream_t st) {
     if (rs.m_size <= 0) return OMB_OK;
     switch (tof.nbins) {
-#define X(n) case n: bp_nb<n>(g, rs, tof, gf, y, img, sens, acc, acc_sens, mode, st); break;
+#define X(n) case n: bp_fixed_launch<n>(g, rs, tof, gf, y, acc, acc_sens, st); break;
         OMB_NB_CASES(X)
 #undef X
         default:
             return set_error(OMB_ERR_UNSUPPORTED, "TOF bin count above 16 is not built");
     }
-    OMB_LAUNCH_CHECK("siddon backward launch");
+    OMB_LAUNCH_CHECK("siddon fixed-point backward launch");
     return OMB_OK;
 }
 

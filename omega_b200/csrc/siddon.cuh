@@ -12,6 +12,10 @@
 //  * parametric positions along the ray are t0 + n*tu (one FMA from an
 //    integer step count) instead of a running sum, so FP32 rounding does not
 //    accumulate along long oblique rays;
+//  * the per-ray set-up (entry/exit parameters, first voxel, intersection
+//    count, in-plane row bounds) runs in FP64 -- rays entering exactly on a
+//    voxel corner lose their first voxel, or the whole ray, to FP32 rounding
+//    in the reference algorithm; the per-voxel walk stays FP32;
 //  * divisions are IEEE (no --use_fast_math); TOF exponentials use __expf;
 //  * the in-plane perpendicular backprojection addresses voxel (i, j, k) as
 //    i + j*Nx + k*Nx*Ny for every image shape (the reference's linear index
@@ -89,54 +93,57 @@ __device__ __forceinline__ Ray load_ray(const RaySet &rs, int64_t r) {
     return ray;
 }
 
-__device__ __forceinline__ int perpendicular_start(float b, float d, float dd, int n) {
-    int t = (int)floorf((d - b) / dd);
+__device__ __forceinline__ int perpendicular_start(double b, double d, double dd, int n) {
+    int t = (int)floor((d - b) / dd);
     if (t < 0 || t >= n) t = 0;
     return t;
 }
 
 // Entry voxel bounds along one axis when the source coordinate is below the
-// detector's (Jacobs et al. eqs. 11-14) -- d_g_s_precomp.
-__device__ __forceinline__ void dgs_precomp(float tmin, float t_min, float tmax, float t_max, unsigned &vmin,
-                                            unsigned &vmax, float &t0, int &u, float diff, float b, float d,
-                                            float s, unsigned n) {
+// detector's (Jacobs et al. eqs. 11-14) -- d_g_s_precomp.  FP64: these
+// decide where a ray starts and how many voxels it crosses, and rays that
+// enter exactly on a voxel corner (common for crystals on the grid axes)
+// resolve differently in FP32.
+__device__ __forceinline__ void dgs_precomp(double tmin, double t_min, double tmax, double t_max, unsigned &vmin,
+                                            unsigned &vmax, double &t0, int &u, double diff, double b, double d,
+                                            double s, unsigned n) {
     if (tmin == t_min) {
         vmin = 1u;
     } else {
-        const float pt = s + tmin * diff;
-        vmin = __float2uint_ru((pt - b) / d);
+        const double pt = s + tmin * diff;
+        vmin = __double2uint_ru((pt - b) / d);
     }
     if (tmax == t_max) {
         vmax = n;
     } else {
-        const float pt = s + tmax * diff;
-        vmax = __float2uint_rd((pt - b) / d);
+        const double pt = s + tmax * diff;
+        vmax = __double2uint_rd((pt - b) / d);
     }
-    t0 += ((float)vmin * d) / diff;
+    t0 += ((double)vmin * d) / diff;
     u = 1;
 }
 
 // Same when the source coordinate is above the detector's (eqs. 15-18) -- s_g_d_precomp.
-__device__ __forceinline__ void sgd_precomp(float tmin, float t_min, float tmax, float t_max, unsigned &vmin,
-                                            unsigned &vmax, float &t0, int &u, float diff, float b, float d,
-                                            float s, unsigned n) {
+__device__ __forceinline__ void sgd_precomp(double tmin, double t_min, double tmax, double t_max, unsigned &vmin,
+                                            unsigned &vmax, double &t0, int &u, double diff, double b, double d,
+                                            double s, unsigned n) {
     if (tmin == t_min) {
         vmax = n - 1u;
     } else {
-        const float pt = s + tmin * diff;
-        vmax = __float2uint_rd((pt - b) / d);
+        const double pt = s + tmin * diff;
+        vmax = __double2uint_rd((pt - b) / d);
     }
     if (tmax == t_max) {
         vmin = 0u;
     } else {
-        const float pt = s + tmax * diff;
-        vmin = __float2uint_ru((pt - b) / d);
+        const double pt = s + tmax * diff;
+        vmin = __double2uint_ru((pt - b) / d);
     }
-    t0 += ((float)vmax * d) / diff;
+    t0 += ((double)vmax * d) / diff;
     u = -1;
 }
 
-// Per-axis walk state: next boundary t0 + n*tu.
+// Per-axis walk state: next boundary t0 + n*tu (FP32, from the FP64 set-up).
 struct Axis {
     float t0;   // first boundary crossing
     float tu;   // spacing of boundary crossings
@@ -145,22 +152,22 @@ struct Axis {
     __device__ __forceinline__ float next() const { return fmaf((float)n, tu, t0); }
 };
 
-// 2-D pre-loop (siddon_pre_loop_2D): fills the two moving axes.  Returns true
-// when the ray misses the grid.
-__device__ __forceinline__ bool pre_loop_2d(float b1, float b2, float diff1, float diff2, float max1, float max2,
-                                            float d1, float d2, int n1, int n2, int &t1, int &t2, Axis &a1,
-                                            Axis &a2, unsigned &np, float xs, float ys, float xd, float yd,
-                                            float &tc) {
-    const float apu_tx = b1 - xs;
-    const float apu_ty = b2 - ys;
-    float t10 = apu_tx / diff1;
-    float t20 = apu_ty / diff2;
-    const float txback = (max1 - xs) / diff1;
-    const float tyback = (max2 - ys) / diff2;
-    const float txmin = fminf(t10, txback), txmax = fmaxf(t10, txback);
-    const float tymin = fminf(t20, tyback), tymax = fmaxf(t20, tyback);
-    tc = fmaxf(txmin, tymin);
-    const float tmax = fminf(txmax, tymax);
+// 2-D pre-loop (siddon_pre_loop_2D) in FP64: fills the two moving axes.
+// Returns true when the ray misses the grid.
+__device__ __forceinline__ bool pre_loop_2d(double b1, double b2, double diff1, double diff2, double max1,
+                                            double max2, double d1, double d2, int n1, int n2, int &t1, int &t2,
+                                            Axis &a1, Axis &a2, unsigned &np, double xs, double ys, double xd,
+                                            double yd, double &tc) {
+    const double apu_tx = b1 - xs;
+    const double apu_ty = b2 - ys;
+    double t10 = apu_tx / diff1;
+    double t20 = apu_ty / diff2;
+    const double txback = (max1 - xs) / diff1;
+    const double tyback = (max2 - ys) / diff2;
+    const double txmin = fmin(t10, txback), txmax = fmax(t10, txback);
+    const double tymin = fmin(t20, tyback), tymax = fmax(t20, tyback);
+    tc = fmax(txmin, tymin);
+    const double tmax = fmin(txmax, tymax);
     if (tc >= tmax) return true;
     unsigned imin, imax, jmin, jmax;
     if (xs < xd)
@@ -172,54 +179,58 @@ __device__ __forceinline__ bool pre_loop_2d(float b1, float b2, float diff1, flo
     else
         sgd_precomp(tc, tymin, tmax, tymax, jmin, jmax, t20, a2.u, diff2, b2, d2, ys, (unsigned)n2);
     np = imax + 1u + jmax + 1u - imin - jmin;
-    const float pt = (fminf(t10, t20) + tc) / 2.f;
-    t1 = __float2int_rz((pt * diff1 - apu_tx) / d1);
-    t2 = __float2int_rz((pt * diff2 - apu_ty) / d2);
-    a1.t0 = t10;
-    a1.tu = d1 / fabsf(diff1);
+    const double pt = (fmin(t10, t20) + tc) / 2.0;
+    t1 = (int)((pt * diff1 - apu_tx) / d1);
+    t2 = (int)((pt * diff2 - apu_ty) / d2);
+    a1.t0 = (float)t10;
+    a1.tu = (float)(d1 / fabs(diff1));
     a1.n = 0;
-    a2.t0 = t20;
-    a2.tu = d2 / fabsf(diff2);
+    a2.t0 = (float)t20;
+    a2.tu = (float)(d2 / fabs(diff2));
     a2.n = 0;
     if (t1 < 0 || t2 < 0 || t1 >= n1 || t2 >= n2) return true;
     return false;
 }
 
-// 3-D pre-loop (siddon_pre_loop_3D).
-__device__ __forceinline__ bool pre_loop_3d(const Grid &g, float3 s, float3 d, float3 diff, int &ti, int &tj,
-                                            int &tk, Axis &ax, Axis &ay, Axis &az, unsigned &np, float &tc) {
-    const float3 apuT = make_float3(g.bx - s.x, g.by - s.y, g.bz - s.z);
-    float3 t0 = make_float3(apuT.x / diff.x, apuT.y / diff.y, apuT.z / diff.z);
-    const float3 tb = make_float3((g.mx - s.x) / diff.x, (g.my - s.y) / diff.y, (g.mz - s.z) / diff.z);
-    const float3 tmn = make_float3(fminf(t0.x, tb.x), fminf(t0.y, tb.y), fminf(t0.z, tb.z));
-    const float3 tmx = make_float3(fmaxf(t0.x, tb.x), fmaxf(t0.y, tb.y), fmaxf(t0.z, tb.z));
-    tc = fmaxf(fmaxf(tmn.x, tmn.z), tmn.y);
-    const float tmax = fminf(fminf(tmx.x, tmx.z), tmx.y);
+struct D3 {
+    double x, y, z;
+};
+
+// 3-D pre-loop (siddon_pre_loop_3D) in FP64.
+__device__ __forceinline__ bool pre_loop_3d(const Grid &g, D3 s, D3 d, D3 diff, int &ti, int &tj, int &tk, Axis &ax,
+                                            Axis &ay, Axis &az, unsigned &np, double &tc) {
+    const double mx = (double)g.mx, my = (double)g.my, mz = (double)g.mz;
+    const double bx = (double)g.bx, by = (double)g.by, bz = (double)g.bz;
+    const double dx = (double)g.dx, dy = (double)g.dy, dz = (double)g.dz;
+    const D3 apuT{bx - s.x, by - s.y, bz - s.z};
+    D3 t0{apuT.x / diff.x, apuT.y / diff.y, apuT.z / diff.z};
+    const D3 tb{(mx - s.x) / diff.x, (my - s.y) / diff.y, (mz - s.z) / diff.z};
+    const D3 tmn{fmin(t0.x, tb.x), fmin(t0.y, tb.y), fmin(t0.z, tb.z)};
+    const D3 tmx{fmax(t0.x, tb.x), fmax(t0.y, tb.y), fmax(t0.z, tb.z)};
+    tc = fmax(fmax(tmn.x, tmn.z), tmn.y);
+    const double tmax = fmin(fmin(tmx.x, tmx.z), tmx.y);
     if (tc >= tmax) return true;
     unsigned imin, imax, jmin, jmax, kmin, kmax;
     if (s.x < d.x)
-        dgs_precomp(tc, tmn.x, tmax, tmx.x, imin, imax, t0.x, ax.u, diff.x, g.bx, g.dx, s.x, (unsigned)g.nx);
+        dgs_precomp(tc, tmn.x, tmax, tmx.x, imin, imax, t0.x, ax.u, diff.x, bx, dx, s.x, (unsigned)g.nx);
     else
-        sgd_precomp(tc, tmn.x, tmax, tmx.x, imin, imax, t0.x, ax.u, diff.x, g.bx, g.dx, s.x, (unsigned)g.nx);
+        sgd_precomp(tc, tmn.x, tmax, tmx.x, imin, imax, t0.x, ax.u, diff.x, bx, dx, s.x, (unsigned)g.nx);
     if (s.y < d.y)
-        dgs_precomp(tc, tmn.y, tmax, tmx.y, jmin, jmax, t0.y, ay.u, diff.y, g.by, g.dy, s.y, (unsigned)g.ny);
+        dgs_precomp(tc, tmn.y, tmax, tmx.y, jmin, jmax, t0.y, ay.u, diff.y, by, dy, s.y, (unsigned)g.ny);
     else
-        sgd_precomp(tc, tmn.y, tmax, tmx.y, jmin, jmax, t0.y, ay.u, diff.y, g.by, g.dy, s.y, (unsigned)g.ny);
+        sgd_precomp(tc, tmn.y, tmax, tmx.y, jmin, jmax, t0.y, ay.u, diff.y, by, dy, s.y, (unsigned)g.ny);
     if (s.z < d.z)
-        dgs_precomp(tc, tmn.z, tmax, tmx.z, kmin, kmax, t0.z, az.u, diff.z, g.bz, g.dz, s.z, (unsigned)g.nz);
+        dgs_precomp(tc, tmn.z, tmax, tmx.z, kmin, kmax, t0.z, az.u, diff.z, bz, dz, s.z, (unsigned)g.nz);
     else
-        sgd_precomp(tc, tmn.z, tmax, tmx.z, kmin, kmax, t0.z, az.u, diff.z, g.bz, g.dz, s.z, (unsigned)g.nz);
+        sgd_precomp(tc, tmn.z, tmax, tmx.z, kmin, kmax, t0.z, az.u, diff.z, bz, dz, s.z, (unsigned)g.nz);
     np = (kmax - kmin + 1u) + (jmax - jmin + 1u) + (imax - imin + 1u);
-    const float pt = (fminf(fminf(t0.z, t0.y), t0.x) + tc) / 2.f;
-    const float fi = fminf(fmaxf(fmaf(pt, diff.x, -apuT.x) / g.dx, 0.f), (float)(g.nx - 1));
-    const float fj = fminf(fmaxf(fmaf(pt, diff.y, -apuT.y) / g.dy, 0.f), (float)(g.ny - 1));
-    const float fk = fminf(fmaxf(fmaf(pt, diff.z, -apuT.z) / g.dz, 0.f), (float)(g.nz - 1));
-    ti = __float2int_rz(fi);
-    tj = __float2int_rz(fj);
-    tk = __float2int_rz(fk);
-    ax.t0 = t0.x; ax.tu = g.dx / fabsf(diff.x); ax.n = 0;
-    ay.t0 = t0.y; ay.tu = g.dy / fabsf(diff.y); ay.n = 0;
-    az.t0 = t0.z; az.tu = g.dz / fabsf(diff.z); az.n = 0;
+    const double pt = (fmin(fmin(t0.z, t0.y), t0.x) + tc) / 2.0;
+    ti = (int)fmin(fmax((pt * diff.x - apuT.x) / dx, 0.0), (double)(g.nx - 1));
+    tj = (int)fmin(fmax((pt * diff.y - apuT.y) / dy, 0.0), (double)(g.ny - 1));
+    tk = (int)fmin(fmax((pt * diff.z - apuT.z) / dz, 0.0), (double)(g.nz - 1));
+    ax.t0 = (float)t0.x; ax.tu = (float)(dx / fabs(diff.x)); ax.n = 0;
+    ay.t0 = (float)t0.y; ay.tu = (float)(dy / fabs(diff.y)); ay.n = 0;
+    az.t0 = (float)t0.z; az.tu = (float)(dz / fabs(diff.z)); az.n = 0;
     return false;
 }
 
@@ -257,58 +268,62 @@ __device__ __forceinline__ float tof_weights(const Tof &tof, float ddsign, float
 template <int NB, class Visit>
 __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool pet, float global_factor,
                                             const Tof &tof, float &temp, Visit &&vis) {
-    const float3 s = ray.s, d = ray.d;
-    const float3 diff = make_float3(d.x - s.x, d.y - s.y, d.z - s.z);
-    if ((diff.x == 0.f && diff.y == 0.f) || isinf(diff.x) || isinf(diff.y) || isinf(diff.z) || isnan(diff.x) ||
+    // Set-up in FP64 (end points are FP32, so their differences are exact);
+    // the per-voxel walk below runs in FP32.
+    const D3 s{ray.s.x, ray.s.y, ray.s.z}, d{ray.d.x, ray.d.y, ray.d.z};
+    const D3 diff{d.x - s.x, d.y - s.y, d.z - s.z};
+    if ((diff.x == 0.0 && diff.y == 0.0) || isinf(diff.x) || isinf(diff.y) || isinf(diff.z) || isnan(diff.x) ||
         isnan(diff.y) || isnan(diff.z))
         return false;
-    const float L = sqrtf(diff.x * diff.x + diff.y * diff.y + diff.z * diff.z);
-    temp = pet ? (1.f / L) * global_factor : 1.f;
+    const double Ld = sqrt(diff.x * diff.x + diff.y * diff.y + diff.z * diff.z);
+    const float L = (float)Ld;
+    temp = pet ? (float)(1.0 / Ld) * global_factor : 1.f;
     const int64_t nxy = (int64_t)g.nx * g.ny;
     float w[NB > 1 ? NB : 1];
+    const double bx = g.bx, by = g.by, bz = g.bz, dxg = g.dx, dyg = g.dy, dzg = g.dz;
+    const double mx = g.mx, my = g.my, mz = g.mz;
 
-    if (fabsf(diff.z) < 1e-6f && (fabsf(diff.y) < 1e-6f || fabsf(diff.x) < 1e-6f)) {
+    if (fabs(diff.z) < 1e-6 && (fabs(diff.y) < 1e-6 || fabs(diff.x) < 1e-6)) {
         // In-plane ray parallel to a grid axis: every voxel of one row.
-        const int tk = (int)(fabsf(s.z - g.bz) / g.dz);
+        const int tk = (int)(fabs(s.z - bz) / dzg);
         if (tk < 0 || tk >= g.nz) return false;
-        int x1, x2, nrow;
-        float dT1, dT2, d_b, dd, d_db, d_d2;
-        int n0;
+        int x1, x2, nrow, n0;
+        double dT1, dT2, d_b, dd, d_db, d_d2;
         bool along_x;
-        if (fabsf(diff.y) < 1e-6f && d.y <= g.my && d.y >= g.by && s.y <= g.my && s.y >= g.by) {
+        if (fabs(diff.y) < 1e-6 && d.y <= my && d.y >= by && s.y <= my && s.y >= by) {
             along_x = true;
             nrow = g.nx;
-            x1 = 0; x2 = g.nx - 1; dT1 = g.dx; dT2 = g.dx;
-            float dist1, dist2;
-            if (s.x > d.x) { dist1 = g.bx - d.x; dist2 = g.bx + (float)g.nx * g.dx - s.x; }
-            else           { dist1 = g.bx - s.x; dist2 = g.bx + (float)g.nx * g.dx - d.x; }
-            if (dist1 < 0.f) {
-                const int kk = (int)ceilf(-dist1 / g.dx);
-                if (kk < g.nx) { x1 = kk; dT1 = fminf(dist1 + (float)kk * g.dx, g.dx); }
+            x1 = 0; x2 = g.nx - 1; dT1 = dxg; dT2 = dxg;
+            double dist1, dist2;
+            if (s.x > d.x) { dist1 = bx - d.x; dist2 = bx + (double)g.nx * dxg - s.x; }
+            else           { dist1 = bx - s.x; dist2 = bx + (double)g.nx * dxg - d.x; }
+            if (dist1 < 0.0) {
+                const int kk = (int)ceil(-dist1 / dxg);
+                if (kk < g.nx) { x1 = kk; dT1 = fmin(dist1 + (double)kk * dxg, dxg); }
             }
-            if (dist2 > 0.f) {
-                const int mm = (int)ceilf(dist2 / g.dx);
+            if (dist2 > 0.0) {
+                const int mm = (int)ceil(dist2 / dxg);
                 const int kk = g.nx - 1 - mm;
-                if (kk >= x1) { x2 = kk; dT2 = fminf((float)mm * g.dx - dist2, g.dx); }
+                if (kk >= x1) { x2 = kk; dT2 = fmin((double)mm * dxg - dist2, dxg); }
             }
-            d_b = g.by; dd = d.y; d_db = g.dy; d_d2 = g.dx; n0 = g.ny;
-        } else if (fabsf(diff.x) < 1e-6f && d.x <= g.mx && d.x >= g.bx && s.x <= g.mx && s.x >= g.bx) {
+            d_b = by; dd = d.y; d_db = dyg; d_d2 = dxg; n0 = g.ny;
+        } else if (fabs(diff.x) < 1e-6 && d.x <= mx && d.x >= bx && s.x <= mx && s.x >= bx) {
             along_x = false;
             nrow = g.ny;
-            x1 = 0; x2 = g.ny - 1; dT1 = g.dy; dT2 = g.dy;
-            float dist1, dist2;
-            if (s.y > d.y) { dist1 = g.by - d.y; dist2 = g.by + (float)g.ny * g.dy - s.y; }
-            else           { dist1 = g.by - s.y; dist2 = g.by + (float)g.ny * g.dy - d.y; }
-            if (dist1 < 0.f) {
-                const int kk = (int)ceilf(-dist1 / g.dy);
-                if (kk < g.ny) { x1 = kk; dT1 = fminf(dist1 + (float)kk * g.dy, g.dy); }
+            x1 = 0; x2 = g.ny - 1; dT1 = dyg; dT2 = dyg;
+            double dist1, dist2;
+            if (s.y > d.y) { dist1 = by - d.y; dist2 = by + (double)g.ny * dyg - s.y; }
+            else           { dist1 = by - s.y; dist2 = by + (double)g.ny * dyg - d.y; }
+            if (dist1 < 0.0) {
+                const int kk = (int)ceil(-dist1 / dyg);
+                if (kk < g.ny) { x1 = kk; dT1 = fmin(dist1 + (double)kk * dyg, dyg); }
             }
-            if (dist2 > 0.f) {
-                const int mm = (int)ceilf(dist2 / g.dy);
+            if (dist2 > 0.0) {
+                const int mm = (int)ceil(dist2 / dyg);
                 const int kk = g.ny - 1 - mm;
-                if (kk >= x1) { x2 = kk; dT2 = fminf((float)mm * g.dy - dist2, g.dy); }
+                if (kk >= x1) { x2 = kk; dT2 = fmin((double)mm * dyg - dist2, dyg); }
             }
-            d_b = g.bx; dd = d.x; d_db = g.dx; d_d2 = g.dy; n0 = g.nx;
+            d_b = bx; dd = d.x; d_db = dxg; d_d2 = dyg; n0 = g.nx;
         } else {
             return false;
         }
@@ -316,6 +331,7 @@ __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool 
         // voxel (i, j, k): along x -> (ii, row, tk); along y -> (row, ii, tk)
         const int64_t base = (int64_t)tk * nxy + (along_x ? (int64_t)row * g.nx : (int64_t)row);
         const int64_t stride = along_x ? 1 : g.nx;
+        const float fd2 = (float)d_d2, fT1 = (float)dT1, fT2 = (float)dT2;
         // TOF along a row: the reference CPU projector's form
         // (projector_functions.h:1617-1685): D starts at +-half the row length
         // with the sign of the near-zero transverse component taken by
@@ -324,20 +340,20 @@ __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool 
         // integrates a full voxel width.
         float D = 0.f, ddsign = 0.f;
         if (NB > 1) {
-            D = (d_d2 * (float)nrow) / copysignf(2.f, along_x ? diff.y : diff.x);
+            D = (float)((d_d2 * (double)nrow) / copysign(2.0, along_x ? diff.y : diff.x));
             ddsign = sgnf(D);
         }
         for (int ii = x1; ii <= x2; ++ii) {
-            float d_in = d_d2;
-            if (x1 > 0 && ii == x1) d_in = dT1;
-            else if (x2 < nrow - 1 && ii == x2) d_in = dT2;
+            float d_in = fd2;
+            if (x1 > 0 && ii == x1) d_in = fT1;
+            else if (x2 < nrow - 1 && ii == x2) d_in = fT2;
             float tsum = 1.f;
             if (NB > 1) {
-                tsum = tof_weights<NB>(tof, ddsign, d_d2, D, w);
-                if (d_in != d_d2) tof_weights<NB>(tof, ddsign, d_in, D, w);
+                tsum = tof_weights<NB>(tof, ddsign, fd2, D, w);
+                if (d_in != fd2) tof_weights<NB>(tof, ddsign, d_in, D, w);
             }
             vis(base + (int64_t)ii * stride, d_in, w, tsum);
-            if (NB > 1) D -= d_d2 * ddsign;
+            if (NB > 1) D -= fd2 * ddsign;
         }
         return true;
     }
@@ -345,34 +361,35 @@ __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool 
     int ti = 0, tj = 0, tk = 0;
     Axis ax{1e8f, 0.f, 0, 0}, ay{1e8f, 0.f, 0, 0}, az{1e8f, 0.f, 0, 0};
     unsigned np = 0u;
-    float tc = 0.f;
+    double tcd = 0.0;
     bool skip;
-    if (fabsf(diff.z) < 1e-6f) {
-        tk = (int)(fabsf(s.z - g.bz) / g.dz);
+    if (fabs(diff.z) < 1e-6) {
+        tk = (int)(fabs(s.z - bz) / dzg);
         if (tk < 0 || tk >= g.nz) return false;
-        skip = pre_loop_2d(g.bx, g.by, diff.x, diff.y, g.mx, g.my, g.dx, g.dy, g.nx, g.ny, ti, tj, ax, ay, np, s.x,
-                           s.y, d.x, d.y, tc);
-    } else if (fabsf(diff.y) < 1e-6f) {
-        tj = perpendicular_start(g.by, d.y, g.dy, g.ny);
-        skip = pre_loop_2d(g.bx, g.bz, diff.x, diff.z, g.mx, g.mz, g.dx, g.dz, g.nx, g.nz, ti, tk, ax, az, np, s.x,
-                           s.z, d.x, d.z, tc);
-        if (d.y > g.my || d.y < g.by) skip = true;
-    } else if (fabsf(diff.x) < 1e-6f) {
-        ti = perpendicular_start(g.bx, d.x, g.dx, g.nx);
-        skip = pre_loop_2d(g.by, g.bz, diff.y, diff.z, g.my, g.mz, g.dy, g.dz, g.ny, g.nz, tj, tk, ay, az, np, s.y,
-                           s.z, d.y, d.z, tc);
-        if (d.x > g.mx || d.x < g.bx) skip = true;
+        skip = pre_loop_2d(bx, by, diff.x, diff.y, mx, my, dxg, dyg, g.nx, g.ny, ti, tj, ax, ay, np, s.x, s.y, d.x,
+                           d.y, tcd);
+    } else if (fabs(diff.y) < 1e-6) {
+        tj = perpendicular_start(by, d.y, dyg, g.ny);
+        skip = pre_loop_2d(bx, bz, diff.x, diff.z, mx, mz, dxg, dzg, g.nx, g.nz, ti, tk, ax, az, np, s.x, s.z, d.x,
+                           d.z, tcd);
+        if (d.y > my || d.y < by) skip = true;
+    } else if (fabs(diff.x) < 1e-6) {
+        ti = perpendicular_start(bx, d.x, dxg, g.nx);
+        skip = pre_loop_2d(by, bz, diff.y, diff.z, my, mz, dyg, dzg, g.ny, g.nz, tj, tk, ay, az, np, s.y, s.z, d.y,
+                           d.z, tcd);
+        if (d.x > mx || d.x < bx) skip = true;
     } else {
-        skip = pre_loop_3d(g, s, d, diff, ti, tj, tk, ax, ay, az, np, tc);
+        skip = pre_loop_3d(g, s, d, diff, ti, tj, tk, ax, ay, az, np, tcd);
     }
     if (skip) return false;
 
     float D = 0.f, ddsign = 0.f;
     if (NB > 1) {
-        const float dxc = diff.x * tc, dyc = diff.y * tc, dzc = diff.z * tc;
-        D = sqrtf(dxc * dxc + dyc * dyc + dzc * dzc) - L / 2.f;
+        const double a = diff.x * tcd, b = diff.y * tcd, c = diff.z * tcd;
+        D = (float)(sqrt(a * a + b * b + c * c) - Ld / 2.0);
         ddsign = sgnf(D);
     }
+    float tc = (float)tcd;
     float tx = ax.next(), ty = ay.next(), tz = az.next();
     for (unsigned ii = 0u; ii < np; ++ii) {
         const int64_t ind = (int64_t)tj * g.nx + ti + (int64_t)tk * nxy;

@@ -529,7 +529,14 @@ class projectorClass:
         return a
 
     def measurementCount(self, subset):
-        return int(_native.lib().omb_measurement_count(self._handle, int(subset)))
+        """Measurements (all TOF bins) of one subset, or of all with -1."""
+        self._check_ready()
+        m = int(_native.lib().omb_measurement_count(self._handle, int(subset)))
+        if m < 0:
+            _native.check("omb_measurement_count", _native.lib().omb_forward(
+                self._handle, int(subset), ctypes.c_void_p(1), ctypes.c_void_p(1), None))
+            raise ValueError(f'invalid subset {subset}')
+        return m
 
     def forwardProject(self, f, subset=-1):
         """y = A_subset f (projfunctions.py:86)."""
