@@ -533,9 +533,7 @@ class projectorClass:
         self._check_ready()
         m = int(_native.lib().omb_measurement_count(self._handle, int(subset)))
         if m < 0:
-            _native.check("omb_measurement_count", _native.lib().omb_forward(
-                self._handle, int(subset), ctypes.c_void_p(1), ctypes.c_void_p(1), None))
-            raise ValueError(f'invalid subset {subset}')
+            _native.check("omb_measurement_count", -1)
         return m
 
     def forwardProject(self, f, subset=-1):
