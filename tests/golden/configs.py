@@ -36,7 +36,7 @@ def _segments(rings, span, ring_difference, nz):
 
 
 CONFIGS = {
-    # BASELINE workload 0 (PET OSEM, plain method)
+    # the CPU-runnable PET OSEM workload (plain method)
     "pet_cfg0": _pet(16, 18, 16, 600, 144, 144, 64, 16, 300, 64, NSinos=31, TotSinos=181),
     # small PET, all oblique segments, 4 subsets
     "pet_mini": _pet(8, 12, 8, 300, 40, 48, 32, 15, 180, 34, subsets=4),
@@ -50,7 +50,7 @@ CONFIGS = {
     "pet_stype2": _pet(8, 6, 4, 300, 20, 24, 16, 7, 180, 18, subsets=3, subset_type=2),
     "pet_stype4": _pet(8, 6, 4, 300, 20, 24, 16, 7, 180, 18, subsets=4, subset_type=4),
     "pet_stype5": _pet(8, 6, 4, 300, 20, 24, 16, 7, 180, 18, subsets=4, subset_type=5),
-    # cone-beam CT, flat panel (scaled-down BASELINE workload 1 geometry)
+    # cone-beam CT, flat panel (scaled-down 512x512-panel, 360-view geometry)
     "ct_mini": dict(CT=True, nRowsD=48, nColsD=40, nProjections=36, dPitchX=1.6, dPitchY=1.6,
                     sourceToCRot=500., sourceToDetector=1000., Nx=32, Ny=32, Nz=24, FOVa_x=64., FOVa_y=64.,
                     axial_fov=48., projector_type=1, subsets=6, subsetType=8, Niter=1, verbose=0,
