@@ -202,6 +202,34 @@ int omb_loglik(const float *y, const float *fp, int64_t n, float epps, double *o
                void *work, void *stream);
 size_t omb_reduce_workspace_bytes(int64_t n);
 
+/*
+ * Largest image (voxels) omb_backward_fixed64_noalloc accepts.  Its int64
+ * scratch is a fixed array of 2 * OMB_NOALLOC_MAX_VOXELS * 8 bytes (16 MiB)
+ * in device memory of every GPU that loads this library, held until exit.
+ */
+#define OMB_NOALLOC_MAX_VOXELS (1u << 20)
+
+/*
+ * Int64 fixed-point backprojection (projector type 1) that allocates nothing,
+ * for callers that cannot call cudaMalloc -- their device memory belongs to
+ * another allocator (a framework's caching pool, or a pipeline that fixes its
+ * memory budget at start-up).  No counterpart in the reference: it is the
+ * allocation-free form of omb_backward(..., OMB_BP_FIXED64, ...) and gives
+ * the same result.
+ * No handle: `desc` is the same descriptor as for omb_create, except that
+ * desc->xy, desc->z and desc->tof_centers are DEVICE pointers (n_meas stays
+ * a host array).  y, image and sens (may be NULL) are device buffers; image
+ * and sens are overwritten.  Images above OMB_NOALLOC_MAX_VOXELS voxels are
+ * rejected with OMB_ERR_UNSUPPORTED.
+ * The scratch array is shared by all calls and keeps the last call's
+ * contents (each call clears what it uses); calls that overlap on the GPU
+ * (different streams or threads on one device) race on it.  The first call
+ * on each device looks up the array's device address (cudaGetSymbolAddress)
+ * and caches it; make that first call before any stream capture.
+ */
+int omb_backward_fixed64_noalloc(const omb_geometry_desc *desc, int32_t subset, const float *y, float *image,
+                                 float *sens, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
