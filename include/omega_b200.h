@@ -192,6 +192,33 @@ int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream);
 int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, void *stream);
 
 /*
+ * One PDHG iteration with a TV-gradient term over all projections (one
+ * subset), on the device, no host synchronisation:
+ *   p      = (p + sigma * (A x - y)) / (1 + sigma)
+ *   rhs    = A^T p + beta * gradTV(x)       (smoothed TV, edge-clamped neighbours)
+ *   u_new  = max(epps, u - tau * rhs)       (max only when positivity != 0)
+ *   x_next = u_new + theta * (u_new - u);   u = u_new
+ * x_next must differ from x (the caller swaps them).  work_meas holds
+ * omb_measurement_count(h, -1) floats, work_img Nx*Ny*Nz.
+ * Restates computeForwardProject.h:227-316 (dual), priors.h:404-409 with
+ * TVKernel auxKernels.cl:1733-1990 (TV gradient), algorithms.h:329-420 with
+ * PDHGUpdate auxKernels.cl:2034-2062 (primal).
+ */
+int omb_pdhg_iteration(omb_handle *h, float *x, float *x_next, float *u, float *p, const float *y, float tau,
+                       float sigma, float theta, float beta, float tv_smooth, int32_t positivity, float *work_meas,
+                       float *work_img, void *stream);
+
+/*
+ * Largest eigenvalue L of A^T A by n_iter power iterations starting from x
+ * (unit norm; overwritten with the last iterate).  The PDHG primal step is
+ * tau = 1/L with sigma = 1 (functions.hpp:2417-2540, 2886-2905).  `work`
+ * holds omb_power_workspace_bytes() bytes.  Synchronises `stream`.
+ */
+int omb_power_method(omb_handle *h, int32_t n_iter, float *x, float *work_meas, float *work_img, void *work,
+                     double *out_host, void *stream);
+size_t omb_power_workspace_bytes(void);
+
+/*
  * Poisson log-likelihood sum_i [ y_i * log(fp_i + epps) - (fp_i + epps) ],
  * accumulated in FP64 on the device, written to *out_host.  Synchronises
  * `stream`.  `work` is caller scratch of at least omb_reduce_workspace_bytes(n)

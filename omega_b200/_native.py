@@ -90,6 +90,14 @@ EXPORTS = [
     ("omb_reduce_workspace_bytes", ctypes.c_size_t, [ctypes.c_int64]),
     ("omb_backward_fixed64_noalloc", ctypes.c_int, [ctypes.POINTER(GeometryDesc), ctypes.c_int32, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_pdhg_iteration", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_float,
+                                          ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_power_method", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.c_void_p]),
+    ("omb_power_workspace_bytes", ctypes.c_size_t, []),
     ("omb_intersection_count", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
                                               ctypes.c_void_p]),
 ]

@@ -1,5 +1,6 @@
 // C-ABI entry points (include/omega_b200.h): handle life cycle, argument
 // validation and dispatch to the projector kernels.
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -35,8 +36,58 @@ struct omb_handle {
     float *d_z = nullptr;
     float *d_tofc = nullptr;
     unsigned long long *d_acc = nullptr;  // 2 * N int64 accumulators (fixed-point BP)
+    float *d_imgT = nullptr;              // y-fastest image copy (type-5 forward projection)
+    BddProj *d_bddp = nullptr;            // per-projection maps (type-5 backprojection)
     int64_t n_img = 0;
 };
+
+// Type-5 backprojection maps of every projection, FP64 on the host from the
+// same vectors the reference's computeGeom5 uses (omegatomo/projector/
+// init.py:6-37): panel corner d3 = d - apuX - apuY, unit axes along apuX and
+// apuY, plane normal cross(apuX - apuY, -apuX - apuY).
+static std::vector<BddProj> bdd_maps(const omb_geometry_desc &d) {
+    std::vector<BddProj> out((size_t)d.n_proj);
+    const double nr2 = (double)d.n_rows_d / 2.0, nc2 = (double)d.n_cols_d / 2.0;
+    for (int64_t p = 0; p < d.n_proj; ++p) {
+        const float *q = d.xy + p * 6;
+        const double s[3] = {q[0], q[1], q[2]}, dd[3] = {q[3], q[4], q[5]};
+        const double ax[3] = {d.z[p * 2] * nr2, d.z[p * 2 + 1] * nr2, 0.0};
+        const double ay[3] = {0.0, 0.0, nc2 * (double)d.dpitch_y};
+        double d3[3], d2[3], e[3];
+        for (int k = 0; k < 3; ++k) {
+            d3[k] = dd[k] - ax[k] - ay[k];
+            d2[k] = ax[k] - ay[k];
+            e[k] = -ax[k] - ay[k];
+        }
+        double n[3] = {d2[1] * e[2] - d2[2] * e[1], d2[2] * e[0] - d2[0] * e[2], d2[0] * e[1] - d2[1] * e[0]};
+        const double nl = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        const double lx = sqrt(ax[0] * ax[0] + ax[1] * ax[1]), ly = fabs(ay[2]);
+        const double ex[3] = {ax[0] / lx, ax[1] / lx, 0.0}, ey[3] = {0.0, 0.0, ay[2] / ly};
+        for (int k = 0; k < 3; ++k) n[k] /= nl;
+        auto dot = [](const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+        const double sd[3] = {s[0] - d3[0], s[1] - d3[1], s[2] - d3[2]};
+        const double A = dot(ex, sd), Av = dot(ey, sd), B = -dot(n, sd);
+        const double D0 = -dot(n, s);  // n.(q - s) at q = 0
+        BddProj P{};
+        double cu[3], cv[3];
+        for (int k = 0; k < 3; ++k) {
+            cu[k] = A * n[k] + B * ex[k];
+            cv[k] = Av * n[k] + B * ey[k];
+        }
+        for (int k = 0; k < 3; ++k) {
+            P.au[k] = (float)(cu[k] / ((double)d.dpitch_x * D0));
+            P.av[k] = (float)(cv[k] / ((double)d.dpitch_y * D0));
+            P.c[k] = (float)(n[k] / D0);
+            P.s[k] = (float)s[k];
+        }
+        P.au0 = (float)(-dot(cu, s) / ((double)d.dpitch_x * D0));
+        P.av0 = (float)(-dot(cv, s) / ((double)d.dpitch_y * D0));
+        P.ysl = fabs(s[0]) <= fabs(s[1]);
+        P.spos = P.ysl ? (s[1] > 0.0) : (s[0] > 0.0);
+        out[(size_t)p] = P;
+    }
+    return out;
+}
 
 static int validate(const omb_geometry_desc *d) {
     if (!d) return set_error(OMB_ERR_INVALID, "geometry descriptor is NULL");
@@ -46,8 +97,14 @@ static int validate(const omb_geometry_desc *d) {
     if (d->abi_version != OMB_ABI_VERSION) return set_error(OMB_ERR_INVALID, "unsupported abi_version");
     if (d->modality != OMB_PET_SINOGRAM && d->modality != OMB_CT_PANEL)
         return set_error(OMB_ERR_INVALID, "modality must be OMB_PET_SINOGRAM or OMB_CT_PANEL");
-    if (d->fp_type != 1) return set_error(OMB_ERR_UNSUPPORTED, "forward projector type " + std::to_string(d->fp_type) + " is not built");
-    if (d->bp_type != 1) return set_error(OMB_ERR_UNSUPPORTED, "backprojector type " + std::to_string(d->bp_type) + " is not built");
+    if (d->fp_type != 1 && d->fp_type != 5)
+        return set_error(OMB_ERR_UNSUPPORTED, "forward projector type " + std::to_string(d->fp_type) + " is not built");
+    if (d->bp_type != 1 && d->bp_type != 5)
+        return set_error(OMB_ERR_UNSUPPORTED, "backprojector type " + std::to_string(d->bp_type) + " is not built");
+    if ((d->fp_type == 5 || d->bp_type == 5) && d->modality != OMB_CT_PANEL)
+        return set_error(OMB_ERR_INVALID, "Projector type 5 is only supported with CT data!");
+    if ((d->fp_type == 5 || d->bp_type == 5) && d->tof_bins > 1)
+        return set_error(OMB_ERR_INVALID, "projector type 5 has no TOF");
     if (d->nx == 0 || d->ny == 0 || d->nz == 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
     if (!(d->dx > 0.f) || !(d->dy > 0.f) || !(d->dz > 0.f)) return set_error(OMB_ERR_INVALID, "voxel size must be positive");
     if (d->n_rows_d == 0 || d->n_cols_d == 0) return set_error(OMB_ERR_INVALID, "detector size must be positive");
@@ -188,6 +245,17 @@ int omb_create(const omb_geometry_desc *desc, omb_handle **out) {
         (e = cudaMemcpy(h->d_tofc, desc->tof_centers, desc->tof_bins * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(cuda_fail(e, "upload tof centres"));
     t.centers = h->d_tofc;
+    if (desc->fp_type == 5) {
+        if ((e = cudaMalloc(&h->d_imgT, h->n_img * sizeof(float))) != cudaSuccess)
+            return fail(cuda_fail(e, "cudaMalloc type-5 image copy"));
+    }
+    if (desc->bp_type == 5) {
+        std::vector<BddProj> maps = bdd_maps(*desc);
+        if ((e = cudaMalloc(&h->d_bddp, maps.size() * sizeof(BddProj))) != cudaSuccess)
+            return fail(cuda_fail(e, "cudaMalloc type-5 projection maps"));
+        if ((e = cudaMemcpy(h->d_bddp, maps.data(), maps.size() * sizeof(BddProj), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(cuda_fail(e, "upload type-5 projection maps"));
+    }
     if (desc->fixed64_workspace) {
         if ((e = cudaMalloc(&h->d_acc, 2 * h->n_img * sizeof(unsigned long long))) != cudaSuccess)
             return fail(cuda_fail(e, "cudaMalloc fixed-point accumulators"));
@@ -205,6 +273,8 @@ int omb_destroy(omb_handle *h) {
     cudaFree(h->d_z);
     cudaFree(h->d_tofc);
     cudaFree(h->d_acc);
+    cudaFree(h->d_imgT);
+    cudaFree(h->d_bddp);
     if (prev != h->device) cudaSetDevice(prev);
     delete h;
     return OMB_OK;
@@ -225,6 +295,9 @@ int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, voi
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
+    if (h->desc.fp_type == 5)
+        return bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj, image,
+                           h->d_imgT, y, (cudaStream_t)stream);
     return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, y, rs.m_size),
                           (cudaStream_t)stream);
 }
@@ -239,6 +312,14 @@ int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const fl
     if (st != OMB_OK) return st;
     if (image_stride < h->n_img || y_stride < rs.m_size * h->desc.tof_bins)
         return set_error(OMB_ERR_INVALID, "frame strides smaller than one image / one measurement vector");
+    if (h->desc.fp_type == 5) {
+        for (int fr = 0; fr < n_frames; ++fr) {
+            st = bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj,
+                             images + fr * image_stride, h->d_imgT, y + fr * y_stride, (cudaStream_t)stream);
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
     Frames f{};
     f.n = n_frames;
     f.img_in = images;
@@ -260,6 +341,11 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
     if (st != OMB_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t nb = h->n_img * sizeof(float);
+    if (h->desc.bp_type == 5) {
+        if (mode != OMB_BP_FLOAT_ATOMIC)
+            return set_error(OMB_ERR_UNSUPPORTED, "the type-5 backprojection is a gather; it has no fixed-point mode");
+        return bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y, image, sens, s);
+    }
     if (mode == OMB_BP_FIXED64) {
         unsigned long long *acc = h->d_acc, *acc_s = sens ? h->d_acc + h->n_img : nullptr;
         OMB_CUDA_TRY(cudaMemsetAsync(h->d_acc, 0, (sens ? 2 : 1) * h->n_img * sizeof(unsigned long long), s));
@@ -285,6 +371,14 @@ int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const f
     if (image_stride < h->n_img || y_stride < rs.m_size * h->desc.tof_bins)
         return set_error(OMB_ERR_INVALID, "frame strides smaller than one image / one measurement vector");
     cudaStream_t s = (cudaStream_t)stream;
+    if (h->desc.bp_type == 5) {
+        for (int fr = 0; fr < n_frames; ++fr) {
+            st = bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y + fr * y_stride,
+                              images + fr * image_stride, nullptr, s);
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
     if (image_stride == h->n_img) {
         OMB_CUDA_TRY(cudaMemsetAsync(images, 0, (size_t)n_frames * h->n_img * sizeof(float), s));
     } else {
@@ -306,6 +400,7 @@ int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
+    if (h->desc.bp_type != 1) return set_error(OMB_ERR_UNSUPPORTED, "omb_sensitivity needs backprojector type 1");
     // A^T 1 through the BP kernel's fused sensitivity accumulator, y = NULL.
     OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, h->n_img * sizeof(float), s));
     st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, nullptr, nullptr, rs.m_size),
@@ -320,6 +415,8 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     if (!image || !y_subset || !sens || !work_meas || !work_img)
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osem_subset");
     if (h->desc.modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
+    if (h->desc.fp_type != 1 || h->desc.bp_type != 1)
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset needs projector type 1");
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
@@ -340,6 +437,7 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
 int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, void *stream) {
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
     if (!out_host) return set_error(OMB_ERR_INVALID, "output pointer is NULL");
+    if (h->desc.fp_type != 1) return set_error(OMB_ERR_UNSUPPORTED, "intersection counts are for projector type 1");
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
@@ -355,6 +453,52 @@ int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, voi
     if (e != cudaSuccess) return cuda_fail(e, "intersection count");
     if (st != OMB_OK) return st;
     *out_host = (int64_t)v;
+    return OMB_OK;
+}
+
+int omb_pdhg_iteration(omb_handle *h, float *x, float *x_next, float *u, float *p, const float *y, float tau,
+                       float sigma, float theta, float beta, float tv_smooth, int32_t positivity, float *work_meas,
+                       float *work_img, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!x || !x_next || !u || !p || !y || !work_meas || !work_img)
+        return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_pdhg_iteration");
+    if (x == x_next) return set_error(OMB_ERR_INVALID, "x and x_next must be different buffers");
+    cudaStream_t s = (cudaStream_t)stream;
+    int st = omb_forward(h, -1, x, work_meas, stream);
+    if (st != OMB_OK) return st;
+    const int64_t m = omb_measurement_count(h, -1);
+    st = pdhg_dual(p, work_meas, y, m, sigma, s);
+    if (st != OMB_OK) return st;
+    st = omb_backward(h, -1, p, work_img, nullptr, OMB_BP_FLOAT_ATOMIC, stream);
+    if (st != OMB_OK) return st;
+    return pdhg_primal_tv(h->grid, x, work_img, u, x_next, beta, tv_smooth, tau, theta, h->desc.epps, positivity, s);
+}
+
+size_t omb_power_workspace_bytes(void) { return 2 * dot_workspace_bytes(); }
+
+int omb_power_method(omb_handle *h, int32_t n_iter, float *x, float *work_meas, float *work_img, void *work,
+                     double *out_host, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!x || !work_meas || !work_img || !work || !out_host)
+        return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_power_method");
+    if (n_iter < 1) return set_error(OMB_ERR_INVALID, "n_iter must be >= 1");
+    cudaStream_t s = (cudaStream_t)stream;
+    double *wl = static_cast<double *>(work);
+    double *wn = wl + dot_workspace_bytes() / sizeof(double);
+    const int64_t n = h->n_img;
+    int st = OMB_OK;
+    for (int it = 0; it < n_iter && st == OMB_OK; ++it) {
+        st = omb_forward(h, -1, x, work_meas, stream);
+        if (st == OMB_OK) st = omb_backward(h, -1, work_meas, work_img, nullptr, OMB_BP_FLOAT_ATOMIC, stream);
+        if (st == OMB_OK && it == n_iter - 1) st = dot2(work_img, x, n, wl, s);  // (A^T A x).x and x.x
+        if (st == OMB_OK) st = dot2(work_img, work_img, n, wn, s);
+        if (st == OMB_OK) st = normalize_into(x, work_img, n, wn + dot_workspace_bytes() / sizeof(double) - 2, s);
+    }
+    if (st != OMB_OK) return st;
+    double d[2];
+    OMB_CUDA_TRY(cudaMemcpyAsync(d, wl + dot_workspace_bytes() / sizeof(double) - 2, sizeof(d), cudaMemcpyDeviceToHost, s));
+    OMB_CUDA_TRY(cudaStreamSynchronize(s));
+    *out_host = d[0] / d[1];
     return OMB_OK;
 }
 

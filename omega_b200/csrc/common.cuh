@@ -75,6 +75,19 @@ struct Tof {
     const float *centers;
 };
 
+// Per-projection constants of the distance-driven backprojection: a
+// projective map from world coordinates q to continuous detector pixel-edge
+// coordinates, u = (au.q + au0) / (c.q + 1), v = (av.q + av0) / (c.q + 1),
+// plus the source position and which axis the footprint mid-plane follows.
+struct BddProj {
+    float au[3], au0;
+    float av[3], av0;
+    float c[3];
+    float s[3];
+    int ysl;    // |s.x| <= |s.y|: voxel mid-plane spans x and z
+    int spos;   // sign of the source's dominant coordinate (s.y if ysl, else s.x) > 0
+};
+
 constexpr int kMaxTofBins = 16;
 constexpr int kBlock = 256;
 

@@ -13,6 +13,20 @@ int siddon_backward_fixed(const Grid &g, const RaySet &rs, const Tof &tof, float
 int siddon_count(const Grid &g, const RaySet &rs, const Tof &tof, unsigned long long *total, cudaStream_t st);
 int fixed_to_float(const unsigned long long *acc, float *out, int64_t n, cudaStream_t st);
 
+// Projector type 5 (branchless distance-driven), CT.
+int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
+                int64_t nproj, const float *img, float *imgT, float *y, cudaStream_t st);
+int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
+                 float *sens, cudaStream_t st);
+
+// PDHG + TV and the power method.
+int pdhg_dual(float *p, const float *fp, const float *y, int64_t n, float sigma, cudaStream_t st);
+int pdhg_primal_tv(const Grid &g, const float *x, const float *rhs, float *u, float *x_out, float beta, float smooth,
+                   float tau, float theta, float epps, int positivity, cudaStream_t st);
+size_t dot_workspace_bytes();
+int dot2(const float *a, const float *b, int64_t n, double *work, cudaStream_t st);
+int normalize_into(float *x, const float *b, int64_t n, const double *dots, cudaStream_t st);
+
 // Elementwise steps of the subset updates.
 int osem_ratio(const float *y, float *fp, int64_t n, float epps, cudaStream_t st);
 int em_update(float *img, const float *sens, const float *rhs, int64_t n, float epps, cudaStream_t st);

@@ -449,6 +449,10 @@ class projectorClass:
             keep['tof'] = np.ascontiguousarray(np.asarray(self.TOFCenter, dtype=np.float32).ravel())
             d.tof_centers = _native.f32_ptr(keep['tof'])
         d.dL = float(self.dL)
+        if fpt == 5 or bpt == 5:
+            d.d_size5[0], d.d_size5[1] = float(self.dSizeX[0]), float(self.dSizeY[0])
+            d.d_scale5[0], d.d_scale5[1], d.d_scale5[2] = (float(self.dScaleX[0]), float(self.dScaleY[0]),
+                                                           float(self.dScaleZ[0]))
         d.fixed64_workspace = 1 if self.use_64bit_atomics else 0
         return d, keep
 

@@ -1,0 +1,160 @@
+"""Subset-update loops driven by the projectors: OSEM (PET) and PDHG with a
+TV-gradient term (CT), plus the power method for the PDHG step size.
+
+These are the loops of OMEGA's compiled reconstruction (reconstructionAF.h:
+1053-1500) for the two algorithms on this path, run on the device through
+the C-ABI with one host call per sub-iteration (or one CUDA-graph replay per
+iteration).  All buffers are float32 CUDA torch tensors; nothing here
+synchronises except the power method (which returns a host scalar).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(dev):
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def power_method(options, n_iter=None, seed=0):
+    """Largest eigenvalue of A^T A (options.powerIterations iterations by
+    default, 20 in the reference; functions.hpp:2417-2540)."""
+    import torch
+    options._check_ready()
+    n_iter = int(n_iter if n_iter is not None else getattr(options, "powerIterations", 20))
+    dev = torch.device("cuda", options._device)
+    n = int(options.N[0])
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    x = torch.randn(n, generator=g).abs()
+    x = (x / x.norm()).to(dev)
+    wm = torch.empty(options.measurementCount(-1), device=dev)
+    wi = torch.empty(n, device=dev)
+    work = torch.empty(int(_native.lib().omb_power_workspace_bytes()) // 8 + 1, dtype=torch.float64, device=dev)
+    L = ctypes.c_double()
+    _native.call("omb_power_method", options._handle, n_iter, _ptr(x), _ptr(wm), _ptr(wi), _ptr(work),
+                 ctypes.byref(L), _stream(dev))
+    return L.value
+
+
+class PDHG:
+    """PDHG with the smoothed TV gradient (options.PDHG with options.TV in the
+    reference), one subset.  Step sizes follow the reference: tau = 1/L from
+    the power method, sigma = 1, theta = 1 (functions.hpp:2886-2905)."""
+
+    def __init__(self, options, y, beta, tv_smooth=None, tau=None, sigma=1.0, theta=1.0, x0=None,
+                 positivity=True):
+        import torch
+        options._check_ready()
+        self.o = options
+        self.dev = torch.device("cuda", options._device)
+        n = int(options.N[0])
+        m = options.measurementCount(-1)
+        self.y = options._as_device(y, m, "measurement")
+        if x0 is None:
+            x0 = np.asarray(options.x0, dtype=np.float32)
+        self.x = options._as_device(x0, n, "initial image").clone()
+        self.x_next = torch.empty_like(self.x)
+        self.u = self.x.clone()
+        self.p = torch.zeros(m, device=self.dev)
+        self.wm = torch.empty(m, device=self.dev)
+        self.wi = torch.empty(n, device=self.dev)
+        self.beta = float(beta)
+        self.smooth = float(tv_smooth if tv_smooth is not None else getattr(options, "TVsmoothing", 1e-4))
+        self.tau = float(tau) if tau is not None else 1.0 / power_method(options)
+        self.sigma, self.theta = float(sigma), float(theta)
+        self.positivity = 1 if positivity else 0
+        self.graph = None
+
+    def _step(self, x, x_next):
+        _native.call("omb_pdhg_iteration", self.o._handle, _ptr(x), _ptr(x_next), _ptr(self.u), _ptr(self.p),
+                     _ptr(self.y), self.tau, self.sigma, self.theta, self.beta, self.smooth, self.positivity,
+                     _ptr(self.wm), _ptr(self.wi), _stream(self.dev))
+
+    def iterate(self, n_iter, use_graph=False):
+        """Runs n_iter iterations; returns the current image (a view)."""
+        import torch
+        if not use_graph or (self.graph is None and n_iter < 2):
+            for _ in range(n_iter):
+                self._step(self.x, self.x_next)
+                self.x, self.x_next = self.x_next, self.x
+            return self.x
+        if self.graph is None:
+            # one graph holds two iterations (x -> x_next -> x), so the
+            # buffers are back in place after every replay
+            s = torch.cuda.Stream(self.dev)
+            s.wait_stream(torch.cuda.current_stream(self.dev))
+            with torch.cuda.stream(s):
+                self._step(self.x, self.x_next)  # warm-up outside the capture
+                self._step(self.x_next, self.x)
+            torch.cuda.current_stream(self.dev).wait_stream(s)
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph):
+                self._step(self.x, self.x_next)
+                self._step(self.x_next, self.x)
+            n_iter -= 2
+        for _ in range(n_iter // 2):
+            self.graph.replay()
+        if n_iter % 2:
+            self._step(self.x, self.x_next)
+            self.x, self.x_next = self.x_next, self.x
+        return self.x
+
+
+class OSEM:
+    """OSEM for PET sinograms (options.OSEM in the reference): per-subset
+    sensitivity images in the first pass, then the EM update per subset
+    (computeForwardProject.h:76-101, algorithms.h:12-15)."""
+
+    def __init__(self, options, m, x0=None):
+        import torch
+        options._check_ready()
+        self.o = options
+        self.dev = torch.device("cuda", options._device)
+        n = int(options.N[0])
+        S = int(options.subsets)
+        if x0 is None:
+            x0 = np.asarray(options.x0, dtype=np.float32)
+        self.x = options._as_device(x0, n, "initial image").clone()
+        self.y = [options._as_device(options.subsetMeasurements(m, s), options.measurementCount(s), "measurement")
+                  for s in range(S)]
+        self.sens = [torch.empty(n, device=self.dev) for _ in range(S)]
+        for s in range(S):
+            _native.call("omb_sensitivity", options._handle, s, _ptr(self.sens[s]), _stream(self.dev))
+        self.wm = torch.empty(max(options.measurementCount(s) for s in range(S)), device=self.dev)
+        self.wi = torch.empty(n, device=self.dev)
+        self.graph = None
+
+    def _iteration(self):
+        st = _stream(self.dev)
+        for s in range(int(self.o.subsets)):
+            _native.call("omb_osem_subset", self.o._handle, s, _ptr(self.x), _ptr(self.y[s]), _ptr(self.sens[s]),
+                         _ptr(self.wm), _ptr(self.wi), st)
+
+    def iterate(self, n_iter, use_graph=False):
+        import torch
+        if not use_graph or (self.graph is None and n_iter < 1):
+            for _ in range(n_iter):
+                self._iteration()
+            return self.x
+        if self.graph is None:
+            s = torch.cuda.Stream(self.dev)
+            s.wait_stream(torch.cuda.current_stream(self.dev))
+            with torch.cuda.stream(s):
+                self._iteration()
+            torch.cuda.current_stream(self.dev).wait_stream(s)
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph):
+                self._iteration()
+            n_iter -= 1
+        for _ in range(n_iter):
+            self.graph.replay()
+        return self.x

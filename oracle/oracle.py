@@ -26,6 +26,19 @@ LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_siddon.so")
 
 
+class OracleCT(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("bx", ctypes.c_double), ("by", ctypes.c_double), ("bz", ctypes.c_double),
+        ("n_rows", ctypes.c_int), ("n_cols", ctypes.c_int),
+        ("proj0", ctypes.c_int64), ("n_proj", ctypes.c_int64),
+        ("pitch_x", ctypes.c_double), ("pitch_y", ctypes.c_double),
+        ("xy", ctypes.POINTER(ctypes.c_float)),
+        ("uv", ctypes.POINTER(ctypes.c_float)),
+    ]
+
+
 class OracleGeom(ctypes.Structure):
     _fields_ = [
         ("modality", ctypes.c_int),
@@ -66,6 +79,9 @@ def lib():
         L.oracle_siddon_bp.argtypes = [G, P, P, P]
         L.oracle_siddon_count.argtypes = [G]
         L.oracle_siddon_count.restype = ctypes.c_int64
+        C = ctypes.POINTER(OracleCT)
+        L.oracle_bdd_fp.argtypes = [C, P, P]
+        L.oracle_bdd_bp.argtypes = [C, P, P, P]
         _lib = L
     return _lib
 
@@ -245,3 +261,109 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.float64).ravel()
     den = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
+
+
+# ---------------------------------------------------------------------------
+# Projector type 5 (branchless distance-driven), CT
+# ---------------------------------------------------------------------------
+
+def _ct_struct(geom: Geometry, subset):
+    g = OracleCT()
+    g.nx, g.ny, g.nz = geom.nx, geom.ny, geom.nz
+    g.dx, g.dy, g.dz = geom.d
+    g.bx, g.by, g.bz = geom.b
+    g.n_rows, g.n_cols = geom.n_rows, geom.n_cols
+    g.proj0 = 0 if subset < 0 else int(geom.n_meas[subset])
+    g.n_proj = geom.n_proj if subset < 0 else int(geom.n_meas[subset + 1] - geom.n_meas[subset])
+    g.pitch_x, g.pitch_y = geom.pitch
+    g.xy = geom.xy.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    g.uv = geom.z.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    return g
+
+
+def bdd_forward(geom: Geometry, image, subset):
+    """FP64 branchless distance-driven forward projection of one subset."""
+    img = np.ascontiguousarray(image, dtype=np.float64).ravel()
+    g = _ct_struct(geom, subset)
+    y = np.zeros(geom.rays(subset), dtype=np.float64)
+    if lib().oracle_bdd_fp(ctypes.byref(g), _dp(img), _dp(y)) != 0:
+        raise MemoryError("oracle_bdd_fp")
+    return y
+
+
+def bdd_backward(geom: Geometry, y, subset, sens=False):
+    """FP64 voxel-driven distance-driven backprojection (and its weight sum)."""
+    yy = np.ascontiguousarray(y, dtype=np.float64).ravel()
+    g = _ct_struct(geom, subset)
+    img = np.zeros(geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    if lib().oracle_bdd_bp(ctypes.byref(g), _dp(yy), _dp(img), _dp(s)) != 0:
+        raise MemoryError("oracle_bdd_bp")
+    return (img, s) if sens else img
+
+
+def tv_gradient(u, shape, smooth, beta):
+    """Smoothed TV gradient of auxKernels.cl:1733-1990 (TVKernel, plain TV,
+    no reference image) with the edge-clamped neighbours of its texture path,
+    in FP64.  ``u`` is Fortran-ordered, ``shape`` = (Nx, Ny, Nz)."""
+    nx, ny, nz = shape
+    U = np.asarray(u, dtype=np.float64).reshape((nx, ny, nz), order="F")
+
+    def sh(a, dx=0, dy=0, dz=0):
+        ix = np.clip(np.arange(nx) + dx, 0, nx - 1)
+        iy = np.clip(np.arange(ny) + dy, 0, ny - 1)
+        iz = np.clip(np.arange(nz) + dz, 0, nz - 1)
+        return a[ix][:, iy][:, :, iz]
+
+    uPx, uPy, uPz = sh(U, 1), sh(U, 0, 1), sh(U, 0, 0, 1)
+    uMx, uMy, uMz = sh(U, -1), sh(U, 0, -1), sh(U, 0, 0, -1)
+    uix, uiy = sh(U, -1, 1), sh(U, -1, 0, 1)
+    ujx, ujy = sh(U, 1, -1), sh(U, 0, -1, 1)
+    ukx, uky = sh(U, 1, 0, -1), sh(U, 0, 1, -1)
+
+    def sq(a, b, c):
+        return np.sqrt(a * a + b * b + c * c + smooth)
+
+    p0 = sq(uPx - U, uPy - U, uPz - U)
+    p1 = sq(U - uMx, uix - uMx, uiy - uMx)
+    p2 = sq(ujx - uMy, U - uMy, ujy - uMy)
+    p3 = sq(ukx - uMz, uky - uMz, U - uMz)
+    g = (3 * U - uPx - uPy - uPz) / p0 + (U - uMx) / p1 + (U - uMy) / p2 + (U - uMz) / p3 + 1e-7
+    return (beta * g).ravel(order="F")
+
+
+def power_method(geom: Geometry, n_iter, seed=0, x0=None):
+    """Largest eigenvalue of A^T A by power iteration (functions.hpp:2417-2540)."""
+    if x0 is None:
+        rng = np.random.default_rng(seed)
+        x = np.abs(rng.standard_normal(geom.n_img))
+    else:
+        x = np.asarray(x0, dtype=np.float64).copy()
+    x /= np.linalg.norm(x)
+    L = 0.0
+    for _ in range(n_iter):
+        r = bdd_backward(geom, bdd_forward(geom, x, -1), -1)
+        L = float(np.dot(x, r) / np.dot(x, x))
+        x = r / np.linalg.norm(r)
+    return L
+
+
+def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1.0, eps=1e-5,
+            positivity=True):
+    """PDHG with a TV-gradient term, one subset (computeForwardProject.h:227-316,
+    algorithms.h:329-420, auxKernels.cl:2034-2062), in FP64."""
+    shape = (geom.nx, geom.ny, geom.nz)
+    x = np.asarray(x0, dtype=np.float64).copy()
+    u = x.copy()
+    p = np.zeros(geom.rays(-1), dtype=np.float64)
+    yy = np.asarray(y, dtype=np.float64)
+    for _ in range(n_iter):
+        res = bdd_forward(geom, x, -1) - yy
+        p = (p + sigma * res) / (1.0 + sigma)
+        rhs = bdd_backward(geom, p, -1) + tv_gradient(x, shape, smooth, beta)
+        u_prev = u.copy()
+        u = u - tau * rhs
+        if positivity:
+            u = np.maximum(eps, u)
+        x = u + theta * (u - u_prev)
+    return x

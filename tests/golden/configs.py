@@ -57,6 +57,8 @@ CONFIGS = {
                     angles=np.linspace(0, 2 * np.pi, 36, endpoint=False).astype(np.float32),
                     SinM=np.zeros((48, 40, 36), dtype=np.float32)),
 }
+# the same CT geometry with the branchless distance-driven projector (type 5)
+CONFIGS["ct_mini5"] = dict(CONFIGS["ct_mini"], projector_type=5, subsets=1)
 # TOF width so that the bins cover the FOV diagonal: 7 bins of 85 mm / (c/2) seconds
 CONFIGS["pet_mini_tof"]["TOF_width"] = 85.0 / (2.99792458e11 / 2.)
 
@@ -70,5 +72,8 @@ def apply(options, cfg):
 # Arrays compared bit for bit against the reference after addProjector()
 GEOMETRY_KEYS = ["x", "z", "index", "nMeas", "nMeasSubset", "nProjSubset", "nTotMeas", "dx", "dy", "dz", "bx", "by",
                  "bz", "segment_table", "x0"]
+# projector scales of types 4 and 5 (coordinates.py:209-269), compared when present
+SCALE_KEYS = ["dScaleX4", "dScaleY4", "dScaleZ4", "dSizeX", "dSizeY", "dScaleX", "dScaleY", "dScaleZ", "dSizeZBP",
+              "dSizeXBP", "kerroin", "dL"]
 SCALAR_KEYS = ["nRowsD", "nColsD", "nProjections", "NSinos", "TotSinos", "dPitchX", "dPitchY", "sigma_x", "PET",
                "TOF", "Nang", "Ndist"]

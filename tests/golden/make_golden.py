@@ -24,7 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 REF = os.environ.get("OMEGA_REFERENCE", "/root/reference")
 sys.path.insert(0, HERE)
-from configs import CONFIGS, GEOMETRY_KEYS, SCALAR_KEYS, _pet, apply  # noqa: E402
+from configs import CONFIGS, GEOMETRY_KEYS, SCALAR_KEYS, SCALE_KEYS, _pet, apply  # noqa: E402
 
 PROJ_SETS = ["pet_mini", "pet_tof_small"]
 # small TOF set for projector fixtures (kept separate to keep the files small)
@@ -48,6 +48,9 @@ def geometry(proj, cfg):
         out[k] = np.asarray(getattr(o, k))
     for k in SCALAR_KEYS:
         out["s_" + k] = np.asarray(getattr(o, k))
+    if o.projector_type in (4, 5, 14, 41, 15, 45, 54, 51):
+        for k in SCALE_KEYS:
+            out["p_" + k] = np.asarray(getattr(o, k))
     if o.TOF:
         out["TOFCenter"] = np.asarray(o.TOFCenter)
     if o.CT:

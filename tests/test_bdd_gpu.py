@@ -1,0 +1,122 @@
+"""Parity of the CUDA branchless distance-driven projector (type 5), the
+PDHG+TV iteration and the power method with the FP64 oracle (the
+reference's SAT formulation evaluated exactly).  Bar: relative L2 <= 1e-5."""
+import numpy as np
+import pytest
+
+from conftest import make_options
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def _init(name, **attrs):
+    """Options with attribute overrides applied before addProjector()."""
+    from configs import CONFIGS, apply
+    from omega_b200.projector import proj
+    o = apply(proj.projectorClass(), dict(CONFIGS[name], **attrs))
+    o.addProjector()
+    o.initProj()
+    return o
+
+
+def _t(a, dev):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev)
+
+
+def _phantom(g, seed=0):
+    rng = np.random.default_rng(seed)
+    xs = (np.arange(g.nx) + 0.5) * g.d[0] + g.b[0]
+    ys = (np.arange(g.ny) + 0.5) * g.d[1] + g.b[1]
+    zs = (np.arange(g.nz) + 0.5) * g.d[2] + g.b[2]
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    img = 0.01 * ((X / 25.) ** 2 + (Y / 20.) ** 2 + (Z / 18.) ** 2 < 1)
+    img = img + 0.02 * (((X - 5) / 6.) ** 2 + (Y / 8.) ** 2 + ((Z + 3) / 5.) ** 2 < 1)
+    return (img + 0.002 * rng.random(img.shape)).ravel(order="F")
+
+
+@pytest.mark.parametrize("subsets", [1, 4])
+def test_bdd_forward_matches_oracle(cuda, subsets):
+    o = _init("ct_mini5", subsets=subsets)
+    g = orc.Geometry(o)
+    x = _phantom(g)
+    for s in range(g.n_subsets):
+        y = o.forwardProject(_t(x, cuda), s).cpu().numpy()
+        ref = orc.bdd_forward(g, x, s)
+        assert y.shape == ref.shape
+        assert orc.rel_l2(y, ref) < TOL, (s, orc.rel_l2(y, ref))
+
+
+@pytest.mark.parametrize("subsets", [1, 3])
+def test_bdd_backward_matches_oracle(cuda, subsets):
+    o = _init("ct_mini5", subsets=subsets)
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(3)
+    for s in range(g.n_subsets):
+        y = rng.uniform(0.0, 2.0, g.rays(s)).astype(np.float32)
+        img, sens = o.backwardProject(_t(y, cuda), s, sens=True)
+        ref, rs = orc.bdd_backward(g, y, s, sens=True)
+        assert orc.rel_l2(img.cpu().numpy(), ref) < TOL, s
+        assert orc.rel_l2(sens.cpu().numpy(), rs) < TOL, s
+
+
+def test_bdd_random_image_forward(cuda):
+    """Random voxel values (large local gradients) stress the footprint edges."""
+    o = _init("ct_mini5")
+    g = orc.Geometry(o)
+    x = np.random.default_rng(5).uniform(0, 1, g.n_img)
+    y = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
+    assert orc.rel_l2(y, orc.bdd_forward(g, x, 0)) < TOL
+
+
+def test_power_method_matches_oracle(cuda):
+    import torch
+    from omega_b200 import reconstruction as rec
+    o = _init("ct_mini5")
+    g = orc.Geometry(o)
+    L = rec.power_method(o, 20, seed=7)
+    x0 = torch.randn(g.n_img, generator=torch.Generator().manual_seed(7)).abs().numpy()
+    Lr = orc.power_method(g, 20, x0=x0)
+    assert abs(L - Lr) < 1e-5 * Lr
+
+
+def test_pdhg_tv_matches_oracle(cuda):
+    from omega_b200 import reconstruction as rec
+    o = _init("ct_mini5")
+    g = orc.Geometry(o)
+    truth = _phantom(g, 1)
+    y = orc.bdd_forward(g, truth, -1)
+    tau = 1.0 / orc.power_method(g, 10, seed=2)
+    x0 = np.full(g.n_img, 1e-4)
+    solver = rec.PDHG(o, y, beta=0.05, tv_smooth=1e-4, tau=tau, x0=x0)
+    x = solver.iterate(4).cpu().numpy()
+    ref = orc.pdhg_tv(g, y, x0, 4, tau, beta=0.05, smooth=1e-4, eps=float(o.epps))
+    assert orc.rel_l2(x, ref) < TOL, orc.rel_l2(x, ref)
+
+
+def test_pdhg_graph_replay_equals_eager(cuda):
+    """The type-5 pair is a gather (no atomics): graph replays are bit-identical."""
+    from omega_b200 import reconstruction as rec
+    o = _init("ct_mini5")
+    g = orc.Geometry(o)
+    y = orc.bdd_forward(g, _phantom(g, 2), -1)
+    a = rec.PDHG(o, y, beta=0.02, tau=1e-3).iterate(6, use_graph=False).cpu().numpy()
+    b = rec.PDHG(o, y, beta=0.02, tau=1e-3).iterate(6, use_graph=True).cpu().numpy()
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_osem_graph_replay_matches_eager(cuda):
+    from omega_b200 import reconstruction as rec
+    o = _init("pet_mini")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(4)
+    truth = rng.uniform(0.5, 2.0, g.n_img)
+    m = np.concatenate([rng.poisson(orc.forward(g, truth, s) * 10.0) for s in range(g.n_subsets)]).astype(np.float32)
+    a = rec.OSEM(o, m).iterate(3, use_graph=False).cpu().numpy()
+    b = rec.OSEM(o, m).iterate(3, use_graph=True).cpu().numpy()
+    assert orc.rel_l2(a, b) < 1e-6
+    ys = [m[int(o.nTotMeas[s]):int(o.nTotMeas[s + 1])] for s in range(g.n_subsets)]
+    ref = orc.osem(g, ys, np.ones(g.n_img), 3)
+    assert orc.rel_l2(a, ref) < 5e-5

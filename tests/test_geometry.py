@@ -23,6 +23,9 @@ def test_geometry_bit_exact(name):
     for k in SCALAR_KEYS:
         ours = np.asarray(getattr(o, k))
         assert np.array_equal(ours, g["s_" + k]), f"{name}: {k} {ours} != {g['s_' + k]}"
+    for k in [k for k in g if k.startswith("p_")]:
+        ours = np.asarray(getattr(o, k[2:]))
+        assert ours.dtype == g[k].dtype and np.array_equal(ours, g[k]), f"{name}: {k[2:]} {ours} != {g[k]}"
     if "TOFCenter" in g:
         assert np.array_equal(np.asarray(o.TOFCenter), g["TOFCenter"])
     if "uV" in g:

@@ -16,9 +16,13 @@ TOL = 1e-5
 
 
 def _init(name, **attrs):
-    o = make_options(name)
-    for k, v in attrs.items():
-        setattr(o, k, v)
+    """Options with attribute overrides applied before addProjector()."""
+    from configs import CONFIGS, apply
+    from make_golden import CONFIGS_EXTRA
+    from omega_b200.projector import proj
+    base = CONFIGS[name] if name in CONFIGS else CONFIGS_EXTRA[name]
+    o = apply(proj.projectorClass(), dict(base, **attrs))
+    o.addProjector()
     o.initProj()
     return o
 
