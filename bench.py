@@ -1,25 +1,33 @@
 #!/usr/bin/env python
 """Projector throughput benchmark (one JSON line on rank 0).
 
-Workload (default ``dynpet``): the batching PET study -- a 384-crystal x 32-ring
-scanner (600 mm ring), 256 radial x 192 angle x 63 plane sinograms
-(3,096,576 rays per frame), a 128 x 128 x 63 image over 300 x 300 x 126 mm,
-24 frames of a dynamic study, improved Siddon (projector type 1), 16 subsets
-of whole sinograms.  One step = forward projection of all 24 frames followed
-by backprojection of the 24 resulting sinograms (every ray of every frame
-once forward and once back), as one launch each.
+Default workload ``cbct``: cone-beam CT with a 512 x 512 flat panel (0.4 mm
+pixels), 360 projections over 360 degrees, source-origin 500 mm and
+source-detector 1000 mm, a 256^3 volume of 0.25 mm voxels, a seeded 3-D
+ellipsoid (Shepp-Logan-style) phantom with attenuation 0-0.02 /mm, Poisson
+transmission data at I0 = 1e5 linearised as log(I0 / I), branchless
+distance-driven projector (type 5), PDHG with a TV-gradient term.
+One step = one PDHG iteration over all 360 projections: forward projection
+(94,371,840 rays), dual update, backprojection, TV gradient and primal update.
 
-metric: rays/s of FP+BP pairs (ray-frames forward- and back-projected per
-second).  ``value`` times device-resident inputs with CUDA events; ``e2e``
-times the same step through the C-ABI with pinned host images copied in and
-the backprojected images copied out.  ``cpu_baseline`` is the reference's own
-OpenMP CPU projector (projector_functions.h:1312, built into oracle/_ref) on
-a bounded sample of the same workload.
+metric: rays/s of FP+BP pairs (rays forward- and back-projected per second).
+``value`` times device-resident data with CUDA events; ``e2e`` times a
+forward+back projection through the C-ABI with the image copied in from
+pinned host memory and the backprojection copied out, every step.
+``cpu_baseline``: the reference has no CPU code for projector type 5
+(proj.py:1212-1213 rejects it), so the CPU figure is the FP64 OpenMP
+restatement of its kernels on a bounded sample, labelled "port".
 
---impl reference times that reference CPU projector alone (all host threads)
-on the same metric; under torchrun only rank 0 runs it.
-Multi-GPU: replicas (each rank projects its own 24-frame batch; no
-collective on the data path); value = all ranks' ray-frames / max rank time.
+Workload ``dynpet``: 24-frame dynamic PET on a 384-crystal x 32-ring
+scanner, 256 x 192 x 63 sinograms, 128 x 128 x 63 image, improved Siddon;
+one step = forward projection of all frames then backprojection of all
+frames; CPU baseline = the reference's own OpenMP projector.
+
+--impl reference times the reference CPU implementation of the same step
+(the OpenMP projector for dynpet, the restatement for cbct) with all host
+threads on a bounded sample.  Under torchrun only rank 0 runs it.
+Multi-GPU: replicas (each rank runs its own copy of the workload, no
+collective on the data path); value = all ranks' rays / max rank time.
 """
 from __future__ import annotations
 
@@ -51,7 +59,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="dynpet", choices=["dynpet", "dynpet_small"])
+    p.add_argument("--workload", default="cbct", choices=["cbct", "cbct_small", "dynpet", "dynpet_small"])
     p.add_argument("--frames", type=int, default=None)
     p.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     return p.parse_args()
@@ -165,223 +173,484 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's own OpenMP projector on a bounded sample
+# cone-beam CT workload
 # ---------------------------------------------------------------------------
 
-def cpu_baseline(o, image, seconds=10.0):
-    from oracle import oracle as orc
-    g = orc.Geometry(o)
-    threads = os.cpu_count() or 1
-    use_ref = orc.ref_lib() is not None
-    subset = 0
-    rays = g.rays(subset)
-    done = 0
-    t0 = time.perf_counter()
-    while True:
-        if use_ref:
-            y = orc.ref_forward(g, image, subset, precision="float", threads=threads)
-            orc.ref_backward(g, y, subset, precision="float", threads=threads)
-        else:
-            y = orc.forward(g, image, subset)
-            orc.backward(g, y, subset)
-        done += rays
-        el = time.perf_counter() - t0
-        if el >= seconds:
-            break
-    cpu_model = ""
+def cbct_options(small=False):
+    from omega_b200.projector import proj
+    o = proj.projectorClass()
+    panel, nproj, n = (128, 90, 64) if small else (512, 360, 256)
+    o.CT = True
+    o.nRowsD = o.nColsD = panel
+    o.nProjections = nproj
+    o.dPitchX = o.dPitchY = 0.4 * (512 // panel)
+    o.sourceToCRot, o.sourceToDetector = 500., 1000.
+    o.Nx = o.Ny = o.Nz = n
+    o.FOVa_x = o.FOVa_y = o.axial_fov = 64.
+    o.angles = np.linspace(0, 2 * np.pi, nproj, endpoint=False).astype(np.float32)
+    o.projector_type = 5
+    o.subsets, o.subsetType = 1, 8
+    o.PDHG, o.TV = True, True
+    o.beta, o.TVsmoothing = 0.05, 1e-4
+    o.verbose = 0
+    o.SinM = np.zeros((panel, panel, nproj), dtype=np.float32)  # marks projection data (not list-mode)
+    o.addProjector()
+    o.SinM = np.empty(0, dtype=np.float32)
+    return o
+
+
+def shepp_logan_3d(o, seed=7):
+    """Seeded 3-D ellipsoid phantom, attenuation 0-0.02 /mm: the ten
+    ellipsoids of the 3-D Shepp-Logan layout with randomly jittered centres."""
+    rng = np.random.default_rng(seed)
+    n = int(o.Nx[0])
+    c = (np.arange(n, dtype=np.float32) + 0.5) / n * 2 - 1
+    X, Y, Z = np.meshgrid(c, c, c, indexing="ij")
+    # (mu, a, b, c, x0, y0, z0, phi) in units of the half FOV
+    E = [(0.020, .69, .92, .81, 0, 0, 0, 0), (-0.016, .6624, .874, .78, 0, -.0184, 0, 0),
+         (-0.004, .11, .31, .22, .22, 0, 0, -18), (-0.004, .16, .41, .28, -.22, 0, 0, 18),
+         (0.002, .21, .25, .41, 0, .35, -.15, 0), (0.002, .046, .046, .05, 0, .1, .25, 0),
+         (0.002, .046, .046, .05, 0, -.1, .25, 0), (0.002, .046, .023, .05, -.08, -.605, 0, 0),
+         (0.002, .023, .023, .02, 0, -.606, 0, 0), (0.002, .023, .046, .02, .06, -.605, 0, 0)]
+    img = np.zeros((n, n, n), dtype=np.float32)
+    for mu, a, b, cc, x0, y0, z0, phi in E:
+        x0, y0, z0 = np.array([x0, y0, z0]) + rng.uniform(-0.01, 0.01, 3)
+        t = np.radians(phi)
+        xr = (X - x0) * np.cos(t) + (Y - y0) * np.sin(t)
+        yr = -(X - x0) * np.sin(t) + (Y - y0) * np.cos(t)
+        img[(xr / a) ** 2 + (yr / b) ** 2 + ((Z - z0) / cc) ** 2 <= 1] += mu
+    return np.clip(img, 0, 0.02).ravel(order="F")
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
             for line in f:
                 if line.startswith("model name"):
-                    cpu_model = line.split(":", 1)[1].strip()
-                    break
+                    return line.split(":", 1)[1].strip()
     except OSError:
         pass
-    return {"value": done / el, "unit": "rays/s", "cores": threads if use_ref else 1,
-            "kind": "reference" if use_ref else "port",
-            "sample": f"frame 0, subset 0 ({g.n_meas[1] - g.n_meas[0]} sinograms, {rays} rays), FP+BP pairs "
-                      f"repeated for {el:.1f} s; {'reference projectorType123Implementation4<float> (OpenMP)' if use_ref else 'FP64 oracle restatement'}"
-                      f"; host CPU {cpu_model}"}
+    return ""
 
 
-# ---------------------------------------------------------------------------
-# our arm
-# ---------------------------------------------------------------------------
+class Timed:
+    """Per-step CUDA-event timing of named phases on one stream."""
 
-def run_ours(args, rank, world, local_rank):
+    def __init__(self, stream):
+        import torch
+        self.torch = torch
+        self.stream = stream
+        self.events = []
+
+    def mark(self):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        self.events.append(e)
+
+    def phases(self):
+        self.events[-1].synchronize()
+        out = [a.elapsed_time(b) / 1e3 for a, b in zip(self.events[:-1], self.events[1:])]
+        self.events = []
+        return out
+
+
+def run_timed(args, world, dev, step, n_phases):
+    """Warm-up, then exactly args.steps steps bracketed by barrier + sync,
+    with an L2 flush between steps outside the events.  Returns per-phase
+    totals (seconds), the clock record and the wall time."""
     import torch
     import torch.distributed as dist
-    from omega_b200 import _native
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    small = args.workload == "dynpet_small"
-    frames = args.frames or (4 if small else 24)
-    o = dynamic_pet_options(small)
-    o.initProj()
-    L = _native.lib()
-    h = o._handle
-    n = int(o.N[0])
-    m = o.measurementCount(-1)
-    rays_per_frame = m
-    imgs_host = dynamic_images(o, frames)
-    imgs = torch.from_numpy(imgs_host).to(dev)
-    ys = torch.empty((frames, m), device=dev)
-    back = torch.empty((frames, n), device=dev)
     stream = torch.cuda.current_stream(dev)
-    sp = ctypes.c_void_p(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, device=dev)
-
-    def step():
-        _native.call("omb_forward_frames", h, -1, frames, ctypes.c_void_p(imgs.data_ptr()), n,
-                     ctypes.c_void_p(ys.data_ptr()), m, sp)
-        ev_mid.record(stream)
-        _native.call("omb_backward_frames", h, -1, frames, ctypes.c_void_p(ys.data_ptr()), m,
-                     ctypes.c_void_p(back.data_ptr()), n, sp)
-
-    ev_mid = torch.cuda.Event(enable_timing=True)
+    tm = Timed(stream)
     for _ in range(max(args.warmup, 0)):
-        step()
-    torch.cuda.synchronize()
-    # total voxel intersections of one frame (for the algorithmic-byte model)
-    npx = ctypes.c_int64()
-    _native.call("omb_intersection_count", h, -1, ctypes.byref(npx), sp)
-    sum_np = npx.value
-
+        step(tm)
+        tm.phases()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local_rank)
+    clocks = ClockSampler(dev.index or 0)
     clocks.start()
-    t_fp, t_bp = [], []
+    tot = [0.0] * n_phases
     wall0 = time.perf_counter()
     for _ in range(args.steps):
-        flush.zero_()  # L2 flush between timed steps (outside the events)
-        e0 = torch.cuda.Event(enable_timing=True)
-        ev_mid = torch.cuda.Event(enable_timing=True)
-        e2 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step()
-        e2.record(stream)
-        e2.synchronize()
-        t_fp.append(e0.elapsed_time(ev_mid) / 1e3)
-        t_bp.append(ev_mid.elapsed_time(e2) / 1e3)
+        flush.zero_()
+        step(tm)
+        for i, t in enumerate(tm.phases()):
+            tot[i] += t
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
-    t_step = [a + b for a, b in zip(t_fp, t_bp)]
-    total = sum(t_step)
-    if world > 1:
-        tt = torch.tensor([total], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total = float(tt.item())
+        t = torch.tensor(tot, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot = t.tolist()
+    return tot, clk, wall
 
-    # end to end through the C-ABI: pinned host images in, backprojections out
-    h_in = torch.from_numpy(imgs_host).pin_memory()
-    h_out = torch.empty((frames, n), dtype=torch.float32).pin_memory()
-    e2e_times = []
+
+def e2e_time(args, world, dev, step_host):
+    import torch
+    import torch.distributed as dist
+    stream = torch.cuda.current_stream(dev)
+    times = []
     for it in range(args.warmup + args.steps):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        imgs.copy_(h_in, non_blocking=True)
-        step()
-        h_out.copy_(back, non_blocking=True)
+        step_host()
         e1.record(stream)
         e1.synchronize()
         if it >= args.warmup:
-            e2e_times.append(e0.elapsed_time(e1) / 1e3)
-    e2e_total = sum(e2e_times)
+            times.append(e0.elapsed_time(e1) / 1e3)
+    total = sum(times)
     if world > 1:
-        tt = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
+        t = torch.tensor([total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    return total
 
+
+def roofline(name, nbytes, duration, traffic_key):
+    peak, src = measured_peak()
+    achieved = nbytes / duration / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": src, "algorithmic_bytes": nbytes,
+            "traffic": PROFILED_TRAFFIC.get(traffic_key)}
+
+
+# ---------------------------------------------------------------------------
+# our arm: cone-beam CT, one PDHG+TV iteration per step
+# ---------------------------------------------------------------------------
+
+
+I0 = 1e5
+
+
+def cbct_sample_geometry(o, n_views):
+    """Oracle geometry restricted to the first n_views projections."""
+    from oracle import oracle as orc
+    g = orc.Geometry(o)
+    g.n_meas = np.array([0, n_views], dtype=np.int64)
+    g.n_subsets = 1
+    return g
+
+
+def cbct_cpu_rate(o, image, seconds, views_per_call=4):
+    """FP64 OpenMP restatement of the type-5 pair (there is no reference CPU
+    code for projector type 5) on a bounded sample of projections, repeated
+    for about `seconds`; returns rays/s of FP+BP pairs and the sample."""
+    from oracle import oracle as orc
+    g = cbct_sample_geometry(o, views_per_call)
+    rays = g.rays(0)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        y = orc.bdd_forward(g, image, 0)
+        orc.bdd_backward(g, y, 0)
+        done += rays
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return done / el, f"{views_per_call} of {int(o.nProjections)} projections ({rays} rays) per FP+BP pair, " \
+                      f"{done // rays} pairs in {el:.1f} s"
+
+
+def run_cbct(args, rank, world, dev):
+    import torch
+    from omega_b200 import _native
+    from omega_b200 import reconstruction as rec
+    small = args.workload == "cbct_small"
+    o = cbct_options(small)
+    o.initProj()
+    h = o._handle
+    n = int(o.N[0])
+    m = o.measurementCount(-1)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    # data: Poisson transmission counts at I0, zeros clamped to 1, log(I0/I)
+    mu_host = shepp_logan_3d(o)
+    mu = torch.from_numpy(mu_host).to(dev)
+    yc = torch.empty(m, device=dev)
+    _native.call("omb_forward", h, -1, P(mu), P(yc), sp)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    counts = torch.poisson(I0 * torch.exp(-yc), generator=gen).clamp_(min=1.0)
+    y = torch.log(I0 / counts)
+    del counts, yc
+    tau = 1.0 / rec.power_method(o, 20, seed=0)
+    sigma, theta = 1.0, 1.0
+    beta, smooth = float(o.beta), float(o.TVsmoothing)
+
+    x = torch.full((n,), 1e-4, device=dev)
+    bufs = [x, torch.empty_like(x)]
+    u = x.clone()
+    p = torch.zeros(m, device=dev)
+    wm = torch.empty(m, device=dev)
+    wi = torch.empty(n, device=dev)
+
+    def step(tm):
+        a, b = bufs
+        tm.mark()
+        _native.call("omb_forward", h, -1, P(a), P(wm), sp)
+        tm.mark()
+        _native.call("omb_pdhg_dual", P(p), P(wm), P(y), m, sigma, sp)
+        tm.mark()
+        _native.call("omb_backward", h, -1, P(p), P(wi), None, 0, sp)
+        tm.mark()
+        _native.call("omb_pdhg_primal", h, P(a), P(wi), P(u), P(b), tau, theta, beta, smooth, 1, sp)
+        tm.mark()
+        bufs.reverse()
+
+    tot, clk, wall = run_timed(args, world, dev, step, 4)
+    t_fp, t_dual, t_bp, t_primal = tot
+    total = sum(tot)
+
+    # end to end: the iterate copied in from pinned host memory, one fused
+    # omb_pdhg_iteration, the new iterate copied out
+    h_in = torch.full((n,), 1e-4).pin_memory()
+    h_out = torch.empty(n, dtype=torch.float32).pin_memory()
+
+    def step_host():
+        a, b = bufs
+        a.copy_(h_in, non_blocking=True)
+        _native.call("omb_pdhg_iteration", h, P(a), P(b), P(u), P(p), P(y), tau, sigma, theta, beta, smooth, 1,
+                     P(wm), P(wi), sp)
+        h_out.copy_(b, non_blocking=True)
+
+    e2e_total = e2e_time(args, world, dev, step_host)
     if rank != 0:
         return None
-    ray_frames = rays_per_frame * frames
-    value = ray_frames * args.steps * world / total
-    # roofline of the dominant kernel (algorithmic bytes per launch / its mean duration)
-    fp_bytes = frames * (4 * sum_np + 32 * rays_per_frame)
-    bp_bytes = frames * (8 * sum_np + 28 * rays_per_frame)
-    mean_fp, mean_bp = sum(t_fp) / len(t_fp), sum(t_bp) / len(t_bp)
-    name, nbytes, dur = ("siddon_bp", bp_bytes, mean_bp) if mean_bp >= mean_fp else ("siddon_fp", fp_bytes, mean_fp)
-    peak, peak_src = FALLBACK_HBM_GBS, "fallback"
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peak, peak_src = float(json.load(f)["hbm_gbs"]), "measured"
-    except Exception:
-        pass
-    achieved = nbytes / dur / 1e9
-    traffic = PROFILED_TRAFFIC.get((args.workload, name))
+    K = args.steps
+    value = m * K * world / total
+    nproj = int(o.nProjections)
+    slices = int(o.Nx[0])  # every ray crosses all slices of its main axis (Nx = Ny here)
+    fp_bytes = m * (slices * 16 + 4)
+    bp_bytes = n * nproj * 16 + n * 4
+    mean_fp, mean_bp = t_fp / K, t_bp / K
+    if mean_bp >= mean_fp:
+        rl = roofline("bdd_bp", bp_bytes, mean_bp, (args.workload, "bdd_bp"))
+    else:
+        rl = roofline("bdd_fp", fp_bytes, mean_fp, (args.workload, "bdd_fp"))
+    rl["model"] = ("cache-less tap bytes: FP = rays x (slices x 4 taps x 4 B + 4 B out); BP = voxels x views x "
+                   "4 taps x 4 B + 4 B out. The 67 MB volume is L2-resident, so the taps are served on chip; "
+                   "traffic is the DRAM bytes ncu counted")
+    rl["compulsory_bytes"] = (n + m) * 4
+    panel = int(o.nRowsD)
     line = {
         "metric": "proj+backproj rays/s", "value": value, "unit": "rays/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * total / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded dynamic phantom, gamma-variate time-activity curves)",
-        "config": {"workload": ("dynamic PET, 24 frames, 384 crystals x 32 rings, 256x192x63 sinograms, "
-                                "128x128x63 image, improved Siddon FP+BP") if not small else
-                   "dynamic PET small (8 rings) for profiling",
-                   "frames": frames, "rays_per_frame": rays_per_frame, "intersections_per_frame": sum_np,
-                   "subsets": int(o.subsets), "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (sinograms %.0f MB per step) plus a 256 MB L2 flush between steps"
-                         % (frames * m * 4 / 1e6)},
-        "fp_ms": 1e3 * mean_fp, "bp_ms": 1e3 * mean_bp,
-        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_src,
-                     "algorithmic_bytes": nbytes, "traffic": traffic},
-        "e2e": {"value": ray_frames * args.steps * world / e2e_total, "unit": "rays/s",
-                "h2d_bytes_per_step": frames * n * 4, "d2h_bytes_per_step": frames * n * 4},
-        "gpu_launches": 2 * args.steps,
+        "data": "synthetic (seeded 3-D ellipsoid phantom, Poisson transmission counts at I0=1e5)",
+        "config": {"workload": (f"cone-beam CT, {panel}x{panel} panel 0.4 mm, {nproj} views over 360 deg, "
+                                "SOD 500 / SDD 1000 mm, 256^3 volume 0.25 mm, branchless distance-driven (type 5), "
+                                "one PDHG+TV iteration per step") if not small else
+                   "cone-beam CT small (128^2 panel, 90 views, 64^3) for profiling",
+                   "rays_per_step": m, "voxels": n, "views": nproj, "subsets": 1,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "256 MB L2 flush between steps; the measurement vectors (%.0f MB each) exceed L2"
+                         % (m * 4 / 1e6)},
+        "fp_ms": 1e3 * mean_fp, "bp_ms": 1e3 * mean_bp, "dual_ms": 1e3 * t_dual / K,
+        "primal_tv_ms": 1e3 * t_primal / K, "tau": tau,
+        "roofline": rl,
+        "e2e": {"value": m * K * world / e2e_total, "unit": "rays/s", "h2d_bytes_per_step": n * 4,
+                "d2h_bytes_per_step": n * 4},
+        "gpu_launches": 5 * K,
         "clocks": clk,
         "wall_s": wall,
     }
     if not args.no_baseline and world == 1:
         try:
-            line["cpu_baseline"] = cpu_baseline(o, imgs_host[0])
+            v, sample = cbct_cpu_rate(o, mu_host, 10.0)
+            line["cpu_baseline"] = {"value": v, "unit": "rays/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                    "sample": sample + "; FP64 OpenMP restatement (the reference has no CPU "
+                                              f"type-5 projector); host CPU {cpu_model()}"}
         except Exception as e:  # baseline failures must not hide the GPU number
             line["cpu_baseline"] = {"error": str(e)}
     return line
 
 
 # ---------------------------------------------------------------------------
-# reference arm
+# our arm: dynamic PET, FP of all frames then BP of all frames per step
+# ---------------------------------------------------------------------------
+
+def dynpet_cpu_rate(o, image, seconds):
+    from oracle import oracle as orc
+    g = orc.Geometry(o)
+    threads = os.cpu_count() or 1
+    use_ref = orc.ref_lib() is not None
+    rays = g.rays(0)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        if use_ref:
+            yy = orc.ref_forward(g, image, 0, precision="float", threads=threads)
+            orc.ref_backward(g, yy, 0, precision="float", threads=threads)
+        else:
+            yy = orc.forward(g, image, 0)
+            orc.backward(g, yy, 0)
+        done += rays
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    desc = "reference projectorType123Implementation4<float> (OpenMP)" if use_ref else "FP64 oracle restatement"
+    return done / el, threads if use_ref else 1, "reference" if use_ref else "port", \
+        f"frame 0, subset 0 ({g.n_meas[1] - g.n_meas[0]} sinograms, {rays} rays) per FP+BP pair, " \
+        f"{done // rays} pairs in {el:.1f} s; {desc}"
+
+
+def run_dynpet(args, rank, world, dev):
+    import torch
+    from omega_b200 import _native
+    small = args.workload == "dynpet_small"
+    frames = args.frames or (4 if small else 24)
+    o = dynamic_pet_options(small)
+    o.initProj()
+    h = o._handle
+    n = int(o.N[0])
+    m = o.measurementCount(-1)
+    imgs_host = dynamic_images(o, frames)
+    imgs = torch.from_numpy(imgs_host).to(dev)
+    ys = torch.empty((frames, m), device=dev)
+    back = torch.empty((frames, n), device=dev)
+    sp = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def step(tm):
+        tm.mark()
+        _native.call("omb_forward_frames", h, -1, frames, P(imgs), n, P(ys), m, sp)
+        tm.mark()
+        _native.call("omb_backward_frames", h, -1, frames, P(ys), m, P(back), n, sp)
+        tm.mark()
+
+    npx = ctypes.c_int64()
+    _native.call("omb_intersection_count", h, -1, ctypes.byref(npx), sp)
+    sum_np = npx.value
+    tot, clk, wall = run_timed(args, world, dev, step, 2)
+    t_fp, t_bp = tot
+    total = t_fp + t_bp
+
+    h_in = torch.from_numpy(imgs_host).pin_memory()
+    h_out = torch.empty((frames, n), dtype=torch.float32).pin_memory()
+
+    class _NoMarks:
+        def mark(self):
+            pass
+
+    def step_host():
+        imgs.copy_(h_in, non_blocking=True)
+        step(_NoMarks())
+        h_out.copy_(back, non_blocking=True)
+
+    e2e_total = e2e_time(args, world, dev, step_host)
+    if rank != 0:
+        return None
+    K = args.steps
+    ray_frames = m * frames
+    fp_bytes = frames * (4 * sum_np + 32 * m)
+    bp_bytes = frames * (8 * sum_np + 28 * m)
+    mean_fp, mean_bp = t_fp / K, t_bp / K
+    if mean_bp >= mean_fp:
+        rl = roofline("siddon_bp", bp_bytes, mean_bp, (args.workload, "siddon_bp"))
+    else:
+        rl = roofline("siddon_fp", fp_bytes, mean_fp, (args.workload, "siddon_fp"))
+    line = {
+        "metric": "proj+backproj rays/s", "value": ray_frames * K * world / total, "unit": "rays/s",
+        "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * total / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded dynamic phantom, gamma-variate time-activity curves)",
+        "config": {"workload": ("dynamic PET, 24 frames, 384 crystals x 32 rings, 256x192x63 sinograms, "
+                                "128x128x63 image, improved Siddon FP+BP") if not small else
+                   "dynamic PET small (8 rings) for profiling",
+                   "frames": frames, "rays_per_frame": m, "intersections_per_frame": sum_np,
+                   "subsets": int(o.subsets), "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (sinograms %.0f MB per step) plus a 256 MB L2 flush between steps"
+                         % (frames * m * 4 / 1e6)},
+        "fp_ms": 1e3 * mean_fp, "bp_ms": 1e3 * mean_bp,
+        "roofline": rl,
+        "e2e": {"value": ray_frames * K * world / e2e_total, "unit": "rays/s",
+                "h2d_bytes_per_step": frames * n * 4, "d2h_bytes_per_step": frames * n * 4},
+        "gpu_launches": 2 * K,
+        "clocks": clk,
+        "wall_s": wall,
+    }
+    if not args.no_baseline and world == 1:
+        try:
+            v, cores, kind, sample = dynpet_cpu_rate(o, imgs_host[0], 10.0)
+            line["cpu_baseline"] = {"value": v, "unit": "rays/s", "cores": cores, "kind": kind,
+                                    "sample": sample + f"; host CPU {cpu_model()}"}
+        except Exception as e:
+            line["cpu_baseline"] = {"error": str(e)}
+    return line
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU implementation of the same step on a bounded sample
 # ---------------------------------------------------------------------------
 
 def run_reference(args):
     from oracle import oracle as orc
-    small = args.workload == "dynpet_small"
-    o = dynamic_pet_options(small)
-    frames = args.frames or (4 if small else 24)
-    img = dynamic_images(o, 1)[0]
-    g = orc.Geometry(o)
-    use_ref = orc.ref_lib() is not None
     threads = os.cpu_count() or 1
-    subset = 0
-    rays = g.rays(subset)
     times = []
-    for it in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        if use_ref:
-            y = orc.ref_forward(g, img, subset, precision="float", threads=threads)
-            orc.ref_backward(g, y, subset, precision="float", threads=threads)
-        else:
-            y = orc.forward(g, img, subset)
-            orc.backward(g, y, subset)
-        if it >= args.warmup:
-            times.append(time.perf_counter() - t0)
+    if args.workload.startswith("cbct"):
+        o = cbct_options(args.workload == "cbct_small")
+        img = shepp_logan_3d(o)
+        g = cbct_sample_geometry(o, 4)
+        rays = g.rays(0)
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            y = orc.bdd_forward(g, img, 0)
+            orc.bdd_backward(g, y, 0)
+            if it >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        kind, cores = "port", threads
+        sample = (f"4 of {int(o.nProjections)} projections ({rays} rays) per step; FP64 OpenMP restatement of the "
+                  "type-5 pair (the reference has no CPU type-5 projector)")
+        workload = "cone-beam CT (same geometry as ours), FP+BP pair over a bounded sample of projections"
+    else:
+        o = dynamic_pet_options(args.workload == "dynpet_small")
+        img = dynamic_images(o, 1)[0]
+        g = orc.Geometry(o)
+        use_ref = orc.ref_lib() is not None
+        rays = g.rays(0)
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            if use_ref:
+                y = orc.ref_forward(g, img, 0, precision="float", threads=threads)
+                orc.ref_backward(g, y, 0, precision="float", threads=threads)
+            else:
+                y = orc.forward(g, img, 0)
+                orc.backward(g, y, 0)
+            if it >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        kind, cores = ("reference", threads) if use_ref else ("port", 1)
+        sample = f"frame 0, subset 0 ({rays} rays) per step"
+        workload = "dynamic PET (same geometry as ours), FP+BP pair over frame 0, subset 0"
     value = rays * args.steps / sum(times)
-    kind = "reference" if use_ref else "port"
     return {
         "impl": "reference", "metric": "proj+backproj rays/s", "value": value, "unit": "rays/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "dynamic PET (same geometry as ours); each step one FP+BP pair over frame 0, "
-                               "subset 0 (bounded sample)", "frames_full_workload": frames,
-                   "sample_rays_per_step": rays, "parallelism": "host OpenMP"},
-        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": threads if use_ref else 1, "kind": kind,
-                         "sample": f"frame 0, subset 0 ({rays} rays) per step"},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if kind == "reference"
+        else "f64", "data": "synthetic",
+        "config": {"workload": workload, "sample_rays_per_step": rays, "parallelism": "host OpenMP"},
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": cores, "kind": kind,
+                         "sample": sample + f"; host CPU {cpu_model()}"},
         "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -395,15 +664,16 @@ def main():
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
         return
+    import torch
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
     if world > 1:
         import datetime
 
-        import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
-    line = run_ours(args, rank, world, local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    run = run_cbct if args.workload.startswith("cbct") else run_dynpet
+    line = run(args, rank, world, dev)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

@@ -209,6 +209,21 @@ int omb_pdhg_iteration(omb_handle *h, float *x, float *x_next, float *u, float *
                        float *work_img, void *stream);
 
 /*
+ * The two non-projector steps of omb_pdhg_iteration, for callers that run
+ * the projections themselves (omb_forward / omb_backward):
+ *   omb_pdhg_dual:   p = (p + sigma * (fp - y)) / (1 + sigma) over n entries
+ *                    (computeForwardProject.h:227-316, one subset, no TOF);
+ *   omb_pdhg_primal: u_new = max(epps, u - tau * (rhs + beta * gradTV(x))),
+ *                    x_next = u_new + theta * (u_new - u), u = u_new, with
+ *                    rhs = A^T p (PDHGUpdate auxKernels.cl:2034-2062).
+ * omb_forward -> omb_pdhg_dual -> omb_backward -> omb_pdhg_primal is exactly
+ * omb_pdhg_iteration.
+ */
+int omb_pdhg_dual(float *p, const float *fp, const float *y, int64_t n, float sigma, void *stream);
+int omb_pdhg_primal(omb_handle *h, const float *x, const float *rhs, float *u, float *x_next, float tau, float theta,
+                    float beta, float tv_smooth, int32_t positivity, void *stream);
+
+/*
  * Largest eigenvalue L of A^T A by n_iter power iterations starting from x
  * (unit norm; overwritten with the last iterate).  The PDHG primal step is
  * tau = 1/L with sigma = 1 (functions.hpp:2417-2540, 2886-2905).  `work`

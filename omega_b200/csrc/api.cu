@@ -474,6 +474,21 @@ int omb_pdhg_iteration(omb_handle *h, float *x, float *x_next, float *u, float *
     return pdhg_primal_tv(h->grid, x, work_img, u, x_next, beta, tv_smooth, tau, theta, h->desc.epps, positivity, s);
 }
 
+int omb_pdhg_dual(float *p, const float *fp, const float *y, int64_t n, float sigma, void *stream) {
+    if (!p || !fp || !y) return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_pdhg_dual");
+    if (n < 0) return set_error(OMB_ERR_INVALID, "n must be >= 0");
+    return pdhg_dual(p, fp, y, n, sigma, (cudaStream_t)stream);
+}
+
+int omb_pdhg_primal(omb_handle *h, const float *x, const float *rhs, float *u, float *x_next, float tau, float theta,
+                    float beta, float tv_smooth, int32_t positivity, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!x || !rhs || !u || !x_next) return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_pdhg_primal");
+    if (x == x_next) return set_error(OMB_ERR_INVALID, "x and x_next must be different buffers");
+    return pdhg_primal_tv(h->grid, x, rhs, u, x_next, beta, tv_smooth, tau, theta, h->desc.epps, positivity,
+                          (cudaStream_t)stream);
+}
+
 size_t omb_power_workspace_bytes(void) { return 2 * dot_workspace_bytes(); }
 
 int omb_power_method(omb_handle *h, int32_t n_iter, float *x, float *work_meas, float *work_img, void *work,

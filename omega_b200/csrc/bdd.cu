@@ -136,27 +136,39 @@ __global__ void __launch_bounds__(256) k_bdd_fp(Grid g, const float *__restrict_
         if (!(cr > cl)) continue;
         const int i0 = (int)floorf(cl);
         const int i1 = min((int)ceilf(cr), nlat) - 1;
-        // axial range of all columns: [zu, zu + ncol*w]
-        const float zl_all = fmaxf(zu, 0.f), zr_all = fminf(fmaf((float)ncol, w, zu), fz);
-        if (!(zr_all > zl_all)) continue;
-        const int k0 = (int)floorf(zl_all);
-        const int k1 = min((int)ceilf(zr_all), g.nz) - 1;
         const float *slice = vol + (int64_t)j * sl_stride;
-        for (int k = k0; k <= k1; ++k) {
-            // lateral integral of row (slice j, z k) over the footprint
-            const float *row = slice + (int64_t)k * z_stride;
-            float rk = 0.f;
-            for (int i = i0; i <= i1; ++i) {
-                const float ox = fminf(cr, (float)(i + 1)) - fmaxf(cl, (float)i);
-                rk = fmaf(ox, __ldg(row + i * lat_stride), rk);
-            }
-            if (rk == 0.f) continue;
-            const float kl = (float)k, kr = (float)(k + 1);
+        // Walk the columns in order; each overlaps 1-2 z voxels and shares its
+        // first voxel with the previous column, so the lateral row integral of
+        // that voxel is reused instead of recomputed.
+        int ck = -1;
+        float cr_k = 0.f;
 #pragma unroll
-            for (int c = 0; c < kColsPerThread; ++c) {
+        for (int c = 0; c < kColsPerThread; ++c) {
+            if (c < ncol) {
                 const float lo = fmaf((float)c, w, zu), hi = fmaf((float)(c + 1), w, zu);
-                const float oz = fminf(hi, kr) - fmaxf(lo, kl);
-                if (c < ncol && oz > 0.f) temp[c] = fmaf(rk * oz, inv_area, temp[c]);
+                const float lc = fmaxf(lo, 0.f), hc = fminf(hi, fz);
+                if (hc > lc) {
+                    const int ka = (int)floorf(lc), kb = min((int)ceilf(hc), g.nz) - 1;
+                    float acc = 0.f;
+                    for (int k = ka; k <= kb; ++k) {
+                        float rk;
+                        if (k == ck) {
+                            rk = cr_k;
+                        } else {
+                            const float *row = slice + (int64_t)k * z_stride;
+                            rk = 0.f;
+                            for (int i = i0; i <= i1; ++i) {
+                                const float ox = fminf(cr, (float)(i + 1)) - fmaxf(cl, (float)i);
+                                rk = fmaf(ox, __ldg(row + i * lat_stride), rk);
+                            }
+                            ck = k;
+                            cr_k = rk;
+                        }
+                        const float oz = fminf(hc, (float)(k + 1)) - fmaxf(lc, (float)k);
+                        acc = fmaf(rk, oz, acc);
+                    }
+                    temp[c] = fmaf(acc, inv_area, temp[c]);
+                }
             }
         }
     }
@@ -193,65 +205,105 @@ __global__ void k_transpose_xy(const float *__restrict__ in, float *__restrict__
 // computeGeom5 uses (omegatomo/projector/init.py:6-37).
 // ---------------------------------------------------------------------------
 
+constexpr int kBpZ = 8;  // voxels along z per thread
+
+// Voxel-driven backprojection, kBpZ voxels along z per thread.  For the flat
+// panels of this path (rows in the xy-plane, columns along z) the detector
+// row coordinate u and the projective denominator do not depend on z, so the
+// row footprint and its weights are formed once per projection and shared by
+// the thread's voxels; neighbouring voxels also share a detector column, whose
+// row-weighted sum is reused.
 __global__ void __launch_bounds__(256) k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
                                                 int64_t nproj, const float *__restrict__ y,
                                                 float *__restrict__ img, float *__restrict__ sens) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
-    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    const int kz0 = blockIdx.z * kBpZ;
+    if (i >= g.nx || j >= g.ny || kz0 >= g.nz) return;
+    const int nzt = min(kBpZ, g.nz - kz0);
     const float qx = fmaf((float)i, g.dx, g.bx + 0.5f * g.dx);
     const float qy = fmaf((float)j, g.dy, g.by + 0.5f * g.dy);
-    const float qz = fmaf((float)k, g.dz, g.bz + 0.5f * g.dz);
+    const float qz0 = fmaf((float)kz0, g.dz, g.bz + 0.5f * g.dz);
     const float hx = 0.5f * g.dx, hy = 0.5f * g.dy, hz = 0.5f * g.dz;
     const float fnr = (float)nr, fnc = (float)nc;
-    float temp = 0.f, wsum = 0.f;
+    float temp[kBpZ], wsum[kBpZ];
+#pragma unroll
+    for (int t = 0; t < kBpZ; ++t) {
+        temp[t] = 0.f;
+        wsum[t] = 0.f;
+    }
     for (int64_t p = 0; p < nproj; ++p) {
         const BddProj P = pj[p];
-        // mid-plane corners LU and RD of the voxel (projectorType5.cl:508-527)
         float lx, ly, rx, ry;
+        const float sgn = P.spos ? 1.f : -1.f;
         if (P.ysl) {
-            const float sgn = P.spos ? 1.f : -1.f;
             lx = qx - sgn * hx; rx = qx + sgn * hx; ly = qy; ry = qy;
         } else {
-            const float sgn = P.spos ? 1.f : -1.f;
             lx = qx; rx = qx; ly = qy + sgn * hy; ry = qy - sgn * hy;
         }
-        const float lz = qz - hz, rz = qz + hz;
-        const float dl = 1.f / fmaf(P.c[0], lx, fmaf(P.c[1], ly, fmaf(P.c[2], lz, 1.f)));
-        const float dr = 1.f / fmaf(P.c[0], rx, fmaf(P.c[1], ry, fmaf(P.c[2], rz, 1.f)));
-        const float ul = fmaf(P.au[0], lx, fmaf(P.au[1], ly, fmaf(P.au[2], lz, P.au0))) * dl;
-        const float ur = fmaf(P.au[0], rx, fmaf(P.au[1], ry, fmaf(P.au[2], rz, P.au0))) * dr;
-        const float vl = fmaf(P.av[0], lx, fmaf(P.av[1], ly, fmaf(P.av[2], lz, P.av0))) * dl;
-        const float vr = fmaf(P.av[0], rx, fmaf(P.av[1], ry, fmaf(P.av[2], rz, P.av0))) * dr;
+        // z-independent parts (P.c[2] == 0 and P.au[2] == 0 for these panels)
+        const float dl = 1.f / fmaf(P.c[0], lx, fmaf(P.c[1], ly, fmaf(P.c[2], qz0, 1.f)));
+        const float dr = 1.f / fmaf(P.c[0], rx, fmaf(P.c[1], ry, fmaf(P.c[2], qz0, 1.f)));
+        const float ul = fmaf(P.au[0], lx, fmaf(P.au[1], ly, fmaf(P.au[2], qz0, P.au0))) * dl;
+        const float ur = fmaf(P.au[0], rx, fmaf(P.au[1], ry, fmaf(P.au[2], qz0, P.au0))) * dr;
         const float ua = fmaxf(fminf(ul, ur), 0.f), ub = fminf(fmaxf(ul, ur), fnr);
-        const float va = fmaxf(fminf(vl, vr), 0.f), vb = fminf(fmaxf(vl, vr), fnc);
-        if (!(ub > ua) || !(vb > va)) continue;
+        if (!(ub > ua)) continue;
         const int r0 = (int)floorf(ua), r1 = min((int)ceilf(ub), nr) - 1;
-        const int c0 = (int)floorf(va), c1 = min((int)ceilf(vb), nc) - 1;
+        // v of the two corners of voxel t: linear in t
+        const float vl0 = fmaf(P.av[0], lx, fmaf(P.av[1], ly, fmaf(P.av[2], qz0 - hz, P.av0))) * dl;
+        const float vr0 = fmaf(P.av[0], rx, fmaf(P.av[1], ry, fmaf(P.av[2], qz0 + hz, P.av0))) * dr;
+        const float svl = P.av[2] * g.dz * dl, svr = P.av[2] * g.dz * dr;
+        // kerroin = d * |v| / |v_axis|, v = voxel centre - source
+        const float vx = qx - P.s[0], vy = qy - P.s[1];
+        const float axy = vx * vx + vy * vy;
+        const float kscale = P.ysl ? g.dy / fabsf(vy) : g.dx / fabsf(vx);
         const float *yp = y + p * (int64_t)nr * nc;
-        float apu = 0.f;
-        for (int c = c0; c <= c1; ++c) {
-            const float ov = fminf(vb, (float)(c + 1)) - fmaxf(va, (float)c);
-            float row = 0.f;
-            for (int rr = r0; rr <= r1; ++rr) {
-                const float ou = fminf(ub, (float)(rr + 1)) - fmaxf(ua, (float)rr);
-                row = fmaf(ou, __ldg(yp + rr + (int64_t)c * nr), row);
+        int cc = -1;
+        float crow = 0.f;
+#pragma unroll
+        for (int t = 0; t < kBpZ; ++t) {
+            if (t < nzt) {
+                const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
+                const float va = fmaxf(fminf(vlt, vrt), 0.f), vb = fminf(fmaxf(vlt, vrt), fnc);
+                if (vb > va) {
+                    const int c0 = (int)floorf(va), c1 = min((int)ceilf(vb), nc) - 1;
+                    float apu = 0.f;
+                    for (int c = c0; c <= c1; ++c) {
+                        float rowsum;
+                        if (c == cc) {
+                            rowsum = crow;
+                        } else {
+                            rowsum = 0.f;
+                            const float *col = yp + (int64_t)c * nr;
+                            for (int rr = r0; rr <= r1; ++rr) {
+                                const float ou = fminf(ub, (float)(rr + 1)) - fmaxf(ua, (float)rr);
+                                rowsum = fmaf(ou, __ldg(col + rr), rowsum);
+                            }
+                            cc = c;
+                            crow = rowsum;
+                        }
+                        const float ov = fminf(vb, (float)(c + 1)) - fmaxf(va, (float)c);
+                        apu = fmaf(ov, rowsum, apu);
+                    }
+                    if (apu != 0.f) {
+                        const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
+                        const float ker = kscale * sqrtf(fmaf(vz, vz, axy));
+                        temp[t] = fmaf(apu, ker, temp[t]);
+                        wsum[t] += ker;
+                    }
+                }
             }
-            apu = fmaf(ov, row, apu);
-        }
-        if (apu != 0.f) {
-            // d * |v| / |v_axis| with v = voxel centre - source
-            const float vx = qx - P.s[0], vy = qy - P.s[1], vz = qz - P.s[2];
-            const float len = sqrtf(vx * vx + vy * vy + vz * vz);
-            const float ker = P.ysl ? g.dy * len / fabsf(vy) : g.dx * len / fabsf(vx);
-            temp = fmaf(apu, ker, temp);
-            wsum += ker;
         }
     }
-    const int64_t n = i + (int64_t)j * g.nx + (int64_t)k * g.nx * g.ny;
-    img[n] = temp;
-    if (sens) sens[n] = wsum;
+    int64_t n = i + (int64_t)j * g.nx + (int64_t)kz0 * g.nx * g.ny;
+#pragma unroll
+    for (int t = 0; t < kBpZ; ++t) {
+        if (t < nzt) {
+            img[n] = temp[t];
+            if (sens) sens[n] = wsum[t];
+        }
+        n += (int64_t)g.nx * g.ny;
+    }
 }
 
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
@@ -273,7 +325,7 @@ int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj
                  float *sens, cudaStream_t st) {
     if (g.nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
     dim3 block(32, 8);
-    dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+    dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kBpZ - 1) / kBpZ);
     k_bdd_bp<<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
     OMB_LAUNCH_CHECK("bdd backward launch");
     return OMB_OK;

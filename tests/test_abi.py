@@ -98,3 +98,7 @@ def test_null_handle_calls_fail_cleanly():
     assert L.omb_backward(None, 0, None, None, None, 0, None) == -1
     assert L.omb_measurement_count(None, 0) == -1
     assert L.omb_destroy(None) == 0
+    assert L.omb_pdhg_dual(None, None, None, 0, 1.0, None) == -1
+    assert L.omb_pdhg_primal(None, None, None, None, None, 1.0, 1.0, 0.0, 1e-4, 1, None) == -1
+    assert L.omb_pdhg_iteration(None, None, None, None, None, None, 1.0, 1.0, 1.0, 0.0, 1e-4, 1, None, None,
+                                None) == -1

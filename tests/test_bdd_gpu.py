@@ -107,6 +107,38 @@ def test_pdhg_graph_replay_equals_eager(cuda):
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+def test_pdhg_split_calls_equal_fused_iteration(cuda):
+    """omb_forward -> omb_pdhg_dual -> omb_backward -> omb_pdhg_primal is the
+    same computation as omb_pdhg_iteration, bit for bit."""
+    import ctypes
+
+    import torch
+    from omega_b200 import _native
+    o = _init("ct_mini5")
+    g = orc.Geometry(o)
+    y = _t(orc.bdd_forward(g, _phantom(g, 3), -1), cuda)
+    n, m = g.n_img, g.rays(-1)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    st = ctypes.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
+    runs = []
+    for split in (False, True):
+        x = torch.full((n,), 1e-3, device=cuda)
+        xn, u, p = torch.empty_like(x), x.clone(), torch.zeros(m, device=cuda)
+        wm, wi = torch.empty(m, device=cuda), torch.empty(n, device=cuda)
+        for _ in range(3):
+            if split:
+                _native.call("omb_forward", o._handle, -1, P(x), P(wm), st)
+                _native.call("omb_pdhg_dual", P(p), P(wm), P(y), m, 1.0, st)
+                _native.call("omb_backward", o._handle, -1, P(p), P(wi), None, 0, st)
+                _native.call("omb_pdhg_primal", o._handle, P(x), P(wi), P(u), P(xn), 1e-3, 1.0, 0.03, 1e-4, 1, st)
+            else:
+                _native.call("omb_pdhg_iteration", o._handle, P(x), P(xn), P(u), P(p), P(y), 1e-3, 1.0, 1.0, 0.03,
+                             1e-4, 1, P(wm), P(wi), st)
+            x, xn = xn, x
+        runs.append(x.cpu().numpy())
+    assert np.array_equal(runs[0].view(np.uint32), runs[1].view(np.uint32))
+
+
 def test_osem_graph_replay_matches_eager(cuda):
     from omega_b200 import reconstruction as rec
     o = _init("pet_mini")
