@@ -61,7 +61,11 @@ def parse_args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="cbct", choices=["cbct", "cbct_small", "dynpet", "dynpet_small"])
     p.add_argument("--frames", type=int, default=None)
+    p.add_argument("--views", type=int, default=None,
+                   help="cbct: number of projections (fewer than 360 only for short profiling captures)")
     p.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--tuning", default=None,
+                   help="fixed launch shapes instead of the autotuner, e.g. bdd_fp_columns=16,bdd_bp_zrun=8")
     return p.parse_args()
 
 
@@ -176,10 +180,11 @@ class ClockSampler:
 # cone-beam CT workload
 # ---------------------------------------------------------------------------
 
-def cbct_options(small=False):
+def cbct_options(small=False, views=None):
     from omega_b200.projector import proj
     o = proj.projectorClass()
     panel, nproj, n = (128, 90, 64) if small else (512, 360, 256)
+    nproj = views or nproj
     o.CT = True
     o.nRowsD = o.nColsD = panel
     o.nProjections = nproj
@@ -225,6 +230,14 @@ def shepp_logan_3d(o, seed=7):
 # ---------------------------------------------------------------------------
 # helpers
 # ---------------------------------------------------------------------------
+
+def choose_tuning(o, args, n_frames):
+    """The autotuner's launch shapes, or the ones given with --tuning."""
+    if args.tuning:
+        o.tuning = {k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))}
+        return o.tuning
+    return o.autotune(n_frames=n_frames, repeats=2)
+
 
 def measured_peak():
     try:
@@ -372,7 +385,7 @@ def run_cbct(args, rank, world, dev):
     from omega_b200 import _native
     from omega_b200 import reconstruction as rec
     small = args.workload == "cbct_small"
-    o = cbct_options(small)
+    o = cbct_options(small, args.views)
     o.initProj()
     h = o._handle
     n = int(o.N[0])
@@ -393,6 +406,7 @@ def run_cbct(args, rank, world, dev):
     counts = torch.poisson(I0 * torch.exp(-yc), generator=gen).clamp_(min=1.0)
     y = torch.log(I0 / counts)
     del counts, yc
+    tuning = choose_tuning(o, args, 1)
     tau = 1.0 / rec.power_method(o, 20, seed=0)
     sigma, theta = 1.0, 1.0
     beta, smooth = float(o.beta), float(o.TVsmoothing)
@@ -461,7 +475,7 @@ def run_cbct(args, rank, world, dev):
                                 "SOD 500 / SDD 1000 mm, 256^3 volume 0.25 mm, branchless distance-driven (type 5), "
                                 "one PDHG+TV iteration per step") if not small else
                    "cone-beam CT small (128^2 panel, 90 views, 64^3) for profiling",
-                   "rays_per_step": m, "voxels": n, "views": nproj, "subsets": 1,
+                   "rays_per_step": m, "voxels": n, "views": nproj, "subsets": 1, "tuning": tuning,
                    "parallelism": f"replicas x{world}",
                    "l2": "256 MB L2 flush between steps; the measurement vectors (%.0f MB each) exceed L2"
                          % (m * 4 / 1e6)},
@@ -539,6 +553,7 @@ def run_dynpet(args, rank, world, dev):
         _native.call("omb_backward_frames", h, -1, frames, P(ys), m, P(back), n, sp)
         tm.mark()
 
+    tuning = choose_tuning(o, args, frames)
     npx = ctypes.c_int64()
     _native.call("omb_intersection_count", h, -1, ctypes.byref(npx), sp)
     sum_np = npx.value
@@ -579,7 +594,7 @@ def run_dynpet(args, rank, world, dev):
                                 "128x128x63 image, improved Siddon FP+BP") if not small else
                    "dynamic PET small (8 rings) for profiling",
                    "frames": frames, "rays_per_frame": m, "intersections_per_frame": sum_np,
-                   "subsets": int(o.subsets), "parallelism": f"replicas x{world}",
+                   "subsets": int(o.subsets), "tuning": tuning, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (sinograms %.0f MB per step) plus a 256 MB L2 flush between steps"
                          % (frames * m * 4 / 1e6)},
         "fp_ms": 1e3 * mean_fp, "bp_ms": 1e3 * mean_bp,
@@ -609,7 +624,7 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     times = []
     if args.workload.startswith("cbct"):
-        o = cbct_options(args.workload == "cbct_small")
+        o = cbct_options(args.workload == "cbct_small", args.views)
         img = shepp_logan_3d(o)
         g = cbct_sample_geometry(o, 4)
         rays = g.rays(0)

@@ -192,6 +192,36 @@ int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream);
 int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, void *stream);
 
 /*
+ * Launch shapes of a handle's projector kernels.  omb_create sets the
+ * defaults below; omb_autotune times the candidates on the handle's own
+ * geometry and keeps the fastest; omb_set_tuning sets them directly.  The
+ * shapes change only how the work is split, not what is computed: results
+ * agree to FP32 rounding (the order of additions differs).  No counterpart in
+ * the reference, whose kernels have fixed launch shapes.
+ */
+typedef struct omb_tuning {
+    uint32_t struct_size;            /* sizeof(omb_tuning) */
+    int32_t siddon_blocks_per_sm;    /* 1..32 (default 8): grid of the grid-stride Siddon kernels */
+    int32_t siddon_frames_per_walk;  /* 1, 2, 4, 8 (default 8): most frames sharing one ray walk */
+    int32_t bdd_fp_columns;          /* 8, 16 (default 8): type-5 forward, detector columns per thread */
+    int32_t bdd_bp_zrun;             /* 4, 8, 16 (default 8): type-5 backward, voxels along z per thread */
+} omb_tuning;
+
+int omb_get_tuning(const omb_handle *h, omb_tuning *out);
+int omb_set_tuning(omb_handle *h, const omb_tuning *in);
+
+/*
+ * Times each candidate launch shape of the handle's forward and backward
+ * projectors over all subsets -- n_frames images at once (type 1 without
+ * TOF; otherwise one) with `repeats` timed calls after one warm-up call --
+ * and keeps the fastest in the handle (also written to *out unless NULL).
+ * Allocates and frees its own scratch buffers on `stream` (about
+ * n_frames * (2 images + 1 measurement vector)) and synchronises it; do not
+ * call it while `stream` is being captured into a CUDA graph.
+ */
+int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *out, void *stream);
+
+/*
  * One PDHG iteration with a TV-gradient term over all projections (one
  * subset), on the device, no host synchronisation:
  *   p      = (p + sigma * (A x - y)) / (1 + sigma)

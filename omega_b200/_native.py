@@ -67,6 +67,20 @@ class GeometryDesc(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    """Mirror of ``omb_tuning``."""
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("siddon_blocks_per_sm", ctypes.c_int32),
+        ("siddon_frames_per_walk", ctypes.c_int32),
+        ("bdd_fp_columns", ctypes.c_int32),
+        ("bdd_bp_zrun", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_[1:]}
+
+
 # (name, restype, argtypes) of every exported entry point of include/omega_b200.h
 EXPORTS = [
     ("omb_abi_version", ctypes.c_int, []),
@@ -103,6 +117,10 @@ EXPORTS = [
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                         ctypes.c_void_p]),
     ("omb_power_workspace_bytes", ctypes.c_size_t, []),
+    ("omb_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
+    ("omb_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
+    ("omb_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Tuning),
+                                    ctypes.c_void_p]),
     ("omb_intersection_count", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
                                               ctypes.c_void_p]),
 ]

@@ -39,6 +39,7 @@ struct omb_handle {
     float *d_imgT = nullptr;              // y-fastest image copy (type-5 forward projection)
     BddProj *d_bddp = nullptr;            // per-projection maps (type-5 backprojection)
     int64_t n_img = 0;
+    Tuning tune{};
 };
 
 // Type-5 backprojection maps of every projection, FP64 on the host from the
@@ -297,8 +298,8 @@ int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, voi
     if (st != OMB_OK) return st;
     if (h->desc.fp_type == 5)
         return bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj, image,
-                           h->d_imgT, y, (cudaStream_t)stream);
-    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, y, rs.m_size),
+                           h->d_imgT, y, h->tune.bdd_fp_cols, (cudaStream_t)stream);
+    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, y, rs.m_size), h->tune,
                           (cudaStream_t)stream);
 }
 
@@ -315,7 +316,8 @@ int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const fl
     if (h->desc.fp_type == 5) {
         for (int fr = 0; fr < n_frames; ++fr) {
             st = bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj,
-                             images + fr * image_stride, h->d_imgT, y + fr * y_stride, (cudaStream_t)stream);
+                             images + fr * image_stride, h->d_imgT, y + fr * y_stride, h->tune.bdd_fp_cols,
+                             (cudaStream_t)stream);
             if (st != OMB_OK) return st;
         }
         return OMB_OK;
@@ -326,7 +328,7 @@ int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const fl
     f.img_stride = image_stride;
     f.meas_out = y;
     f.meas_stride = y_stride;
-    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, f, (cudaStream_t)stream);
+    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, f, h->tune, (cudaStream_t)stream);
 }
 
 int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, float *sens, int32_t mode,
@@ -344,7 +346,8 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
     if (h->desc.bp_type == 5) {
         if (mode != OMB_BP_FLOAT_ATOMIC)
             return set_error(OMB_ERR_UNSUPPORTED, "the type-5 backprojection is a gather; it has no fixed-point mode");
-        return bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y, image, sens, s);
+        return bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y, image, sens,
+                            h->tune.bdd_bp_z, s);
     }
     if (mode == OMB_BP_FIXED64) {
         unsigned long long *acc = h->d_acc, *acc_s = sens ? h->d_acc + h->n_img : nullptr;
@@ -357,7 +360,8 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
     }
     OMB_CUDA_TRY(cudaMemsetAsync(image, 0, nb, s));
     if (sens) OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, nb, s));
-    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, y, image, rs.m_size), sens, s);
+    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, y, image, rs.m_size), sens,
+                           h->tune, s);
 }
 
 int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const float *y, int64_t y_stride,
@@ -374,7 +378,7 @@ int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const f
     if (h->desc.bp_type == 5) {
         for (int fr = 0; fr < n_frames; ++fr) {
             st = bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y + fr * y_stride,
-                              images + fr * image_stride, nullptr, s);
+                              images + fr * image_stride, nullptr, h->tune.bdd_bp_z, s);
             if (st != OMB_OK) return st;
         }
         return OMB_OK;
@@ -390,7 +394,7 @@ int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const f
     f.meas_stride = y_stride;
     f.img = images;
     f.img_stride = image_stride;
-    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, nullptr, s);
+    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, nullptr, h->tune, s);
 }
 
 int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
@@ -404,7 +408,7 @@ int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
     // A^T 1 through the BP kernel's fused sensitivity accumulator, y = NULL.
     OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, h->n_img * sizeof(float), s));
     st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, nullptr, nullptr, rs.m_size),
-                         sens, s);
+                         sens, h->tune, s);
     if (st != OMB_OK) return st;
     return clamp_min(sens, h->n_img, h->desc.epps, s);
 }
@@ -423,13 +427,14 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     cudaStream_t s = (cudaStream_t)stream;
     const float eps = h->desc.epps;
     const int64_t m = rs.m_size * h->desc.tof_bins;
-    st = siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, work_meas, rs.m_size), s);
+    st = siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, work_meas, rs.m_size),
+                        h->tune, s);
     if (st != OMB_OK) return st;
     st = osem_ratio(y_subset, work_meas, m, eps, s);
     if (st != OMB_OK) return st;
     OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
     st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, work_meas, work_img, rs.m_size),
-                         nullptr, s);
+                         nullptr, h->tune, s);
     if (st != OMB_OK) return st;
     return em_update(image, sens, work_img, h->n_img, eps, s);
 }
@@ -453,6 +458,167 @@ int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, voi
     if (e != cudaSuccess) return cuda_fail(e, "intersection count");
     if (st != OMB_OK) return st;
     *out_host = (int64_t)v;
+    return OMB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Launch-shape tuning
+// ---------------------------------------------------------------------------
+
+static bool one_of(int v, std::initializer_list<int> ok) {
+    for (int o : ok)
+        if (v == o) return true;
+    return false;
+}
+
+static int tuning_from(const omb_tuning *in, Tuning &t) {
+    if (!in) return set_error(OMB_ERR_INVALID, "tuning pointer is NULL");
+    if (in->struct_size != sizeof(omb_tuning))
+        return set_error(OMB_ERR_INVALID, "omb_tuning.struct_size does not match this library (" +
+                                              std::to_string(sizeof(omb_tuning)) + " bytes)");
+    if (in->siddon_blocks_per_sm < 1 || in->siddon_blocks_per_sm > 32)
+        return set_error(OMB_ERR_INVALID, "siddon_blocks_per_sm must be in 1..32");
+    if (!one_of(in->siddon_frames_per_walk, {1, 2, 4, 8}))
+        return set_error(OMB_ERR_INVALID, "siddon_frames_per_walk must be 1, 2, 4 or 8");
+    if (!one_of(in->bdd_fp_columns, {8, 16})) return set_error(OMB_ERR_INVALID, "bdd_fp_columns must be 8 or 16");
+    if (!one_of(in->bdd_bp_zrun, {4, 8, 16})) return set_error(OMB_ERR_INVALID, "bdd_bp_zrun must be 4, 8 or 16");
+    t.siddon_blocks_per_sm = in->siddon_blocks_per_sm;
+    t.siddon_frames = in->siddon_frames_per_walk;
+    t.bdd_fp_cols = in->bdd_fp_columns;
+    t.bdd_bp_z = in->bdd_bp_zrun;
+    return OMB_OK;
+}
+
+static void tuning_to(const Tuning &t, omb_tuning *out) {
+    out->struct_size = sizeof(omb_tuning);
+    out->siddon_blocks_per_sm = t.siddon_blocks_per_sm;
+    out->siddon_frames_per_walk = t.siddon_frames;
+    out->bdd_fp_columns = t.bdd_fp_cols;
+    out->bdd_bp_zrun = t.bdd_bp_z;
+}
+
+int omb_get_tuning(const omb_handle *h, omb_tuning *out) {
+    if (!h || !out) return set_error(OMB_ERR_INVALID, "handle/output pointer is NULL");
+    if (out->struct_size != sizeof(omb_tuning))
+        return set_error(OMB_ERR_INVALID, "omb_tuning.struct_size does not match this library");
+    tuning_to(h->tune, out);
+    return OMB_OK;
+}
+
+int omb_set_tuning(omb_handle *h, const omb_tuning *in) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    Tuning t{};
+    int st = tuning_from(in, t);
+    if (st == OMB_OK) h->tune = t;
+    return st;
+}
+
+int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *out, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (n_frames < 1 || repeats < 1) return set_error(OMB_ERR_INVALID, "n_frames and repeats must be >= 1");
+    if (out && out->struct_size != sizeof(omb_tuning))
+        return set_error(OMB_ERR_INVALID, "omb_tuning.struct_size does not match this library");
+    const bool siddon = h->desc.fp_type == 1 && h->desc.bp_type == 1;
+    if (!siddon || h->desc.tof_bins > 1) n_frames = 1;
+    const int64_t m = omb_measurement_count(h, -1);
+    if (m < 0) return -1;
+    const int64_t n = h->n_img;
+    cudaStream_t s = (cudaStream_t)stream;
+    float *img = nullptr, *y = nullptr, *back = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int st = OMB_OK;
+    cudaError_t e = cudaMallocAsync(&img, (size_t)n_frames * n * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&back, (size_t)n_frames * n * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&y, (size_t)n_frames * m * sizeof(float), s);
+    // positive filler (byte 0x3C -> 0.0115f): timing does not depend on values
+    if (e == cudaSuccess) e = cudaMemsetAsync(img, 0x3C, (size_t)n_frames * n * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(y, 0x3C, (size_t)n_frames * m * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    const Tuning saved = h->tune;
+    auto fwd = [&]() { return omb_forward_frames(h, -1, n_frames, img, n, y, m, stream); };
+    auto bwd = [&]() { return omb_backward_frames(h, -1, n_frames, y, m, back, n, stream); };
+    // mean milliseconds of `repeats` calls of f after one warm-up call; < 0 on failure
+    auto timed = [&](auto &&f) -> float {
+        if (f() != OMB_OK) return -1.f;
+        if (cudaEventRecord(e0, s) != cudaSuccess) return -1.f;
+        for (int r = 0; r < repeats; ++r)
+            if (f() != OMB_OK) return -1.f;
+        float ms = -1.f;
+        if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+            return -1.f;
+        return ms / repeats;
+    };
+    Tuning best = saved;
+    if (e == cudaSuccess && siddon) {
+        float best_ms = 3.4e38f;
+        const int frames_max = h->desc.tof_bins > 1 ? 1 : 8;
+        for (int ps : {2, 4, 8, 16}) {
+            for (int fr = 1; fr <= frames_max && fr <= n_frames && st == OMB_OK; fr *= 2) {
+                h->tune = saved;
+                h->tune.siddon_blocks_per_sm = ps;
+                h->tune.siddon_frames = fr;
+                const float a = timed(fwd), b = a < 0.f ? -1.f : timed(bwd);
+                if (a < 0.f || b < 0.f) {
+                    st = -1;
+                    break;
+                }
+                if (a + b < best_ms) {
+                    best_ms = a + b;
+                    best.siddon_blocks_per_sm = ps;
+                    best.siddon_frames = fr;
+                }
+            }
+        }
+    }
+    if (e == cudaSuccess && st == OMB_OK && h->desc.fp_type == 5) {
+        float best_ms = 3.4e38f;
+        for (int c : {8, 16}) {
+            h->tune = best;
+            h->tune.bdd_fp_cols = c;
+            const float a = timed(fwd);
+            if (a < 0.f) {
+                st = -1;
+                break;
+            }
+            if (a < best_ms) {
+                best_ms = a;
+                best.bdd_fp_cols = c;
+            }
+        }
+    }
+    if (e == cudaSuccess && st == OMB_OK && h->desc.bp_type == 5) {
+        float best_ms = 3.4e38f;
+        for (int z : {4, 8, 16}) {
+            h->tune = best;
+            h->tune.bdd_bp_z = z;
+            const float b = timed(bwd);
+            if (b < 0.f) {
+                st = -1;
+                break;
+            }
+            if (b < best_ms) {
+                best_ms = b;
+                best.bdd_bp_z = z;
+            }
+        }
+    }
+    h->tune = (e == cudaSuccess && st == OMB_OK) ? best : saved;
+    const std::string keep = g_last_error;
+    if (img) cudaFreeAsync(img, s);
+    if (back) cudaFreeAsync(back, s);
+    if (y) cudaFreeAsync(y, s);
+    const cudaError_t es = cudaStreamSynchronize(s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(e, "autotune set-up");
+    if (st != OMB_OK) {
+        g_last_error = keep.empty() ? "autotune: a timed call failed" : keep;
+        return st;
+    }
+    if (es != cudaSuccess) return cuda_fail(es, "autotune");
+    if (out) tuning_to(h->tune, out);
     return OMB_OK;
 }
 

@@ -23,7 +23,6 @@
 
 namespace omb {
 
-constexpr int kColsPerThread = 8;
 
 // Per-ray constants of the forward projection: footprint edge lines in voxel
 // units, e(j) = e0 + j * e1 for slice j, and the pixel's weight.
@@ -95,11 +94,56 @@ __device__ __forceinline__ BddRay bdd_ray_setup(const Grid &g, const float *__re
     return b;
 }
 
+// The forward weight dx*dy*dz / |u_axis| of the ray through pixel (r, c).
+__device__ __forceinline__ float bdd_kerroin(const Grid &g, const float *__restrict__ xy,
+                                             const float *__restrict__ uv, int64_t gp, int r, int c, int nr, int nc,
+                                             float pitch_y, bool ysl) {
+    const float *q = xy + gp * 6;
+    const double sx = __ldg(q), sy = __ldg(q + 1), sz = __ldg(q + 2);
+    const double ux = __ldg(uv + gp * 2), uy = __ldg(uv + gp * 2 + 1);
+    const double ia = (double)r - (double)nr / 2.0 + 0.5;
+    const double ib = (double)c - (double)nc / 2.0 + 0.5;
+    const double vx = __ldg(q + 3) + ia * ux - sx, vy = __ldg(q + 4) + ia * uy - sy;
+    const double vz = __ldg(q + 5) + ib * (double)pitch_y - sz;
+    const double L = sqrt(vx * vx + vy * vy + vz * vz);
+    return (float)((double)g.dx * g.dy * g.dz / fabs((ysl ? vy : vx) / L));
+}
+
+// Weighted sum along one contiguous run of voxels / detector pixels that
+// overlap [lo, hi]: element 0 (at `base`, lo >= base) partial, then full
+// elements, the last one partial again.  Up to three elements take a fixed
+// three-load path with zero weights for the missing ones (index clamped).
+struct Seg {
+    float w0, w1, w2, hi;
+    int o1, o2, n, base;
+};
+
+__device__ __forceinline__ Seg make_seg(float lo, float hi, int base, int n) {
+    Seg s;
+    s.hi = hi;
+    s.base = base;
+    s.n = n;
+    s.w0 = fminf(hi, (float)(base + 1)) - lo;
+    s.w1 = n == 0 ? 0.f : (n == 1 ? hi - (float)(base + 1) : 1.f);
+    s.w2 = n < 2 ? 0.f : (n == 2 ? hi - (float)(base + 2) : 1.f);
+    s.o1 = min(n, 1);
+    s.o2 = min(n, 2);
+    return s;
+}
+
+__device__ __forceinline__ float seg_sum(const Seg &s, const float *__restrict__ p) {
+    float acc = fmaf(s.w2, __ldg(p + s.o2), fmaf(s.w1, __ldg(p + s.o1), s.w0 * __ldg(p)));
+    for (int i = 3; i <= s.n; ++i)
+        acc = fmaf(fminf(s.hi, (float)(s.base + i + 1)) - (float)(s.base + i), __ldg(p + i), acc);
+    return acc;
+}
+
 // Forward projection.  Thread = (detector row, group of 8 columns, projection).
 // `img` is x-fastest, `imgT` the same image y-fastest; slices along y read
 // `img`, slices along x read `imgT`, so a warp's 32 rows read consecutive
 // addresses in both cases.
-__global__ void __launch_bounds__(256) k_bdd_fp(Grid g, const float *__restrict__ xy, const float *__restrict__ uv,
+template <int kColsPerThread>
+__global__ void k_bdd_fp(Grid g, const float *__restrict__ xy, const float *__restrict__ uv,
                                                 int nr, int nc, float pitch_y, int64_t proj0, int64_t nproj,
                                                 const float *__restrict__ img, const float *__restrict__ imgT,
                                                 float *__restrict__ y) {
@@ -110,9 +154,12 @@ __global__ void __launch_bounds__(256) k_bdd_fp(Grid g, const float *__restrict_
     if (r >= nr || c0 >= nc || p >= nproj) return;
     const int ncol = min(kColsPerThread, nc - c0);
     const BddRay b = bdd_ray_setup(g, xy, uv, proj0 + p, r, c0, nr, nc, pitch_y);
+    // The weight belongs to groups of 8 columns, taken at each group's first
+    // column (projectorType5.cl:166-174, 327-331): a 16-column thread holds two.
+    const float kerroin8 =
+        kColsPerThread > 8 && c0 + 8 < nc ? bdd_kerroin(g, xy, uv, proj0 + p, r, c0 + 8, nr, nc, pitch_y, b.ysl) : 0.f;
     const int nsl = b.ysl ? g.ny : g.nx;       // slices
     const int nlat = b.ysl ? g.nx : g.ny;      // voxels across a slice
-    const int64_t lat_stride = 1;              // both layouts: lateral axis fastest
     const int64_t sl_stride = nlat;
     const int64_t z_stride = (int64_t)g.nx * g.ny;
     const float *__restrict__ vol = b.ysl ? img : imgT;
@@ -122,60 +169,49 @@ __global__ void __launch_bounds__(256) k_bdd_fp(Grid g, const float *__restrict_
 #pragma unroll
     for (int c = 0; c < kColsPerThread; ++c) temp[c] = 0.f;
 
+    const int zmax = g.nz - 1;
     for (int j = 0; j < nsl; ++j) {
         const float fj = (float)j;
-        float xa = fmaf(fj, b.xa1, b.xa0), xb = fmaf(fj, b.xb1, b.xb0);
-        float za = fmaf(fj, b.za1, b.za0), zb = fmaf(fj, b.zb1, b.zb0);
+        const float xa = fmaf(fj, b.xa1, b.xa0), xb = fmaf(fj, b.xb1, b.xb0);
+        const float za = fmaf(fj, b.za1, b.za0), zb = fmaf(fj, b.zb1, b.zb0);
         const float el = fminf(xa, xb), er = fmaxf(xa, xb);
         const float zu = fminf(za, zb);
         const float w = fabsf(fmaf(fj, b.dz1, b.dz0));
-        const float area = fabsf(fmaf(fj, b.dw1, b.dw0)) * dlat * w * g.dz;
-        const float inv_area = 1.f / area;
+        const float inv_area = 1.f / (fabsf(fmaf(fj, b.dw1, b.dw0)) * dlat * w * g.dz);
         // lateral overlap range (clamped to the slice)
         const float cl = fmaxf(el, 0.f), cr = fminf(er, flat);
         if (!(cr > cl)) continue;
-        const int i0 = (int)floorf(cl);
-        const int i1 = min((int)ceilf(cr), nlat) - 1;
-        const float *slice = vol + (int64_t)j * sl_stride;
-        // Walk the columns in order; each overlaps 1-2 z voxels and shares its
-        // first voxel with the previous column, so the lateral row integral of
-        // that voxel is reused instead of recomputed.
-        int ck = -1;
-        float cr_k = 0.f;
+        const int i0 = (int)cl;  // cl >= 0: truncation is floor
+        const Seg seg = make_seg(cl, cr, i0, min((int)ceilf(cr), nlat) - 1 - i0);
+        const float *slice = vol + (int64_t)j * sl_stride + i0;
+#define row_integral(k) seg_sum(seg, slice + (int64_t)(k) * z_stride)
+        // The 8 columns partition [zu, zu + 8w] along z.  With C(b) the
+        // integral of the lateral row integrals from zu up to b, column c is
+        // C(b_{c+1}) - C(b_c): walk b_0 < ... < b_8 and the voxel rows
+        // together, one row integral per row crossed.
+        float bz = fminf(fmaxf(zu, 0.f), fz);
+        int kc = min((int)bz, zmax);
+        float R = row_integral(kc);
+        float S = 0.f;
+        float Cprev = (bz - (float)kc) * R;
 #pragma unroll
         for (int c = 0; c < kColsPerThread; ++c) {
-            if (c < ncol) {
-                const float lo = fmaf((float)c, w, zu), hi = fmaf((float)(c + 1), w, zu);
-                const float lc = fmaxf(lo, 0.f), hc = fminf(hi, fz);
-                if (hc > lc) {
-                    const int ka = (int)floorf(lc), kb = min((int)ceilf(hc), g.nz) - 1;
-                    float acc = 0.f;
-                    for (int k = ka; k <= kb; ++k) {
-                        float rk;
-                        if (k == ck) {
-                            rk = cr_k;
-                        } else {
-                            const float *row = slice + (int64_t)k * z_stride;
-                            rk = 0.f;
-                            for (int i = i0; i <= i1; ++i) {
-                                const float ox = fminf(cr, (float)(i + 1)) - fmaxf(cl, (float)i);
-                                rk = fmaf(ox, __ldg(row + i * lat_stride), rk);
-                            }
-                            ck = k;
-                            cr_k = rk;
-                        }
-                        const float oz = fminf(hc, (float)(k + 1)) - fmaxf(lc, (float)k);
-                        acc = fmaf(rk, oz, acc);
-                    }
-                    temp[c] = fmaf(acc, inv_area, temp[c]);
-                }
+            bz = fminf(fmaxf(fmaf((float)(c + 1), w, zu), 0.f), fz);
+            const int kn = min((int)bz, zmax);
+            while (kc < kn) {
+                S += R;
+                R = row_integral(++kc);
             }
+            const float C = fmaf(bz - (float)kc, R, S);
+            temp[c] = fmaf(C - Cprev, inv_area, temp[c]);
+            Cprev = C;
         }
     }
+#undef row_integral
     int64_t idx = r + (int64_t)c0 * nr + p * (int64_t)nr * nc;
 #pragma unroll
     for (int c = 0; c < kColsPerThread; ++c)
-        if (c < ncol) y[idx + (int64_t)c * nr] = temp[c] * b.kerroin;
+        if (c < ncol) y[idx + (int64_t)c * nr] = temp[c] * (c < 8 ? b.kerroin : kerroin8);
 }
 
 // y-fastest copy of an x-fastest volume (per z slice, a 2-D transpose).
@@ -205,22 +241,33 @@ __global__ void k_transpose_xy(const float *__restrict__ in, float *__restrict__
 // computeGeom5 uses (omegatomo/projector/init.py:6-37).
 // ---------------------------------------------------------------------------
 
-constexpr int kBpZ = 8;  // voxels along z per thread
+constexpr int kBpThreads = 256;
+// detector columns one thread's run of kBpZ voxels may cover before it takes
+// the per-voxel path (about 1.25 columns per voxel at magnification 2)
+__host__ __device__ constexpr int bp_slots(int kBpZ) { return kBpZ + kBpZ / 2 + (kBpZ < 16 ? 4 : 0); }
 
 // Voxel-driven backprojection, kBpZ voxels along z per thread.  For the flat
 // panels of this path (rows in the xy-plane, columns along z) the detector
 // row coordinate u and the projective denominator do not depend on z, so the
-// row footprint and its weights are formed once per projection and shared by
-// the thread's voxels; neighbouring voxels also share a detector column, whose
-// row-weighted sum is reused.
-__global__ void __launch_bounds__(256) k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
-                                                int64_t nproj, const float *__restrict__ y,
-                                                float *__restrict__ img, float *__restrict__ sens) {
+// row footprint [ua, ub] and its weights are formed once per projection and
+// shared by the thread's voxels.  The row-weighted column sums RS_c over the
+// columns the voxel run covers are accumulated into prefix sums P_c (kept in
+// shared memory, one slot column per thread); the footprint integral of a
+// voxel over [va, vb] is then D(vb) - D(va) with D(v) = P_m + (v - m) RS_m,
+// m = floor(v): two shared-memory reads per voxel instead of a walk over its
+// detector pixels.
+template <int kBpZ, bool SENS, bool FULL>
+__global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
+                                                       int64_t nproj, const float *__restrict__ y,
+                                                       float *__restrict__ img, float *__restrict__ sens) {
+    constexpr int kBpCols = bp_slots(kBpZ);
+    __shared__ float2 pref[kBpCols][kBpThreads];  // (P_m, RS_m) of column cA + m
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int kz0 = blockIdx.z * kBpZ;
     if (i >= g.nx || j >= g.ny || kz0 >= g.nz) return;
-    const int nzt = min(kBpZ, g.nz - kz0);
+    const int nzt = FULL ? kBpZ : min(kBpZ, g.nz - kz0);  // FULL: nz is a multiple of kBpZ
     const float qx = fmaf((float)i, g.dx, g.bx + 0.5f * g.dx);
     const float qy = fmaf((float)j, g.dy, g.by + 0.5f * g.dy);
     const float qz0 = fmaf((float)kz0, g.dz, g.bz + 0.5f * g.dz);
@@ -248,85 +295,136 @@ __global__ void __launch_bounds__(256) k_bdd_bp(Grid g, const BddProj *__restric
         const float ur = fmaf(P.au[0], rx, fmaf(P.au[1], ry, fmaf(P.au[2], qz0, P.au0))) * dr;
         const float ua = fmaxf(fminf(ul, ur), 0.f), ub = fminf(fmaxf(ul, ur), fnr);
         if (!(ub > ua)) continue;
-        const int r0 = (int)floorf(ua), r1 = min((int)ceilf(ub), nr) - 1;
+        const int r0 = (int)ua;  // ua >= 0: truncation is floor
+        const Seg seg = make_seg(ua, ub, r0, min((int)ceilf(ub), nr) - 1 - r0);
         // v of the two corners of voxel t: linear in t
         const float vl0 = fmaf(P.av[0], lx, fmaf(P.av[1], ly, fmaf(P.av[2], qz0 - hz, P.av0))) * dl;
         const float vr0 = fmaf(P.av[0], rx, fmaf(P.av[1], ry, fmaf(P.av[2], qz0 + hz, P.av0))) * dr;
         const float svl = P.av[2] * g.dz * dl, svr = P.av[2] * g.dz * dr;
+        const float tl = (float)(nzt - 1);
+        const float vA = fmaxf(fminf(fminf(vl0, vr0), fminf(fmaf(tl, svl, vl0), fmaf(tl, svr, vr0))), 0.f);
+        const float vB = fminf(fmaxf(fmaxf(vl0, vr0), fmaxf(fmaf(tl, svl, vl0), fmaf(tl, svr, vr0))), fnc);
+        if (!(vB > vA)) continue;
         // kerroin = d * |v| / |v_axis|, v = voxel centre - source
         const float vx = qx - P.s[0], vy = qy - P.s[1];
         const float axy = vx * vx + vy * vy;
-        const float kscale = P.ysl ? g.dy / fabsf(vy) : g.dx / fabsf(vx);
-        const float *yp = y + p * (int64_t)nr * nc;
-        int cc = -1;
-        float crow = 0.f;
+        const float kscale = P.ysl ? __fdividef(g.dy, fabsf(vy)) : __fdividef(g.dx, fabsf(vx));
+        const float *yp = y + p * (int64_t)nr * nc + r0;
+#define col_sum(c) seg_sum(seg, yp + (int64_t)(c) * nr)
+        const int cA = (int)vA;
+        const int ncols = min((int)ceilf(vB), nc) - cA;
+        if (ncols <= kBpCols) {
+            float acc = 0.f;
+            for (int m = 0; m < ncols; ++m) {
+                const float rs = col_sum(cA + m);
+                pref[m][tid] = make_float2(acc, rs);
+                acc += rs;
+            }
+            const float fA = (float)cA;
+            const int mmax = ncols - 1;
 #pragma unroll
-        for (int t = 0; t < kBpZ; ++t) {
-            if (t < nzt) {
+            for (int t = 0; t < kBpZ; ++t) {
+                if (FULL || t < nzt) {
+                    const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
+                    // clamp to [vA, vB] (inside [0, nc]); an empty footprint gives va == vb
+                    const float qa = fminf(fmaxf(fminf(vlt, vrt), vA), vB) - fA;
+                    const float qb = fminf(fmaxf(fmaxf(vlt, vrt), vA), vB) - fA;
+                    const int ma = min((int)qa, mmax), mb = min((int)qb, mmax);
+                    const float2 ea = pref[ma][tid], eb = pref[mb][tid];
+                    const float apu = fmaf(qb - (float)mb, eb.y, eb.x) - fmaf(qa - (float)ma, ea.y, ea.x);
+                    if (apu != 0.f) {
+                        const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
+                        const float q2 = fmaf(vz, vz, axy);
+                        const float ker = kscale * (q2 * rsqrtf(q2));
+                        temp[t] = fmaf(apu, ker, temp[t]);
+                        if (SENS) wsum[t] += ker;
+                    }
+                }
+            }
+        } else {
+            // footprints wider than the slot array: per voxel, walk its columns
+#pragma unroll
+            for (int t = 0; t < kBpZ; ++t) {
                 const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
                 const float va = fmaxf(fminf(vlt, vrt), 0.f), vb = fminf(fmaxf(vlt, vrt), fnc);
-                if (vb > va) {
-                    const int c0 = (int)floorf(va), c1 = min((int)ceilf(vb), nc) - 1;
+                if ((FULL || t < nzt) && vb > va) {
+                    const int c0 = (int)va, c1 = min((int)ceilf(vb), nc) - 1;
                     float apu = 0.f;
                     for (int c = c0; c <= c1; ++c) {
-                        float rowsum;
-                        if (c == cc) {
-                            rowsum = crow;
-                        } else {
-                            rowsum = 0.f;
-                            const float *col = yp + (int64_t)c * nr;
-                            for (int rr = r0; rr <= r1; ++rr) {
-                                const float ou = fminf(ub, (float)(rr + 1)) - fmaxf(ua, (float)rr);
-                                rowsum = fmaf(ou, __ldg(col + rr), rowsum);
-                            }
-                            cc = c;
-                            crow = rowsum;
-                        }
                         const float ov = fminf(vb, (float)(c + 1)) - fmaxf(va, (float)c);
-                        apu = fmaf(ov, rowsum, apu);
+                        apu = fmaf(ov, col_sum(c), apu);
                     }
                     if (apu != 0.f) {
                         const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
-                        const float ker = kscale * sqrtf(fmaf(vz, vz, axy));
+                        const float q2 = fmaf(vz, vz, axy);
+                        const float ker = kscale * (q2 * rsqrtf(q2));
                         temp[t] = fmaf(apu, ker, temp[t]);
-                        wsum[t] += ker;
+                        if (SENS) wsum[t] += ker;
                     }
                 }
             }
         }
+#undef col_sum
     }
     int64_t n = i + (int64_t)j * g.nx + (int64_t)kz0 * g.nx * g.ny;
 #pragma unroll
     for (int t = 0; t < kBpZ; ++t) {
         if (t < nzt) {
             img[n] = temp[t];
-            if (sens) sens[n] = wsum[t];
+            if (SENS) sens[n] = wsum[t];
         }
         n += (int64_t)g.nx * g.ny;
     }
 }
 
+template <int C>
+static void launch_fp(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
+                      int64_t nproj, const float *img, const float *imgT, float *y, cudaStream_t st) {
+    const int groups = (nc + C - 1) / C;
+    dim3 block(32, 8);
+    dim3 grid((nr + 31) / 32, (groups + 7) / 8, (unsigned)nproj);
+    k_bdd_fp<C><<<grid, block, 0, st>>>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y);
+}
+
+template <int Z>
+static void launch_bp(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
+                      float *sens, cudaStream_t st) {
+    dim3 block(32, kBpThreads / 32);
+    dim3 grid((g.nx + 31) / 32, (g.ny + block.y - 1) / block.y, (g.nz + Z - 1) / Z);
+    const bool full = g.nz % Z == 0;
+    if (sens && full)
+        k_bdd_bp<Z, true, true><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+    else if (sens)
+        k_bdd_bp<Z, true, false><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+    else if (full)
+        k_bdd_bp<Z, false, true><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+    else
+        k_bdd_bp<Z, false, false><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+}
+
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
-                int64_t nproj, const float *img, float *imgT, float *y, cudaStream_t st) {
+                int64_t nproj, const float *img, float *imgT, float *y, int cols, cudaStream_t st) {
     if (nproj <= 0) return OMB_OK;
     if (nproj > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 projections in one call");
     dim3 tg((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz);
     k_transpose_xy<<<tg, dim3(32, 8), 0, st>>>(img, imgT, g.nx, g.ny, g.nz);
     OMB_LAUNCH_CHECK("transpose launch");
-    const int groups = (nc + kColsPerThread - 1) / kColsPerThread;
-    dim3 block(32, 8);
-    dim3 grid((nr + 31) / 32, (groups + 7) / 8, (unsigned)nproj);
-    k_bdd_fp<<<grid, block, 0, st>>>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y);
+    switch (cols) {
+        case 16: launch_fp<16>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, st); break;
+        default: launch_fp<8>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, st); break;
+    }
     OMB_LAUNCH_CHECK("bdd forward launch");
     return OMB_OK;
 }
 
 int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                 float *sens, cudaStream_t st) {
-    if (g.nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
-    dim3 block(32, 8);
-    dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kBpZ - 1) / kBpZ);
-    k_bdd_bp<<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+                 float *sens, int zrun, cudaStream_t st) {
+    if (g.nz > 65535 * 4) return set_error(OMB_ERR_UNSUPPORTED, "too many slices");
+    switch (zrun) {
+        case 4: launch_bp<4>(g, pj, nr, nc, nproj, y, img, sens, st); break;
+        case 16: launch_bp<16>(g, pj, nr, nc, nproj, y, img, sens, st); break;
+        default: launch_bp<8>(g, pj, nr, nc, nproj, y, img, sens, st); break;
+    }
     OMB_LAUNCH_CHECK("bdd backward launch");
     return OMB_OK;
 }

@@ -88,6 +88,14 @@ struct BddProj {
     int spos;   // sign of the source's dominant coordinate (s.y if ysl, else s.x) > 0
 };
 
+// Launch shapes the autotuner chooses between (per handle).
+struct Tuning {
+    int siddon_blocks_per_sm = 8;   // grid-stride grid of the Siddon kernels: blocks per SM
+    int siddon_frames = 8;          // most frames sharing one ray walk (1, 2, 4, 8)
+    int bdd_fp_cols = 8;            // type-5 forward: detector columns per thread (8, 16)
+    int bdd_bp_z = 8;               // type-5 backward: voxels along z per thread (4, 8, 16)
+};
+
 constexpr int kMaxTofBins = 16;
 constexpr int kBlock = 256;
 

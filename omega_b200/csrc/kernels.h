@@ -5,9 +5,10 @@
 
 namespace omb {
 
-int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, cudaStream_t st);
+int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, const Tuning &tn,
+                   cudaStream_t st);
 int siddon_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, float *sens,
-                    cudaStream_t st);
+                    const Tuning &tn, cudaStream_t st);
 int siddon_backward_fixed(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *y,
                           unsigned long long *acc, unsigned long long *acc_sens, cudaStream_t st);
 int siddon_count(const Grid &g, const RaySet &rs, const Tof &tof, unsigned long long *total, cudaStream_t st);
@@ -15,9 +16,9 @@ int fixed_to_float(const unsigned long long *acc, float *out, int64_t n, cudaStr
 
 // Projector type 5 (branchless distance-driven), CT.
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
-                int64_t nproj, const float *img, float *imgT, float *y, cudaStream_t st);
+                int64_t nproj, const float *img, float *imgT, float *y, int cols, cudaStream_t st);
 int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                 float *sens, cudaStream_t st);
+                 float *sens, int zrun, cudaStream_t st);
 
 // PDHG + TV and the power method.
 int pdhg_dual(float *p, const float *fp, const float *y, int64_t n, float sigma, cudaStream_t st);

@@ -204,16 +204,17 @@ __global__ void k_fixed_to_float(const unsigned long long *__restrict__ acc, flo
 }
 
 template <int NB, int FB>
-static void fp_launch(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, cudaStream_t st) {
-    dim3 grid(grid_for(rs.m_size), (fr.n + FB - 1) / FB);
+static void fp_launch(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, int per_sm,
+                      cudaStream_t st) {
+    dim3 grid(grid_for(rs.m_size, per_sm), (fr.n + FB - 1) / FB);
     k_siddon_fp<NB, FB><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, fr.img_in, fr.img_stride, fr.meas_out,
                                                   fr.meas_stride, fr.n);
 }
 
 template <int NB, int FB>
 static void bp_launch(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, float *sens,
-                      cudaStream_t st) {
-    dim3 grid(grid_for(rs.m_size), (fr.n + FB - 1) / FB);
+                      int per_sm, cudaStream_t st) {
+    dim3 grid(grid_for(rs.m_size, per_sm), (fr.n + FB - 1) / FB);
     if (sens)
         k_siddon_bp<NB, FB, true><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, fr.meas, fr.meas_stride, fr.img,
                                                              fr.img_stride, sens, fr.n);
@@ -235,22 +236,27 @@ static void bp_fixed_launch(const Grid &g, const RaySet &rs, const Tof &tof, flo
 #define OMB_NB_CASES(X) \
     X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 
-// Frames per walk for non-TOF batches.
-static int frames_per_walk(int n) { return n >= 8 ? 8 : (n >= 4 ? 4 : (n >= 2 ? 2 : 1)); }
+// Frames per walk for non-TOF batches (at most `most`).
+static int frames_per_walk(int n, int most) {
+    n = n < most ? n : most;
+    return n >= 8 ? 8 : (n >= 4 ? 4 : (n >= 2 ? 2 : 1));
+}
 
-int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, cudaStream_t st) {
+int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, const Tuning &tn,
+                   cudaStream_t st) {
+    const int ps = tn.siddon_blocks_per_sm;
     if (rs.m_size <= 0 || fr.n <= 0) return OMB_OK;
     if (tof.nbins > 1 && fr.n != 1) return set_error(OMB_ERR_UNSUPPORTED, "TOF projections take one frame per call");
     if (tof.nbins == 1) {
-        switch (frames_per_walk(fr.n)) {
-            case 8: fp_launch<1, 8>(g, rs, tof, gf, fr, st); break;
-            case 4: fp_launch<1, 4>(g, rs, tof, gf, fr, st); break;
-            case 2: fp_launch<1, 2>(g, rs, tof, gf, fr, st); break;
-            default: fp_launch<1, 1>(g, rs, tof, gf, fr, st); break;
+        switch (frames_per_walk(fr.n, tn.siddon_frames)) {
+            case 8: fp_launch<1, 8>(g, rs, tof, gf, fr, ps, st); break;
+            case 4: fp_launch<1, 4>(g, rs, tof, gf, fr, ps, st); break;
+            case 2: fp_launch<1, 2>(g, rs, tof, gf, fr, ps, st); break;
+            default: fp_launch<1, 1>(g, rs, tof, gf, fr, ps, st); break;
         }
     } else {
         switch (tof.nbins) {
-#define X(n) case n: fp_launch<n, 1>(g, rs, tof, gf, fr, st); break;
+#define X(n) case n: fp_launch<n, 1>(g, rs, tof, gf, fr, ps, st); break;
             OMB_NB_CASES(X)
 #undef X
             default:
@@ -262,19 +268,20 @@ int siddon_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, co
 }
 
 int siddon_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, float *sens,
-                    cudaStream_t st) {
+                    const Tuning &tn, cudaStream_t st) {
+    const int ps = tn.siddon_blocks_per_sm;
     if (rs.m_size <= 0 || fr.n <= 0) return OMB_OK;
     if (tof.nbins > 1 && fr.n != 1) return set_error(OMB_ERR_UNSUPPORTED, "TOF projections take one frame per call");
     if (tof.nbins == 1) {
-        switch (frames_per_walk(fr.n)) {
-            case 8: bp_launch<1, 8>(g, rs, tof, gf, fr, sens, st); break;
-            case 4: bp_launch<1, 4>(g, rs, tof, gf, fr, sens, st); break;
-            case 2: bp_launch<1, 2>(g, rs, tof, gf, fr, sens, st); break;
-            default: bp_launch<1, 1>(g, rs, tof, gf, fr, sens, st); break;
+        switch (frames_per_walk(fr.n, tn.siddon_frames)) {
+            case 8: bp_launch<1, 8>(g, rs, tof, gf, fr, sens, ps, st); break;
+            case 4: bp_launch<1, 4>(g, rs, tof, gf, fr, sens, ps, st); break;
+            case 2: bp_launch<1, 2>(g, rs, tof, gf, fr, sens, ps, st); break;
+            default: bp_launch<1, 1>(g, rs, tof, gf, fr, sens, ps, st); break;
         }
     } else {
         switch (tof.nbins) {
-#define X(n) case n: bp_launch<n, 1>(g, rs, tof, gf, fr, sens, st); break;
+#define X(n) case n: bp_launch<n, 1>(g, rs, tof, gf, fr, sens, ps, st); break;
             OMB_NB_CASES(X)
 #undef X
             default:

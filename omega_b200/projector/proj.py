@@ -573,6 +573,37 @@ class projectorClass:
                      int(mode), ctypes.c_void_p(stream))
         return (f, s) if sens else f
 
+    @property
+    def tuning(self):
+        """Launch shapes of this object's projector kernels (a dict)."""
+        self._check_ready()
+        t = _native.Tuning(struct_size=ctypes.sizeof(_native.Tuning))
+        _native.call("omb_get_tuning", self._handle, ctypes.byref(t))
+        return t.as_dict()
+
+    @tuning.setter
+    def tuning(self, values):
+        self._check_ready()
+        t = _native.Tuning(struct_size=ctypes.sizeof(_native.Tuning))
+        _native.call("omb_get_tuning", self._handle, ctypes.byref(t))
+        for k, v in dict(values).items():
+            if k not in t.as_dict():
+                raise KeyError(f"unknown tuning key {k!r}")
+            setattr(t, k, int(v))
+        _native.call("omb_set_tuning", self._handle, ctypes.byref(t))
+
+    def autotune(self, n_frames=1, repeats=3):
+        """Times the candidate launch shapes of the forward and backward
+        projectors on this geometry (all subsets, n_frames images at once),
+        keeps the fastest and returns them.  Synchronises the device."""
+        self._check_ready()
+        import torch
+        dev = torch.device("cuda", self._device)
+        t = _native.Tuning(struct_size=ctypes.sizeof(_native.Tuning))
+        _native.call("omb_autotune", self._handle, int(n_frames), int(repeats), ctypes.byref(t),
+                     ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        return t.as_dict()
+
     def T(self):
         self.trans = True
         return self

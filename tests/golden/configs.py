@@ -59,6 +59,14 @@ CONFIGS = {
 }
 # the same CT geometry with the branchless distance-driven projector (type 5)
 CONFIGS["ct_mini5"] = dict(CONFIGS["ct_mini"], projector_type=5, subsets=1)
+# type 5 with 0.5 mm voxels under 4 mm pixels: a pixel's footprint spans about
+# four voxels laterally and axially (the opposite regime of ct_mini5, where a
+# voxel's footprint spans several pixels)
+CONFIGS["ct_fine5"] = dict(CT=True, nRowsD=24, nColsD=20, nProjections=30, dPitchX=4.0, dPitchY=4.0,
+                           sourceToCRot=500., sourceToDetector=1000., Nx=64, Ny=64, Nz=48, FOVa_x=32.,
+                           FOVa_y=32., axial_fov=24., projector_type=5, subsets=1, subsetType=8, Niter=1,
+                           verbose=0, angles=np.linspace(0, 2 * np.pi, 30, endpoint=False).astype(np.float32),
+                           SinM=np.zeros((24, 20, 30), dtype=np.float32))
 # TOF width so that the bins cover the FOV diagonal: 7 bins of 85 mm / (c/2) seconds
 CONFIGS["pet_mini_tof"]["TOF_width"] = 85.0 / (2.99792458e11 / 2.)
 

@@ -102,3 +102,7 @@ def test_null_handle_calls_fail_cleanly():
     assert L.omb_pdhg_primal(None, None, None, None, None, 1.0, 1.0, 0.0, 1e-4, 1, None) == -1
     assert L.omb_pdhg_iteration(None, None, None, None, None, None, 1.0, 1.0, 1.0, 0.0, 1e-4, 1, None, None,
                                 None) == -1
+    t = _native.Tuning(struct_size=ctypes.sizeof(_native.Tuning))
+    assert L.omb_get_tuning(None, ctypes.byref(t)) == -1
+    assert L.omb_set_tuning(None, ctypes.byref(t)) == -1
+    assert L.omb_autotune(None, 1, 1, ctypes.byref(t), None) == -1

@@ -1,0 +1,95 @@
+"""Launch-shape tuning: every candidate shape computes the same projections
+(parity with the FP64 oracle at 1e-5 relative L2 for each), the autotuner
+returns a valid shape, and invalid shapes are rejected."""
+import itertools
+
+import numpy as np
+import pytest
+
+from conftest import make_options
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def _init(name):
+    o = make_options(name)
+    o.initProj()
+    return o
+
+
+def _t(a, dev):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev)
+
+
+@pytest.mark.parametrize("name", ["ct_mini5", "ct_fine5"])
+def test_bdd_every_shape_matches_oracle(cuda, name):
+    o = _init(name)
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(11)
+    x = rng.uniform(0.0, 1.0, g.n_img)
+    y = rng.uniform(0.0, 2.0, g.rays(0))
+    ref_fp = orc.bdd_forward(g, x, 0)
+    ref_bp, ref_s = orc.bdd_backward(g, y, 0, sens=True)
+    for cols, zrun in itertools.product([8, 16], [4, 8, 16]):
+        o.tuning = {"bdd_fp_columns": cols, "bdd_bp_zrun": zrun}
+        fp = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
+        bp, s = o.backwardProject(_t(y, cuda), 0, sens=True)
+        assert orc.rel_l2(fp, ref_fp) < TOL, (cols, orc.rel_l2(fp, ref_fp))
+        assert orc.rel_l2(bp.cpu().numpy(), ref_bp) < TOL, (zrun, orc.rel_l2(bp.cpu().numpy(), ref_bp))
+        assert orc.rel_l2(s.cpu().numpy(), ref_s) < TOL, zrun
+
+
+def test_siddon_every_shape_matches_oracle(cuda):
+    import ctypes
+
+    import torch
+    from omega_b200 import _native
+    o = _init("pet_mini")
+    g = orc.Geometry(o)
+    n, m = g.n_img, o.measurementCount(-1)
+    frames = 5
+    rng = np.random.default_rng(12)
+    imgs = rng.uniform(0.5, 2.0, (frames, n))
+    ref = np.concatenate([orc.forward(g, imgs[0], s) for s in range(g.n_subsets)])
+    X = _t(imgs, cuda)
+    Y = torch.empty((frames, m), device=cuda)
+    st = ctypes.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
+    for ps, fw in itertools.product([1, 2, 8, 16], [1, 2, 4, 8]):
+        o.tuning = {"siddon_blocks_per_sm": ps, "siddon_frames_per_walk": fw}
+        _native.call("omb_forward_frames", o._handle, -1, frames, ctypes.c_void_p(X.data_ptr()), n,
+                     ctypes.c_void_p(Y.data_ptr()), m, st)
+        y = Y.cpu().numpy()
+        assert orc.rel_l2(y[0], ref) < TOL, (ps, fw)
+        for f in range(1, frames):
+            ref_f = np.concatenate([orc.forward(g, imgs[f], s) for s in range(g.n_subsets)])
+            assert orc.rel_l2(y[f], ref_f) < TOL, (ps, fw, f)
+
+
+@pytest.mark.parametrize("name,frames", [("ct_mini5", 1), ("pet_mini", 4)])
+def test_autotune_returns_valid_shape(cuda, name, frames):
+    o = _init(name)
+    t = o.autotune(n_frames=frames, repeats=1)
+    assert t == o.tuning
+    assert 1 <= t["siddon_blocks_per_sm"] <= 32
+    assert t["siddon_frames_per_walk"] in (1, 2, 4, 8)
+    assert t["bdd_fp_columns"] in (8, 16)
+    assert t["bdd_bp_zrun"] in (4, 8, 16)
+    g = orc.Geometry(o)
+    x = np.random.default_rng(13).uniform(0.5, 1.5, g.n_img)
+    fp = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
+    ref = orc.bdd_forward(g, x, 0) if name == "ct_mini5" else orc.forward(g, x, 0)
+    assert orc.rel_l2(fp, ref) < TOL
+
+
+@pytest.mark.parametrize("key,value", [("siddon_blocks_per_sm", 0), ("siddon_frames_per_walk", 3),
+                                       ("bdd_fp_columns", 4), ("bdd_bp_zrun", 32)])
+def test_invalid_shape_rejected(cuda, key, value):
+    from omega_b200 import _native
+    o = _init("ct_mini5")
+    before = o.tuning
+    with pytest.raises(_native.NativeError):
+        o.tuning = {key: value}
+    assert o.tuning == before
