@@ -85,6 +85,8 @@ static std::vector<BddProj> bdd_maps(const omb_geometry_desc &d) {
         P.av0 = (float)(-dot(cv, s) / ((double)d.dpitch_y * D0));
         P.ysl = fabs(s[0]) <= fabs(s[1]);
         P.spos = P.ysl ? (s[1] > 0.0) : (s[0] > 0.0);
+        const double dms[3] = {dd[0] - s[0], dd[1] - s[1], dd[2] - s[2]};
+        P.k = (float)(dot(n, dms) / D0);
         out[(size_t)p] = P;
     }
     return out;
@@ -98,14 +100,18 @@ static int validate(const omb_geometry_desc *d) {
     if (d->abi_version != OMB_ABI_VERSION) return set_error(OMB_ERR_INVALID, "unsupported abi_version");
     if (d->modality != OMB_PET_SINOGRAM && d->modality != OMB_CT_PANEL)
         return set_error(OMB_ERR_INVALID, "modality must be OMB_PET_SINOGRAM or OMB_CT_PANEL");
-    if (d->fp_type != 1 && d->fp_type != 5)
+    if (d->fp_type != 1 && d->fp_type != 4 && d->fp_type != 5)
         return set_error(OMB_ERR_UNSUPPORTED, "forward projector type " + std::to_string(d->fp_type) + " is not built");
-    if (d->bp_type != 1 && d->bp_type != 5)
+    if (d->bp_type != 1 && d->bp_type != 4 && d->bp_type != 5)
         return set_error(OMB_ERR_UNSUPPORTED, "backprojector type " + std::to_string(d->bp_type) + " is not built");
     if ((d->fp_type == 5 || d->bp_type == 5) && d->modality != OMB_CT_PANEL)
         return set_error(OMB_ERR_INVALID, "Projector type 5 is only supported with CT data!");
     if ((d->fp_type == 5 || d->bp_type == 5) && d->tof_bins > 1)
         return set_error(OMB_ERR_INVALID, "projector type 5 has no TOF");
+    if ((d->fp_type == 4 || d->bp_type == 4) && !(d->dL > 0.f))
+        return set_error(OMB_ERR_INVALID, "projector type 4 needs a positive sampling length dL");
+    if (d->bp_type == 4 && d->modality == OMB_CT_PANEL && !(d->kerroin > 0.f))
+        return set_error(OMB_ERR_INVALID, "the type-4 CT backprojection needs its weight kerroin > 0");
     if (d->nx == 0 || d->ny == 0 || d->nz == 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
     if (!(d->dx > 0.f) || !(d->dy > 0.f) || !(d->dz > 0.f)) return set_error(OMB_ERR_INVALID, "voxel size must be positive");
     if (d->n_rows_d == 0 || d->n_cols_d == 0) return set_error(OMB_ERR_INVALID, "detector size must be positive");
@@ -196,6 +202,37 @@ static Frames one_frame_bp(const omb_handle *h, const float *y, float *img, int6
     return f;
 }
 
+// Ray-driven forward projection of a batch of frames (types 1 and 4).
+static int rays_forward(const omb_handle *h, const RaySet &rs, const Frames &f, cudaStream_t s) {
+    if (h->desc.fp_type == 4) {
+        for (int fr = 0; fr < f.n; ++fr) {
+            const int st = interp_forward(h->grid, rs, h->tof, h->desc.global_factor, h->desc.dL,
+                                          f.img_in + fr * f.img_stride, f.meas_out + fr * f.meas_stride, h->tune, s);
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
+    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, f, h->tune, s);
+}
+
+// Ray-driven backprojection (float atomics, types 1 and 4) of a batch of
+// frames into zeroed images; `sens` (zeroed) receives A^T 1 of the first
+// frame's rays.  f.meas == NULL backprojects ones, f.img == NULL keeps only
+// the sensitivity.
+static int rays_backward(const omb_handle *h, const RaySet &rs, const Frames &f, float *sens, cudaStream_t s) {
+    if (h->desc.bp_type == 4) {
+        for (int fr = 0; fr < f.n; ++fr) {
+            const int st = interp_backward(h->grid, rs, h->tof, h->desc.global_factor, h->desc.dL,
+                                           f.meas ? f.meas + fr * f.meas_stride : nullptr,
+                                           f.img ? f.img + fr * f.img_stride : nullptr, fr == 0 ? sens : nullptr,
+                                           nullptr, nullptr, h->tune, s);
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
+    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, sens, h->tune, s);
+}
+
 extern "C" {
 
 int omb_abi_version(void) { return OMB_ABI_VERSION; }
@@ -250,7 +287,7 @@ int omb_create(const omb_geometry_desc *desc, omb_handle **out) {
         if ((e = cudaMalloc(&h->d_imgT, h->n_img * sizeof(float))) != cudaSuccess)
             return fail(cuda_fail(e, "cudaMalloc type-5 image copy"));
     }
-    if (desc->bp_type == 5) {
+    if (desc->bp_type == 5 || (desc->bp_type == 4 && desc->modality == OMB_CT_PANEL)) {
         std::vector<BddProj> maps = bdd_maps(*desc);
         if ((e = cudaMalloc(&h->d_bddp, maps.size() * sizeof(BddProj))) != cudaSuccess)
             return fail(cuda_fail(e, "cudaMalloc type-5 projection maps"));
@@ -299,8 +336,7 @@ int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, voi
     if (h->desc.fp_type == 5)
         return bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj, image,
                            h->d_imgT, y, h->tune.bdd_fp_cols, (cudaStream_t)stream);
-    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, y, rs.m_size), h->tune,
-                          (cudaStream_t)stream);
+    return rays_forward(h, rs, one_frame_fp(h, image, y, rs.m_size), (cudaStream_t)stream);
 }
 
 int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const float *images, int64_t image_stride,
@@ -328,7 +364,7 @@ int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const fl
     f.img_stride = image_stride;
     f.meas_out = y;
     f.meas_stride = y_stride;
-    return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, f, h->tune, (cudaStream_t)stream);
+    return rays_forward(h, rs, f, (cudaStream_t)stream);
 }
 
 int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, float *sens, int32_t mode,
@@ -349,10 +385,20 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
         return bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y, image, sens,
                             h->tune.bdd_bp_z, s);
     }
+    if (h->desc.bp_type == 4 && h->desc.modality == OMB_CT_PANEL) {
+        if (mode != OMB_BP_FLOAT_ATOMIC)
+            return set_error(OMB_ERR_UNSUPPORTED, "the type-4 CT backprojection is a gather; it has no fixed-point mode");
+        return interp_ct_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, h->desc.kerroin, y,
+                                  image, sens, s);
+    }
     if (mode == OMB_BP_FIXED64) {
         unsigned long long *acc = h->d_acc, *acc_s = sens ? h->d_acc + h->n_img : nullptr;
         OMB_CUDA_TRY(cudaMemsetAsync(h->d_acc, 0, (sens ? 2 : 1) * h->n_img * sizeof(unsigned long long), s));
-        st = siddon_backward_fixed(h->grid, rs, h->tof, h->desc.global_factor, y, acc, acc_s, s);
+        if (h->desc.bp_type == 4)
+            st = interp_backward(h->grid, rs, h->tof, h->desc.global_factor, h->desc.dL, y, nullptr, nullptr, acc,
+                                 acc_s, h->tune, s);
+        else
+            st = siddon_backward_fixed(h->grid, rs, h->tof, h->desc.global_factor, y, acc, acc_s, s);
         if (st != OMB_OK) return st;
         st = fixed_to_float(acc, image, h->n_img, s);
         if (st == OMB_OK && sens) st = fixed_to_float(acc_s, sens, h->n_img, s);
@@ -360,8 +406,7 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
     }
     OMB_CUDA_TRY(cudaMemsetAsync(image, 0, nb, s));
     if (sens) OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, nb, s));
-    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, y, image, rs.m_size), sens,
-                           h->tune, s);
+    return rays_backward(h, rs, one_frame_bp(h, y, image, rs.m_size), sens, s);
 }
 
 int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const float *y, int64_t y_stride,
@@ -375,10 +420,10 @@ int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const f
     if (image_stride < h->n_img || y_stride < rs.m_size * h->desc.tof_bins)
         return set_error(OMB_ERR_INVALID, "frame strides smaller than one image / one measurement vector");
     cudaStream_t s = (cudaStream_t)stream;
-    if (h->desc.bp_type == 5) {
+    if (h->desc.bp_type == 5 || (h->desc.bp_type == 4 && h->desc.modality == OMB_CT_PANEL)) {
         for (int fr = 0; fr < n_frames; ++fr) {
-            st = bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y + fr * y_stride,
-                              images + fr * image_stride, nullptr, h->tune.bdd_bp_z, s);
+            st = omb_backward(h, subset, y + fr * y_stride, images + fr * image_stride, nullptr, OMB_BP_FLOAT_ATOMIC,
+                              stream);
             if (st != OMB_OK) return st;
         }
         return OMB_OK;
@@ -394,7 +439,7 @@ int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const f
     f.meas_stride = y_stride;
     f.img = images;
     f.img_stride = image_stride;
-    return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, nullptr, h->tune, s);
+    return rays_backward(h, rs, f, nullptr, s);
 }
 
 int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
@@ -404,11 +449,11 @@ int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
-    if (h->desc.bp_type != 1) return set_error(OMB_ERR_UNSUPPORTED, "omb_sensitivity needs backprojector type 1");
+    if (h->desc.modality != OMB_PET_SINOGRAM || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_sensitivity needs a ray-driven PET backprojector (type 1 or 4)");
     // A^T 1 through the BP kernel's fused sensitivity accumulator, y = NULL.
     OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, h->n_img * sizeof(float), s));
-    st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, nullptr, nullptr, rs.m_size),
-                         sens, h->tune, s);
+    st = rays_backward(h, rs, one_frame_bp(h, nullptr, nullptr, rs.m_size), sens, s);
     if (st != OMB_OK) return st;
     return clamp_min(sens, h->n_img, h->desc.epps, s);
 }
@@ -419,22 +464,20 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     if (!image || !y_subset || !sens || !work_meas || !work_img)
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osem_subset");
     if (h->desc.modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
-    if (h->desc.fp_type != 1 || h->desc.bp_type != 1)
-        return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset needs projector type 1");
+    if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset needs projector types 1 or 4");
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     const float eps = h->desc.epps;
     const int64_t m = rs.m_size * h->desc.tof_bins;
-    st = siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_fp(h, image, work_meas, rs.m_size),
-                        h->tune, s);
+    st = rays_forward(h, rs, one_frame_fp(h, image, work_meas, rs.m_size), s);
     if (st != OMB_OK) return st;
     st = osem_ratio(y_subset, work_meas, m, eps, s);
     if (st != OMB_OK) return st;
     OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
-    st = siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, one_frame_bp(h, work_meas, work_img, rs.m_size),
-                         nullptr, h->tune, s);
+    st = rays_backward(h, rs, one_frame_bp(h, work_meas, work_img, rs.m_size), nullptr, s);
     if (st != OMB_OK) return st;
     return em_update(image, sens, work_img, h->n_img, eps, s);
 }
@@ -518,8 +561,12 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
     if (n_frames < 1 || repeats < 1) return set_error(OMB_ERR_INVALID, "n_frames and repeats must be >= 1");
     if (out && out->struct_size != sizeof(omb_tuning))
         return set_error(OMB_ERR_INVALID, "omb_tuning.struct_size does not match this library");
-    const bool siddon = h->desc.fp_type == 1 && h->desc.bp_type == 1;
-    if (!siddon || h->desc.tof_bins > 1) n_frames = 1;
+    // ray-driven kernels (types 1 and 4 forward, PET types 1 and 4 backward)
+    // share the blocks-per-SM and frames-per-walk shapes
+    const bool ray_fp = h->desc.fp_type == 1 || h->desc.fp_type == 4;
+    const bool ray_bp = h->desc.bp_type == 1 || (h->desc.bp_type == 4 && h->desc.modality == OMB_PET_SINOGRAM);
+    const bool siddon = ray_fp || ray_bp;
+    if (!(h->desc.fp_type == 1 && h->desc.bp_type == 1) || h->desc.tof_bins > 1) n_frames = 1;
     const int64_t m = omb_measurement_count(h, -1);
     if (m < 0) return -1;
     const int64_t n = h->n_img;
@@ -559,7 +606,7 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
                 h->tune = saved;
                 h->tune.siddon_blocks_per_sm = ps;
                 h->tune.siddon_frames = fr;
-                const float a = timed(fwd), b = a < 0.f ? -1.f : timed(bwd);
+                const float a = ray_fp ? timed(fwd) : 0.f, b = a < 0.f ? -1.f : (ray_bp ? timed(bwd) : 0.f);
                 if (a < 0.f || b < 0.f) {
                     st = -1;
                     break;

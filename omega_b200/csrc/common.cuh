@@ -86,6 +86,8 @@ struct BddProj {
     float s[3];
     int ysl;    // |s.x| <= |s.y|: voxel mid-plane spans x and z
     int spos;   // sign of the source's dominant coordinate (s.y if ysl, else s.x) > 0
+    float k;    // the ray s -> q meets the panel at s + (k / (c.q + 1)) (q - s)
+    float pad[3];
 };
 
 // Launch shapes the autotuner chooses between (per handle).
@@ -97,6 +99,8 @@ struct Tuning {
 };
 
 constexpr int kMaxTofBins = 16;
+// Fixed-point scale of the int64 backprojection mode (the reference's TH).
+constexpr double kFixedScale = 1e11;
 constexpr int kBlock = 256;
 
 inline int num_sms() {

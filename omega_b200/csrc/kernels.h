@@ -20,6 +20,15 @@ int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc,
 int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
                  float *sens, int zrun, cudaStream_t st);
 
+// Projector type 4 (interpolation), PET and CT.
+int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img, float *y,
+                   const Tuning &tn, cudaStream_t st);
+int interp_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *y, float *img,
+                    float *sens, unsigned long long *acc, unsigned long long *acc_s, const Tuning &tn,
+                    cudaStream_t st);
+int interp_ct_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, float kerroin,
+                       const float *y, float *img, float *sens, cudaStream_t st);
+
 // PDHG + TV and the power method.
 int pdhg_dual(float *p, const float *fp, const float *y, int64_t n, float sigma, cudaStream_t st);
 int pdhg_primal_tv(const Grid &g, const float *x, const float *rhs, float *u, float *x_out, float beta, float smooth,

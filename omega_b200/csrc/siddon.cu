@@ -12,7 +12,6 @@ namespace omb {
 
 // Fixed-point scale of the deterministic backprojection: the reference's
 // TH = 1e11 (omegatomo/projector/init.py:105).
-constexpr double kFixedScale = 1e11;
 
 // Forward projection.  Each thread walks one ray once and accumulates it for
 // FB frames of a dynamic study (blockIdx.y selects the group of frames), so

@@ -117,6 +117,18 @@ class projectorClass:
     n_rays_transaxial = 1
     n_rays_axial = 1
     dL = 0
+    # projector scales (coordinates.py:209-269 fills those of the chosen type)
+    dScaleX4 = np.empty(0, dtype=np.float32)
+    dScaleY4 = np.empty(0, dtype=np.float32)
+    dScaleZ4 = np.empty(0, dtype=np.float32)
+    dSizeX = np.empty(0, dtype=np.float32)
+    dSizeY = np.empty(0, dtype=np.float32)
+    dScaleX = np.empty(0, dtype=np.float32)
+    dScaleY = np.empty(0, dtype=np.float32)
+    dScaleZ = np.empty(0, dtype=np.float32)
+    dSizeZBP = 0.
+    dSizeXBP = 0.
+    kerroin = np.empty(0, dtype=np.float32)
     useTotLength = True
     useImages = True
     useMAD = True
@@ -449,6 +461,11 @@ class projectorClass:
             keep['tof'] = np.ascontiguousarray(np.asarray(self.TOFCenter, dtype=np.float32).ravel())
             d.tof_centers = _native.f32_ptr(keep['tof'])
         d.dL = float(self.dL)
+        if fpt == 4 or bpt == 4:
+            d.d_scale4[0], d.d_scale4[1], d.d_scale4[2] = (float(np.ravel(self.dScaleX4)[0]),
+                                                           float(np.ravel(self.dScaleY4)[0]),
+                                                           float(np.ravel(self.dScaleZ4)[0]))
+            d.kerroin = float(np.ravel(self.kerroin)[0])
         if fpt == 5 or bpt == 5:
             d.d_size5[0], d.d_size5[1] = float(self.dSizeX[0]), float(self.dSizeY[0])
             d.d_scale5[0], d.d_scale5[1], d.d_scale5[2] = (float(self.dScaleX[0]), float(self.dScaleY[0]),

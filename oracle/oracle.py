@@ -82,6 +82,9 @@ def lib():
         C = ctypes.POINTER(OracleCT)
         L.oracle_bdd_fp.argtypes = [C, P, P]
         L.oracle_bdd_bp.argtypes = [C, P, P, P]
+        L.oracle_interp_fp.argtypes = [G, ctypes.c_double, P, P]
+        L.oracle_interp_bp.argtypes = [G, ctypes.c_double, P, P, P]
+        L.oracle_interp_ct_bp.argtypes = [C, ctypes.c_double, P, P, P]
         _lib = L
     return _lib
 
@@ -122,6 +125,9 @@ class Geometry:
         self.sigma_x = float(o.sigma_x)
         self.tofc = np.ascontiguousarray(np.asarray(o.TOFCenter, dtype=np.float64).ravel()) if o.TOF else \
             np.zeros(1, dtype=np.float64)
+        # projector type 4: sampling length and the CT backprojection weight
+        self.dL = float(o.dL)
+        self.kerroin = float(np.ravel(o.kerroin)[0]) if np.size(o.kerroin) else 0.0
 
     @property
     def n_img(self):
@@ -196,21 +202,24 @@ def intersections(geom: Geometry, subset):
     return int(lib().oracle_siddon_count(ctypes.byref(g)))
 
 
-def osem(geom: Geometry, y_subsets, x0, n_iter):
-    """Restated OSEM loop in FP64; returns the image after n_iter iterations."""
+def osem(geom: Geometry, y_subsets, x0, n_iter, forward=None, backward=None):
+    """Restated OSEM loop in FP64; returns the image after n_iter iterations.
+    The projector pair defaults to the Siddon restatement (type 1)."""
+    fwd = forward or globals()["forward"]
+    bwd = backward or globals()["backward"]
     x = np.asarray(x0, dtype=np.float64).copy()
     eps = geom.epps
     sens = []
     for s in range(geom.n_subsets):
-        _, sv = backward(geom, None, s, sens=True)
+        _, sv = bwd(geom, None, s, sens=True)
         sens.append(np.maximum(sv, eps))
     for _ in range(n_iter):
         for s in range(geom.n_subsets):
-            fp = forward(geom, x, s) + eps
+            fp = fwd(geom, x, s) + eps
             with np.errstate(divide="ignore", invalid="ignore"):
                 r = np.asarray(y_subsets[s], dtype=np.float64) / fp
             r[~np.isfinite(r)] = eps
-            rhs = backward(geom, r, s)
+            rhs = bwd(geom, r, s)
             x = x / sens[s] * (rhs + eps)
     return x
 
@@ -367,3 +376,41 @@ def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1
             u = np.maximum(eps, u)
         x = u + theta * (u - u_prev)
     return x
+
+
+# ---------------------------------------------------------------------------
+# Projector type 4 (interpolation), PET and CT
+# ---------------------------------------------------------------------------
+
+def interp_forward(geom: Geometry, image, subset):
+    """FP64 type-4 forward projection (ray-marched trilinear samples) of one
+    subset; all TOF bins, bin-major."""
+    img = np.ascontiguousarray(image, dtype=np.float64).ravel()
+    g = geom.struct(subset)
+    y = np.zeros(geom.rays(subset) * geom.nbins, dtype=np.float64)
+    if lib().oracle_interp_fp(ctypes.byref(g), geom.dL, _dp(img), _dp(y)) != 0:
+        raise ValueError("oracle_interp_fp")
+    return y
+
+
+def interp_backward(geom: Geometry, y, subset, sens=False):
+    """FP64 type-4 PET backprojection (nearest voxel per sample); y=None
+    backprojects ones."""
+    g = geom.struct(subset)
+    img = np.zeros(geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    yy = None if y is None else np.ascontiguousarray(y, dtype=np.float64).ravel()
+    if lib().oracle_interp_bp(ctypes.byref(g), geom.dL, _dp(yy), _dp(img), _dp(s)) != 0:
+        raise ValueError("oracle_interp_bp")
+    return (img, s) if sens else img
+
+
+def interp_ct_backward(geom: Geometry, y, subset, sens=False):
+    """FP64 type-4 CT backprojection (voxel driven, bilinear detector samples)."""
+    yy = np.ascontiguousarray(y, dtype=np.float64).ravel()
+    g = _ct_struct(geom, subset)
+    img = np.zeros(geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    if lib().oracle_interp_ct_bp(ctypes.byref(g), geom.kerroin, _dp(yy), _dp(img), _dp(s)) != 0:
+        raise ValueError("oracle_interp_ct_bp")
+    return (img, s) if sens else img

@@ -26,25 +26,7 @@
 #include <stdint.h>
 #include <string.h>
 
-typedef struct oracle_geom {
-    int modality;            /* 0 PET sinogram, 1 CT panel */
-    int nx, ny, nz;
-    double dx, dy, dz, bx, by, bz;
-    int n_rows, n_cols;
-    int64_t proj0, n_proj, m_size;
-    int stype, n_subsets, cur_subset;
-    double pitch_x, pitch_y;
-    double global_factor, epps;
-    int nbins;
-    double sigma_x;
-    const double *tof_centers;
-    const float *xy;
-    const float *z;
-} oracle_geom;
-
-typedef struct { double x, y, z; } v3;
-
-static double sgn(double v) { return (double)((0.0 < v) - (v < 0.0)); }
+#include "oracle_common.h"
 
 static unsigned to_u_ceil(double v) {
     v = ceil(v);
@@ -66,43 +48,6 @@ static int perp_start(double b, double d, double dd, int n) {
     return t;
 }
 
-static void load_ray(const oracle_geom *g, int64_t r, v3 *s, v3 *d) {
-    int64_t ix, iy, iz;
-    if (g->stype == 0) {
-        int64_t nbin = (int64_t)g->n_rows * g->n_cols;
-        iz = r / nbin;
-        int64_t b = r - iz * nbin;
-        iy = b / g->n_rows;
-        ix = b - iy * g->n_rows;
-        iz += g->proj0;
-    } else {
-        int64_t S = g->n_subsets, nr = g->n_rows, nc = g->n_cols, x = r;
-        if (g->stype == 1) {
-            x = x * S + g->cur_subset; iy = x % nc; iz = x / (nr * nc); ix = (x / nc) % nr;
-        } else if (g->stype == 2) {
-            x = x * S + g->cur_subset; iz = x / (nr * nc); iy = (x / nr) % nc; ix = x % nr;
-        } else if (g->stype == 4) {
-            x = (x / nr) * nr * S + nr * g->cur_subset + x % nr; iz = x / (nr * nc); iy = (x / nr) % nc; ix = x % nr;
-        } else {
-            iy = x % nc; x = x / nc * S + g->cur_subset; iz = x / nr; ix = x % nr;
-        }
-    }
-    if (g->modality == 0) {
-        const float *q = g->xy + (ix + iy * g->n_rows) * 4;
-        s->x = q[0]; s->y = q[1]; s->z = g->z[iz * 2];
-        d->x = q[2]; d->y = q[3]; d->z = g->z[iz * 2 + 1];
-    } else {
-        const float *p = g->xy + iz * 6;
-        s->x = p[0]; s->y = p[1]; s->z = p[2];
-        d->x = p[3]; d->y = p[4]; d->z = p[5];
-        double ux = g->z[iz * 2], uy = g->z[iz * 2 + 1];
-        double ia = (double)ix - (double)g->n_rows / 2.0 + 0.5;
-        double ib = (double)iy - (double)g->n_cols / 2.0 + 0.5;
-        d->x += ia * ux;
-        d->y += ia * uy;
-        d->z += ib * g->pitch_y;
-    }
-}
 
 static void dgs(double tmin, double t_min, double tmax, double t_max, unsigned *vmin, unsigned *vmax, double *t0,
                 int *u, double diff, double b, double d, double s, unsigned n) {
@@ -182,28 +127,6 @@ static int pre3d(const oracle_geom *g, double mx, double my, double mz, v3 s, v3
     return 0;
 }
 
-#define MAXB 64
-
-static double tof_weights(const oracle_geom *g, double ddsign, double ele, double D, double *w) {
-    const double inv = 1.0 / g->sigma_x;
-    const double coef = 0.3989422804014327 * inv;
-    double dX = ele / 3.0, sdX = dX * ddsign, sum = 0.0;
-    for (int to = 0; to < g->nbins; ++to) {
-        double c = g->tof_centers[to], a, out;
-        a = (D - c) * inv;
-        out = coef * exp(-0.5 * a * a);
-        for (int tr = 1; tr < 3; ++tr) {
-            a = ((D - sdX * (double)tr) - c) * inv;
-            out += coef * exp(-0.5 * a * a) * 2.0;
-        }
-        a = ((D - ele * ddsign) - c) * inv;
-        out += coef * exp(-0.5 * a * a);
-        w[to] = out * dX;
-        sum += w[to];
-    }
-    if (sum < g->epps) sum = g->epps;
-    return sum;
-}
 
 /* Visitor: called per intersected voxel with the element length and the TOF weights. */
 typedef void (*visit_fn)(void *ctx, int64_t ind, double ele, const double *w, double tsum);

@@ -69,6 +69,12 @@ CONFIGS["ct_fine5"] = dict(CT=True, nRowsD=24, nColsD=20, nProjections=30, dPitc
                            SinM=np.zeros((24, 20, 30), dtype=np.float32))
 # TOF width so that the bins cover the FOV diagonal: 7 bins of 85 mm / (c/2) seconds
 CONFIGS["pet_mini_tof"]["TOF_width"] = 85.0 / (2.99792458e11 / 2.)
+# projector type 4 (interpolation): PET, PET with TOF, PET with a sampling
+# length of half a voxel and 3 subsets of type 1, CT
+CONFIGS["pet_mini4"] = dict(CONFIGS["pet_mini"], projector_type=4)
+CONFIGS["pet_mini4_tof"] = dict(CONFIGS["pet_mini_tof"], projector_type=4)
+CONFIGS["pet_half4"] = dict(CONFIGS["pet_mini"], projector_type=4, dL=0.5, subsets=3, subsetType=1)
+CONFIGS["ct_mini4"] = dict(CONFIGS["ct_mini"], projector_type=4, subsets=3)
 
 
 def apply(options, cfg):
