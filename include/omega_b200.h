@@ -183,6 +183,23 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
 int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream);
 
 /*
+ * One OSEM sub-iteration for a batch of n_frames images that share the
+ * geometry and the subset's sensitivity image `sens` (omb_sensitivity):
+ * for every frame f, fp = A_s x_f, r = y_f / (fp + epps) (NaN/Inf -> epps),
+ * x_f = x_f / sens * (A_s^T r + epps) -- the reference's per-timestep OSEM
+ * step (reconstructionAF.h:1089-1265 with computeForwardProject.h:4-101 and
+ * algorithms.h:12-15) for all frames with one forward and one backward
+ * launch (type 1 shares each ray walk between frames).  images: frame f at
+ * images + f * image_stride; y_subset: this subset's measurements of frame f
+ * at y_subset + f * y_stride; work_meas holds n_frames *
+ * omb_measurement_count(h, subset) floats, work_img n_frames * Nx*Ny*Nz.
+ * Projector types 1 and 4, PET.
+ */
+int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, float *images, int64_t image_stride,
+                           const float *y_subset, int64_t y_stride, const float *sens, float *work_meas,
+                           float *work_img, void *stream);
+
+/*
  * Total voxel intersections (sum over the subset's rays of the Siddon walk
  * length Np) written to *out_host; synchronises `stream`.  The
  * algorithmic-byte model of the projector roofline counts bytes per

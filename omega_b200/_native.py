@@ -81,7 +81,9 @@ class Tuning(ctypes.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_[1:]}
 
 
-# (name, restype, argtypes) of every exported entry point of include/omega_b200.h
+_v, _i32, _i64, _f = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+
+# (name, restype, argtypes) of every exported entry point of include/*.h
 EXPORTS = [
     ("omb_abi_version", ctypes.c_int, []),
     ("omb_last_error", ctypes.c_char_p, []),
@@ -99,6 +101,9 @@ EXPORTS = [
     ("omb_osem_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_sensitivity", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_osem_subset_frames", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                              ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_loglik", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                   ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_reduce_workspace_bytes", ctypes.c_size_t, [ctypes.c_int64]),
@@ -123,6 +128,22 @@ EXPORTS = [
                                     ctypes.c_void_p]),
     ("omb_intersection_count", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
                                               ctypes.c_void_p]),
+    # learned warm start (include/omega_b200_unet.h)
+    ("omb_unet_conv", ctypes.c_int, [_i32, _i32, _v, _v, _v, _v, _v, _i32, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_conv_wgrad", ctypes.c_int, [_i32, _i32, _v, _v, _v, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_bias_grad", ctypes.c_int, [_i32, _v, _v, _i64, _v]),
+    ("omb_unet_flip_weights", ctypes.c_int, [_v, _v, _i32, _i32, _v]),
+    ("omb_unet_avgpool", ctypes.c_int, [_v, _v, _i32, _i32, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_up_concat", ctypes.c_int, [_v, _v, _v, _i32, _i32, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_up_concat_bwd", ctypes.c_int, [_v, _v, _v, _i32, _i32, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_relu_mask", ctypes.c_int, [_v, _v, _i64, _v]),
+    ("omb_unet_make_input", ctypes.c_int, [_v, _i64, _v, _v, _f, _v, _i32, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_head_fwd", ctypes.c_int, [_v, _v, _v, _v, _v, _i64, _v]),
+    ("omb_unet_head_bwd", ctypes.c_int, [_v, _v, _v, _i64, _v, _v, _v, _v, _v, _v, _i32, _i32, _i32, _i32, _i32,
+                                         _v]),
+    ("omb_unet_head_out", ctypes.c_int, [_v, _v, _v, _i64, _f, _i32, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_adam", ctypes.c_int, [_v, _v, _v, _v, _v, _i64, _f, _f, _f, _i32, _f, _v]),
+    ("omb_unet_to_bf16", ctypes.c_int, [_v, _v, _i64, _v]),
 ]
 
 _lib = None

@@ -482,6 +482,47 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     return em_update(image, sens, work_img, h->n_img, eps, s);
 }
 
+int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, float *images, int64_t image_stride,
+                           const float *y_subset, int64_t y_stride, const float *sens, float *work_meas,
+                           float *work_img, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!images || !y_subset || !sens || !work_meas || !work_img)
+        return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osem_subset_frames");
+    if (n_frames < 0) return set_error(OMB_ERR_INVALID, "n_frames must be >= 0");
+    if (h->desc.modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
+    if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset_frames needs projector types 1 or 4");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    const int64_t m = rs.m_size * h->desc.tof_bins;
+    if (image_stride < h->n_img || y_stride < m)
+        return set_error(OMB_ERR_INVALID, "frame strides smaller than one image / one measurement vector");
+    if (n_frames == 0) return OMB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const float eps = h->desc.epps;
+    Frames f{};
+    f.n = n_frames;
+    f.img_in = images;
+    f.img_stride = image_stride;
+    f.meas_out = work_meas;
+    f.meas_stride = m;
+    st = rays_forward(h, rs, f, s);
+    if (st != OMB_OK) return st;
+    st = osem_ratio_frames(y_subset, y_stride, work_meas, m, m, n_frames, eps, s);
+    if (st != OMB_OK) return st;
+    OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, (size_t)n_frames * h->n_img * sizeof(float), s));
+    Frames b{};
+    b.n = n_frames;
+    b.meas = work_meas;
+    b.meas_stride = m;
+    b.img = work_img;
+    b.img_stride = h->n_img;
+    st = rays_backward(h, rs, b, nullptr, s);
+    if (st != OMB_OK) return st;
+    return em_update_frames(images, image_stride, sens, work_img, h->n_img, h->n_img, n_frames, eps, s);
+}
+
 int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, void *stream) {
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
     if (!out_host) return set_error(OMB_ERR_INVALID, "output pointer is NULL");

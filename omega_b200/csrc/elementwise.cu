@@ -46,7 +46,46 @@ __global__ void k_clamp_min(float *__restrict__ x, int64_t n, float lo) {
         if (x[i] < lo) x[i] = lo;
 }
 
+// Frame batches: blockIdx.y selects the frame.
+__global__ void k_osem_ratio_frames(const float *__restrict__ y, int64_t y_stride, float *__restrict__ fp,
+                                    int64_t fp_stride, int64_t n, float epps) {
+    const float *yf = y + blockIdx.y * y_stride;
+    float *ff = fp + blockIdx.y * fp_stride;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        ff[i] = ratio1(__ldg(yf + i), ff[i], epps);
+}
+
+__global__ void k_em_update_frames(float *__restrict__ img, int64_t img_stride, const float *__restrict__ sens,
+                                   const float *__restrict__ rhs, int64_t rhs_stride, int64_t n, float epps) {
+    float *xf = img + blockIdx.y * img_stride;
+    const float *rf = rhs + blockIdx.y * rhs_stride;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        xf[i] = xf[i] / __ldg(sens + i) * (__ldg(rf + i) + epps);
+}
+
 static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+int osem_ratio_frames(const float *y, int64_t y_stride, float *fp, int64_t fp_stride, int64_t n, int frames,
+                      float epps, cudaStream_t st) {
+    if (n <= 0 || frames <= 0) return OMB_OK;
+    if (frames > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 frames");
+    dim3 grid((grid_for(n, 4) + frames - 1) / frames + 1, frames);
+    k_osem_ratio_frames<<<grid, kBlock, 0, st>>>(y, y_stride, fp, fp_stride, n, epps);
+    OMB_LAUNCH_CHECK("osem ratio launch");
+    return OMB_OK;
+}
+
+int em_update_frames(float *img, int64_t img_stride, const float *sens, const float *rhs, int64_t rhs_stride,
+                     int64_t n, int frames, float epps, cudaStream_t st) {
+    if (n <= 0 || frames <= 0) return OMB_OK;
+    if (frames > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 frames");
+    dim3 grid((grid_for(n, 4) + frames - 1) / frames + 1, frames);
+    k_em_update_frames<<<grid, kBlock, 0, st>>>(img, img_stride, sens, rhs, rhs_stride, n, epps);
+    OMB_LAUNCH_CHECK("EM update launch");
+    return OMB_OK;
+}
 
 int osem_ratio(const float *y, float *fp, int64_t n, float epps, cudaStream_t st) {
     if (n <= 0) return OMB_OK;

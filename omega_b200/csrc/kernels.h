@@ -41,6 +41,10 @@ int normalize_into(float *x, const float *b, int64_t n, const double *dots, cuda
 int osem_ratio(const float *y, float *fp, int64_t n, float epps, cudaStream_t st);
 int em_update(float *img, const float *sens, const float *rhs, int64_t n, float epps, cudaStream_t st);
 int clamp_min(float *x, int64_t n, float lo, cudaStream_t st);
+int osem_ratio_frames(const float *y, int64_t y_stride, float *fp, int64_t fp_stride, int64_t n, int frames,
+                      float epps, cudaStream_t st);
+int em_update_frames(float *img, int64_t img_stride, const float *sens, const float *rhs, int64_t rhs_stride,
+                     int64_t n, int frames, float epps, cudaStream_t st);
 size_t reduce_workspace_bytes(int64_t n);
 int loglik(const float *y, const float *fp, int64_t n, float epps, double *out_host, void *work,
            cudaStream_t st);

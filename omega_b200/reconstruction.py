@@ -158,3 +158,68 @@ class OSEM:
         for _ in range(n_iter):
             self.graph.replay()
         return self.x
+
+
+class OSEMBatch:
+    """OSEM for a batch of studies (or frames) that share one PET geometry:
+    every sub-iteration is one omb_osem_subset_frames call, i.e. one forward
+    and one backward launch for the whole batch.  `m`: (F, nTotMeas)
+    measurements in subset order (host array or CUDA tensor); `x0`: (F, N)
+    or one image broadcast to all F."""
+
+    def __init__(self, options, m, x0=None):
+        import torch
+        options._check_ready()
+        self.o = options
+        self.dev = torch.device("cuda", options._device)
+        n = int(options.N[0])
+        S = int(options.subsets)
+        M = options.measurementCount(-1)
+        m = torch.as_tensor(m, dtype=torch.float32)
+        if m.dim() != 2 or m.shape[1] != M:
+            raise ValueError(f"measurements must be (frames, {M})")
+        self.F = int(m.shape[0])
+        self.y = m.to(self.dev).contiguous()
+        if x0 is None:
+            x0 = np.asarray(options.x0, dtype=np.float32).ravel()
+        x0 = torch.as_tensor(np.asarray(x0, dtype=np.float32) if not torch.is_tensor(x0) else x0,
+                             dtype=torch.float32).to(self.dev)
+        self.x = (x0.reshape(1, n).expand(self.F, n) if x0.numel() == n else x0.reshape(self.F, n)).contiguous()
+        self.offsets = [int(v) for v in np.asarray(options.nTotMeas).ravel()]
+        self.sens = [torch.empty(n, device=self.dev) for _ in range(S)]
+        for s in range(S):
+            _native.call("omb_sensitivity", options._handle, s, _ptr(self.sens[s]), _stream(self.dev))
+        mmax = max(options.measurementCount(s) for s in range(S))
+        self.wm = torch.empty(self.F * mmax, device=self.dev)
+        self.wi = torch.empty(self.F * n, device=self.dev)
+        self.graph = None
+
+    def _iteration(self):
+        st = _stream(self.dev)
+        n = int(self.o.N[0])
+        M = self.y.shape[1]
+        base = self.y.data_ptr()
+        for s in range(int(self.o.subsets)):
+            _native.call("omb_osem_subset_frames", self.o._handle, s, self.F, _ptr(self.x), n,
+                         ctypes.c_void_p(base + 4 * self.offsets[s]), M, _ptr(self.sens[s]), _ptr(self.wm),
+                         _ptr(self.wi), st)
+
+    def iterate(self, n_iter, use_graph=False):
+        import torch
+        if not use_graph or (self.graph is None and n_iter < 1):
+            for _ in range(n_iter):
+                self._iteration()
+            return self.x
+        if self.graph is None:
+            s = torch.cuda.Stream(self.dev)
+            s.wait_stream(torch.cuda.current_stream(self.dev))
+            with torch.cuda.stream(s):
+                self._iteration()
+            torch.cuda.current_stream(self.dev).wait_stream(s)
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph):
+                self._iteration()
+            n_iter -= 1
+        for _ in range(n_iter):
+            self.graph.replay()
+        return self.x

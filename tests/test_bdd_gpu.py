@@ -152,3 +152,21 @@ def test_osem_graph_replay_matches_eager(cuda):
     ys = [m[int(o.nTotMeas[s]):int(o.nTotMeas[s + 1])] for s in range(g.n_subsets)]
     ref = orc.osem(g, ys, np.ones(g.n_img), 3)
     assert orc.rel_l2(a, ref) < 5e-5
+
+
+def test_osem_batch_equals_per_frame_osem(cuda):
+    """omb_osem_subset_frames: three studies in one batch give each study's
+    own OSEM result."""
+    from omega_b200 import reconstruction as rec
+    o = _init("pet_mini")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(8)
+    ms = []
+    for f in range(3):
+        truth = rng.uniform(0.5, 2.0, g.n_img)
+        ms.append(np.concatenate([rng.poisson(orc.forward(g, truth, s) * 10.0) for s in range(g.n_subsets)]))
+    m = np.stack(ms).astype(np.float32)
+    xb = rec.OSEMBatch(o, m).iterate(3, use_graph=True).cpu().numpy()
+    for f in range(3):
+        x1 = rec.OSEM(o, m[f]).iterate(3).cpu().numpy()
+        assert orc.rel_l2(xb[f], x1) < 1e-6, f
