@@ -51,6 +51,11 @@ typedef enum omb_modality {
     OMB_CT_PANEL = 1      /* CT flat panel: xy = nProj x [sx, sy, sz, dx, dy, dz]; z = nProj x [ux*pitchX, uy*pitchX] */
 } omb_modality;
 
+typedef enum omb_read_precision {
+    OMB_READ_FP32 = 0, /* forward projections read the FP32 image (default) */
+    OMB_READ_BF16 = 1  /* forward projections read a BF16 rounding of it; accumulation stays FP32 */
+} omb_read_precision;
+
 typedef enum omb_bp_mode {
     OMB_BP_FLOAT_ATOMIC = 0, /* float32 atomics (the reference's CUDA path) */
     OMB_BP_FIXED64 = 1       /* int64 fixed point, bit-identical run to run (the reference's OpenCL -DATOMIC path) */
@@ -223,6 +228,19 @@ typedef struct omb_tuning {
     int32_t bdd_fp_columns;          /* 8, 16 (default 8): type-5 forward, detector columns per thread */
     int32_t bdd_bp_zrun;             /* 4, 8, 16 (default 8): type-5 backward, voxels along z per thread */
 } omb_tuning;
+
+/*
+ * Image read precision of the forward projections of types 1 and 4
+ * (omb_read_precision).  With OMB_READ_BF16 every forward call first rounds
+ * its images to BF16 (round to nearest even) into copies owned by the handle
+ * and the kernels read those: half the image bytes per sample, FP32
+ * accumulation; the relative L2 error against the FP64 oracle is stated per
+ * projector by the tests (below 4e-3).  max_frames: the most images one
+ * forward call may carry; the copies are allocated here, not during a
+ * forward call.  No counterpart in the reference (its images are FP32
+ * textures).
+ */
+int omb_set_read_precision(omb_handle *h, int32_t mode, int32_t max_frames);
 
 int omb_get_tuning(const omb_handle *h, omb_tuning *out);
 int omb_set_tuning(omb_handle *h, const omb_tuning *in);

@@ -17,6 +17,8 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libo
 OMB_ABI_VERSION = 1
 OMB_PET_SINOGRAM = 0
 OMB_CT_PANEL = 1
+OMB_READ_FP32 = 0
+OMB_READ_BF16 = 1
 OMB_BP_FLOAT_ATOMIC = 0
 OMB_BP_FIXED64 = 1
 
@@ -122,6 +124,7 @@ EXPORTS = [
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                         ctypes.c_void_p]),
     ("omb_power_workspace_bytes", ctypes.c_size_t, []),
+    ("omb_set_read_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     ("omb_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
     ("omb_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
     ("omb_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Tuning),

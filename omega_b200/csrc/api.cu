@@ -40,6 +40,9 @@ struct omb_handle {
     BddProj *d_bddp = nullptr;            // per-projection maps (type-5 backprojection)
     int64_t n_img = 0;
     Tuning tune{};
+    int read_mode = OMB_READ_FP32;        // image precision of the type-1/4 forward projections
+    __nv_bfloat16 *d_img16 = nullptr;     // BF16 image copies (read_mode == OMB_READ_BF16)
+    int img16_frames = 0;                 // frames d_img16 holds
 };
 
 // Type-5 backprojection maps of every projection, FP64 on the host from the
@@ -202,12 +205,26 @@ static Frames one_frame_bp(const omb_handle *h, const float *y, float *img, int6
     return f;
 }
 
-// Ray-driven forward projection of a batch of frames (types 1 and 4).
-static int rays_forward(const omb_handle *h, const RaySet &rs, const Frames &f, cudaStream_t s) {
+// Ray-driven forward projection of a batch of frames (types 1 and 4).  With
+// BF16 reads the images are first rounded into the handle's BF16 copies.
+static int rays_forward(const omb_handle *h, const RaySet &rs, const Frames &f_in, cudaStream_t s) {
+    Frames f = f_in;
+    if (h->read_mode == OMB_READ_BF16 && f.n > 0) {
+        if (f.n > h->img16_frames)
+            return set_error(OMB_ERR_INVALID, "more frames than omb_set_read_precision reserved BF16 copies for");
+        for (int fr = 0; fr < f.n; ++fr) {
+            const int st = unet_to_bf16(f.img_in + fr * f.img_stride, h->d_img16 + fr * h->n_img, h->n_img, s);
+            if (st != OMB_OK) return st;
+        }
+        f.img_in16 = h->d_img16;
+        f.img_stride = h->n_img;
+    }
     if (h->desc.fp_type == 4) {
         for (int fr = 0; fr < f.n; ++fr) {
             const int st = interp_forward(h->grid, rs, h->tof, h->desc.global_factor, h->desc.dL,
-                                          f.img_in + fr * f.img_stride, f.meas_out + fr * f.meas_stride, h->tune, s);
+                                          f.img_in16 ? nullptr : f.img_in + fr * f.img_stride,
+                                          f.img_in16 ? f.img_in16 + fr * f.img_stride : nullptr,
+                                          f.meas_out + fr * f.meas_stride, h->tune, s);
             if (st != OMB_OK) return st;
         }
         return OMB_OK;
@@ -313,6 +330,7 @@ int omb_destroy(omb_handle *h) {
     cudaFree(h->d_acc);
     cudaFree(h->d_imgT);
     cudaFree(h->d_bddp);
+    cudaFree(h->d_img16);
     if (prev != h->device) cudaSetDevice(prev);
     delete h;
     return OMB_OK;
@@ -595,6 +613,24 @@ int omb_set_tuning(omb_handle *h, const omb_tuning *in) {
     int st = tuning_from(in, t);
     if (st == OMB_OK) h->tune = t;
     return st;
+}
+
+int omb_set_read_precision(omb_handle *h, int32_t mode, int32_t max_frames) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (mode != OMB_READ_FP32 && mode != OMB_READ_BF16) return set_error(OMB_ERR_INVALID, "unknown read precision");
+    if (mode == OMB_READ_BF16 && h->desc.fp_type != 1 && h->desc.fp_type != 4)
+        return set_error(OMB_ERR_UNSUPPORTED, "BF16 image reads are built for forward projector types 1 and 4");
+    if (mode == OMB_READ_BF16 && max_frames < 1) return set_error(OMB_ERR_INVALID, "max_frames must be >= 1");
+    if (mode == OMB_READ_BF16 && max_frames > h->img16_frames) {
+        __nv_bfloat16 *p = nullptr;
+        const cudaError_t e = cudaMalloc(&p, (size_t)max_frames * h->n_img * sizeof(__nv_bfloat16));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc BF16 image copies");
+        cudaFree(h->d_img16);
+        h->d_img16 = p;
+        h->img16_frames = max_frames;
+    }
+    h->read_mode = mode;
+    return OMB_OK;
 }
 
 int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *out, void *stream) {

@@ -1,6 +1,7 @@
 // Shared host/device definitions of the omega_b200 projector library.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -60,6 +61,7 @@ struct RaySet {
 struct Frames {
     int n;
     const float *img_in;   // forward: input images
+    const __nv_bfloat16 *img_in16;  // forward: BF16 copies of the images (read instead of img_in when set)
     float *img;            // backward: output images
     int64_t img_stride;
     const float *meas;     // backward: input measurements
@@ -97,6 +99,10 @@ struct Tuning {
     int bdd_fp_cols = 8;            // type-5 forward: detector columns per thread (8, 16)
     int bdd_bp_z = 8;               // type-5 backward: voxels along z per thread (4, 8, 16)
 };
+
+// Read-only image load as float from an FP32 or BF16 array.
+__device__ __forceinline__ float ld_img(const float *p) { return __ldg(p); }
+__device__ __forceinline__ float ld_img(const __nv_bfloat16 *p) { return __bfloat162float(__ldg(p)); }
 
 constexpr int kMaxTofBins = 16;
 // Fixed-point scale of the int64 backprojection mode (the reference's TH).

@@ -94,7 +94,8 @@ __device__ __forceinline__ unsigned voxel_of(double p) {
 
 // Trilinear interpolation with clamp-to-edge addressing; (x, y, z) are texel
 // coordinates (voxel centres at integers).
-__device__ __forceinline__ float trilinear(const float *__restrict__ img, const Grid &g, float x, float y, float z) {
+template <typename T>
+__device__ __forceinline__ float trilinear(const T *__restrict__ img, const Grid &g, float x, float y, float z) {
     x = fminf(fmaxf(x, -1.f), (float)g.nx);
     y = fminf(fmaxf(y, -1.f), (float)g.ny);
     z = fminf(fmaxf(z, -1.f), (float)g.nz);
@@ -105,19 +106,19 @@ __device__ __forceinline__ float trilinear(const float *__restrict__ img, const 
     const int64_t nxy = (int64_t)g.nx * g.ny;
     const int64_t y0 = (int64_t)min(max(iy, 0), g.ny - 1) * g.nx, y1 = (int64_t)min(max(iy + 1, 0), g.ny - 1) * g.nx;
     const int64_t z0 = (int64_t)min(max(iz, 0), g.nz - 1) * nxy, z1 = (int64_t)min(max(iz + 1, 0), g.nz - 1) * nxy;
-    const float v000 = __ldg(img + x0 + y0 + z0), v100 = __ldg(img + x1 + y0 + z0);
-    const float v010 = __ldg(img + x0 + y1 + z0), v110 = __ldg(img + x1 + y1 + z0);
-    const float v001 = __ldg(img + x0 + y0 + z1), v101 = __ldg(img + x1 + y0 + z1);
-    const float v011 = __ldg(img + x0 + y1 + z1), v111 = __ldg(img + x1 + y1 + z1);
+    const float v000 = ld_img(img + x0 + y0 + z0), v100 = ld_img(img + x1 + y0 + z0);
+    const float v010 = ld_img(img + x0 + y1 + z0), v110 = ld_img(img + x1 + y1 + z0);
+    const float v001 = ld_img(img + x0 + y0 + z1), v101 = ld_img(img + x1 + y0 + z1);
+    const float v011 = ld_img(img + x0 + y1 + z1), v111 = ld_img(img + x1 + y1 + z1);
     const float c00 = fmaf(ax, v100 - v000, v000), c10 = fmaf(ax, v110 - v010, v010);
     const float c01 = fmaf(ax, v101 - v001, v001), c11 = fmaf(ax, v111 - v011, v011);
     const float c0 = fmaf(ay, c10 - c00, c00), c1 = fmaf(ay, c11 - c01, c01);
     return fmaf(az, c1 - c0, c0);
 }
 
-template <int NB>
-__global__ void k_interp_fp(Grid g, RaySet rs, Tof tof, float gf, float dL,
-                                                      const float *__restrict__ img, float *__restrict__ y) {
+template <int NB, typename T>
+__global__ void k_interp_fp(Grid g, RaySet rs, Tof tof, float gf, float dL, const T *__restrict__ img,
+                            float *__restrict__ y) {
     const bool pet = rs.modality == OMB_PET_SINOGRAM;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
@@ -308,12 +309,18 @@ __global__ void k_interp_ct_bp(Grid g, const BddProj *__restrict__ pj, int nr, i
 #define OMB_NB_CASES(X) \
     X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 
-int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img, float *y,
-                   const Tuning &tn, cudaStream_t st) {
+int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img,
+                   const __nv_bfloat16 *img16, float *y, const Tuning &tn, cudaStream_t st) {
     if (rs.m_size <= 0) return OMB_OK;
     const unsigned grid = grid_for(rs.m_size, tn.siddon_blocks_per_sm);
     switch (tof.nbins) {
-#define X(n) case n: k_interp_fp<n><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, dL, img, y); break;
+#define X(n)                                                                                    \
+    case n:                                                                                     \
+        if (img16)                                                                              \
+            k_interp_fp<n, __nv_bfloat16><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, dL, img16, y);  \
+        else                                                                                    \
+            k_interp_fp<n, float><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, dL, img, y);            \
+        break;
         OMB_NB_CASES(X)
 #undef X
         default:

@@ -21,8 +21,10 @@ int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj
                  float *sens, int zrun, cudaStream_t st);
 
 // Projector type 4 (interpolation), PET and CT.
-int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img, float *y,
-                   const Tuning &tn, cudaStream_t st);
+int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img,
+                   const __nv_bfloat16 *img16, float *y, const Tuning &tn, cudaStream_t st);
+// BF16 copy of n floats (also the network's weight conversion).
+int unet_to_bf16(const float *a, void *b, int64_t n, cudaStream_t st);
 int interp_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *y, float *img,
                     float *sens, unsigned long long *acc, unsigned long long *acc_s, const Tuning &tn,
                     cudaStream_t st);

@@ -16,9 +16,9 @@ namespace omb {
 // Forward projection.  Each thread walks one ray once and accumulates it for
 // FB frames of a dynamic study (blockIdx.y selects the group of frames), so
 // the traversal cost is shared by up to FB images.
-template <int NB, int FB>
+template <int NB, int FB, typename T>
 __global__ void __launch_bounds__(kBlock) k_siddon_fp(Grid g, RaySet rs, Tof tof, float gf,
-                                                      const float *__restrict__ img, int64_t img_stride,
+                                                      const T *__restrict__ img, int64_t img_stride,
                                                       float *__restrict__ y, int64_t y_stride, int n_frames) {
     const bool pet = rs.modality == OMB_PET_SINOGRAM;
     const int f0 = blockIdx.y * FB;
@@ -37,9 +37,9 @@ __global__ void __launch_bounds__(kBlock) k_siddon_fp(Grid g, RaySet rs, Tof tof
                                             if (NB == 1) {
 #pragma unroll
                                                 for (int f = 0; f < FB; ++f)
-                                                    if (f < nf) ax[f] += ele * __ldg(img + f * img_stride + ind);
+                                                    if (f < nf) ax[f] += ele * ld_img(img + f * img_stride + ind);
                                             } else {
-                                                const float dX = ele * __ldg(img + ind) / tsum;
+                                                const float dX = ele * ld_img(img + ind) / tsum;
 #pragma unroll
                                                 for (int to = 0; to < NB; ++to) ax[to] += w[to] * dX;
                                             }
@@ -206,8 +206,12 @@ template <int NB, int FB>
 static void fp_launch(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const Frames &fr, int per_sm,
                       cudaStream_t st) {
     dim3 grid(grid_for(rs.m_size, per_sm), (fr.n + FB - 1) / FB);
-    k_siddon_fp<NB, FB><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, fr.img_in, fr.img_stride, fr.meas_out,
-                                                  fr.meas_stride, fr.n);
+    if (fr.img_in16)
+        k_siddon_fp<NB, FB, __nv_bfloat16><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, fr.img_in16, fr.img_stride,
+                                                                    fr.meas_out, fr.meas_stride, fr.n);
+    else
+        k_siddon_fp<NB, FB, float><<<grid, kBlock, 0, st>>>(g, rs, tof, gf, fr.img_in, fr.img_stride, fr.meas_out,
+                                                            fr.meas_stride, fr.n);
 }
 
 template <int NB, int FB>

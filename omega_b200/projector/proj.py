@@ -117,6 +117,10 @@ class projectorClass:
     n_rays_transaxial = 1
     n_rays_axial = 1
     dL = 0
+    # forward-projection image reads: 'fp32' (default) or 'bf16' (types 1 and
+    # 4; FP32 accumulation), with BF16 copies reserved for maxFramesBF16 images
+    imageReadPrecision = 'fp32'
+    maxFramesBF16 = 1
     # projector scales (coordinates.py:209-269 fills those of the chosen type)
     dScaleX4 = np.empty(0, dtype=np.float32)
     dScaleY4 = np.empty(0, dtype=np.float32)
@@ -493,6 +497,10 @@ class projectorClass:
             _native.lib().omb_destroy(self._handle)
         self._handle = h
         self._device = torch.cuda.current_device()
+        if self.imageReadPrecision not in ('fp32', 'bf16'):
+            raise ValueError("imageReadPrecision must be 'fp32' or 'bf16'")
+        if self.imageReadPrecision == 'bf16':
+            _native.call("omb_set_read_precision", h, _native.OMB_READ_BF16, int(self.maxFramesBF16))
         del keep
 
     def _parse_inputs(self):

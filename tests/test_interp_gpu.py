@@ -114,3 +114,18 @@ def test_interp_osem_matches_oracle(cuda):
     ref = orc.osem(g, ys, np.ones(g.n_img), 2, forward=orc.interp_forward,
                    backward=lambda gg, yy, ss, sens=False: orc.interp_backward(gg, yy, ss, sens=sens))
     assert orc.rel_l2(x, ref) < 5e-5
+
+
+@pytest.mark.parametrize("name", ["pet_mini4", "pet_mini4_tof", "ct_mini4", "pet_mini"])
+def test_bf16_image_reads_error_is_stated(cuda, name):
+    """BF16 image reads (FP32 accumulation): the relative L2 error against the
+    FP64 oracle stays below 4e-3 (BF16 keeps 8 significant bits; the sums
+    average the per-voxel rounding) and is not zero (the BF16 path ran)."""
+    o = _init(name, imageReadPrecision="bf16", maxFramesBF16=2)
+    g = orc.Geometry(o)
+    x = _image(g, 11)
+    fwd = orc.interp_forward if int(o.projector_type) == 4 else orc.forward
+    for s in range(g.n_subsets):
+        y = o.forwardProject(_t(x, cuda), s).cpu().numpy()
+        err = orc.rel_l2(y, fwd(g, x, s))
+        assert 1e-6 < err < 4e-3, (s, err)
