@@ -59,7 +59,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="cbct", choices=["cbct", "cbct_small", "dynpet", "dynpet_small"])
+    p.add_argument("--workload", default="cbct",
+                   choices=["cbct", "cbct_small", "dynpet", "dynpet_small", "fanbeam64", "fanbeam64_small"])
     p.add_argument("--frames", type=int, default=None)
     p.add_argument("--views", type=int, default=None,
                    help="cbct: number of projections (fewer than 360 only for short profiling captures)")
@@ -616,6 +617,126 @@ def run_dynpet(args, rank, world, dev):
 
 
 # ---------------------------------------------------------------------------
+# our arm: 64 fan-beam CT slices of uneven sizes, one persistent launch per
+# direction (omb_batch_forward / omb_batch_backward)
+# ---------------------------------------------------------------------------
+
+def fanbeam_items(small=False, seed=64):
+    """Seeded slice sizes: n x n images, n in 128..512 (multiples of 16),
+    180-720 views, ceil(1.5 n) detectors per view."""
+    from omega_b200.projector.batch import fanbeam_slice
+    rng = np.random.default_rng(seed)
+    count = 8 if small else 64
+    sizes = [(16 * int(rng.integers(8, 33)), int(rng.integers(180, 721))) for _ in range(count)]
+    return [fanbeam_slice(n, v) for n, v in sizes], sizes
+
+
+def run_fanbeam(args, rank, world, dev):
+    import torch
+    from omega_b200 import _native
+    from omega_b200.projector.batch import ProjectorBatch
+    small = args.workload == "fanbeam64_small"
+    items, sizes = fanbeam_items(small)
+    batch = ProjectorBatch(items)
+    nimg, nmeas = int(batch.image_offsets[-1]), int(batch.measurement_offsets[-1])
+    rng = np.random.default_rng(5)
+    x_host = rng.uniform(0.0, 1.0, nimg).astype(np.float32)
+    x = torch.from_numpy(x_host).to(dev)
+    y = torch.empty(nmeas, device=dev)
+    back = torch.empty(nimg, device=dev)
+    sp = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def step(tm):
+        tm.mark()
+        _native.call("omb_batch_forward", batch._handle, P(x), P(y), sp)
+        tm.mark()
+        _native.call("omb_batch_backward", batch._handle, P(y), P(back), sp)
+        tm.mark()
+
+    tot, clk, wall = run_timed(args, world, dev, step, 2)
+    t_fp, t_bp = tot
+    total = t_fp + t_bp
+    K = args.steps
+    # the same work with one launch pair per slice (separate handles)
+    for o in items:
+        o.initProj()
+    npx = 0
+    for o in items:
+        c = ctypes.c_int64()
+        _native.call("omb_intersection_count", o._handle, -1, ctypes.byref(c), sp)
+        npx += c.value
+    xs = [x[int(batch.image_offsets[i]):int(batch.image_offsets[i + 1])] for i in range(len(items))]
+    ys = [y[int(batch.measurement_offsets[i]):int(batch.measurement_offsets[i + 1])] for i in range(len(items))]
+    bs = [back[int(batch.image_offsets[i]):int(batch.image_offsets[i + 1])] for i in range(len(items))]
+
+    def step_single(tm):
+        tm.mark()
+        for o, xi, yi in zip(items, xs, ys):
+            _native.call("omb_forward", o._handle, -1, P(xi), P(yi), sp)
+        tm.mark()
+        for o, yi, bi in zip(items, ys, bs):
+            _native.call("omb_backward", o._handle, -1, P(yi), P(bi), None, 0, sp)
+        tm.mark()
+
+    single, _, _ = run_timed(args, world, dev, step_single, 2)
+    h_in = torch.from_numpy(x_host).pin_memory()
+    h_out = torch.empty(nimg, dtype=torch.float32).pin_memory()
+
+    def step_host():
+        x.copy_(h_in, non_blocking=True)
+        _native.call("omb_batch_forward", batch._handle, P(x), P(y), sp)
+        _native.call("omb_batch_backward", batch._handle, P(y), P(back), sp)
+        h_out.copy_(back, non_blocking=True)
+
+    e2e_total = e2e_time(args, world, dev, step_host)
+    if rank != 0:
+        return None
+    mean_fp, mean_bp = t_fp / K, t_bp / K
+    fp_bytes = 4 * npx + 32 * nmeas
+    bp_bytes = 8 * npx + 28 * nmeas
+    if mean_bp >= mean_fp:
+        rl = roofline("batch_siddon_bp", bp_bytes, mean_bp, (args.workload, "bp"))
+    else:
+        rl = roofline("batch_siddon_fp", fp_bytes, mean_fp, (args.workload, "fp"))
+    line = {
+        "metric": "proj+backproj rays/s", "value": nmeas * K * world / total, "unit": "rays/s", "n_gpus": world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * total / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform random images)",
+        "config": {"workload": f"{len(items)} 2-D fan-beam CT slices of uneven sizes (n x n images, n 128-512; "
+                               "180-720 views; ceil(1.5 n) detectors), improved Siddon, one persistent launch per "
+                               "direction", "slices": len(items), "rays_per_step": nmeas, "voxels": nimg,
+                   "intersections": npx, "sizes": sizes, "parallelism": f"replicas x{world}",
+                   "l2": "256 MB L2 flush between steps"},
+        "fp_ms": 1e3 * mean_fp, "bp_ms": 1e3 * mean_bp,
+        "per_slice_launches_ms": 1e3 * sum(single) / K,
+        "roofline": rl,
+        "e2e": {"value": nmeas * K * world / e2e_total, "unit": "rays/s", "h2d_bytes_per_step": nimg * 4,
+                "d2h_bytes_per_step": nimg * 4},
+        "gpu_launches": 2 * K, "clocks": clk, "wall_s": wall,
+    }
+    if not args.no_baseline and world == 1:
+        try:
+            from oracle import oracle as orc
+            g = orc.Geometry(items[0])
+            xi = x_host[:int(batch.image_offsets[1])]
+            done, t0 = 0, time.perf_counter()
+            while time.perf_counter() - t0 < 10.0:
+                orc.backward(g, orc.forward(g, xi, -1), -1)
+                done += g.rays(-1)
+            el = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": done / el, "unit": "rays/s", "cores": 1, "kind": "port",
+                                    "sample": f"slice 0 ({sizes[0][0]}^2 image, {sizes[0][1]} views) FP+BP pairs for "
+                                              f"{el:.1f} s; FP64 restatement of the type-1 projector (the reference's "
+                                              f"CPU projector build here is PET-only); host CPU {cpu_model()}"}
+        except Exception as e:
+            line["cpu_baseline"] = {"error": str(e)}
+    return line
+
+
+# ---------------------------------------------------------------------------
 # reference arm: the CPU implementation of the same step on a bounded sample
 # ---------------------------------------------------------------------------
 
@@ -638,6 +759,20 @@ def run_reference(args):
         sample = (f"4 of {int(o.nProjections)} projections ({rays} rays) per step; FP64 OpenMP restatement of the "
                   "type-5 pair (the reference has no CPU type-5 projector)")
         workload = "cone-beam CT (same geometry as ours), FP+BP pair over a bounded sample of projections"
+    elif args.workload.startswith("fanbeam"):
+        items, sizes = fanbeam_items(args.workload == "fanbeam64_small")
+        g = orc.Geometry(items[0])
+        img = np.random.default_rng(5).uniform(0.0, 1.0, g.n_img)
+        rays = g.rays(-1)
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            orc.backward(g, orc.forward(g, img, -1), -1)
+            if it >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        kind, cores = "port", 1
+        sample = (f"slice 0 ({sizes[0][0]}^2 image, {sizes[0][1]} views, {rays} rays) per step; FP64 restatement of "
+                  "the type-1 projector (the reference's CPU projector build here is PET-only)")
+        workload = "64 fan-beam CT slices (same sizes as ours), FP+BP pair over slice 0"
     else:
         o = dynamic_pet_options(args.workload == "dynpet_small")
         img = dynamic_images(o, 1)[0]
@@ -687,7 +822,8 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-    run = run_cbct if args.workload.startswith("cbct") else run_dynpet
+    run = run_cbct if args.workload.startswith("cbct") else (
+        run_fanbeam if args.workload.startswith("fanbeam") else run_dynpet)
     line = run(args, rank, world, dev)
     if world > 1:
         import torch.distributed as dist

@@ -337,6 +337,27 @@ size_t omb_reduce_workspace_bytes(int64_t n);
 int omb_backward_fixed64_noalloc(const omb_geometry_desc *desc, int32_t subset, const float *y, float *image,
                                  float *sens, void *stream);
 
+/*
+ * Batches of independent CT reconstructions -- e.g. 2-D fan-beam slices of
+ * different image sizes and view counts -- projected by ONE persistent
+ * launch per direction instead of one launch per item.  Every item is a CT
+ * geometry with projector type 1 and no TOF; all of its projections are
+ * projected (subset order).  Images of all items are concatenated in one
+ * float buffer (item i starts at omb_batch_image_offset(b, i)), measurements
+ * likewise (omb_batch_measurement_offset); offset n is the total.  The
+ * reference launches one kernel per reconstruction object (projfunctions.py:
+ * 86, 735); this has no counterpart there.
+ */
+typedef struct omb_batch omb_batch;
+int omb_batch_create(const omb_geometry_desc *descs, int32_t n, omb_batch **out);
+int omb_batch_destroy(omb_batch *b);
+int64_t omb_batch_image_offset(const omb_batch *b, int32_t item);
+int64_t omb_batch_measurement_offset(const omb_batch *b, int32_t item);
+/* y = A images for every item (y overwritten). */
+int omb_batch_forward(omb_batch *b, const float *images, float *y, void *stream);
+/* images = A^T y for every item (images overwritten). */
+int omb_batch_backward(omb_batch *b, const float *y, float *images, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -131,6 +131,12 @@ EXPORTS = [
                                     ctypes.c_void_p]),
     ("omb_intersection_count", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
                                               ctypes.c_void_p]),
+    ("omb_batch_create", ctypes.c_int, [ctypes.POINTER(GeometryDesc), ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    ("omb_batch_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("omb_batch_image_offset", ctypes.c_int64, [ctypes.c_void_p, ctypes.c_int32]),
+    ("omb_batch_measurement_offset", ctypes.c_int64, [ctypes.c_void_p, ctypes.c_int32]),
+    ("omb_batch_forward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_batch_backward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     # learned warm start (include/omega_b200_unet.h)
     ("omb_unet_conv", ctypes.c_int, [_i32, _i32, _v, _v, _v, _v, _v, _i32, _i32, _i32, _i32, _i32, _v]),
     ("omb_unet_conv_wgrad", ctypes.c_int, [_i32, _i32, _v, _v, _v, _i32, _i32, _i32, _i32, _v]),

@@ -1,5 +1,6 @@
 // C-ABI entry points (include/omega_b200.h): handle life cycle, argument
 // validation and dispatch to the projector kernels.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -814,5 +815,150 @@ int omb_loglik(const float *y, const float *fp, int64_t n, float epps, double *o
 }
 
 size_t omb_reduce_workspace_bytes(int64_t n) { return reduce_workspace_bytes(n); }
+
+
+// ---------------------------------------------------------------------------
+// Batches of independent CT geometries (one persistent launch per direction)
+// ---------------------------------------------------------------------------
+
+struct omb_batch {
+    int device = 0;
+    int n = 0;
+    std::vector<int64_t> img_off, meas_off;  // n + 1 cumulative offsets
+    float *d_geom = nullptr;                 // all items' xy and z arrays
+    BatchItem *d_items = nullptr;
+    int2 *d_work = nullptr;
+    int n_work = 0;
+    int *d_counter = nullptr;
+};
+
+int omb_batch_destroy(omb_batch *b) {
+    if (!b) return OMB_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != b->device) cudaSetDevice(b->device);
+    cudaFree(b->d_geom);
+    cudaFree(b->d_items);
+    cudaFree(b->d_work);
+    cudaFree(b->d_counter);
+    if (prev != b->device) cudaSetDevice(prev);
+    delete b;
+    return OMB_OK;
+}
+
+int omb_batch_create(const omb_geometry_desc *descs, int32_t n, omb_batch **out) {
+    if (!out) return set_error(OMB_ERR_INVALID, "output batch pointer is NULL");
+    *out = nullptr;
+    if (!descs || n < 1) return set_error(OMB_ERR_INVALID, "a batch needs at least one geometry");
+    for (int i = 0; i < n; ++i) {
+        const int st = validate(descs + i);
+        if (st != OMB_OK) return set_error(st, "batch item " + std::to_string(i) + ": " + g_last_error);
+        const omb_geometry_desc &d = descs[i];
+        if (d.modality != OMB_CT_PANEL || d.fp_type != 1 || d.bp_type != 1 || d.tof_bins != 1)
+            return set_error(OMB_ERR_UNSUPPORTED, "batch item " + std::to_string(i) +
+                                                      ": batches take CT geometries with projector type 1, no TOF");
+        if (d.n_proj * (int64_t)d.n_rows_d * d.n_cols_d >= (1ll << 31))
+            return set_error(OMB_ERR_UNSUPPORTED, "batch item " + std::to_string(i) + ": too many rays");
+    }
+    omb_batch *b = new omb_batch();
+    cudaGetDevice(&b->device);
+    b->n = n;
+    b->img_off.assign(n + 1, 0);
+    b->meas_off.assign(n + 1, 0);
+    int64_t geom_floats = 0;
+    for (int i = 0; i < n; ++i) {
+        const omb_geometry_desc &d = descs[i];
+        b->img_off[i + 1] = b->img_off[i] + (int64_t)d.nx * d.ny * d.nz;
+        b->meas_off[i + 1] = b->meas_off[i] + d.n_proj * (int64_t)d.n_rows_d * d.n_cols_d;
+        geom_floats += d.n_xy + d.n_z;
+    }
+    auto fail = [&](cudaError_t e, const char *what) {
+        omb_batch_destroy(b);
+        return cuda_fail(e, what);
+    };
+    cudaError_t e = cudaMalloc(&b->d_geom, geom_floats * sizeof(float));
+    if (e != cudaSuccess) return fail(e, "cudaMalloc batch geometry");
+    std::vector<BatchItem> items((size_t)n);
+    int64_t pos = 0;
+    for (int i = 0; i < n; ++i) {
+        const omb_geometry_desc &d = descs[i];
+        float *xy = b->d_geom + pos, *z = xy + d.n_xy;
+        if ((e = cudaMemcpy(xy, d.xy, d.n_xy * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(e, "upload batch xy");
+        if ((e = cudaMemcpy(z, d.z, d.n_z * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(e, "upload batch z");
+        pos += d.n_xy + d.n_z;
+        BatchItem &it = items[(size_t)i];
+        Grid &g = it.g;
+        g.nx = (int)d.nx; g.ny = (int)d.ny; g.nz = (int)d.nz;
+        g.dx = d.dx; g.dy = d.dy; g.dz = d.dz;
+        g.bx = d.bx; g.by = d.by; g.bz = d.bz;
+        g.mx = d.bx + (float)d.nx * d.dx;
+        g.my = d.by + (float)d.ny * d.dy;
+        g.mz = d.bz + (float)d.nz * d.dz;
+        RaySet &rs = it.rs;
+        rs = RaySet{};
+        rs.xy = xy;
+        rs.z = z;
+        rs.modality = OMB_CT_PANEL;
+        rs.n_rows = (int)d.n_rows_d;
+        rs.n_cols = (int)d.n_cols_d;
+        rs.pitch_x = d.dpitch_x;
+        rs.pitch_y = d.dpitch_y;
+        rs.proj0 = 0;
+        rs.n_proj = d.n_proj;
+        rs.m_size = b->meas_off[i + 1] - b->meas_off[i];
+        rs.stype = 0;
+        rs.n_subsets = 1;
+        rs.cur_subset = 0;
+        it.img_off = b->img_off[i];
+        it.meas_off = b->meas_off[i];
+    }
+    // chunks of one block's rays, the costliest items (rays x walk length) first
+    std::vector<int> order((size_t)n);
+    for (int i = 0; i < n; ++i) order[(size_t)i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int c) {
+        const double ca = (double)items[(size_t)a].rs.m_size * (descs[a].nx + descs[a].ny);
+        const double cc = (double)items[(size_t)c].rs.m_size * (descs[c].nx + descs[c].ny);
+        return ca > cc;
+    });
+    std::vector<int2> work;
+    for (int i : order)
+        for (int64_t r = 0; r < items[(size_t)i].rs.m_size; r += kBlock) work.push_back(make_int2(i, (int)r));
+    b->n_work = (int)work.size();
+    if ((e = cudaMalloc(&b->d_items, items.size() * sizeof(BatchItem))) != cudaSuccess) return fail(e, "cudaMalloc batch items");
+    if ((e = cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e, "upload batch items");
+    if ((e = cudaMalloc(&b->d_work, work.size() * sizeof(int2))) != cudaSuccess) return fail(e, "cudaMalloc batch work");
+    if ((e = cudaMemcpy(b->d_work, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e, "upload batch work");
+    if ((e = cudaMalloc(&b->d_counter, sizeof(int))) != cudaSuccess) return fail(e, "cudaMalloc batch counter");
+    *out = b;
+    return OMB_OK;
+}
+
+int64_t omb_batch_image_offset(const omb_batch *b, int32_t item) {
+    if (!b || item < 0 || item > b->n) return -1;
+    return b->img_off[(size_t)item];
+}
+
+int64_t omb_batch_measurement_offset(const omb_batch *b, int32_t item) {
+    if (!b || item < 0 || item > b->n) return -1;
+    return b->meas_off[(size_t)item];
+}
+
+int omb_batch_forward(omb_batch *b, const float *images, float *y, void *stream) {
+    if (!b) return set_error(OMB_ERR_INVALID, "batch is NULL");
+    if (!images || !y) return set_error(OMB_ERR_INVALID, "images/y pointer is NULL");
+    return batch_project(b->d_items, b->d_work, b->n_work, b->d_counter, images, y, false, (cudaStream_t)stream);
+}
+
+int omb_batch_backward(omb_batch *b, const float *y, float *images, void *stream) {
+    if (!b) return set_error(OMB_ERR_INVALID, "batch is NULL");
+    if (!images || !y) return set_error(OMB_ERR_INVALID, "images/y pointer is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    OMB_CUDA_TRY(cudaMemsetAsync(images, 0, b->img_off[(size_t)b->n] * sizeof(float), s));
+    return batch_project(b->d_items, b->d_work, b->n_work, b->d_counter, y, images, true, s);
+}
 
 }  // extern "C"

@@ -55,6 +55,16 @@ struct RaySet {
     float pitch_x, pitch_y;
 };
 
+// One reconstruction of a batch projected by one persistent launch: its
+// grid, its rays and where its image and measurements start in the batch's
+// concatenated buffers.
+struct BatchItem {
+    Grid g;
+    RaySet rs;
+    int64_t img_off;
+    int64_t meas_off;
+};
+
 // A batch of frames (images and their measurement vectors) processed by one
 // launch; frame f's image starts at img + f*img_stride and its measurements
 // at meas + f*meas_stride.

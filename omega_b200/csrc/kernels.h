@@ -31,6 +31,10 @@ int interp_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, f
 int interp_ct_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, float kerroin,
                        const float *y, float *img, float *sens, cudaStream_t st);
 
+// Batches of independent CT geometries in one persistent launch (batch.cu).
+int batch_project(const BatchItem *items, const int2 *work, int n_work, int *counter, const float *in, float *out,
+                  bool backward, cudaStream_t st);
+
 // PDHG + TV and the power method.
 int pdhg_dual(float *p, const float *fp, const float *y, int64_t n, float sigma, cudaStream_t st);
 int pdhg_primal_tv(const Grid &g, const float *x, const float *rhs, float *u, float *x_out, float beta, float smooth,
