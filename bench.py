@@ -65,6 +65,7 @@ def parse_args():
     p.add_argument("--views", type=int, default=None,
                    help="cbct: number of projections (fewer than 360 only for short profiling captures)")
     p.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain OSEM time-to-logL leg")
     p.add_argument("--tuning", default=None,
                    help="fixed launch shapes instead of the autotuner, e.g. bdd_fp_columns=16,bdd_bp_zrun=8")
     return p.parse_args()
@@ -381,6 +382,30 @@ def cbct_cpu_rate(o, image, seconds, views_per_call=4):
                       f"{done // rays} pairs in {el:.1f} s"
 
 
+def learned_time_to_logl(studies=8, timing_studies=4):
+    """Time to the plain 20-iteration OSEM log-likelihood, learned warm start
+    vs plain OSEM, on held-out seeded studies of the dynamic-PET geometry
+    (16 subsets), with the committed network weights."""
+    import torch
+    from omega_b200 import warmstart as ws
+    path = os.path.join(ROOT, "omega_b200", "weights", "warmstart_pet128.npz")
+    state = dict(np.load(path))
+    o = ws.pet_geometry()
+    o.initProj()
+    o.autotune(n_frames=studies, repeats=1)
+    summary, _ = ws.evaluate(o, state, 3_000_000, studies, (1e7, 1e8), converged=20, batch=studies,
+                             timing_studies=timing_studies)
+    torch.cuda.synchronize()
+    return {"studies": summary["studies"], "reached_plain_L20": summary["reached_L20"],
+            "continuation_iterations_median": summary["k_median"], "continuation_iterations_max": summary["k_max"],
+            "plain_20_iterations_ms": summary["plain_ms_median"], "warm_start_ms": summary["warm_ms_median"],
+            "time_ratio": summary["time_ratio_median"],
+            "rel_l2_warm_vs_plain20": summary["rel_l2_warm_vs_plain20_median"],
+            "setup": "384 crystals x 32 rings, 128x128x63 image, 16 subsets, 1e7-1e8 counts; warm start = 2 OSEM "
+                     "iterations + BF16 U-Net + OSEM until the plain 20-iteration logL; CUDA events per study",
+            "weights": "omega_b200/weights/warmstart_pet128.npz (5000 training studies)"}
+
+
 def run_cbct(args, rank, world, dev):
     import torch
     from omega_b200 import _native
@@ -489,6 +514,11 @@ def run_cbct(args, rank, world, dev):
         "clocks": clk,
         "wall_s": wall,
     }
+    if not args.no_learned and world == 1 and not small:
+        try:
+            line["time_to_logl"] = learned_time_to_logl()
+        except Exception as e:  # must not hide the projector number
+            line["time_to_logl"] = {"error": str(e)}
     if not args.no_baseline and world == 1:
         try:
             v, sample = cbct_cpu_rate(o, mu_host, 10.0)
