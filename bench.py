@@ -49,7 +49,11 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes (read + write) per launch from ncu captures, scaled to the full
 # workload by rays; see profiles/ for the captures they come from.
-PROFILED_TRAFFIC = {}
+PROFILED_TRAFFIC = {
+    # profiles/bdd_cbct_capture.md (36-view capture x 10)
+    ("cbct", "bdd_fp"): 5.88e9,
+    ("cbct", "bdd_bp"): 3.51e8,
+}
 FALLBACK_HBM_GBS = 6650.0
 
 

@@ -29,6 +29,19 @@ extern "C" {
 int omb_unet_conv(int32_t cin, int32_t cout, const void *in, const void *w, const float *bias, void *out,
                   const void *relu_mask, int32_t relu, int32_t X, int32_t Y, int32_t Z, int32_t B, void *stream);
 
+/*
+ * The same convolution on the 5th-generation tensor cores (tcgen05.mma with
+ * the accumulator in tensor memory, 128 voxels x cout per CTA), for the same
+ * shapes and arguments as omb_unet_conv.  Its waits on the tensor core are
+ * bounded: a wait that gives up skips the output and raises the flag that
+ * omb_unet_take_error reads.
+ */
+int omb_unet_conv_tc(int32_t cin, int32_t cout, const void *in, const void *w, const float *bias, void *out,
+                     const void *relu_mask, int32_t relu, int32_t X, int32_t Y, int32_t Z, int32_t B, void *stream);
+
+/* Reads and clears the tensor-core convolutions' timeout flag (synchronises the device). */
+int omb_unet_take_error(int32_t *out_host);
+
 /* dw[27][cout][cin] += sum_v dz[v][co] in[v + off(tap)][ci] (FP32; dw must be zeroed by the caller). */
 int omb_unet_conv_wgrad(int32_t cin, int32_t cout, const void *in, const void *dz, float *dw, int32_t X, int32_t Y,
                         int32_t Z, int32_t B, void *stream);

@@ -139,6 +139,8 @@ EXPORTS = [
     ("omb_batch_backward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     # learned warm start (include/omega_b200_unet.h)
     ("omb_unet_conv", ctypes.c_int, [_i32, _i32, _v, _v, _v, _v, _v, _i32, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_conv_tc", ctypes.c_int, [_i32, _i32, _v, _v, _v, _v, _v, _i32, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_take_error", ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     ("omb_unet_conv_wgrad", ctypes.c_int, [_i32, _i32, _v, _v, _v, _i32, _i32, _i32, _i32, _v]),
     ("omb_unet_bias_grad", ctypes.c_int, [_i32, _v, _v, _i64, _v]),
     ("omb_unet_flip_weights", ctypes.c_int, [_v, _v, _i32, _i32, _v]),

@@ -189,12 +189,9 @@ __global__ void k_bdd_fp(Grid g, const float *__restrict__ xy, const float *__re
         // integral of the lateral row integrals from zu up to b, column c is
         // C(b_{c+1}) - C(b_c): walk b_0 < ... < b_8 and the voxel rows
         // together, one row integral per row crossed.
-        // The next row's integral is loaded one step ahead (Rn), so its
-        // reads overlap the current column's arithmetic.
         float bz = fminf(fmaxf(zu, 0.f), fz);
         int kc = min((int)bz, zmax);
         float R = row_integral(kc);
-        float Rn = row_integral(min(kc + 1, zmax));
         float S = 0.f;
         float Cprev = (bz - (float)kc) * R;
 #pragma unroll
@@ -203,9 +200,7 @@ __global__ void k_bdd_fp(Grid g, const float *__restrict__ xy, const float *__re
             const int kn = min((int)bz, zmax);
             while (kc < kn) {
                 S += R;
-                ++kc;
-                R = Rn;
-                Rn = row_integral(min(kc + 1, zmax));
+                R = row_integral(++kc);
             }
             const float C = fmaf(bz - (float)kc, R, S);
             temp[c] = fmaf(C - Cprev, inv_area, temp[c]);

@@ -75,20 +75,23 @@ def test_precision_workload_bf16_error_and_int64_determinism(cuda):
     g = orc.Geometry(o16)
     assert g.nbins == 15 and (g.nx, g.ny, g.nz) == (200, 200, 109)
     assert g.rays(-1) == 400 * 336 * 109
-    x = _cylinder_phantom(g, 7)
+    # values off the BF16 grid (0, 1 and 4 are exact in BF16)
+    x = _cylinder_phantom(g, 7) * 1.2345 + 0.1 * np.random.default_rng(8).random(g.n_img)
     # BF16 reads against the FP64 oracle on subset 0 (one sixteenth of the rays)
     y16 = o16.forwardProject(_t(x, cuda), 0).cpu().numpy()
     err = orc.rel_l2(y16, orc.interp_forward(g, x, 0))
     assert 1e-6 < err < 4e-3, err
     del o16
     # int64 fixed-point TOF backprojection of all 219.7 M bins: bit-identical
-    o64 = _precision_options(use_64bit_atomics=True)
-    m = o64.measurementCount(-1)
+    # (one subset: backwardProject(y, -1) means "the object's current subset",
+    # as in the reference)
+    o64 = _precision_options(use_64bit_atomics=True, subsets=1)
+    m = o64.measurementCount(0)
     assert m == 400 * 336 * 109 * 15
     y = torch.rand(m, generator=torch.Generator(device=cuda).manual_seed(5), device=cuda)
-    a = o64.backwardProject(y, -1).cpu().numpy()
-    b = o64.backwardProject(y, -1).cpu().numpy()
+    a = o64.backwardProject(y, 0).cpu().numpy()
+    b = o64.backwardProject(y, 0).cpu().numpy()
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     o64.use_64bit_atomics = False
-    f = o64.backwardProject(y, -1).cpu().numpy()
+    f = o64.backwardProject(y, 0).cpu().numpy()
     assert orc.rel_l2(f, a) < 1e-5
