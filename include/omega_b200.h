@@ -227,6 +227,8 @@ typedef struct omb_tuning {
     int32_t siddon_frames_per_walk;  /* 1, 2, 4, 8 (default 8): most frames sharing one ray walk */
     int32_t bdd_fp_columns;          /* 8, 16 (default 8): type-5 forward, detector columns per thread */
     int32_t bdd_bp_zrun;             /* 4, 8, 16 (default 8): type-5 backward, voxels along z per thread */
+    int32_t bdd_fp_block_rows;       /* 4, 8 (default 8): type-5 forward, warps per block */
+    int32_t bdd_bp_block_rows;       /* 4, 8 (default 8): type-5 backward, warps per block */
 } omb_tuning;
 
 /*

@@ -77,6 +77,8 @@ class Tuning(ctypes.Structure):
         ("siddon_frames_per_walk", ctypes.c_int32),
         ("bdd_fp_columns", ctypes.c_int32),
         ("bdd_bp_zrun", ctypes.c_int32),
+        ("bdd_fp_block_rows", ctypes.c_int32),
+        ("bdd_bp_block_rows", ctypes.c_int32),
     ]
 
     def as_dict(self):

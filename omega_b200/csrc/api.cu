@@ -354,7 +354,7 @@ int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, voi
     if (st != OMB_OK) return st;
     if (h->desc.fp_type == 5)
         return bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj, image,
-                           h->d_imgT, y, h->tune.bdd_fp_cols, (cudaStream_t)stream);
+                           h->d_imgT, y, h->tune.bdd_fp_cols, h->tune.bdd_fp_rows, (cudaStream_t)stream);
     return rays_forward(h, rs, one_frame_fp(h, image, y, rs.m_size), (cudaStream_t)stream);
 }
 
@@ -372,7 +372,7 @@ int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const fl
         for (int fr = 0; fr < n_frames; ++fr) {
             st = bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj,
                              images + fr * image_stride, h->d_imgT, y + fr * y_stride, h->tune.bdd_fp_cols,
-                             (cudaStream_t)stream);
+                             h->tune.bdd_fp_rows, (cudaStream_t)stream);
             if (st != OMB_OK) return st;
         }
         return OMB_OK;
@@ -402,7 +402,7 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
         if (mode != OMB_BP_FLOAT_ATOMIC)
             return set_error(OMB_ERR_UNSUPPORTED, "the type-5 backprojection is a gather; it has no fixed-point mode");
         return bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y, image, sens,
-                            h->tune.bdd_bp_z, s);
+                            h->tune.bdd_bp_z, h->tune.bdd_bp_rows, s);
     }
     if (h->desc.bp_type == 4 && h->desc.modality == OMB_CT_PANEL) {
         if (mode != OMB_BP_FLOAT_ATOMIC)
@@ -585,10 +585,14 @@ static int tuning_from(const omb_tuning *in, Tuning &t) {
         return set_error(OMB_ERR_INVALID, "siddon_frames_per_walk must be 1, 2, 4 or 8");
     if (!one_of(in->bdd_fp_columns, {8, 16})) return set_error(OMB_ERR_INVALID, "bdd_fp_columns must be 8 or 16");
     if (!one_of(in->bdd_bp_zrun, {4, 8, 16})) return set_error(OMB_ERR_INVALID, "bdd_bp_zrun must be 4, 8 or 16");
+    if (!one_of(in->bdd_fp_block_rows, {4, 8}) || !one_of(in->bdd_bp_block_rows, {4, 8}))
+        return set_error(OMB_ERR_INVALID, "bdd block rows must be 4 or 8");
     t.siddon_blocks_per_sm = in->siddon_blocks_per_sm;
     t.siddon_frames = in->siddon_frames_per_walk;
     t.bdd_fp_cols = in->bdd_fp_columns;
     t.bdd_bp_z = in->bdd_bp_zrun;
+    t.bdd_fp_rows = in->bdd_fp_block_rows;
+    t.bdd_bp_rows = in->bdd_bp_block_rows;
     return OMB_OK;
 }
 
@@ -598,6 +602,8 @@ static void tuning_to(const Tuning &t, omb_tuning *out) {
     out->siddon_frames_per_walk = t.siddon_frames;
     out->bdd_fp_columns = t.bdd_fp_cols;
     out->bdd_bp_zrun = t.bdd_bp_z;
+    out->bdd_fp_block_rows = t.bdd_fp_rows;
+    out->bdd_bp_block_rows = t.bdd_bp_rows;
 }
 
 int omb_get_tuning(const omb_handle *h, omb_tuning *out) {
@@ -700,33 +706,43 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
     if (e == cudaSuccess && st == OMB_OK && h->desc.fp_type == 5) {
         float best_ms = 3.4e38f;
         for (int c : {8, 16}) {
-            h->tune = best;
-            h->tune.bdd_fp_cols = c;
-            const float a = timed(fwd);
-            if (a < 0.f) {
-                st = -1;
-                break;
+            for (int rows : {4, 8}) {
+                h->tune = best;
+                h->tune.bdd_fp_cols = c;
+                h->tune.bdd_fp_rows = rows;
+                const float a = timed(fwd);
+                if (a < 0.f) {
+                    st = -1;
+                    break;
+                }
+                if (a < best_ms) {
+                    best_ms = a;
+                    best.bdd_fp_cols = c;
+                    best.bdd_fp_rows = rows;
+                }
             }
-            if (a < best_ms) {
-                best_ms = a;
-                best.bdd_fp_cols = c;
-            }
+            if (st != OMB_OK) break;
         }
     }
     if (e == cudaSuccess && st == OMB_OK && h->desc.bp_type == 5) {
         float best_ms = 3.4e38f;
         for (int z : {4, 8, 16}) {
-            h->tune = best;
-            h->tune.bdd_bp_z = z;
-            const float b = timed(bwd);
-            if (b < 0.f) {
-                st = -1;
-                break;
+            for (int rows : {4, 8}) {
+                h->tune = best;
+                h->tune.bdd_bp_z = z;
+                h->tune.bdd_bp_rows = rows;
+                const float b = timed(bwd);
+                if (b < 0.f) {
+                    st = -1;
+                    break;
+                }
+                if (b < best_ms) {
+                    best_ms = b;
+                    best.bdd_bp_z = z;
+                    best.bdd_bp_rows = rows;
+                }
             }
-            if (b < best_ms) {
-                best_ms = b;
-                best.bdd_bp_z = z;
-            }
+            if (st != OMB_OK) break;
         }
     }
     h->tune = (e == cudaSuccess && st == OMB_OK) ? best : saved;

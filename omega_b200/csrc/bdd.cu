@@ -241,7 +241,6 @@ __global__ void k_transpose_xy(const float *__restrict__ in, float *__restrict__
 // computeGeom5 uses (omegatomo/projector/init.py:6-37).
 // ---------------------------------------------------------------------------
 
-constexpr int kBpThreads = 256;
 // detector columns one thread's run of kBpZ voxels may cover before it takes
 // the per-voxel path (about 1.25 columns per voxel at magnification 2)
 __host__ __device__ constexpr int bp_slots(int kBpZ) { return kBpZ + kBpZ / 2 + (kBpZ < 16 ? 4 : 0); }
@@ -256,7 +255,7 @@ __host__ __device__ constexpr int bp_slots(int kBpZ) { return kBpZ + kBpZ / 2 + 
 // voxel over [va, vb] is then D(vb) - D(va) with D(v) = P_m + (v - m) RS_m,
 // m = floor(v): two shared-memory reads per voxel instead of a walk over its
 // detector pixels.
-template <int kBpZ, bool SENS, bool FULL>
+template <int kBpZ, bool SENS, bool FULL, int kBpThreads>
 __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
                                                        int64_t nproj, const float *__restrict__ y,
                                                        float *__restrict__ img, float *__restrict__ sens) {
@@ -378,53 +377,63 @@ __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
     }
 }
 
+// rows: warps per block (blocks of 32 x rows threads)
 template <int C>
 static void launch_fp(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
-                      int64_t nproj, const float *img, const float *imgT, float *y, cudaStream_t st) {
+                      int64_t nproj, const float *img, const float *imgT, float *y, int rows, cudaStream_t st) {
     const int groups = (nc + C - 1) / C;
-    dim3 block(32, 8);
-    dim3 grid((nr + 31) / 32, (groups + 7) / 8, (unsigned)nproj);
+    dim3 block(32, rows);
+    dim3 grid((nr + 31) / 32, (groups + rows - 1) / rows, (unsigned)nproj);
     k_bdd_fp<C><<<grid, block, 0, st>>>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y);
+}
+
+template <int Z, int T>
+static void launch_bp_t(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
+                        float *sens, cudaStream_t st) {
+    dim3 block(32, T / 32);
+    dim3 grid((g.nx + 31) / 32, (g.ny + block.y - 1) / block.y, (g.nz + Z - 1) / Z);
+    const bool full = g.nz % Z == 0;
+    if (sens && full)
+        k_bdd_bp<Z, true, true, T><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+    else if (sens)
+        k_bdd_bp<Z, true, false, T><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+    else if (full)
+        k_bdd_bp<Z, false, true, T><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+    else
+        k_bdd_bp<Z, false, false, T><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
 }
 
 template <int Z>
 static void launch_bp(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                      float *sens, cudaStream_t st) {
-    dim3 block(32, kBpThreads / 32);
-    dim3 grid((g.nx + 31) / 32, (g.ny + block.y - 1) / block.y, (g.nz + Z - 1) / Z);
-    const bool full = g.nz % Z == 0;
-    if (sens && full)
-        k_bdd_bp<Z, true, true><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
-    else if (sens)
-        k_bdd_bp<Z, true, false><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
-    else if (full)
-        k_bdd_bp<Z, false, true><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+                      float *sens, int rows, cudaStream_t st) {
+    if (rows == 4)
+        launch_bp_t<Z, 128>(g, pj, nr, nc, nproj, y, img, sens, st);
     else
-        k_bdd_bp<Z, false, false><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+        launch_bp_t<Z, 256>(g, pj, nr, nc, nproj, y, img, sens, st);
 }
 
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
-                int64_t nproj, const float *img, float *imgT, float *y, int cols, cudaStream_t st) {
+                int64_t nproj, const float *img, float *imgT, float *y, int cols, int rows, cudaStream_t st) {
     if (nproj <= 0) return OMB_OK;
     if (nproj > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 projections in one call");
     dim3 tg((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz);
     k_transpose_xy<<<tg, dim3(32, 8), 0, st>>>(img, imgT, g.nx, g.ny, g.nz);
     OMB_LAUNCH_CHECK("transpose launch");
     switch (cols) {
-        case 16: launch_fp<16>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, st); break;
-        default: launch_fp<8>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, st); break;
+        case 16: launch_fp<16>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, rows, st); break;
+        default: launch_fp<8>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, rows, st); break;
     }
     OMB_LAUNCH_CHECK("bdd forward launch");
     return OMB_OK;
 }
 
 int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                 float *sens, int zrun, cudaStream_t st) {
+                 float *sens, int zrun, int rows, cudaStream_t st) {
     if (g.nz > 65535 * 4) return set_error(OMB_ERR_UNSUPPORTED, "too many slices");
     switch (zrun) {
-        case 4: launch_bp<4>(g, pj, nr, nc, nproj, y, img, sens, st); break;
-        case 16: launch_bp<16>(g, pj, nr, nc, nproj, y, img, sens, st); break;
-        default: launch_bp<8>(g, pj, nr, nc, nproj, y, img, sens, st); break;
+        case 4: launch_bp<4>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;
+        case 16: launch_bp<16>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;
+        default: launch_bp<8>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;
     }
     OMB_LAUNCH_CHECK("bdd backward launch");
     return OMB_OK;

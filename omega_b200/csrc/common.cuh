@@ -108,6 +108,8 @@ struct Tuning {
     int siddon_frames = 8;          // most frames sharing one ray walk (1, 2, 4, 8)
     int bdd_fp_cols = 8;            // type-5 forward: detector columns per thread (8, 16)
     int bdd_bp_z = 8;               // type-5 backward: voxels along z per thread (4, 8, 16)
+    int bdd_fp_rows = 8;            // type-5 forward: warps per block (4, 8)
+    int bdd_bp_rows = 8;            // type-5 backward: warps per block (4, 8)
 };
 
 // Read-only image load as float from an FP32 or BF16 array.

@@ -16,9 +16,9 @@ int fixed_to_float(const unsigned long long *acc, float *out, int64_t n, cudaStr
 
 // Projector type 5 (branchless distance-driven), CT.
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
-                int64_t nproj, const float *img, float *imgT, float *y, int cols, cudaStream_t st);
+                int64_t nproj, const float *img, float *imgT, float *y, int cols, int rows, cudaStream_t st);
 int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                 float *sens, int zrun, cudaStream_t st);
+                 float *sens, int zrun, int rows, cudaStream_t st);
 
 // Projector type 4 (interpolation), PET and CT.
 int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img,

@@ -1,8 +1,10 @@
 """Learned OSEM warm start: a 3-D U-Net that maps the 2-iteration OSEM image
 (plus the sensitivity image) to a 20-iteration-quality image, after which
 plain OSEM continues.  The network is trained and run on the GPU by the
-library's own kernels (include/omega_b200_unet.h): BF16 tensor-core 3x3x3
-convolutions with FP32 accumulation, their data and weight gradients, pooling,
+library's own kernels (include/omega_b200_unet.h): BF16 3x3x3 convolutions
+on the tcgen05 tensor cores (FP32 accumulator in tensor memory) for the
+forward pass and the data gradients, warp-level MMA for the weight
+gradients, pooling,
 upsampling, the loss and Adam.  torch only allocates device memory.
 
 Architecture (3 levels, 16/32/64 channels, 3x3x3 convolutions + ReLU):
@@ -41,6 +43,11 @@ class UNet3D:
     Volumes are (X, Y, Zs) Fortran-order images; the network works on Z =
     Zs rounded up to a multiple of 4 (extra slices are zero padding and are
     excluded from the loss).  `batch` studies go through one call."""
+
+    # convolution engine of the forward pass and the data gradients:
+    # "omb_unet_conv_tc" (tcgen05, accumulator in tensor memory) or
+    # "omb_unet_conv" (warp-level mma.sync)
+    conv_entry = "omb_unet_conv_tc"
 
     def __init__(self, X, Y, Zs, batch, device, seed=0):
         import torch
@@ -128,7 +135,7 @@ class UNet3D:
     def _conv(self, i, src, dst, level, relu=True):
         ci, co = LAYERS[i]
         X, Y, Z = self._dims(level)
-        _native.call("omb_unet_conv", ci, co, _p(src), _p(self.params[i]["wb"]), _p(self.params[i]["b"]), _p(dst),
+        _native.call(self.conv_entry, ci, co, _p(src), _p(self.params[i]["wb"]), _p(self.params[i]["b"]), _p(dst),
                      None, 1 if relu else 0, X, Y, Z, self.B, self._stream())
 
     def _dims(self, level):
@@ -184,7 +191,7 @@ class UNet3D:
     def _dgrad(self, i, dz, dst, level, mask):
         ci, co = LAYERS[i]
         X, Y, Z = self._dims(level)
-        _native.call("omb_unet_conv", co, ci, _p(dz), _p(self.params[i]["wf"]), None, _p(dst), _p(mask), 0,
+        _native.call(self.conv_entry, co, ci, _p(dz), _p(self.params[i]["wf"]), None, _p(dst), _p(mask), 0,
                      X, Y, Z, self.B, self._stream())
 
     def backward(self, target, target_stride):

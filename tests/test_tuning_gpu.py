@@ -33,13 +33,14 @@ def test_bdd_every_shape_matches_oracle(cuda, name):
     y = rng.uniform(0.0, 2.0, g.rays(0))
     ref_fp = orc.bdd_forward(g, x, 0)
     ref_bp, ref_s = orc.bdd_backward(g, y, 0, sens=True)
-    for cols, zrun in itertools.product([8, 16], [4, 8, 16]):
-        o.tuning = {"bdd_fp_columns": cols, "bdd_bp_zrun": zrun}
+    for cols, zrun, rows in itertools.product([8, 16], [4, 8, 16], [4, 8]):
+        o.tuning = {"bdd_fp_columns": cols, "bdd_bp_zrun": zrun, "bdd_fp_block_rows": rows,
+                    "bdd_bp_block_rows": rows}
         fp = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
         bp, s = o.backwardProject(_t(y, cuda), 0, sens=True)
-        assert orc.rel_l2(fp, ref_fp) < TOL, (cols, orc.rel_l2(fp, ref_fp))
-        assert orc.rel_l2(bp.cpu().numpy(), ref_bp) < TOL, (zrun, orc.rel_l2(bp.cpu().numpy(), ref_bp))
-        assert orc.rel_l2(s.cpu().numpy(), ref_s) < TOL, zrun
+        assert orc.rel_l2(fp, ref_fp) < TOL, (cols, rows, orc.rel_l2(fp, ref_fp))
+        assert orc.rel_l2(bp.cpu().numpy(), ref_bp) < TOL, (zrun, rows, orc.rel_l2(bp.cpu().numpy(), ref_bp))
+        assert orc.rel_l2(s.cpu().numpy(), ref_s) < TOL, (zrun, rows)
 
 
 def test_siddon_every_shape_matches_oracle(cuda):
@@ -77,6 +78,7 @@ def test_autotune_returns_valid_shape(cuda, name, frames):
     assert t["siddon_frames_per_walk"] in (1, 2, 4, 8)
     assert t["bdd_fp_columns"] in (8, 16)
     assert t["bdd_bp_zrun"] in (4, 8, 16)
+    assert t["bdd_fp_block_rows"] in (4, 8) and t["bdd_bp_block_rows"] in (4, 8)
     g = orc.Geometry(o)
     x = np.random.default_rng(13).uniform(0.5, 1.5, g.n_img)
     fp = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
@@ -85,7 +87,8 @@ def test_autotune_returns_valid_shape(cuda, name, frames):
 
 
 @pytest.mark.parametrize("key,value", [("siddon_blocks_per_sm", 0), ("siddon_frames_per_walk", 3),
-                                       ("bdd_fp_columns", 4), ("bdd_bp_zrun", 32)])
+                                       ("bdd_fp_columns", 4), ("bdd_bp_zrun", 32),
+                                       ("bdd_fp_block_rows", 2), ("bdd_bp_block_rows", 16)])
 def test_invalid_shape_rejected(cuda, key, value):
     from omega_b200 import _native
     o = _init("ct_mini5")
