@@ -229,6 +229,16 @@ typedef struct omb_tuning {
     int32_t bdd_bp_zrun;             /* 4, 8, 16 (default 8): type-5 backward, voxels along z per thread */
     int32_t bdd_fp_block_rows;       /* 4, 8 (default 8): type-5 forward, warps per block */
     int32_t bdd_bp_block_rows;       /* 4, 8 (default 8): type-5 backward, warps per block */
+    int32_t siddon_frame_layout;     /* 0, 1 (default 1): type-1 non-TOF batches of >= 4 frames.
+                                        0: the kernels read and update each frame's image in place;
+                                        1: through a voxel-interleaved copy (the 4 or 8 frames of a walk
+                                        stored together per voxel: 16-byte loads, float4 atomics), kept
+                                        on the handle (ceil(frames / 8) * 8 images, allocated by the
+                                        first such call made outside CUDA-graph capture; calls on one
+                                        handle must therefore be ordered on one stream) */
+    int32_t siddon_fp_steps;         /* 1, 2, 4 (default 4): non-TOF type-1 forward walks compute this
+                                        many crossings before gathering their voxels, so that many
+                                        loads are in flight per thread */
 } omb_tuning;
 
 /*

@@ -79,6 +79,8 @@ class Tuning(ctypes.Structure):
         ("bdd_bp_zrun", ctypes.c_int32),
         ("bdd_fp_block_rows", ctypes.c_int32),
         ("bdd_bp_block_rows", ctypes.c_int32),
+        ("siddon_frame_layout", ctypes.c_int32),
+        ("siddon_fp_steps", ctypes.c_int32),
     ]
 
     def as_dict(self):

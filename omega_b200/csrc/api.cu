@@ -44,7 +44,37 @@ struct omb_handle {
     int read_mode = OMB_READ_FP32;        // image precision of the type-1/4 forward projections
     __nv_bfloat16 *d_img16 = nullptr;     // BF16 image copies (read_mode == OMB_READ_BF16)
     int img16_frames = 0;                 // frames d_img16 holds
+    float *d_ilv = nullptr;               // voxel-interleaved frame scratch (type-1 frame batches)
+    int64_t ilv_floats = 0;               // its capacity
+    // Buffers replaced by larger ones.  They are freed only with the handle:
+    // a CUDA graph captured earlier may still address them.
+    std::vector<void *> retired;
 };
+
+// Attaches the voxel-interleaved scratch to a type-1 frame batch, growing it
+// to ceil(n / 8) * 8 images when needed.  Growing allocates, so it is skipped
+// while the stream is being captured into a CUDA graph: the batch then takes
+// the frame-major kernels (the capture's warm-up call normally grew it).
+static void attach_interleave(omb_handle *h, Frames &f, cudaStream_t s) {
+    f.ilv = nullptr;
+    f.ilv_floats = 0;
+    if (h->tune.siddon_layout != 1 || h->desc.tof_bins != 1 || f.n < 4) return;
+    const int64_t need = (int64_t)((f.n + 7) / 8) * 8 * h->n_img;
+    if (need > h->ilv_floats) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+        float *p = nullptr;
+        if (cudaMalloc(&p, (size_t)need * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();  // out of memory: keep the frame-major kernels
+            return;
+        }
+        if (h->d_ilv) h->retired.push_back(h->d_ilv);
+        h->d_ilv = p;
+        h->ilv_floats = need;
+    }
+    f.ilv = h->d_ilv;
+    f.ilv_floats = h->ilv_floats;
+}
 
 // Type-5 backprojection maps of every projection, FP64 on the host from the
 // same vectors the reference's computeGeom5 uses (omegatomo/projector/
@@ -208,7 +238,7 @@ static Frames one_frame_bp(const omb_handle *h, const float *y, float *img, int6
 
 // Ray-driven forward projection of a batch of frames (types 1 and 4).  With
 // BF16 reads the images are first rounded into the handle's BF16 copies.
-static int rays_forward(const omb_handle *h, const RaySet &rs, const Frames &f_in, cudaStream_t s) {
+static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cudaStream_t s) {
     Frames f = f_in;
     if (h->read_mode == OMB_READ_BF16 && f.n > 0) {
         if (f.n > h->img16_frames)
@@ -230,6 +260,7 @@ static int rays_forward(const omb_handle *h, const RaySet &rs, const Frames &f_i
         }
         return OMB_OK;
     }
+    if (!f.img_in16) attach_interleave(h, f, s);
     return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, f, h->tune, s);
 }
 
@@ -237,7 +268,8 @@ static int rays_forward(const omb_handle *h, const RaySet &rs, const Frames &f_i
 // frames into zeroed images; `sens` (zeroed) receives A^T 1 of the first
 // frame's rays.  f.meas == NULL backprojects ones, f.img == NULL keeps only
 // the sensitivity.
-static int rays_backward(const omb_handle *h, const RaySet &rs, const Frames &f, float *sens, cudaStream_t s) {
+static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, float *sens, cudaStream_t s) {
+    Frames f = f_in;
     if (h->desc.bp_type == 4) {
         for (int fr = 0; fr < f.n; ++fr) {
             const int st = interp_backward(h->grid, rs, h->tof, h->desc.global_factor, h->desc.dL,
@@ -248,6 +280,7 @@ static int rays_backward(const omb_handle *h, const RaySet &rs, const Frames &f,
         }
         return OMB_OK;
     }
+    if (!sens && f.meas && f.img) attach_interleave(h, f, s);
     return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, sens, h->tune, s);
 }
 
@@ -332,6 +365,8 @@ int omb_destroy(omb_handle *h) {
     cudaFree(h->d_imgT);
     cudaFree(h->d_bddp);
     cudaFree(h->d_img16);
+    cudaFree(h->d_ilv);
+    for (void *p : h->retired) cudaFree(p);
     if (prev != h->device) cudaSetDevice(prev);
     delete h;
     return OMB_OK;
@@ -587,12 +622,16 @@ static int tuning_from(const omb_tuning *in, Tuning &t) {
     if (!one_of(in->bdd_bp_zrun, {4, 8, 16})) return set_error(OMB_ERR_INVALID, "bdd_bp_zrun must be 4, 8 or 16");
     if (!one_of(in->bdd_fp_block_rows, {4, 8}) || !one_of(in->bdd_bp_block_rows, {4, 8}))
         return set_error(OMB_ERR_INVALID, "bdd block rows must be 4 or 8");
+    if (!one_of(in->siddon_frame_layout, {0, 1})) return set_error(OMB_ERR_INVALID, "siddon_frame_layout must be 0 or 1");
+    if (!one_of(in->siddon_fp_steps, {1, 2, 4})) return set_error(OMB_ERR_INVALID, "siddon_fp_steps must be 1, 2 or 4");
     t.siddon_blocks_per_sm = in->siddon_blocks_per_sm;
     t.siddon_frames = in->siddon_frames_per_walk;
     t.bdd_fp_cols = in->bdd_fp_columns;
     t.bdd_bp_z = in->bdd_bp_zrun;
     t.bdd_fp_rows = in->bdd_fp_block_rows;
     t.bdd_bp_rows = in->bdd_bp_block_rows;
+    t.siddon_layout = in->siddon_frame_layout;
+    t.siddon_fp_steps = in->siddon_fp_steps;
     return OMB_OK;
 }
 
@@ -604,6 +643,8 @@ static void tuning_to(const Tuning &t, omb_tuning *out) {
     out->bdd_bp_zrun = t.bdd_bp_z;
     out->bdd_fp_block_rows = t.bdd_fp_rows;
     out->bdd_bp_block_rows = t.bdd_bp_rows;
+    out->siddon_frame_layout = t.siddon_layout;
+    out->siddon_fp_steps = t.siddon_fp_steps;
 }
 
 int omb_get_tuning(const omb_handle *h, omb_tuning *out) {
@@ -632,7 +673,7 @@ int omb_set_read_precision(omb_handle *h, int32_t mode, int32_t max_frames) {
         __nv_bfloat16 *p = nullptr;
         const cudaError_t e = cudaMalloc(&p, (size_t)max_frames * h->n_img * sizeof(__nv_bfloat16));
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc BF16 image copies");
-        cudaFree(h->d_img16);
+        if (h->d_img16) h->retired.push_back(h->d_img16);
         h->d_img16 = p;
         h->img16_frames = max_frames;
     }
@@ -687,19 +728,43 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
         const int frames_max = h->desc.tof_bins > 1 ? 1 : 8;
         for (int ps : {2, 4, 8, 16}) {
             for (int fr = 1; fr <= frames_max && fr <= n_frames && st == OMB_OK; fr *= 2) {
-                h->tune = saved;
-                h->tune.siddon_blocks_per_sm = ps;
-                h->tune.siddon_frames = fr;
-                const float a = ray_fp ? timed(fwd) : 0.f, b = a < 0.f ? -1.f : (ray_bp ? timed(bwd) : 0.f);
-                if (a < 0.f || b < 0.f) {
-                    st = -1;
-                    break;
+                // the voxel-interleaved layout applies to type-1 walks of 4 or 8 frames
+                const bool both = fr >= 4 && h->desc.fp_type == 1 && h->desc.bp_type == 1;
+                for (int layout = both ? 0 : saved.siddon_layout; layout <= (both ? 1 : saved.siddon_layout);
+                     ++layout) {
+                    h->tune = saved;
+                    h->tune.siddon_blocks_per_sm = ps;
+                    h->tune.siddon_frames = fr;
+                    h->tune.siddon_layout = layout;
+                    const float a = ray_fp ? timed(fwd) : 0.f, b = a < 0.f ? -1.f : (ray_bp ? timed(bwd) : 0.f);
+                    if (a < 0.f || b < 0.f) {
+                        st = -1;
+                        break;
+                    }
+                    if (a + b < best_ms) {
+                        best_ms = a + b;
+                        best.siddon_blocks_per_sm = ps;
+                        best.siddon_frames = fr;
+                        best.siddon_layout = layout;
+                    }
                 }
-                if (a + b < best_ms) {
-                    best_ms = a + b;
-                    best.siddon_blocks_per_sm = ps;
-                    best.siddon_frames = fr;
-                }
+            }
+        }
+    }
+    // then the forward walk's batched crossings (type 1 without TOF)
+    if (e == cudaSuccess && st == OMB_OK && h->desc.fp_type == 1 && h->desc.tof_bins == 1) {
+        float best_ms = 3.4e38f;
+        for (int k : {1, 2, 4}) {
+            h->tune = best;
+            h->tune.siddon_fp_steps = k;
+            const float a = timed(fwd);
+            if (a < 0.f) {
+                st = -1;
+                break;
+            }
+            if (a < best_ms) {
+                best_ms = a;
+                best.siddon_fp_steps = k;
             }
         }
     }

@@ -77,6 +77,8 @@ struct Frames {
     const float *meas;     // backward: input measurements
     float *meas_out;       // forward: output measurements
     int64_t meas_stride;
+    float *ilv;            // scratch of ceil(n / FB) * FB images in voxel-interleaved order, or NULL
+    int64_t ilv_floats;    // its capacity
 };
 
 struct Tof {
@@ -110,6 +112,8 @@ struct Tuning {
     int bdd_bp_z = 8;               // type-5 backward: voxels along z per thread (4, 8, 16)
     int bdd_fp_rows = 8;            // type-5 forward: warps per block (4, 8)
     int bdd_bp_rows = 8;            // type-5 backward: warps per block (4, 8)
+    int siddon_layout = 1;          // frame batches: 0 = frame-major reads/atomics, 1 = voxel-interleaved
+    int siddon_fp_steps = 4;        // non-TOF forward walks: crossings gathered per batched step (1, 2, 4)
 };
 
 // Read-only image load as float from an FP32 or BF16 array.

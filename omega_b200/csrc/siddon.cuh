@@ -265,7 +265,14 @@ __device__ __forceinline__ float tof_weights(const Tof &tof, float ddsign, float
 // tof_weights, tof_sum) for every intersected voxel.  `temp` receives the
 // ray's normalisation (1/L * global_factor for PET, 1 for CT).  Returns false
 // when the ray contributes nothing.
-template <int NB, class Visit>
+//
+// K > 1 (non-TOF only) takes the crossings K at a time: the K voxel indices
+// and lengths are computed first and the K visits follow in straight-line
+// code, so a gathering visitor has K independent loads in flight instead of
+// waiting on one per voxel.  Steps past the ray's end are visited with length
+// 0 at the batch's first (valid) voxel.  The visits and their order are those
+// of K = 1.
+template <int NB, int K = 1, class Visit>
 __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool pet, float global_factor,
                                             const Tof &tof, float &temp, Visit &&vis) {
     // Set-up in FP64 (end points are FP32, so their differences are exact);
@@ -391,33 +398,73 @@ __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool 
     }
     float tc = (float)tcd;
     float tx = ax.next(), ty = ay.next(), tz = az.next();
-    for (unsigned ii = 0u; ii < np; ++ii) {
-        const int64_t ind = (int64_t)tj * g.nx + ti + (int64_t)tk * nxy;
-        float t0;
-        if (tz < ty && tz < tx) {
-            t0 = tz;
-            tk += az.u;
-            az.n++;
-            tz = az.next();
-        } else if (ty < tx) {
-            t0 = ty;
-            tj += ay.u;
-            ay.n++;
-            ty = ay.next();
-        } else {
-            t0 = tx;
-            ti += ax.u;
-            ax.n++;
-            tx = ax.next();
+    if constexpr (K > 1) {
+        static_assert(NB == 1, "batched crossings are built for non-TOF walks");
+        bool done = false;
+        for (unsigned ii = 0u; ii < np && !done; ii += K) {
+            int64_t inds[K];
+            float eles[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                inds[k] = k ? inds[0] : 0;
+                eles[k] = 0.f;
+                if (!done && ii + k < np) {
+                    inds[k] = (int64_t)tj * g.nx + ti + (int64_t)tk * nxy;
+                    float t0;
+                    if (tz < ty && tz < tx) {
+                        t0 = tz;
+                        tk += az.u;
+                        az.n++;
+                        tz = az.next();
+                    } else if (ty < tx) {
+                        t0 = ty;
+                        tj += ay.u;
+                        ay.n++;
+                        ty = ay.next();
+                    } else {
+                        t0 = tx;
+                        ti += ax.u;
+                        ax.n++;
+                        tx = ax.next();
+                    }
+                    const bool pass = (t0 >= 0.f && t0 <= 1.f) || (tc >= 0.f && tc <= 1.f);
+                    eles[k] = pass ? (fminf(t0, 1.f) - fmaxf(tc, 0.f)) * L : 0.f;
+                    tc = t0;
+                    done = ti < 0 || ti >= g.nx || tj < 0 || tj >= g.ny || tk < 0 || tk >= g.nz;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) vis(inds[k], eles[k], w, 1.f);
         }
-        const bool pass = (t0 >= 0.f && t0 <= 1.f) || (tc >= 0.f && tc <= 1.f);
-        const float ele = pass ? (fminf(t0, 1.f) - fmaxf(tc, 0.f)) * L : 0.f;
-        tc = t0;
-        float tsum = 1.f;
-        if (NB > 1) tsum = tof_weights<NB>(tof, ddsign, ele, D, w);
-        vis(ind, ele, w, tsum);
-        if (NB > 1) D -= ele * ddsign;
-        if (ti < 0 || ti >= g.nx || tj < 0 || tj >= g.ny || tk < 0 || tk >= g.nz) break;
+    } else {
+        for (unsigned ii = 0u; ii < np; ++ii) {
+            const int64_t ind = (int64_t)tj * g.nx + ti + (int64_t)tk * nxy;
+            float t0;
+            if (tz < ty && tz < tx) {
+                t0 = tz;
+                tk += az.u;
+                az.n++;
+                tz = az.next();
+            } else if (ty < tx) {
+                t0 = ty;
+                tj += ay.u;
+                ay.n++;
+                ty = ay.next();
+            } else {
+                t0 = tx;
+                ti += ax.u;
+                ax.n++;
+                tx = ax.next();
+            }
+            const bool pass = (t0 >= 0.f && t0 <= 1.f) || (tc >= 0.f && tc <= 1.f);
+            const float ele = pass ? (fminf(t0, 1.f) - fmaxf(tc, 0.f)) * L : 0.f;
+            tc = t0;
+            float tsum = 1.f;
+            if (NB > 1) tsum = tof_weights<NB>(tof, ddsign, ele, D, w);
+            vis(ind, ele, w, tsum);
+            if (NB > 1) D -= ele * ddsign;
+            if (ti < 0 || ti >= g.nx || tj < 0 || tj >= g.ny || tk < 0 || tk >= g.nz) break;
+        }
     }
     return true;
 }

@@ -55,18 +55,32 @@ def test_siddon_every_shape_matches_oracle(cuda):
     rng = np.random.default_rng(12)
     imgs = rng.uniform(0.5, 2.0, (frames, n))
     ref = np.concatenate([orc.forward(g, imgs[0], s) for s in range(g.n_subsets)])
+    ref_fp = [np.concatenate([orc.forward(g, imgs[f], s) for s in range(g.n_subsets)]) for f in range(frames)]
+    assert orc.rel_l2(ref_fp[0], ref) == 0.0
+    # backprojection of every frame over all subsets (measurements subset-contiguous)
+    ys = rng.uniform(0.0, 2.0, (frames, m))
+    ys[:, ::7] = 0.0
+    cut = np.cumsum([0] + [g.rays(s) for s in range(g.n_subsets)])
+    ref_bp = [sum(orc.backward(g, ys[f, cut[s]:cut[s + 1]], s) for s in range(g.n_subsets)) for f in range(frames)]
     X = _t(imgs, cuda)
+    Yin = _t(ys, cuda)
     Y = torch.empty((frames, m), device=cuda)
+    B = torch.empty((frames, n), device=cuda)
     st = ctypes.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
-    for ps, fw in itertools.product([1, 2, 8, 16], [1, 2, 4, 8]):
-        o.tuning = {"siddon_blocks_per_sm": ps, "siddon_frames_per_walk": fw}
+    shapes = [(ps, fw, lay, 1) for ps, fw, lay in itertools.product([1, 2, 8, 16], [1, 2, 4, 8], [0, 1])]
+    shapes += [(8, fw, lay, k) for fw, lay, k in itertools.product([1, 4, 8], [0, 1], [2, 4])]
+    for ps, fw, lay, k in shapes:
+        o.tuning = {"siddon_blocks_per_sm": ps, "siddon_frames_per_walk": fw, "siddon_frame_layout": lay,
+                    "siddon_fp_steps": k}
         _native.call("omb_forward_frames", o._handle, -1, frames, ctypes.c_void_p(X.data_ptr()), n,
                      ctypes.c_void_p(Y.data_ptr()), m, st)
-        y = Y.cpu().numpy()
-        assert orc.rel_l2(y[0], ref) < TOL, (ps, fw)
-        for f in range(1, frames):
-            ref_f = np.concatenate([orc.forward(g, imgs[f], s) for s in range(g.n_subsets)])
-            assert orc.rel_l2(y[f], ref_f) < TOL, (ps, fw, f)
+        B.fill_(-1.0)
+        _native.call("omb_backward_frames", o._handle, -1, frames, ctypes.c_void_p(Yin.data_ptr()), m,
+                     ctypes.c_void_p(B.data_ptr()), n, st)
+        y, b = Y.cpu().numpy(), B.cpu().numpy()
+        for f in range(frames):
+            assert orc.rel_l2(y[f], ref_fp[f]) < TOL, (ps, fw, lay, k, f)
+            assert orc.rel_l2(b[f], ref_bp[f]) < TOL, (ps, fw, lay, f, orc.rel_l2(b[f], ref_bp[f]))
 
 
 @pytest.mark.parametrize("name,frames", [("ct_mini5", 1), ("pet_mini", 4)])
@@ -79,6 +93,7 @@ def test_autotune_returns_valid_shape(cuda, name, frames):
     assert t["bdd_fp_columns"] in (8, 16)
     assert t["bdd_bp_zrun"] in (4, 8, 16)
     assert t["bdd_fp_block_rows"] in (4, 8) and t["bdd_bp_block_rows"] in (4, 8)
+    assert t["siddon_frame_layout"] in (0, 1) and t["siddon_fp_steps"] in (1, 2, 4)
     g = orc.Geometry(o)
     x = np.random.default_rng(13).uniform(0.5, 1.5, g.n_img)
     fp = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
@@ -88,7 +103,8 @@ def test_autotune_returns_valid_shape(cuda, name, frames):
 
 @pytest.mark.parametrize("key,value", [("siddon_blocks_per_sm", 0), ("siddon_frames_per_walk", 3),
                                        ("bdd_fp_columns", 4), ("bdd_bp_zrun", 32),
-                                       ("bdd_fp_block_rows", 2), ("bdd_bp_block_rows", 16)])
+                                       ("bdd_fp_block_rows", 2), ("bdd_bp_block_rows", 16),
+                                       ("siddon_frame_layout", 2), ("siddon_fp_steps", 3)])
 def test_invalid_shape_rejected(cuda, key, value):
     from omega_b200 import _native
     o = _init("ct_mini5")
