@@ -239,6 +239,9 @@ typedef struct omb_tuning {
     int32_t siddon_fp_steps;         /* 1, 2, 4 (default 4): non-TOF type-1 forward walks compute this
                                         many crossings before gathering their voxels, so that many
                                         loads are in flight per thread */
+    int32_t bdd_fp_staged;           /* 0, 1 (default 1): type-5 forward projection with each CTA's
+                                        per-slice image boxes staged in shared memory by TMA (applies
+                                        with bdd_fp_columns = 8; needs Nx, Ny multiples of 4) */
 } omb_tuning;
 
 /*
@@ -255,6 +258,14 @@ typedef struct omb_tuning {
 int omb_set_read_precision(omb_handle *h, int32_t mode, int32_t max_frames);
 
 int omb_get_tuning(const omb_handle *h, omb_tuning *out);
+
+/*
+ * Device error word of the kernels' bounded waits (TMA and tensor-core
+ * pipelines): 0 when no wait ran out since the last call, 1 when one did (the
+ * results of that launch are invalid); reading it resets it.  < 0 if the
+ * word could not be read.  Synchronises the device.
+ */
+int omb_take_device_error(void);
 int omb_set_tuning(omb_handle *h, const omb_tuning *in);
 
 /*

@@ -81,6 +81,7 @@ class Tuning(ctypes.Structure):
         ("bdd_bp_block_rows", ctypes.c_int32),
         ("siddon_frame_layout", ctypes.c_int32),
         ("siddon_fp_steps", ctypes.c_int32),
+        ("bdd_fp_staged", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -129,6 +130,7 @@ EXPORTS = [
                                         ctypes.c_void_p]),
     ("omb_power_workspace_bytes", ctypes.c_size_t, []),
     ("omb_set_read_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    ("omb_take_device_error", ctypes.c_int, []),
     ("omb_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
     ("omb_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
     ("omb_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Tuning),

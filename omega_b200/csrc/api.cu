@@ -389,7 +389,7 @@ int omb_forward(omb_handle *h, int32_t subset, const float *image, float *y, voi
     if (st != OMB_OK) return st;
     if (h->desc.fp_type == 5)
         return bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj, image,
-                           h->d_imgT, y, h->tune.bdd_fp_cols, h->tune.bdd_fp_rows, (cudaStream_t)stream);
+                           h->d_imgT, y, h->tune, (cudaStream_t)stream);
     return rays_forward(h, rs, one_frame_fp(h, image, y, rs.m_size), (cudaStream_t)stream);
 }
 
@@ -406,8 +406,8 @@ int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const fl
     if (h->desc.fp_type == 5) {
         for (int fr = 0; fr < n_frames; ++fr) {
             st = bdd_forward(h->grid, h->d_xy, h->d_z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj,
-                             images + fr * image_stride, h->d_imgT, y + fr * y_stride, h->tune.bdd_fp_cols,
-                             h->tune.bdd_fp_rows, (cudaStream_t)stream);
+                             images + fr * image_stride, h->d_imgT, y + fr * y_stride, h->tune,
+                             (cudaStream_t)stream);
             if (st != OMB_OK) return st;
         }
         return OMB_OK;
@@ -624,6 +624,7 @@ static int tuning_from(const omb_tuning *in, Tuning &t) {
         return set_error(OMB_ERR_INVALID, "bdd block rows must be 4 or 8");
     if (!one_of(in->siddon_frame_layout, {0, 1})) return set_error(OMB_ERR_INVALID, "siddon_frame_layout must be 0 or 1");
     if (!one_of(in->siddon_fp_steps, {1, 2, 4})) return set_error(OMB_ERR_INVALID, "siddon_fp_steps must be 1, 2 or 4");
+    if (!one_of(in->bdd_fp_staged, {0, 1})) return set_error(OMB_ERR_INVALID, "bdd_fp_staged must be 0 or 1");
     t.siddon_blocks_per_sm = in->siddon_blocks_per_sm;
     t.siddon_frames = in->siddon_frames_per_walk;
     t.bdd_fp_cols = in->bdd_fp_columns;
@@ -632,6 +633,7 @@ static int tuning_from(const omb_tuning *in, Tuning &t) {
     t.bdd_bp_rows = in->bdd_bp_block_rows;
     t.siddon_layout = in->siddon_frame_layout;
     t.siddon_fp_steps = in->siddon_fp_steps;
+    t.bdd_fp_staged = in->bdd_fp_staged;
     return OMB_OK;
 }
 
@@ -645,6 +647,13 @@ static void tuning_to(const Tuning &t, omb_tuning *out) {
     out->bdd_bp_block_rows = t.bdd_bp_rows;
     out->siddon_frame_layout = t.siddon_layout;
     out->siddon_fp_steps = t.siddon_fp_steps;
+    out->bdd_fp_staged = t.bdd_fp_staged;
+}
+
+int omb_take_device_error(void) {
+    const int v = take_device_error();
+    if (v < 0) return set_error(OMB_ERR_CUDA, "reading the device error word failed");
+    return v;
 }
 
 int omb_get_tuning(const omb_handle *h, omb_tuning *out) {
@@ -770,23 +779,24 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
     }
     if (e == cudaSuccess && st == OMB_OK && h->desc.fp_type == 5) {
         float best_ms = 3.4e38f;
-        for (int c : {8, 16}) {
-            for (int rows : {4, 8}) {
-                h->tune = best;
-                h->tune.bdd_fp_cols = c;
-                h->tune.bdd_fp_rows = rows;
-                const float a = timed(fwd);
-                if (a < 0.f) {
-                    st = -1;
-                    break;
-                }
-                if (a < best_ms) {
-                    best_ms = a;
-                    best.bdd_fp_cols = c;
-                    best.bdd_fp_rows = rows;
-                }
+        // (columns, warps per block, staged); the staged kernel has 8 columns and 4 warps
+        const int shapes[5][3] = {{8, 4, 0}, {8, 8, 0}, {16, 4, 0}, {16, 8, 0}, {8, 4, 1}};
+        for (const auto &sh : shapes) {
+            h->tune = best;
+            h->tune.bdd_fp_cols = sh[0];
+            h->tune.bdd_fp_rows = sh[1];
+            h->tune.bdd_fp_staged = sh[2];
+            const float a = timed(fwd);
+            if (a < 0.f) {
+                st = -1;
+                break;
             }
-            if (st != OMB_OK) break;
+            if (a < best_ms) {
+                best_ms = a;
+                best.bdd_fp_cols = sh[0];
+                best.bdd_fp_rows = sh[1];
+                best.bdd_fp_staged = sh[2];
+            }
         }
     }
     if (e == cudaSuccess && st == OMB_OK && h->desc.bp_type == 5) {

@@ -16,7 +16,13 @@ int fixed_to_float(const unsigned long long *acc, float *out, int64_t n, cudaStr
 
 // Projector type 5 (branchless distance-driven), CT.
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
-                int64_t nproj, const float *img, float *imgT, float *y, int cols, int rows, cudaStream_t st);
+                int64_t nproj, const float *img, float *imgT, float *y, const Tuning &tn, cudaStream_t st);
+// The same projection with per-slice image boxes staged by TMA (8 columns per thread).
+bool bdd_fp_tma_supported(const Grid &g, const float *img, const float *imgT);
+int bdd_forward_tma(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
+                    int64_t nproj, const float *img, const float *imgT, float *y, cudaStream_t st);
+// Device error word of the bounded waits (1 after a wait ran out; reset when read), < 0 on failure.
+int take_device_error();
 int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
                  float *sens, int zrun, int rows, cudaStream_t st);
 

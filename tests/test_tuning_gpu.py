@@ -33,14 +33,23 @@ def test_bdd_every_shape_matches_oracle(cuda, name):
     y = rng.uniform(0.0, 2.0, g.rays(0))
     ref_fp = orc.bdd_forward(g, x, 0)
     ref_bp, ref_s = orc.bdd_backward(g, y, 0, sens=True)
-    for cols, zrun, rows in itertools.product([8, 16], [4, 8, 16], [4, 8]):
+    from omega_b200 import _native
+    shapes = [(c, z, r, 0) for c, z, r in itertools.product([8, 16], [4, 8, 16], [4, 8])]
+    shapes += [(8, z, 4, 1) for z in (4, 8, 16)]
+    fps = {}
+    for cols, zrun, rows, staged in shapes:
         o.tuning = {"bdd_fp_columns": cols, "bdd_bp_zrun": zrun, "bdd_fp_block_rows": rows,
-                    "bdd_bp_block_rows": rows}
+                    "bdd_bp_block_rows": rows, "bdd_fp_staged": staged}
         fp = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
         bp, s = o.backwardProject(_t(y, cuda), 0, sens=True)
         assert orc.rel_l2(fp, ref_fp) < TOL, (cols, rows, orc.rel_l2(fp, ref_fp))
         assert orc.rel_l2(bp.cpu().numpy(), ref_bp) < TOL, (zrun, rows, orc.rel_l2(bp.cpu().numpy(), ref_bp))
         assert orc.rel_l2(s.cpu().numpy(), ref_s) < TOL, (zrun, rows)
+        fps[(cols, rows, staged)] = fp
+    assert _native.call("omb_take_device_error") == 0
+    # staging the image boxes in shared memory changes where the voxels are
+    # read from, not the arithmetic
+    assert np.array_equal(fps[(8, 4, 1)].view(np.uint32), fps[(8, 4, 0)].view(np.uint32))
 
 
 def test_siddon_every_shape_matches_oracle(cuda):
