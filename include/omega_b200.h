@@ -242,6 +242,10 @@ typedef struct omb_tuning {
     int32_t bdd_fp_staged;           /* 0, 1 (default 1): type-5 forward projection with each CTA's
                                         per-slice image boxes staged in shared memory by TMA (applies
                                         with bdd_fp_columns = 8; needs Nx, Ny multiples of 4) */
+    int32_t bdd_bp_staged;           /* 0, 1 (default 1): type-5 backprojection with each CTA's
+                                        per-projection detector boxes staged in shared memory by TMA
+                                        (applies with bdd_bp_zrun = 8; needs a row count that is a
+                                        multiple of 4) */
 } omb_tuning;
 
 /*

@@ -437,7 +437,7 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
         if (mode != OMB_BP_FLOAT_ATOMIC)
             return set_error(OMB_ERR_UNSUPPORTED, "the type-5 backprojection is a gather; it has no fixed-point mode");
         return bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y, image, sens,
-                            h->tune.bdd_bp_z, h->tune.bdd_bp_rows, s);
+                            h->tune, s);
     }
     if (h->desc.bp_type == 4 && h->desc.modality == OMB_CT_PANEL) {
         if (mode != OMB_BP_FLOAT_ATOMIC)
@@ -624,7 +624,8 @@ static int tuning_from(const omb_tuning *in, Tuning &t) {
         return set_error(OMB_ERR_INVALID, "bdd block rows must be 4 or 8");
     if (!one_of(in->siddon_frame_layout, {0, 1})) return set_error(OMB_ERR_INVALID, "siddon_frame_layout must be 0 or 1");
     if (!one_of(in->siddon_fp_steps, {1, 2, 4})) return set_error(OMB_ERR_INVALID, "siddon_fp_steps must be 1, 2 or 4");
-    if (!one_of(in->bdd_fp_staged, {0, 1})) return set_error(OMB_ERR_INVALID, "bdd_fp_staged must be 0 or 1");
+    if (!one_of(in->bdd_fp_staged, {0, 1}) || !one_of(in->bdd_bp_staged, {0, 1}))
+        return set_error(OMB_ERR_INVALID, "bdd_fp_staged and bdd_bp_staged must be 0 or 1");
     t.siddon_blocks_per_sm = in->siddon_blocks_per_sm;
     t.siddon_frames = in->siddon_frames_per_walk;
     t.bdd_fp_cols = in->bdd_fp_columns;
@@ -634,6 +635,7 @@ static int tuning_from(const omb_tuning *in, Tuning &t) {
     t.siddon_layout = in->siddon_frame_layout;
     t.siddon_fp_steps = in->siddon_fp_steps;
     t.bdd_fp_staged = in->bdd_fp_staged;
+    t.bdd_bp_staged = in->bdd_bp_staged;
     return OMB_OK;
 }
 
@@ -648,6 +650,7 @@ static void tuning_to(const Tuning &t, omb_tuning *out) {
     out->siddon_frame_layout = t.siddon_layout;
     out->siddon_fp_steps = t.siddon_fp_steps;
     out->bdd_fp_staged = t.bdd_fp_staged;
+    out->bdd_bp_staged = t.bdd_bp_staged;
 }
 
 int omb_take_device_error(void) {
@@ -801,23 +804,24 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
     }
     if (e == cudaSuccess && st == OMB_OK && h->desc.bp_type == 5) {
         float best_ms = 3.4e38f;
-        for (int z : {4, 8, 16}) {
-            for (int rows : {4, 8}) {
-                h->tune = best;
-                h->tune.bdd_bp_z = z;
-                h->tune.bdd_bp_rows = rows;
-                const float b = timed(bwd);
-                if (b < 0.f) {
-                    st = -1;
-                    break;
-                }
-                if (b < best_ms) {
-                    best_ms = b;
-                    best.bdd_bp_z = z;
-                    best.bdd_bp_rows = rows;
-                }
+        // (voxels along z, warps per block, staged); the staged kernel has 8 voxels and 4 warps
+        const int shapes[7][3] = {{4, 4, 0}, {4, 8, 0}, {8, 4, 0}, {8, 8, 0}, {16, 4, 0}, {16, 8, 0}, {8, 4, 1}};
+        for (const auto &sh : shapes) {
+            h->tune = best;
+            h->tune.bdd_bp_z = sh[0];
+            h->tune.bdd_bp_rows = sh[1];
+            h->tune.bdd_bp_staged = sh[2];
+            const float b = timed(bwd);
+            if (b < 0.f) {
+                st = -1;
+                break;
             }
-            if (st != OMB_OK) break;
+            if (b < best_ms) {
+                best_ms = b;
+                best.bdd_bp_z = sh[0];
+                best.bdd_bp_rows = sh[1];
+                best.bdd_bp_staged = sh[2];
+            }
         }
     }
     h->tune = (e == cudaSuccess && st == OMB_OK) ? best : saved;

@@ -128,9 +128,6 @@ __global__ void k_transpose_xy(const float *__restrict__ in, float *__restrict__
 // computeGeom5 uses (omegatomo/projector/init.py:6-37).
 // ---------------------------------------------------------------------------
 
-// detector columns one thread's run of kBpZ voxels may cover before it takes
-// the per-voxel path (about 1.25 columns per voxel at magnification 2)
-__host__ __device__ constexpr int bp_slots(int kBpZ) { return kBpZ + kBpZ / 2 + (kBpZ < 16 ? 4 : 0); }
 
 // Voxel-driven backprojection, kBpZ voxels along z per thread.  For the flat
 // panels of this path (rows in the xy-plane, columns along z) the detector
@@ -317,9 +314,12 @@ int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc,
 }
 
 int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                 float *sens, int zrun, int rows, cudaStream_t st) {
+                 float *sens, const Tuning &tn, cudaStream_t st) {
     if (g.nz > 65535 * 4) return set_error(OMB_ERR_UNSUPPORTED, "too many slices");
-    switch (zrun) {
+    if (tn.bdd_bp_staged && tn.bdd_bp_z == 8 && bdd_bp_tma_supported(nr, y))
+        return bdd_backward_tma(g, pj, nr, nc, nproj, y, img, sens, st);
+    const int rows = tn.bdd_bp_rows;
+    switch (tn.bdd_bp_z) {
         case 4: launch_bp<4>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;
         case 16: launch_bp<16>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;
         default: launch_bp<8>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;

@@ -120,6 +120,10 @@ __device__ __forceinline__ float seg_sum(const Seg &s, const float *__restrict__
     return acc;
 }
 
+// detector columns one thread's run of kBpZ voxels may cover before it takes
+// the per-voxel path (about 1.25 columns per voxel at magnification 2)
+__host__ __device__ constexpr int bp_slots(int kBpZ) { return kBpZ + kBpZ / 2 + (kBpZ < 16 ? 4 : 0); }
+
 // seg_sum over a run staged in shared memory (plain loads, same arithmetic).
 __device__ __forceinline__ float seg_sum_shared(const Seg &s, const float *p) {
     float acc = fmaf(s.w2, p[s.o2], fmaf(s.w1, p[s.o1], s.w0 * p[0]));

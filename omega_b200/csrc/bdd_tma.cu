@@ -239,6 +239,227 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
         if (c < ncol) y[idx + (int64_t)c * nr] = temp[c] * kerroin;
 }
 
+// ---------------------------------------------------------------------------
+// Backprojection with the projection data staged by TMA.
+//
+// Same per-voxel arithmetic as k_bdd_bp<8, ...> (bdd.cu).  A CTA covers 32 x
+// 4 voxel columns and a run of kBpZ voxels along z; for projection p its
+// voxels' footprints lie in a box of detector rows x columns, found by
+// projecting the block's 8 corners (the projective map sends the box to the
+// convex hull of their images).  The box of projection p + kStages is loaded
+// with cp.async.bulk.tensor while projection p is processed.  Column sums of a
+// voxel column whose footprint leaves the box read global memory.
+// ---------------------------------------------------------------------------
+namespace bb {
+
+constexpr int kZ = 8;                              // voxels along z per thread
+constexpr int kThreads = 128;                      // 32 x 4 voxel columns
+constexpr int kSlots = bp_slots(kZ);               // prefix-sum slots per thread
+constexpr int kRW = 52;                            // detector rows of a box (multiple of 4)
+constexpr int kCW = kSlots + 4;                    // detector columns of a box
+constexpr int kStageFloats = (kRW * kCW + 31) / 32 * 32;  // 128-byte aligned stages
+constexpr int kStages = 4;
+
+struct Shared {
+    alignas(128) float box[kStages][kStageFloats];
+    alignas(8) uint64_t full[kStages];
+    int2 origin[kStages];  // (row, column) of the box's first element
+    float2 pref[kSlots][kThreads];
+};
+
+}  // namespace bb
+
+template <bool SENS, bool FULL>
+__global__ void k_bdd_bp_tma(const __grid_constant__ CUtensorMap map_y, Grid g, const BddProj *__restrict__ pj,
+                             int nr, int nc, int64_t nproj, const float *__restrict__ y, float *__restrict__ img,
+                             float *__restrict__ sens) {
+    using namespace bb;
+    constexpr int kBpZ = kZ;
+    __shared__ Shared sh;
+    const int tid = threadIdx.x + threadIdx.y * 32;
+    const int lane = threadIdx.x;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 4 + threadIdx.y;
+    const int kz0 = blockIdx.z * kBpZ;
+    const bool active = i < g.nx && j < g.ny && kz0 < g.nz;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bt::smem_u32(&sh.full[s])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    // corner `lane & 7` of the CTA's voxel block (edges of its voxels)
+    const float cx = g.bx + (float)((lane & 1) ? min((int)blockIdx.x * 32 + 32, g.nx) : (int)blockIdx.x * 32) * g.dx;
+    const float cy = g.by + (float)((lane & 2) ? min((int)blockIdx.y * 4 + 4, g.ny) : (int)blockIdx.y * 4) * g.dy;
+    const float cz = g.bz + (float)((lane & 4) ? min(kz0 + kBpZ, g.nz) : kz0) * g.dz;
+    // loads the box of projection pn into stage s (a whole warp; lane 0 issues)
+    auto produce = [&](int64_t pn, int s) {
+        const BddProj P = pj[pn];
+        const float den = 1.f / fmaf(P.c[0], cx, fmaf(P.c[1], cy, fmaf(P.c[2], cz, 1.f)));
+        float u = fmaf(P.au[0], cx, fmaf(P.au[1], cy, fmaf(P.au[2], cz, P.au0))) * den;
+        float v = fmaf(P.av[0], cx, fmaf(P.av[1], cy, fmaf(P.av[2], cz, P.av0))) * den;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            u = fminf(u, __shfl_xor_sync(0xffffffffu, u, o));
+            v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        }
+        if (lane == 0) {
+            int r = (int)floorf(fmaxf(u - 1.f, 0.f));
+            r = min(r, nr - 1) & ~3;
+            int c = (int)floorf(fmaxf(v - 1.f, 0.f));
+            c = min(c, nc - 1);
+            sh.origin[s] = make_int2(r, c);
+            const uint32_t bar = bt::smem_u32(&sh.full[s]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
+                         "r"((uint32_t)(kRW * kCW * sizeof(float)))
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+                "%4}], [%5];\n" ::"r"(bt::smem_u32(sh.box[s])),
+                "l"(reinterpret_cast<uint64_t>(&map_y)), "r"(r), "r"(c), "r"((int)pn), "r"(bar)
+                : "memory");
+        }
+    };
+    if (threadIdx.y == 0)
+        for (int s = 0; s < kStages && s < nproj; ++s) produce(s, s);
+
+    const int nzt = FULL ? kBpZ : min(kBpZ, g.nz - kz0);
+    const float qx = fmaf((float)i, g.dx, g.bx + 0.5f * g.dx);
+    const float qy = fmaf((float)j, g.dy, g.by + 0.5f * g.dy);
+    const float qz0 = fmaf((float)kz0, g.dz, g.bz + 0.5f * g.dz);
+    const float hx = 0.5f * g.dx, hy = 0.5f * g.dy, hz = 0.5f * g.dz;
+    const float fnr = (float)nr, fnc = (float)nc;
+    float temp[kBpZ], wsum[kBpZ];
+#pragma unroll
+    for (int t = 0; t < kBpZ; ++t) {
+        temp[t] = 0.f;
+        wsum[t] = 0.f;
+    }
+    int tries = bt::kWaitTries;
+    for (int64_t p = 0; p < nproj; ++p) {
+        const int s = (int)(p % kStages);
+        if (!bt::mbar_wait(bt::smem_u32(&sh.full[s]), (uint32_t)((p / kStages) & 1), tries)) {
+            atomicExch(&g_device_error, 1);
+            tries = bt::kWaitTriesAfterFailure;
+        }
+        do {
+            if (!active) break;
+            const BddProj P = pj[p];
+            float lx, ly, rx, ry;
+            const float sgn = P.spos ? 1.f : -1.f;
+            if (P.ysl) {
+                lx = qx - sgn * hx; rx = qx + sgn * hx; ly = qy; ry = qy;
+            } else {
+                lx = qx; rx = qx; ly = qy + sgn * hy; ry = qy - sgn * hy;
+            }
+            const float dl = 1.f / fmaf(P.c[0], lx, fmaf(P.c[1], ly, fmaf(P.c[2], qz0, 1.f)));
+            const float dr = 1.f / fmaf(P.c[0], rx, fmaf(P.c[1], ry, fmaf(P.c[2], qz0, 1.f)));
+            const float ul = fmaf(P.au[0], lx, fmaf(P.au[1], ly, fmaf(P.au[2], qz0, P.au0))) * dl;
+            const float ur = fmaf(P.au[0], rx, fmaf(P.au[1], ry, fmaf(P.au[2], qz0, P.au0))) * dr;
+            const float ua = fmaxf(fminf(ul, ur), 0.f), ub = fminf(fmaxf(ul, ur), fnr);
+            if (!(ub > ua)) break;
+            const int r0 = (int)ua;
+            const Seg seg = make_seg(ua, ub, r0, min((int)ceilf(ub), nr) - 1 - r0);
+            const float vl0 = fmaf(P.av[0], lx, fmaf(P.av[1], ly, fmaf(P.av[2], qz0 - hz, P.av0))) * dl;
+            const float vr0 = fmaf(P.av[0], rx, fmaf(P.av[1], ry, fmaf(P.av[2], qz0 + hz, P.av0))) * dr;
+            const float svl = P.av[2] * g.dz * dl, svr = P.av[2] * g.dz * dr;
+            const float tl = (float)(nzt - 1);
+            const float vmin = fminf(fminf(vl0, vr0), fminf(fmaf(tl, svl, vl0), fmaf(tl, svr, vr0)));
+            const float vmax = fmaxf(fmaxf(vl0, vr0), fmaxf(fmaf(tl, svl, vl0), fmaf(tl, svr, vr0)));
+            const float vA = fmaxf(vmin, 0.f);
+            const float vB = fminf(vmax, fnc);
+            if (!(vB > vA)) break;
+            const float vx = qx - P.s[0], vy = qy - P.s[1];
+            const float axy = vx * vx + vy * vy;
+            const float kscale = P.ysl ? __fdividef(g.dy, fabsf(vy)) : __fdividef(g.dx, fabsf(vx));
+            const int cA = (int)vA;
+            const int ncols = min((int)ceilf(vB), nc) - cA;
+            const int2 o = sh.origin[s];
+            const bool staged = r0 >= o.x && r0 + seg.n < o.x + kRW && cA >= o.y && cA + ncols <= o.y + kCW;
+            if (ncols <= kSlots) {
+                float acc = 0.f;
+                if (staged && seg.n <= 2) {
+                    const float *q = sh.box[s] + (cA - o.y) * kRW + (r0 - o.x);
+#pragma unroll 4
+                    for (int m = 0; m < ncols; ++m) {
+                        const float rs = fmaf(seg.w2, q[seg.o2], fmaf(seg.w1, q[seg.o1], seg.w0 * q[0]));
+                        sh.pref[m][tid] = make_float2(acc, rs);
+                        acc += rs;
+                        q += kRW;
+                    }
+                } else {
+                    const float *yp = y + p * (int64_t)nr * nc + r0;
+#pragma unroll 4
+                    for (int m = 0; m < ncols; ++m) {
+                        const float rs = seg_sum(seg, yp + (int64_t)(cA + m) * nr);
+                        sh.pref[m][tid] = make_float2(acc, rs);
+                        acc += rs;
+                    }
+                }
+                const float fA = (float)cA;
+                const int mmax = ncols - 1;
+                // inside the panel the clamps to [vA, vB] below are identities
+                const bool inside = vmin >= 0.f && vmax <= fnc;
+#pragma unroll
+                for (int t = 0; t < kBpZ; ++t) {
+                    if (FULL || t < nzt) {
+                        const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
+                        const float lo = fminf(vlt, vrt), hi = fmaxf(vlt, vrt);
+                        const float qa = (inside ? lo : fminf(fmaxf(lo, vA), vB)) - fA;
+                        const float qb = (inside ? hi : fminf(fmaxf(hi, vA), vB)) - fA;
+                        const int ma = min((int)qa, mmax), mb = min((int)qb, mmax);
+                        const float2 ea = sh.pref[ma][tid], eb = sh.pref[mb][tid];
+                        const float apu = fmaf(qb - (float)mb, eb.y, eb.x) - fmaf(qa - (float)ma, ea.y, ea.x);
+                        if (apu != 0.f) {
+                            const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
+                            const float q2 = fmaf(vz, vz, axy);
+                            const float ker = kscale * (q2 * rsqrtf(q2));
+                            temp[t] = fmaf(apu, ker, temp[t]);
+                            if (SENS) wsum[t] += ker;
+                        }
+                    }
+                }
+            } else {
+                const float *yp = y + p * (int64_t)nr * nc + r0;
+#pragma unroll
+                for (int t = 0; t < kBpZ; ++t) {
+                    const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
+                    const float va = fmaxf(fminf(vlt, vrt), 0.f), vb = fminf(fmaxf(vlt, vrt), fnc);
+                    if ((FULL || t < nzt) && vb > va) {
+                        const int c0 = (int)va, c1 = min((int)ceilf(vb), nc) - 1;
+                        float apu = 0.f;
+                        for (int c = c0; c <= c1; ++c) {
+                            const float ov = fminf(vb, (float)(c + 1)) - fmaxf(va, (float)c);
+                            apu = fmaf(ov, seg_sum(seg, yp + (int64_t)c * nr), apu);
+                        }
+                        if (apu != 0.f) {
+                            const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
+                            const float q2 = fmaf(vz, vz, axy);
+                            const float ker = kscale * (q2 * rsqrtf(q2));
+                            temp[t] = fmaf(apu, ker, temp[t]);
+                            if (SENS) wsum[t] += ker;
+                        }
+                    }
+                }
+            }
+        } while (false);
+        __syncthreads();  // stage s is free again
+        if (threadIdx.y == (int)(p % 4) && p + kStages < nproj) produce(p + kStages, s);
+    }
+    if (!active) return;
+    int64_t n = i + (int64_t)j * g.nx + (int64_t)kz0 * g.nx * g.ny;
+#pragma unroll
+    for (int t = 0; t < kBpZ; ++t) {
+        if (t < nzt) {
+            img[n] = temp[t];
+            if (SENS) sens[n] = wsum[t];
+        }
+        n += (int64_t)g.nx * g.ny;
+    }
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda).
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -286,6 +507,38 @@ int bdd_forward_tma(const Grid &g, const float *xy, const float *uv, int nr, int
     dim3 grid((nr + 31) / 32, (groups + bt::kRB - 1) / bt::kRB, (unsigned)nproj);
     k_bdd_fp_tma<<<grid, block, 0, st>>>(m_img, m_imgT, g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y);
     OMB_LAUNCH_CHECK("type-5 TMA forward launch");
+    return OMB_OK;
+}
+
+bool bdd_bp_tma_supported(int nr, const float *y) {
+    return nr % 4 == 0 && ((uintptr_t)y & 15) == 0 && encode_fn() != nullptr;
+}
+
+int bdd_backward_tma(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
+                     float *sens, cudaStream_t st) {
+    if (nproj <= 0) return OMB_OK;
+    auto fn = encode_fn();
+    CUtensorMap m_y;
+    const cuuint64_t dims[3] = {(cuuint64_t)nr, (cuuint64_t)nc, (cuuint64_t)nproj};
+    const cuuint64_t strides[2] = {(cuuint64_t)nr * sizeof(float), (cuuint64_t)nr * nc * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)bb::kRW, (cuuint32_t)bb::kCW, 1u};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    if (!fn || fn(&m_y, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(y), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return set_error(OMB_ERR_CUDA, "cuTensorMapEncodeTiled failed for the type-5 projection map");
+    dim3 block(32, 4);
+    dim3 grid((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + bb::kZ - 1) / bb::kZ);
+    const bool full = g.nz % bb::kZ == 0;
+    if (sens && full)
+        k_bdd_bp_tma<true, true><<<grid, block, 0, st>>>(m_y, g, pj, nr, nc, nproj, y, img, sens);
+    else if (sens)
+        k_bdd_bp_tma<true, false><<<grid, block, 0, st>>>(m_y, g, pj, nr, nc, nproj, y, img, sens);
+    else if (full)
+        k_bdd_bp_tma<false, true><<<grid, block, 0, st>>>(m_y, g, pj, nr, nc, nproj, y, img, sens);
+    else
+        k_bdd_bp_tma<false, false><<<grid, block, 0, st>>>(m_y, g, pj, nr, nc, nproj, y, img, sens);
+    OMB_LAUNCH_CHECK("type-5 TMA backward launch");
     return OMB_OK;
 }
 

@@ -36,20 +36,23 @@ def test_bdd_every_shape_matches_oracle(cuda, name):
     from omega_b200 import _native
     shapes = [(c, z, r, 0) for c, z, r in itertools.product([8, 16], [4, 8, 16], [4, 8])]
     shapes += [(8, z, 4, 1) for z in (4, 8, 16)]
-    fps = {}
+    fps, bps = {}, {}
     for cols, zrun, rows, staged in shapes:
         o.tuning = {"bdd_fp_columns": cols, "bdd_bp_zrun": zrun, "bdd_fp_block_rows": rows,
-                    "bdd_bp_block_rows": rows, "bdd_fp_staged": staged}
+                    "bdd_bp_block_rows": rows, "bdd_fp_staged": staged, "bdd_bp_staged": staged}
         fp = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
         bp, s = o.backwardProject(_t(y, cuda), 0, sens=True)
         assert orc.rel_l2(fp, ref_fp) < TOL, (cols, rows, orc.rel_l2(fp, ref_fp))
         assert orc.rel_l2(bp.cpu().numpy(), ref_bp) < TOL, (zrun, rows, orc.rel_l2(bp.cpu().numpy(), ref_bp))
         assert orc.rel_l2(s.cpu().numpy(), ref_s) < TOL, (zrun, rows)
         fps[(cols, rows, staged)] = fp
+        bps[(zrun, rows, staged)] = (bp.cpu().numpy(), s.cpu().numpy())
     assert _native.call("omb_take_device_error") == 0
-    # staging the image boxes in shared memory changes where the voxels are
-    # read from, not the arithmetic
+    # staging the image / detector boxes in shared memory changes where the
+    # data are read from, not the arithmetic
     assert np.array_equal(fps[(8, 4, 1)].view(np.uint32), fps[(8, 4, 0)].view(np.uint32))
+    for a, b in zip(bps[(8, 4, 1)], bps[(8, 4, 0)]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
 def test_siddon_every_shape_matches_oracle(cuda):
