@@ -50,9 +50,22 @@ sys.path.insert(0, ROOT)
 # DRAM bytes (read + write) per launch from ncu captures, scaled to the full
 # workload by rays; see profiles/ for the captures they come from.
 PROFILED_TRAFFIC = {
-    # profiles/bdd_cbct_capture.md (36-view capture x 10)
-    ("cbct", "bdd_fp"): 5.88e9,
-    ("cbct", "bdd_bp"): 3.51e8,
+    # DRAM bytes read + written per launch, from the ncu captures summarised
+    # in profiles/: bdd_cbct_capture.md (36-view capture x 10) and
+    # siddon_dynpet_launches.md (full-size capture)
+    ("cbct", "bdd_fp"): 9.40e9,
+    ("cbct", "bdd_bp"): 3.87e8,
+    ("dynpet", "siddon_fp"): 3.55e8,
+    ("dynpet", "siddon_bp"): 4.83e8,
+}
+# What bounds each kernel instead of HBM (the volumes and images are
+# L2-resident, so DRAM moves a few per cent of the cache-less bytes): the
+# issue-active and SM-throughput percentages of the same ncu captures.
+PROFILED_LIMITER = {
+    ("cbct", "bdd_fp"): {"issue_active_pct": 83.0, "sm_throughput_pct": 79.7, "dram_pct": 5.2},
+    ("cbct", "bdd_bp"): {"issue_active_pct": 74.2, "sm_throughput_pct": 73.8, "dram_pct": 0.2},
+    ("dynpet", "siddon_fp"): {"issue_active_pct": 42.5, "l1tex_pct": 58.2, "dram_pct": 0.7},
+    ("dynpet", "siddon_bp"): {"issue_active_pct": 46.4, "lts_pct": 65.7, "dram_pct": 1.0},
 }
 FALLBACK_HBM_GBS = 6650.0
 
@@ -347,7 +360,7 @@ def roofline(name, nbytes, duration, traffic_key):
     achieved = nbytes / duration / 1e9
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": src, "algorithmic_bytes": nbytes,
-            "traffic": PROFILED_TRAFFIC.get(traffic_key)}
+            "traffic": PROFILED_TRAFFIC.get(traffic_key), "limiter": PROFILED_LIMITER.get(traffic_key)}
 
 
 # ---------------------------------------------------------------------------
