@@ -264,6 +264,24 @@ int omb_set_read_precision(omb_handle *h, int32_t mode, int32_t max_frames);
 int omb_get_tuning(const omb_handle *h, omb_tuning *out);
 
 /*
+ * PET corrections of the projector type-1 forward and backward projections
+ * (the reference's NORM, SCATTER, ATNM and ATN kernel options,
+ * projectorType123.cl:373-376, 975-987; CPU projector
+ * projector_functions.h:1754-1832).  meas_weights: one multiplicative factor
+ * per measurement of all subsets in subset order (normalisation x
+ * multiplicative scatter x LOR attenuation factors, premultiplied), shared by
+ * a measurement's TOF bins; atten_image: attenuation coefficients (1/mm), one
+ * per voxel, whose line integral along each ray gives the factor
+ * exp(-sum mu x length).  Each ray's factor multiplies its normalisation
+ * (1/L x global_factor), so it scales forward projections, backprojections
+ * and sensitivity images alike.  Either pointer may be NULL (that correction
+ * off); host or device memory, copied into the handle.  Other projector types
+ * return OMB_ERR_UNSUPPORTED while corrections are set.
+ */
+int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weights, const float *atten_image,
+                        int64_t n_atten, void *stream);
+
+/*
  * Device error word of the kernels' bounded waits (TMA and tensor-core
  * pipelines): 0 when no wait ran out since the last call, 1 when one did (the
  * results of that launch are invalid); reading it resets it.  < 0 if the

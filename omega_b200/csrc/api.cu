@@ -46,6 +46,8 @@ struct omb_handle {
     int img16_frames = 0;                 // frames d_img16 holds
     float *d_ilv = nullptr;               // voxel-interleaved frame scratch (type-1 frame batches)
     int64_t ilv_floats = 0;               // its capacity
+    float *d_w = nullptr;                 // PET: multiplicative weight per measurement (all subsets), or NULL
+    float *d_mu = nullptr;                // PET: attenuation image, or NULL
     // Buffers replaced by larger ones.  They are freed only with the handle:
     // a CUDA graph captured earlier may still address them.
     std::vector<void *> retired;
@@ -213,6 +215,8 @@ static int ray_set(const omb_handle *h, int32_t subset, RaySet &rs) {
         rs.n_proj = subset < 0 ? d.n_proj : h->n_meas[subset + 1] - h->n_meas[subset];
         rs.m_size = rs.n_proj * nbin;
     }
+    rs.w = h->d_w ? h->d_w + (meas_level ? h->n_meas[subset] : rs.proj0 * nbin) : nullptr;
+    rs.mu = h->d_mu;
     return OMB_OK;
 }
 
@@ -251,6 +255,7 @@ static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cud
         f.img_stride = h->n_img;
     }
     if (h->desc.fp_type == 4) {
+        if (rs.w || rs.mu) return set_error(OMB_ERR_UNSUPPORTED, "PET corrections are built for projector type 1");
         for (int fr = 0; fr < f.n; ++fr) {
             const int st = interp_forward(h->grid, rs, h->tof, h->desc.global_factor, h->desc.dL,
                                           f.img_in16 ? nullptr : f.img_in + fr * f.img_stride,
@@ -271,6 +276,7 @@ static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cud
 static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, float *sens, cudaStream_t s) {
     Frames f = f_in;
     if (h->desc.bp_type == 4) {
+        if (rs.w || rs.mu) return set_error(OMB_ERR_UNSUPPORTED, "PET corrections are built for projector type 1");
         for (int fr = 0; fr < f.n; ++fr) {
             const int st = interp_backward(h->grid, rs, h->tof, h->desc.global_factor, h->desc.dL,
                                            f.meas ? f.meas + fr * f.meas_stride : nullptr,
@@ -366,6 +372,8 @@ int omb_destroy(omb_handle *h) {
     cudaFree(h->d_bddp);
     cudaFree(h->d_img16);
     cudaFree(h->d_ilv);
+    cudaFree(h->d_w);
+    cudaFree(h->d_mu);
     for (void *p : h->retired) cudaFree(p);
     if (prev != h->device) cudaSetDevice(prev);
     delete h;
@@ -651,6 +659,35 @@ static void tuning_to(const Tuning &t, omb_tuning *out) {
     out->siddon_fp_steps = t.siddon_fp_steps;
     out->bdd_fp_staged = t.bdd_fp_staged;
     out->bdd_bp_staged = t.bdd_bp_staged;
+}
+
+int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weights, const float *atten_image,
+                        int64_t n_atten, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if ((meas_weights || atten_image) && h->desc.modality != OMB_PET_SINOGRAM)
+        return set_error(OMB_ERR_UNSUPPORTED, "corrections apply to PET data");
+    // rays of all subsets (TOF bins share their ray's weight)
+    const bool meas_level = h->desc.n_subsets > 1 && h->desc.subset_type < 8;
+    const int64_t total = meas_level ? h->n_meas[h->desc.n_subsets]
+                                     : h->desc.n_proj * (int64_t)h->desc.n_rows_d * h->desc.n_cols_d;
+    if (meas_weights && n_weights != total)
+        return set_error(OMB_ERR_INVALID, "meas_weights must hold one value per measurement of all subsets (" +
+                                              std::to_string(total) + ")");
+    if (atten_image && n_atten != h->n_img)
+        return set_error(OMB_ERR_INVALID, "atten_image must hold one value per voxel");
+    cudaStream_t s = (cudaStream_t)stream;
+    auto replace = [&](float *&dst, const float *src, int64_t n) -> int {
+        if (dst) h->retired.push_back(dst);  // a captured graph may still read it
+        dst = nullptr;
+        if (!src) return OMB_OK;
+        OMB_CUDA_TRY(cudaMalloc(&dst, (size_t)n * sizeof(float)));
+        OMB_CUDA_TRY(cudaMemcpyAsync(dst, src, (size_t)n * sizeof(float), cudaMemcpyDefault, s));
+        OMB_CUDA_TRY(cudaStreamSynchronize(s));
+        return OMB_OK;
+    };
+    int st = replace(h->d_w, meas_weights, n_weights);
+    if (st == OMB_OK) st = replace(h->d_mu, atten_image, n_atten);
+    return st;
 }
 
 int omb_take_device_error(void) {

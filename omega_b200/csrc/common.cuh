@@ -53,6 +53,8 @@ struct RaySet {
     int n_subsets;
     int cur_subset;
     float pitch_x, pitch_y;
+    const float *w;     // PET: multiplicative weight of each of the launch's rays, or NULL
+    const float *mu;    // PET: attenuation image (1/mm), or NULL
 };
 
 // One reconstruction of a batch projected by one persistent launch: its

@@ -28,11 +28,12 @@ __global__ void __launch_bounds__(kBlock) k_siddon_fp(Grid g, RaySet rs, Tof tof
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
         const Ray ray = load_ray(rs, r);
+        const float gfr = pet && (rs.w || rs.mu) ? gf * ray_correction(g, rs, ray, r) : gf;
         float ax[NB * FB];
 #pragma unroll
         for (int to = 0; to < NB * FB; ++to) ax[to] = 0.f;
         float temp = 0.f;
-        const bool ok = siddon_walk<NB, K>(g, ray, pet, gf, tof, temp,
+        const bool ok = siddon_walk<NB, K>(g, ray, pet, gfr, tof, temp,
                                         [&](int64_t ind, float ele, const float *w, float tsum) {
                                             if (NB == 1) {
 #pragma unroll
@@ -113,11 +114,12 @@ __global__ void __launch_bounds__(kBlock) k_siddon_fp_ilv(Grid g, RaySet rs, flo
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
         const Ray ray = load_ray(rs, r);
+        const float gfr = pet && (rs.w || rs.mu) ? gf * ray_correction(g, rs, ray, r) : gf;
         float ax[FB];
 #pragma unroll
         for (int f = 0; f < FB; ++f) ax[f] = 0.f;
         float temp = 0.f;
-        const bool ok = siddon_walk<1, K>(g, ray, pet, gf, tof, temp, [&](int64_t ind, float ele, const float *, float) {
+        const bool ok = siddon_walk<1, K>(g, ray, pet, gfr, tof, temp, [&](int64_t ind, float ele, const float *, float) {
 #pragma unroll
             for (int q = 0; q < FB / 4; ++q) {
                 const float4 t = __ldg(im + ind * (FB / 4) + q);
@@ -154,8 +156,9 @@ __global__ void __launch_bounds__(kBlock) k_siddon_bp_ilv(Grid g, RaySet rs, flo
         }
         if (!any) continue;  // adds only zeros
         const Ray ray = load_ray(rs, r);
+        const float gfr = pet && (rs.w || rs.mu) ? gf * ray_correction(g, rs, ray, r) : gf;
         float temp = 0.f;
-        siddon_walk<1>(g, ray, pet, gf, tof, temp, [&](int64_t ind, float ele, const float *, float) {
+        siddon_walk<1>(g, ray, pet, gfr, tof, temp, [&](int64_t ind, float ele, const float *, float) {
             const float le = ele * temp;
             if (isnan(le) || le == 0.f) return;
 #pragma unroll
@@ -198,8 +201,9 @@ __global__ void __launch_bounds__(kBlock) k_siddon_bp(Grid g, RaySet rs, Tof tof
         }
         if (!any) continue;  // adds only zeros
         const Ray ray = load_ray(rs, r);
+        const float gfr = pet && (rs.w || rs.mu) ? gf * ray_correction(g, rs, ray, r) : gf;
         float temp = 0.f;
-        siddon_walk<NB>(g, ray, pet, gf, tof, temp, [&](int64_t ind, float ele, const float *w, float tsum) {
+        siddon_walk<NB>(g, ray, pet, gfr, tof, temp, [&](int64_t ind, float ele, const float *w, float tsum) {
             const float le = ele * temp;
             if (NB == 1) {
                 if (!isnan(le)) {
@@ -247,8 +251,9 @@ __global__ void __launch_bounds__(kBlock) k_siddon_bp_fixed(Grid g, RaySet rs, T
         }
         if (!any) continue;
         const Ray ray = load_ray(rs, r);
+        const float gfr = pet && (rs.w || rs.mu) ? gf * ray_correction(g, rs, ray, r) : gf;
         float temp = 0.f;
-        siddon_walk<NB>(g, ray, pet, gf, tof, temp, [&](int64_t ind, float ele, const float *w, float tsum) {
+        siddon_walk<NB>(g, ray, pet, gfr, tof, temp, [&](int64_t ind, float ele, const float *w, float tsum) {
             const float le = ele * temp;
             float yax, val;
             if (NB == 1) {

@@ -272,7 +272,11 @@ __device__ __forceinline__ float tof_weights(const Tof &tof, float ddsign, float
 // waiting on one per voxel.  Steps past the ray's end are visited with length
 // 0 at the batch's first (valid) voxel.  The visits and their order are those
 // of K = 1.
-template <int NB, int K = 1, class Visit>
+//
+// FULL_ROW: a ray along an image row visits every voxel of the row at full
+// voxel length (the row attenuation sum of the reference's CPU projector,
+// projector_functions.h:1193-1205) instead of the part between its end points.
+template <int NB, int K = 1, bool FULL_ROW = false, class Visit>
 __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool pet, float global_factor,
                                             const Tof &tof, float &temp, Visit &&vis) {
     // Set-up in FP64 (end points are FP32, so their differences are exact);
@@ -350,7 +354,12 @@ __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool 
             D = (float)((d_d2 * (double)nrow) / copysign(2.0, along_x ? diff.y : diff.x));
             ddsign = sgnf(D);
         }
-        for (int ii = x1; ii <= x2; ++ii) {
+        // FULL_ROW: from voxel 0 to the row's end
+        for (int ii = FULL_ROW ? 0 : x1; ii <= (FULL_ROW ? nrow - 1 : x2); ++ii) {
+            if (FULL_ROW) {
+                vis(base + (int64_t)ii * stride, fd2, w, 1.f);
+                continue;
+            }
             float d_in = fd2;
             if (x1 > 0 && ii == x1) d_in = fT1;
             else if (x2 < nrow - 1 && ii == x2) d_in = fT2;
@@ -467,6 +476,23 @@ __device__ __forceinline__ bool siddon_walk(const Grid &g, const Ray &ray, bool 
         }
     }
     return true;
+}
+
+// Per-ray correction factor of PET rays (projector_functions.h:1754-1832):
+// the measurement's multiplicative weight (normalisation x scatter x LOR
+// attenuation, premultiplied by the caller) and, with an attenuation image,
+// exp(-sum of mu x intersection length) along the ray.  1 without either.
+__device__ __forceinline__ float ray_correction(const Grid &g, const RaySet &rs, const Ray &ray, int64_t r) {
+    float f = rs.w ? __ldg(rs.w + r) : 1.f;
+    if (rs.mu) {
+        const Tof tof1{1, 0.f, 0.f, 0.f, nullptr};
+        float jel = 0.f, t;
+        siddon_walk<1, 1, true>(g, ray, true, 1.f, tof1, t, [&](int64_t ind, float ele, const float *, float) {
+            jel += ele * -__ldg(rs.mu + ind);
+        });
+        f *= expf(jel);
+    }
+    return f;
 }
 
 }  // namespace omb

@@ -155,12 +155,19 @@ class projectorClass:
     useIndexBasedReconstruction = False
     SinM = np.empty(0, dtype=np.float32)
     verbose = 1
-    # Corrections (not on this path; must stay off)
+    # PET corrections applied inside the projector type-1 kernels
+    # (projectorType123.cl NORM / ATN / ATNM / SCATTER options):
+    # normalization and corrVector are per-measurement multipliers, vaimennus
+    # an attenuation image (1/mm, CTAttenuation) or per-measurement factors
     attenuation_correction = 0
     normalization_correction = 0
     randoms_correction = 0
     scatter_correction = 0
     additionalCorrection = 0
+    CTAttenuation = True
+    normalization = np.empty(0, dtype=np.float32)
+    vaimennus = np.empty(0, dtype=np.float32)
+    corrVector = np.empty(0, dtype=np.float32)
     maskFP = np.empty(0, dtype=np.uint8)
     maskBP = np.empty(0, dtype=np.uint8)
     # Execution flags of the reference surface (accepted for compatibility)
@@ -501,11 +508,68 @@ class projectorClass:
             raise ValueError("imageReadPrecision must be 'fp32' or 'bf16'")
         if self.imageReadPrecision == 'bf16':
             _native.call("omb_set_read_precision", h, _native.OMB_READ_BF16, int(self.maxFramesBF16))
+        self._set_corrections()
+        del keep
+
+    def _measurement_vectors(self):
+        """The per-measurement correction vectors in use (name -> array)."""
+        out = {}
+        if self.normalization_correction:
+            out['normalization'] = self.normalization
+        if self.attenuation_correction and not self.CTAttenuation:
+            out['vaimennus'] = self.vaimennus
+        if self.additionalCorrection:
+            out['corrVector'] = self.corrVector
+        return out
+
+    def _set_corrections(self):
+        """Uploads the PET corrections: the product of the per-measurement
+        multipliers (in subset order) and the attenuation image."""
+        if self.CT or not (self.normalization_correction or self.attenuation_correction or self.additionalCorrection):
+            return
+        total = int(np.ravel(self.nTotMeas)[-1])
+        w = None
+        for name, v in self._measurement_vectors().items():
+            v = np.asarray(v, dtype=np.float64).ravel(order='F')
+            if v.size != total:
+                raise ValueError(f'{name} must hold one value per measurement ({total}), got {v.size}')
+            w = v if w is None else w * v
+        mu = None
+        if self.attenuation_correction and self.CTAttenuation:
+            mu = np.asarray(self.vaimennus, dtype=np.float32).ravel(order='F')
+            n_img = int(np.ravel(self.N)[0])
+            if mu.size != n_img:
+                raise ValueError(f'vaimennus must be an image of {n_img} voxels, got {mu.size}')
+        keep = []
+
+        def ptr(a):
+            if a is None:
+                return None, 0
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            keep.append(a)
+            return a.ctypes.data_as(ctypes.c_void_p), a.size
+
+        wp, nw = ptr(w)
+        mp, nm = ptr(mu)
+        _native.call("omb_set_corrections", self._handle, wp, nw, mp, nm, None)
         del keep
 
     def _parse_inputs(self):
-        """Reorders SinM into subset order (prepass.py:282-355, static data)."""
-        if not (self.subsets > 1 and self.subsetType > 0) or self.SinM.size == 0:
+        """Reorders SinM and the per-measurement correction vectors into subset
+        order (prepass.py:282-472, static data)."""
+        if not (self.subsets > 1 and self.subsetType > 0):
+            return
+        if not getattr(self, '_corrections_ordered', False):
+            for name, v in self._measurement_vectors().items():
+                v = np.asarray(v, dtype=np.float32).ravel(order='F')
+                if self.subsetType >= 8:
+                    v = np.reshape(v, (self.nRowsD, self.nColsD, self.nProjections), order='F')[:, :, self.index]
+                    v = v.ravel(order='F')
+                elif v.size == np.size(self.index):
+                    v = v[self.index]
+                setattr(self, name, v)
+            self._corrections_ordered = True
+        if self.SinM.size == 0:
             return
         if self.Nt > 1:
             raise ValueError('dynamic data: reorder each frame with subsetMeasurements()')

@@ -55,6 +55,8 @@ class OracleGeom(ctypes.Structure):
         ("tof_centers", ctypes.POINTER(ctypes.c_double)),
         ("xy", ctypes.POINTER(ctypes.c_float)),
         ("z", ctypes.POINTER(ctypes.c_float)),
+        ("w", ctypes.POINTER(ctypes.c_double)),
+        ("mu", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -99,6 +101,9 @@ def ref_lib():
             u = ctypes.c_uint32
             getattr(L, name).argtypes = [ctypes.c_int, u, u, u, T, T, T, T, T, T, u, u, u, P, P, P, P, P, u, T, P, T,
                                          T, u]
+        P = ctypes.POINTER(ctypes.c_double)
+        L.ref_siddon_corr_d.argtypes = [ctypes.c_int, u, u, u] + [ctypes.c_double] * 6 + [u, u, u] + [P] * 5 + \
+            [u, ctypes.c_double, P, ctypes.c_double, ctypes.c_double, u, P, P, ctypes.c_int, P]
         _ref = L
     return _ref
 
@@ -128,6 +133,10 @@ class Geometry:
         # projector type 4: sampling length and the CT backprojection weight
         self.dL = float(o.dL)
         self.kerroin = float(np.ravel(o.kerroin)[0]) if np.size(o.kerroin) else 0.0
+        # PET corrections: weight per measurement of all subsets (subset
+        # order) and attenuation image, FP64; None when off
+        self.w = None
+        self.mu = None
 
     @property
     def n_img(self):
@@ -170,6 +179,15 @@ class Geometry:
         g.tof_centers = self.tofc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         g.xy = self.xy.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
         g.z = self.z.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        P = ctypes.POINTER(ctypes.c_double)
+        if self.w is not None:
+            w0 = int(self.n_meas[max(subset, 0)]) if self.meas_level() else \
+                (0 if subset < 0 else int(self.n_meas[subset]) * self.n_rows * self.n_cols)
+            self._w = np.ascontiguousarray(self.w, dtype=np.float64).ravel()[w0:w0 + g.m_size]
+            g.w = self._w.ctypes.data_as(P)
+        if self.mu is not None:
+            self._mu = np.ascontiguousarray(self.mu, dtype=np.float64).ravel()
+            g.mu = self._mu.ctypes.data_as(P)
         return g
 
 
@@ -262,6 +280,30 @@ def _ref_call(L, geom, inp, subset, fp, precision, threads, sens=False):
     tofc = geom.tofc.astype(T)
     fn(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, geom.n_rows, geom.n_cols, n1 - n0, p(xy), p(z),
        p(inp), p(out), p(s), geom.nbins, geom.sigma_x, p(tofc), geom.global_factor, geom.epps, int(threads))
+    return (out, s) if sens else out
+
+
+def ref_corrected(geom: Geometry, inp, subset, fp, norm=None, atten=None, ct_atten=True, scat=None, threads=0,
+                  sens=False):
+    """The reference CPU projector (FP64) with PET corrections: norm / scat
+    per measurement of the subset, atten an image (ct_atten) or per
+    measurement.  Whole-sinogram subsets only."""
+    L = ref_lib()
+    P = ctypes.POINTER(ctypes.c_double)
+    p = (lambda a: a.ctypes.data_as(P) if a is not None else None)
+    n0, n1 = (0, geom.n_proj) if subset < 0 else (int(geom.n_meas[subset]), int(geom.n_meas[subset + 1]))
+    xy = geom.xy.astype(np.float64)
+    z = np.ascontiguousarray(geom.z.astype(np.float64)[n0 * 2:n1 * 2])
+    inp = np.ascontiguousarray(inp, dtype=np.float64).ravel()
+    nmeas = geom.n_rows * geom.n_cols * (n1 - n0)
+    out = np.zeros(nmeas * geom.nbins if fp else geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    d = (lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel())
+    norm, atten, scat = d(norm), d(atten), d(scat)
+    tofc = geom.tofc.astype(np.float64)
+    L.ref_siddon_corr_d(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, geom.n_rows, geom.n_cols,
+                        n1 - n0, p(xy), p(z), p(inp), p(out), p(s), geom.nbins, geom.sigma_x, p(tofc),
+                        geom.global_factor, geom.epps, int(threads), p(norm), p(atten), 1 if ct_atten else 0, p(scat))
     return (out, s) if sens else out
 
 

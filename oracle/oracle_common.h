@@ -25,6 +25,10 @@ typedef struct oracle_geom {
     const double *tof_centers;
     const float *xy;
     const float *z;
+    /* PET corrections (projector_functions.h:1754-1832), NULL when off:
+     * multiplicative weight of each of the launch's rays, attenuation image */
+    const double *w;
+    const double *mu;
 } oracle_geom;
 
 typedef struct { double x, y, z; } v3;

@@ -17,7 +17,8 @@
 template <typename T>
 static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, T bx, T by, T bz, uint32_t n_rows,
                uint32_t n_cols, uint32_t n_proj, const T *xy, const T *z, T *input, T *output, T *sens, uint32_t nbins,
-               T sigma_x, T *tof_centers, T global_factor, T epps, uint32_t n_threads) {
+               T sigma_x, T *tof_centers, T global_factor, T epps, uint32_t n_threads, T *norm = nullptr,
+               T *atten = nullptr, int ct_atten = 1, T *scat = nullptr) {
     paramStruct<T> p;
     p.subsetType = 8;
     p.subsets = 1;
@@ -37,6 +38,14 @@ static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, 
     p.TOFCenters = tof_centers;
     p.noSensImage = sens == nullptr;
     p.nMeas = 0;
+    // corrections (normCoefs[lo], atten image or atten[lo], scatterCoefs[lo])
+    p.normalizationCorrection = norm != nullptr;
+    p.normCoefs = norm;
+    p.attenuationCorrection = atten != nullptr;
+    p.CTAttenuation = ct_atten != 0;
+    p.atten = atten;
+    p.scatterCorrectionMult = scat != nullptr;
+    p.scatterCoefs = scat;
     const int64_t n_meas = (int64_t)n_rows * n_cols * n_proj;
     projectorType123Implementation4<T>(p, n_meas, output, xy, z, input, false, false, (uint8_t)(fp ? 1 : 2), sens,
                                        nullptr, n_threads);
@@ -44,6 +53,16 @@ static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, 
 }
 
 extern "C" {
+/* With PET corrections: norm / scat per measurement of the call (NULL: off);
+ * atten: image (ct_atten != 0) or per measurement (ct_atten == 0), NULL: off. */
+int ref_siddon_corr_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx,
+                      double by, double bz, uint32_t n_rows, uint32_t n_cols, uint32_t n_proj, const double *xy,
+                      const double *z, double *input, double *output, double *sens, uint32_t nbins, double sigma_x,
+                      double *tof_centers, double global_factor, double epps, uint32_t n_threads, double *norm,
+                      double *atten, int ct_atten, double *scat) {
+    return run<double>(fp, nx, ny, nz, dx, dy, dz, bx, by, bz, n_rows, n_cols, n_proj, xy, z, input, output, sens,
+                       nbins, sigma_x, tof_centers, global_factor, epps, n_threads, norm, atten, ct_atten, scat);
+}
 int ref_siddon_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx, double by,
                  double bz, uint32_t n_rows, uint32_t n_cols, uint32_t n_proj, const double *xy, const double *z,
                  double *input, double *output, double *sens, uint32_t nbins, double sigma_x, double *tof_centers,

@@ -131,8 +131,11 @@ static int pre3d(const oracle_geom *g, double mx, double my, double mz, v3 s, v3
 /* Visitor: called per intersected voxel with the element length and the TOF weights. */
 typedef void (*visit_fn)(void *ctx, int64_t ind, double ele, const double *w, double tsum);
 
-/* Walks ray r; returns 0 when the ray is skipped.  *temp gets the ray normalisation. */
-static int walk(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, void *ctx) {
+/* Walks ray r; returns 0 when the ray is skipped.  *temp gets the ray
+ * normalisation.  full_row: a ray along an image row visits every voxel of
+ * the row at full length (the reference CPU projector's row attenuation sum,
+ * projector_functions.h:1193-1205). */
+static int walk_ex(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, void *ctx, int full_row) {
     v3 s, d;
     load_ray(g, r, &s, &d);
     const double mx = g->bx + (double)g->nx * g->dx;
@@ -180,6 +183,10 @@ static int walk(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, voi
          * (projector_functions.h:1641-1685): copysign for the starting side,
          * normalisation over a full voxel width, weights over the element. */
         if (tofon) { D = (d_d2 * (double)nrow) / copysign(2.0, along_x ? diff.y : diff.x); ddsign = sgn(D); }
+        if (full_row) {
+            for (int ii = 0; ii < nrow; ++ii) vis(ctx, base + (int64_t)ii * stride, d_d2, w, 1.0);
+            return 1;
+        }
         for (int ii = x1; ii <= x2; ++ii) {
             double d_in = d_d2;
             if (x1 > 0 && ii == x1) d_in = dT1;
@@ -247,6 +254,31 @@ static int walk(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, voi
     return 1;
 }
 
+static int walk(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, void *ctx) {
+    return walk_ex(g, r, temp, vis, ctx, 0);
+}
+
+typedef struct { const double *mu; double jel; } atn_ctx;
+
+static void atn_visit(void *c, int64_t ind, double ele, const double *w, double tsum) {
+    (void)w; (void)tsum;
+    atn_ctx *a = (atn_ctx *)c;
+    a->jel += ele * -a->mu[ind];
+}
+
+/* Correction factor of PET ray r: its weight times exp(-line integral of mu). */
+static double ray_corr(const oracle_geom *g, int64_t r) {
+    if (g->modality != 0) return 1.0;
+    double f = g->w ? g->w[r] : 1.0;
+    if (g->mu) {
+        atn_ctx a = {g->mu, 0.0};
+        double t;
+        walk_ex(g, r, &t, atn_visit, &a, 1);
+        f *= exp(a.jel);
+    }
+    return f;
+}
+
 typedef struct { const double *img; double ax[MAXB]; int nb; } fp_ctx;
 
 static void fp_visit(void *c, int64_t ind, double ele, const double *w, double tsum) {
@@ -267,7 +299,8 @@ int oracle_siddon_fp(const oracle_geom *g, const double *img, double *y) {
         for (int to = 0; to < g->nbins; ++to) f.ax[to] = 0.0;
         double temp = 0.0;
         int ok = walk(g, r, &temp, fp_visit, &f);
-        for (int to = 0; to < g->nbins; ++to) y[r + to * g->m_size] = ok ? f.ax[to] * temp : 0.0;
+        const double corr = ok ? ray_corr(g, r) : 0.0;
+        for (int to = 0; to < g->nbins; ++to) y[r + to * g->m_size] = ok ? f.ax[to] * temp * corr : 0.0;
     }
     return 0;
 }
@@ -312,7 +345,7 @@ int oracle_siddon_bp(const oracle_geom *g, const double *y, double *img, double 
         load_ray(g, r, &s, &d);
         double dxl = d.x - s.x, dyl = d.y - s.y, dzl = d.z - s.z;
         double L = sqrt(dxl * dxl + dyl * dyl + dzl * dzl);
-        b.temp = g->modality == 0 ? (1.0 / L) * g->global_factor : 1.0;
+        b.temp = g->modality == 0 ? (1.0 / L) * g->global_factor * ray_corr(g, r) : 1.0;
         walk(g, r, &temp, bp_visit, &b);
     }
     return 0;
