@@ -282,6 +282,16 @@ int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weig
                         int64_t n_atten, void *stream);
 
 /*
+ * Randoms (or additive scatter) estimate of the OSEM sub-iterations
+ * (omb_osem_subset, omb_osem_subset_frames): the ratio becomes
+ * y / (A x + epps + r) (computeForwardProject.h:46-71), r shared by a
+ * measurement's TOF bins and by the frames of a batch.  One value per
+ * measurement of all subsets in subset order; host or device memory, copied;
+ * NULL turns it off.
+ */
+int omb_set_randoms(omb_handle *h, const float *randoms, int64_t n, void *stream);
+
+/*
  * Device error word of the kernels' bounded waits (TMA and tensor-core
  * pipelines): 0 when no wait ran out since the last call, 1 when one did (the
  * results of that launch are invalid); reading it resets it.  < 0 if the

@@ -132,6 +132,7 @@ EXPORTS = [
     ("omb_power_workspace_bytes", ctypes.c_size_t, []),
     ("omb_set_read_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     ("omb_take_device_error", ctypes.c_int, []),
+    ("omb_set_randoms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     ("omb_set_corrections", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_void_p]),
     ("omb_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),

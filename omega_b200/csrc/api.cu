@@ -48,6 +48,7 @@ struct omb_handle {
     int64_t ilv_floats = 0;               // its capacity
     float *d_w = nullptr;                 // PET: multiplicative weight per measurement (all subsets), or NULL
     float *d_mu = nullptr;                // PET: attenuation image, or NULL
+    float *d_rand = nullptr;              // PET: randoms per measurement (all subsets) for the OSEM ratio, or NULL
     // Buffers replaced by larger ones.  They are freed only with the handle:
     // a CUDA graph captured earlier may still address them.
     std::vector<void *> retired;
@@ -220,6 +221,12 @@ static int ray_set(const omb_handle *h, int32_t subset, RaySet &rs) {
     return OMB_OK;
 }
 
+// First measurement (ray) of a subset in the all-subsets measurement order.
+static int64_t subset_ray0(const omb_handle *h, const RaySet &rs, int32_t subset) {
+    const bool meas_level = h->desc.n_subsets > 1 && h->desc.subset_type < 8;
+    return meas_level ? h->n_meas[subset] : rs.proj0 * (int64_t)h->desc.n_rows_d * h->desc.n_cols_d;
+}
+
 static Frames one_frame_fp(const omb_handle *h, const float *img, float *y, int64_t m) {
     Frames f{};
     f.n = 1;
@@ -374,6 +381,7 @@ int omb_destroy(omb_handle *h) {
     cudaFree(h->d_ilv);
     cudaFree(h->d_w);
     cudaFree(h->d_mu);
+    cudaFree(h->d_rand);
     for (void *p : h->retired) cudaFree(p);
     if (prev != h->device) cudaSetDevice(prev);
     delete h;
@@ -536,7 +544,11 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     const int64_t m = rs.m_size * h->desc.tof_bins;
     st = rays_forward(h, rs, one_frame_fp(h, image, work_meas, rs.m_size), s);
     if (st != OMB_OK) return st;
-    st = osem_ratio(y_subset, work_meas, m, eps, s);
+    if (h->d_rand)
+        st = osem_ratio_randoms(y_subset, m, work_meas, m, m, 1, h->d_rand + subset_ray0(h, rs, subset), rs.m_size,
+                                eps, s);
+    else
+        st = osem_ratio(y_subset, work_meas, m, eps, s);
     if (st != OMB_OK) return st;
     OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
     st = rays_backward(h, rs, one_frame_bp(h, work_meas, work_img, rs.m_size), nullptr, s);
@@ -571,7 +583,11 @@ int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, floa
     f.meas_stride = m;
     st = rays_forward(h, rs, f, s);
     if (st != OMB_OK) return st;
-    st = osem_ratio_frames(y_subset, y_stride, work_meas, m, m, n_frames, eps, s);
+    if (h->d_rand)
+        st = osem_ratio_randoms(y_subset, y_stride, work_meas, m, m, n_frames, h->d_rand + subset_ray0(h, rs, subset),
+                                rs.m_size, eps, s);
+    else
+        st = osem_ratio_frames(y_subset, y_stride, work_meas, m, m, n_frames, eps, s);
     if (st != OMB_OK) return st;
     OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, (size_t)n_frames * h->n_img * sizeof(float), s));
     Frames b{};
@@ -688,6 +704,25 @@ int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weig
     int st = replace(h->d_w, meas_weights, n_weights);
     if (st == OMB_OK) st = replace(h->d_mu, atten_image, n_atten);
     return st;
+}
+
+int omb_set_randoms(omb_handle *h, const float *randoms, int64_t n, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (randoms && h->desc.modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_UNSUPPORTED, "randoms apply to PET data");
+    const bool meas_level = h->desc.n_subsets > 1 && h->desc.subset_type < 8;
+    const int64_t total = meas_level ? h->n_meas[h->desc.n_subsets]
+                                     : h->desc.n_proj * (int64_t)h->desc.n_rows_d * h->desc.n_cols_d;
+    if (randoms && n != total)
+        return set_error(OMB_ERR_INVALID, "randoms must hold one value per measurement of all subsets (" +
+                                              std::to_string(total) + ")");
+    if (h->d_rand) h->retired.push_back(h->d_rand);
+    h->d_rand = nullptr;
+    if (!randoms) return OMB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    OMB_CUDA_TRY(cudaMalloc(&h->d_rand, (size_t)n * sizeof(float)));
+    OMB_CUDA_TRY(cudaMemcpyAsync(h->d_rand, randoms, (size_t)n * sizeof(float), cudaMemcpyDefault, s));
+    OMB_CUDA_TRY(cudaStreamSynchronize(s));
+    return OMB_OK;
 }
 
 int omb_take_device_error(void) {

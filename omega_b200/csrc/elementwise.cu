@@ -47,6 +47,31 @@ __global__ void k_clamp_min(float *__restrict__ x, int64_t n, float lo) {
 }
 
 // Frame batches: blockIdx.y selects the frame.
+// With randoms (computeForwardProject.h:46-71): input = fp + epps + r, the
+// ray's randoms shared by its TOF bins (bin stride n_rays).
+__global__ void k_osem_ratio_randoms(const float *__restrict__ y, int64_t y_stride, float *__restrict__ fp,
+                                     int64_t fp_stride, int64_t n, const float *__restrict__ rnd, int64_t n_rays,
+                                     float epps) {
+    const float *yf = y + blockIdx.y * y_stride;
+    float *ff = fp + blockIdx.y * fp_stride;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float r = __ldg(yf + i) / ((ff[i] + epps) + __ldg(rnd + i % n_rays));
+        if (isnan(r) || isinf(r)) r = epps;
+        ff[i] = r;
+    }
+}
+
+int osem_ratio_randoms(const float *y, int64_t y_stride, float *fp, int64_t fp_stride, int64_t n, int frames,
+                       const float *rnd, int64_t n_rays, float epps, cudaStream_t st) {
+    if (n <= 0 || frames <= 0) return OMB_OK;
+    if (frames > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 frames");
+    dim3 grid((grid_for(n, 4) + frames - 1) / frames + 1, frames);
+    k_osem_ratio_randoms<<<grid, kBlock, 0, st>>>(y, y_stride, fp, fp_stride, n, rnd, n_rays, epps);
+    OMB_LAUNCH_CHECK("osem ratio launch");
+    return OMB_OK;
+}
+
 __global__ void k_osem_ratio_frames(const float *__restrict__ y, int64_t y_stride, float *__restrict__ fp,
                                     int64_t fp_stride, int64_t n, float epps) {
     const float *yf = y + blockIdx.y * y_stride;

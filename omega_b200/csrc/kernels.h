@@ -55,6 +55,9 @@ int normalize_into(float *x, const float *b, int64_t n, const double *dots, cuda
 
 // Elementwise steps of the subset updates.
 int osem_ratio(const float *y, float *fp, int64_t n, float epps, cudaStream_t st);
+// y / (fp + epps + randoms[i % n_rays]) for `frames` frames sharing the randoms
+int osem_ratio_randoms(const float *y, int64_t y_stride, float *fp, int64_t fp_stride, int64_t n, int frames,
+                       const float *rnd, int64_t n_rays, float epps, cudaStream_t st);
 int em_update(float *img, const float *sens, const float *rhs, int64_t n, float epps, cudaStream_t st);
 int clamp_min(float *x, int64_t n, float lo, cudaStream_t st);
 int osem_ratio_frames(const float *y, int64_t y_stride, float *fp, int64_t fp_stride, int64_t n, int frames,

@@ -168,6 +168,9 @@ class projectorClass:
     normalization = np.empty(0, dtype=np.float32)
     vaimennus = np.empty(0, dtype=np.float32)
     corrVector = np.empty(0, dtype=np.float32)
+    # randoms (or additive scatter) added to the forward projection of the
+    # OSEM sub-iterations (randoms_correction), one value per measurement
+    SinDelayed = np.empty(0, dtype=np.float32)
     maskFP = np.empty(0, dtype=np.uint8)
     maskBP = np.empty(0, dtype=np.uint8)
     # Execution flags of the reference surface (accepted for compatibility)
@@ -524,10 +527,15 @@ class projectorClass:
 
     def _set_corrections(self):
         """Uploads the PET corrections: the product of the per-measurement
-        multipliers (in subset order) and the attenuation image."""
+        multipliers (in subset order), the attenuation image and the randoms."""
+        total = int(np.ravel(self.nTotMeas)[-1])
+        if self.randoms_correction and not self.CT:
+            r = np.ascontiguousarray(np.asarray(self.SinDelayed, dtype=np.float32).ravel(order='F'))
+            if r.size != total:
+                raise ValueError(f'SinDelayed must hold one value per measurement ({total}), got {r.size}')
+            _native.call("omb_set_randoms", self._handle, r.ctypes.data_as(ctypes.c_void_p), r.size, None)
         if self.CT or not (self.normalization_correction or self.attenuation_correction or self.additionalCorrection):
             return
-        total = int(np.ravel(self.nTotMeas)[-1])
         w = None
         for name, v in self._measurement_vectors().items():
             v = np.asarray(v, dtype=np.float64).ravel(order='F')
@@ -560,7 +568,10 @@ class projectorClass:
         if not (self.subsets > 1 and self.subsetType > 0):
             return
         if not getattr(self, '_corrections_ordered', False):
-            for name, v in self._measurement_vectors().items():
+            vecs = dict(self._measurement_vectors())
+            if self.randoms_correction:
+                vecs['SinDelayed'] = self.SinDelayed
+            for name, v in vecs.items():
                 v = np.asarray(v, dtype=np.float32).ravel(order='F')
                 if self.subsetType >= 8:
                     v = np.reshape(v, (self.nRowsD, self.nColsD, self.nProjections), order='F')[:, :, self.index]

@@ -220,9 +220,11 @@ def intersections(geom: Geometry, subset):
     return int(lib().oracle_siddon_count(ctypes.byref(g)))
 
 
-def osem(geom: Geometry, y_subsets, x0, n_iter, forward=None, backward=None):
+def osem(geom: Geometry, y_subsets, x0, n_iter, forward=None, backward=None, randoms=None):
     """Restated OSEM loop in FP64; returns the image after n_iter iterations.
-    The projector pair defaults to the Siddon restatement (type 1)."""
+    The projector pair defaults to the Siddon restatement (type 1).
+    randoms: per subset, added to the forward projection before the ratio
+    (computeForwardProject.h:46-71), tiled over TOF bins."""
     fwd = forward or globals()["forward"]
     bwd = backward or globals()["backward"]
     x = np.asarray(x0, dtype=np.float64).copy()
@@ -234,6 +236,8 @@ def osem(geom: Geometry, y_subsets, x0, n_iter, forward=None, backward=None):
     for _ in range(n_iter):
         for s in range(geom.n_subsets):
             fp = fwd(geom, x, s) + eps
+            if randoms is not None:
+                fp = fp + np.tile(np.asarray(randoms[s], dtype=np.float64), geom.nbins)
             with np.errstate(divide="ignore", invalid="ignore"):
                 r = np.asarray(y_subsets[s], dtype=np.float64) / fp
             r[~np.isfinite(r)] = eps
