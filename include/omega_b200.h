@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define OMB_ABI_VERSION 1
+#define OMB_ABI_VERSION 2
 
 typedef enum omb_status {
     OMB_OK = 0,
@@ -48,7 +48,13 @@ typedef enum omb_status {
 
 typedef enum omb_modality {
     OMB_PET_SINOGRAM = 0, /* PET sinogram: xy = (Ndist*Nang) x [xs, ys, xd, yd]; z = nProj x [zs, zd] */
-    OMB_CT_PANEL = 1      /* CT flat panel: xy = nProj x [sx, sy, sz, dx, dy, dz]; z = nProj x [ux*pitchX, uy*pitchX] */
+    OMB_CT_PANEL = 1,     /* CT flat panel: xy = nProj x [sx, sy, sz, dx, dy, dz]; z = nProj x [ux*pitchX, uy*pitchX] */
+    OMB_PET_LISTMODE = 2, /* PET list-mode events (getDetectorCoordinatesListmode, general_opencl_functions.h:
+                             1304-1320): xy = events x [xs, ys, zs, xd, yd, zd] in subset order, z unused (n_z 0
+                             allowed); n_proj = events, n_rows_d = n_cols_d = 1, n_meas = cumulative events */
+    OMB_PET_INDEXED = 3   /* PET index-based events (general_opencl_functions.h:1277-1301): xy = crystal table
+                             [x, y] per transaxial detector, z = axial positions; per event the detector index
+                             pairs tr_index[2e..2e+1] and ax_index[2e..2e+1]; sizes as OMB_PET_LISTMODE */
 } omb_modality;
 
 typedef enum omb_read_precision {
@@ -100,6 +106,8 @@ typedef struct omb_geometry_desc {
     float d_scale5[3];       /* type 5 dScaleX/Y/Z */
     float kerroin;           /* type 4 CT backprojection weight */
     int32_t fixed64_workspace; /* nonzero: allocate the int64 accumulators omb_backward needs for OMB_BP_FIXED64 */
+    const uint16_t *tr_index;  /* OMB_PET_INDEXED: 2 x n_proj transaxial detector indices (source, detector) */
+    const uint16_t *ax_index;  /* OMB_PET_INDEXED: 2 x n_proj axial indices into z */
 } omb_geometry_desc;
 
 typedef struct omb_handle omb_handle;

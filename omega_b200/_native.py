@@ -14,9 +14,11 @@ import numpy as np
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libomega_b200.so")
 
-OMB_ABI_VERSION = 1
+OMB_ABI_VERSION = 2
 OMB_PET_SINOGRAM = 0
 OMB_CT_PANEL = 1
+OMB_PET_LISTMODE = 2
+OMB_PET_INDEXED = 3
 OMB_READ_FP32 = 0
 OMB_READ_BF16 = 1
 OMB_BP_FLOAT_ATOMIC = 0
@@ -66,6 +68,8 @@ class GeometryDesc(ctypes.Structure):
         ("d_scale5", ctypes.c_float * 3),
         ("kerroin", ctypes.c_float),
         ("fixed64_workspace", ctypes.c_int32),
+        ("tr_index", ctypes.POINTER(ctypes.c_uint16)),
+        ("ax_index", ctypes.POINTER(ctypes.c_uint16)),
     ]
 
 

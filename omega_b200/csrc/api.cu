@@ -34,6 +34,8 @@ struct omb_handle {
     Grid grid{};
     Tof tof{};
     float *d_xy = nullptr;
+    uint16_t *d_tr = nullptr;             // index-based events: transaxial / axial index pairs
+    uint16_t *d_ax = nullptr;
     float *d_z = nullptr;
     float *d_tofc = nullptr;
     unsigned long long *d_acc = nullptr;  // 2 * N int64 accumulators (fixed-point BP)
@@ -129,14 +131,28 @@ static std::vector<BddProj> bdd_maps(const omb_geometry_desc &d) {
     return out;
 }
 
+// Measurement-level subsets (types 1, 2, 4, 5) of sinogram data; list-mode
+// events arrive already in subset order and split into contiguous ranges.
+static bool meas_level_subsets(const omb_geometry_desc &d) {
+    return d.n_subsets > 1 && d.subset_type < 8 && d.modality == OMB_PET_SINOGRAM;
+}
+
 static int validate(const omb_geometry_desc *d) {
     if (!d) return set_error(OMB_ERR_INVALID, "geometry descriptor is NULL");
     if (d->struct_size != sizeof(omb_geometry_desc))
         return set_error(OMB_ERR_INVALID, "omb_geometry_desc.struct_size does not match this library (" +
                                               std::to_string(sizeof(omb_geometry_desc)) + " bytes)");
     if (d->abi_version != OMB_ABI_VERSION) return set_error(OMB_ERR_INVALID, "unsupported abi_version");
-    if (d->modality != OMB_PET_SINOGRAM && d->modality != OMB_CT_PANEL)
-        return set_error(OMB_ERR_INVALID, "modality must be OMB_PET_SINOGRAM or OMB_CT_PANEL");
+    if (d->modality < OMB_PET_SINOGRAM || d->modality > OMB_PET_INDEXED)
+        return set_error(OMB_ERR_INVALID, "unknown modality");
+    const bool events = d->modality == OMB_PET_LISTMODE || d->modality == OMB_PET_INDEXED;
+    if (events) {
+        if (d->n_rows_d != 1 || d->n_cols_d != 1)
+            return set_error(OMB_ERR_INVALID, "list-mode data: n_rows_d and n_cols_d must be 1");
+        if (d->tof_bins > 1) return set_error(OMB_ERR_UNSUPPORTED, "TOF list-mode data is not built");
+        if (d->modality == OMB_PET_INDEXED && (!d->tr_index || !d->ax_index))
+            return set_error(OMB_ERR_INVALID, "index-based data needs tr_index and ax_index");
+    }
     if (d->fp_type != 1 && d->fp_type != 4 && d->fp_type != 5)
         return set_error(OMB_ERR_UNSUPPORTED, "forward projector type " + std::to_string(d->fp_type) + " is not built");
     if (d->bp_type != 1 && d->bp_type != 4 && d->bp_type != 5)
@@ -155,8 +171,10 @@ static int validate(const omb_geometry_desc *d) {
     if (d->n_proj <= 0) return set_error(OMB_ERR_INVALID, "n_proj must be positive");
     if (d->n_subsets < 1) return set_error(OMB_ERR_INVALID, "n_subsets must be >= 1");
     if (!d->n_meas) return set_error(OMB_ERR_INVALID, "n_meas is NULL");
-    if (!d->xy || !d->z) return set_error(OMB_ERR_INVALID, "xy/z coordinate arrays are NULL");
-    const bool meas_level = d->n_subsets > 1 && d->subset_type < 8;
+    if (!d->xy || (!d->z && d->modality != OMB_PET_LISTMODE))
+        return set_error(OMB_ERR_INVALID, "xy/z coordinate arrays are NULL");
+    // list-mode events come in subset order: contiguous ranges, like whole sinograms
+    const bool meas_level = d->n_subsets > 1 && d->subset_type < 8 && !events;
     if (meas_level) {
         if (d->modality != OMB_PET_SINOGRAM)
             return set_error(OMB_ERR_UNSUPPORTED, "measurement-level subset types are PET-only");
@@ -167,16 +185,25 @@ static int validate(const omb_geometry_desc *d) {
     if (d->modality == OMB_PET_SINOGRAM) {
         if (d->n_xy != nbin * 4) return set_error(OMB_ERR_INVALID, "PET xy must hold 4 floats per sinogram bin");
         if (d->n_z != d->n_proj * 2) return set_error(OMB_ERR_INVALID, "PET z must hold 2 floats per sinogram");
-    } else {
+    } else if (d->modality == OMB_CT_PANEL) {
         if (d->n_xy != d->n_proj * 6) return set_error(OMB_ERR_INVALID, "CT xy must hold 6 floats per projection");
         if (d->n_z != d->n_proj * 2) return set_error(OMB_ERR_INVALID, "CT z must hold 2 floats per projection");
+    } else if (d->modality == OMB_PET_LISTMODE) {
+        if (d->n_xy != d->n_proj * 6) return set_error(OMB_ERR_INVALID, "list-mode xy must hold 6 floats per event");
+    } else {
+        if (d->n_xy < 2 || d->n_xy % 2 || d->n_z < 1)
+            return set_error(OMB_ERR_INVALID, "index-based data needs the crystal table (2 floats each) and z");
+        // every index must address the tables: checked here once instead of in the kernels
+        for (int64_t e = 0; e < 2 * d->n_proj; ++e)
+            if ((int64_t)d->tr_index[e] * 2 + 1 >= d->n_xy || (int64_t)d->ax_index[e] >= d->n_z)
+                return set_error(OMB_ERR_INVALID, "event " + std::to_string(e / 2) + ": detector index out of range");
     }
     if (d->tof_bins < 1) return set_error(OMB_ERR_INVALID, "tof_bins must be >= 1");
     if (d->tof_bins > kMaxTofBins) return set_error(OMB_ERR_UNSUPPORTED, "TOF bin count above 16 is not built");
     if (d->tof_bins > 1) {
         if (!d->tof_centers) return set_error(OMB_ERR_INVALID, "tof_centers is NULL");
         if (!(d->sigma_x > 0.f)) return set_error(OMB_ERR_INVALID, "TOF sigma must be positive");
-        if (d->modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_INVALID, "TOF is PET-only");
+        if (d->modality == OMB_CT_PANEL) return set_error(OMB_ERR_INVALID, "TOF is PET-only");
     }
     const int64_t *nm = d->n_meas;
     if (nm[0] != 0) return set_error(OMB_ERR_INVALID, "n_meas[0] must be 0");
@@ -194,6 +221,8 @@ static int ray_set(const omb_handle *h, int32_t subset, RaySet &rs) {
         return set_error(OMB_ERR_INVALID, "subset " + std::to_string(subset) + " out of range");
     rs.xy = h->d_xy;
     rs.z = h->d_z;
+    rs.tr = h->d_tr;
+    rs.ax = h->d_ax;
     rs.modality = d.modality;
     rs.n_rows = (int)d.n_rows_d;
     rs.n_cols = (int)d.n_cols_d;
@@ -201,7 +230,7 @@ static int ray_set(const omb_handle *h, int32_t subset, RaySet &rs) {
     rs.pitch_y = d.dpitch_y;
     rs.n_subsets = d.n_subsets;
     const int64_t nbin = (int64_t)d.n_rows_d * d.n_cols_d;
-    const bool meas_level = d.n_subsets > 1 && d.subset_type < 8;
+    const bool meas_level = meas_level_subsets(d);
     if (meas_level) {
         if (subset < 0) return set_error(OMB_ERR_UNSUPPORTED, "subset -1 needs a whole-sinogram subset type");
         rs.stype = d.subset_type;
@@ -223,7 +252,7 @@ static int ray_set(const omb_handle *h, int32_t subset, RaySet &rs) {
 
 // First measurement (ray) of a subset in the all-subsets measurement order.
 static int64_t subset_ray0(const omb_handle *h, const RaySet &rs, int32_t subset) {
-    const bool meas_level = h->desc.n_subsets > 1 && h->desc.subset_type < 8;
+    const bool meas_level = meas_level_subsets(h->desc);
     return meas_level ? h->n_meas[subset] : rs.proj0 * (int64_t)h->desc.n_rows_d * h->desc.n_cols_d;
 }
 
@@ -336,11 +365,22 @@ int omb_create(const omb_geometry_desc *desc, omb_handle **out) {
     };
     cudaError_t e;
     if ((e = cudaMalloc(&h->d_xy, desc->n_xy * sizeof(float))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc xy"));
-    if ((e = cudaMalloc(&h->d_z, desc->n_z * sizeof(float))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc z"));
+    if ((e = cudaMalloc(&h->d_z, (desc->n_z > 0 ? desc->n_z : 1) * sizeof(float))) != cudaSuccess)
+        return fail(cuda_fail(e, "cudaMalloc z"));
     if ((e = cudaMemcpy(h->d_xy, desc->xy, desc->n_xy * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(cuda_fail(e, "upload xy"));
-    if ((e = cudaMemcpy(h->d_z, desc->z, desc->n_z * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+    if (desc->n_z > 0 && (e = cudaMemcpy(h->d_z, desc->z, desc->n_z * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(cuda_fail(e, "upload z"));
+    h->desc.tr_index = nullptr;
+    h->desc.ax_index = nullptr;
+    if (desc->modality == OMB_PET_INDEXED) {
+        const size_t nb = (size_t)desc->n_proj * 2 * sizeof(uint16_t);
+        if ((e = cudaMalloc(&h->d_tr, nb)) != cudaSuccess || (e = cudaMalloc(&h->d_ax, nb)) != cudaSuccess)
+            return fail(cuda_fail(e, "cudaMalloc event indices"));
+        if ((e = cudaMemcpy(h->d_tr, desc->tr_index, nb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(h->d_ax, desc->ax_index, nb, cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(cuda_fail(e, "upload event indices"));
+    }
     if ((e = cudaMalloc(&h->d_tofc, kMaxTofBins * sizeof(float))) != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc tof"));
     if ((e = cudaMemset(h->d_tofc, 0, kMaxTofBins * sizeof(float))) != cudaSuccess) return fail(cuda_fail(e, "clear tof"));
     if (desc->tof_bins > 1 &&
@@ -372,6 +412,8 @@ int omb_destroy(omb_handle *h) {
     cudaGetDevice(&prev);
     if (prev != h->device) cudaSetDevice(h->device);
     cudaFree(h->d_xy);
+    cudaFree(h->d_tr);
+    cudaFree(h->d_ax);
     cudaFree(h->d_z);
     cudaFree(h->d_tofc);
     cudaFree(h->d_acc);
@@ -533,7 +575,7 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
     if (!image || !y_subset || !sens || !work_meas || !work_img)
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osem_subset");
-    if (h->desc.modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
+    if (h->desc.modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
     if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
         return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset needs projector types 1 or 4");
     RaySet rs{};
@@ -563,7 +605,7 @@ int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, floa
     if (!images || !y_subset || !sens || !work_meas || !work_img)
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osem_subset_frames");
     if (n_frames < 0) return set_error(OMB_ERR_INVALID, "n_frames must be >= 0");
-    if (h->desc.modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
+    if (h->desc.modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
     if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
         return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset_frames needs projector types 1 or 4");
     RaySet rs{};
@@ -680,10 +722,10 @@ static void tuning_to(const Tuning &t, omb_tuning *out) {
 int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weights, const float *atten_image,
                         int64_t n_atten, void *stream) {
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
-    if ((meas_weights || atten_image) && h->desc.modality != OMB_PET_SINOGRAM)
+    if ((meas_weights || atten_image) && h->desc.modality == OMB_CT_PANEL)
         return set_error(OMB_ERR_UNSUPPORTED, "corrections apply to PET data");
     // rays of all subsets (TOF bins share their ray's weight)
-    const bool meas_level = h->desc.n_subsets > 1 && h->desc.subset_type < 8;
+    const bool meas_level = meas_level_subsets(h->desc);
     const int64_t total = meas_level ? h->n_meas[h->desc.n_subsets]
                                      : h->desc.n_proj * (int64_t)h->desc.n_rows_d * h->desc.n_cols_d;
     if (meas_weights && n_weights != total)
@@ -708,8 +750,8 @@ int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weig
 
 int omb_set_randoms(omb_handle *h, const float *randoms, int64_t n, void *stream) {
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
-    if (randoms && h->desc.modality != OMB_PET_SINOGRAM) return set_error(OMB_ERR_UNSUPPORTED, "randoms apply to PET data");
-    const bool meas_level = h->desc.n_subsets > 1 && h->desc.subset_type < 8;
+    if (randoms && h->desc.modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "randoms apply to PET data");
+    const bool meas_level = meas_level_subsets(h->desc);
     const int64_t total = meas_level ? h->n_meas[h->desc.n_subsets]
                                      : h->desc.n_proj * (int64_t)h->desc.n_rows_d * h->desc.n_cols_d;
     if (randoms && n != total)
@@ -773,7 +815,7 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
     // ray-driven kernels (types 1 and 4 forward, PET types 1 and 4 backward)
     // share the blocks-per-SM and frames-per-walk shapes
     const bool ray_fp = h->desc.fp_type == 1 || h->desc.fp_type == 4;
-    const bool ray_bp = h->desc.bp_type == 1 || (h->desc.bp_type == 4 && h->desc.modality == OMB_PET_SINOGRAM);
+    const bool ray_bp = h->desc.bp_type == 1 || (h->desc.bp_type == 4 && h->desc.modality != OMB_CT_PANEL);
     const bool siddon = ray_fp || ray_bp;
     if (!(h->desc.fp_type == 1 && h->desc.bp_type == 1) || h->desc.tof_bins > 1) n_frames = 1;
     const int64_t m = omb_measurement_count(h, -1);

@@ -53,6 +53,8 @@ struct RaySet {
     int n_subsets;
     int cur_subset;
     float pitch_x, pitch_y;
+    const uint16_t *tr; // OMB_PET_INDEXED: transaxial index pairs of all events
+    const uint16_t *ax; // OMB_PET_INDEXED: axial index pairs of all events
     const float *w;     // PET: multiplicative weight of each of the launch's rays, or NULL
     const float *mu;    // PET: attenuation image (1/mm), or NULL
 };

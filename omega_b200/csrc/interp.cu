@@ -119,7 +119,7 @@ __device__ __forceinline__ float trilinear(const T *__restrict__ img, const Grid
 template <int NB, typename T>
 __global__ void k_interp_fp(Grid g, RaySet rs, Tof tof, float gf, float dL, const T *__restrict__ img,
                             float *__restrict__ y) {
-    const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const bool pet = rs.modality != OMB_CT_PANEL;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
         float ax[NB];

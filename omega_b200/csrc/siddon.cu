@@ -20,7 +20,7 @@ template <int NB, int FB, typename T, int K>
 __global__ void __launch_bounds__(kBlock) k_siddon_fp(Grid g, RaySet rs, Tof tof, float gf,
                                                       const T *__restrict__ img, int64_t img_stride,
                                                       float *__restrict__ y, int64_t y_stride, int n_frames) {
-    const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const bool pet = rs.modality != OMB_CT_PANEL;
     const int f0 = blockIdx.y * FB;
     const int nf = min(FB, n_frames - f0);
     img += f0 * img_stride;
@@ -105,7 +105,7 @@ template <int FB, int K>
 __global__ void __launch_bounds__(kBlock) k_siddon_fp_ilv(Grid g, RaySet rs, float gf, const float *__restrict__ img,
                                                           int64_t n_img, float *__restrict__ y, int64_t y_stride,
                                                           int n_frames) {
-    const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const bool pet = rs.modality != OMB_CT_PANEL;
     const Tof tof{1, 0.f, 0.f, 0.f, nullptr};
     const int f0 = blockIdx.y * FB;
     const int nf = min(FB, n_frames - f0);
@@ -139,7 +139,7 @@ template <int FB>
 __global__ void __launch_bounds__(kBlock) k_siddon_bp_ilv(Grid g, RaySet rs, float gf, const float *__restrict__ y,
                                                           int64_t y_stride, float *__restrict__ img, int64_t n_img,
                                                           int n_frames) {
-    const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const bool pet = rs.modality != OMB_CT_PANEL;
     const Tof tof{1, 0.f, 0.f, 0.f, nullptr};
     const int f0 = blockIdx.y * FB;
     const int nf = min(FB, n_frames - f0);
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kBlock) k_siddon_bp(Grid g, RaySet rs, Tof tof
                                                       const float *__restrict__ y, int64_t y_stride,
                                                       float *__restrict__ img, int64_t img_stride,
                                                       float *__restrict__ sens, int n_frames) {
-    const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const bool pet = rs.modality != OMB_CT_PANEL;
     const int f0 = blockIdx.y * FB;
     const int nf = min(FB, n_frames - f0);
     if (y) y += f0 * y_stride;
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kBlock) k_siddon_bp_fixed(Grid g, RaySet rs, T
                                                             const float *__restrict__ y,
                                                             unsigned long long *__restrict__ acc,
                                                             unsigned long long *__restrict__ acc_sens) {
-    const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const bool pet = rs.modality != OMB_CT_PANEL;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
         float ax[NB];
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(kBlock) k_siddon_bp_fixed(Grid g, RaySet rs, T
 // the algorithmic-byte model); one int64 atomic per block.
 __global__ void __launch_bounds__(kBlock) k_siddon_count(Grid g, RaySet rs, Tof tof,
                                                          unsigned long long *__restrict__ total) {
-    const bool pet = rs.modality == OMB_PET_SINOGRAM;
+    const bool pet = rs.modality != OMB_CT_PANEL;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     unsigned long long n = 0;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {

@@ -37,6 +37,21 @@ struct Ray {
 // Ray end points of launch-local ray `r`; also returns the measurement index
 // (output position) of the ray in the launch's output vector.
 __device__ __forceinline__ Ray load_ray(const RaySet &rs, int64_t r) {
+    Ray ray;
+    if (rs.modality == OMB_PET_LISTMODE) {
+        const float *q = rs.xy + (rs.proj0 + r) * 6;
+        ray.s = make_float3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+        ray.d = make_float3(__ldg(q + 3), __ldg(q + 4), __ldg(q + 5));
+        return ray;
+    }
+    if (rs.modality == OMB_PET_INDEXED) {
+        const int64_t e = (rs.proj0 + r) * 2;
+        const int t0 = __ldg(rs.tr + e), t1 = __ldg(rs.tr + e + 1);
+        const int a0 = __ldg(rs.ax + e), a1 = __ldg(rs.ax + e + 1);
+        ray.s = make_float3(__ldg(rs.xy + 2 * t0), __ldg(rs.xy + 2 * t0 + 1), __ldg(rs.z + a0));
+        ray.d = make_float3(__ldg(rs.xy + 2 * t1), __ldg(rs.xy + 2 * t1 + 1), __ldg(rs.z + a1));
+        return ray;
+    }
     int64_t ix, iy, iz;
     if (rs.stype == 0) {
         const int64_t nbin = (int64_t)rs.n_rows * rs.n_cols;
@@ -72,7 +87,6 @@ __device__ __forceinline__ Ray load_ray(const RaySet &rs, int64_t r) {
             ix = x % nr;
         }
     }
-    Ray ray;
     if (rs.modality == OMB_PET_SINOGRAM) {
         const float4 q = __ldg(reinterpret_cast<const float4 *>(rs.xy) + (ix + iy * rs.n_rows));
         const float2 zz = __ldg(reinterpret_cast<const float2 *>(rs.z) + iz);

@@ -551,7 +551,9 @@ def projector_scaling(o):
         o.dSizeZBP = (o.nColsD + 1) * o.dPitchX
         o.dSizeXBP = (o.nRowsD + 1) * o.dPitchY
     if o.projector_type in (4, 14, 41, 42, 43, 44, 45, 54):
-        o.kerroin = (o.dx * o.dy * o.dz) / (o.dPitchX * o.dPitchY * o.sourceToDetector)
+        # the CT backprojection weight; PET data (no sourceToDetector) gives inf, as in the reference, unused
+        with np.errstate(divide='ignore'):
+            o.kerroin = (o.dx * o.dy * o.dz) / (o.dPitchX * o.dPitchY * o.sourceToDetector)
         fov0 = float(np.asarray(o.FOVa_x).ravel()[0])
         nx0 = float(np.asarray(o.Nx).ravel()[0])
         if o.dL == 0:

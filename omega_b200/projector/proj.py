@@ -39,6 +39,10 @@ class projectorClass:
     x = np.empty(0, dtype=np.float32)
     y = np.empty(0, dtype=np.float32)
     z = np.empty(0, dtype=np.float32)
+    # index-based events: (source, detector) crystal indices into x (2 per
+    # crystal) and ring indices into z, 2 x events each
+    trIndex = np.empty(0, dtype=np.uint16)
+    axIndex = np.empty(0, dtype=np.uint16)
     x0 = np.empty(0, dtype=np.float32)
     Nx = 1
     Ny = 1
@@ -273,7 +277,7 @@ class projectorClass:
             self.Nt = self.partitions
         if self.Nt > 1 and self.subsetType == 3:
             raise ValueError('Subset type 3 is not supported with dynamic data!')
-        self.listmode = 0
+        self._listmode_setup()
         if (not self.CT and not self.SPECT) and (((self.subsetType > 7 or (self.subsetType == 0 and self.listmode == 0))
                                                    and self.subsets > 1) or self.subsets == 1):
             self.nProjections = self.NSinos
@@ -281,12 +285,20 @@ class projectorClass:
         else:
             self.PET = False
             self.nProjections = self.NSinos
-        self.index, self.nMeas = geo.subset_indices(self)
+        if self.listmode:
+            self.index, self.nMeas = self._listmode_subsets()
+        else:
+            self.index, self.nMeas = geo.subset_indices(self)
         self.x0 = np.asarray(self.x0).ravel('F')
         if self.CT and self.projector_type == 11 and not self.useCPU:
             self.projector_type = 4
         if self.CT:
             x_det, z_det = self.x, self.z
+        elif self.listmode:
+            x_det, z_det = self._listmode_coordinates()
+            self.nRowsD = self.nColsD = 1
+            # events in the subsets (the random split of subset type 3 leaves one out, as the reference's)
+            self.nProjections = int(np.sum(self.nMeas))
         else:
             x_det, z_det = geo.pet_sinogram_coordinates(self)
             self.dPitch = self.cr_p
@@ -307,8 +319,9 @@ class projectorClass:
                 self.uV = self.uV[self.index, :]
             else:
                 z_det = np.reshape(z_det, (self.nProjections, -1))[self.index, :].ravel('C')
-        self.x = x_det
-        self.z = z_det
+        self.x = np.asarray(x_det).astype(dtype=np.float32)
+        self.z = np.asarray(z_det).astype(dtype=np.float32)
+        self._x_sinogram = self.x if not (self.CT or self.listmode) else None
         self.x_center = np.array(self.bx[0].item(), ndmin=1).astype(np.float32)
         self.y_center = np.array(self.by[0].item(), ndmin=1).astype(np.float32)
         self.z_center = np.array(self.bz[0].item(), ndmin=1).astype(np.float32)
@@ -332,8 +345,82 @@ class projectorClass:
         if self.use_32bit_atomics and self.use_64bit_atomics:
             self.use_64bit_atomics = False
         self.x0 = self.x0.astype(dtype=np.float32)
-        self.x = np.asarray(self.x).astype(dtype=np.float32)
-        self.z = np.asarray(self.z).astype(dtype=np.float32)
+
+    # ------------------------------------------------------------------
+    # List-mode and index-based event data (proj.py:777-850, 862-905;
+    # indices.py:79-160, 346-412)
+    # ------------------------------------------------------------------
+    def _listmode_setup(self):
+        """Detects event data: 6 coordinates per event in ``x`` (or ``x``,
+        ``y``, ``z`` of 2 rows each), or detector index pairs ``trIndex`` /
+        ``axIndex`` with ``useIndexBasedReconstruction``; each event is then
+        one 1 x 1 "sinogram"."""
+        self.listmode = 0
+        if self.CT or self.SPECT or self.x is getattr(self, '_x_sinogram', None):
+            return  # (the sinogram coordinates of an earlier addProjector are not events)
+        if self.useIndexBasedReconstruction:
+            n_events = np.size(self.trIndex) // 2
+        else:
+            x = np.asarray(self.x)
+            nx = x.size
+            sin_n = np.size(self.SinM)
+            if nx == 0 or not (nx // 6 == sin_n and nx % 6 == 0 or nx // 2 == sin_n and x.ndim == 2 or
+                               (sin_n == 0 and nx >= 6)):
+                return
+            if x.ndim == 2 and 2 in x.shape and np.size(self.y) == nx:
+                # separate x, y, z of (source, detector): stack into 6 rows
+                two = (lambda a: np.asarray(a).reshape(2, -1) if np.asarray(a).shape[0] == 2 else np.asarray(a).T)
+                xx, yy, zz = two(self.x), two(self.y), two(self.z)
+                self.x = np.vstack([xx[0], yy[0], zz[0], xx[1], yy[1], zz[1]])
+            n_events = np.size(self.x) // 6
+        if self.TOF_bins > 1:
+            raise ValueError('TOF list-mode data is not supported by this projector build')
+        self.Nang = 1
+        self.Ndist = 1
+        self.NSinos = int(n_events)
+        self.TotSinos = self.NSinos
+        self.listmode = 1
+
+    def _listmode_subsets(self):
+        """Subset indices of event data: type 0 contiguous blocks, 1 every
+        subsets-th event, 3 a seeded random split (indices.py:79-160)."""
+        n, S = int(self.NSinos), int(self.subsets)
+        if S == 1:
+            return np.zeros(1, dtype=np.uint32), np.array([n], dtype=np.int64)
+        if self.subsetType not in (0, 1, 3):
+            self.subsetType = 0
+        if self.subsetType == 0:
+            val = n // S
+            last = n - val * (S - 1) if n % S > 0 else val
+            return np.zeros(1, dtype=np.uint32), np.append(np.full(S - 1, val, dtype=np.int64), last)
+        if self.subsetType == 1:
+            parts = [np.arange(i, n, S, dtype=np.uint32) for i in range(S)]
+        else:
+            port = n // S
+            gen = np.random.default_rng() if self.seed < 0 else np.random.default_rng(self.seed)
+            perm = gen.permutation(n).astype(np.uint32)
+            parts = [perm[port * i:-1] if i == S - 1 else perm[port * i:port * (i + 1)] for i in range(S)]
+        return np.concatenate(parts), np.array([p.size for p in parts], dtype=np.int64)
+
+    def _listmode_coordinates(self):
+        """Event coordinates in subset order (indices.py:346-412): the 6 x
+        events matrix, or (index-based) the crystal table and z with the
+        index pairs reordered."""
+        sub = self.subsets > 1 and self.subsetType > 0
+        if self.useIndexBasedReconstruction:
+            tr = np.asarray(self.trIndex, dtype=np.uint16).reshape(2, -1, order='F')
+            ax = np.asarray(self.axIndex, dtype=np.uint16).reshape(2, -1, order='F')
+            if sub:
+                tr, ax = tr[:, self.index], ax[:, self.index]
+            self.trIndex = np.asfortranarray(tr).ravel(order='F')
+            self.axIndex = np.asfortranarray(ax).ravel(order='F')
+            return np.asarray(self.x, dtype=np.float32).ravel(order='F'), \
+                np.asarray(self.z, dtype=np.float32).ravel(order='F')
+        x = np.asarray(self.x, dtype=np.float32)
+        x = x.reshape(6, -1, order='F') if x.shape[0] != 6 else x
+        if sub:
+            x = x[:, self.index]
+        return np.asfortranarray(x).ravel(order='F'), np.zeros(0, dtype=np.float32)
 
     @staticmethod
     def _n(v):
@@ -447,7 +534,12 @@ class projectorClass:
         d = _native.GeometryDesc()
         d.struct_size = ctypes.sizeof(_native.GeometryDesc)
         d.abi_version = _native.OMB_ABI_VERSION
-        d.modality = _native.OMB_CT_PANEL if self.CT else _native.OMB_PET_SINOGRAM
+        if self.CT:
+            d.modality = _native.OMB_CT_PANEL
+        elif self.listmode:
+            d.modality = _native.OMB_PET_INDEXED if self.useIndexBasedReconstruction else _native.OMB_PET_LISTMODE
+        else:
+            d.modality = _native.OMB_PET_SINOGRAM
         d.fp_type, d.bp_type = fpt, bpt
         d.nx, d.ny, d.nz = self._n(self.Nx), self._n(self.Ny), self._n(self.Nz)
         d.dx, d.dy, d.dz = float(self.dx[0]), float(self.dy[0]), float(self.dz[0])
@@ -485,6 +577,11 @@ class projectorClass:
             d.d_scale5[0], d.d_scale5[1], d.d_scale5[2] = (float(self.dScaleX[0]), float(self.dScaleY[0]),
                                                            float(self.dScaleZ[0]))
         d.fixed64_workspace = 1 if self.use_64bit_atomics else 0
+        if self.listmode and self.useIndexBasedReconstruction:
+            keep['tr'] = np.ascontiguousarray(np.asarray(self.trIndex, dtype=np.uint16).ravel())
+            keep['ax'] = np.ascontiguousarray(np.asarray(self.axIndex, dtype=np.uint16).ravel())
+            d.tr_index = keep['tr'].ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))
+            d.ax_index = keep['ax'].ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))
         return d, keep
 
     def initProj(self):

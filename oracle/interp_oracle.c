@@ -116,7 +116,7 @@ int oracle_interp_fp(const oracle_geom *g, double dL, const double *img, double 
                 for (int to = 0; to < nb; ++to) ax[to] += w[to] * (val / tsum);
             }
         }
-        const double temp = n == 0 ? 0.0 : (g->modality == 0 ? g->global_factor / L : 1.0);
+        const double temp = n == 0 ? 0.0 : (g->modality != 1 ? g->global_factor / L : 1.0);
         for (int to = 0; to < nb; ++to) y[r + (int64_t)to * g->m_size] = ax[to] * temp;
     }
     return 0;

@@ -57,6 +57,8 @@ class OracleGeom(ctypes.Structure):
         ("z", ctypes.POINTER(ctypes.c_float)),
         ("w", ctypes.POINTER(ctypes.c_double)),
         ("mu", ctypes.POINTER(ctypes.c_double)),
+        ("tr", ctypes.POINTER(ctypes.c_uint16)),
+        ("ax", ctypes.POINTER(ctypes.c_uint16)),
     ]
 
 
@@ -102,6 +104,8 @@ def ref_lib():
             getattr(L, name).argtypes = [ctypes.c_int, u, u, u, T, T, T, T, T, T, u, u, u, P, P, P, P, P, u, T, P, T,
                                          T, u]
         P = ctypes.POINTER(ctypes.c_double)
+        L.ref_listmode_d.argtypes = [ctypes.c_int, u, u, u] + [ctypes.c_double] * 6 + [ctypes.c_int64, P, P, P, P,
+                                                                                      ctypes.c_double, ctypes.c_double, u]
         L.ref_siddon_corr_d.argtypes = [ctypes.c_int, u, u, u] + [ctypes.c_double] * 6 + [u, u, u] + [P] * 5 + \
             [u, ctypes.c_double, P, ctypes.c_double, ctypes.c_double, u, P, P, ctypes.c_int, P]
         _ref = L
@@ -113,6 +117,12 @@ class Geometry:
 
     def __init__(self, o):
         self.ct = bool(o.CT)
+        # 0 sinogram, 1 CT, 2 list-mode events, 3 index-based events
+        self.modality = 1 if self.ct else (0 if not getattr(o, 'listmode', 0) else
+                                           (3 if o.useIndexBasedReconstruction else 2))
+        if self.modality == 3:
+            self.tr = np.ascontiguousarray(np.asarray(o.trIndex, dtype=np.uint16).ravel())
+            self.ax = np.ascontiguousarray(np.asarray(o.axIndex, dtype=np.uint16).ravel())
         self.nx, self.ny, self.nz = (int(np.asarray(v).ravel()[0]) for v in (o.Nx, o.Ny, o.Nz))
         self.d = tuple(float(np.asarray(v).ravel()[0]) for v in (o.dx, o.dy, o.dz))
         self.b = tuple(float(np.asarray(v).ravel()[0]) for v in (o.bx, o.by, o.bz))
@@ -143,7 +153,8 @@ class Geometry:
         return self.nx * self.ny * self.nz
 
     def meas_level(self):
-        return self.n_subsets > 1 and self.stype < 8
+        # list-mode events come in subset order: contiguous, like whole sinograms
+        return self.n_subsets > 1 and self.stype < 8 and self.modality == 0
 
     def rays(self, subset):
         nbin = self.n_rows * self.n_cols
@@ -155,7 +166,7 @@ class Geometry:
 
     def struct(self, subset):
         g = OracleGeom()
-        g.modality = 1 if self.ct else 0
+        g.modality = self.modality
         g.nx, g.ny, g.nz = self.nx, self.ny, self.nz
         g.dx, g.dy, g.dz = self.d
         g.bx, g.by, g.bz = self.b
@@ -188,6 +199,10 @@ class Geometry:
         if self.mu is not None:
             self._mu = np.ascontiguousarray(self.mu, dtype=np.float64).ravel()
             g.mu = self._mu.ctypes.data_as(P)
+        if self.modality == 3:
+            U = ctypes.POINTER(ctypes.c_uint16)
+            g.tr = self.tr.ctypes.data_as(U)
+            g.ax = self.ax.ctypes.data_as(U)
         return g
 
 
@@ -308,6 +323,21 @@ def ref_corrected(geom: Geometry, inp, subset, fp, norm=None, atten=None, ct_att
     L.ref_siddon_corr_d(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, geom.n_rows, geom.n_cols,
                         n1 - n0, p(xy), p(z), p(inp), p(out), p(s), geom.nbins, geom.sigma_x, p(tofc),
                         geom.global_factor, geom.epps, int(threads), p(norm), p(atten), 1 if ct_atten else 0, p(scat))
+    return (out, s) if sens else out
+
+
+def ref_listmode(geom: Geometry, inp, subset, fp, threads=0, sens=False):
+    """The reference CPU projector (FP64) on the list-mode events of a subset."""
+    L = ref_lib()
+    P = ctypes.POINTER(ctypes.c_double)
+    p = (lambda a: a.ctypes.data_as(P) if a is not None else None)
+    e0, e1 = (0, geom.n_proj) if subset < 0 else (int(geom.n_meas[subset]), int(geom.n_meas[subset + 1]))
+    xyz = np.ascontiguousarray(geom.xy.astype(np.float64)[e0 * 6:e1 * 6])
+    inp = np.ascontiguousarray(inp, dtype=np.float64).ravel()
+    out = np.zeros(e1 - e0 if fp else geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    L.ref_listmode_d(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, e1 - e0, p(xyz), p(inp), p(out), p(s),
+                     geom.global_factor, geom.epps, int(threads))
     return (out, s) if sens else out
 
 

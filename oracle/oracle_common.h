@@ -29,6 +29,9 @@ typedef struct oracle_geom {
      * multiplicative weight of each of the launch's rays, attenuation image */
     const double *w;
     const double *mu;
+    /* modality 3 (index-based events): index pairs of every event */
+    const uint16_t *tr;
+    const uint16_t *ax;
 } oracle_geom;
 
 typedef struct { double x, y, z; } v3;
@@ -36,6 +39,19 @@ typedef struct { double x, y, z; } v3;
 static double sgn(double v) { return (double)((0.0 < v) - (v < 0.0)); }
 
 static void load_ray(const oracle_geom *g, int64_t r, v3 *s, v3 *d) {
+    if (g->modality == 2) { /* list-mode events: 6 coordinates each (general_opencl_functions.h:1304-1320) */
+        const float *q = g->xy + (g->proj0 + r) * 6;
+        s->x = q[0]; s->y = q[1]; s->z = q[2];
+        d->x = q[3]; d->y = q[4]; d->z = q[5];
+        return;
+    }
+    if (g->modality == 3) { /* index-based events (general_opencl_functions.h:1277-1301) */
+        const int64_t e = (g->proj0 + r) * 2;
+        const int t0 = g->tr[e], t1 = g->tr[e + 1], a0 = g->ax[e], a1 = g->ax[e + 1];
+        s->x = g->xy[2 * t0]; s->y = g->xy[2 * t0 + 1]; s->z = g->z[a0];
+        d->x = g->xy[2 * t1]; d->y = g->xy[2 * t1 + 1]; d->z = g->z[a1];
+        return;
+    }
     int64_t ix, iy, iz;
     if (g->stype == 0) {
         int64_t nbin = (int64_t)g->n_rows * g->n_cols;

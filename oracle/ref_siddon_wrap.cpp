@@ -53,6 +53,36 @@ static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, 
 }
 
 extern "C" {
+/* List-mode events: xyz = 6 coordinates per event (get_detector_coordinates_raw,
+ * projector_functions.h:357-368), n_events rays, no TOF. */
+int ref_listmode_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx,
+                   double by, double bz, int64_t n_events, const double *xyz, double *input, double *output,
+                   double *sens, double global_factor, double epps, uint32_t n_threads) {
+    paramStruct<double> p;
+    p.subsetType = 0;
+    p.subsets = 1;
+    p.currentSubset = 0;
+    p.size_x = 1;
+    p.size_y = 1;
+    p.dx = dx; p.dy = dy; p.dz = dz;
+    p.Nx = nx; p.Ny = ny; p.Nz = nz;
+    p.bx = bx; p.by = by; p.bz = bz;
+    p.projType = 1;
+    p.listMode = 1;
+    p.nProjections = 1;
+    p.globalFactor = global_factor;
+    p.epps = epps;
+    p.TOF = false;
+    p.nBins = 1;
+    double tofc = 0.0;
+    p.TOFCenters = &tofc;
+    p.noSensImage = sens == nullptr;
+    p.nMeas = 0;
+    double z0 = 0.0;
+    projectorType123Implementation4<double>(p, n_events, output, xyz, &z0, input, false, false, (uint8_t)(fp ? 1 : 2),
+                                            sens, nullptr, n_threads);
+    return 0;
+}
 /* With PET corrections: norm / scat per measurement of the call (NULL: off);
  * atten: image (ct_atten != 0) or per measurement (ct_atten == 0), NULL: off. */
 int ref_siddon_corr_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx,

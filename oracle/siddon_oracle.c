@@ -146,7 +146,7 @@ static int walk_ex(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, 
         isnan(diff.y) || isnan(diff.z))
         return 0;
     const double L = sqrt(diff.x * diff.x + diff.y * diff.y + diff.z * diff.z);
-    *temp = g->modality == 0 ? (1.0 / L) * g->global_factor : 1.0;
+    *temp = g->modality != 1 ? (1.0 / L) * g->global_factor : 1.0;
     const int64_t nxy = (int64_t)g->nx * g->ny;
     double w[MAXB];
     const int tofon = g->nbins > 1;
@@ -268,7 +268,7 @@ static void atn_visit(void *c, int64_t ind, double ele, const double *w, double 
 
 /* Correction factor of PET ray r: its weight times exp(-line integral of mu). */
 static double ray_corr(const oracle_geom *g, int64_t r) {
-    if (g->modality != 0) return 1.0;
+    if (g->modality == 1) return 1.0;
     double f = g->w ? g->w[r] : 1.0;
     if (g->mu) {
         atn_ctx a = {g->mu, 0.0};
@@ -345,7 +345,7 @@ int oracle_siddon_bp(const oracle_geom *g, const double *y, double *img, double 
         load_ray(g, r, &s, &d);
         double dxl = d.x - s.x, dyl = d.y - s.y, dzl = d.z - s.z;
         double L = sqrt(dxl * dxl + dyl * dyl + dzl * dzl);
-        b.temp = g->modality == 0 ? (1.0 / L) * g->global_factor * ray_corr(g, r) : 1.0;
+        b.temp = g->modality != 1 ? (1.0 / L) * g->global_factor * ray_corr(g, r) : 1.0;
         walk(g, r, &temp, bp_visit, &b);
     }
     return 0;
