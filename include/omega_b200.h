@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define OMB_ABI_VERSION 2
+#define OMB_ABI_VERSION 3
 
 typedef enum omb_status {
     OMB_OK = 0,
@@ -108,6 +108,9 @@ typedef struct omb_geometry_desc {
     int32_t fixed64_workspace; /* nonzero: allocate the int64 accumulators omb_backward needs for OMB_BP_FIXED64 */
     const uint16_t *tr_index;  /* OMB_PET_INDEXED: 2 x n_proj transaxial detector indices (source, detector) */
     const uint16_t *ax_index;  /* OMB_PET_INDEXED: 2 x n_proj axial indices into z */
+    int32_t n_rays_xy;         /* PET multi-ray (proj.py n_rays_transaxial, 0 or 1: one ray): rays per LOR
+                                  spread over dpitch_x transaxially */
+    int32_t n_rays_z;          /* (n_rays_axial) rays spread over dpitch_y axially; projector type 1 only */
 } omb_geometry_desc;
 
 typedef struct omb_handle omb_handle;

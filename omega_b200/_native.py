@@ -14,7 +14,7 @@ import numpy as np
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libomega_b200.so")
 
-OMB_ABI_VERSION = 2
+OMB_ABI_VERSION = 3
 OMB_PET_SINOGRAM = 0
 OMB_CT_PANEL = 1
 OMB_PET_LISTMODE = 2
@@ -70,6 +70,8 @@ class GeometryDesc(ctypes.Structure):
         ("fixed64_workspace", ctypes.c_int32),
         ("tr_index", ctypes.POINTER(ctypes.c_uint16)),
         ("ax_index", ctypes.POINTER(ctypes.c_uint16)),
+        ("n_rays_xy", ctypes.c_int32),
+        ("n_rays_z", ctypes.c_int32),
     ]
 
 

@@ -165,6 +165,15 @@ static int validate(const omb_geometry_desc *d) {
         return set_error(OMB_ERR_INVALID, "projector type 4 needs a positive sampling length dL");
     if (d->bp_type == 4 && d->modality == OMB_CT_PANEL && !(d->kerroin > 0.f))
         return set_error(OMB_ERR_INVALID, "the type-4 CT backprojection needs its weight kerroin > 0");
+    if (d->n_rays_xy < 0 || d->n_rays_z < 0 || d->n_rays_xy > 64 || d->n_rays_z > 64)
+        return set_error(OMB_ERR_INVALID, "rays per LOR must be in 0..64");
+    if (std::max(d->n_rays_xy, 1) * std::max(d->n_rays_z, 1) > 1) {
+        if (d->modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "multi-ray projection is PET-only");
+        if (d->fp_type != 1 || d->bp_type != 1)
+            return set_error(OMB_ERR_UNSUPPORTED, "multi-ray projection is built for projector type 1");
+        if (!(d->dpitch_x > 0.f) || !(d->dpitch_y > 0.f))
+            return set_error(OMB_ERR_INVALID, "multi-ray projection needs the crystal pitches dpitch_x, dpitch_y");
+    }
     if (d->nx == 0 || d->ny == 0 || d->nz == 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
     if (!(d->dx > 0.f) || !(d->dy > 0.f) || !(d->dz > 0.f)) return set_error(OMB_ERR_INVALID, "voxel size must be positive");
     if (d->n_rows_d == 0 || d->n_cols_d == 0) return set_error(OMB_ERR_INVALID, "detector size must be positive");
@@ -245,6 +254,10 @@ static int ray_set(const omb_handle *h, int32_t subset, RaySet &rs) {
         rs.n_proj = subset < 0 ? d.n_proj : h->n_meas[subset + 1] - h->n_meas[subset];
         rs.m_size = rs.n_proj * nbin;
     }
+    rs.nr_xy = std::max(d.n_rays_xy, 1);
+    rs.nr_z = std::max(d.n_rays_z, 1);
+    rs.cr_xy = d.dpitch_x;  // crystalSize.x / .y of the reference's kernels (init.py:736)
+    rs.cr_z = d.dpitch_y;
     rs.w = h->d_w ? h->d_w + (meas_level ? h->n_meas[subset] : rs.proj0 * nbin) : nullptr;
     rs.mu = h->d_mu;
     return OMB_OK;
@@ -301,6 +314,15 @@ static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cud
         }
         return OMB_OK;
     }
+    if (rs.nr_xy * rs.nr_z > 1) {
+        if (f.img_in16) return set_error(OMB_ERR_UNSUPPORTED, "multi-ray projection reads FP32 images");
+        for (int fr = 0; fr < f.n; ++fr) {
+            const int st = multiray_forward(h->grid, rs, h->tof, h->desc.global_factor, f.img_in + fr * f.img_stride,
+                                            f.meas_out + fr * f.meas_stride, h->tune.siddon_blocks_per_sm, s);
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
     if (!f.img_in16) attach_interleave(h, f, s);
     return siddon_forward(h->grid, rs, h->tof, h->desc.global_factor, f, h->tune, s);
 }
@@ -318,6 +340,16 @@ static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, fl
                                            f.meas ? f.meas + fr * f.meas_stride : nullptr,
                                            f.img ? f.img + fr * f.img_stride : nullptr, fr == 0 ? sens : nullptr,
                                            nullptr, nullptr, h->tune, s);
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
+    if (rs.nr_xy * rs.nr_z > 1) {
+        for (int fr = 0; fr < f.n; ++fr) {
+            const int st = multiray_backward(h->grid, rs, h->tof, h->desc.global_factor,
+                                             f.meas ? f.meas + fr * f.meas_stride : nullptr,
+                                             f.img ? f.img + fr * f.img_stride : nullptr, fr == 0 ? sens : nullptr,
+                                             h->tune.siddon_blocks_per_sm, s);
             if (st != OMB_OK) return st;
         }
         return OMB_OK;
@@ -504,6 +536,8 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
                                   image, sens, s);
     }
     if (mode == OMB_BP_FIXED64) {
+        if (rs.nr_xy * rs.nr_z > 1)
+            return set_error(OMB_ERR_UNSUPPORTED, "the fixed-point backprojection takes one ray per LOR");
         unsigned long long *acc = h->d_acc, *acc_s = sens ? h->d_acc + h->n_img : nullptr;
         OMB_CUDA_TRY(cudaMemsetAsync(h->d_acc, 0, (sens ? 2 : 1) * h->n_img * sizeof(unsigned long long), s));
         if (h->desc.bp_type == 4)

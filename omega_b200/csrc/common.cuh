@@ -55,6 +55,8 @@ struct RaySet {
     float pitch_x, pitch_y;
     const uint16_t *tr; // OMB_PET_INDEXED: transaxial index pairs of all events
     const uint16_t *ax; // OMB_PET_INDEXED: axial index pairs of all events
+    int nr_xy, nr_z;    // PET multi-ray: rays per LOR transaxially / axially (1, 1 = one ray)
+    float cr_xy, cr_z;  // crystal sizes the rays are spread over (mm)
     const float *w;     // PET: multiplicative weight of each of the launch's rays, or NULL
     const float *mu;    // PET: attenuation image (1/mm), or NULL
 };

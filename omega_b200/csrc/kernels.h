@@ -14,6 +14,12 @@ int siddon_backward_fixed(const Grid &g, const RaySet &rs, const Tof &tof, float
 int siddon_count(const Grid &g, const RaySet &rs, const Tof &tof, unsigned long long *total, cudaStream_t st);
 int fixed_to_float(const unsigned long long *acc, float *out, int64_t n, cudaStream_t st);
 
+// Multi-ray PET projections (rs.nr_xy x rs.nr_z rays per LOR), one frame.
+int multiray_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *img, float *y,
+                     int per_sm, cudaStream_t st);
+int multiray_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *y, float *img,
+                      float *sens, int per_sm, cudaStream_t st);
+
 // Projector type 5 (branchless distance-driven), CT.
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
                 int64_t nproj, const float *img, float *imgT, float *y, const Tuning &tn, cudaStream_t st);

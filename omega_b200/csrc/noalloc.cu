@@ -54,6 +54,8 @@ int check_desc(const omb_geometry_desc *d, int32_t subset) {
     if (d->modality != OMB_PET_SINOGRAM && d->modality != OMB_CT_PANEL)
         return set_error(OMB_ERR_INVALID, "modality must be OMB_PET_SINOGRAM or OMB_CT_PANEL");
     if (d->bp_type != 1) return set_error(OMB_ERR_UNSUPPORTED, "the allocation-free backprojection is projector type 1");
+    if (d->n_rays_xy > 1 || d->n_rays_z > 1)
+        return set_error(OMB_ERR_UNSUPPORTED, "the allocation-free backprojection takes one ray per LOR");
     if (d->nx == 0 || d->ny == 0 || d->nz == 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
     const uint64_t n_vox = (uint64_t)d->nx * d->ny * d->nz;
     if (n_vox > (uint64_t)OMB_NOALLOC_MAX_VOXELS)

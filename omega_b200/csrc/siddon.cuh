@@ -107,6 +107,34 @@ __device__ __forceinline__ Ray load_ray(const RaySet &rs, int64_t r) {
     return ray;
 }
 
+// Ray lorZ x lorXY of a multi-ray LOR (multirayCoordinateShiftZ / XY,
+// general_opencl_functions.h:1120-1140): both end points moved by the same
+// offset, the rays spaced evenly over the crystal, axial shift first.
+__device__ __forceinline__ Ray multiray_shift(Ray ray, const RaySet &rs, int lor_xy, int lor_z) {
+    if (rs.nr_z > 1) {
+        float interval = rs.cr_z / (float)(rs.nr_z * 2);
+        ray.s.z += (interval - rs.cr_z / 2.f);
+        ray.d.z += (interval - rs.cr_z / 2.f);
+        interval *= 2.f;
+        ray.s.z += interval * lor_z;
+        ray.d.z += interval * lor_z;
+    }
+    if (rs.nr_xy > 1) {
+        float interval = rs.cr_xy / (float)(rs.nr_xy * 2);
+        const float c = interval - rs.cr_xy / 2.f;
+        ray.s.x += c;
+        ray.d.x += c;
+        ray.s.y += c;
+        ray.d.y += c;
+        interval *= 2.f;
+        ray.s.x += interval * lor_xy;
+        ray.d.x += interval * lor_xy;
+        ray.s.y += interval * lor_xy;
+        ray.d.y += interval * lor_xy;
+    }
+    return ray;
+}
+
 __device__ __forceinline__ int perpendicular_start(double b, double d, double dd, int n) {
     int t = (int)floor((d - b) / dd);
     if (t < 0 || t >= n) t = 0;

@@ -577,6 +577,9 @@ class projectorClass:
             d.d_scale5[0], d.d_scale5[1], d.d_scale5[2] = (float(self.dScaleX[0]), float(self.dScaleY[0]),
                                                            float(self.dScaleZ[0]))
         d.fixed64_workspace = 1 if self.use_64bit_atomics else 0
+        if not self.CT:
+            d.n_rays_xy = int(self.n_rays_transaxial)
+            d.n_rays_z = int(self.n_rays_axial)
         if self.listmode and self.useIndexBasedReconstruction:
             keep['tr'] = np.ascontiguousarray(np.asarray(self.trIndex, dtype=np.uint16).ravel())
             keep['ax'] = np.ascontiguousarray(np.asarray(self.axIndex, dtype=np.uint16).ravel())

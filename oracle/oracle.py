@@ -59,6 +59,8 @@ class OracleGeom(ctypes.Structure):
         ("mu", ctypes.POINTER(ctypes.c_double)),
         ("tr", ctypes.POINTER(ctypes.c_uint16)),
         ("ax", ctypes.POINTER(ctypes.c_uint16)),
+        ("nr_xy", ctypes.c_int), ("nr_z", ctypes.c_int),
+        ("cr_xy", ctypes.c_double), ("cr_z", ctypes.c_double),
     ]
 
 
@@ -106,6 +108,8 @@ def ref_lib():
         P = ctypes.POINTER(ctypes.c_double)
         L.ref_listmode_d.argtypes = [ctypes.c_int, u, u, u] + [ctypes.c_double] * 6 + [ctypes.c_int64, P, P, P, P,
                                                                                       ctypes.c_double, ctypes.c_double, u]
+        L.ref_multiray_d.argtypes = [ctypes.c_int, u, u, u] + [ctypes.c_double] * 6 + [u, u, u] + [P] * 5 + \
+            [u, ctypes.c_double, P, ctypes.c_double, ctypes.c_double, u, u, u, ctypes.c_double, ctypes.c_double]
         L.ref_siddon_corr_d.argtypes = [ctypes.c_int, u, u, u] + [ctypes.c_double] * 6 + [u, u, u] + [P] * 5 + \
             [u, ctypes.c_double, P, ctypes.c_double, ctypes.c_double, u, P, P, ctypes.c_int, P]
         _ref = L
@@ -143,6 +147,10 @@ class Geometry:
         # projector type 4: sampling length and the CT backprojection weight
         self.dL = float(o.dL)
         self.kerroin = float(np.ravel(o.kerroin)[0]) if np.size(o.kerroin) else 0.0
+        # PET multi-ray: rays per LOR over the crystal pitches (dPitchX
+        # transaxially, dPitchY axially, as the reference's kernels take them)
+        self.nr_xy = 1 if self.ct else int(getattr(o, 'n_rays_transaxial', 1))
+        self.nr_z = 1 if self.ct else int(getattr(o, 'n_rays_axial', 1))
         # PET corrections: weight per measurement of all subsets (subset
         # order) and attenuation image, FP64; None when off
         self.w = None
@@ -199,6 +207,8 @@ class Geometry:
         if self.mu is not None:
             self._mu = np.ascontiguousarray(self.mu, dtype=np.float64).ravel()
             g.mu = self._mu.ctypes.data_as(P)
+        g.nr_xy, g.nr_z = self.nr_xy, self.nr_z
+        g.cr_xy, g.cr_z = self.pitch
         if self.modality == 3:
             U = ctypes.POINTER(ctypes.c_uint16)
             g.tr = self.tr.ctypes.data_as(U)
@@ -323,6 +333,26 @@ def ref_corrected(geom: Geometry, inp, subset, fp, norm=None, atten=None, ct_att
     L.ref_siddon_corr_d(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, geom.n_rows, geom.n_cols,
                         n1 - n0, p(xy), p(z), p(inp), p(out), p(s), geom.nbins, geom.sigma_x, p(tofc),
                         geom.global_factor, geom.epps, int(threads), p(norm), p(atten), 1 if ct_atten else 0, p(scat))
+    return (out, s) if sens else out
+
+
+def ref_multiray(geom: Geometry, inp, subset, fp, threads=0, sens=False):
+    """The reference CPU projector (FP64) with geom.nr_xy x geom.nr_z rays per
+    LOR over the crystal pitches geom.pitch.  Whole-sinogram subsets."""
+    L = ref_lib()
+    P = ctypes.POINTER(ctypes.c_double)
+    p = (lambda a: a.ctypes.data_as(P) if a is not None else None)
+    n0, n1 = (0, geom.n_proj) if subset < 0 else (int(geom.n_meas[subset]), int(geom.n_meas[subset + 1]))
+    xy = geom.xy.astype(np.float64)
+    z = np.ascontiguousarray(geom.z.astype(np.float64)[n0 * 2:n1 * 2])
+    inp = np.ascontiguousarray(inp, dtype=np.float64).ravel()
+    nmeas = geom.n_rows * geom.n_cols * (n1 - n0)
+    out = np.zeros(nmeas * geom.nbins if fp else geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    tofc = geom.tofc.astype(np.float64)
+    L.ref_multiray_d(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, geom.n_rows, geom.n_cols, n1 - n0,
+                     p(xy), p(z), p(inp), p(out), p(s), geom.nbins, geom.sigma_x, p(tofc), geom.global_factor,
+                     geom.epps, int(threads), geom.nr_xy, geom.nr_z, geom.pitch[0], geom.pitch[1])
     return (out, s) if sens else out
 
 

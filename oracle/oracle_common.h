@@ -32,7 +32,11 @@ typedef struct oracle_geom {
     /* modality 3 (index-based events): index pairs of every event */
     const uint16_t *tr;
     const uint16_t *ax;
+    /* PET multi-ray: rays per LOR and the crystal sizes they spread over */
+    int nr_xy, nr_z;
+    double cr_xy, cr_z;
 } oracle_geom;
+
 
 typedef struct { double x, y, z; } v3;
 
@@ -86,6 +90,24 @@ static void load_ray(const oracle_geom *g, int64_t r, v3 *s, v3 *d) {
         d->x += ia * ux;
         d->y += ia * uy;
         d->z += ib * g->pitch_y;
+    }
+}
+
+/* Ray lor_z x lor_xy of a multi-ray LOR (multirayCoordinateShiftZ / XY,
+ * projector_functions.h:440-461): both end points moved alike. */
+static void multiray_shift(const oracle_geom *g, int lor_xy, int lor_z, v3 *s, v3 *d) {
+    if (g->nr_z > 1) {
+        double iv = g->cr_z / (double)(g->nr_z * 2);
+        s->z += iv - g->cr_z / 2.0; d->z += iv - g->cr_z / 2.0;
+        iv *= 2.0;
+        s->z += iv * lor_z; d->z += iv * lor_z;
+    }
+    if (g->nr_xy > 1) {
+        double iv = g->cr_xy / (double)(g->nr_xy * 2);
+        double c = iv - g->cr_xy / 2.0;
+        s->x += c; d->x += c; s->y += c; d->y += c;
+        iv *= 2.0;
+        s->x += iv * lor_xy; d->x += iv * lor_xy; s->y += iv * lor_xy; d->y += iv * lor_xy;
     }
 }
 

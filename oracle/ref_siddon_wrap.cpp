@@ -18,7 +18,8 @@ template <typename T>
 static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, T bx, T by, T bz, uint32_t n_rows,
                uint32_t n_cols, uint32_t n_proj, const T *xy, const T *z, T *input, T *output, T *sens, uint32_t nbins,
                T sigma_x, T *tof_centers, T global_factor, T epps, uint32_t n_threads, T *norm = nullptr,
-               T *atten = nullptr, int ct_atten = 1, T *scat = nullptr) {
+               T *atten = nullptr, int ct_atten = 1, T *scat = nullptr, uint16_t n_rays_xy = 1,
+               uint16_t n_rays_z = 1, T cr_xy = 0, T cr_z = 0) {
     paramStruct<T> p;
     p.subsetType = 8;
     p.subsets = 1;
@@ -46,6 +47,11 @@ static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, 
     p.atten = atten;
     p.scatterCorrectionMult = scat != nullptr;
     p.scatterCoefs = scat;
+    // multi-ray: rays over the crystal pitch (dPitchXY transaxially, dPitchZ axially)
+    p.nRays2D = n_rays_xy;
+    p.nRays3D = n_rays_z;
+    p.dPitchXY = cr_xy;
+    p.dPitchZ = cr_z;
     const int64_t n_meas = (int64_t)n_rows * n_cols * n_proj;
     projectorType123Implementation4<T>(p, n_meas, output, xy, z, input, false, false, (uint8_t)(fp ? 1 : 2), sens,
                                        nullptr, n_threads);
@@ -82,6 +88,16 @@ int ref_listmode_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, dou
     projectorType123Implementation4<double>(p, n_events, output, xyz, &z0, input, false, false, (uint8_t)(fp ? 1 : 2),
                                             sens, nullptr, n_threads);
     return 0;
+}
+/* Multi-ray sinogram projection: n_rays_xy x n_rays_z rays per LOR. */
+int ref_multiray_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx,
+                   double by, double bz, uint32_t n_rows, uint32_t n_cols, uint32_t n_proj, const double *xy,
+                   const double *z, double *input, double *output, double *sens, uint32_t nbins, double sigma_x,
+                   double *tof_centers, double global_factor, double epps, uint32_t n_threads, uint32_t n_rays_xy,
+                   uint32_t n_rays_z, double cr_xy, double cr_z) {
+    return run<double>(fp, nx, ny, nz, dx, dy, dz, bx, by, bz, n_rows, n_cols, n_proj, xy, z, input, output, sens,
+                       nbins, sigma_x, tof_centers, global_factor, epps, n_threads, nullptr, nullptr, 1, nullptr,
+                       (uint16_t)n_rays_xy, (uint16_t)n_rays_z, cr_xy, cr_z);
 }
 /* With PET corrections: norm / scat per measurement of the call (NULL: off);
  * atten: image (ct_atten != 0) or per measurement (ct_atten == 0), NULL: off. */

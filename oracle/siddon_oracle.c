@@ -135,9 +135,11 @@ typedef void (*visit_fn)(void *ctx, int64_t ind, double ele, const double *w, do
  * normalisation.  full_row: a ray along an image row visits every voxel of
  * the row at full length (the reference CPU projector's row attenuation sum,
  * projector_functions.h:1193-1205). */
-static int walk_ex(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, void *ctx, int full_row) {
+static int walk_ex(const oracle_geom *g, int64_t r, int lxy, int lz, double *temp, visit_fn vis, void *ctx,
+                   int full_row) {
     v3 s, d;
     load_ray(g, r, &s, &d);
+    multiray_shift(g, lxy, lz, &s, &d);
     const double mx = g->bx + (double)g->nx * g->dx;
     const double my = g->by + (double)g->ny * g->dy;
     const double mz = g->bz + (double)g->nz * g->dz;
@@ -146,7 +148,8 @@ static int walk_ex(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, 
         isnan(diff.y) || isnan(diff.z))
         return 0;
     const double L = sqrt(diff.x * diff.x + diff.y * diff.y + diff.z * diff.z);
-    *temp = g->modality != 1 ? (1.0 / L) * g->global_factor : 1.0;
+    const int nrays = (g->nr_xy > 1 ? g->nr_xy : 1) * (g->nr_z > 1 ? g->nr_z : 1);
+    *temp = g->modality != 1 ? (1.0 / (L * nrays)) * g->global_factor : 1.0;
     const int64_t nxy = (int64_t)g->nx * g->ny;
     double w[MAXB];
     const int tofon = g->nbins > 1;
@@ -255,8 +258,10 @@ static int walk_ex(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, 
 }
 
 static int walk(const oracle_geom *g, int64_t r, double *temp, visit_fn vis, void *ctx) {
-    return walk_ex(g, r, temp, vis, ctx, 0);
+    return walk_ex(g, r, 0, 0, temp, vis, ctx, 0);
 }
+
+static int nr(int n) { return n > 1 ? n : 1; }
 
 typedef struct { const double *mu; double jel; } atn_ctx;
 
@@ -267,13 +272,13 @@ static void atn_visit(void *c, int64_t ind, double ele, const double *w, double 
 }
 
 /* Correction factor of PET ray r: its weight times exp(-line integral of mu). */
-static double ray_corr(const oracle_geom *g, int64_t r) {
+static double ray_corr(const oracle_geom *g, int64_t r, int lxy, int lz) {
     if (g->modality == 1) return 1.0;
     double f = g->w ? g->w[r] : 1.0;
     if (g->mu) {
         atn_ctx a = {g->mu, 0.0};
         double t;
-        walk_ex(g, r, &t, atn_visit, &a, 1);
+        walk_ex(g, r, lxy, lz, &t, atn_visit, &a, 1);
         f *= exp(a.jel);
     }
     return f;
@@ -293,14 +298,20 @@ int oracle_siddon_fp(const oracle_geom *g, const double *img, double *y) {
     if (g->nbins < 1 || g->nbins > MAXB) return -1;
 #pragma omp parallel for schedule(dynamic, 256)
     for (int64_t r = 0; r < g->m_size; ++r) {
-        fp_ctx f;
-        f.img = img;
-        f.nb = g->nbins;
-        for (int to = 0; to < g->nbins; ++to) f.ax[to] = 0.0;
-        double temp = 0.0;
-        int ok = walk(g, r, &temp, fp_visit, &f);
-        const double corr = ok ? ray_corr(g, r) : 0.0;
-        for (int to = 0; to < g->nbins; ++to) y[r + to * g->m_size] = ok ? f.ax[to] * temp * corr : 0.0;
+        double out[MAXB];
+        for (int to = 0; to < g->nbins; ++to) out[to] = 0.0;
+        for (int lz = 0; lz < nr(g->nr_z); ++lz)
+            for (int lxy = 0; lxy < nr(g->nr_xy); ++lxy) {
+                fp_ctx f;
+                f.img = img;
+                f.nb = g->nbins;
+                for (int to = 0; to < g->nbins; ++to) f.ax[to] = 0.0;
+                double temp = 0.0;
+                int ok = walk_ex(g, r, lxy, lz, &temp, fp_visit, &f, 0);
+                const double corr = ok ? ray_corr(g, r, lxy, lz) : 0.0;
+                for (int to = 0; to < g->nbins; ++to) out[to] += ok ? f.ax[to] * temp * corr : 0.0;
+            }
+        for (int to = 0; to < g->nbins; ++to) y[r + to * g->m_size] = out[to];
     }
     return 0;
 }
@@ -339,14 +350,19 @@ int oracle_siddon_bp(const oracle_geom *g, const double *y, double *img, double 
             any |= b.ax[to] != 0.0;
         }
         if (!any) continue;
-        /* temp is set by walk() before the first visit */
-        double temp = 0.0;
-        v3 s, d;
-        load_ray(g, r, &s, &d);
-        double dxl = d.x - s.x, dyl = d.y - s.y, dzl = d.z - s.z;
-        double L = sqrt(dxl * dxl + dyl * dyl + dzl * dzl);
-        b.temp = g->modality != 1 ? (1.0 / L) * g->global_factor * ray_corr(g, r) : 1.0;
-        walk(g, r, &temp, bp_visit, &b);
+        const int nrays = nr(g->nr_xy) * nr(g->nr_z);
+        for (int lz = 0; lz < nr(g->nr_z); ++lz)
+            for (int lxy = 0; lxy < nr(g->nr_xy); ++lxy) {
+                /* the visitor needs the ray's normalisation before the walk sets it */
+                double temp = 0.0;
+                v3 s, d;
+                load_ray(g, r, &s, &d);
+                multiray_shift(g, lxy, lz, &s, &d);
+                double dxl = d.x - s.x, dyl = d.y - s.y, dzl = d.z - s.z;
+                double L = sqrt(dxl * dxl + dyl * dyl + dzl * dzl);
+                b.temp = g->modality != 1 ? (1.0 / (L * nrays)) * g->global_factor * ray_corr(g, r, lxy, lz) : 1.0;
+                walk_ex(g, r, lxy, lz, &temp, bp_visit, &b, 0);
+            }
     }
     return 0;
 }
