@@ -275,6 +275,42 @@ int omb_set_read_precision(omb_handle *h, int32_t mode, int32_t max_frames);
 int omb_get_tuning(const omb_handle *h, omb_tuning *out);
 
 /*
+ * The built-in reconstruction behind one call (the reference's compiled
+ * omegaMain entry, libHeader.h:1466, with reconstructionAF.h:1053-1500, for
+ * the algorithms of this path).  Explicit parameters instead of the
+ * reference's 200-field options struct.
+ */
+typedef enum omb_recon_algorithm {
+    OMB_RECON_OSEM = 1,     /* options.OSEM: per-subset sensitivity images, EM update per subset (PET) */
+    OMB_RECON_PDHG_TV = 2   /* options.PDHG with options.TV: one subset, smoothed TV gradient */
+} omb_recon_algorithm;
+
+typedef struct omb_recon_params {
+    uint32_t struct_size;     /* sizeof(omb_recon_params) */
+    int32_t algorithm;        /* omb_recon_algorithm */
+    int32_t n_iter;           /* options.Niter */
+    float beta;               /* PDHG: TV weight (options.beta) */
+    float tv_smoothing;       /* PDHG: options.TVsmoothing */
+    float tau;                /* PDHG primal step (options.tauCP); <= 0: 1 / the power-method eigenvalue */
+    float sigma;              /* PDHG dual step (options.sigmaCP) */
+    float theta;              /* PDHG extrapolation (options.thetaCP) */
+    int32_t power_iterations; /* options.powerIterations (0: 20) */
+    int32_t positivity;       /* options.enforcePositivity */
+    int32_t use_graph;        /* nonzero: capture one iteration as a CUDA graph and replay it */
+    float tau_used;           /* out: the primal step of the run */
+} omb_recon_params;
+
+/*
+ * Runs p->n_iter iterations from x0 (device, one image) into x_out (device).
+ * y (device): OSEM, the measurements of all subsets concatenated in subset
+ * order, each subset as omb_osem_subset takes it (TOF bins outermost); PDHG,
+ * the measurement vector of all subsets (omb_measurement_count(h, -1)).
+ * Allocates its scratch with cudaMallocAsync on `stream` (OSEM: one image
+ * per subset for the sensitivities) and synchronises `stream` on return.
+ */
+int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const float *x0, float *x_out, void *stream);
+
+/*
  * PET corrections of the projector type-1 forward and backward projections
  * (the reference's NORM, SCATTER, ATNM and ATN kernel options,
  * projectorType123.cl:373-376, 975-987; CPU projector

@@ -75,6 +75,28 @@ class GeometryDesc(ctypes.Structure):
     ]
 
 
+class ReconParams(ctypes.Structure):
+    """Mirror of ``omb_recon_params``."""
+    _fields_ = [
+        ("struct_size", ctypes.c_uint32),
+        ("algorithm", ctypes.c_int32),
+        ("n_iter", ctypes.c_int32),
+        ("beta", ctypes.c_float),
+        ("tv_smoothing", ctypes.c_float),
+        ("tau", ctypes.c_float),
+        ("sigma", ctypes.c_float),
+        ("theta", ctypes.c_float),
+        ("power_iterations", ctypes.c_int32),
+        ("positivity", ctypes.c_int32),
+        ("use_graph", ctypes.c_int32),
+        ("tau_used", ctypes.c_float),
+    ]
+
+
+OMB_RECON_OSEM = 1
+OMB_RECON_PDHG_TV = 2
+
+
 class Tuning(ctypes.Structure):
     """Mirror of ``omb_tuning``."""
     _fields_ = [
@@ -138,6 +160,8 @@ EXPORTS = [
     ("omb_power_workspace_bytes", ctypes.c_size_t, []),
     ("omb_set_read_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     ("omb_take_device_error", ctypes.c_int, []),
+    ("omb_reconstruct", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ReconParams), ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_set_randoms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     ("omb_set_corrections", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_void_p]),

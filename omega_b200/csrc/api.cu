@@ -358,6 +358,8 @@ static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, fl
     return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, sens, h->tune, s);
 }
 
+int omb::handle_subsets(const omb_handle *h) { return h ? h->desc.n_subsets : 0; }
+
 extern "C" {
 
 int omb_abi_version(void) { return OMB_ABI_VERSION; }

@@ -1,0 +1,158 @@
+// The built-in reconstruction loop behind one call (the reference's compiled
+// omegaMain entry, libHeader.h:1466, reconstructionAF.h:1053-1500, for the two
+// algorithms of this path): OSEM for PET data and PDHG with the smoothed TV
+// gradient, with every sub-iteration issued on the caller's stream by the
+// same entry points a custom loop uses, and (use_graph) one iteration captured
+// as a CUDA graph and replayed.
+#include <cmath>
+#include <random>
+#include <vector>
+
+#include "kernels.h"
+
+namespace omb {
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    cudaStream_t s = nullptr;
+    ~DevBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+    float *f() const { return static_cast<float *>(p); }
+};
+
+int alloc(DevBuf &b, size_t bytes, cudaStream_t s) {
+    b.s = s;
+    OMB_CUDA_TRY(cudaMallocAsync(&b.p, bytes > 0 ? bytes : 4, s));
+    return OMB_OK;
+}
+
+// Runs `body` n times: eagerly, or captured once as a graph and replayed.
+template <class F>
+int repeat(int n, bool use_graph, cudaStream_t s, F &&body) {
+    if (!use_graph || n < 2 || s == nullptr) {
+        for (int i = 0; i < n; ++i) {
+            const int st = body();
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
+    int st = body();  // warm-up outside the capture (lazy scratch allocations happen here)
+    if (st != OMB_OK) return st;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    OMB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    st = body();
+    const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (st != OMB_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "graph capture of a reconstruction iteration");
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    for (int i = 1; i < n && e == cudaSuccess; ++i) e = cudaGraphLaunch(exec, s);
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "graph replay of a reconstruction iteration");
+    return OMB_OK;
+}
+
+}  // namespace
+}  // namespace omb
+
+using namespace omb;
+
+extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const float *x0, float *x_out,
+                               void *stream) {
+    if (!h || !p) return set_error(OMB_ERR_INVALID, "handle/params pointer is NULL");
+    if (p->struct_size != sizeof(omb_recon_params))
+        return set_error(OMB_ERR_INVALID, "omb_recon_params.struct_size does not match this library");
+    if (!y || !x0 || !x_out) return set_error(OMB_ERR_INVALID, "y/x0/x_out pointer is NULL");
+    if (p->n_iter < 0) return set_error(OMB_ERR_INVALID, "n_iter must be >= 0");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t n = omb_image_count(h);
+    if (n < 0) return -1;
+    const int32_t n_subsets = handle_subsets(h);
+    OMB_CUDA_TRY(cudaMemcpyAsync(x_out, x0, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    const bool graph = p->use_graph != 0;
+    int st = OMB_OK;
+    if (p->algorithm == OMB_RECON_OSEM) {
+        // per-subset sensitivity images, then sub-iterations in subset order
+        std::vector<int64_t> off(n_subsets + 1, 0);
+        int64_t m_max = 0;
+        for (int s_ = 0; s_ < n_subsets; ++s_) {
+            const int64_t ms = omb_measurement_count(h, s_);
+            off[s_ + 1] = off[s_] + ms;
+            m_max = ms > m_max ? ms : m_max;
+        }
+        DevBuf sens, wm, wi;
+        if ((st = alloc(sens, (size_t)n_subsets * n * sizeof(float), s)) != OMB_OK) return st;
+        if ((st = alloc(wm, (size_t)m_max * sizeof(float), s)) != OMB_OK) return st;
+        if ((st = alloc(wi, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        for (int s_ = 0; s_ < n_subsets && st == OMB_OK; ++s_) st = omb_sensitivity(h, s_, sens.f() + s_ * n, stream);
+        if (st != OMB_OK) return st;
+        st = repeat(p->n_iter, graph, s, [&]() {
+            for (int s_ = 0; s_ < n_subsets; ++s_) {
+                const int e = omb_osem_subset(h, s_, x_out, y + off[s_], sens.f() + s_ * n, wm.f(), wi.f(), stream);
+                if (e != OMB_OK) return e;
+            }
+            return (int)OMB_OK;
+        });
+    } else if (p->algorithm == OMB_RECON_PDHG_TV) {
+        const int64_t m_all = omb_measurement_count(h, -1);  // one subset: all measurements
+        if (m_all < 0) return -1;
+        DevBuf xn, u, pd, wm, wi, work;
+        if ((st = alloc(xn, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        if ((st = alloc(u, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        if ((st = alloc(pd, (size_t)m_all * sizeof(float), s)) != OMB_OK) return st;
+        if ((st = alloc(wm, (size_t)m_all * sizeof(float), s)) != OMB_OK) return st;
+        if ((st = alloc(wi, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        float tau = p->tau;
+        if (!(tau > 0.f)) {
+            // |N(0,1)| start normalised to unit length (functions.hpp:2430-2437)
+            if ((st = alloc(work, omb_power_workspace_bytes(), s)) != OMB_OK) return st;
+            std::vector<float> v((size_t)n);
+            std::mt19937 rng(1u);
+            std::normal_distribution<float> nd(0.f, 1.f);
+            double norm = 0.0;
+            for (auto &a : v) {
+                a = std::fabs(nd(rng));
+                norm += (double)a * a;
+            }
+            const float inv = (float)(1.0 / std::sqrt(norm));
+            for (auto &a : v) a *= inv;
+            OMB_CUDA_TRY(cudaMemcpyAsync(xn.p, v.data(), (size_t)n * sizeof(float), cudaMemcpyHostToDevice, s));
+            double L = 0.0;
+            st = omb_power_method(h, p->power_iterations > 0 ? p->power_iterations : 20, xn.f(), wm.f(), wi.f(),
+                                  work.p, &L, stream);
+            if (st != OMB_OK) return st;
+            if (!(L > 0.0)) return set_error(OMB_ERR_INVALID, "power method gave a non-positive eigenvalue");
+            tau = (float)(1.0 / L);
+        }
+        p->tau_used = tau;
+        OMB_CUDA_TRY(cudaMemcpyAsync(u.p, x_out, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        OMB_CUDA_TRY(cudaMemsetAsync(pd.p, 0, (size_t)m_all * sizeof(float), s));
+        // two iterations per repetition keep x_out / xn in place for graph replays
+        auto two = [&]() {
+            int e = omb_pdhg_iteration(h, x_out, xn.f(), u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
+                                       p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
+            if (e == OMB_OK)
+                e = omb_pdhg_iteration(h, xn.f(), x_out, u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
+                                       p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
+            return e;
+        };
+        st = repeat(p->n_iter / 2, graph, s, two);
+        if (st == OMB_OK && p->n_iter % 2) {
+            st = omb_pdhg_iteration(h, x_out, xn.f(), u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
+                                    p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
+            if (st == OMB_OK)
+                OMB_CUDA_TRY(cudaMemcpyAsync(x_out, xn.p, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        }
+    } else {
+        return set_error(OMB_ERR_INVALID, "unknown reconstruction algorithm");
+    }
+    if (st != OMB_OK) return st;
+    OMB_CUDA_TRY(cudaStreamSynchronize(s));
+    return OMB_OK;
+}

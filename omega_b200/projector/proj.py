@@ -116,6 +116,21 @@ class projectorClass:
     TOF_offset = 0.
     TOFCenter = np.empty(0, dtype=np.float32)
     sigma_x = 0.
+    # Built-in reconstruction (reconstructions_main): the algorithms of this
+    # path and their parameters (proj.py:116-120, 236, 271, 275, 317, 370-420)
+    OSEM = False
+    PDHG = False
+    TV = False
+    MAP = False
+    beta = 0.
+    TVsmoothing = 1e-4
+    tauCP = 0.
+    sigmaCP = 1.
+    thetaCP = 1.
+    powerIterations = 20
+    enforcePositivity = True
+    usingLinearizedData = False
+    storeFP = False
     # Projector
     projector_type = 11
     n_rays_transaxial = 1

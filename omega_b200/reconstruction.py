@@ -223,3 +223,72 @@ class OSEMBatch:
         for _ in range(n_iter):
             self.graph.replay()
         return self.x
+
+
+def reconstructions_main(options):
+    """The built-in reconstruction (omegatomo/reconstruction/recomain.py:427-725,
+    the compiled omegaMain entry) for the algorithms of this path:
+    options.OSEM (PET) or options.PDHG with options.TV, options.Niter
+    iterations from options.x0, run natively by omb_reconstruct.  CT data are
+    linearised as log(flat / SinM) first (prepass.py:22-36; flat = max(SinM)
+    when options.flat <= 0), negative PET counts set to 0.  Returns
+    (image of shape (Nx, Ny, Nz, 1) in Fortran order, empty forward
+    projections), as the reference does with storeFP off.  Reads
+    options.use_graph (default True) to replay iterations as CUDA graphs."""
+    import torch
+    if not (options.OSEM or options.PDHG):
+        raise ValueError('No reconstruction method selected, aborting.')
+    if options.OSEM and options.PDHG:
+        raise ValueError('Select one reconstruction method (OSEM or PDHG)')
+    if options.PDHG and not options.TV:
+        raise ValueError('PDHG is built with the TV prior (options.TV = True)')
+    if options.OSEM and options.CT:
+        raise ValueError('OSEM is built for PET data')
+    sin = np.asarray(options.SinM, dtype=np.float32)
+    if options.CT and not options.usingLinearizedData:
+        if options.flat <= 0:
+            options.flat = float(np.max(sin))
+        sin = np.log(np.float32(options.flat) / sin).astype(np.float32)
+        options.usingLinearizedData = True
+    elif not options.CT:
+        sin = np.where(sin < 0, 0, sin).astype(np.float32)
+    options.SinM = sin
+    if not options.projectorAdded:
+        options.addProjector()
+    options.initProj()  # reorders SinM (and the correction vectors) into subset order
+    dev = torch.device("cuda", options._device)
+    n = int(np.ravel(options.N)[0])
+    m = np.asarray(options.SinM, dtype=np.float32).ravel(order='F')
+    S = int(options.subsets)
+    if options.OSEM:
+        parts = [np.asarray(options.subsetMeasurements(m, s)) for s in range(S)]
+        y = torch.from_numpy(np.ascontiguousarray(np.concatenate(parts), dtype=np.float32)).to(dev)
+    else:
+        y = torch.from_numpy(np.ascontiguousarray(m, dtype=np.float32)).to(dev)
+    x0 = np.asarray(options.x0, dtype=np.float32).ravel(order='F')
+    if x0.size != n:
+        x0 = np.ones(n, dtype=np.float32) * (float(x0[0]) if x0.size else 1e-4)
+    x0 = torch.from_numpy(np.ascontiguousarray(x0)).to(dev)
+    x = torch.empty(n, device=dev)
+    p = _native.ReconParams(struct_size=ctypes.sizeof(_native.ReconParams))
+    p.algorithm = _native.OMB_RECON_OSEM if options.OSEM else _native.OMB_RECON_PDHG_TV
+    p.n_iter = int(options.Niter)
+    p.beta = float(options.beta)
+    p.tv_smoothing = float(options.TVsmoothing)
+    p.tau = float(np.ravel(options.tauCP)[0]) if np.size(options.tauCP) else 0.0
+    p.sigma = float(np.ravel(options.sigmaCP)[0])
+    p.theta = float(np.ravel(options.thetaCP)[0])
+    p.power_iterations = int(options.powerIterations)
+    p.positivity = 1 if options.enforcePositivity else 0
+    p.use_graph = 1 if getattr(options, 'use_graph', True) else 0
+    _native.call("omb_reconstruct", options._handle, ctypes.byref(p), _ptr(y), _ptr(x0), _ptr(x), _stream(dev))
+    options.tau_used = p.tau_used
+    out = x.cpu().numpy().reshape((int(np.ravel(options.Nx)[0]), int(np.ravel(options.Ny)[0]),
+                                   int(np.ravel(options.Nz)[0]), 1), order='F')
+    return out, np.empty(0, dtype=np.float32)
+
+
+def reconstructions_mainCT(options):
+    """CT entry of the built-in reconstruction (recomain.py:377-401)."""
+    options.CT = True
+    return reconstructions_main(options)
