@@ -311,6 +311,24 @@ typedef struct omb_recon_params {
 int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const float *x0, float *x_out, void *stream);
 
 /*
+ * PSF blur (Convolution3D_f, auxKernels.cl:192-245): out = window applied at
+ * every voxel of `in` (device), the window (device, (2gx+1)(2gy+1)(2gz+1)
+ * weights, x fastest; proj.py PSFKernel gives the Gaussian one) read with the
+ * image mirrored at its faces, edge voxel repeated.  The reference blurs
+ * before the forward projection and after the backprojection.  Not in place.
+ */
+int omb_psf_convolve(const float *in, float *out, int32_t nx, int32_t ny, int32_t nz, const float *window,
+                     int32_t gx, int32_t gy, int32_t gz, void *stream);
+
+/*
+ * Relative difference prior gradient (RDPKernel, auxKernels.cl:664-872,
+ * 6-neighbour form; neighbours outside the image read 0 as with the CUDA
+ * border addressing): grad += beta * dRDP(u)/du with parameters gamma, epps.
+ */
+int omb_rdp_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float gamma, float epps,
+                     float beta, void *stream);
+
+/*
  * PET corrections of the projector type-1 forward and backward projections
  * (the reference's NORM, SCATTER, ATNM and ATN kernel options,
  * projectorType123.cl:373-376, 975-987; CPU projector

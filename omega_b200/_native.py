@@ -160,6 +160,12 @@ EXPORTS = [
     ("omb_power_workspace_bytes", ctypes.c_size_t, []),
     ("omb_set_read_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     ("omb_take_device_error", ctypes.c_int, []),
+    ("omb_psf_convolve", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_void_p]),
+    ("omb_rdp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                        ctypes.c_void_p]),
     ("omb_reconstruct", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ReconParams), ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_set_randoms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),

@@ -131,6 +131,10 @@ class projectorClass:
     enforcePositivity = True
     usingLinearizedData = False
     storeFP = False
+    # PSF blur around the projections (proj.py:1885-1911, projfunctions.py:
+    # 194-200, 1403-1407): FWHM (mm) in x, y (and z)
+    use_psf = False
+    FWHM = np.array([0., 0., 0.], dtype=np.float32)
     # Projector
     projector_type = 11
     n_rays_transaxial = 1
@@ -342,6 +346,7 @@ class projectorClass:
         self.z_center = np.array(self.bz[0].item(), ndmin=1).astype(np.float32)
         if self.projector_type in (4, 5, 14, 41, 15, 45, 54, 51, 42, 43, 24, 34):
             geo.projector_scaling(self)
+        self.PSFKernel()
         if self.nMeas.size == 1:
             self.nMeas = np.insert(self.nMeas, 0, 0)
         if self.subsets > 1:
@@ -365,6 +370,43 @@ class projectorClass:
     # List-mode and index-based event data (proj.py:777-850, 862-905;
     # indices.py:79-160, 346-412)
     # ------------------------------------------------------------------
+    def PSFKernel(self):
+        """The Gaussian PSF window (proj.py:1885-1911): half-widths
+        ceil(2 sigma / d) voxels per axis (no z blur with two FWHM values),
+        exp(-sum x^2 / (2 sigma^2)) normalised to sum 1, float32, x fastest."""
+        if not self.use_psf:
+            return
+        # Python floats (weak scalars): the window is computed in float32, as the reference's
+        fw = [float(v) for v in np.ravel(self.FWHM)]
+        k = 2. * math.sqrt(2. * math.log(2.))
+        d = [float(np.ravel(v)[0]) for v in (self.dx, self.dy, self.dz)]
+        g = [math.ceil(2. * (fw[i] / k) / d[i]) for i in range(2)]
+        g.append(math.ceil(2. * (fw[2] / k) / d[2]) if len(fw) >= 3 else 0)
+        ax = [np.linspace(-g[i] * d[i], g[i] * d[i], 2 * g[i] + 1, dtype=np.float32) for i in range(2)]
+        X = ax[0].reshape(-1, 1, 1)
+        Y = ax[1].reshape(1, -1, 1)
+        sx, sy = fw[0] / k, fw[1] / k
+        if len(fw) >= 3:
+            Z = np.linspace(-g[2] * d[2], g[2] * d[2], 2 * g[2] + 1, dtype=np.float32).reshape(1, 1, -1)
+            gk = np.exp(-(X ** 2 / (2. * sx ** 2) + Y ** 2 / (2. * sy ** 2) + Z ** 2 / (2. * (fw[2] / k) ** 2)))
+        else:
+            gk = np.exp(-(X ** 2 / (2. * sx ** 2) + Y ** 2 / (2. * sy ** 2)))
+        self.gaussK = np.asfortranarray((gk / np.sum(gk)).astype(np.float32))
+        self.g_dim_x, self.g_dim_y, self.g_dim_z = g
+
+    def _psf(self, f):
+        """f blurred by the PSF window (a new device tensor)."""
+        import torch
+        if getattr(self, '_d_psf', None) is None or self._d_psf.device != f.device:
+            self._d_psf = torch.from_numpy(np.ascontiguousarray(np.ravel(self.gaussK, order='F'),
+                                                                dtype=np.float32)).to(f.device)
+        out = torch.empty_like(f)
+        nx, ny, nz = self._n(self.Nx), self._n(self.Ny), self._n(self.Nz)
+        _native.call("omb_psf_convolve", ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(out.data_ptr()), nx, ny,
+                     nz, ctypes.c_void_p(self._d_psf.data_ptr()), int(self.g_dim_x), int(self.g_dim_y),
+                     int(self.g_dim_z), ctypes.c_void_p(torch.cuda.current_stream(f.device).cuda_stream))
+        return out
+
     def _listmode_setup(self):
         """Detects event data: 6 coordinates per event in ``x`` (or ``x``,
         ``y``, ``z`` of 2 rows each), or detector index pairs ``trIndex`` /
@@ -762,6 +804,8 @@ class projectorClass:
         if subset == -1:
             subset = self.subset
         f = self._as_device(f, int(self.N[0]), 'image')
+        if self.use_psf:
+            f = self._psf(f)
         m = self.measurementCount(subset)
         y = torch.empty(m, dtype=torch.float32, device=f.device)
         stream = torch.cuda.current_stream(f.device).cuda_stream
@@ -786,6 +830,9 @@ class projectorClass:
         _native.call("omb_backward", self._handle, int(subset), ctypes.c_void_p(y.data_ptr()),
                      ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(s.data_ptr() if s is not None else 0),
                      int(mode), ctypes.c_void_p(stream))
+        if self.use_psf:
+            f = self._psf(f)
+            s = self._psf(s) if sens else None
         return (f, s) if sens else f
 
     @property

@@ -94,8 +94,20 @@ def ref_project(L, o, subset, fp, inp, sens=False):
     return out, s
 
 
+def psf_fixture(proj):
+    """The reference's PSF window (proj.py PSFKernel, run by its addProjector)
+    for pet_mini with FWHM 4 x 4 x 6 mm, stored in psf_pet_mini.npz."""
+    o = apply(proj.projectorClass(), dict(CONFIGS["pet_mini"], use_psf=True, FWHM=np.array([4., 4., 6.])))
+    o.addProjector()
+    out = {"gaussK": np.asarray(o.gaussK, dtype=np.float32).ravel(order='F'),
+           "g_dim": np.array([o.g_dim_x, o.g_dim_y, o.g_dim_z], dtype=np.int64), "FWHM": np.array([4., 4., 6.])}
+    np.savez_compressed(os.path.join(HERE, "psf_pet_mini.npz"), **out)
+    print("psf_pet_mini", out["g_dim"], out["gaussK"].shape)
+
+
 def main():
     proj = reference_projector()
+    psf_fixture(proj)
     allc = dict(CONFIGS)
     allc.update(CONFIGS_EXTRA)
     L = None
