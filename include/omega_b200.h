@@ -282,7 +282,9 @@ int omb_get_tuning(const omb_handle *h, omb_tuning *out);
  */
 typedef enum omb_recon_algorithm {
     OMB_RECON_OSEM = 1,     /* options.OSEM: per-subset sensitivity images, EM update per subset (PET) */
-    OMB_RECON_PDHG_TV = 2   /* options.PDHG with options.TV: one subset, smoothed TV gradient */
+    OMB_RECON_PDHG_TV = 2,  /* options.PDHG with options.TV: one subset, smoothed TV gradient */
+    OMB_RECON_OSL_OSEM_RDP = 3  /* options.OSL_OSEM with options.RDP: one-step-late OSEM, x / (sens + dU) * rhs,
+                                   dU = beta * RDP gradient of the current image (priors.h:447-451) */
 } omb_recon_algorithm;
 
 typedef struct omb_recon_params {
@@ -298,6 +300,7 @@ typedef struct omb_recon_params {
     int32_t positivity;       /* options.enforcePositivity */
     int32_t use_graph;        /* nonzero: capture one iteration as a CUDA graph and replay it */
     float tau_used;           /* out: the primal step of the run */
+    float rdp_gamma;          /* OSL-OSEM: options.RDP_gamma (beta is options.beta) */
 } omb_recon_params;
 
 /*
@@ -309,6 +312,14 @@ typedef struct omb_recon_params {
  * per subset for the sensitivities) and synchronises `stream` on return.
  */
 int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const float *x0, float *x_out, void *stream);
+
+/*
+ * One one-step-late OSEM sub-iteration (subiterStep.h:219-226): as
+ * omb_osem_subset, with the update image / (sens + du) * rhs; du (device,
+ * one image) is the prior gradient including its weight.
+ */
+int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
+                   const float *du, float *work_meas, float *work_img, void *stream);
 
 /*
  * PSF blur (Convolution3D_f, auxKernels.cl:192-245): out = window applied at

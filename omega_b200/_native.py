@@ -90,11 +90,13 @@ class ReconParams(ctypes.Structure):
         ("positivity", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
         ("tau_used", ctypes.c_float),
+        ("rdp_gamma", ctypes.c_float),
     ]
 
 
 OMB_RECON_OSEM = 1
 OMB_RECON_PDHG_TV = 2
+OMB_RECON_OSL_OSEM_RDP = 3
 
 
 class Tuning(ctypes.Structure):
@@ -160,6 +162,9 @@ EXPORTS = [
     ("omb_power_workspace_bytes", ctypes.c_size_t, []),
     ("omb_set_read_precision", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     ("omb_take_device_error", ctypes.c_int, []),
+    ("omb_osl_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]),
     ("omb_psf_convolve", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_void_p]),

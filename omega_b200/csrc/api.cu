@@ -359,6 +359,8 @@ static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, fl
 }
 
 int omb::handle_subsets(const omb_handle *h) { return h ? h->desc.n_subsets : 0; }
+Grid omb::handle_grid(const omb_handle *h) { return h ? h->grid : Grid{}; }
+float omb::handle_epps(const omb_handle *h) { return h ? h->desc.epps : 0.f; }
 
 extern "C" {
 
@@ -632,6 +634,34 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     st = rays_backward(h, rs, one_frame_bp(h, work_meas, work_img, rs.m_size), nullptr, s);
     if (st != OMB_OK) return st;
     return em_update(image, sens, work_img, h->n_img, eps, s);
+}
+
+int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
+                   const float *du, float *work_meas, float *work_img, void *stream) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!image || !y_subset || !sens || !du || !work_meas || !work_img)
+        return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osl_subset");
+    if (h->desc.modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
+    if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_osl_subset needs projector types 1 or 4");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const float eps = h->desc.epps;
+    const int64_t m = rs.m_size * h->desc.tof_bins;
+    st = rays_forward(h, rs, one_frame_fp(h, image, work_meas, rs.m_size), s);
+    if (st != OMB_OK) return st;
+    if (h->d_rand)
+        st = osem_ratio_randoms(y_subset, m, work_meas, m, m, 1, h->d_rand + subset_ray0(h, rs, subset), rs.m_size,
+                                eps, s);
+    else
+        st = osem_ratio(y_subset, work_meas, m, eps, s);
+    if (st != OMB_OK) return st;
+    OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
+    st = rays_backward(h, rs, one_frame_bp(h, work_meas, work_img, rs.m_size), nullptr, s);
+    if (st != OMB_OK) return st;
+    return osl_update(image, sens, du, work_img, h->n_img, s);
 }
 
 int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, float *images, int64_t image_stride,

@@ -62,6 +62,22 @@ __global__ void k_osem_ratio_randoms(const float *__restrict__ y, int64_t y_stri
     }
 }
 
+// One-step-late EM update (algorithms.h:24-27 OSL, subiterStep.h:219-226):
+// x = x / (sens + dU) * rhs, dU the prior gradient (beta included).
+__global__ void k_osl_update(float *__restrict__ img, const float *__restrict__ sens, const float *__restrict__ du,
+                             const float *__restrict__ rhs, int64_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        img[i] = img[i] / (__ldg(sens + i) + __ldg(du + i)) * __ldg(rhs + i);
+}
+
+int osl_update(float *img, const float *sens, const float *du, const float *rhs, int64_t n, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_osl_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, sens, du, rhs, n);
+    OMB_LAUNCH_CHECK("OSL update launch");
+    return OMB_OK;
+}
+
 int osem_ratio_randoms(const float *y, int64_t y_stride, float *fp, int64_t fp_stride, int64_t n, int frames,
                        const float *rnd, int64_t n_rays, float epps, cudaStream_t st) {
     if (n <= 0 || frames <= 0) return OMB_OK;

@@ -14,8 +14,12 @@ int siddon_backward_fixed(const Grid &g, const RaySet &rs, const Tof &tof, float
 int siddon_count(const Grid &g, const RaySet &rs, const Tof &tof, unsigned long long *total, cudaStream_t st);
 int fixed_to_float(const unsigned long long *acc, float *out, int64_t n, cudaStream_t st);
 
-// Subset count of a handle (the handle layout is private to api.cu).
+// Subset count and image grid of a handle (the handle layout is private to api.cu).
 int handle_subsets(const omb_handle *h);
+Grid handle_grid(const omb_handle *h);
+float handle_epps(const omb_handle *h);
+// x = x / (sens + du) * rhs
+int osl_update(float *img, const float *sens, const float *du, const float *rhs, int64_t n, cudaStream_t st);
 
 // Multi-ray PET projections (rs.nr_xy x rs.nr_z rays per LOR), one frame.
 int multiray_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *img, float *y,

@@ -77,7 +77,10 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
     OMB_CUDA_TRY(cudaMemcpyAsync(x_out, x0, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
     const bool graph = p->use_graph != 0;
     int st = OMB_OK;
-    if (p->algorithm == OMB_RECON_OSEM) {
+    if (p->algorithm == OMB_RECON_OSEM || p->algorithm == OMB_RECON_OSL_OSEM_RDP) {
+        const bool osl = p->algorithm == OMB_RECON_OSL_OSEM_RDP;
+        const Grid g = handle_grid(h);
+        const float epps = handle_epps(h);
         // per-subset sensitivity images, then sub-iterations in subset order
         std::vector<int64_t> off(n_subsets + 1, 0);
         int64_t m_max = 0;
@@ -86,15 +89,27 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             off[s_ + 1] = off[s_] + ms;
             m_max = ms > m_max ? ms : m_max;
         }
-        DevBuf sens, wm, wi;
+        DevBuf sens, wm, wi, du;
         if ((st = alloc(sens, (size_t)n_subsets * n * sizeof(float), s)) != OMB_OK) return st;
+        if (osl && (st = alloc(du, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(wm, (size_t)m_max * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(wi, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         for (int s_ = 0; s_ < n_subsets && st == OMB_OK; ++s_) st = omb_sensitivity(h, s_, sens.f() + s_ * n, stream);
         if (st != OMB_OK) return st;
         st = repeat(p->n_iter, graph, s, [&]() {
             for (int s_ = 0; s_ < n_subsets; ++s_) {
-                const int e = omb_osem_subset(h, s_, x_out, y + off[s_], sens.f() + s_ * n, wm.f(), wi.f(), stream);
+                int e;
+                if (osl) {
+                    // dU of the current image, then the one-step-late update
+                    if (cudaMemsetAsync(du.p, 0, (size_t)n * sizeof(float), s) != cudaSuccess)
+                        return set_error(OMB_ERR_CUDA, "clearing the prior gradient failed");
+                    e = omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
+                    if (e == OMB_OK)
+                        e = omb_osl_subset(h, s_, x_out, y + off[s_], sens.f() + s_ * n, du.f(), wm.f(), wi.f(),
+                                           stream);
+                } else {
+                    e = omb_osem_subset(h, s_, x_out, y + off[s_], sens.f() + s_ * n, wm.f(), wi.f(), stream);
+                }
                 if (e != OMB_OK) return e;
             }
             return (int)OMB_OK;

@@ -119,8 +119,11 @@ class projectorClass:
     # Built-in reconstruction (reconstructions_main): the algorithms of this
     # path and their parameters (proj.py:116-120, 236, 271, 275, 317, 370-420)
     OSEM = False
+    OSL_OSEM = False
     PDHG = False
     TV = False
+    RDP = False
+    RDP_gamma = 1.
     MAP = False
     beta = 0.
     TVsmoothing = 1e-4

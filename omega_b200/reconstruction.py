@@ -228,7 +228,8 @@ class OSEMBatch:
 def reconstructions_main(options):
     """The built-in reconstruction (omegatomo/reconstruction/recomain.py:427-725,
     the compiled omegaMain entry) for the algorithms of this path:
-    options.OSEM (PET) or options.PDHG with options.TV, options.Niter
+    options.OSEM (PET), options.OSL_OSEM with options.RDP (PET, one-step-late
+    MAP with the relative difference prior) or options.PDHG with options.TV, options.Niter
     iterations from options.x0, run natively by omb_reconstruct.  CT data are
     linearised as log(flat / SinM) first (prepass.py:22-36; flat = max(SinM)
     when options.flat <= 0), negative PET counts set to 0.  Returns
@@ -236,10 +237,15 @@ def reconstructions_main(options):
     projections), as the reference does with storeFP off.  Reads
     options.use_graph (default True) to replay iterations as CUDA graphs."""
     import torch
-    if not (options.OSEM or options.PDHG):
+    osl = bool(getattr(options, 'OSL_OSEM', False))
+    if not (options.OSEM or options.PDHG or osl):
         raise ValueError('No reconstruction method selected, aborting.')
-    if options.OSEM and options.PDHG:
-        raise ValueError('Select one reconstruction method (OSEM or PDHG)')
+    if int(bool(options.OSEM)) + int(bool(options.PDHG)) + int(osl) > 1:
+        raise ValueError('Select one reconstruction method (OSEM, OSL_OSEM or PDHG)')
+    if osl and not options.RDP:
+        raise ValueError('OSL_OSEM is built with the RDP prior (options.RDP = True)')
+    if osl and options.CT:
+        raise ValueError('OSL_OSEM is built for PET data')
     if options.PDHG and not options.TV:
         raise ValueError('PDHG is built with the TV prior (options.TV = True)')
     if options.OSEM and options.CT:
@@ -260,7 +266,7 @@ def reconstructions_main(options):
     n = int(np.ravel(options.N)[0])
     m = np.asarray(options.SinM, dtype=np.float32).ravel(order='F')
     S = int(options.subsets)
-    if options.OSEM:
+    if options.OSEM or osl:
         parts = [np.asarray(options.subsetMeasurements(m, s)) for s in range(S)]
         y = torch.from_numpy(np.ascontiguousarray(np.concatenate(parts), dtype=np.float32)).to(dev)
     else:
@@ -271,7 +277,9 @@ def reconstructions_main(options):
     x0 = torch.from_numpy(np.ascontiguousarray(x0)).to(dev)
     x = torch.empty(n, device=dev)
     p = _native.ReconParams(struct_size=ctypes.sizeof(_native.ReconParams))
-    p.algorithm = _native.OMB_RECON_OSEM if options.OSEM else _native.OMB_RECON_PDHG_TV
+    p.algorithm = (_native.OMB_RECON_OSEM if options.OSEM else
+                   (_native.OMB_RECON_OSL_OSEM_RDP if osl else _native.OMB_RECON_PDHG_TV))
+    p.rdp_gamma = float(getattr(options, 'RDP_gamma', 1.0))
     p.n_iter = int(options.Niter)
     p.beta = float(options.beta)
     p.tv_smoothing = float(options.TVsmoothing)

@@ -245,11 +245,12 @@ def intersections(geom: Geometry, subset):
     return int(lib().oracle_siddon_count(ctypes.byref(g)))
 
 
-def osem(geom: Geometry, y_subsets, x0, n_iter, forward=None, backward=None, randoms=None):
+def osem(geom: Geometry, y_subsets, x0, n_iter, forward=None, backward=None, randoms=None, prior_grad=None):
     """Restated OSEM loop in FP64; returns the image after n_iter iterations.
     The projector pair defaults to the Siddon restatement (type 1).
     randoms: per subset, added to the forward projection before the ratio
-    (computeForwardProject.h:46-71), tiled over TOF bins."""
+    (computeForwardProject.h:46-71), tiled over TOF bins.  prior_grad(x):
+    one-step-late OSEM with that prior gradient (weight included)."""
     fwd = forward or globals()["forward"]
     bwd = backward or globals()["backward"]
     x = np.asarray(x0, dtype=np.float64).copy()
@@ -266,6 +267,12 @@ def osem(geom: Geometry, y_subsets, x0, n_iter, forward=None, backward=None, ran
             with np.errstate(divide="ignore", invalid="ignore"):
                 r = np.asarray(y_subsets[s], dtype=np.float64) / fp
             r[~np.isfinite(r)] = eps
+            if prior_grad is not None:
+                # one-step-late (subiterStep.h:219-226): dU of the current image
+                du = prior_grad(x)
+                rhs = bwd(geom, r, s)
+                x = x / (sens[s] + du) * rhs
+                continue
             rhs = bwd(geom, r, s)
             x = x / sens[s] * (rhs + eps)
     return x

@@ -83,3 +83,29 @@ def test_builtin_pdhg_ct_matches_custom_loop_and_oracle(cuda):
     assert orc.rel_l2(out.ravel(order='F'), ref) < 1e-4, orc.rel_l2(out.ravel(order='F'), ref)
     # the power-method step agrees with the custom loop's estimate
     assert abs(tau * rec.power_method(o) - 1.0) < 1e-2
+
+
+def test_builtin_osl_osem_rdp_matches_oracle(cuda):
+    from omega_b200 import reconstruction as rec
+    from oracle import image_oracle as io
+    o = make_options("pet_mini")
+    o._cfg_name = "pet_mini"
+    g, y = _pet_data(o, 4)
+    o.SinM = y.copy()
+    o.OSL_OSEM = True
+    o.RDP = True
+    o.RDP_gamma = 2.0
+    # one-step-late is stable only for small weights: at beta = 0.02 this
+    # case is chaotic (a 1e-6 change of x0 moves the result by 30 %)
+    o.beta = 0.002
+    o.Niter = 2
+    out, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    shape = (g.nx, g.ny, g.nz)
+    ref = orc.osem(g, ys, np.ones(g.n_img), 2,
+                   prior_grad=lambda x: io.rdp_gradient(x, shape, 2.0, 0.002, g.epps))
+    plain = orc.osem(g, ys, np.ones(g.n_img), 2)
+    x = out.ravel(order='F')
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    assert orc.rel_l2(ref, plain) > 1e-3  # the prior changes the result
