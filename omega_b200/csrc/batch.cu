@@ -19,7 +19,7 @@ __device__ __forceinline__ int next_chunk(int *counter) {
     return v;
 }
 
-__global__ void __launch_bounds__(kBlock) k_batch_fp(const BatchItem *__restrict__ items,
+__global__ void __launch_bounds__(kBlock, 4) k_batch_fp(const BatchItem *__restrict__ items,
                                                      const int2 *__restrict__ work, int n_work,
                                                      int *__restrict__ counter, const float *__restrict__ img,
                                                      float *__restrict__ y) {

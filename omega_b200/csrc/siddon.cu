@@ -15,9 +15,13 @@ namespace omb {
 
 // Forward projection.  Each thread walks one ray once and accumulates it for
 // FB frames of a dynamic study (blockIdx.y selects the group of frames), so
-// the traversal cost is shared by up to FB images.
+// the traversal cost is shared by up to FB images.  Non-TOF forward walks are
+// latency-bound gathers: capping them at 64 registers (4 blocks, 32 warps per
+// SM) beats the spills it costs (measured: 30.6 -> 23.6 ms single-frame, 6.0
+// -> 3.9 ms for the interleaved 8-frame walk); the TOF variants keep their
+// registers (their weight arrays would spill hundreds of bytes).
 template <int NB, int FB, typename T, int K>
-__global__ void __launch_bounds__(kBlock) k_siddon_fp(Grid g, RaySet rs, Tof tof, float gf,
+__global__ void __launch_bounds__(kBlock, NB == 1 ? 4 : 1) k_siddon_fp(Grid g, RaySet rs, Tof tof, float gf,
                                                       const T *__restrict__ img, int64_t img_stride,
                                                       float *__restrict__ y, int64_t y_stride, int n_frames) {
     const bool pet = rs.modality != OMB_CT_PANEL;
@@ -102,7 +106,7 @@ __global__ void __launch_bounds__(kBlock) k_frames_deinterleave(const float *__r
 }
 
 template <int FB, int K>
-__global__ void __launch_bounds__(kBlock) k_siddon_fp_ilv(Grid g, RaySet rs, float gf, const float *__restrict__ img,
+__global__ void __launch_bounds__(kBlock, 4) k_siddon_fp_ilv(Grid g, RaySet rs, float gf, const float *__restrict__ img,
                                                           int64_t n_img, float *__restrict__ y, int64_t y_stride,
                                                           int n_frames) {
     const bool pet = rs.modality != OMB_CT_PANEL;
