@@ -1199,7 +1199,7 @@ int omb_batch_create(const omb_geometry_desc *descs, int32_t n, omb_batch **out)
     });
     std::vector<int2> work;
     for (int i : order)
-        for (int64_t r = 0; r < items[(size_t)i].rs.m_size; r += kBlock) work.push_back(make_int2(i, (int)r));
+        for (int64_t r = 0; r < items[(size_t)i].rs.m_size; r += 32) work.push_back(make_int2(i, (int)r));  // warp chunks
     b->n_work = (int)work.size();
     if ((e = cudaMalloc(&b->d_items, items.size() * sizeof(BatchItem))) != cudaSuccess) return fail(e, "cudaMalloc batch items");
     if ((e = cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice)) != cudaSuccess)
