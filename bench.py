@@ -55,8 +55,8 @@ PROFILED_TRAFFIC = {
     # siddon_dynpet_launches.md (full-size capture)
     ("cbct", "bdd_fp"): 9.40e9,
     ("cbct", "bdd_bp"): 3.87e8,
-    ("dynpet", "siddon_fp"): 3.55e8,
-    ("dynpet", "siddon_bp"): 4.83e8,
+    ("dynpet", "siddon_fp"): 3.81e8,
+    ("dynpet", "siddon_bp"): 4.77e8,
 }
 # What bounds each kernel instead of HBM (the volumes and images are
 # L2-resident, so DRAM moves a few per cent of the cache-less bytes): the
@@ -64,8 +64,8 @@ PROFILED_TRAFFIC = {
 PROFILED_LIMITER = {
     ("cbct", "bdd_fp"): {"issue_active_pct": 83.0, "sm_throughput_pct": 79.7, "dram_pct": 5.2},
     ("cbct", "bdd_bp"): {"issue_active_pct": 74.2, "sm_throughput_pct": 73.8, "dram_pct": 0.2},
-    ("dynpet", "siddon_fp"): {"issue_active_pct": 42.5, "l1tex_pct": 58.2, "dram_pct": 0.7},
-    ("dynpet", "siddon_bp"): {"issue_active_pct": 46.4, "lts_pct": 65.7, "dram_pct": 1.0},
+    ("dynpet", "siddon_fp"): {"issue_active_pct": 66.5, "l1tex_pct": 92.0, "dram_pct": 1.0},
+    ("dynpet", "siddon_bp"): {"issue_active_pct": 44.4, "lts_pct": 65.9, "dram_pct": 1.0},
 }
 FALLBACK_HBM_GBS = 6650.0
 
