@@ -270,7 +270,7 @@ struct Shared {
 }  // namespace bb
 
 template <bool SENS, bool FULL>
-__global__ void k_bdd_bp_tma(const __grid_constant__ CUtensorMap map_y, Grid g, const BddProj *__restrict__ pj,
+__global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_constant__ CUtensorMap map_y, Grid g, const BddProj *__restrict__ pj,
                              int nr, int nc, int64_t nproj, const float *__restrict__ y, float *__restrict__ img,
                              float *__restrict__ sens) {
     using namespace bb;
