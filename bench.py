@@ -298,6 +298,12 @@ class Timed:
         return out
 
 
+def max_over_ranks(values, device=None):
+    """The slowest rank's times (omega_b200.distributed.max_over_ranks)."""
+    from omega_b200.distributed import max_over_ranks as m
+    return m(values, device=device)
+
+
 def run_timed(args, world, dev, step, n_phases):
     """Warm-up, then exactly args.steps steps bracketed by barrier + sync,
     with an L2 flush between steps outside the events.  Returns per-phase
@@ -327,9 +333,7 @@ def run_timed(args, world, dev, step, n_phases):
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
-        t = torch.tensor(tot, dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot = t.tolist()
+        tot = max_over_ranks(tot, device=dev)
     return tot, clk, wall
 
 
@@ -349,9 +353,7 @@ def e2e_time(args, world, dev, step_host):
             times.append(e0.elapsed_time(e1) / 1e3)
     total = sum(times)
     if world > 1:
-        t = torch.tensor([total], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+        total = max_over_ranks([total], device=dev)[0]
     return total
 
 
