@@ -148,7 +148,11 @@ def dynamic_images(o, frames, seed=2024):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clock / throttle samples every 50 ms.  Started before the
+    warm-up (nvidia-smi needs a few hundred ms to begin sampling), it keeps
+    only the samples whose timestamps fall inside the timed region marked by
+    mark_start() / mark_stop() (the nearest ones if none does)."""
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -156,6 +160,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
@@ -163,10 +168,24 @@ class ClockSampler:
             os.close(fd)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_stop(self):
+        self.t1 = time.time()
+
+    @staticmethod
+    def _epoch(ts):
+        import datetime
+        try:
+            return datetime.datetime.strptime(ts.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
 
     def stop(self):
         if self.proc is None:
@@ -181,11 +200,20 @@ class ClockSampler:
         with open(self.path) as f:
             for line in f:
                 parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
+                if len(parts) >= 10:
                     rows.append(parts)
         os.unlink(self.path)
         if not rows:
             return None
+        if self.t0 is not None and self.t1 is not None:
+            stamped = [(self._epoch(r[0]), r) for r in rows]
+            inside = [r for t, r in stamped if t is not None and self.t0 - 0.05 <= t <= self.t1 + 0.05]
+            if not inside:
+                near = sorted((abs(t - 0.5 * (self.t0 + self.t1)), i) for i, (t, r) in enumerate(stamped)
+                              if t is not None)
+                inside = [stamped[i][1] for _, i in near[:2]]
+            rows = inside or rows
+        rows = [r[1:] for r in rows]  # drop the timestamp
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -313,15 +341,16 @@ def run_timed(args, world, dev, step, n_phases):
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, device=dev)
     tm = Timed(stream)
+    clocks = ClockSampler(dev.index or 0)
+    clocks.start()
     for _ in range(max(args.warmup, 0)):
         step(tm)
         tm.phases()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev.index or 0)
-    clocks.start()
     tot = [0.0] * n_phases
+    clocks.mark_start()
     wall0 = time.perf_counter()
     for _ in range(args.steps):
         flush.zero_()
@@ -330,6 +359,7 @@ def run_timed(args, world, dev, step, n_phases):
             tot[i] += t
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
+    clocks.mark_stop()
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
