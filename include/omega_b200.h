@@ -283,9 +283,15 @@ int omb_get_tuning(const omb_handle *h, omb_tuning *out);
 typedef enum omb_recon_algorithm {
     OMB_RECON_OSEM = 1,     /* options.OSEM: per-subset sensitivity images, EM update per subset (PET) */
     OMB_RECON_PDHG_TV = 2,  /* options.PDHG with options.TV: one subset, smoothed TV gradient */
-    OMB_RECON_OSL_OSEM_RDP = 3  /* options.OSL_OSEM with options.RDP: one-step-late OSEM, x / (sens + dU) * rhs,
-                                   dU = beta * RDP gradient of the current image (priors.h:447-451) */
+    OMB_RECON_OSL_OSEM = 3  /* options.OSL_OSEM: one-step-late OSEM, x / (sens + dU) * rhs, dU = beta * the
+                               prior's gradient at the current image (priors.h:376-451) */
 } omb_recon_algorithm;
+
+typedef enum omb_prior {
+    OMB_PRIOR_RDP = 1,      /* options.RDP: relative difference prior, parameter rdp_gamma */
+    OMB_PRIOR_QUAD = 2,     /* options.Quad: the quadratic window (prior_window) applied with mirrored edges */
+    OMB_PRIOR_HUBER = 3     /* options.Huber: the same with the gradient clamped to +-huber_delta */
+} omb_prior;
 
 typedef struct omb_recon_params {
     uint32_t struct_size;     /* sizeof(omb_recon_params) */
@@ -301,6 +307,11 @@ typedef struct omb_recon_params {
     int32_t use_graph;        /* nonzero: capture one iteration as a CUDA graph and replay it */
     float tau_used;           /* out: the primal step of the run */
     float rdp_gamma;          /* OSL-OSEM: options.RDP_gamma (beta is options.beta) */
+    int32_t prior;            /* OSL-OSEM: omb_prior */
+    const float *prior_window;/* Quad / Huber: device window of (2g0+1)(2g1+1)(2g2+1) weights, x fastest: the
+                                 neighbours' -w and the centre sum(w) (libHeader.h:1147-1154) */
+    int32_t prior_g[3];       /* Quad / Huber: options.Ndx, Ndy, Ndz */
+    float huber_delta;        /* Huber: options.huber_delta */
 } omb_recon_params;
 
 /*

@@ -91,12 +91,19 @@ class ReconParams(ctypes.Structure):
         ("use_graph", ctypes.c_int32),
         ("tau_used", ctypes.c_float),
         ("rdp_gamma", ctypes.c_float),
+        ("prior", ctypes.c_int32),
+        ("prior_window", ctypes.c_void_p),
+        ("prior_g", ctypes.c_int32 * 3),
+        ("huber_delta", ctypes.c_float),
     ]
 
 
 OMB_RECON_OSEM = 1
 OMB_RECON_PDHG_TV = 2
-OMB_RECON_OSL_OSEM_RDP = 3
+OMB_RECON_OSL_OSEM = 3
+OMB_PRIOR_RDP = 1
+OMB_PRIOR_QUAD = 2
+OMB_PRIOR_HUBER = 3
 
 
 class Tuning(ctypes.Structure):

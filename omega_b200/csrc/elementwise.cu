@@ -78,6 +78,21 @@ int osl_update(float *img, const float *sens, const float *du, const float *rhs,
     return OMB_OK;
 }
 
+// du = beta * clamp(du, -delta, delta) (Huber_prior, priors.h:44-52; delta
+// infinite for the quadratic prior)
+__global__ void k_scale_clamp(float *__restrict__ du, int64_t n, float beta, float delta) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        du[i] = beta * fminf(fmaxf(du[i], -delta), delta);
+}
+
+int scale_clamp(float *du, int64_t n, float beta, float delta, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_scale_clamp<<<grid_for(n, 4), kBlock, 0, st>>>(du, n, beta, delta);
+    OMB_LAUNCH_CHECK("prior scale launch");
+    return OMB_OK;
+}
+
 int osem_ratio_randoms(const float *y, int64_t y_stride, float *fp, int64_t fp_stride, int64_t n, int frames,
                        const float *rnd, int64_t n_rays, float epps, cudaStream_t st) {
     if (n <= 0 || frames <= 0) return OMB_OK;

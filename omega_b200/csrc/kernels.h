@@ -18,6 +18,8 @@ int fixed_to_float(const unsigned long long *acc, float *out, int64_t n, cudaStr
 int handle_subsets(const omb_handle *h);
 Grid handle_grid(const omb_handle *h);
 float handle_epps(const omb_handle *h);
+// du = beta * clamp(du, -delta, delta)
+int scale_clamp(float *du, int64_t n, float beta, float delta, cudaStream_t st);
 // x = x / (sens + du) * rhs
 int osl_update(float *img, const float *sens, const float *du, const float *rhs, int64_t n, cudaStream_t st);
 

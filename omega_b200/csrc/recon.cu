@@ -77,8 +77,12 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
     OMB_CUDA_TRY(cudaMemcpyAsync(x_out, x0, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
     const bool graph = p->use_graph != 0;
     int st = OMB_OK;
-    if (p->algorithm == OMB_RECON_OSEM || p->algorithm == OMB_RECON_OSL_OSEM_RDP) {
-        const bool osl = p->algorithm == OMB_RECON_OSL_OSEM_RDP;
+    if (p->algorithm == OMB_RECON_OSEM || p->algorithm == OMB_RECON_OSL_OSEM) {
+        const bool osl = p->algorithm == OMB_RECON_OSL_OSEM;
+        if (osl && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_HUBER))
+            return set_error(OMB_ERR_INVALID, "unknown prior");
+        if (osl && p->prior != OMB_PRIOR_RDP && !p->prior_window)
+            return set_error(OMB_ERR_INVALID, "the quadratic / Huber prior needs its window");
         const Grid g = handle_grid(h);
         const float epps = handle_epps(h);
         // per-subset sensitivity images, then sub-iterations in subset order
@@ -103,7 +107,16 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                     // dU of the current image, then the one-step-late update
                     if (cudaMemsetAsync(du.p, 0, (size_t)n * sizeof(float), s) != cudaSuccess)
                         return set_error(OMB_ERR_CUDA, "clearing the prior gradient failed");
-                    e = omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
+                    if (p->prior == OMB_PRIOR_RDP) {
+                        e = omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
+                    } else {
+                        // quadratic: the window applied at every voxel (priors.h:27-42); Huber clamps it
+                        e = omb_psf_convolve(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_window, p->prior_g[0],
+                                             p->prior_g[1], p->prior_g[2], stream);
+                        if (e == OMB_OK)
+                            e = scale_clamp(du.f(), n, p->beta,
+                                            p->prior == OMB_PRIOR_HUBER ? p->huber_delta : INFINITY, s);
+                    }
                     if (e == OMB_OK)
                         e = omb_osl_subset(h, s_, x_out, y + off[s_], sens.f() + s_ * n, du.f(), wm.f(), wi.f(),
                                            stream);

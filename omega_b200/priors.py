@@ -25,3 +25,54 @@ def RDP(im, Nx, Ny, Nz, gamma, beta, rType=2, epps=1e-8):
     _native.call("omb_rdp_gradient", ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(grad.data_ptr()), n[0], n[1],
                  n[2], float(gamma), float(epps), float(beta), st)
     return grad
+
+
+def neighbourhood_weights(options):
+    """Distance weights 1/d of the (2Ndx+1)(2Ndy+1)(2Ndz+1) neighbourhood
+    (prepass.py:634-700, the non-GGMRF branch): voxel pitch FOV/N per axis,
+    offsets from +Nd down to -Nd, x fastest; the centre is inf."""
+    Ndx, Ndy, Ndz = int(options.Ndx), int(options.Ndy), int(options.Ndz)
+    distX = float(np.ravel(options.FOVa_x)[0]) / float(np.ravel(options.Nx)[0])
+    distY = float(np.ravel(options.FOVa_y)[0]) / float(np.ravel(options.Ny)[0])
+    distZ = float(np.ravel(options.axial_fov)[0]) / float(np.ravel(options.Nz)[0])
+    nz1 = int(np.ravel(options.Nz)[0]) == 1
+    w = np.zeros((2 * Ndx + 1) * (2 * Ndy + 1) * (2 * Ndz + 1), dtype=np.float32)
+    cc = np.zeros((2 * Ndy + 1) * (2 * Ndx + 1), dtype=np.float32)
+    for lt, jj in enumerate(range(Ndz, -Ndz - 1, -1)):
+        for ll, kk in enumerate(range(Ndy, -Ndy - 1, -1)):
+            xs = np.arange(Ndx, -Ndx - 1, -1) * distX
+            ys = np.repeat(kk, Ndy * 2 + 1) * distY
+            if Ndz == 0 or nz1:
+                apu = np.column_stack((xs, ys))
+            elif Ndz != Ndx:
+                zs = np.concatenate((np.zeros(Ndx - Ndz), np.repeat(jj, Ndz * 2 + 1) * distZ, np.zeros(Ndx - Ndz)))
+                apu = np.column_stack((xs, ys, zs))
+            else:
+                apu = np.column_stack((xs, ys, np.repeat(jj, Ndz * 2 + 1) * distZ))
+            cc[(Ndy * 2 + 1) * ll:(Ndy * 2 + 1) * (ll + 1)] = np.sqrt(np.sum(apu ** 2, axis=1))
+        w[(Ndx * 2 + 1) * (Ndy * 2 + 1) * lt:(Ndx * 2 + 1) * (Ndy * 2 + 1) * (lt + 1)] = cc
+    with np.errstate(divide='ignore'):
+        return (1.0 / w).astype(np.float32)
+
+
+def normalised_weights(weights):
+    """quadWeights / huberWeights (prepass.py:703-744) for computed weights:
+    divided by the sum of the finite ones, the centre left out."""
+    w = np.asarray(weights, dtype=np.float32)
+    wn = w / np.sum(w[~np.isinf(w)])
+    half = np.size(wn) // 2
+    wn = np.concatenate((wn[:half], wn[half + 1:]))
+    return wn[~np.isinf(wn)].astype(np.float32)
+
+
+def prior_window(wq, Ndx, Ndy, Ndz):
+    """The gradient window of the quadratic / Huber prior (libHeader.h:
+    1147-1154): the neighbours' weights negated, the centre the absolute sum,
+    x fastest; applied with mirrored edges it gives sum_k w_k (x_j - x_k)."""
+    n = (2 * Ndx + 1) * (2 * Ndy + 1) * (2 * Ndz + 1)
+    neg = -np.asarray(wq, dtype=np.float32)
+    win = np.zeros(n, dtype=np.float32)
+    win[:n // 2] = neg[:n // 2]
+    win[n // 2 + 1:] = neg[n // 2:]
+    win[n // 2] = np.abs(np.sum(neg, dtype=np.float32))
+    return win

@@ -124,6 +124,13 @@ class projectorClass:
     TV = False
     RDP = False
     RDP_gamma = 1.
+    Quad = False
+    Huber = False
+    huber_delta = 1.
+    Ndx = 1
+    Ndy = 1
+    Ndz = 1
+    weights = np.empty(0, dtype=np.float32)
     MAP = False
     beta = 0.
     TVsmoothing = 1e-4

@@ -228,8 +228,9 @@ class OSEMBatch:
 def reconstructions_main(options):
     """The built-in reconstruction (omegatomo/reconstruction/recomain.py:427-725,
     the compiled omegaMain entry) for the algorithms of this path:
-    options.OSEM (PET), options.OSL_OSEM with options.RDP (PET, one-step-late
-    MAP with the relative difference prior) or options.PDHG with options.TV, options.Niter
+    options.OSEM (PET), options.OSL_OSEM with options.RDP, options.Quad or
+    options.Huber (PET, one-step-late MAP; Ndx/Ndy/Ndz neighbourhood weights as
+    the reference forms them) or options.PDHG with options.TV, options.Niter
     iterations from options.x0, run natively by omb_reconstruct.  CT data are
     linearised as log(flat / SinM) first (prepass.py:22-36; flat = max(SinM)
     when options.flat <= 0), negative PET counts set to 0.  Returns
@@ -242,8 +243,9 @@ def reconstructions_main(options):
         raise ValueError('No reconstruction method selected, aborting.')
     if int(bool(options.OSEM)) + int(bool(options.PDHG)) + int(osl) > 1:
         raise ValueError('Select one reconstruction method (OSEM, OSL_OSEM or PDHG)')
-    if osl and not options.RDP:
-        raise ValueError('OSL_OSEM is built with the RDP prior (options.RDP = True)')
+    quad, huber = bool(getattr(options, 'Quad', False)), bool(getattr(options, 'Huber', False))
+    if osl and int(bool(options.RDP)) + int(quad) + int(huber) != 1:
+        raise ValueError('OSL_OSEM needs one prior: options.RDP, options.Quad or options.Huber')
     if osl and options.CT:
         raise ValueError('OSL_OSEM is built for PET data')
     if options.PDHG and not options.TV:
@@ -278,8 +280,23 @@ def reconstructions_main(options):
     x = torch.empty(n, device=dev)
     p = _native.ReconParams(struct_size=ctypes.sizeof(_native.ReconParams))
     p.algorithm = (_native.OMB_RECON_OSEM if options.OSEM else
-                   (_native.OMB_RECON_OSL_OSEM_RDP if osl else _native.OMB_RECON_PDHG_TV))
+                   (_native.OMB_RECON_OSL_OSEM if osl else _native.OMB_RECON_PDHG_TV))
     p.rdp_gamma = float(getattr(options, 'RDP_gamma', 1.0))
+    window = None
+    if osl:
+        p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
+                   (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))
+        if quad or huber:
+            from . import priors
+            nd = (int(options.Ndx), int(options.Ndy), int(options.Ndz))
+            w = np.asarray(options.weights, dtype=np.float32) if np.size(options.weights) else \
+                priors.neighbourhood_weights(options)
+            wq = priors.normalised_weights(w) if not np.size(options.weights) else w[~np.isinf(w)]
+            options.weights_quad = wq
+            window = torch.from_numpy(priors.prior_window(wq, *nd)).to(dev)
+            p.prior_window = ctypes.c_void_p(window.data_ptr())
+            p.prior_g[0], p.prior_g[1], p.prior_g[2] = nd
+            p.huber_delta = float(getattr(options, 'huber_delta', 1.0))
     p.n_iter = int(options.Niter)
     p.beta = float(options.beta)
     p.tv_smoothing = float(options.TVsmoothing)

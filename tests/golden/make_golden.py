@@ -105,9 +105,41 @@ def psf_fixture(proj):
     print("psf_pet_mini", out["g_dim"], out["gaussK"].shape)
 
 
+def prior_weight_fixture(proj):
+    """The reference's neighbourhood weights (prepass.py computeWeights +
+    quadWeights / huberWeights) for pet_mini with Ndx = Ndy = Ndz = 1 and
+    Ndx = Ndy = 2, Ndz = 1, stored in priorw_pet_mini.npz."""
+    # prepass.py loaded on its own: the package's __init__ imports a module
+    # that does not parse under Python 3.12 (mixed tabs in recomain.py)
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "omega_prepass", os.path.join(REF, "source", "Python", "omegatomo", "reconstruction", "prepass.py"))
+    prepass = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(prepass)
+    out = {}
+    for tag, nd in (("111", (1, 1, 1)), ("221", (2, 2, 1))):
+        o = apply(proj.projectorClass(), CONFIGS["pet_mini"])
+        o.addProjector()
+        o.Ndx, o.Ndy, o.Ndz = nd
+        o.weights = np.empty(0, dtype=np.float32)
+        o.GGMRF = False
+        prepass.computeWeights(o, False)
+        w = np.asarray(o.weights, dtype=np.float32).copy()
+        prepass.quadWeights(o, True)
+        out["quad_" + tag] = np.asarray(o.weights_quad, dtype=np.float32)
+        o.weights = w
+        o.weights_huber = np.empty(0, dtype=np.float32)
+        prepass.huberWeights(o)
+        out["huber_" + tag] = np.asarray(o.weights_huber, dtype=np.float32)
+        out["weights_" + tag] = w
+    np.savez_compressed(os.path.join(HERE, "priorw_pet_mini.npz"), **out)
+    print("priorw_pet_mini", {k: v.shape for k, v in out.items()})
+
+
 def main():
     proj = reference_projector()
     psf_fixture(proj)
+    prior_weight_fixture(proj)
     allc = dict(CONFIGS)
     allc.update(CONFIGS_EXTRA)
     L = None

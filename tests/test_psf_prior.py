@@ -143,3 +143,55 @@ def test_projections_with_psf(cuda):
     ref_bp, ref_s = orc.backward(g, y, 1, sens=True)
     assert orc.rel_l2(bp.cpu().numpy(), io.psf_convolve(ref_bp, shape, gk, gd)) < 1e-5
     assert orc.rel_l2(sens.cpu().numpy(), io.psf_convolve(ref_s, shape, gk, gd)) < 1e-5
+
+
+@pytest.mark.parametrize("tag,nd", [("111", (1, 1, 1)), ("221", (2, 2, 1))])
+def test_prior_weights_match_reference(tag, nd):
+    """computeWeights + quadWeights / huberWeights of the reference
+    (golden priorw_pet_mini.npz), and the assembled window's properties."""
+    from omega_b200 import priors
+    p = load_golden("priorw", "pet_mini")
+    o = make_options("pet_mini")
+    o.Ndx, o.Ndy, o.Ndz = nd
+    w = priors.neighbourhood_weights(o)
+    assert np.array_equal(w, p["weights_" + tag])
+    wq = priors.normalised_weights(w)
+    assert np.array_equal(wq, p["quad_" + tag]) and np.array_equal(wq, p["huber_" + tag])
+    win = priors.prior_window(wq, *nd)
+    assert abs(float(np.sum(win, dtype=np.float64))) < 1e-6
+    shape = (9, 8, 7)
+    flat = np.full(np.prod(shape), 3.0)
+    assert np.max(np.abs(io.psf_convolve(flat, shape, win, nd))) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prior", ["Quad", "Huber"])
+def test_builtin_osl_quadratic_and_huber(cuda, prior):
+    from omega_b200 import priors
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(5)
+    truth = rng.uniform(0.5, 2.0, g.n_img)
+    full = make_options("pet_mini")
+    full.subsets, full.subsetType = 1, 8
+    full.addProjector()
+    y = rng.poisson(orc.forward(orc.Geometry(full), truth, 0) * 200).astype(np.float32) / 200
+    o.SinM = y.copy()
+    o.OSL_OSEM = True
+    setattr(o, prior, True)
+    o.beta = 0.002  # one-step-late stays well-conditioned at this weight (see the RDP case)
+    o.huber_delta = 0.05
+    o.Niter = 2
+    out, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    shape = (g.nx, g.ny, g.nz)
+    win = priors.prior_window(priors.normalised_weights(priors.neighbourhood_weights(o)), 1, 1, 1)
+    delta = 0.05 if prior == "Huber" else np.inf
+
+    def grad(x):
+        return 0.002 * np.clip(io.psf_convolve(x, shape, win, (1, 1, 1)), -delta, delta)
+    ref = orc.osem(g, ys, np.ones(g.n_img), 2, prior_grad=grad)
+    assert orc.rel_l2(out.ravel(order='F'), ref) < 5e-5, orc.rel_l2(out.ravel(order='F'), ref)
+    assert orc.rel_l2(ref, orc.osem(g, ys, np.ones(g.n_img), 2)) > 1e-4
