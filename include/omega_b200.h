@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define OMB_ABI_VERSION 3
+#define OMB_ABI_VERSION 4
 
 typedef enum omb_status {
     OMB_OK = 0,
@@ -283,8 +283,14 @@ int omb_get_tuning(const omb_handle *h, omb_tuning *out);
 typedef enum omb_recon_algorithm {
     OMB_RECON_OSEM = 1,     /* options.OSEM: per-subset sensitivity images, EM update per subset (PET) */
     OMB_RECON_PDHG_TV = 2,  /* options.PDHG with options.TV: one subset, smoothed TV gradient */
-    OMB_RECON_OSL_OSEM = 3  /* options.OSL_OSEM: one-step-late OSEM, x / (sens + dU) * rhs, dU = beta * the
+    OMB_RECON_OSL_OSEM = 3, /* options.OSL_OSEM: one-step-late OSEM, x / (sens + dU) * rhs, dU = beta * the
                                prior's gradient at the current image (priors.h:376-451) */
+    OMB_RECON_ROSEM = 4,    /* options.ROSEM: x + lam * x / sens * (rhs - sens) per subset (algorithms.h:102-106) */
+    OMB_RECON_RAMLA = 5,    /* options.RAMLA: x + lam * rhs * x with rhs the backprojection of y / fp - 1
+                               (computeForwardProject.h:98-122, auxKernels.cl:1997-2026) */
+    OMB_RECON_BSREM = 6,    /* options.BSREM: RAMLA sub-iterations, then once per iteration the MAP step
+                               x -= lam * x * dU, x >= epps (iterStep.h:14-34, algorithms.h:130-135) */
+    OMB_RECON_ROSEM_MAP = 7 /* options.ROSEM_MAP: ROSEM sub-iterations, then the same MAP step */
 } omb_recon_algorithm;
 
 typedef enum omb_prior {
@@ -306,12 +312,14 @@ typedef struct omb_recon_params {
     int32_t positivity;       /* options.enforcePositivity */
     int32_t use_graph;        /* nonzero: capture one iteration as a CUDA graph and replay it */
     float tau_used;           /* out: the primal step of the run */
-    float rdp_gamma;          /* OSL-OSEM: options.RDP_gamma (beta is options.beta) */
-    int32_t prior;            /* OSL-OSEM: omb_prior */
+    float rdp_gamma;          /* OSL-OSEM, BSREM, ROSEM-MAP: options.RDP_gamma (beta is options.beta) */
+    int32_t prior;            /* OSL-OSEM, BSREM, ROSEM-MAP: omb_prior */
     const float *prior_window;/* Quad / Huber: device window of (2g0+1)(2g1+1)(2g2+1) weights, x fastest: the
                                  neighbours' -w and the centre sum(w) (libHeader.h:1147-1154) */
     int32_t prior_g[3];       /* Quad / Huber: options.Ndx, Ndy, Ndz */
     float huber_delta;        /* Huber: options.huber_delta */
+    const float *relaxation;  /* ROSEM / RAMLA / BSREM / ROSEM-MAP: host, n_iter values lam[iter]
+                                 (options.lambdaN); NULL: 1 / (iter / 20 + 1) (prepass.py:962-972) */
 } omb_recon_params;
 
 /*
@@ -331,6 +339,31 @@ int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const fl
  */
 int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
                    const float *du, float *work_meas, float *work_img, void *stream);
+
+/*
+ * One relaxed OSEM (ROSEM) sub-iteration (subiterStep.h:137-145,
+ * algorithms.h:102-106): the OSEM ratio y / (fp + epps [+ randoms]), its
+ * backprojection rhs, then image + lambda * image / sens * (rhs - sens).
+ */
+int omb_rosem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
+                     float lambda, float *work_meas, float *work_img, void *stream);
+
+/*
+ * One RAMLA / BSREM sub-iteration (subiterStep.h:130-135, 232-236;
+ * algorithms.h:54-64 on the GPU path): rhs = the backprojection of
+ * y / (fp + epps [+ randoms]) - 1 (NaN / Inf -> epps), then
+ * image + lambda * rhs * image, clamped to >= epps when `positivity` is set
+ * (PoissonUpdate, auxKernels.cl:1997-2026).  No sensitivity image.
+ */
+int omb_ramla_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda,
+                     int32_t positivity, float *work_meas, float *work_img, void *stream);
+
+/*
+ * The MAP step of BSREM and ROSEM-MAP after each iteration (algorithms.h:
+ * 130-135): image -= lambda * image * du, then image = max(image, epps);
+ * du (device, n voxels) is the prior gradient with its weight.
+ */
+int omb_map_step(float *image, const float *du, int64_t n, float lambda, float epps, void *stream);
 
 /*
  * PSF blur (Convolution3D_f, auxKernels.cl:192-245): out = window applied at

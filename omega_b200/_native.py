@@ -14,7 +14,7 @@ import numpy as np
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libomega_b200.so")
 
-OMB_ABI_VERSION = 3
+OMB_ABI_VERSION = 4
 OMB_PET_SINOGRAM = 0
 OMB_CT_PANEL = 1
 OMB_PET_LISTMODE = 2
@@ -95,12 +95,17 @@ class ReconParams(ctypes.Structure):
         ("prior_window", ctypes.c_void_p),
         ("prior_g", ctypes.c_int32 * 3),
         ("huber_delta", ctypes.c_float),
+        ("relaxation", ctypes.c_void_p),
     ]
 
 
 OMB_RECON_OSEM = 1
 OMB_RECON_PDHG_TV = 2
 OMB_RECON_OSL_OSEM = 3
+OMB_RECON_ROSEM = 4
+OMB_RECON_RAMLA = 5
+OMB_RECON_BSREM = 6
+OMB_RECON_ROSEM_MAP = 7
 OMB_PRIOR_RDP = 1
 OMB_PRIOR_QUAD = 2
 OMB_PRIOR_HUBER = 3
@@ -172,6 +177,14 @@ EXPORTS = [
     ("omb_osl_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p]),
+    ("omb_rosem_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
+    ("omb_ramla_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_float, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
+    ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_void_p]),
     ("omb_psf_convolve", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_void_p]),

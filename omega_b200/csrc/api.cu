@@ -664,6 +664,63 @@ int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
     return osl_update(image, sens, du, work_img, h->n_img, s);
 }
 
+}  // extern "C"
+
+namespace omb {
+int relaxed_subset(omb_handle *h, int32_t subset, bool ramla, float *image, const float *y_subset,
+                   const float *sens, Relax lam, bool positivity, float *work_meas, float *work_img,
+                   cudaStream_t s) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!image || !y_subset || (!ramla && !sens) || !work_meas || !work_img)
+        return set_error(OMB_ERR_INVALID, "NULL buffer passed to a relaxed sub-iteration");
+    if (h->desc.modality == OMB_CT_PANEL)
+        return set_error(OMB_ERR_UNSUPPORTED, "the relaxed sub-iterations are PET-only");
+    if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
+        return set_error(OMB_ERR_UNSUPPORTED, "the relaxed sub-iterations need projector types 1 or 4");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    const float eps = h->desc.epps;
+    const int64_t m = rs.m_size * h->desc.tof_bins;
+    st = rays_forward(h, rs, one_frame_fp(h, image, work_meas, rs.m_size), s);
+    if (st != OMB_OK) return st;
+    st = ratio_shift(y_subset, work_meas, m, h->d_rand ? h->d_rand + subset_ray0(h, rs, subset) : nullptr,
+                     rs.m_size, eps, ramla ? 1.f : 0.f, s);
+    if (st != OMB_OK) return st;
+    OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
+    st = rays_backward(h, rs, one_frame_bp(h, work_meas, work_img, rs.m_size), nullptr, s);
+    if (st != OMB_OK) return st;
+    return ramla ? bsrem_update(image, work_img, h->n_img, lam, eps, positivity, s)
+                 : rosem_update(image, sens, work_img, h->n_img, lam, s);
+}
+}  // namespace omb
+
+extern "C" {
+
+int omb_rosem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
+                     float lambda, float *work_meas, float *work_img, void *stream) {
+    Relax lam;
+    lam.v = lambda;
+    return relaxed_subset(h, subset, false, image, y_subset, sens, lam, false, work_meas, work_img,
+                          (cudaStream_t)stream);
+}
+
+int omb_ramla_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda,
+                     int32_t positivity, float *work_meas, float *work_img, void *stream) {
+    Relax lam;
+    lam.v = lambda;
+    return relaxed_subset(h, subset, true, image, y_subset, nullptr, lam, positivity != 0, work_meas, work_img,
+                          (cudaStream_t)stream);
+}
+
+int omb_map_step(float *image, const float *du, int64_t n, float lambda, float epps, void *stream) {
+    if (n < 0) return set_error(OMB_ERR_INVALID, "n must be >= 0");
+    if (n > 0 && (!image || !du)) return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_map_step");
+    Relax lam;
+    lam.v = lambda;
+    return map_step(image, du, n, lam, epps, (cudaStream_t)stream);
+}
+
 int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, float *images, int64_t image_stride,
                            const float *y_subset, int64_t y_stride, const float *sens, float *work_meas,
                            float *work_img, void *stream) {

@@ -93,6 +93,98 @@ int scale_clamp(float *du, int64_t n, float beta, float delta, cudaStream_t st) 
     return OMB_OK;
 }
 
+// The relaxed updates (ROSEM algorithms.h:102-106; RAMLA / BSREM through
+// PoissonUpdate, auxKernels.cl:1997-2026; the MAP step algorithms.h:130-135),
+// the relaxation read per launch so that a captured iteration replays with
+// the schedule's next value.
+__device__ __forceinline__ float relax_value(const float *lam, const int *iter, float v) {
+    return lam ? lam[*iter] : v;
+}
+
+__global__ void k_ratio_shift(const float *__restrict__ y, float *__restrict__ fp, int64_t n,
+                              const float *__restrict__ rnd, int64_t n_rays, float epps, float shift) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float d = fp[i] + epps;
+        if (rnd) d += __ldg(rnd + i % n_rays);
+        float r = __ldg(y + i) / d - shift;
+        if (isnan(r) || isinf(r)) r = epps;
+        fp[i] = r;
+    }
+}
+
+__global__ void k_rosem_update(float *__restrict__ img, const float *__restrict__ sens, const float *__restrict__ rhs,
+                               int64_t n, const float *__restrict__ lam_s, const int *__restrict__ it, float lam_v) {
+    const float lam = relax_value(lam_s, it, lam_v);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float x = img[i], sm = __ldg(sens + i);
+        img[i] = x + lam * x / sm * (__ldg(rhs + i) - sm);
+    }
+}
+
+__global__ void k_bsrem_update(float *__restrict__ img, const float *__restrict__ rhs, int64_t n,
+                               const float *__restrict__ lam_s, const int *__restrict__ it, float lam_v, float epps,
+                               int positivity) {
+    const float lam = relax_value(lam_s, it, lam_v);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float x = img[i];
+        float v = x + lam * __ldg(rhs + i) * x;
+        if (positivity) v = fmaxf(epps, v);
+        img[i] = v;
+    }
+}
+
+__global__ void k_map_step(float *__restrict__ img, const float *__restrict__ du, int64_t n,
+                           const float *__restrict__ lam_s, const int *__restrict__ it, float lam_v, float epps) {
+    const float lam = relax_value(lam_s, it, lam_v);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float x = img[i];
+        const float v = x - lam * x * __ldg(du + i);
+        img[i] = v < epps ? epps : v;
+    }
+}
+
+__global__ void k_relax_advance(int *it) { *it += 1; }
+
+int ratio_shift(const float *y, float *fp, int64_t n, const float *rnd, int64_t n_rays, float epps, float shift,
+                cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    if (rnd && n_rays <= 0) return set_error(OMB_ERR_INVALID, "randoms need n_rays > 0");
+    k_ratio_shift<<<grid_for(n, 4), kBlock, 0, st>>>(y, fp, n, rnd, n_rays, epps, shift);
+    OMB_LAUNCH_CHECK("ratio launch");
+    return OMB_OK;
+}
+
+int rosem_update(float *img, const float *sens, const float *rhs, int64_t n, Relax lam, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_rosem_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, sens, rhs, n, lam.lam, lam.iter, lam.v);
+    OMB_LAUNCH_CHECK("ROSEM update launch");
+    return OMB_OK;
+}
+
+int bsrem_update(float *img, const float *rhs, int64_t n, Relax lam, float epps, bool positivity, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_bsrem_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, rhs, n, lam.lam, lam.iter, lam.v, epps, positivity ? 1 : 0);
+    OMB_LAUNCH_CHECK("BSREM update launch");
+    return OMB_OK;
+}
+
+int map_step(float *img, const float *du, int64_t n, Relax lam, float epps, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_map_step<<<grid_for(n, 4), kBlock, 0, st>>>(img, du, n, lam.lam, lam.iter, lam.v, epps);
+    OMB_LAUNCH_CHECK("MAP step launch");
+    return OMB_OK;
+}
+
+int relax_advance(int *iter, cudaStream_t st) {
+    k_relax_advance<<<1, 1, 0, st>>>(iter);
+    OMB_LAUNCH_CHECK("relaxation counter launch");
+    return OMB_OK;
+}
+
 int osem_ratio_randoms(const float *y, int64_t y_stride, float *fp, int64_t fp_stride, int64_t n, int frames,
                        const float *rnd, int64_t n_rays, float epps, cudaStream_t st) {
     if (n <= 0 || frames <= 0) return OMB_OK;

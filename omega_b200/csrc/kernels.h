@@ -23,6 +23,30 @@ int scale_clamp(float *du, int64_t n, float beta, float delta, cudaStream_t st);
 // x = x / (sens + du) * rhs
 int osl_update(float *img, const float *sens, const float *du, const float *rhs, int64_t n, cudaStream_t st);
 
+// Relaxation of one sub-iteration: lam[*iter] from a device schedule (the
+// built-in loop, so a captured iteration replays with the next value), else
+// the host value v.
+struct Relax {
+    const float *lam = nullptr;
+    const int *iter = nullptr;
+    float v = 1.f;
+};
+// fp = y / ((fp + epps) [+ r]) - shift, NaN / Inf -> epps; r (nullable) per ray, shared by TOF bins
+int ratio_shift(const float *y, float *fp, int64_t n, const float *rnd, int64_t n_rays, float epps, float shift,
+                cudaStream_t st);
+// ROSEM: x = x + lam * x / sens * (rhs - sens)
+int rosem_update(float *img, const float *sens, const float *rhs, int64_t n, Relax lam, cudaStream_t st);
+// RAMLA / BSREM: x = x + lam * rhs * x, then max(epps, x) when positivity
+int bsrem_update(float *img, const float *rhs, int64_t n, Relax lam, float epps, bool positivity, cudaStream_t st);
+// MAP step: x = x - lam * x * du, then max(epps, x)
+int map_step(float *img, const float *du, int64_t n, Relax lam, float epps, cudaStream_t st);
+// ++*iter on the stream
+int relax_advance(int *iter, cudaStream_t st);
+// One ROSEM (ramla = false) or RAMLA / BSREM (ramla = true) sub-iteration of a handle.
+int relaxed_subset(omb_handle *h, int32_t subset, bool ramla, float *image, const float *y_subset,
+                   const float *sens, Relax lam, bool positivity, float *work_meas, float *work_img,
+                   cudaStream_t st);
+
 // Multi-ray PET projections (rs.nr_xy x rs.nr_z rays per LOR), one frame.
 int multiray_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *img, float *y,
                      int per_sm, cudaStream_t st);

@@ -1,7 +1,8 @@
 // The built-in reconstruction loop behind one call (the reference's compiled
-// omegaMain entry, libHeader.h:1466, reconstructionAF.h:1053-1500, for the two
-// algorithms of this path): OSEM for PET data and PDHG with the smoothed TV
-// gradient, with every sub-iteration issued on the caller's stream by the
+// omegaMain entry, libHeader.h:1466, reconstructionAF.h:1053-1500, for the
+// algorithms of this path): OSEM, OSL-OSEM, the relaxed ROSEM / RAMLA / BSREM /
+// ROSEM-MAP for PET data, and PDHG with the smoothed TV gradient, with every
+// sub-iteration issued on the caller's stream by the
 // same entry points a custom loop uses, and (use_graph) one iteration captured
 // as a CUDA graph and replayed.
 #include <cmath>
@@ -77,11 +78,16 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
     OMB_CUDA_TRY(cudaMemcpyAsync(x_out, x0, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
     const bool graph = p->use_graph != 0;
     int st = OMB_OK;
-    if (p->algorithm == OMB_RECON_OSEM || p->algorithm == OMB_RECON_OSL_OSEM) {
-        const bool osl = p->algorithm == OMB_RECON_OSL_OSEM;
-        if (osl && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_HUBER))
+    const int alg = p->algorithm;
+    if (alg == OMB_RECON_OSEM || alg == OMB_RECON_OSL_OSEM || alg == OMB_RECON_ROSEM || alg == OMB_RECON_RAMLA ||
+        alg == OMB_RECON_BSREM || alg == OMB_RECON_ROSEM_MAP) {
+        const bool osl = alg == OMB_RECON_OSL_OSEM;
+        const bool map = alg == OMB_RECON_BSREM || alg == OMB_RECON_ROSEM_MAP;  // MAP step once per iteration
+        const bool ramla = alg == OMB_RECON_RAMLA || alg == OMB_RECON_BSREM;    // no sensitivity image
+        const bool relaxed = alg >= OMB_RECON_ROSEM;
+        if ((osl || map) && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_HUBER))
             return set_error(OMB_ERR_INVALID, "unknown prior");
-        if (osl && p->prior != OMB_PRIOR_RDP && !p->prior_window)
+        if ((osl || map) && p->prior != OMB_PRIOR_RDP && !p->prior_window)
             return set_error(OMB_ERR_INVALID, "the quadratic / Huber prior needs its window");
         const Grid g = handle_grid(h);
         const float epps = handle_epps(h);
@@ -93,39 +99,63 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             off[s_ + 1] = off[s_] + ms;
             m_max = ms > m_max ? ms : m_max;
         }
-        DevBuf sens, wm, wi, du;
-        if ((st = alloc(sens, (size_t)n_subsets * n * sizeof(float), s)) != OMB_OK) return st;
-        if (osl && (st = alloc(du, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        DevBuf sens, wm, wi, du, lam;
+        if (!ramla && (st = alloc(sens, (size_t)n_subsets * n * sizeof(float), s)) != OMB_OK) return st;
+        if ((osl || map) && (st = alloc(du, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(wm, (size_t)m_max * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(wi, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
-        for (int s_ = 0; s_ < n_subsets && st == OMB_OK; ++s_) st = omb_sensitivity(h, s_, sens.f() + s_ * n, stream);
+        Relax rl;
+        if (relaxed && p->n_iter > 0) {
+            // lam[iter] in device memory with the iteration counter behind it, so that a replayed
+            // iteration reads the next value (libHeader.h:1331-1333; default prepass.py:962-972)
+            std::vector<float> host((size_t)p->n_iter + 1, 0.f);
+            for (int i = 0; i < p->n_iter; ++i)
+                host[i] = p->relaxation ? p->relaxation[i] : (float)(1.0 / (i / 20.0 + 1.0));
+            if ((st = alloc(lam, host.size() * sizeof(float) + 16, s)) != OMB_OK) return st;
+            int *counter = reinterpret_cast<int *>(lam.f() + host.size());
+            OMB_CUDA_TRY(cudaMemcpyAsync(lam.p, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+            OMB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), s));
+            // the host vector leaves scope: wait for the copy
+            OMB_CUDA_TRY(cudaStreamSynchronize(s));
+            rl.lam = lam.f();
+            rl.iter = counter;
+        }
+        for (int s_ = 0; s_ < n_subsets && !ramla && st == OMB_OK; ++s_)
+            st = omb_sensitivity(h, s_, sens.f() + s_ * n, stream);
         if (st != OMB_OK) return st;
+        // dU = beta * the prior's gradient at x_out
+        auto prior_grad = [&]() -> int {
+            if (cudaMemsetAsync(du.p, 0, (size_t)n * sizeof(float), s) != cudaSuccess)
+                return set_error(OMB_ERR_CUDA, "clearing the prior gradient failed");
+            if (p->prior == OMB_PRIOR_RDP)
+                return omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
+            // quadratic: the window applied at every voxel (priors.h:27-42); Huber clamps it
+            int e = omb_psf_convolve(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_window, p->prior_g[0], p->prior_g[1],
+                                     p->prior_g[2], stream);
+            if (e == OMB_OK)
+                e = scale_clamp(du.f(), n, p->beta, p->prior == OMB_PRIOR_HUBER ? p->huber_delta : INFINITY, s);
+            return e;
+        };
         st = repeat(p->n_iter, graph, s, [&]() {
-            for (int s_ = 0; s_ < n_subsets; ++s_) {
-                int e;
+            int e = OMB_OK;
+            for (int s_ = 0; s_ < n_subsets && e == OMB_OK; ++s_) {
+                float *ss = ramla ? nullptr : sens.f() + s_ * n;
                 if (osl) {
                     // dU of the current image, then the one-step-late update
-                    if (cudaMemsetAsync(du.p, 0, (size_t)n * sizeof(float), s) != cudaSuccess)
-                        return set_error(OMB_ERR_CUDA, "clearing the prior gradient failed");
-                    if (p->prior == OMB_PRIOR_RDP) {
-                        e = omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
-                    } else {
-                        // quadratic: the window applied at every voxel (priors.h:27-42); Huber clamps it
-                        e = omb_psf_convolve(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_window, p->prior_g[0],
-                                             p->prior_g[1], p->prior_g[2], stream);
-                        if (e == OMB_OK)
-                            e = scale_clamp(du.f(), n, p->beta,
-                                            p->prior == OMB_PRIOR_HUBER ? p->huber_delta : INFINITY, s);
-                    }
-                    if (e == OMB_OK)
-                        e = omb_osl_subset(h, s_, x_out, y + off[s_], sens.f() + s_ * n, du.f(), wm.f(), wi.f(),
-                                           stream);
+                    e = prior_grad();
+                    if (e == OMB_OK) e = omb_osl_subset(h, s_, x_out, y + off[s_], ss, du.f(), wm.f(), wi.f(), stream);
+                } else if (relaxed) {
+                    e = relaxed_subset(h, s_, ramla, x_out, y + off[s_], ss, rl, p->positivity != 0, wm.f(), wi.f(),
+                                       s);
                 } else {
-                    e = omb_osem_subset(h, s_, x_out, y + off[s_], sens.f() + s_ * n, wm.f(), wi.f(), stream);
+                    e = omb_osem_subset(h, s_, x_out, y + off[s_], ss, wm.f(), wi.f(), stream);
                 }
-                if (e != OMB_OK) return e;
             }
-            return (int)OMB_OK;
+            // BSREM / ROSEM-MAP: the prior at the iterate, then the MAP step (iterStep.h:14-34)
+            if (e == OMB_OK && map) e = prior_grad();
+            if (e == OMB_OK && map) e = map_step(x_out, du.f(), n, rl, epps, s);
+            if (e == OMB_OK && relaxed) e = relax_advance(const_cast<int *>(rl.iter), s);
+            return e;
         });
     } else if (p->algorithm == OMB_RECON_PDHG_TV) {
         const int64_t m_all = omb_measurement_count(h, -1);  // one subset: all measurements

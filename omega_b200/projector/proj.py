@@ -120,6 +120,11 @@ class projectorClass:
     # path and their parameters (proj.py:116-120, 236, 271, 275, 317, 370-420)
     OSEM = False
     OSL_OSEM = False
+    ROSEM = False
+    RAMLA = False
+    BSREM = False
+    ROSEM_MAP = False
+    lambdaN = np.empty(0, dtype=np.float32)
     PDHG = False
     TV = False
     RDP = False

@@ -1,5 +1,7 @@
 """Subset-update loops driven by the projectors: OSEM (PET) and PDHG with a
-TV-gradient term (CT), plus the power method for the PDHG step size.
+TV-gradient term (CT), plus the power method for the PDHG step size; the
+built-in entry adds OSL-OSEM and the relaxed ROSEM / RAMLA / BSREM /
+ROSEM-MAP (PET).
 
 These are the loops of OMEGA's compiled reconstruction (reconstructionAF.h:
 1053-1500) for the two algorithms on this path, run on the device through
@@ -225,33 +227,65 @@ class OSEMBatch:
         return self.x
 
 
+_PET_METHODS = {'OSEM': _native.OMB_RECON_OSEM, 'OSL_OSEM': _native.OMB_RECON_OSL_OSEM,
+                'ROSEM': _native.OMB_RECON_ROSEM, 'RAMLA': _native.OMB_RECON_RAMLA,
+                'BSREM': _native.OMB_RECON_BSREM, 'ROSEM_MAP': _native.OMB_RECON_ROSEM_MAP}
+_PRIOR_METHODS = ('OSL_OSEM', 'BSREM', 'ROSEM_MAP')
+
+
+def relaxation(options):
+    """Relaxation values lam[iter] of ROSEM / RAMLA / BSREM / ROSEM-MAP as the
+    reference's prepass sets them (prepass.py:962-987): options.lambdaN when
+    it holds at least Niter values (extra values ignored), else
+    1 / (iter / 20 + 1); float32."""
+    n = int(options.Niter)
+    lam = np.asarray(getattr(options, 'lambdaN', np.empty(0)), dtype=np.float32).ravel()
+    if lam.size == 0 or float(np.sum(lam)) == 0.:
+        lam = np.zeros(0, dtype=np.float32)
+    elif lam.size < n:
+        print('Warning: The number of relaxation values must be at least the number of iterations times the '
+              'number of subsets! Computing custom relaxation values.')
+        lam = np.zeros(0, dtype=np.float32)
+    elif lam.size > n:
+        print('Warning: The number of relaxation values is more than the number of iterations. '
+              'Later values are ignored!')
+    if lam.size == 0:
+        lam = np.array([1. / (i / 20. + 1.) for i in range(n)], dtype=np.float32)
+    options.lambdaN = lam
+    return np.ascontiguousarray(lam[:n], dtype=np.float32)
+
+
 def reconstructions_main(options):
     """The built-in reconstruction (omegatomo/reconstruction/recomain.py:427-725,
     the compiled omegaMain entry) for the algorithms of this path:
-    options.OSEM (PET), options.OSL_OSEM with options.RDP, options.Quad or
-    options.Huber (PET, one-step-late MAP; Ndx/Ndy/Ndz neighbourhood weights as
-    the reference forms them) or options.PDHG with options.TV, options.Niter
-    iterations from options.x0, run natively by omb_reconstruct.  CT data are
-    linearised as log(flat / SinM) first (prepass.py:22-36; flat = max(SinM)
-    when options.flat <= 0), negative PET counts set to 0.  Returns
-    (image of shape (Nx, Ny, Nz, 1) in Fortran order, empty forward
-    projections), as the reference does with storeFP off.  Reads
-    options.use_graph (default True) to replay iterations as CUDA graphs."""
+    options.OSEM, options.ROSEM and options.RAMLA (PET), options.OSL_OSEM,
+    options.BSREM and options.ROSEM_MAP with options.RDP, options.Quad or
+    options.Huber (PET, MAP; Ndx/Ndy/Ndz neighbourhood weights as the
+    reference forms them; relaxation options.lambdaN) or options.PDHG with
+    options.TV, options.Niter iterations from options.x0, run natively by
+    omb_reconstruct.  CT data are linearised as log(flat / SinM) first
+    (prepass.py:22-36; flat = max(SinM) when options.flat <= 0), negative PET
+    counts set to 0.  Returns (image of shape (Nx, Ny, Nz, 1) in Fortran
+    order, empty forward projections), as the reference does with storeFP
+    off.  Reads options.use_graph (default True) to replay iterations as CUDA
+    graphs."""
     import torch
-    osl = bool(getattr(options, 'OSL_OSEM', False))
-    if not (options.OSEM or options.PDHG or osl):
+    chosen = [k for k in _PET_METHODS if bool(getattr(options, k, False))]
+    if options.PDHG:
+        chosen.append('PDHG')
+    if not chosen:
         raise ValueError('No reconstruction method selected, aborting.')
-    if int(bool(options.OSEM)) + int(bool(options.PDHG)) + int(osl) > 1:
-        raise ValueError('Select one reconstruction method (OSEM, OSL_OSEM or PDHG)')
+    if len(chosen) > 1:
+        raise ValueError('Select one reconstruction method (' + ', '.join(list(_PET_METHODS) + ['PDHG']) + ')')
+    method = chosen[0]
     quad, huber = bool(getattr(options, 'Quad', False)), bool(getattr(options, 'Huber', False))
-    if osl and int(bool(options.RDP)) + int(quad) + int(huber) != 1:
-        raise ValueError('OSL_OSEM needs one prior: options.RDP, options.Quad or options.Huber')
-    if osl and options.CT:
-        raise ValueError('OSL_OSEM is built for PET data')
+    prior = method in _PRIOR_METHODS
+    if prior and int(bool(options.RDP)) + int(quad) + int(huber) != 1:
+        raise ValueError(method + ' needs one prior: options.RDP, options.Quad or options.Huber')
+    if method != 'PDHG' and options.CT:
+        raise ValueError(method + ' is built for PET data')
     if options.PDHG and not options.TV:
         raise ValueError('PDHG is built with the TV prior (options.TV = True)')
-    if options.OSEM and options.CT:
-        raise ValueError('OSEM is built for PET data')
     sin = np.asarray(options.SinM, dtype=np.float32)
     if options.CT and not options.usingLinearizedData:
         if options.flat <= 0:
@@ -268,7 +302,7 @@ def reconstructions_main(options):
     n = int(np.ravel(options.N)[0])
     m = np.asarray(options.SinM, dtype=np.float32).ravel(order='F')
     S = int(options.subsets)
-    if options.OSEM or osl:
+    if method != 'PDHG':
         parts = [np.asarray(options.subsetMeasurements(m, s)) for s in range(S)]
         y = torch.from_numpy(np.ascontiguousarray(np.concatenate(parts), dtype=np.float32)).to(dev)
     else:
@@ -279,11 +313,14 @@ def reconstructions_main(options):
     x0 = torch.from_numpy(np.ascontiguousarray(x0)).to(dev)
     x = torch.empty(n, device=dev)
     p = _native.ReconParams(struct_size=ctypes.sizeof(_native.ReconParams))
-    p.algorithm = (_native.OMB_RECON_OSEM if options.OSEM else
-                   (_native.OMB_RECON_OSL_OSEM if osl else _native.OMB_RECON_PDHG_TV))
+    p.algorithm = _PET_METHODS.get(method, _native.OMB_RECON_PDHG_TV)
     p.rdp_gamma = float(getattr(options, 'RDP_gamma', 1.0))
     window = None
-    if osl:
+    lam = None
+    if method in ('ROSEM', 'RAMLA', 'BSREM', 'ROSEM_MAP'):
+        lam = relaxation(options)
+        p.relaxation = ctypes.c_void_p(lam.ctypes.data)
+    if prior:
         p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
                    (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))
         if quad or huber:

@@ -278,6 +278,58 @@ def osem(geom: Geometry, y_subsets, x0, n_iter, forward=None, backward=None, ran
     return x
 
 
+def default_relaxation(n_iter):
+    """lam[iter] = 1 / (iter / 20 + 1) in float32 (prepass.py:962-972)."""
+    return np.array([1. / (i / 20. + 1.) for i in range(n_iter)], dtype=np.float32)
+
+
+def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None, backward=None, randoms=None,
+            prior_grad=None, positivity=True):
+    """Restated relaxed loops in FP64 (kind: "ROSEM", "RAMLA", "BSREM",
+    "ROSEM_MAP"); returns the image after n_iter iterations.
+    ROSEM sub-iteration (algorithms.h:102-106): x + lam x / sens (rhs - sens),
+    rhs the backprojection of y / (fp + epps [+ r]).
+    RAMLA / BSREM (computeForwardProject.h:98-122, auxKernels.cl:1997-2026):
+    x + lam rhs x, rhs the backprojection of y / (fp + epps [+ r]) - 1, then
+    max(epps, x) with positivity.  BSREM / ROSEM-MAP end each iteration with
+    the MAP step x - lam x dU, x < epps -> epps (iterStep.h:14-34,
+    algorithms.h:130-135); dU = prior_grad(x), weight included."""
+    fwd = forward or globals()["forward"]
+    bwd = backward or globals()["backward"]
+    lam = np.asarray(default_relaxation(n_iter) if lam is None else lam, dtype=np.float32)
+    ramla = kind in ("RAMLA", "BSREM")
+    mapstep = kind in ("BSREM", "ROSEM_MAP")
+    x = np.asarray(x0, dtype=np.float64).copy()
+    eps = geom.epps
+    sens = []
+    if not ramla:
+        for s in range(geom.n_subsets):
+            _, sv = bwd(geom, None, s, sens=True)
+            sens.append(np.maximum(sv, eps))
+    for it in range(n_iter):
+        lm = float(lam[it])
+        for s in range(geom.n_subsets):
+            fp = fwd(geom, x, s) + eps
+            if randoms is not None:
+                fp = fp + np.tile(np.asarray(randoms[s], dtype=np.float64), geom.nbins)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                r = np.asarray(y_subsets[s], dtype=np.float64) / fp
+            if ramla:
+                r = r - 1.0
+            r[~np.isfinite(r)] = eps
+            rhs = bwd(geom, r, s)
+            if ramla:
+                x = x + lm * rhs * x
+                if positivity:
+                    x = np.maximum(eps, x)
+            else:
+                x = x + lm * x / sens[s] * (rhs - sens[s])
+        if mapstep:
+            x = x - lm * x * prior_grad(x)
+            x[x < eps] = eps
+    return x
+
+
 def loglik(y, fp, eps):
     """Poisson log-likelihood sum[y log(fp + eps) - (fp + eps)] in FP64."""
     f = np.asarray(fp, dtype=np.float64) + eps
