@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define OMB_ABI_VERSION 4
+#define OMB_ABI_VERSION 5
 
 typedef enum omb_status {
     OMB_OK = 0,
@@ -79,8 +79,9 @@ typedef struct omb_geometry_desc {
     uint32_t struct_size;
     uint32_t abi_version;
     int32_t modality;        /* omb_modality */
-    int32_t fp_type;         /* forward projector: 1 (improved Siddon), 4 (interpolation), 5 (branchless distance-driven) */
-    int32_t bp_type;         /* backprojector: 1, 4 or 5 */
+    int32_t fp_type;         /* forward projector: 1 (improved Siddon), 2 (orthogonal distance), 3 (volume of
+                                intersection), 4 (interpolation), 5 (branchless distance-driven) */
+    int32_t bp_type;         /* backprojector: 1 to 5 */
     uint32_t nx, ny, nz;     /* image size */
     float dx, dy, dz;        /* voxel size (mm) */
     float bx, by, bz;        /* FOV corner (mm), the lower edge of voxel 0 */
@@ -111,6 +112,15 @@ typedef struct omb_geometry_desc {
     int32_t n_rays_xy;         /* PET multi-ray (proj.py n_rays_transaxial, 0 or 1: one ray): rays per LOR
                                   spread over dpitch_x transaxially */
     int32_t n_rays_z;          /* (n_rays_axial) rays spread over dpitch_y axially; projector type 1 only */
+    /* Projector types 2 / 3 (PET; the tube of response of projectorType123.cl -DORTH / -DVOL).  The image must
+     * be square transaxially (nx == ny, dx == dy, bx == by). */
+    float tube_width;          /* type 2: options.tube_width_z (mm), the distance where the weight reaches 0 */
+    float tube_radius;         /* type 3: options.tube_radius (mm) */
+    int32_t orth_xy;           /* options.orthTransaxial: the tube spreads in the slice (CRYSTXY) */
+    int32_t orth_z;            /* options.orthAxial: the tube spreads axially (CRYSTZ) */
+    float vol_bmin, vol_bmax, vol_vmax; /* type 3: options.bmin, bmax, Vmax (coordinates.py:192-206) */
+    const float *vol_v;        /* type 3: options.V, the intersection volume per 1/1000 mm above bmin */
+    int64_t n_vol_v;           /* entries in vol_v */
 } omb_geometry_desc;
 
 typedef struct omb_handle omb_handle;

@@ -14,7 +14,7 @@ import numpy as np
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libomega_b200.so")
 
-OMB_ABI_VERSION = 4
+OMB_ABI_VERSION = 5
 OMB_PET_SINOGRAM = 0
 OMB_CT_PANEL = 1
 OMB_PET_LISTMODE = 2
@@ -72,6 +72,15 @@ class GeometryDesc(ctypes.Structure):
         ("ax_index", ctypes.POINTER(ctypes.c_uint16)),
         ("n_rays_xy", ctypes.c_int32),
         ("n_rays_z", ctypes.c_int32),
+        ("tube_width", ctypes.c_float),
+        ("tube_radius", ctypes.c_float),
+        ("orth_xy", ctypes.c_int32),
+        ("orth_z", ctypes.c_int32),
+        ("vol_bmin", ctypes.c_float),
+        ("vol_bmax", ctypes.c_float),
+        ("vol_vmax", ctypes.c_float),
+        ("vol_v", ctypes.POINTER(ctypes.c_float)),
+        ("n_vol_v", ctypes.c_int64),
     ]
 
 

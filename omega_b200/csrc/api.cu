@@ -51,6 +51,8 @@ struct omb_handle {
     float *d_w = nullptr;                 // PET: multiplicative weight per measurement (all subsets), or NULL
     float *d_mu = nullptr;                // PET: attenuation image, or NULL
     float *d_rand = nullptr;              // PET: randoms per measurement (all subsets) for the OSEM ratio, or NULL
+    float *d_vol = nullptr;               // type 3: the intersection-volume table
+    Orth orth_fp{}, orth_bp{};            // types 2 / 3: the tube of the forward / backward projector
     // Buffers replaced by larger ones.  They are freed only with the handle:
     // a CUDA graph captured earlier may still address them.
     std::vector<void *> retired;
@@ -153,10 +155,29 @@ static int validate(const omb_geometry_desc *d) {
         if (d->modality == OMB_PET_INDEXED && (!d->tr_index || !d->ax_index))
             return set_error(OMB_ERR_INVALID, "index-based data needs tr_index and ax_index");
     }
-    if (d->fp_type != 1 && d->fp_type != 4 && d->fp_type != 5)
+    if (d->fp_type < 1 || d->fp_type > 5)
         return set_error(OMB_ERR_UNSUPPORTED, "forward projector type " + std::to_string(d->fp_type) + " is not built");
-    if (d->bp_type != 1 && d->bp_type != 4 && d->bp_type != 5)
+    if (d->bp_type < 1 || d->bp_type > 5)
         return set_error(OMB_ERR_UNSUPPORTED, "backprojector type " + std::to_string(d->bp_type) + " is not built");
+    const bool orth = d->fp_type == 2 || d->fp_type == 3 || d->bp_type == 2 || d->bp_type == 3;
+    if (orth) {
+        if (d->modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "projector types 2 / 3 are built for PET");
+        if ((d->fp_type == 2 || d->fp_type == 3) && (d->bp_type == 2 || d->bp_type == 3) && d->fp_type != d->bp_type)
+            return set_error(OMB_ERR_UNSUPPORTED, "projector types 23 / 32 are not built");
+        if (d->nx != d->ny || d->dx != d->dy || d->bx != d->by)
+            return set_error(OMB_ERR_UNSUPPORTED,
+                             "projector types 2 / 3 need a square transaxial grid (nx == ny, dx == dy, bx == by)");
+        if ((d->fp_type == 2 || d->bp_type == 2) && !(d->tube_width > 0.f))
+            return set_error(OMB_ERR_INVALID, "projector type 2 needs tube_width (options.tube_width_z) > 0");
+        if ((d->fp_type == 2 || d->bp_type == 2) && d->tof_bins > 1)
+            return set_error(OMB_ERR_INVALID, "TOF is not supported with projector type 2");
+        if (d->fp_type == 3 || d->bp_type == 3) {
+            if (!(d->tube_radius > 0.f)) return set_error(OMB_ERR_INVALID, "projector type 3 needs tube_radius > 0");
+            if (!d->vol_v || d->n_vol_v < 1 || d->n_vol_v > (1 << 24))
+                return set_error(OMB_ERR_INVALID, "projector type 3 needs its volume table vol_v");
+            if (!(d->vol_bmax > d->vol_bmin)) return set_error(OMB_ERR_INVALID, "projector type 3 needs vol_bmax > vol_bmin");
+        }
+    }
     if ((d->fp_type == 5 || d->bp_type == 5) && d->modality != OMB_CT_PANEL)
         return set_error(OMB_ERR_INVALID, "Projector type 5 is only supported with CT data!");
     if ((d->fp_type == 5 || d->bp_type == 5) && d->tof_bins > 1)
@@ -303,6 +324,15 @@ static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cud
         f.img_in16 = h->d_img16;
         f.img_stride = h->n_img;
     }
+    if (h->desc.fp_type == 2 || h->desc.fp_type == 3) {
+        if (f.img_in16) return set_error(OMB_ERR_UNSUPPORTED, "projector types 2 / 3 read FP32 images");
+        for (int fr = 0; fr < f.n; ++fr) {
+            const int st = orth_forward(h->grid, rs, h->orth_fp, h->tof, h->desc.global_factor,
+                                        f.img_in + fr * f.img_stride, f.meas_out + fr * f.meas_stride, s);
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
     if (h->desc.fp_type == 4) {
         if (rs.w || rs.mu) return set_error(OMB_ERR_UNSUPPORTED, "PET corrections are built for projector type 1");
         for (int fr = 0; fr < f.n; ++fr) {
@@ -333,6 +363,15 @@ static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cud
 // the sensitivity.
 static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, float *sens, cudaStream_t s) {
     Frames f = f_in;
+    if (h->desc.bp_type == 2 || h->desc.bp_type == 3) {
+        for (int fr = 0; fr < f.n; ++fr) {
+            const int st = orth_backward(h->grid, rs, h->orth_bp, h->tof, h->desc.global_factor,
+                                         f.meas ? f.meas + fr * f.meas_stride : nullptr,
+                                         f.img ? f.img + fr * f.img_stride : nullptr, fr == 0 ? sens : nullptr, s);
+            if (st != OMB_OK) return st;
+        }
+        return OMB_OK;
+    }
     if (h->desc.bp_type == 4) {
         if (rs.w || rs.mu) return set_error(OMB_ERR_UNSUPPORTED, "PET corrections are built for projector type 1");
         for (int fr = 0; fr < f.n; ++fr) {
@@ -438,6 +477,29 @@ int omb_create(const omb_geometry_desc *desc, omb_handle **out) {
         if ((e = cudaMalloc(&h->d_acc, 2 * h->n_img * sizeof(unsigned long long))) != cudaSuccess)
             return fail(cuda_fail(e, "cudaMalloc fixed-point accumulators"));
     }
+    h->desc.vol_v = nullptr;
+    if (desc->fp_type == 3 || desc->bp_type == 3) {
+        if ((e = cudaMalloc(&h->d_vol, desc->n_vol_v * sizeof(float))) != cudaSuccess)
+            return fail(cuda_fail(e, "cudaMalloc volume table"));
+        if ((e = cudaMemcpy(h->d_vol, desc->vol_v, desc->n_vol_v * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail(cuda_fail(e, "upload volume table"));
+    }
+    // the tube of each direction: the width argument follows the kernel's own type (init.py:650-655)
+    auto tube = [&](int type) {
+        Orth o{};
+        o.type = type;
+        o.width = type == 2 ? desc->tube_width : desc->tube_radius;
+        o.xy = desc->orth_xy != 0;
+        o.z = desc->orth_z != 0;
+        o.bmin = desc->vol_bmin;
+        o.bmax = desc->vol_bmax;
+        o.vmax = desc->vol_vmax;
+        o.v = h->d_vol;
+        o.nv = type == 3 ? (int)desc->n_vol_v : 0;
+        return o;
+    };
+    h->orth_fp = tube(desc->fp_type);
+    h->orth_bp = tube(desc->bp_type);
     *out = h;
     return OMB_OK;
 }
@@ -460,6 +522,7 @@ int omb_destroy(omb_handle *h) {
     cudaFree(h->d_w);
     cudaFree(h->d_mu);
     cudaFree(h->d_rand);
+    cudaFree(h->d_vol);
     for (void *p : h->retired) cudaFree(p);
     if (prev != h->device) cudaSetDevice(prev);
     delete h;
@@ -599,8 +662,8 @@ int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
-    if (h->desc.modality != OMB_PET_SINOGRAM || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
-        return set_error(OMB_ERR_UNSUPPORTED, "omb_sensitivity needs a ray-driven PET backprojector (type 1 or 4)");
+    if (h->desc.modality != OMB_PET_SINOGRAM || h->desc.bp_type < 1 || h->desc.bp_type > 4)
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_sensitivity needs a ray-driven PET backprojector (types 1 to 4)");
     // A^T 1 through the BP kernel's fused sensitivity accumulator, y = NULL.
     OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, h->n_img * sizeof(float), s));
     st = rays_backward(h, rs, one_frame_bp(h, nullptr, nullptr, rs.m_size), sens, s);
@@ -614,8 +677,8 @@ int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_
     if (!image || !y_subset || !sens || !work_meas || !work_img)
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osem_subset");
     if (h->desc.modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
-    if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
-        return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset needs projector types 1 or 4");
+    if (h->desc.fp_type < 1 || h->desc.fp_type > 4 || h->desc.bp_type < 1 || h->desc.bp_type > 4)
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset needs projector types 1 to 4");
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
@@ -642,8 +705,8 @@ int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
     if (!image || !y_subset || !sens || !du || !work_meas || !work_img)
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osl_subset");
     if (h->desc.modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
-    if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
-        return set_error(OMB_ERR_UNSUPPORTED, "omb_osl_subset needs projector types 1 or 4");
+    if (h->desc.fp_type < 1 || h->desc.fp_type > 4 || h->desc.bp_type < 1 || h->desc.bp_type > 4)
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_osl_subset needs projector types 1 to 4");
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
@@ -675,8 +738,8 @@ int relaxed_subset(omb_handle *h, int32_t subset, bool ramla, float *image, cons
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to a relaxed sub-iteration");
     if (h->desc.modality == OMB_CT_PANEL)
         return set_error(OMB_ERR_UNSUPPORTED, "the relaxed sub-iterations are PET-only");
-    if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
-        return set_error(OMB_ERR_UNSUPPORTED, "the relaxed sub-iterations need projector types 1 or 4");
+    if (h->desc.fp_type < 1 || h->desc.fp_type > 4 || h->desc.bp_type < 1 || h->desc.bp_type > 4)
+        return set_error(OMB_ERR_UNSUPPORTED, "the relaxed sub-iterations need projector types 1 to 4");
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;
@@ -729,8 +792,8 @@ int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, floa
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_osem_subset_frames");
     if (n_frames < 0) return set_error(OMB_ERR_INVALID, "n_frames must be >= 0");
     if (h->desc.modality == OMB_CT_PANEL) return set_error(OMB_ERR_UNSUPPORTED, "OSEM sub-iteration is PET-only");
-    if ((h->desc.fp_type != 1 && h->desc.fp_type != 4) || (h->desc.bp_type != 1 && h->desc.bp_type != 4))
-        return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset_frames needs projector types 1 or 4");
+    if (h->desc.fp_type < 1 || h->desc.fp_type > 4 || h->desc.bp_type < 1 || h->desc.bp_type > 4)
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_osem_subset_frames needs projector types 1 to 4");
     RaySet rs{};
     int st = ray_set(h, subset, rs);
     if (st != OMB_OK) return st;

@@ -61,6 +61,16 @@ struct RaySet {
     const float *mu;    // PET: attenuation image (1/mm), or NULL
 };
 
+// Projector types 2 / 3: the tube of response.
+struct Orth {
+    int type;            // 2 orthogonal distance, 3 volume of intersection
+    float width;         // type 2: tube width (FWHM-like, mm); type 3: tube radius (mm)
+    int xy, z;           // tube spread transaxially / axially
+    float bmin, bmax, vmax;
+    const float *v;      // type 3: intersection volume per 1/1000 mm of distance above bmin
+    int nv;
+};
+
 // One reconstruction of a batch projected by one persistent launch: its
 // grid, its rays and where its image and measurements start in the batch's
 // concatenated buffers.

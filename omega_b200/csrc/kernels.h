@@ -47,6 +47,12 @@ int relaxed_subset(omb_handle *h, int32_t subset, bool ramla, float *image, cons
                    const float *sens, Relax lam, bool positivity, float *work_meas, float *work_img,
                    cudaStream_t st);
 
+// Projector types 2 / 3 (PET), one frame.
+int orth_forward(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof, float gf, const float *img, float *y,
+                 cudaStream_t st);
+int orth_backward(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof, float gf, const float *y, float *img,
+                  float *sens, cudaStream_t st);
+
 // Multi-ray PET projections (rs.nr_xy x rs.nr_z rays per LOR), one frame.
 int multiray_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *img, float *y,
                      int per_sm, cudaStream_t st);

@@ -154,6 +154,13 @@ class projectorClass:
     projector_type = 11
     n_rays_transaxial = 1
     n_rays_axial = 1
+    # Projector types 2 / 3 (proj.py:195, 256-257, 369): the orthogonal
+    # tracer's width (tube_width_z; tube_width_xy > 0 spreads it in the slice)
+    # and the volume tracer's tube / voxel radii
+    tube_width_xy = 0.
+    tube_width_z = 0.
+    tube_radius = 1.
+    voxel_radius = 1.
     dL = 0
     # forward-projection image reads: 'fp32' (default) or 'bf16' (types 1 and
     # 4; FP32 accumulation), with BF16 copies reserved for maxFramesBF16 images
@@ -361,6 +368,17 @@ class projectorClass:
         self.z_center = np.array(self.bz[0].item(), ndmin=1).astype(np.float32)
         if self.projector_type in (4, 5, 14, 41, 15, 45, 54, 51, 42, 43, 24, 34):
             geo.projector_scaling(self)
+        # tube spread of types 2 / 3 (proj.py:1041-1055) and the type-3 table (proj.py:990)
+        if self.projector_type in (3, 33, 13, 31, 32, 23, 43, 34):
+            self.orthTransaxial = self.orthAxial = True
+        elif self.projector_type in (2, 22, 12, 21, 24, 42):
+            self.orthTransaxial = self.tube_width_xy > 0 or self.SPECT
+            self.orthAxial = self.tube_width_z > 0 or self.SPECT
+        if self.projector_type in (3, 33, 13, 31, 34, 43):
+            from .orth import voxel_volumes
+            voxel_volumes(self)
+        else:
+            self.V = np.zeros(1, dtype=np.float32)
         self.PSFKernel()
         if self.nMeas.size == 1:
             self.nMeas = np.insert(self.nMeas, 0, 0)
@@ -593,9 +611,11 @@ class projectorClass:
     def _fp_bp_types(self):
         pt = self.projector_type
         fp = {1: 1, 11: 1, 14: 1, 15: 1, 12: 1, 13: 1, 4: 4, 41: 4, 42: 4, 43: 4, 44: 4, 45: 4,
-              5: 5, 51: 5, 52: 5, 53: 5, 54: 5, 55: 5}.get(pt)
+              5: 5, 51: 5, 52: 5, 53: 5, 54: 5, 55: 5,
+              2: 2, 22: 2, 21: 2, 24: 2, 3: 3, 33: 3, 31: 3, 34: 3}.get(pt)
         bp = {1: 1, 11: 1, 21: 1, 31: 1, 41: 1, 51: 1, 4: 4, 14: 4, 24: 4, 34: 4, 44: 4, 54: 4,
-              5: 5, 15: 5, 25: 5, 35: 5, 45: 5, 55: 5}.get(pt)
+              5: 5, 15: 5, 25: 5, 35: 5, 45: 5, 55: 5,
+              2: 2, 22: 2, 12: 2, 42: 2, 3: 3, 33: 3, 13: 3, 43: 3}.get(pt)
         if fp is None or bp is None:
             raise ValueError(f'Projector type {pt} is not supported by this build')
         return fp, bp
@@ -652,6 +672,16 @@ class projectorClass:
         if not self.CT:
             d.n_rays_xy = int(self.n_rays_transaxial)
             d.n_rays_z = int(self.n_rays_axial)
+        if 2 in (fpt, bpt) or 3 in (fpt, bpt):
+            d.tube_width = float(self.tube_width_z)
+            d.tube_radius = float(self.tube_radius)
+            d.orth_xy = 1 if self.orthTransaxial else 0
+            d.orth_z = 1 if self.orthAxial else 0
+            if 3 in (fpt, bpt):
+                keep['vol'] = np.ascontiguousarray(np.asarray(self.V, dtype=np.float32).ravel())
+                d.vol_v = _native.f32_ptr(keep['vol'])
+                d.n_vol_v = keep['vol'].size
+                d.vol_bmin, d.vol_bmax, d.vol_vmax = float(self.bmin), float(self.bmax), float(self.Vmax)
         if self.listmode and self.useIndexBasedReconstruction:
             keep['tr'] = np.ascontiguousarray(np.asarray(self.trIndex, dtype=np.uint16).ravel())
             keep['ax'] = np.ascontiguousarray(np.asarray(self.axIndex, dtype=np.uint16).ravel())

@@ -61,6 +61,11 @@ class OracleGeom(ctypes.Structure):
         ("ax", ctypes.POINTER(ctypes.c_uint16)),
         ("nr_xy", ctypes.c_int), ("nr_z", ctypes.c_int),
         ("cr_xy", ctypes.c_double), ("cr_z", ctypes.c_double),
+        ("proj_type", ctypes.c_int), ("orth_width", ctypes.c_double),
+        ("crystxy", ctypes.c_int), ("crystz", ctypes.c_int),
+        ("bmin", ctypes.c_double), ("bmax", ctypes.c_double), ("vmax", ctypes.c_double),
+        ("V", ctypes.POINTER(ctypes.c_double)), ("nv", ctypes.c_int),
+        ("cpu_mode", ctypes.c_int),
     ]
 
 
@@ -88,6 +93,8 @@ def lib():
         C = ctypes.POINTER(OracleCT)
         L.oracle_bdd_fp.argtypes = [C, P, P]
         L.oracle_bdd_bp.argtypes = [C, P, P, P]
+        L.oracle_orth_fp.argtypes = [G, P, P]
+        L.oracle_orth_bp.argtypes = [G, P, P, P]
         L.oracle_interp_fp.argtypes = [G, ctypes.c_double, P, P]
         L.oracle_interp_bp.argtypes = [G, ctypes.c_double, P, P, P]
         L.oracle_interp_ct_bp.argtypes = [C, ctypes.c_double, P, P, P]
@@ -112,6 +119,9 @@ def ref_lib():
             [u, ctypes.c_double, P, ctypes.c_double, ctypes.c_double, u, u, u, ctypes.c_double, ctypes.c_double]
         L.ref_siddon_corr_d.argtypes = [ctypes.c_int, u, u, u] + [ctypes.c_double] * 6 + [u, u, u] + [P] * 5 + \
             [u, ctypes.c_double, P, ctypes.c_double, ctypes.c_double, u, P, P, ctypes.c_int, P]
+        L.ref_orth_d.argtypes = [ctypes.c_int, u, u, u] + [ctypes.c_double] * 6 + [u, u, u] + [P] * 5 + \
+            [u, ctypes.c_double, P, ctypes.c_double, ctypes.c_double, u, ctypes.c_int, ctypes.c_double, P, P, P,
+             ctypes.c_double, ctypes.c_double, ctypes.c_double, P, P, P]
         _ref = L
     return _ref
 
@@ -155,6 +165,16 @@ class Geometry:
         # order) and attenuation image, FP64; None when off
         self.w = None
         self.mu = None
+        # projector types 2 / 3: the forward / backward type, the tube and the type-3 table
+        fb = o._fp_bp_types() if hasattr(o, '_fp_bp_types') and not self.ct else (1, 1)
+        self.fp_type, self.bp_type = fb
+        self.tube_width = float(getattr(o, 'tube_width_z', 0.0))
+        self.tube_radius = float(getattr(o, 'tube_radius', 1.0))
+        self.crystxy = int(bool(getattr(o, 'orthTransaxial', False)))
+        self.crystz = int(bool(getattr(o, 'orthAxial', False)))
+        self.V = np.ascontiguousarray(np.asarray(getattr(o, 'V', np.zeros(1)), dtype=np.float64).ravel())
+        self.vol = tuple(float(getattr(o, k, 0.0)) for k in ('bmin', 'bmax', 'Vmax'))
+        self.cpu_mode = 0
 
     @property
     def n_img(self):
@@ -213,6 +233,17 @@ class Geometry:
             U = ctypes.POINTER(ctypes.c_uint16)
             g.tr = self.tr.ctypes.data_as(U)
             g.ax = self.ax.ctypes.data_as(U)
+        g.crystxy, g.crystz = self.crystxy, self.crystz
+        g.bmin, g.bmax, g.vmax = self.vol
+        g.V = self.V.ctypes.data_as(P)
+        g.nv = self.V.size
+        g.cpu_mode = self.cpu_mode
+        return g
+
+    def orth_struct(self, subset, proj_type):
+        g = self.struct(subset)
+        g.proj_type = proj_type
+        g.orth_width = self.tube_width if proj_type == 2 else self.tube_radius
         return g
 
 
@@ -236,6 +267,27 @@ def backward(geom: Geometry, y, subset, sens=False):
     img = np.zeros(geom.n_img, dtype=np.float64)
     s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
     lib().oracle_siddon_bp(ctypes.byref(g), _dp(yy), _dp(img), _dp(s))
+    return (img, s) if sens else img
+
+
+def orth_forward(geom: Geometry, image, subset):
+    """FP64 y = A_s image with the forward projector type 2 or 3 of geom."""
+    img = np.ascontiguousarray(image, dtype=np.float64).ravel()
+    g = geom.orth_struct(subset, geom.fp_type)
+    y = np.zeros(g.m_size * geom.nbins, dtype=np.float64)
+    if lib().oracle_orth_fp(ctypes.byref(g), _dp(img), _dp(y)) != 0:
+        raise ValueError("oracle_orth_fp: projector type must be 2 or 3")
+    return y
+
+
+def orth_backward(geom: Geometry, y, subset, sens=False):
+    """FP64 A_s^T y (and A_s^T 1 when sens) with the backprojector type 2 or 3 of geom."""
+    g = geom.orth_struct(subset, geom.bp_type)
+    yy = None if y is None else np.ascontiguousarray(y, dtype=np.float64).ravel()
+    img = np.zeros(geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    if lib().oracle_orth_bp(ctypes.byref(g), _dp(yy), _dp(img), _dp(s)) != 0:
+        raise ValueError("oracle_orth_bp: projector type must be 2 or 3")
     return (img, s) if sens else img
 
 
@@ -427,6 +479,44 @@ def ref_listmode(geom: Geometry, inp, subset, fp, threads=0, sens=False):
     s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
     L.ref_listmode_d(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, e1 - e0, p(xyz), p(inp), p(out), p(s),
                      geom.global_factor, geom.epps, int(threads))
+    return (out, s) if sens else out
+
+
+def ref_orth(geom: Geometry, inp, subset, fp, proj_type, sens=False, norm=None, atten=None, threads=0):
+    """The reference CPU projector (FP64) with projector type 2 or 3 on
+    whole-sinogram subsets.  The voxel-centre arrays it indexes are padded
+    with far-away sentinels on both sides: it reads one centre past the end
+    of a slice and rows outside the grid at the ends of the tube."""
+    L = ref_lib()
+    P = ctypes.POINTER(ctypes.c_double)
+    p = (lambda a: a.ctypes.data_as(P) if a is not None else None)
+    n0, n1 = (0, geom.n_proj) if subset < 0 else (int(geom.n_meas[subset]), int(geom.n_meas[subset + 1]))
+    xy = geom.xy.astype(np.float64)
+    z = np.ascontiguousarray(geom.z.astype(np.float64)[n0 * 2:n1 * 2])
+    inp = np.ascontiguousarray(inp, dtype=np.float64).ravel()
+    nmeas = geom.n_rows * geom.n_cols * (n1 - n0)
+    out = np.zeros(nmeas * geom.nbins if fp else geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    pad = 64
+    centres = []
+    for n, b, d in zip((geom.nx, geom.ny, geom.nz), geom.b, geom.d):
+        c = np.full(n + 2 * pad, 1e12, dtype=np.float64)
+        c[pad:pad + n] = b + d * np.arange(n, dtype=np.float64) + d / 2.0
+        centres.append(c)
+    cp = [c.ctypes.data_as(P) for c in centres]
+    cp = [ctypes.cast(ctypes.addressof(q.contents) + pad * 8, P) for q in cp]
+    # the reference indexes the table up to (bmax - bmin) * 1000, past its last entry when entries
+    # were dropped; the padding repeats the last entry there, as the restatement reads it
+    V = np.concatenate([geom.V.astype(np.float64), np.full(4096, geom.V[-1], dtype=np.float64)])
+    d64 = (lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel())
+    norm, atten = d64(norm), d64(atten)
+    tofc = geom.tofc.astype(np.float64)
+    width = geom.tube_width if proj_type == 2 else geom.tube_radius
+    L.ref_orth_d(1 if fp else 0, geom.nx, geom.ny, geom.nz, *geom.d, *geom.b, geom.n_rows, geom.n_cols, n1 - n0,
+                 p(xy), p(z), p(inp), p(out), p(s), geom.nbins, geom.sigma_x, p(tofc), geom.global_factor, geom.epps,
+                 int(threads), proj_type, width, cp[0], cp[1], cp[2], geom.vol[0], geom.vol[1], geom.vol[2], p(V),
+                 p(norm), p(atten))
+    del centres
     return (out, s) if sens else out
 
 

@@ -35,6 +35,14 @@ typedef struct oracle_geom {
     /* PET multi-ray: rays per LOR and the crystal sizes they spread over */
     int nr_xy, nr_z;
     double cr_xy, cr_z;
+    /* projector types 2 / 3 (orth_oracle part of siddon_oracle.c) */
+    int proj_type;          /* 2 orthogonal distance, 3 volume of intersection */
+    double orth_width;      /* type 2: tube_width_z; type 3: tube_radius */
+    int crystxy, crystz;    /* tube spread transaxially / axially (CRYSTXY / CRYSTZ) */
+    double bmin, bmax, vmax;
+    const double *V;        /* type 3 volume table, nv entries */
+    int nv;
+    int cpu_mode;           /* nonzero: the reference CPU projector's variant (see oracle_orth_fp) */
 } oracle_geom;
 
 

@@ -109,6 +109,54 @@ int ref_siddon_corr_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, 
     return run<double>(fp, nx, ny, nz, dx, dy, dz, bx, by, bz, n_rows, n_cols, n_proj, xy, z, input, output, sens,
                        nbins, sigma_x, tof_centers, global_factor, epps, n_threads, norm, atten, ct_atten, scat);
 }
+/* Projector types 2 / 3 on sinogram data: the voxel-centre arrays are the
+ * caller's, padded on both sides with far-away sentinels (the CPU projector
+ * reads one past the end of the in-slice centres and, in its first / last
+ * slices, rows outside the grid; a sentinel centre is never inside the
+ * tube, so those reads end the scan as they would at the grid edge). */
+int ref_orth_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx, double by,
+               double bz, uint32_t n_rows, uint32_t n_cols, uint32_t n_proj, const double *xy, const double *z,
+               double *input, double *output, double *sens, uint32_t nbins, double sigma_x, double *tof_centers,
+               double global_factor, double epps, uint32_t n_threads, int proj_type, double orth_width,
+               double *x_center, double *y_center, double *z_center, double bmin, double bmax, double vmax,
+               double *V, double *norm, double *atten) {
+    paramStruct<double> p;
+    p.subsetType = 8;
+    p.subsets = 1;
+    p.currentSubset = 0;
+    p.size_x = n_rows;
+    p.size_y = n_cols;
+    p.dx = dx; p.dy = dy; p.dz = dz;
+    p.Nx = nx; p.Ny = ny; p.Nz = nz;
+    p.bx = bx; p.by = by; p.bz = bz;
+    p.projType = proj_type;
+    p.orthWidth = orth_width;
+    p.x_center = x_center;
+    p.y_center = y_center;
+    p.z_center = z_center;
+    p.bmin = bmin;
+    p.bmax = bmax;
+    p.Vmax = vmax;
+    p.V = V;
+    p.nProjections = n_proj;
+    p.globalFactor = global_factor;
+    p.epps = epps;
+    p.TOF = nbins > 1;
+    p.nBins = nbins;
+    p.sigma_x = sigma_x;
+    p.TOFCenters = tof_centers;
+    p.noSensImage = sens == nullptr;
+    p.nMeas = 0;
+    p.normalizationCorrection = norm != nullptr;
+    p.normCoefs = norm;
+    p.attenuationCorrection = atten != nullptr;
+    p.CTAttenuation = true;
+    p.atten = atten;
+    const int64_t n_meas = (int64_t)n_rows * n_cols * n_proj;
+    projectorType123Implementation4<double>(p, n_meas, output, xy, z, input, false, false, (uint8_t)(fp ? 1 : 2),
+                                            sens, nullptr, n_threads);
+    return 0;
+}
 int ref_siddon_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx, double by,
                  double bz, uint32_t n_rows, uint32_t n_cols, uint32_t n_proj, const double *xy, const double *z,
                  double *input, double *output, double *sens, uint32_t nbins, double sigma_x, double *tof_centers,

@@ -3,7 +3,8 @@
 Run in a container that holds the OMEGA sources (default /root/reference, or
 $OMEGA_REFERENCE):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # everything
+    python tests/golden/make_golden.py volumes    # the type-3 tables only
 
 For every option set in configs.py it imports the reference's own Python
 projector surface (omegatomo.projector.proj.projectorClass), runs its
@@ -136,8 +137,40 @@ def prior_weight_fixture(proj):
     print("priorw_pet_mini", {k: v.shape for k, v in out.items()})
 
 
+def volume_fixture():
+    """The reference's type-3 table (coordinates.py computeVoxelVolumes) for
+    two tube / voxel sizes, stored in vol_tables.npz."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "omega_coordinates", os.path.join(REF, "source", "Python", "omegatomo", "projector", "coordinates.py"))
+    coords = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(coords)
+
+    class Opt:
+        pass
+    out = {}
+    for tag, (R, r, d) in VOLUME_CASES.items():
+        o = Opt()
+        o.projector_type = 3
+        o.tube_radius, o.voxel_radius = R, r
+        o.dx, o.dy, o.dz = (np.array([v], dtype=np.float32) for v in d)
+        coords.computeVoxelVolumes(o)
+        out["V_" + tag] = np.asarray(o.V, dtype=np.float32)
+        out["s_" + tag] = np.array([o.bmin, o.bmax, o.Vmax, o.voxel_radius], dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "vol_tables.npz"), **out)
+    print("vol_tables", {k: v.shape for k, v in out.items()})
+
+
+# type-3 table cases: tube radius, voxel radius (before scaling), voxel size (dx, dy, dz)
+VOLUME_CASES = {"a": (1.0, 1.0, (2.0, 2.0, 2.5)), "b": (2.5, 1.0, (1.5, 1.5, 1.5))}
+
+
 def main():
+    if sys.argv[1:] == ["volumes"]:
+        volume_fixture()
+        return
     proj = reference_projector()
+    volume_fixture()
     psf_fixture(proj)
     prior_weight_fixture(proj)
     allc = dict(CONFIGS)
