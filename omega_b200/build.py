@@ -23,6 +23,12 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-Xptxas", "-O3", "-I", INCLUDE, "-I", CSRC]
+# Per-file flags.  orth.cu: no multiply-add contraction -- the tube tracer
+# takes its walk steps, and with them the TOF weights of each scanned slice,
+# from exact comparisons of crossing parameters, which tie on rays through
+# voxel corners; without contraction they round exactly as the FP64
+# restatement's do.
+FILE_FLAGS = {"orth.cu": ["-fmad=false"]}
 
 
 def _sources():
@@ -58,7 +64,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
         if not force and _mtime(obj) > max(_mtime(src), newest_header, _mtime(__file__)):
             return obj, ""
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+        cmd = [NVCC, *ARCH, *FLAGS, *FILE_FLAGS.get(os.path.basename(src), []), "-c", src, "-o", obj]
         if ptxas_info:
             cmd += ["-Xptxas", "-v"]
         r = subprocess.run(cmd, capture_output=True, text=True)
