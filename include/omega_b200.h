@@ -300,7 +300,11 @@ typedef enum omb_recon_algorithm {
                                (computeForwardProject.h:98-122, auxKernels.cl:1997-2026) */
     OMB_RECON_BSREM = 6,    /* options.BSREM: RAMLA sub-iterations, then once per iteration the MAP step
                                x -= lam * x * dU, x >= epps (iterStep.h:14-34, algorithms.h:130-135) */
-    OMB_RECON_ROSEM_MAP = 7 /* options.ROSEM_MAP: ROSEM sub-iterations, then the same MAP step */
+    OMB_RECON_ROSEM_MAP = 7,/* options.ROSEM_MAP: ROSEM sub-iterations, then the same MAP step */
+    OMB_RECON_PKMA = 8,     /* options.PKMA: x_a = max(epps, x - lam * (A^T (1 - y / fp) + dU)), x = (1 - a) x +
+                               a x_a per subset (algorithms.h:151-212, auxKernels.cl:2008-2018); dU only with a prior */
+    OMB_RECON_MRAMLA = 9,   /* options.MRAMLA: x = x + lam * A^T (y / fp - 1), clamped to [epps, U) (algorithms.h:31-52) */
+    OMB_RECON_MBSREM = 10   /* options.MBSREM: the same with dU added to the backprojection (priors.h:361-370) */
 } omb_recon_algorithm;
 
 typedef enum omb_prior {
@@ -328,8 +332,12 @@ typedef struct omb_recon_params {
                                  neighbours' -w and the centre sum(w) (libHeader.h:1147-1154) */
     int32_t prior_g[3];       /* Quad / Huber: options.Ndx, Ndy, Ndz */
     float huber_delta;        /* Huber: options.huber_delta */
-    const float *relaxation;  /* ROSEM / RAMLA / BSREM / ROSEM-MAP: host, n_iter values lam[iter]
-                                 (options.lambdaN); NULL: 1 / (iter / 20 + 1) (prepass.py:962-972) */
+    const float *relaxation;  /* ROSEM / RAMLA / BSREM / ROSEM-MAP / PKMA / MRAMLA / MBSREM: host, n_iter values
+                                 lam[iter] (options.lambdaN); NULL: 1 / (iter / 20 + 1) (prepass.py:962-972) */
+    const float *momentum;    /* PKMA: host, n_iter * n_subsets values alpha[iter * n_subsets + subset]
+                                 (options.alpha_PKMA); NULL: 1 + 0.45 k / (k + 100), k the sub-iteration count
+                                 (prepass.py:998-1006) */
+    float upper_bound;        /* MRAMLA / MBSREM: options.U; <= 0: 10000 (prepass.py:955-959) */
 } omb_recon_params;
 
 /*
@@ -367,6 +375,28 @@ int omb_rosem_subset(omb_handle *h, int32_t subset, float *image, const float *y
  */
 int omb_ramla_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda,
                      int32_t positivity, float *work_meas, float *work_img, void *stream);
+
+/*
+ * One PKMA sub-iteration (subiterStep.h:281-295, algorithms.h:151-212 with
+ * neither preconditioner nor automatic relaxation): rhs = the backprojection
+ * of 1 - y / (fp + epps [+ randoms]) (NaN / Inf -> epps) plus du (device,
+ * the prior gradient with its weight; NULL: none); x_a = x - lambda * rhs,
+ * max(epps, x_a) when `positivity`; image = (1 - alpha) image + alpha x_a.
+ */
+int omb_pkma_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda, float alpha,
+                    const float *du, int32_t positivity, float *work_meas, float *work_img, void *stream);
+
+/*
+ * One MRAMLA / MBSREM sub-iteration (subiterStep.h:123-128, 237-241,
+ * algorithms.h:31-52 without preconditioner): rhs = the backprojection of
+ * y / (fp + epps [+ randoms]) - 1 plus du (NULL: none, MRAMLA); image +
+ * lambda * rhs, max(epps, .) when `positivity`, values >= upper set to
+ * upper - epps.  Randoms, when set, must be positive: the reference treats
+ * zero-randoms bins with a separate bound (epsilon_mramla) not built here.
+ */
+int omb_mbsrem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda,
+                      float upper, const float *du, int32_t positivity, float *work_meas, float *work_img,
+                      void *stream);
 
 /*
  * The MAP step of BSREM and ROSEM-MAP after each iteration (algorithms.h:

@@ -105,6 +105,8 @@ class ReconParams(ctypes.Structure):
         ("prior_g", ctypes.c_int32 * 3),
         ("huber_delta", ctypes.c_float),
         ("relaxation", ctypes.c_void_p),
+        ("momentum", ctypes.c_void_p),
+        ("upper_bound", ctypes.c_float),
     ]
 
 
@@ -115,6 +117,9 @@ OMB_RECON_ROSEM = 4
 OMB_RECON_RAMLA = 5
 OMB_RECON_BSREM = 6
 OMB_RECON_ROSEM_MAP = 7
+OMB_RECON_PKMA = 8
+OMB_RECON_MRAMLA = 9
+OMB_RECON_MBSREM = 10
 OMB_PRIOR_RDP = 1
 OMB_PRIOR_QUAD = 2
 OMB_PRIOR_HUBER = 3
@@ -192,6 +197,12 @@ EXPORTS = [
     ("omb_ramla_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_float, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_void_p]),
+    ("omb_pkma_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int32,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_mbsrem_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int32,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_void_p]),
     ("omb_psf_convolve", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,

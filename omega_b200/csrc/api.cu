@@ -730,11 +730,10 @@ int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
 }  // extern "C"
 
 namespace omb {
-int relaxed_subset(omb_handle *h, int32_t subset, bool ramla, float *image, const float *y_subset,
-                   const float *sens, Relax lam, bool positivity, float *work_meas, float *work_img,
-                   cudaStream_t s) {
+int relaxed_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const RelaxedArgs &a,
+                   float *work_meas, float *work_img, cudaStream_t s) {
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
-    if (!image || !y_subset || (!ramla && !sens) || !work_meas || !work_img)
+    if (!image || !y_subset || (a.kind == kRosem && !a.sens) || !work_meas || !work_img)
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to a relaxed sub-iteration");
     if (h->desc.modality == OMB_CT_PANEL)
         return set_error(OMB_ERR_UNSUPPORTED, "the relaxed sub-iterations are PET-only");
@@ -747,14 +746,23 @@ int relaxed_subset(omb_handle *h, int32_t subset, bool ramla, float *image, cons
     const int64_t m = rs.m_size * h->desc.tof_bins;
     st = rays_forward(h, rs, one_frame_fp(h, image, work_meas, rs.m_size), s);
     if (st != OMB_OK) return st;
+    // ROSEM: y / fp; RAMLA, BSREM, MRAMLA, MBSREM: y / fp - 1; PKMA: 1 - y / fp
+    // (computeForwardProject.h:76-101, 98-122, 126-150, 153-180)
+    const float shift = a.kind == kRosem ? 0.f : 1.f;
+    const float sign = a.kind == kPkma ? -1.f : 1.f;
     st = ratio_shift(y_subset, work_meas, m, h->d_rand ? h->d_rand + subset_ray0(h, rs, subset) : nullptr,
-                     rs.m_size, eps, ramla ? 1.f : 0.f, s);
+                     rs.m_size, eps, shift, sign, s);
     if (st != OMB_OK) return st;
     OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
     st = rays_backward(h, rs, one_frame_bp(h, work_meas, work_img, rs.m_size), nullptr, s);
     if (st != OMB_OK) return st;
-    return ramla ? bsrem_update(image, work_img, h->n_img, lam, eps, positivity, s)
-                 : rosem_update(image, sens, work_img, h->n_img, lam, s);
+    switch (a.kind) {
+        case kRosem: return rosem_update(image, a.sens, work_img, h->n_img, a.lam, s);
+        case kRamla: return bsrem_update(image, work_img, h->n_img, a.lam, eps, a.positivity, s);
+        case kPkma: return pkma_update(image, work_img, a.du, h->n_img, a.lam, a.alpha, eps, a.positivity, s);
+        case kMbsrem: return mbsrem_update(image, work_img, a.du, h->n_img, a.lam, eps, a.upper, a.positivity, s);
+        default: return set_error(OMB_ERR_INVALID, "unknown relaxed update");
+    }
 }
 }  // namespace omb
 
@@ -762,18 +770,44 @@ extern "C" {
 
 int omb_rosem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
                      float lambda, float *work_meas, float *work_img, void *stream) {
-    Relax lam;
-    lam.v = lambda;
-    return relaxed_subset(h, subset, false, image, y_subset, sens, lam, false, work_meas, work_img,
-                          (cudaStream_t)stream);
+    RelaxedArgs a;
+    a.kind = kRosem;
+    a.sens = sens;
+    a.lam.v = lambda;
+    return relaxed_subset(h, subset, image, y_subset, a, work_meas, work_img, (cudaStream_t)stream);
 }
 
 int omb_ramla_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda,
                      int32_t positivity, float *work_meas, float *work_img, void *stream) {
-    Relax lam;
-    lam.v = lambda;
-    return relaxed_subset(h, subset, true, image, y_subset, nullptr, lam, positivity != 0, work_meas, work_img,
-                          (cudaStream_t)stream);
+    RelaxedArgs a;
+    a.kind = kRamla;
+    a.lam.v = lambda;
+    a.positivity = positivity != 0;
+    return relaxed_subset(h, subset, image, y_subset, a, work_meas, work_img, (cudaStream_t)stream);
+}
+
+int omb_pkma_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda, float alpha,
+                    const float *du, int32_t positivity, float *work_meas, float *work_img, void *stream) {
+    RelaxedArgs a;
+    a.kind = kPkma;
+    a.du = du;
+    a.lam.v = lambda;
+    a.alpha.v = alpha;
+    a.positivity = positivity != 0;
+    return relaxed_subset(h, subset, image, y_subset, a, work_meas, work_img, (cudaStream_t)stream);
+}
+
+int omb_mbsrem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda,
+                      float upper, const float *du, int32_t positivity, float *work_meas, float *work_img,
+                      void *stream) {
+    if (!(upper > 0.f)) return set_error(OMB_ERR_INVALID, "the upper bound U must be positive");
+    RelaxedArgs a;
+    a.kind = kMbsrem;
+    a.du = du;
+    a.lam.v = lambda;
+    a.upper = upper;
+    a.positivity = positivity != 0;
+    return relaxed_subset(h, subset, image, y_subset, a, work_meas, work_img, (cudaStream_t)stream);
 }
 
 int omb_map_step(float *image, const float *du, int64_t n, float lambda, float epps, void *stream) {

@@ -102,14 +102,45 @@ __device__ __forceinline__ float relax_value(const float *lam, const int *iter, 
 }
 
 __global__ void k_ratio_shift(const float *__restrict__ y, float *__restrict__ fp, int64_t n,
-                              const float *__restrict__ rnd, int64_t n_rays, float epps, float shift) {
+                              const float *__restrict__ rnd, int64_t n_rays, float epps, float shift, float sign) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         float d = fp[i] + epps;
         if (rnd) d += __ldg(rnd + i % n_rays);
-        float r = __ldg(y + i) / d - shift;
+        float r = sign * (__ldg(y + i) / d - shift);
         if (isnan(r) || isinf(r)) r = epps;
         fp[i] = r;
+    }
+}
+
+// PoissonUpdate, PKMA and MBSREM forms (auxKernels.cl:2008-2022)
+__global__ void k_pkma_update(float *__restrict__ img, const float *__restrict__ rhs, const float *__restrict__ du,
+                              int64_t n, const float *__restrict__ lam_s, const int *__restrict__ it, float lam_v,
+                              const float *__restrict__ al_s, int n_sub, int sub, float al_v, float epps,
+                              int positivity) {
+    const float lam = relax_value(lam_s, it, lam_v);
+    const float a = al_s ? al_s[*it * n_sub + sub] : al_v;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float x = img[i];
+        const float g = du ? __ldg(rhs + i) + __ldg(du + i) : __ldg(rhs + i);
+        float v = x - lam * g;
+        if (positivity) v = fmaxf(epps, v);
+        img[i] = (1.f - a) * x + a * v;
+    }
+}
+
+__global__ void k_mbsrem_update(float *__restrict__ img, const float *__restrict__ rhs, const float *__restrict__ du,
+                                int64_t n, const float *__restrict__ lam_s, const int *__restrict__ it, float lam_v,
+                                float epps, float upper, int positivity) {
+    const float lam = relax_value(lam_s, it, lam_v);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float g = du ? __ldg(rhs + i) + __ldg(du + i) : __ldg(rhs + i);
+        float v = img[i] + lam * g;
+        if (positivity) v = fmaxf(epps, v);
+        if (v >= upper) v = upper - epps;
+        img[i] = v;
     }
 }
 
@@ -150,10 +181,10 @@ __global__ void k_map_step(float *__restrict__ img, const float *__restrict__ du
 __global__ void k_relax_advance(int *it) { *it += 1; }
 
 int ratio_shift(const float *y, float *fp, int64_t n, const float *rnd, int64_t n_rays, float epps, float shift,
-                cudaStream_t st) {
+                float sign, cudaStream_t st) {
     if (n <= 0) return OMB_OK;
     if (rnd && n_rays <= 0) return set_error(OMB_ERR_INVALID, "randoms need n_rays > 0");
-    k_ratio_shift<<<grid_for(n, 4), kBlock, 0, st>>>(y, fp, n, rnd, n_rays, epps, shift);
+    k_ratio_shift<<<grid_for(n, 4), kBlock, 0, st>>>(y, fp, n, rnd, n_rays, epps, shift, sign);
     OMB_LAUNCH_CHECK("ratio launch");
     return OMB_OK;
 }
@@ -169,6 +200,24 @@ int bsrem_update(float *img, const float *rhs, int64_t n, Relax lam, float epps,
     if (n <= 0) return OMB_OK;
     k_bsrem_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, rhs, n, lam.lam, lam.iter, lam.v, epps, positivity ? 1 : 0);
     OMB_LAUNCH_CHECK("BSREM update launch");
+    return OMB_OK;
+}
+
+int pkma_update(float *img, const float *rhs, const float *du, int64_t n, Relax lam, Momentum a, float epps,
+                bool positivity, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_pkma_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, rhs, du, n, lam.lam, lam.iter, lam.v, a.alpha, a.n_subsets,
+                                                     a.subset, a.v, epps, positivity ? 1 : 0);
+    OMB_LAUNCH_CHECK("PKMA update launch");
+    return OMB_OK;
+}
+
+int mbsrem_update(float *img, const float *rhs, const float *du, int64_t n, Relax lam, float epps, float upper,
+                  bool positivity, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_mbsrem_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, rhs, du, n, lam.lam, lam.iter, lam.v, epps, upper,
+                                                       positivity ? 1 : 0);
+    OMB_LAUNCH_CHECK("MBSREM update launch");
     return OMB_OK;
 }
 

@@ -31,21 +31,45 @@ struct Relax {
     const int *iter = nullptr;
     float v = 1.f;
 };
-// fp = y / ((fp + epps) [+ r]) - shift, NaN / Inf -> epps; r (nullable) per ray, shared by TOF bins
+// PKMA momentum of one sub-iteration: alpha[*iter * n_subsets + subset] from
+// a device schedule, else the host value v.
+struct Momentum {
+    const float *alpha = nullptr;
+    const int *iter = nullptr;
+    int n_subsets = 1;
+    int subset = 0;
+    float v = 1.f;
+};
+// fp = sign * (y / ((fp + epps) [+ r]) - shift), NaN / Inf -> epps; r (nullable) per ray, shared by TOF bins
 int ratio_shift(const float *y, float *fp, int64_t n, const float *rnd, int64_t n_rays, float epps, float shift,
-                cudaStream_t st);
+                float sign, cudaStream_t st);
 // ROSEM: x = x + lam * x / sens * (rhs - sens)
 int rosem_update(float *img, const float *sens, const float *rhs, int64_t n, Relax lam, cudaStream_t st);
 // RAMLA / BSREM: x = x + lam * rhs * x, then max(epps, x) when positivity
 int bsrem_update(float *img, const float *rhs, int64_t n, Relax lam, float epps, bool positivity, cudaStream_t st);
+// PKMA: g = rhs [+ du]; xa = x - lam * g, max(epps, xa) when positivity; x = (1 - a) x + a xa
+int pkma_update(float *img, const float *rhs, const float *du, int64_t n, Relax lam, Momentum a, float epps,
+                bool positivity, cudaStream_t st);
+// MRAMLA / MBSREM: x = x + lam * (rhs [+ du]), max(epps, x) when positivity, x >= U -> U - epps
+int mbsrem_update(float *img, const float *rhs, const float *du, int64_t n, Relax lam, float epps, float upper,
+                  bool positivity, cudaStream_t st);
 // MAP step: x = x - lam * x * du, then max(epps, x)
 int map_step(float *img, const float *du, int64_t n, Relax lam, float epps, cudaStream_t st);
 // ++*iter on the stream
 int relax_advance(int *iter, cudaStream_t st);
-// One ROSEM (ramla = false) or RAMLA / BSREM (ramla = true) sub-iteration of a handle.
-int relaxed_subset(omb_handle *h, int32_t subset, bool ramla, float *image, const float *y_subset,
-                   const float *sens, Relax lam, bool positivity, float *work_meas, float *work_img,
-                   cudaStream_t st);
+// The relaxed sub-iterations of a handle.
+enum RelaxedKind { kRosem = 0, kRamla = 1, kPkma = 2, kMbsrem = 3 };
+struct RelaxedArgs {
+    int kind = kRosem;
+    const float *sens = nullptr;   // ROSEM
+    const float *du = nullptr;     // PKMA / MBSREM: prior gradient (weight included) added to the gradient, or NULL
+    Relax lam;
+    Momentum alpha;                // PKMA
+    float upper = 10000.f;         // MRAMLA / MBSREM: U
+    bool positivity = true;
+};
+int relaxed_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const RelaxedArgs &a,
+                   float *work_meas, float *work_img, cudaStream_t st);
 
 // Projector types 2 / 3 (PET), one frame.
 int orth_forward(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof, float gf, const float *img, float *y,

@@ -1,7 +1,8 @@
 // The built-in reconstruction loop behind one call (the reference's compiled
 // omegaMain entry, libHeader.h:1466, reconstructionAF.h:1053-1500, for the
 // algorithms of this path): OSEM, OSL-OSEM, the relaxed ROSEM / RAMLA / BSREM /
-// ROSEM-MAP for PET data, and PDHG with the smoothed TV gradient, with every
+// ROSEM-MAP / PKMA / MRAMLA / MBSREM for PET data, and PDHG with the smoothed
+// TV gradient, with every
 // sub-iteration issued on the caller's stream by the
 // same entry points a custom loop uses, and (use_graph) one iteration captured
 // as a CUDA graph and replayed.
@@ -79,15 +80,20 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
     const bool graph = p->use_graph != 0;
     int st = OMB_OK;
     const int alg = p->algorithm;
-    if (alg == OMB_RECON_OSEM || alg == OMB_RECON_OSL_OSEM || alg == OMB_RECON_ROSEM || alg == OMB_RECON_RAMLA ||
-        alg == OMB_RECON_BSREM || alg == OMB_RECON_ROSEM_MAP) {
+    if (alg >= OMB_RECON_OSEM && alg <= OMB_RECON_MBSREM && alg != OMB_RECON_PDHG_TV) {
         const bool osl = alg == OMB_RECON_OSL_OSEM;
         const bool map = alg == OMB_RECON_BSREM || alg == OMB_RECON_ROSEM_MAP;  // MAP step once per iteration
+        const bool pkma = alg == OMB_RECON_PKMA;
+        const bool mb = alg == OMB_RECON_MRAMLA || alg == OMB_RECON_MBSREM;
         const bool ramla = alg == OMB_RECON_RAMLA || alg == OMB_RECON_BSREM;    // no sensitivity image
         const bool relaxed = alg >= OMB_RECON_ROSEM;
-        if ((osl || map) && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_HUBER))
+        // the prior's gradient at every sub-iteration's image, added to the gradient (priors.h:361-370)
+        const bool sub_prior = alg == OMB_RECON_MBSREM || (pkma && p->prior != 0);
+        const bool need_prior = osl || map || sub_prior;
+        const bool no_sens = ramla || pkma || mb;
+        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_HUBER))
             return set_error(OMB_ERR_INVALID, "unknown prior");
-        if ((osl || map) && p->prior != OMB_PRIOR_RDP && !p->prior_window)
+        if (need_prior && p->prior != OMB_PRIOR_RDP && !p->prior_window)
             return set_error(OMB_ERR_INVALID, "the quadratic / Huber prior needs its window");
         const Grid g = handle_grid(h);
         const float epps = handle_epps(h);
@@ -100,17 +106,22 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             m_max = ms > m_max ? ms : m_max;
         }
         DevBuf sens, wm, wi, du, lam;
-        if (!ramla && (st = alloc(sens, (size_t)n_subsets * n * sizeof(float), s)) != OMB_OK) return st;
-        if ((osl || map) && (st = alloc(du, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        if (!no_sens && (st = alloc(sens, (size_t)n_subsets * n * sizeof(float), s)) != OMB_OK) return st;
+        if (need_prior && (st = alloc(du, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(wm, (size_t)m_max * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(wi, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         Relax rl;
+        Momentum mo;
         if (relaxed && p->n_iter > 0) {
-            // lam[iter] in device memory with the iteration counter behind it, so that a replayed
-            // iteration reads the next value (libHeader.h:1331-1333; default prepass.py:962-972)
-            std::vector<float> host((size_t)p->n_iter + 1, 0.f);
+            // lam[iter] (and PKMA's alpha[iter * S + subset]) in device memory with the iteration
+            // counter behind them, so that a replayed iteration reads the next values
+            // (libHeader.h:1331-1343; defaults prepass.py:962-972, 998-1006)
+            const size_t nl = (size_t)p->n_iter, na = pkma ? (size_t)p->n_iter * n_subsets : 0;
+            std::vector<float> host(nl + na + 1, 0.f);
             for (int i = 0; i < p->n_iter; ++i)
                 host[i] = p->relaxation ? p->relaxation[i] : (float)(1.0 / (i / 20.0 + 1.0));
+            for (size_t k = 0; k < na; ++k)
+                host[nl + k] = p->momentum ? p->momentum[k] : (float)(1.0 + (0.45 * (double)k) / ((double)k + 100.0));
             if ((st = alloc(lam, host.size() * sizeof(float) + 16, s)) != OMB_OK) return st;
             int *counter = reinterpret_cast<int *>(lam.f() + host.size());
             OMB_CUDA_TRY(cudaMemcpyAsync(lam.p, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s));
@@ -119,8 +130,14 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             OMB_CUDA_TRY(cudaStreamSynchronize(s));
             rl.lam = lam.f();
             rl.iter = counter;
+            if (pkma) {
+                mo.alpha = lam.f() + nl;
+                mo.iter = counter;
+                mo.n_subsets = n_subsets;
+            }
         }
-        for (int s_ = 0; s_ < n_subsets && !ramla && st == OMB_OK; ++s_)
+        const float upper = p->upper_bound > 0.f ? p->upper_bound : 10000.f;
+        for (int s_ = 0; s_ < n_subsets && !no_sens && st == OMB_OK; ++s_)
             st = omb_sensitivity(h, s_, sens.f() + s_ * n, stream);
         if (st != OMB_OK) return st;
         // dU = beta * the prior's gradient at x_out
@@ -139,14 +156,25 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         st = repeat(p->n_iter, graph, s, [&]() {
             int e = OMB_OK;
             for (int s_ = 0; s_ < n_subsets && e == OMB_OK; ++s_) {
-                float *ss = ramla ? nullptr : sens.f() + s_ * n;
+                float *ss = no_sens ? nullptr : sens.f() + s_ * n;
                 if (osl) {
                     // dU of the current image, then the one-step-late update
                     e = prior_grad();
                     if (e == OMB_OK) e = omb_osl_subset(h, s_, x_out, y + off[s_], ss, du.f(), wm.f(), wi.f(), stream);
                 } else if (relaxed) {
-                    e = relaxed_subset(h, s_, ramla, x_out, y + off[s_], ss, rl, p->positivity != 0, wm.f(), wi.f(),
-                                       s);
+                    RelaxedArgs ra;
+                    ra.kind = pkma ? kPkma : (mb ? kMbsrem : (ramla ? kRamla : kRosem));
+                    ra.sens = ss;
+                    ra.lam = rl;
+                    ra.alpha = mo;
+                    ra.alpha.subset = s_;
+                    ra.upper = upper;
+                    ra.positivity = p->positivity != 0;
+                    if (sub_prior) {
+                        e = prior_grad();
+                        ra.du = du.f();
+                    }
+                    if (e == OMB_OK) e = relaxed_subset(h, s_, x_out, y + off[s_], ra, wm.f(), wi.f(), s);
                 } else {
                     e = omb_osem_subset(h, s_, x_out, y + off[s_], ss, wm.f(), wi.f(), stream);
                 }

@@ -29,12 +29,16 @@ def sphere_cylinder_volume(R, r, b):
     A = np.maximum(r * r, (b + R) ** 2)
     B = np.minimum(r * r, (b + R) ** 2)
     C = (b - R) ** 2
-    k = np.abs((B - C) / (A - C))
-    alpha = (B - C) / C
+    # b = R gives C = 0: an infinite alpha and a NaN volume there, which the
+    # table drops as the reference's does
+    with np.errstate(divide='ignore', invalid='ignore'):
+        k = np.abs((B - C) / (A - C))
+        alpha = (B - C) / C
     s = (b + R) * (b - R)
-    third = np.array([quad(lambda x, a=a, m=m: 1.0 / ((1.0 + a * x * x) * math.sqrt(1.0 - x * x) *
-                                                      math.sqrt(1.0 - m * x * x)), 0.0, 1.0)[0]
-                      for a, m in zip(alpha, k)], dtype=np.float64)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        third = np.array([quad(lambda x, a=a, m=m: 1.0 / ((1.0 + a * x * x) * math.sqrt(1.0 - x * x) *
+                                                          math.sqrt(1.0 - m * x * x)), 0.0, 1.0)[0]
+                          for a, m in zip(alpha, k)], dtype=np.float64)
     K = ellipk(k)
     E = ellipe(k)
     # Heaviside step of R - b with H(0) = 1/2

@@ -124,7 +124,14 @@ class projectorClass:
     RAMLA = False
     BSREM = False
     ROSEM_MAP = False
+    PKMA = False
+    MRAMLA = False
+    MBSREM = False
     lambdaN = np.empty(0, dtype=np.float32)
+    alpha_PKMA = np.empty(0, dtype=np.float32)
+    rho_PKMA = .45
+    delta_PKMA = 100.
+    U = 0.
     PDHG = False
     TV = False
     RDP = False

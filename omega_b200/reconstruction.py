@@ -229,8 +229,11 @@ class OSEMBatch:
 
 _PET_METHODS = {'OSEM': _native.OMB_RECON_OSEM, 'OSL_OSEM': _native.OMB_RECON_OSL_OSEM,
                 'ROSEM': _native.OMB_RECON_ROSEM, 'RAMLA': _native.OMB_RECON_RAMLA,
-                'BSREM': _native.OMB_RECON_BSREM, 'ROSEM_MAP': _native.OMB_RECON_ROSEM_MAP}
-_PRIOR_METHODS = ('OSL_OSEM', 'BSREM', 'ROSEM_MAP')
+                'BSREM': _native.OMB_RECON_BSREM, 'ROSEM_MAP': _native.OMB_RECON_ROSEM_MAP,
+                'PKMA': _native.OMB_RECON_PKMA, 'MRAMLA': _native.OMB_RECON_MRAMLA,
+                'MBSREM': _native.OMB_RECON_MBSREM}
+_PRIOR_METHODS = ('OSL_OSEM', 'BSREM', 'ROSEM_MAP', 'MBSREM')
+_RELAXED = ('ROSEM', 'RAMLA', 'BSREM', 'ROSEM_MAP', 'PKMA', 'MRAMLA', 'MBSREM')
 
 
 def relaxation(options):
@@ -255,13 +258,36 @@ def relaxation(options):
     return np.ascontiguousarray(lam[:n], dtype=np.float32)
 
 
+def momentum(options):
+    """PKMA momentum alpha[iter * subsets + subset] as the reference's prepass
+    sets it (prepass.py:998-1009): options.alpha_PKMA when it holds at least
+    Niter * subsets values and is not all zero, else
+    1 + rho_PKMA k / (k + delta_PKMA) over the sub-iteration count k; float32."""
+    n = int(options.Niter) * int(options.subsets)
+    a = np.asarray(getattr(options, 'alpha_PKMA', np.empty(0)), dtype=np.float32).ravel()
+    if a.size < n or float(np.sum(a)) == 0.:
+        if a.size < n:
+            print('Warning: The number of PKMA alpha (momentum) values must be at least the number of iterations '
+                  'times the number of subsets! Computing custom alpha values.')
+        k = np.arange(n, dtype=np.float64)
+        rho, delta = float(getattr(options, 'rho_PKMA', .45)), float(getattr(options, 'delta_PKMA', 100.))
+        a = (1. + (rho * k) / (k + delta)).astype(np.float32)
+    elif a.size > n:
+        print('Warning: The number of PKMA alpha (momentum) values is higher than the total number of iterations '
+              'times subsets. The final values will be ignored.')
+    options.alpha_PKMA = a
+    return np.ascontiguousarray(a[:n], dtype=np.float32)
+
+
 def reconstructions_main(options):
     """The built-in reconstruction (omegatomo/reconstruction/recomain.py:427-725,
     the compiled omegaMain entry) for the algorithms of this path:
-    options.OSEM, options.ROSEM and options.RAMLA (PET), options.OSL_OSEM,
-    options.BSREM and options.ROSEM_MAP with options.RDP, options.Quad or
-    options.Huber (PET, MAP; Ndx/Ndy/Ndz neighbourhood weights as the
-    reference forms them; relaxation options.lambdaN) or options.PDHG with
+    options.OSEM, options.ROSEM, options.RAMLA, options.MRAMLA and options.PKMA
+    (PET; PKMA takes a prior when one is set), options.OSL_OSEM,
+    options.BSREM, options.ROSEM_MAP and options.MBSREM with options.RDP,
+    options.Quad or options.Huber (PET, MAP; Ndx/Ndy/Ndz neighbourhood weights
+    as the reference forms them; relaxation options.lambdaN, PKMA momentum
+    options.alpha_PKMA, MRAMLA / MBSREM bound options.U) or options.PDHG with
     options.TV, options.Niter iterations from options.x0, run natively by
     omb_reconstruct.  CT data are linearised as log(flat / SinM) first
     (prepass.py:22-36; flat = max(SinM) when options.flat <= 0), negative PET
@@ -279,9 +305,14 @@ def reconstructions_main(options):
         raise ValueError('Select one reconstruction method (' + ', '.join(list(_PET_METHODS) + ['PDHG']) + ')')
     method = chosen[0]
     quad, huber = bool(getattr(options, 'Quad', False)), bool(getattr(options, 'Huber', False))
-    prior = method in _PRIOR_METHODS
-    if prior and int(bool(options.RDP)) + int(quad) + int(huber) != 1:
+    n_priors = int(bool(options.RDP)) + int(quad) + int(huber)
+    prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
+    if prior and n_priors != 1:
         raise ValueError(method + ' needs one prior: options.RDP, options.Quad or options.Huber')
+    if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
+            np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
+        raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
+                         'epsilon_mramla is not built)')
     if method != 'PDHG' and options.CT:
         raise ValueError(method + ' is built for PET data')
     if options.PDHG and not options.TV:
@@ -317,9 +348,16 @@ def reconstructions_main(options):
     p.rdp_gamma = float(getattr(options, 'RDP_gamma', 1.0))
     window = None
     lam = None
-    if method in ('ROSEM', 'RAMLA', 'BSREM', 'ROSEM_MAP'):
+    mom = None
+    if method in _RELAXED:
         lam = relaxation(options)
         p.relaxation = ctypes.c_void_p(lam.ctypes.data)
+    if method == 'PKMA':
+        mom = momentum(options)
+        p.momentum = ctypes.c_void_p(mom.ctypes.data)
+    if method in ('MRAMLA', 'MBSREM'):
+        u = float(getattr(options, 'U', 0.))
+        p.upper_bound = u if u > 0 else 10000.
     if prior:
         p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
                    (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))

@@ -335,42 +335,76 @@ def default_relaxation(n_iter):
     return np.array([1. / (i / 20. + 1.) for i in range(n_iter)], dtype=np.float32)
 
 
+def default_momentum(n_iter, n_subsets, rho=0.45, delta=100.0):
+    """PKMA alpha[k] = 1 + rho k / (k + delta), k the sub-iteration count, float32 (prepass.py:998-1006)."""
+    k = np.arange(n_iter * n_subsets, dtype=np.float64)
+    return (1.0 + (rho * k) / (k + delta)).astype(np.float32)
+
+
 def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None, backward=None, randoms=None,
-            prior_grad=None, positivity=True):
+            prior_grad=None, positivity=True, alpha=None, upper=10000.0):
     """Restated relaxed loops in FP64 (kind: "ROSEM", "RAMLA", "BSREM",
-    "ROSEM_MAP"); returns the image after n_iter iterations.
+    "ROSEM_MAP", "PKMA", "MRAMLA", "MBSREM"); returns the image after n_iter
+    iterations.
     ROSEM sub-iteration (algorithms.h:102-106): x + lam x / sens (rhs - sens),
     rhs the backprojection of y / (fp + epps [+ r]).
     RAMLA / BSREM (computeForwardProject.h:98-122, auxKernels.cl:1997-2026):
     x + lam rhs x, rhs the backprojection of y / (fp + epps [+ r]) - 1, then
     max(epps, x) with positivity.  BSREM / ROSEM-MAP end each iteration with
     the MAP step x - lam x dU, x < epps -> epps (iterStep.h:14-34,
-    algorithms.h:130-135); dU = prior_grad(x), weight included."""
+    algorithms.h:130-135); dU = prior_grad(x), weight included.
+    PKMA (computeForwardProject.h:126-150, algorithms.h:151-212,
+    auxKernels.cl:2008-2018): g = A^T (1 - y / (fp + epps [+ r])) [+ dU at the
+    sub-iteration's image]; xa = x - lam g, max(epps, xa) with positivity;
+    x = (1 - a) x + a xa, a = alpha[iter * S + subset].
+    MRAMLA / MBSREM (computeForwardProject.h:153-180, algorithms.h:31-52,
+    auxKernels.cl:2011-2022): x + lam (A^T (y / (fp + epps [+ r]) - 1)
+    [+ dU]), max(epps, .) with positivity, values >= U set to U - epps."""
     fwd = forward or globals()["forward"]
     bwd = backward or globals()["backward"]
     lam = np.asarray(default_relaxation(n_iter) if lam is None else lam, dtype=np.float32)
+    S = geom.n_subsets
+    if kind == "PKMA" and alpha is None:
+        alpha = default_momentum(n_iter, S)
     ramla = kind in ("RAMLA", "BSREM")
     mapstep = kind in ("BSREM", "ROSEM_MAP")
+    additive = kind in ("PKMA", "MRAMLA", "MBSREM")
     x = np.asarray(x0, dtype=np.float64).copy()
     eps = geom.epps
     sens = []
-    if not ramla:
-        for s in range(geom.n_subsets):
+    if kind in ("ROSEM", "ROSEM_MAP"):
+        for s in range(S):
             _, sv = bwd(geom, None, s, sens=True)
             sens.append(np.maximum(sv, eps))
     for it in range(n_iter):
         lm = float(lam[it])
-        for s in range(geom.n_subsets):
+        for s in range(S):
+            du = prior_grad(x) if additive and prior_grad is not None else None
             fp = fwd(geom, x, s) + eps
             if randoms is not None:
                 fp = fp + np.tile(np.asarray(randoms[s], dtype=np.float64), geom.nbins)
             with np.errstate(divide="ignore", invalid="ignore"):
                 r = np.asarray(y_subsets[s], dtype=np.float64) / fp
-            if ramla:
+            if kind == "PKMA":
+                r = 1.0 - r
+            elif ramla or kind in ("MRAMLA", "MBSREM"):
                 r = r - 1.0
             r[~np.isfinite(r)] = eps
             rhs = bwd(geom, r, s)
-            if ramla:
+            if du is not None:
+                rhs = rhs + du
+            if kind == "PKMA":
+                a = float(alpha[it * S + s])
+                xa = x - lm * rhs
+                if positivity:
+                    xa = np.maximum(eps, xa)
+                x = (1.0 - a) * x + a * xa
+            elif kind in ("MRAMLA", "MBSREM"):
+                x = x + lm * rhs
+                if positivity:
+                    x = np.maximum(eps, x)
+                x = np.where(x >= upper, upper - eps, x)
+            elif ramla:
                 x = x + lm * rhs * x
                 if positivity:
                     x = np.maximum(eps, x)

@@ -248,3 +248,126 @@ def test_relaxed_rejects_ct_and_missing_prior(cuda):
     o.BSREM, o.RAMLA, o.OSEM = False, True, True
     with pytest.raises(ValueError, match="Select one"):
         rec.reconstructions_main(o)
+
+
+def test_default_momentum_matches_prepass_rule(capsys):
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    o.Niter = 3
+    a = rec.momentum(o)
+    S = int(o.subsets)
+    want = np.zeros(3 * S, dtype=np.float32)
+    oo = 0
+    for kk in range(3):
+        for ll in range(S):
+            want[oo] = 1. + (0.45 * (kk * S + ll)) / (kk * S + ll + 100.)
+            oo += 1
+    assert np.array_equal(a, want) and np.array_equal(orc.default_momentum(3, S), want)
+    assert 'Computing custom alpha values' in capsys.readouterr().out
+    o.alpha_PKMA = np.linspace(1.0, 1.2, 3 * S + 2).astype(np.float32)
+    assert np.array_equal(rec.momentum(o), o.alpha_PKMA[:3 * S])
+    assert 'final values will be ignored' in capsys.readouterr().out
+
+
+def test_pkma_and_mramla_restatement_properties():
+    o, g = _pet("pet_mini", 31)
+    ys = _subset_measurements(o, g)
+    lam = np.array([0.3], np.float32)
+    # alpha = 1: PKMA is the projected gradient step x - lam A^T(1 - y / fp)
+    x1 = orc.relaxed(g, ys, np.ones(g.n_img), 1, "PKMA", lam=lam, alpha=np.ones(g.n_subsets, np.float32))
+    assert np.all(x1 >= g.epps)
+    # MRAMLA = PKMA at alpha = 1 with the gradient negated (before the bounds)
+    x2 = orc.relaxed(g, ys, np.ones(g.n_img), 1, "MRAMLA", lam=lam)
+    assert orc.rel_l2(x1, x2) < 1e-12
+    # the upper bound: values at or above U land at U - epps
+    x3 = orc.relaxed(g, ys, np.ones(g.n_img), 1, "MRAMLA", lam=np.array([5.0], np.float32), upper=1.5)
+    assert np.max(x3) <= 1.5 and np.any(x3 == 1.5 - g.epps)
+    # MBSREM with a zero prior is MRAMLA
+    x4 = orc.relaxed(g, ys, np.ones(g.n_img), 1, "MBSREM", lam=lam, prior_grad=lambda v: np.zeros_like(v))
+    assert np.array_equal(x4, x2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,graph", [("pet_mini", True), ("pet_mini", False), ("pet_mini_tof", True)])
+def test_builtin_pkma_matches_oracle(cuda, name, graph):
+    o, g = _pet(name, 32)
+    lam = [0.3, 0.2, 0.15]
+    x = _run_builtin(o, "PKMA", 3, lam=lam, graph=graph)
+    ref = orc.relaxed(g, _subset_measurements(o, g), np.ones(g.n_img), 3, "PKMA", lam=np.float32(lam))
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    assert np.array_equal(o.alpha_PKMA, orc.default_momentum(3, g.n_subsets))
+
+
+@pytest.mark.gpu
+def test_builtin_pkma_with_rdp_matches_oracle(cuda):
+    o, g = _pet("pet_mini", 33)
+    lam = [0.3, 0.2, 0.15]
+    x = _run_builtin(o, "PKMA", 3, lam=lam, RDP=True, RDP_gamma=2.0, beta=0.05)
+    shape = (g.nx, g.ny, g.nz)
+    ys = _subset_measurements(o, g)
+    ref = orc.relaxed(g, ys, np.ones(g.n_img), 3, "PKMA", lam=np.float32(lam),
+                      prior_grad=lambda v: io.rdp_gradient(v, shape, 2.0, 0.05, g.epps))
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    assert orc.rel_l2(ref, orc.relaxed(g, ys, np.ones(g.n_img), 3, "PKMA", lam=np.float32(lam))) > 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("upper", [0.0, 1.6])
+def test_builtin_mramla_matches_oracle(cuda, upper):
+    o, g = _pet("pet_mini", 34)
+    lam = [0.2, 0.12, 0.08]
+    o.U = upper
+    x = _run_builtin(o, "MRAMLA", 3, lam=lam)
+    ref = orc.relaxed(g, _subset_measurements(o, g), np.ones(g.n_img), 3, "MRAMLA", lam=np.float32(lam),
+                      upper=upper if upper > 0 else 10000.0)
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    if upper > 0:
+        assert np.max(x) < upper
+
+
+@pytest.mark.gpu
+def test_builtin_mbsrem_quad_matches_oracle(cuda):
+    from omega_b200 import priors
+    o, g = _pet("pet_mini", 35)
+    lam = [0.2, 0.12, 0.08]
+    x = _run_builtin(o, "MBSREM", 3, lam=lam, Quad=True, beta=0.05)
+    shape = (g.nx, g.ny, g.nz)
+    win = priors.prior_window(priors.normalised_weights(priors.neighbourhood_weights(o)), 1, 1, 1)
+
+    def grad(v):
+        return 0.05 * io.psf_convolve(v, shape, win, (1, 1, 1))
+    ys = _subset_measurements(o, g)
+    ref = orc.relaxed(g, ys, np.ones(g.n_img), 3, "MBSREM", lam=np.float32(lam), prior_grad=grad)
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    assert orc.rel_l2(ref, orc.relaxed(g, ys, np.ones(g.n_img), 3, "MRAMLA", lam=np.float32(lam))) > 1e-4
+
+
+@pytest.mark.gpu
+def test_pkma_mbsrem_entries_match_builtin(cuda):
+    import torch
+    from omega_b200 import _native
+    from omega_b200.reconstruction import _ptr, _stream
+    o, g = _pet("pet_mini", 36)
+    lam = np.array([0.3, 0.2], np.float32)
+    built = _run_builtin(o, "PKMA", 2, lam=lam)
+    alpha = orc.default_momentum(2, g.n_subsets)
+    dev = torch.device("cuda", o._device)
+    st = _stream(dev)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [torch.from_numpy(np.ascontiguousarray(o.subsetMeasurements(m, s), dtype=np.float32)).to(dev)
+          for s in range(g.n_subsets)]
+    x = torch.ones(g.n_img, device=dev)
+    wm = torch.empty(max(int(v.numel()) for v in ys), device=dev)
+    wi = torch.empty(g.n_img, device=dev)
+    for it in range(2):
+        for s in range(g.n_subsets):
+            _native.call("omb_pkma_subset", o._handle, s, _ptr(x), _ptr(ys[s]), float(lam[it]),
+                         float(alpha[it * g.n_subsets + s]), None, 1, _ptr(wm), _ptr(wi), st)
+    assert orc.rel_l2(x.cpu().numpy(), built) < 1e-6
+    o2, _ = _pet("pet_mini", 36)
+    built2 = _run_builtin(o2, "MRAMLA", 1, lam=[0.2])
+    x = torch.ones(g.n_img, device=dev)
+    for s in range(g.n_subsets):
+        _native.call("omb_mbsrem_subset", o2._handle, s, _ptr(x), _ptr(ys[s]), 0.2, 10000.0, None, 1, _ptr(wm),
+                     _ptr(wi), st)
+    assert orc.rel_l2(x.cpu().numpy(), built2) < 1e-6
