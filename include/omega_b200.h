@@ -310,7 +310,8 @@ typedef enum omb_recon_algorithm {
 typedef enum omb_prior {
     OMB_PRIOR_RDP = 1,      /* options.RDP: relative difference prior, parameter rdp_gamma */
     OMB_PRIOR_QUAD = 2,     /* options.Quad: the quadratic window (prior_window) applied with mirrored edges */
-    OMB_PRIOR_HUBER = 3     /* options.Huber: the same with the gradient clamped to +-huber_delta */
+    OMB_PRIOR_HUBER = 3,    /* options.Huber: the same with the gradient clamped to +-huber_delta */
+    OMB_PRIOR_NLM = 4       /* options.NLM (with NLTV / NLM_MRP / NLRD / NLLange / NLGGMRF): omb_nlm_gradient */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -338,6 +339,15 @@ typedef struct omb_recon_params {
                                  (options.alpha_PKMA); NULL: 1 + 0.45 k / (k + 100), k the sub-iteration count
                                  (prepass.py:998-1006) */
     float upper_bound;        /* MRAMLA / MBSREM: options.U; <= 0: 10000 (prepass.py:955-959) */
+    int32_t nlm_type;         /* OMB_PRIOR_NLM: 0 NLM, 1 NLTV, 2 NLM-MRP, 3 NLRD, 4 NL Lange, 5 MRP + Lange, 6 NLGGMRF;
+                                 the search window is prior_g (Ndx, Ndy, Ndz), gamma is rdp_gamma */
+    int32_t nlm_patch[3];     /* options.Nlx, Nly, Nlz */
+    float nlm_h;              /* options.NLMsigma^2 (libHeader.h:1285-1286) */
+    const float *nlm_gaussian;/* device: (2 Nlx + 1)(2 Nly + 1)(2 Nlz + 1) patch weights, x fastest */
+    const float *nlm_ref;     /* device reference image of the patch distances (NLM_use_anatomical), or NULL */
+    float ggmrf[3];           /* NLGGMRF: options.GGMRF_p, GGMRF_q, GGMRF_c */
+    int32_t nlm_adaptive;     /* options.NLAdaptive */
+    float nlm_adaptive_s;     /* options.NLAdaptiveConstant */
 } omb_recon_params;
 
 /*
@@ -357,6 +367,21 @@ int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const fl
  */
 int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
                    const float *du, float *work_meas, float *work_img, void *stream);
+
+/*
+ * Non-local regulariser gradient (the NLM kernel, auxKernels.cl:297-620, the
+ * image read clamped to its edges as the reference's texture sampler reads
+ * it): grad += beta * g(u), g of `type` as omb_recon_params.nlm_type lists,
+ * over search[3] (Ndx, Ndy, Ndz) offsets with (2 patch + 1)^3 patches
+ * weighted by `gaussian` (device, x fastest) and w = exp(-distance / h);
+ * `ref` (device, or NULL) supplies the patches instead of u.  ggmrf_pqc
+ * (host, 3 values) only for type 6.  adaptive != 0 (options.NLAdaptive):
+ * w = exp(-distance / (distance / patch_voxels * h + adaptive_s)).
+ */
+int omb_nlm_gradient(const float *u, const float *ref, float *grad, int32_t nx, int32_t ny, int32_t nz,
+                     const int32_t *search, const int32_t *patch, const float *gaussian, float h, float epps,
+                     float beta, int32_t type, float gamma, const float *ggmrf_pqc, int32_t adaptive,
+                     float adaptive_s, void *stream);
 
 /*
  * One relaxed OSEM (ROSEM) sub-iteration (subiterStep.h:137-145,

@@ -107,6 +107,14 @@ class ReconParams(ctypes.Structure):
         ("relaxation", ctypes.c_void_p),
         ("momentum", ctypes.c_void_p),
         ("upper_bound", ctypes.c_float),
+        ("nlm_type", ctypes.c_int32),
+        ("nlm_patch", ctypes.c_int32 * 3),
+        ("nlm_h", ctypes.c_float),
+        ("nlm_gaussian", ctypes.c_void_p),
+        ("nlm_ref", ctypes.c_void_p),
+        ("ggmrf", ctypes.c_float * 3),
+        ("nlm_adaptive", ctypes.c_int32),
+        ("nlm_adaptive_s", ctypes.c_float),
     ]
 
 
@@ -123,6 +131,7 @@ OMB_RECON_MBSREM = 10
 OMB_PRIOR_RDP = 1
 OMB_PRIOR_QUAD = 2
 OMB_PRIOR_HUBER = 3
+OMB_PRIOR_NLM = 4
 
 
 class Tuning(ctypes.Structure):
@@ -205,6 +214,12 @@ EXPORTS = [
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_void_p]),
+    ("omb_nlm_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                        ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p, ctypes.c_float,
+                                        ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_float,
+                                        ctypes.POINTER(ctypes.c_float), ctypes.c_int32, ctypes.c_float,
+                                        ctypes.c_void_p]),
     ("omb_psf_convolve", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_void_p]),

@@ -1,5 +1,5 @@
-// Image-domain steps around the projectors: the PSF blur and the relative
-// difference prior (RDP) gradient.
+// Image-domain steps around the projectors: the PSF blur, the relative
+// difference prior (RDP) gradient and the non-local (NLM family) gradients.
 //
 // PSF: Convolution3D_f (auxKernels.cl:192-245) -- a 3-D window of
 // (2gx+1)(2gy+1)(2gz+1) weights (x fastest) applied at every voxel, the
@@ -96,5 +96,137 @@ extern "C" int omb_rdp_gradient(const float *u, float *grad, int32_t nx, int32_t
     dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
     k_rdp_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, gamma, epps, beta);
     OMB_LAUNCH_CHECK("RDP gradient launch");
+    return OMB_OK;
+}
+
+namespace omb {
+
+// Non-local regularisers (the NLM kernel, auxKernels.cl:297-620, with the
+// image read clamped to its edges as the reference's texture sampler reads
+// it): for voxel j, over the search offsets k != 0 with patch distance
+// d_k = sum_p g_p (P(j + p) - P(j + k + p))^2 (P the reference image when one
+// is given) and weight w_k = exp(-d_k / h), W = epps + sum_k w_k:
+//   0 NLM      sum w (u_j - u_k) / W
+//   1 NLTV     the same / sqrt((epps + sum w (u_j - u_k)^2) / W + epps)
+//   2 NLM-MRP  u_j - sum w u_k / W
+//   3 NLRD     sum w d (gamma |d| + u_j + 3 u_k + epps^2) / (u_j + u_k + gamma |d| + epps)^2 / W
+//   4 NL Lange sum w (s - s / (|d| / gamma + 1)) / W, s = sign(d)
+//   5 NLM-MRP with Lange applied to it
+//   6 NLGGMRF  sum w |d|^(p-1) / (1 + |d / c|^(p-q)) (p - gamma |d|^(p-q) / (1 + |d/c|^(p-q))) s / W
+// (d = u_j - u_k) and grad += beta * that; with `adaptive` (NLMADAPTIVE)
+// w_k = exp(-d_k / (d_k / |patch| * h + s)).  One thread per voxel; the image
+// is L2-resident and its neighbourhood served from L1.
+__device__ __forceinline__ int clampi(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
+__device__ __forceinline__ float sgnn(float v) { return (float)((0.f < v) - (v < 0.f)); }
+
+template <int TYPE>
+__global__ void k_nlm(const float *__restrict__ u, const float *__restrict__ ref, float *__restrict__ grad, int nx,
+                      int ny, int nz, int sx, int sy, int sz, int px, int py, int pz, const float *__restrict__ gauss,
+                      float h, float epps, float beta, float gamma, float gp, float gq, float gc, int adaptive,
+                      float adapt_s) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const int64_t nxy = (int64_t)nx * ny;
+    const float *P = ref ? ref : u;
+    auto at = [&](const float *a, int xx, int yy, int zz) {
+        return __ldg(a + clampi(xx, nx) + (int64_t)clampi(yy, ny) * nx + (int64_t)clampi(zz, nz) * nxy);
+    };
+    const float uj = __ldg(u + x + (int64_t)y * nx + (int64_t)z * nxy);
+    float wsum = epps, out = 0.f, ala = epps;
+    const float cpq = TYPE == 6 ? powf(gc, gp - gq) : 0.f;
+    const float psize = (float)((2 * px + 1) * (2 * py + 1) * (2 * pz + 1));
+    for (int i = -sx; i <= sx; ++i)
+        for (int j = -sy; j <= sy; ++j)
+            for (int k = -sz; k <= sz; ++k) {
+                if (i == 0 && j == 0 && k == 0) continue;
+                float dist = 0.f;
+                for (int qz = -pz; qz <= pz; ++qz)
+                    for (int qy = -py; qy <= py; ++qy) {
+                        int dg = (qz + pz) * (2 * px + 1) * (2 * py + 1) + (qy + py) * (2 * px + 1);
+                        for (int qx = -px; qx <= px; ++qx) {
+                            const float gg = __ldg(gauss + dg++);
+                            const float d = at(P, x + qx, y + qy, z + qz) - at(P, x + i + qx, y + j + qy, z + k + qz);
+                            dist += gg * d * d;
+                        }
+                    }
+                // NLMADAPTIVE: h scaled by the patch's mean squared difference plus a constant
+                const float w = adaptive ? expf(-dist / ((dist / psize) * h + adapt_s)) : expf(-dist / h);
+                wsum += w;
+                const float uk = at(u, x + i, y + j, z + k);
+                if (TYPE == 2 || TYPE == 5) {
+                    out += w * uk;
+                } else if (TYPE == 0) {
+                    out += w * (uj - uk);
+                } else if (TYPE == 3) {
+                    const float d = uj - uk;
+                    const float dp = uj + uk + gamma * fabsf(d) + epps;
+                    out += w * d * (gamma * fabsf(d) + uj + 3.f * uk + epps * epps) / (dp * dp);
+                } else if (TYPE == 4) {
+                    const float d = uj - uk;
+                    const float s = sgnn(d);
+                    out += w * (s - s / (fabsf(d) / gamma + 1.f));
+                } else if (TYPE == 6) {
+                    const float d = uj - uk;
+                    const float dcpq = powf(fabsf(d / gc), gp - gq);
+                    const float dpq = 1.f + dcpq;
+                    out += w * (powf(fabsf(d), gp - 1.f) / dpq) * (gp - gamma * ((dcpq * cpq) / dpq)) * sgnn(d);
+                } else {
+                    const float d = uj - uk;
+                    out += w * d;
+                    ala += w * d * d;
+                }
+            }
+    wsum = 1.f / wsum;
+    out *= wsum;
+    if (TYPE == 2) {
+        out = uj - out;
+    } else if (TYPE == 5) {
+        out = uj - out;
+        const float s = sgnn(out);
+        out = s - s / (fabsf(out) / gamma + 1.f);
+    } else if (TYPE == 1) {
+        out /= sqrtf(ala * wsum + epps);
+    }
+    grad[x + (int64_t)y * nx + (int64_t)z * nxy] += beta * out;
+}
+
+}  // namespace omb
+
+extern "C" int omb_nlm_gradient(const float *u, const float *ref, float *grad, int32_t nx, int32_t ny, int32_t nz,
+                                const int32_t *search, const int32_t *patch, const float *gaussian, float h,
+                                float epps, float beta, int32_t type, float gamma, const float *ggmrf_pqc,
+                                int32_t adaptive, float adaptive_s, void *stream) {
+    using namespace omb;
+    if (!u || !grad || !gaussian || !search || !patch) return set_error(OMB_ERR_INVALID, "NULL pointer passed to omb_nlm_gradient");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    for (int a = 0; a < 3; ++a)
+        if (search[a] < 0 || search[a] > 16 || patch[a] < 0 || patch[a] > 16)
+            return set_error(OMB_ERR_INVALID, "NLM windows must be in 0..16");
+    if (!(h > 0.f)) return set_error(OMB_ERR_INVALID, "NLM filter parameter h must be positive");
+    if (type == 6 && !ggmrf_pqc) return set_error(OMB_ERR_INVALID, "NLGGMRF needs p, q and c");
+    const float gp = type == 6 ? ggmrf_pqc[0] : 0.f, gq = type == 6 ? ggmrf_pqc[1] : 0.f,
+                gc = type == 6 ? ggmrf_pqc[2] : 1.f;
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    cudaStream_t st = (cudaStream_t)stream;
+#define OMB_NLM(T)                                                                                                \
+    k_nlm<T><<<grid, block, 0, st>>>(u, ref, grad, nx, ny, nz, search[0], search[1], search[2], patch[0], patch[1], \
+                                     patch[2], gaussian, h, epps, beta, gamma, gp, gq, gc, \
+                                     adaptive != 0, adaptive_s)
+    switch (type) {
+        case 0: OMB_NLM(0); break;
+        case 1: OMB_NLM(1); break;
+        case 2: OMB_NLM(2); break;
+        case 3: OMB_NLM(3); break;
+        case 4: OMB_NLM(4); break;
+        case 5: OMB_NLM(5); break;
+        case 6: OMB_NLM(6); break;
+        default: return set_error(OMB_ERR_INVALID, "NLM type must be 0..6");
+    }
+#undef OMB_NLM
+    OMB_LAUNCH_CHECK("NLM gradient launch");
     return OMB_OK;
 }

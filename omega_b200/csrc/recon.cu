@@ -91,10 +91,12 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         const bool sub_prior = alg == OMB_RECON_MBSREM || (pkma && p->prior != 0);
         const bool need_prior = osl || map || sub_prior;
         const bool no_sens = ramla || pkma || mb;
-        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_HUBER))
+        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_NLM))
             return set_error(OMB_ERR_INVALID, "unknown prior");
-        if (need_prior && p->prior != OMB_PRIOR_RDP && !p->prior_window)
+        if (need_prior && (p->prior == OMB_PRIOR_QUAD || p->prior == OMB_PRIOR_HUBER) && !p->prior_window)
             return set_error(OMB_ERR_INVALID, "the quadratic / Huber prior needs its window");
+        if (need_prior && p->prior == OMB_PRIOR_NLM && !p->nlm_gaussian)
+            return set_error(OMB_ERR_INVALID, "the NLM prior needs its patch weights");
         const Grid g = handle_grid(h);
         const float epps = handle_epps(h);
         // per-subset sensitivity images, then sub-iterations in subset order
@@ -146,6 +148,10 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                 return set_error(OMB_ERR_CUDA, "clearing the prior gradient failed");
             if (p->prior == OMB_PRIOR_RDP)
                 return omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
+            if (p->prior == OMB_PRIOR_NLM)
+                return omb_nlm_gradient(x_out, p->nlm_ref, du.f(), g.nx, g.ny, g.nz, p->prior_g, p->nlm_patch,
+                                        p->nlm_gaussian, p->nlm_h, epps, p->beta, p->nlm_type, p->rdp_gamma, p->ggmrf,
+                                        p->nlm_adaptive, p->nlm_adaptive_s, stream);
             // quadratic: the window applied at every voxel (priors.h:27-42); Huber clamps it
             int e = omb_psf_convolve(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_window, p->prior_g[0], p->prior_g[1],
                                      p->prior_g[2], stream);

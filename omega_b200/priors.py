@@ -76,3 +76,31 @@ def prior_window(wq, Ndx, Ndy, Ndz):
     win[n // 2 + 1:] = neg[n // 2:]
     win[n // 2] = np.abs(np.sum(neg, dtype=np.float32))
     return win
+
+
+def nlm_gaussian(options):
+    """Patch weights of the non-local priors (NLMPrepass, prepass.py:797-804):
+    exp(-(x^2 + y^2 + z^2) / (2 NLM_gauss^2)) on the (2 Nlx + 1)(2 Nly + 1)
+    (2 Nlz + 1) patch offsets, x fastest, float32."""
+    s = float(getattr(options, 'NLM_gauss', 2.0))
+    axes = [np.linspace(-n, n, 2 * n + 1, dtype=np.float32)
+            for n in (int(options.Nlx), int(options.Nly), int(options.Nlz))]
+    g = np.exp(-(np.add.outer(np.add.outer(axes[0] ** 2 / (2 * s ** 2), axes[1] ** 2 / (2 * s ** 2)),
+                              axes[2] ** 2 / (2 * s ** 2))))
+    options.gaussianNLM = g.flatten('F').astype(np.float32)
+    return options.gaussianNLM
+
+
+def nlm_type(options):
+    """NLTYPE of the options (ProjectorClass.h:841-862)."""
+    if getattr(options, 'NLM_MRP', False):
+        return 2
+    if getattr(options, 'NLTV', False):
+        return 1
+    if getattr(options, 'NLRD', False):
+        return 3
+    if getattr(options, 'NLLange', False):
+        return 4
+    if getattr(options, 'NLGGMRF', False):
+        return 6
+    return 0

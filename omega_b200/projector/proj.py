@@ -139,6 +139,25 @@ class projectorClass:
     Quad = False
     Huber = False
     huber_delta = 1.
+    # non-local priors (proj.py:329-349, 434-436, 454)
+    NLM = False
+    NLTV = False
+    NLRD = False
+    NLLange = False
+    NLGGMRF = False
+    NLM_MRP = False
+    NLM_use_anatomical = False
+    NLAdaptive = False
+    NLAdaptiveConstant = 1.
+    NLM_referenceImage = np.empty(0, dtype=np.float32)
+    NLMsigma = 1.
+    NLM_gauss = 2.
+    Nlx = 1
+    Nly = 1
+    Nlz = 1
+    GGMRF_p = 0.
+    GGMRF_q = 0.
+    GGMRF_c = 0.
     Ndx = 1
     Ndy = 1
     Ndz = 1

@@ -305,10 +305,11 @@ def reconstructions_main(options):
         raise ValueError('Select one reconstruction method (' + ', '.join(list(_PET_METHODS) + ['PDHG']) + ')')
     method = chosen[0]
     quad, huber = bool(getattr(options, 'Quad', False)), bool(getattr(options, 'Huber', False))
-    n_priors = int(bool(options.RDP)) + int(quad) + int(huber)
+    nlm = bool(getattr(options, 'NLM', False))
+    n_priors = int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm)
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
-        raise ValueError(method + ' needs one prior: options.RDP, options.Quad or options.Huber')
+        raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber or options.NLM')
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
         raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
@@ -358,9 +359,32 @@ def reconstructions_main(options):
     if method in ('MRAMLA', 'MBSREM'):
         u = float(getattr(options, 'U', 0.))
         p.upper_bound = u if u > 0 else 10000.
+    keep = []
     if prior:
         p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
-                   (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))
+                   (_native.OMB_PRIOR_NLM if nlm else (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER)))
+        if nlm:
+            # search window Ndx / Ndy / Ndz, patch Nlx / Nly / Nlz, h = NLMsigma^2 (libHeader.h:1285-1286;
+            # ProjectorClass.h:841-870), gamma = RDP_gamma, GGMRF p / q / c
+            from . import priors
+            g = torch.from_numpy(priors.nlm_gaussian(options)).to(dev)
+            keep.append(g)
+            p.nlm_gaussian = ctypes.c_void_p(g.data_ptr())
+            p.nlm_type = priors.nlm_type(options)
+            p.prior_g[0], p.prior_g[1], p.prior_g[2] = int(options.Ndx), int(options.Ndy), int(options.Ndz)
+            p.nlm_patch[0], p.nlm_patch[1], p.nlm_patch[2] = int(options.Nlx), int(options.Nly), int(options.Nlz)
+            p.nlm_h = float(options.NLMsigma) ** 2
+            p.nlm_adaptive = 1 if getattr(options, 'NLAdaptive', False) else 0
+            p.nlm_adaptive_s = float(getattr(options, 'NLAdaptiveConstant', 1.0))
+            p.ggmrf[0], p.ggmrf[1], p.ggmrf[2] = (float(getattr(options, k, 0.0)) for k in ('GGMRF_p', 'GGMRF_q',
+                                                                                            'GGMRF_c'))
+            if getattr(options, 'NLM_use_anatomical', False):
+                r = np.asarray(options.NLM_referenceImage, dtype=np.float32).ravel(order='F')
+                if r.size != n:
+                    raise ValueError('NLM_referenceImage must have the size of the image')
+                rt = torch.from_numpy(np.ascontiguousarray(r)).to(dev)
+                keep.append(rt)
+                p.nlm_ref = ctypes.c_void_p(rt.data_ptr())
         if quad or huber:
             from . import priors
             nd = (int(options.Ndx), int(options.Ndy), int(options.Ndz))

@@ -6,7 +6,12 @@ steps around the projectors, for the parity tests:
   (edge voxel repeated: index -1 reads 0, N reads N-1);
 * rdp_gradient: RDPKernel (auxKernels.cl:664-872), 6-neighbour form,
   neighbours outside the image 0 (the CUDA border addressing of the
-  reference's PyTorch/CuPy path, util/priors.py:178-181).
+  reference's PyTorch/CuPy path, util/priors.py:178-181);
+* nlm_gradient: the non-local kernels NLM (auxKernels.cl:297-620) with the
+  image read clamped to its edges (the texture sampler of the reference's
+  kernel path), and, with cpu_mode, the reference CPU function NLMFunc
+  (source/cpp/NLM.h:15-142: interior voxels only, weight sum 1 / (sum +
+  epps), NLTV's squared sum from 0), which oracle/_ref exports and pins.
 """
 import numpy as np
 
@@ -43,3 +48,93 @@ def rdp_gradient(u, shape, gamma, beta, epps=1e-8):
     minus[np.isnan(minus)] = 0.0
     assert c.shape == a.shape
     return (beta * (plus + minus)).ravel(order='F')
+
+
+def _sgn(v):
+    return np.sign(v)
+
+
+def nlm_gradient(u, shape, gaussian, sw, pw, h, epps, nl_type, gamma=10.0, ggmrf=(2.0, 1.5, 0.001), u_ref=None,
+                 cpu_mode=False, adaptive_s=None):
+    """Non-local gradient of image u (flat, x fastest), without the weight:
+    for every voxel j, over the search offsets k != 0 with patch distance
+    d_k = sum_p g_p (P(j + p) - P(j + k + p))^2 (P = u_ref when given) and
+    weight w_k = exp(-d_k / h):
+      0 NLM:     sum w (u_j - u_k) / W        1 NLTV: the same / sqrt(sum w (u_j - u_k)^2 / W + epps)
+      2 NLM-MRP: u_j - sum w u_k / W          3 NLRD, 4 NL Lange, 5 MRP + Lange, 6 NLGGMRF,
+    W = epps + sum w (cpu_mode: 1 / (sum w + epps) and the NLTV sum from 0;
+    a border of sw + pw voxels left 0).  adaptive_s (NLMADAPTIVE,
+    auxKernels.cl:562-563): w_k = exp(-d_k / (d_k / |patch| h + adaptive_s))."""
+    nx, ny, nz = shape
+    sx, sy, sz = (int(v) for v in sw)
+    px, py, pz = (int(v) for v in pw)
+    ax, ay, az = sx + px, sy + py, sz + pz
+    U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
+    R = U if u_ref is None else np.asarray(u_ref, dtype=np.float64).reshape((nz, ny, nx))
+    Up = np.pad(U, ((az, az), (ay, ay), (ax, ax)), mode='edge')
+    Rp = np.pad(R, ((az, az), (ay, ay), (ax, ax)), mode='edge')
+    g = np.asarray(gaussian, dtype=np.float64).reshape((2 * pz + 1, 2 * py + 1, 2 * px + 1))
+
+    def sh(A, dz, dy, dx):
+        return A[az + dz:az + dz + nz, ay + dy:ay + dy + ny, ax + dx:ax + dx + nx]
+    uj = U
+    wsum = np.zeros_like(U) if cpu_mode else np.full_like(U, epps)
+    out = np.zeros_like(U)
+    ala = np.zeros_like(U) if cpu_mode else np.full_like(U, epps)
+    p_, q_, c_ = (float(v) for v in ggmrf)
+    for i in range(-sx, sx + 1):
+        for j in range(-sy, sy + 1):
+            for k in range(-sz, sz + 1):
+                if i == 0 and j == 0 and k == 0:
+                    continue
+                dist = np.zeros_like(U)
+                for qz in range(-pz, pz + 1):
+                    for qy in range(-py, py + 1):
+                        for qx in range(-px, px + 1):
+                            d = sh(Rp, qz, qy, qx) - sh(Rp, k + qz, j + qy, i + qx)
+                            dist += g[qz + pz, qy + py, qx + px] * d * d
+                if adaptive_s is not None:
+                    psize = float((2 * px + 1) * (2 * py + 1) * (2 * pz + 1))
+                    w = np.exp(-dist / ((dist / psize) * h + adaptive_s))
+                else:
+                    w = np.exp(-dist / h)
+                wsum = wsum + w
+                uk = sh(Up, k, j, i)
+                if nl_type in (2, 5):
+                    out += w * uk
+                elif nl_type == 0:
+                    out += w * (uj - uk)
+                elif nl_type == 3:
+                    dd = uj - uk
+                    dp = uj + uk + gamma * np.abs(dd) + epps
+                    out += w * dd * (gamma * np.abs(dd) + uj + 3.0 * uk + epps * epps) / (dp * dp)
+                elif nl_type == 4:
+                    dd = uj - uk
+                    s_ = _sgn(dd)
+                    out += w * (s_ - s_ / (np.abs(dd) / gamma + 1.0))
+                elif nl_type == 6:
+                    dd = uj - uk
+                    dpq = 1.0 + np.abs(dd / c_) ** (p_ - q_)
+                    out += w * (np.abs(dd) ** (p_ - 1.0) / dpq) * (p_ - gamma * (np.abs(dd) ** (p_ - q_) / dpq)) * _sgn(dd)
+                else:
+                    dd = uj - uk
+                    out += w * dd
+                    ala += w * dd * dd
+    if cpu_mode:
+        ws = np.where(wsum != 0.0, 1.0 / (wsum + epps), wsum)
+    else:
+        ws = 1.0 / wsum
+    out = out * ws
+    if nl_type == 2:
+        out = uj - out
+    elif nl_type == 5:
+        o_ = uj - out
+        s_ = _sgn(o_)
+        out = s_ - s_ / (np.abs(o_) / gamma + 1.0)
+    elif nl_type == 1:
+        out = out / np.sqrt(ala * ws + epps)
+    if cpu_mode:
+        mask = np.zeros_like(U, dtype=bool)
+        mask[az:nz - az, ay:ny - ay, ax:nx - ax] = True
+        out = np.where(mask, out, 0.0)
+    return out.ravel()

@@ -5,7 +5,9 @@
  * sources where they lie (oracle/Makefile passes -I to them); nothing of the
  * reference is copied here.  Output goes to oracle/_ref/libref_siddon.so.
  * Used to pin the FP64 restatement (oracle/siddon_oracle.c) against the
- * reference itself, and as the timed CPU baseline of bench.py.
+ * reference itself, and as the timed CPU baseline of bench.py; also the
+ * reference's CPU non-local means gradient (NLM.h), which pins
+ * oracle/image_oracle.py's restatement.
  *
  * PET sinogram data, whole-sinogram subsets: the caller passes the z pairs of
  * the sinograms to project, so the function runs with subsets = 1.
@@ -13,6 +15,7 @@
 #include <cstdint>
 
 #include "projector_functions.h"
+#include "NLM.h"
 
 template <typename T>
 static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, T bx, T by, T bz, uint32_t n_rows,
@@ -155,6 +158,15 @@ int ref_orth_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double 
     const int64_t n_meas = (int64_t)n_rows * n_cols * n_proj;
     projectorType123Implementation4<double>(p, n_meas, output, xy, z, input, false, false, (uint8_t)(fp ? 1 : 2),
                                             sens, nullptr, n_threads);
+    return 0;
+}
+/* The reference's CPU non-local means gradient (NLM.h NLMFunc): interior
+ * voxels only (a border of search + patch window is left untouched). */
+int ref_nlm_d(double *grad, const double *u_ref, const double *u, const double *gaussian, int32_t sx, int32_t sy,
+              int32_t sz, int32_t px, int32_t py, int32_t pz, uint32_t nx, uint32_t ny, uint32_t nz, double h,
+              int32_t type, double gamma, double epps, double p, double q, double c, int32_t anatomical) {
+    NLMFunc<double>(grad, u_ref, u, gaussian, sx, sy, sz, px, py, pz, nx, ny, nz, (int32_t)(nx * ny), h, type, gamma,
+                    epps, p, q, c, anatomical != 0);
     return 0;
 }
 int ref_siddon_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx, double by,

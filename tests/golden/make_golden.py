@@ -5,6 +5,7 @@ $OMEGA_REFERENCE):
 
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py volumes    # the type-3 tables only
+    python tests/golden/make_golden.py nlm        # the NLM patch weights only
 
 For every option set in configs.py it imports the reference's own Python
 projector surface (omegatomo.projector.proj.projectorClass), runs its
@@ -161,6 +162,29 @@ def volume_fixture():
     print("vol_tables", {k: v.shape for k, v in out.items()})
 
 
+def nlm_fixture():
+    """The reference's NLM patch weights (prepass.py NLMPrepass) for two patch
+    sizes, stored in nlm_gauss.npz."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "omega_prepass", os.path.join(REF, "source", "Python", "omegatomo", "reconstruction", "prepass.py"))
+    prepass = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(prepass)
+
+    class Opt:
+        pass
+    out = {}
+    for tag, (nl, sd) in {"111": ((1, 1, 1), 2.0), "221": ((2, 2, 1), 1.5)}.items():
+        o = Opt()
+        o.Nlx, o.Nly, o.Nlz = nl
+        o.NLM_gauss = sd
+        o.NLM_use_anatomical = False
+        prepass.NLMPrepass(o)
+        out["g_" + tag] = np.asarray(o.gaussianNLM, dtype=np.float32)
+    np.savez_compressed(os.path.join(HERE, "nlm_gauss.npz"), **out)
+    print("nlm_gauss", {k: v.shape for k, v in out.items()})
+
+
 # type-3 table cases: tube radius, voxel radius (before scaling), voxel size (dx, dy, dz)
 VOLUME_CASES = {"a": (1.0, 1.0, (2.0, 2.0, 2.5)), "b": (2.5, 1.0, (1.5, 1.5, 1.5))}
 
@@ -169,8 +193,12 @@ def main():
     if sys.argv[1:] == ["volumes"]:
         volume_fixture()
         return
+    if sys.argv[1:] == ["nlm"]:
+        nlm_fixture()
+        return
     proj = reference_projector()
     volume_fixture()
+    nlm_fixture()
     psf_fixture(proj)
     prior_weight_fixture(proj)
     allc = dict(CONFIGS)
