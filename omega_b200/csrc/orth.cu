@@ -19,7 +19,8 @@
 // Deliberate differences from the reference kernel:
 //  * the walk and every distance are FP64 (the reference: FP32), so whether
 //    a voxel centre lies inside the tube is decided as the FP64 oracle
-//    decides it; weights and TOF are FP32;
+//    decides it; weights and TOF are FP32 (the type-3 table index is the
+//    FP64 one);
 //  * voxel centres are b + (i + 1/2) d each time (the reference steps some of
 //    them by repeated addition);
 //  * a type-3 table index past its last entry reads the last entry (the
@@ -46,6 +47,8 @@ struct OrthRay {
     double sx, sy, sz;          // source, slice axis first
     double fx, fy, fz;          // d - s, same order
     double orl;                 // orth_ray_length
+    double cut2;                // squared cut-off distance times orl^2: type 2 (1 - 0.01)^2, type 3 bmax^2
+    float inv_orl;              // 1 / orl (FP32 weights)
     double b1, d1;              // slice axis
     double b2, d2;              // in-slice axis
     int n1;                     // in-slice count
@@ -53,6 +56,10 @@ struct OrthRay {
 };
 
 // orthogonalHelper3D: false = outside the tube (stop the scan), true = visited.
+// Whether a voxel is inside is decided on the FP64 squared distance against
+// the ray's FP64 cut-off (no square root); the type-2 weight is then formed in
+// FP32 (1e-7 relative), the type-3 table index from the FP64 distance, as the
+// restatement forms it.
 template <class Visit>
 __device__ __forceinline__ bool orth_voxel(const Orth &o, const OrthRay &r, int slice, int uu, int zz, double lx,
                                            double ly, double lz, Visit &vis) {
@@ -61,21 +68,13 @@ __device__ __forceinline__ bool orth_voxel(const Orth &o, const OrthRay &r, int 
     const double y1 = r.fz * x0 - ly;
     const double z1 = -r.fx * x0 + lz;
     const double n2 = lx * lx + y1 * y1 + z1 * z1;
+    if (o.type == 3 ? n2 > r.cut2 : n2 >= r.cut2) return false;
     float ele;
     if (o.type == 3) {
-        const double bmax = (double)o.bmax;
-        if (n2 > bmax * bmax * r.orl * r.orl) return false;
         const double dd = sqrt(n2) / r.orl;
-        if (dd < (double)o.bmin) {
-            ele = o.vmax;
-        } else {
-            int iv = (int)rint((dd - (double)o.bmin) * kCC);
-            iv = min(iv, o.nv - 1);
-            ele = __ldg(o.v + iv);
-        }
+        ele = dd < (double)o.bmin ? o.vmax : __ldg(o.v + min((int)rint((dd - (double)o.bmin) * kCC), o.nv - 1));
     } else {
-        if (n2 >= (1.0 - kThr) * (1.0 - kThr) * r.orl * r.orl) return false;
-        ele = (float)(1.0 - sqrt(n2) / r.orl);
+        ele = 1.f - sqrtf((float)n2) * r.inv_orl;
     }
     vis((int64_t)slice * r.st_slice + (int64_t)uu * r.st_in + (int64_t)zz * r.nxy, ele);
     return true;
@@ -253,6 +252,9 @@ __device__ bool orth_trace(const Grid &g, const Orth &o, const Ray &ray, float g
     auto put = [&](int64_t ind, float ele) { vis(ind, ele, w, tsum); };
     OrthRay r;
     r.orl = o.type == 2 ? L * (double)o.width : L;
+    r.cut2 = o.type == 3 ? (double)o.bmax * (double)o.bmax * r.orl * r.orl
+                         : (1.0 - kThr) * (1.0 - kThr) * r.orl * r.orl;
+    r.inv_orl = (float)(1.0 / r.orl);
     r.nxy = (int64_t)g.nx * g.ny;
     int tempk_b = 0;
     const double bx = g.bx, by = g.by, bz = g.bz, dxg = g.dx, dyg = g.dy, dzg = g.dz;
