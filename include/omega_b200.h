@@ -348,6 +348,8 @@ typedef struct omb_recon_params {
     float ggmrf[3];           /* NLGGMRF: options.GGMRF_p, GGMRF_q, GGMRF_c */
     int32_t nlm_adaptive;     /* options.NLAdaptive */
     float nlm_adaptive_s;     /* options.NLAdaptiveConstant */
+    int32_t precond;          /* PKMA / MRAMLA / MBSREM image preconditioner: 0 none, 1 type 0 (rhs / D), 2 type 1
+                                 (rhs * x / D), see omb_precond_image */
 } omb_recon_params;
 
 /*
@@ -402,14 +404,16 @@ int omb_ramla_subset(omb_handle *h, int32_t subset, float *image, const float *y
                      int32_t positivity, float *work_meas, float *work_img, void *stream);
 
 /*
- * One PKMA sub-iteration (subiterStep.h:281-295, algorithms.h:151-212 with
- * neither preconditioner nor automatic relaxation): rhs = the backprojection
+ * One PKMA sub-iteration (subiterStep.h:281-295, algorithms.h:151-212
+ * without automatic relaxation; image preconditioner as omb_precond_image
+ * lists, precond_d its D or NULL with precond 0): rhs = the backprojection
  * of 1 - y / (fp + epps [+ randoms]) (NaN / Inf -> epps) plus du (device,
  * the prior gradient with its weight; NULL: none); x_a = x - lambda * rhs,
  * max(epps, x_a) when `positivity`; image = (1 - alpha) image + alpha x_a.
  */
 int omb_pkma_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda, float alpha,
-                    const float *du, int32_t positivity, float *work_meas, float *work_img, void *stream);
+                    const float *du, int32_t positivity, const float *precond_d, int32_t precond, float *work_meas,
+                    float *work_img, void *stream);
 
 /*
  * One MRAMLA / MBSREM sub-iteration (subiterStep.h:123-128, 237-241,
@@ -420,8 +424,18 @@ int omb_pkma_subset(omb_handle *h, int32_t subset, float *image, const float *y_
  * zero-randoms bins with a separate bound (epsilon_mramla) not built here.
  */
 int omb_mbsrem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda,
-                      float upper, const float *du, int32_t positivity, float *work_meas, float *work_img,
-                      void *stream);
+                      float upper, const float *du, int32_t positivity, const float *precond_d, int32_t precond,
+                      float *work_meas, float *work_img, void *stream);
+
+/*
+ * The image preconditioners of PKMA / MRAMLA / MBSREM (applyImagePreconditioning,
+ * functions.hpp:2057-2106; the sub-iteration entries take `precond` 0 none,
+ * 1 rhs / D (options.precondTypeImage[0]), 2 rhs * x / D ([1]; MBSREM folds x
+ * >= U / 2 to U - x)) and their D (device, one image): the subsets' summed
+ * A^T 1 divided by the subset count, zeros set to 1 (reconstructionAF.h:
+ * 779-816).  work_img: one image of scratch.  PET sinogram data.
+ */
+int omb_precond_image(omb_handle *h, float *d, float *work_img, void *stream);
 
 /*
  * The MAP step of BSREM and ROSEM-MAP after each iteration (algorithms.h:

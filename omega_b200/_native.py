@@ -115,6 +115,7 @@ class ReconParams(ctypes.Structure):
         ("ggmrf", ctypes.c_float * 3),
         ("nlm_adaptive", ctypes.c_int32),
         ("nlm_adaptive_s", ctypes.c_float),
+        ("precond", ctypes.c_int32),
     ]
 
 
@@ -208,10 +209,13 @@ EXPORTS = [
                                         ctypes.c_void_p]),
     ("omb_pkma_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int32,
-                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+                                       ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p]),
     ("omb_mbsrem_subset", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_int32,
-                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+                                         ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
+    ("omb_precond_image", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_void_p]),
     ("omb_nlm_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,

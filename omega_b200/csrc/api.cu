@@ -401,6 +401,19 @@ int omb::handle_subsets(const omb_handle *h) { return h ? h->desc.n_subsets : 0;
 Grid omb::handle_grid(const omb_handle *h) { return h ? h->grid : Grid{}; }
 float omb::handle_epps(const omb_handle *h) { return h ? h->desc.epps : 0.f; }
 
+int omb::sensitivity_raw(omb_handle *h, int32_t subset, float *sens, cudaStream_t s) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!sens) return set_error(OMB_ERR_INVALID, "sens pointer is NULL");
+    RaySet rs{};
+    int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    if (h->desc.modality != OMB_PET_SINOGRAM || h->desc.bp_type < 1 || h->desc.bp_type > 4)
+        return set_error(OMB_ERR_UNSUPPORTED, "omb_sensitivity needs a ray-driven PET backprojector (types 1 to 4)");
+    // A^T 1 through the BP kernel's fused sensitivity accumulator, y = NULL.
+    OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, h->n_img * sizeof(float), s));
+    return rays_backward(h, rs, one_frame_bp(h, nullptr, nullptr, rs.m_size), sens, s);
+}
+
 extern "C" {
 
 int omb_abi_version(void) { return OMB_ABI_VERSION; }
@@ -656,19 +669,9 @@ int omb_backward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const f
 }
 
 int omb_sensitivity(omb_handle *h, int32_t subset, float *sens, void *stream) {
-    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
-    if (!sens) return set_error(OMB_ERR_INVALID, "sens pointer is NULL");
-    RaySet rs{};
-    int st = ray_set(h, subset, rs);
+    const int st = sensitivity_raw(h, subset, sens, (cudaStream_t)stream);
     if (st != OMB_OK) return st;
-    cudaStream_t s = (cudaStream_t)stream;
-    if (h->desc.modality != OMB_PET_SINOGRAM || h->desc.bp_type < 1 || h->desc.bp_type > 4)
-        return set_error(OMB_ERR_UNSUPPORTED, "omb_sensitivity needs a ray-driven PET backprojector (types 1 to 4)");
-    // A^T 1 through the BP kernel's fused sensitivity accumulator, y = NULL.
-    OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, h->n_img * sizeof(float), s));
-    st = rays_backward(h, rs, one_frame_bp(h, nullptr, nullptr, rs.m_size), sens, s);
-    if (st != OMB_OK) return st;
-    return clamp_min(sens, h->n_img, h->desc.epps, s);
+    return clamp_min(sens, h->n_img, h->desc.epps, (cudaStream_t)stream);
 }
 
 int omb_osem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
@@ -735,6 +738,8 @@ int relaxed_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
     if (!image || !y_subset || (a.kind == kRosem && !a.sens) || !work_meas || !work_img)
         return set_error(OMB_ERR_INVALID, "NULL buffer passed to a relaxed sub-iteration");
+    if (a.precond < 0 || a.precond > 2 || (a.precond && !a.precond_d))
+        return set_error(OMB_ERR_INVALID, "image preconditioner: mode 0..2, modes 1 and 2 need their D image");
     if (h->desc.modality == OMB_CT_PANEL)
         return set_error(OMB_ERR_UNSUPPORTED, "the relaxed sub-iterations are PET-only");
     if (h->desc.fp_type < 1 || h->desc.fp_type > 4 || h->desc.bp_type < 1 || h->desc.bp_type > 4)
@@ -759,8 +764,12 @@ int relaxed_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
     switch (a.kind) {
         case kRosem: return rosem_update(image, a.sens, work_img, h->n_img, a.lam, s);
         case kRamla: return bsrem_update(image, work_img, h->n_img, a.lam, eps, a.positivity, s);
-        case kPkma: return pkma_update(image, work_img, a.du, h->n_img, a.lam, a.alpha, eps, a.positivity, s);
-        case kMbsrem: return mbsrem_update(image, work_img, a.du, h->n_img, a.lam, eps, a.upper, a.positivity, s);
+        case kPkma:
+            return pkma_update(image, work_img, a.du, h->n_img, a.lam, a.alpha, eps, a.positivity, a.precond_d,
+                               a.precond, s);
+        case kMbsrem:
+            return mbsrem_update(image, work_img, a.du, h->n_img, a.lam, eps, a.upper, a.positivity, a.precond_d,
+                                 a.precond, s);
         default: return set_error(OMB_ERR_INVALID, "unknown relaxed update");
     }
 }
@@ -787,8 +796,11 @@ int omb_ramla_subset(omb_handle *h, int32_t subset, float *image, const float *y
 }
 
 int omb_pkma_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda, float alpha,
-                    const float *du, int32_t positivity, float *work_meas, float *work_img, void *stream) {
+                    const float *du, int32_t positivity, const float *precond_d, int32_t precond, float *work_meas,
+                    float *work_img, void *stream) {
     RelaxedArgs a;
+    a.precond_d = precond_d;
+    a.precond = precond;
     a.kind = kPkma;
     a.du = du;
     a.lam.v = lambda;
@@ -798,10 +810,12 @@ int omb_pkma_subset(omb_handle *h, int32_t subset, float *image, const float *y_
 }
 
 int omb_mbsrem_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, float lambda,
-                      float upper, const float *du, int32_t positivity, float *work_meas, float *work_img,
-                      void *stream) {
+                      float upper, const float *du, int32_t positivity, const float *precond_d, int32_t precond,
+                      float *work_meas, float *work_img, void *stream) {
     if (!(upper > 0.f)) return set_error(OMB_ERR_INVALID, "the upper bound U must be positive");
     RelaxedArgs a;
+    a.precond_d = precond_d;
+    a.precond = precond;
     a.kind = kMbsrem;
     a.du = du;
     a.lam.v = lambda;
@@ -1391,3 +1405,15 @@ int omb_batch_backward(omb_batch *b, const float *y, float *images, void *stream
 }
 
 }  // extern "C"
+
+extern "C" int omb_precond_image(omb_handle *h, float *d, float *work_img, void *stream) {
+    if (!h || !d || !work_img) return set_error(OMB_ERR_INVALID, "NULL pointer passed to omb_precond_image");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int S = h->desc.n_subsets;
+    for (int s_ = 0; s_ < S; ++s_) {
+        int st = sensitivity_raw(h, s_, s_ == 0 ? d : work_img, s);
+        if (st == OMB_OK && s_ > 0) st = add_into(d, work_img, h->n_img, s);
+        if (st != OMB_OK) return st;
+    }
+    return precond_finish(d, h->n_img, S, s);
+}

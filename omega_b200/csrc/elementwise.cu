@@ -114,16 +114,27 @@ __global__ void k_ratio_shift(const float *__restrict__ y, float *__restrict__ f
 }
 
 // PoissonUpdate, PKMA and MBSREM forms (auxKernels.cl:2008-2022)
+// Image preconditioning of the gradient (applyImagePreconditioning,
+// functions.hpp:2057-2106, types 0 and 1): 1 = g / D, 2 = g * (x_p / D) with
+// x_p the image (PKMA) or min-folded image (MBSREM: U - x where x >= U / 2,
+// algorithms.h:35-41); D the mean sensitivity over the subsets, 0 -> 1.
+__device__ __forceinline__ float precondition(float g, int mode, const float *__restrict__ dd, int64_t i, float xp) {
+    if (mode == 1) return g / __ldg(dd + i);
+    if (mode == 2) return g * (xp / __ldg(dd + i));
+    return g;
+}
+
 __global__ void k_pkma_update(float *__restrict__ img, const float *__restrict__ rhs, const float *__restrict__ du,
                               int64_t n, const float *__restrict__ lam_s, const int *__restrict__ it, float lam_v,
                               const float *__restrict__ al_s, int n_sub, int sub, float al_v, float epps,
-                              int positivity) {
+                              int positivity, const float *__restrict__ dd, int mode) {
     const float lam = relax_value(lam_s, it, lam_v);
     const float a = al_s ? al_s[*it * n_sub + sub] : al_v;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float x = img[i];
-        const float g = du ? __ldg(rhs + i) + __ldg(du + i) : __ldg(rhs + i);
+        float g = du ? __ldg(rhs + i) + __ldg(du + i) : __ldg(rhs + i);
+        g = precondition(g, mode, dd, i, x);
         float v = x - lam * g;
         if (positivity) v = fmaxf(epps, v);
         img[i] = (1.f - a) * x + a * v;
@@ -132,16 +143,47 @@ __global__ void k_pkma_update(float *__restrict__ img, const float *__restrict__
 
 __global__ void k_mbsrem_update(float *__restrict__ img, const float *__restrict__ rhs, const float *__restrict__ du,
                                 int64_t n, const float *__restrict__ lam_s, const int *__restrict__ it, float lam_v,
-                                float epps, float upper, int positivity) {
+                                float epps, float upper, int positivity, const float *__restrict__ dd, int mode) {
     const float lam = relax_value(lam_s, it, lam_v);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const float g = du ? __ldg(rhs + i) + __ldg(du + i) : __ldg(rhs + i);
-        float v = img[i] + lam * g;
+        const float x = img[i];
+        float g = du ? __ldg(rhs + i) + __ldg(du + i) : __ldg(rhs + i);
+        g = precondition(g, mode, dd, i, x >= upper / 2.f ? upper - x : x);
+        float v = x + lam * g;
         if (positivity) v = fmaxf(epps, v);
         if (v >= upper) v = upper - epps;
         img[i] = v;
     }
+}
+
+// D = (sum of the subsets' sensitivities) / S, zeros -> 1 (reconstructionAF.h:779-816)
+__global__ void k_precond_finish(float *__restrict__ dd, int64_t n, float subsets) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float v = dd[i];
+        if (subsets > 1.f) v /= subsets;
+        dd[i] = v == 0.f ? 1.f : v;
+    }
+}
+
+__global__ void k_add_into(float *__restrict__ acc, const float *__restrict__ v, int64_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) acc[i] += __ldg(v + i);
+}
+
+int precond_finish(float *dd, int64_t n, int subsets, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_precond_finish<<<grid_for(n, 4), kBlock, 0, st>>>(dd, n, (float)subsets);
+    OMB_LAUNCH_CHECK("preconditioner image launch");
+    return OMB_OK;
+}
+
+int add_into(float *acc, const float *v, int64_t n, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_add_into<<<grid_for(n, 4), kBlock, 0, st>>>(acc, v, n);
+    OMB_LAUNCH_CHECK("image add launch");
+    return OMB_OK;
 }
 
 __global__ void k_rosem_update(float *__restrict__ img, const float *__restrict__ sens, const float *__restrict__ rhs,
@@ -204,19 +246,19 @@ int bsrem_update(float *img, const float *rhs, int64_t n, Relax lam, float epps,
 }
 
 int pkma_update(float *img, const float *rhs, const float *du, int64_t n, Relax lam, Momentum a, float epps,
-                bool positivity, cudaStream_t st) {
+                bool positivity, const float *dd, int mode, cudaStream_t st) {
     if (n <= 0) return OMB_OK;
     k_pkma_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, rhs, du, n, lam.lam, lam.iter, lam.v, a.alpha, a.n_subsets,
-                                                     a.subset, a.v, epps, positivity ? 1 : 0);
+                                                     a.subset, a.v, epps, positivity ? 1 : 0, dd, mode);
     OMB_LAUNCH_CHECK("PKMA update launch");
     return OMB_OK;
 }
 
 int mbsrem_update(float *img, const float *rhs, const float *du, int64_t n, Relax lam, float epps, float upper,
-                  bool positivity, cudaStream_t st) {
+                  bool positivity, const float *dd, int mode, cudaStream_t st) {
     if (n <= 0) return OMB_OK;
     k_mbsrem_update<<<grid_for(n, 4), kBlock, 0, st>>>(img, rhs, du, n, lam.lam, lam.iter, lam.v, epps, upper,
-                                                       positivity ? 1 : 0);
+                                                       positivity ? 1 : 0, dd, mode);
     OMB_LAUNCH_CHECK("MBSREM update launch");
     return OMB_OK;
 }

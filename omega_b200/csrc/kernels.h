@@ -49,10 +49,15 @@ int rosem_update(float *img, const float *sens, const float *rhs, int64_t n, Rel
 int bsrem_update(float *img, const float *rhs, int64_t n, Relax lam, float epps, bool positivity, cudaStream_t st);
 // PKMA: g = rhs [+ du]; xa = x - lam * g, max(epps, xa) when positivity; x = (1 - a) x + a xa
 int pkma_update(float *img, const float *rhs, const float *du, int64_t n, Relax lam, Momentum a, float epps,
-                bool positivity, cudaStream_t st);
+                bool positivity, const float *dd, int mode, cudaStream_t st);
 // MRAMLA / MBSREM: x = x + lam * (rhs [+ du]), max(epps, x) when positivity, x >= U -> U - epps
 int mbsrem_update(float *img, const float *rhs, const float *du, int64_t n, Relax lam, float epps, float upper,
-                  bool positivity, cudaStream_t st);
+                  bool positivity, const float *dd, int mode, cudaStream_t st);
+// PKMA / MBSREM image preconditioning: D = sum / S with zeros -> 1; acc += v
+int precond_finish(float *dd, int64_t n, int subsets, cudaStream_t st);
+int add_into(float *acc, const float *v, int64_t n, cudaStream_t st);
+// A^T 1 of one subset without the epps floor of omb_sensitivity
+int sensitivity_raw(omb_handle *h, int32_t subset, float *sens, cudaStream_t st);
 // MAP step: x = x - lam * x * du, then max(epps, x)
 int map_step(float *img, const float *du, int64_t n, Relax lam, float epps, cudaStream_t st);
 // ++*iter on the stream
@@ -67,6 +72,8 @@ struct RelaxedArgs {
     Momentum alpha;                // PKMA
     float upper = 10000.f;         // MRAMLA / MBSREM: U
     bool positivity = true;
+    const float *precond_d = nullptr;  // PKMA / MBSREM: D of the image preconditioner
+    int precond = 0;               // 0 none, 1 g / D (type 0), 2 g * x / D (type 1)
 };
 int relaxed_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const RelaxedArgs &a,
                    float *work_meas, float *work_img, cudaStream_t st);

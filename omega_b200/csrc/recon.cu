@@ -139,6 +139,14 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             }
         }
         const float upper = p->upper_bound > 0.f ? p->upper_bound : 10000.f;
+        // PKMA / MBSREM image preconditioner: D once, before the iterations
+        DevBuf pd;
+        if (p->precond < 0 || p->precond > 2 || (p->precond && !(pkma || mb)))
+            return set_error(OMB_ERR_INVALID, "image preconditioners 1 and 2 are for PKMA / MRAMLA / MBSREM");
+        if (p->precond) {
+            if ((st = alloc(pd, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+            if ((st = omb_precond_image(h, pd.f(), wi.f(), stream)) != OMB_OK) return st;
+        }
         for (int s_ = 0; s_ < n_subsets && !no_sens && st == OMB_OK; ++s_)
             st = omb_sensitivity(h, s_, sens.f() + s_ * n, stream);
         if (st != OMB_OK) return st;
@@ -176,6 +184,8 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                     ra.alpha.subset = s_;
                     ra.upper = upper;
                     ra.positivity = p->positivity != 0;
+                    ra.precond = p->precond;
+                    ra.precond_d = p->precond ? pd.f() : nullptr;
                     if (sub_prior) {
                         e = prior_grad();
                         ra.du = du.f();

@@ -132,6 +132,7 @@ class projectorClass:
     rho_PKMA = .45
     delta_PKMA = 100.
     U = 0.
+    precondTypeImage = np.full((7, 1), False)
     PDHG = False
     TV = False
     RDP = False

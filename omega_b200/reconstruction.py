@@ -359,6 +359,16 @@ def reconstructions_main(options):
     if method in ('MRAMLA', 'MBSREM'):
         u = float(getattr(options, 'U', 0.))
         p.upper_bound = u if u > 0 else 10000.
+    # image preconditioners of PKMA / MRAMLA / MBSREM: types 0 (rhs / D) and 1
+    # (rhs * x / D) of options.precondTypeImage; other algorithms ignore them,
+    # as the reference does (proj.py:1079-1082)
+    pt_im = np.ravel(np.asarray(getattr(options, 'precondTypeImage', np.zeros(7, dtype=bool)), dtype=bool))
+    if method in ('PKMA', 'MRAMLA', 'MBSREM') and pt_im.size and pt_im.any():
+        if pt_im.size > 2 and pt_im[2:].any():
+            raise ValueError('Image preconditioners other than types 0 and 1 are not built')
+        if pt_im[0] and pt_im.size > 1 and pt_im[1]:
+            raise ValueError('Only one of the image preconditioners 0-2 can be selected')
+        p.precond = 1 if pt_im[0] else 2
     keep = []
     if prior:
         p.prior = (_native.OMB_PRIOR_RDP if options.RDP else

@@ -341,8 +341,18 @@ def default_momentum(n_iter, n_subsets, rho=0.45, delta=100.0):
     return (1.0 + (rho * k) / (k + delta)).astype(np.float32)
 
 
+def precond_image(geom: Geometry, backward=None):
+    """D of the PKMA / MBSREM image preconditioners (reconstructionAF.h:779-816):
+    the subsets' summed A^T 1 over the subset count, zeros set to 1."""
+    bwd = backward or globals()["backward"]
+    d = sum(bwd(geom, None, s, sens=True)[1] for s in range(geom.n_subsets))
+    if geom.n_subsets > 1:
+        d = d / geom.n_subsets
+    return np.where(d == 0.0, 1.0, d)
+
+
 def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None, backward=None, randoms=None,
-            prior_grad=None, positivity=True, alpha=None, upper=10000.0):
+            prior_grad=None, positivity=True, alpha=None, upper=10000.0, precond=0):
     """Restated relaxed loops in FP64 (kind: "ROSEM", "RAMLA", "BSREM",
     "ROSEM_MAP", "PKMA", "MRAMLA", "MBSREM"); returns the image after n_iter
     iterations.
@@ -359,7 +369,9 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
     x = (1 - a) x + a xa, a = alpha[iter * S + subset].
     MRAMLA / MBSREM (computeForwardProject.h:153-180, algorithms.h:31-52,
     auxKernels.cl:2011-2022): x + lam (A^T (y / (fp + epps [+ r]) - 1)
-    [+ dU]), max(epps, .) with positivity, values >= U set to U - epps."""
+    [+ dU]), max(epps, .) with positivity, values >= U set to U - epps.
+    precond (PKMA / MRAMLA / MBSREM, functions.hpp:2057-2106): 1 divides the
+    gradient by D, 2 multiplies it by x / D (MBSREM: U - x where x >= U / 2)."""
     fwd = forward or globals()["forward"]
     bwd = backward or globals()["backward"]
     lam = np.asarray(default_relaxation(n_iter) if lam is None else lam, dtype=np.float32)
@@ -371,6 +383,7 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
     additive = kind in ("PKMA", "MRAMLA", "MBSREM")
     x = np.asarray(x0, dtype=np.float64).copy()
     eps = geom.epps
+    D = precond_image(geom, bwd) if precond else None
     sens = []
     if kind in ("ROSEM", "ROSEM_MAP"):
         for s in range(S):
@@ -393,6 +406,11 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
             rhs = bwd(geom, r, s)
             if du is not None:
                 rhs = rhs + du
+            if precond == 1:
+                rhs = rhs / D
+            elif precond == 2:
+                xp = np.where(x >= upper / 2.0, upper - x, x) if kind in ("MRAMLA", "MBSREM") else x
+                rhs = rhs * (xp / D)
             if kind == "PKMA":
                 a = float(alpha[it * S + s])
                 xa = x - lm * rhs

@@ -362,12 +362,45 @@ def test_pkma_mbsrem_entries_match_builtin(cuda):
     for it in range(2):
         for s in range(g.n_subsets):
             _native.call("omb_pkma_subset", o._handle, s, _ptr(x), _ptr(ys[s]), float(lam[it]),
-                         float(alpha[it * g.n_subsets + s]), None, 1, _ptr(wm), _ptr(wi), st)
+                         float(alpha[it * g.n_subsets + s]), None, 1, None, 0, _ptr(wm), _ptr(wi), st)
     assert orc.rel_l2(x.cpu().numpy(), built) < 1e-6
     o2, _ = _pet("pet_mini", 36)
     built2 = _run_builtin(o2, "MRAMLA", 1, lam=[0.2])
     x = torch.ones(g.n_img, device=dev)
     for s in range(g.n_subsets):
-        _native.call("omb_mbsrem_subset", o2._handle, s, _ptr(x), _ptr(ys[s]), 0.2, 10000.0, None, 1, _ptr(wm),
-                     _ptr(wi), st)
+        _native.call("omb_mbsrem_subset", o2._handle, s, _ptr(x), _ptr(ys[s]), 0.2, 10000.0, None, 1, None, 0,
+                     _ptr(wm), _ptr(wi), st)
     assert orc.rel_l2(x.cpu().numpy(), built2) < 1e-6
+
+
+@pytest.mark.gpu
+def test_precond_image_matches_oracle(cuda):
+    import torch
+    from omega_b200 import _native
+    from omega_b200.reconstruction import _ptr, _stream
+    o, g = _pet("pet_mini", 40)
+    o.initProj()
+    dev = torch.device("cuda", o._device)
+    d = torch.empty(g.n_img, device=dev)
+    w = torch.empty(g.n_img, device=dev)
+    _native.call("omb_precond_image", o._handle, _ptr(d), _ptr(w), _stream(dev))
+    ref = orc.precond_image(g)
+    assert np.any(ref == 1.0)      # voxels no ray crosses
+    assert orc.rel_l2(d.cpu().numpy(), ref) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method,mode", [("PKMA", 1), ("PKMA", 2), ("MRAMLA", 2), ("MBSREM", 1)])
+def test_builtin_preconditioned_matches_oracle(cuda, method, mode):
+    o, g = _pet("pet_mini", 41)
+    lam = [0.6, 0.4, 0.3] if mode == 2 else [0.3, 0.2, 0.15]
+    o.precondTypeImage = np.array([mode == 1, mode == 2, False, False, False, False, False])
+    extra = {"RDP": True, "RDP_gamma": 2.0, "beta": 0.05} if method == "MBSREM" else {}
+    x = _run_builtin(o, method, 3, lam=lam, **extra)
+    shape = (g.nx, g.ny, g.nz)
+    grad = (lambda v: io.rdp_gradient(v, shape, 2.0, 0.05, g.epps)) if method == "MBSREM" else None
+    ys = _subset_measurements(o, g)
+    ref = orc.relaxed(g, ys, np.ones(g.n_img), 3, method, lam=np.float32(lam), prior_grad=grad, precond=mode)
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    plain = orc.relaxed(g, ys, np.ones(g.n_img), 3, method, lam=np.float32(lam), prior_grad=grad)
+    assert orc.rel_l2(ref, plain) > 1e-3
