@@ -311,7 +311,8 @@ typedef enum omb_prior {
     OMB_PRIOR_RDP = 1,      /* options.RDP: relative difference prior, parameter rdp_gamma */
     OMB_PRIOR_QUAD = 2,     /* options.Quad: the quadratic window (prior_window) applied with mirrored edges */
     OMB_PRIOR_HUBER = 3,    /* options.Huber: the same with the gradient clamped to +-huber_delta */
-    OMB_PRIOR_NLM = 4       /* options.NLM (with NLTV / NLM_MRP / NLRD / NLLange / NLGGMRF): omb_nlm_gradient */
+    OMB_PRIOR_NLM = 4,      /* options.NLM (with NLTV / NLM_MRP / NLRD / NLLange / NLGGMRF): omb_nlm_gradient */
+    OMB_PRIOR_MRP = 5       /* options.MRP: omb_mrp_gradient over the prior_g window (Ndx, Ndy, Ndz) */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -350,6 +351,7 @@ typedef struct omb_recon_params {
     float nlm_adaptive_s;     /* options.NLAdaptiveConstant */
     int32_t precond;          /* PKMA / MRAMLA / MBSREM image preconditioner: 0 none, 1 type 0 (rhs / D), 2 type 1
                                  (rhs * x / D), see omb_precond_image */
+    int32_t mrp_no_norm;      /* MRP: options.med_no_norm */
 } omb_recon_params;
 
 /*
@@ -369,6 +371,15 @@ int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const fl
  */
 int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
                    const float *du, float *work_meas, float *work_img, void *stream);
+
+/*
+ * Median root prior gradient (priors.h:4-25, medianFilter3D auxKernels.cl:
+ * 981-1027): grad += beta * (u - med) / (med + epps) (no_norm: beta *
+ * (u - med)), med the median of the (2mx+1)(2my+1)(2mz+1) neighbourhood of u
+ * mirrored at its faces (functions.hpp:216-260).  Windows up to 125 voxels.
+ */
+int omb_mrp_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx, int32_t my,
+                     int32_t mz, float epps, float beta, int32_t no_norm, void *stream);
 
 /*
  * Non-local regulariser gradient (the NLM kernel, auxKernels.cl:297-620, the

@@ -116,6 +116,7 @@ class ReconParams(ctypes.Structure):
         ("nlm_adaptive", ctypes.c_int32),
         ("nlm_adaptive_s", ctypes.c_float),
         ("precond", ctypes.c_int32),
+        ("mrp_no_norm", ctypes.c_int32),
     ]
 
 
@@ -133,6 +134,7 @@ OMB_PRIOR_RDP = 1
 OMB_PRIOR_QUAD = 2
 OMB_PRIOR_HUBER = 3
 OMB_PRIOR_NLM = 4
+OMB_PRIOR_MRP = 5
 
 
 class Tuning(ctypes.Structure):
@@ -218,6 +220,9 @@ EXPORTS = [
     ("omb_precond_image", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_void_p]),
+    ("omb_mrp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p]),
     ("omb_nlm_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                         ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p, ctypes.c_float,

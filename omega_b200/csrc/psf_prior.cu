@@ -230,3 +230,59 @@ extern "C" int omb_nlm_gradient(const float *u, const float *ref, float *grad, i
     OMB_LAUNCH_CHECK("NLM gradient launch");
     return OMB_OK;
 }
+
+namespace omb {
+
+// Median root prior (MRP, priors.h:4-25 with medianFilter3D,
+// auxKernels.cl:981-1027): the median of the (2mx+1)(2my+1)(2mz+1)
+// neighbourhood of the image mirrored at its faces (padding(),
+// functions.hpp:216-260: index -1 reads 0), the element of rank K / 2 with
+// ties ranked by position; grad += beta * (u - med) / (med + epps), or
+// beta * (u - med) with no_norm.  One thread per voxel, the window in local
+// memory (K <= 125).
+constexpr int kMrpMax = 125;
+
+__global__ void k_mrp_gradient(const float *__restrict__ u, float *__restrict__ grad, int nx, int ny, int nz, int mx,
+                               int my, int mz, float epps, float beta, int no_norm) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const int64_t nxy = (int64_t)nx * ny;
+    float win[kMrpMax];
+    int k = 0;
+    for (int i = -mx; i <= mx; ++i)
+        for (int j = -my; j <= my; ++j)
+            for (int l = -mz; l <= mz; ++l)
+                win[k++] = __ldg(u + mirror(x + i, nx) + (int64_t)mirror(y + j, ny) * nx + (int64_t)mirror(z + l, nz) * nxy);
+    float med = win[0];
+    for (int h = 0; h < k; ++h) {
+        int rank = 0;
+        for (int l = 0; l < k; ++l) rank += (win[h] > win[l] || (win[h] == win[l] && h < l)) ? 1 : 0;
+        if (rank == k / 2) {
+            med = win[h];
+            break;
+        }
+    }
+    const int64_t n = x + (int64_t)y * nx + (int64_t)z * nxy;
+    const float d = __ldg(u + n) - med;
+    grad[n] += no_norm ? d * beta : d / (med + epps) * beta;
+}
+
+}  // namespace omb
+
+extern "C" int omb_mrp_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx,
+                                int32_t my, int32_t mz, float epps, float beta, int32_t no_norm, void *stream) {
+    using namespace omb;
+    if (!u || !grad) return set_error(OMB_ERR_INVALID, "u/grad pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    if (mx < 0 || my < 0 || mz < 0 || (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1) > kMrpMax)
+        return set_error(OMB_ERR_UNSUPPORTED, "MRP windows of more than 125 voxels are not built");
+    if (mx > nx || my > ny || mz > nz) return set_error(OMB_ERR_INVALID, "MRP window larger than the image");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    k_mrp_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, mx, my, mz, epps, beta, no_norm);
+    OMB_LAUNCH_CHECK("MRP gradient launch");
+    return OMB_OK;
+}

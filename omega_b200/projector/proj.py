@@ -140,6 +140,9 @@ class projectorClass:
     Quad = False
     Huber = False
     huber_delta = 1.
+    # median root prior (proj.py MRP, med_no_norm)
+    MRP = False
+    med_no_norm = False
     # non-local priors (proj.py:329-349, 434-436, 454)
     NLM = False
     NLTV = False

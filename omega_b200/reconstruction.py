@@ -306,10 +306,12 @@ def reconstructions_main(options):
     method = chosen[0]
     quad, huber = bool(getattr(options, 'Quad', False)), bool(getattr(options, 'Huber', False))
     nlm = bool(getattr(options, 'NLM', False))
-    n_priors = int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm)
+    mrp = bool(getattr(options, 'MRP', False))
+    n_priors = int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp)
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
-        raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber or options.NLM')
+        raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM or '
+                                  'options.MRP')
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
         raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
@@ -372,7 +374,13 @@ def reconstructions_main(options):
     keep = []
     if prior:
         p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
-                   (_native.OMB_PRIOR_NLM if nlm else (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER)))
+                   (_native.OMB_PRIOR_NLM if nlm else
+                    (_native.OMB_PRIOR_MRP if mrp else
+                     (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))))
+        if mrp:
+            # the median window is Ndx / Ndy / Ndz (priors.h:371-375)
+            p.prior_g[0], p.prior_g[1], p.prior_g[2] = int(options.Ndx), int(options.Ndy), int(options.Ndz)
+            p.mrp_no_norm = 1 if getattr(options, 'med_no_norm', False) else 0
         if nlm:
             # search window Ndx / Ndy / Ndz, patch Nlx / Nly / Nlz, h = NLMsigma^2 (libHeader.h:1285-1286;
             # ProjectorClass.h:841-870), gamma = RDP_gamma, GGMRF p / q / c

@@ -11,7 +11,10 @@ steps around the projectors, for the parity tests:
   image read clamped to its edges (the texture sampler of the reference's
   kernel path), and, with cpu_mode, the reference CPU function NLMFunc
   (source/cpp/NLM.h:15-142: interior voxels only, weight sum 1 / (sum +
-  epps), NLTV's squared sum from 0), which oracle/_ref exports and pins.
+  epps), NLTV's squared sum from 0), which oracle/_ref exports and pins;
+* mrp_gradient: the median root prior (priors.h:4-25) on the symmetric
+  padding; its median equals the reference CPU medianFilter3D (MRP.h),
+  which oracle/_ref exports.
 """
 import numpy as np
 
@@ -138,3 +141,26 @@ def nlm_gradient(u, shape, gaussian, sw, pw, h, epps, nl_type, gamma=10.0, ggmrf
         mask[az:nz - az, ay:ny - ay, ax:nx - ax] = True
         out = np.where(mask, out, 0.0)
     return out.ravel()
+
+
+def mrp_gradient(u, shape, m, beta, epps, no_norm=False):
+    """Median root prior gradient (priors.h:4-25): beta (u - med) / (med + epps)
+    (no_norm: beta (u - med)), med the median of the (2m+1)^3-type window of u
+    padded symmetrically (functions.hpp:216-260)."""
+    nx, ny, nz = shape
+    mx, my, mz = (int(v) for v in m)
+    U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
+    P = np.pad(U, ((mz, mz), (my, my), (mx, mx)), mode='symmetric')
+    stack = [P[mz + k:mz + k + nz, my + j:my + j + ny, mx + i:mx + i + nx]
+             for i in range(-mx, mx + 1) for j in range(-my, my + 1) for k in range(-mz, mz + 1)]
+    med = np.median(np.stack(stack), axis=0)
+    d = U - med
+    return (beta * d if no_norm else d / (med + epps) * beta).ravel()
+
+
+def padded_symmetric(u, shape, m):
+    """u padded by the window on every side, x fastest (the median filter's input)."""
+    nx, ny, nz = shape
+    mx, my, mz = (int(v) for v in m)
+    U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
+    return np.ascontiguousarray(np.pad(U, ((mz, mz), (my, my), (mx, mx)), mode='symmetric').ravel())

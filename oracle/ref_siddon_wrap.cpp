@@ -16,6 +16,7 @@
 
 #include "projector_functions.h"
 #include "NLM.h"
+#include "MRP.h"
 
 template <typename T>
 static int run(int fp, uint32_t nx, uint32_t ny, uint32_t nz, T dx, T dy, T dz, T bx, T by, T bz, uint32_t n_rows,
@@ -167,6 +168,13 @@ int ref_nlm_d(double *grad, const double *u_ref, const double *u, const double *
               int32_t type, double gamma, double epps, double p, double q, double c, int32_t anatomical) {
     NLMFunc<double>(grad, u_ref, u, gaussian, sx, sy, sz, px, py, pz, nx, ny, nz, (int32_t)(nx * ny), h, type, gamma,
                     epps, p, q, c, anatomical != 0);
+    return 0;
+}
+/* The reference's CPU median filter (MRP.h medianFilter3D) of an image padded
+ * by the window on every side (x fastest, padded sizes nx + 2 sx, ...). */
+int ref_median_d(const double *padded, double *out, int32_t nx, int32_t ny, int32_t nz, int32_t sx, int32_t sy,
+                 int32_t sz) {
+    medianFilter3D<double>(padded, out, nx, ny, nz, nx, ny, nz, sx, sy, sz);
     return 0;
 }
 int ref_siddon_d(int fp, uint32_t nx, uint32_t ny, uint32_t nz, double dx, double dy, double dz, double bx, double by,

@@ -1,0 +1,74 @@
+"""Median root prior: the median pinned against the reference's CPU
+medianFilter3D (oracle/_ref, MRP.h), the CUDA gradient against the
+restatement, and OSL-OSEM with MRP."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import image_oracle as io
+from oracle import oracle as orc
+
+SHAPE = (12, 11, 9)
+
+
+@pytest.mark.parametrize("m", [(1, 1, 1), (2, 1, 1), (1, 1, 0)])
+def test_median_matches_reference(m):
+    if orc.ref_lib() is None:
+        pytest.skip("oracle/_ref not built")
+    L = orc.ref_lib()
+    P = ctypes.POINTER(ctypes.c_double)
+    i32 = ctypes.c_int32
+    L.ref_median_d.argtypes = [P, P, i32, i32, i32, i32, i32, i32]
+    rng = np.random.default_rng(sum(m))
+    u = np.round(rng.uniform(0.5, 1.5, int(np.prod(SHAPE))), 2)   # rounded: ties in most windows
+    pad = io.padded_symmetric(u, SHAPE, m)
+    med = np.zeros(u.size)
+    L.ref_median_d(pad.ctypes.data_as(P), med.ctypes.data_as(P), *SHAPE, *m)
+    # the restatement's gradient with no_norm and beta 1 is u - median
+    got = u - io.mrp_gradient(u, SHAPE, m, 1.0, 1e-8, no_norm=True)
+    assert np.array_equal(got, med)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m,no_norm", [((1, 1, 1), False), ((2, 1, 1), True), ((1, 1, 0), False)])
+def test_kernel_matches_restatement(cuda, m, no_norm):
+    import torch
+    from omega_b200 import _native
+    from omega_b200.reconstruction import _stream
+    rng = np.random.default_rng(3)
+    n = int(np.prod(SHAPE))
+    u = np.round(rng.uniform(0.5, 1.5, n), 2).astype(np.float32)
+    U = torch.tensor(u, device=cuda)
+    out = torch.full((n,), 0.5, device=cuda)
+    _native.call("omb_mrp_gradient", ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(out.data_ptr()), *SHAPE, *m,
+                 1e-8, 0.3, 1 if no_norm else 0, _stream(cuda))
+    want = 0.5 + io.mrp_gradient(u.astype(np.float64), SHAPE, m, 0.3, 1e-8, no_norm=no_norm)
+    assert np.max(np.abs(out.cpu().numpy() - want)) < 1e-6
+
+
+@pytest.mark.gpu
+def test_builtin_osl_osem_with_mrp(cuda):
+    from conftest import make_options
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(8)
+    full = make_options("pet_mini")
+    full.subsets, full.subsetType = 1, 8
+    full.addProjector()
+    y = rng.poisson(orc.forward(orc.Geometry(full), rng.uniform(0.5, 2.0, g.n_img), 0) * 200).astype(np.float32) / 200
+    o.SinM = y.copy()
+    o.OSL_OSEM = True
+    o.MRP = True
+    o.beta = 0.01
+    o.Niter = 2
+    out, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    shape = (g.nx, g.ny, g.nz)
+    nd = (int(o.Ndx), int(o.Ndy), int(o.Ndz))
+    ref = orc.osem(g, ys, np.ones(g.n_img), 2, prior_grad=lambda v: io.mrp_gradient(v, shape, nd, 0.01, g.epps))
+    x = out.ravel(order='F')
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    assert orc.rel_l2(ref, orc.osem(g, ys, np.ones(g.n_img), 2)) > 1e-4
