@@ -312,7 +312,8 @@ typedef enum omb_prior {
     OMB_PRIOR_QUAD = 2,     /* options.Quad: the quadratic window (prior_window) applied with mirrored edges */
     OMB_PRIOR_HUBER = 3,    /* options.Huber: the same with the gradient clamped to +-huber_delta */
     OMB_PRIOR_NLM = 4,      /* options.NLM (with NLTV / NLM_MRP / NLRD / NLLange / NLGGMRF): omb_nlm_gradient */
-    OMB_PRIOR_MRP = 5       /* options.MRP: omb_mrp_gradient over the prior_g window (Ndx, Ndy, Ndz) */
+    OMB_PRIOR_MRP = 5,      /* options.MRP: omb_mrp_gradient over the prior_g window (Ndx, Ndy, Ndz) */
+    OMB_PRIOR_TV = 6        /* options.TV with a MAP algorithm other than PDHG: omb_tv_gradient, tv_smoothing */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -371,6 +372,14 @@ int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const fl
  */
 int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
                    const float *du, float *work_meas, float *work_img, void *stream);
+
+/*
+ * Smoothed TV gradient (priors.h:404-409, TVKernel auxKernels.cl:1733-1990,
+ * plain TV; neighbours outside the image read the edge voxel): grad += beta *
+ * grad TV(u) with the smoothing `smooth` (options.TVsmoothing).
+ */
+int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float beta, float smooth,
+                    void *stream);
 
 /*
  * Median root prior gradient (priors.h:4-25, medianFilter3D auxKernels.cl:

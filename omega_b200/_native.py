@@ -135,6 +135,7 @@ OMB_PRIOR_QUAD = 2
 OMB_PRIOR_HUBER = 3
 OMB_PRIOR_NLM = 4
 OMB_PRIOR_MRP = 5
+OMB_PRIOR_TV = 6
 
 
 class Tuning(ctypes.Structure):
@@ -220,6 +221,8 @@ EXPORTS = [
     ("omb_precond_image", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_void_p]),
+    ("omb_tv_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_void_p]),
     ("omb_mrp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p]),

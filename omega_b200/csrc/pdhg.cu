@@ -27,6 +27,39 @@ __device__ __forceinline__ float tv_at(const float *__restrict__ u, int x, int y
     return __ldg(u + x + (int64_t)y * nx + (int64_t)z * nx * ny);
 }
 
+// Smoothed isotropic TV gradient at voxel (i, j, k) (TVKernel, plain TV).
+__device__ __forceinline__ float tv_grad(const float *__restrict__ x, int i, int j, int k, int nx, int ny, int nz,
+                                         float smooth) {
+    const float c = tv_at(x, i, j, k, nx, ny, nz);
+    const float px = tv_at(x, i + 1, j, k, nx, ny, nz), py = tv_at(x, i, j + 1, k, nx, ny, nz),
+                pz = tv_at(x, i, j, k + 1, nx, ny, nz);
+    const float mx = tv_at(x, i - 1, j, k, nx, ny, nz), my = tv_at(x, i, j - 1, k, nx, ny, nz),
+                mz = tv_at(x, i, j, k - 1, nx, ny, nz);
+    const float uix = tv_at(x, i - 1, j + 1, k, nx, ny, nz), uiy = tv_at(x, i - 1, j, k + 1, nx, ny, nz);
+    const float ujx = tv_at(x, i + 1, j - 1, k, nx, ny, nz), ujy = tv_at(x, i, j - 1, k + 1, nx, ny, nz);
+    const float ukx = tv_at(x, i + 1, j, k - 1, nx, ny, nz), uky = tv_at(x, i, j + 1, k - 1, nx, ny, nz);
+    const float a0 = px - c, a1 = py - c, a2 = pz - c;
+    const float p0 = sqrtf(a0 * a0 + a1 * a1 + a2 * a2 + smooth);
+    const float b0 = c - mx, b1 = uix - mx, b2 = uiy - mx;
+    const float p1 = sqrtf(b0 * b0 + b1 * b1 + b2 * b2 + smooth);
+    const float c0 = ujx - my, c1 = c - my, c2 = ujy - my;
+    const float p2 = sqrtf(c0 * c0 + c1 * c1 + c2 * c2 + smooth);
+    const float d0 = ukx - mz, d1 = uky - mz, d2 = c - mz;
+    const float p3 = sqrtf(d0 * d0 + d1 * d1 + d2 * d2 + smooth);
+    return (3.f * c - px - py - pz) / p0 + (c - mx) / p1 + (c - my) / p2 + (c - mz) / p3 + 1e-7f;
+}
+
+// grad += beta * the TV gradient (the TV prior of the one-step-late and
+// relaxed algorithms, priors.h:404-409).
+__global__ void __launch_bounds__(256) k_tv_gradient(const float *__restrict__ x, float *__restrict__ grad, int nx,
+                                                     int ny, int nz, float beta, float smooth) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nx || j >= ny || k >= nz) return;
+    grad[i + (int64_t)j * nx + (int64_t)k * nx * ny] += beta * tv_grad(x, i, j, k, nx, ny, nz, smooth);
+}
+
 // Primal step fused with the TV gradient: reads x (stencil), rhs and u,
 // writes u and the extrapolated image into x_out (x_out != x).
 __global__ void __launch_bounds__(256) k_pdhg_primal_tv(const float *__restrict__ x, const float *__restrict__ rhs,
@@ -38,26 +71,7 @@ __global__ void __launch_bounds__(256) k_pdhg_primal_tv(const float *__restrict_
     const int k = blockIdx.z;
     if (i >= nx || j >= ny || k >= nz) return;
     const int64_t n = i + (int64_t)j * nx + (int64_t)k * nx * ny;
-    float g = 0.f;
-    if (beta != 0.f) {
-        const float c = tv_at(x, i, j, k, nx, ny, nz);
-        const float px = tv_at(x, i + 1, j, k, nx, ny, nz), py = tv_at(x, i, j + 1, k, nx, ny, nz),
-                    pz = tv_at(x, i, j, k + 1, nx, ny, nz);
-        const float mx = tv_at(x, i - 1, j, k, nx, ny, nz), my = tv_at(x, i, j - 1, k, nx, ny, nz),
-                    mz = tv_at(x, i, j, k - 1, nx, ny, nz);
-        const float uix = tv_at(x, i - 1, j + 1, k, nx, ny, nz), uiy = tv_at(x, i - 1, j, k + 1, nx, ny, nz);
-        const float ujx = tv_at(x, i + 1, j - 1, k, nx, ny, nz), ujy = tv_at(x, i, j - 1, k + 1, nx, ny, nz);
-        const float ukx = tv_at(x, i + 1, j, k - 1, nx, ny, nz), uky = tv_at(x, i, j + 1, k - 1, nx, ny, nz);
-        const float a0 = px - c, a1 = py - c, a2 = pz - c;
-        const float p0 = sqrtf(a0 * a0 + a1 * a1 + a2 * a2 + smooth);
-        const float b0 = c - mx, b1 = uix - mx, b2 = uiy - mx;
-        const float p1 = sqrtf(b0 * b0 + b1 * b1 + b2 * b2 + smooth);
-        const float c0 = ujx - my, c1 = c - my, c2 = ujy - my;
-        const float p2 = sqrtf(c0 * c0 + c1 * c1 + c2 * c2 + smooth);
-        const float d0 = ukx - mz, d1 = uky - mz, d2 = c - mz;
-        const float p3 = sqrtf(d0 * d0 + d1 * d1 + d2 * d2 + smooth);
-        g = beta * ((3.f * c - px - py - pz) / p0 + (c - mx) / p1 + (c - my) / p2 + (c - mz) / p3 + 1e-7f);
-    }
+    const float g = beta != 0.f ? beta * tv_grad(x, i, j, k, nx, ny, nz, smooth) : 0.f;
     const float r = __ldg(rhs + n) + g;
     const float uprev = u[n];
     float unew = uprev - tau * r;
@@ -155,3 +169,16 @@ int normalize_into(float *x, const float *b, int64_t n, const double *dots, cuda
 }
 
 }  // namespace omb
+
+extern "C" int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float beta,
+                               float smooth, void *stream) {
+    using namespace omb;
+    if (!u || !grad) return set_error(OMB_ERR_INVALID, "u/grad pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    k_tv_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, beta, smooth);
+    OMB_LAUNCH_CHECK("TV gradient launch");
+    return OMB_OK;
+}

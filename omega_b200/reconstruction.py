@@ -307,11 +307,12 @@ def reconstructions_main(options):
     quad, huber = bool(getattr(options, 'Quad', False)), bool(getattr(options, 'Huber', False))
     nlm = bool(getattr(options, 'NLM', False))
     mrp = bool(getattr(options, 'MRP', False))
-    n_priors = int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp)
+    tvp = bool(getattr(options, 'TV', False)) and not options.PDHG   # TV as a prior of the MAP algorithms
+    n_priors = int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp)
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
-        raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM or '
-                                  'options.MRP')
+        raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM, '
+                                  'options.MRP or options.TV')
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
         raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
@@ -376,7 +377,8 @@ def reconstructions_main(options):
         p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
                    (_native.OMB_PRIOR_NLM if nlm else
                     (_native.OMB_PRIOR_MRP if mrp else
-                     (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))))
+                     (_native.OMB_PRIOR_TV if tvp else
+                      (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER)))))
         if mrp:
             # the median window is Ndx / Ndy / Ndz (priors.h:371-375)
             p.prior_g[0], p.prior_g[1], p.prior_g[2] = int(options.Ndx), int(options.Ndy), int(options.Ndz)

@@ -72,3 +72,55 @@ def test_builtin_osl_osem_with_mrp(cuda):
     x = out.ravel(order='F')
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
     assert orc.rel_l2(ref, orc.osem(g, ys, np.ones(g.n_img), 2)) > 1e-4
+
+
+@pytest.mark.gpu
+def test_tv_gradient_kernel_matches_oracle(cuda):
+    import torch
+    from omega_b200 import _native
+    from omega_b200.reconstruction import _stream
+    rng = np.random.default_rng(4)
+    n = int(np.prod(SHAPE))
+    u = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    U = torch.tensor(u, device=cuda)
+    out = torch.full((n,), 0.5, device=cuda)
+    _native.call("omb_tv_gradient", ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(out.data_ptr()), *SHAPE, 0.3,
+                 1e-4, _stream(cuda))
+    want = 0.5 + orc.tv_gradient(u.astype(np.float64), SHAPE, 1e-4, 0.3)
+    assert orc.rel_l2(out.cpu().numpy() - 0.5, want - 0.5) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["OSL_OSEM", "BSREM"])
+def test_builtin_with_tv_prior(cuda, method):
+    from conftest import make_options
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(9)
+    full = make_options("pet_mini")
+    full.subsets, full.subsetType = 1, 8
+    full.addProjector()
+    y = rng.poisson(orc.forward(orc.Geometry(full), rng.uniform(0.5, 2.0, g.n_img), 0) * 200).astype(np.float32) / 200
+    o.SinM = y.copy()
+    setattr(o, method, True)
+    o.TV = True
+    o.TVsmoothing = 1e-2
+    o.beta = 0.002
+    o.Niter = 2
+    lam = np.array([0.2, 0.12], np.float32)
+    if method == "BSREM":
+        o.lambdaN = lam
+    out, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    shape = (g.nx, g.ny, g.nz)
+
+    def grad(v):
+        return orc.tv_gradient(v, shape, 1e-2, 0.002)
+    if method == "OSL_OSEM":
+        ref = orc.osem(g, ys, np.ones(g.n_img), 2, prior_grad=grad)
+    else:
+        ref = orc.relaxed(g, ys, np.ones(g.n_img), 2, "BSREM", lam=lam, prior_grad=grad)
+    x = out.ravel(order='F')
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
