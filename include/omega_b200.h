@@ -313,7 +313,8 @@ typedef enum omb_prior {
     OMB_PRIOR_HUBER = 3,    /* options.Huber: the same with the gradient clamped to +-huber_delta */
     OMB_PRIOR_NLM = 4,      /* options.NLM (with NLTV / NLM_MRP / NLRD / NLLange / NLGGMRF): omb_nlm_gradient */
     OMB_PRIOR_MRP = 5,      /* options.MRP: omb_mrp_gradient over the prior_g window (Ndx, Ndy, Ndz) */
-    OMB_PRIOR_TV = 6        /* options.TV with a MAP algorithm other than PDHG: omb_tv_gradient, tv_smoothing */
+    OMB_PRIOR_TV = 6,       /* options.TV with a MAP algorithm other than PDHG: omb_tv_gradient, tv_smoothing */
+    OMB_PRIOR_GGMRF = 7     /* options.GGMRF: omb_ggmrf_gradient over prior_g with ggmrf_weights and ggmrf[3] */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -353,6 +354,7 @@ typedef struct omb_recon_params {
     int32_t precond;          /* PKMA / MRAMLA / MBSREM image preconditioner: 0 none, 1 type 0 (rhs / D), 2 type 1
                                  (rhs * x / D), see omb_precond_image */
     int32_t mrp_no_norm;      /* MRP: options.med_no_norm */
+    const float *ggmrf_weights;/* GGMRF: device, the neighbours' weights (centre left out, z fastest) */
 } omb_recon_params;
 
 /*
@@ -380,6 +382,16 @@ int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
  */
 int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float beta, float smooth,
                     void *stream);
+
+/*
+ * GGMRF prior gradient (GGMRFKernel, auxKernels.cl:878-980; the image read
+ * clamped to its edges): grad += beta * sum_k w_k |d|^(p-1) / (1 + |d/c|^(p-q))
+ * (p - pqc |d|^(p-q) / (1 + |d/c|^(p-q))) sign(d), d = u_j - u_k, over the
+ * (2sx+1)(2sy+1)(2sz+1) - 1 neighbours in the order x outermost, z fastest,
+ * pqc = (p - q) / c^(p-q); `weights` device (quadWeights of the GGMRF branch).
+ */
+int omb_ggmrf_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t sx, int32_t sy,
+                       int32_t sz, const float *weights, float p, float q, float c, float beta, void *stream);
 
 /*
  * Median root prior gradient (priors.h:4-25, medianFilter3D auxKernels.cl:

@@ -117,6 +117,7 @@ class ReconParams(ctypes.Structure):
         ("nlm_adaptive_s", ctypes.c_float),
         ("precond", ctypes.c_int32),
         ("mrp_no_norm", ctypes.c_int32),
+        ("ggmrf_weights", ctypes.c_void_p),
     ]
 
 
@@ -136,6 +137,7 @@ OMB_PRIOR_HUBER = 3
 OMB_PRIOR_NLM = 4
 OMB_PRIOR_MRP = 5
 OMB_PRIOR_TV = 6
+OMB_PRIOR_GGMRF = 7
 
 
 class Tuning(ctypes.Structure):
@@ -221,6 +223,10 @@ EXPORTS = [
     ("omb_precond_image", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_void_p]),
+    ("omb_ggmrf_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                          ctypes.c_float, ctypes.c_void_p]),
     ("omb_tv_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_void_p]),
     ("omb_mrp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,

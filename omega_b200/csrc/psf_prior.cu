@@ -286,3 +286,60 @@ extern "C" int omb_mrp_gradient(const float *u, float *grad, int32_t nx, int32_t
     OMB_LAUNCH_CHECK("MRP gradient launch");
     return OMB_OK;
 }
+
+namespace omb {
+
+// GGMRF prior (GGMRFKernel, auxKernels.cl:878-980; the image read clamped to
+// its edges): grad += beta * sum_k w_k |d|^(p-1) / (1 + |d / c|^(p-q))
+//   * (p - pqc |d / c|^(p-q) c^(p-q) / (1 + |d / c|^(p-q))) * sign(d),
+// d = u_j - u_k over the neighbours (x outermost, z fastest, centre skipped),
+// pqc = (p - q) / c^(p-q) (libHeader.h:1180), terms with d = 0 left out.
+__global__ void k_ggmrf_gradient(const float *__restrict__ u, float *__restrict__ grad, int nx, int ny, int nz, int sx,
+                                 int sy, int sz, const float *__restrict__ w, float p, float q, float c, float pqc,
+                                 float beta) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const int64_t nxy = (int64_t)nx * ny;
+    const int64_t n = x + (int64_t)y * nx + (int64_t)z * nxy;
+    const float uj = __ldg(u + n);
+    const float cpq = powf(c, p - q);
+    float out = 0.f;
+    int uu = 0;
+    for (int i = -sx; i <= sx; ++i)
+        for (int j = -sy; j <= sy; ++j)
+            for (int k = -sz; k <= sz; ++k) {
+                if (i == 0 && j == 0 && k == 0) continue;
+                const float uk =
+                    __ldg(u + clampi(x + i, nx) + (int64_t)clampi(y + j, ny) * nx + (int64_t)clampi(z + k, nz) * nxy);
+                const float d = uj - uk;
+                if (d != 0.f) {
+                    const float dcpq = powf(fabsf(d / c), p - q);
+                    const float dpq = 1.f + dcpq;
+                    out += __ldg(w + uu) * (powf(fabsf(d), p - 1.f) / dpq) * (p - pqc * ((dcpq * cpq) / dpq)) * sgnn(d);
+                }
+                ++uu;
+            }
+    grad[n] += beta * out;
+}
+
+}  // namespace omb
+
+extern "C" int omb_ggmrf_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t sx,
+                                  int32_t sy, int32_t sz, const float *weights, float p, float q, float c, float beta,
+                                  void *stream) {
+    using namespace omb;
+    if (!u || !grad || !weights) return set_error(OMB_ERR_INVALID, "u/grad/weights pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    if (sx < 0 || sy < 0 || sz < 0 || sx > 8 || sy > 8 || sz > 8) return set_error(OMB_ERR_INVALID, "GGMRF window 0..8");
+    if (!(c > 0.f)) return set_error(OMB_ERR_INVALID, "GGMRF needs c > 0");
+    const float pqc = (p - q) / powf(c, p - q);
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    k_ggmrf_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, sx, sy, sz, weights, p, q, c, pqc,
+                                                                beta);
+    OMB_LAUNCH_CHECK("GGMRF gradient launch");
+    return OMB_OK;
+}

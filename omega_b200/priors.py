@@ -104,3 +104,25 @@ def nlm_type(options):
     if getattr(options, 'NLGGMRF', False):
         return 6
     return 0
+
+
+def ggmrf_weights(options):
+    """GGMRF neighbour weights (computeWeights' GGMRF branch + quadWeights,
+    prepass.py:661-682, 703-730): 1 / distance over the offsets x from +Nd
+    down to -Nd (outermost), then y, then z (fastest), normalised by their
+    sum, the centre left out; float32.  Built for cubic neighbourhoods
+    (Ndx = Ndy = Ndz) of a 3-D image, the case the reference's branch forms
+    consistently."""
+    nd = int(options.Ndx)
+    if int(options.Ndy) != nd or int(options.Ndz) != nd:
+        raise ValueError('GGMRF weights are built for Ndx = Ndy = Ndz')
+    dx = np.float32(np.ravel(options.FOVa_x)[0]) / np.float32(np.ravel(options.Nx)[0])
+    dy = np.float32(np.ravel(options.FOVa_y)[0]) / np.float32(np.ravel(options.Ny)[0])
+    dz = np.float32(np.ravel(options.axial_fov)[0]) / np.float32(np.ravel(options.Nz)[0])
+    r = np.arange(nd, -nd - 1, -1)
+    ox, oy, oz = np.meshgrid(r, r, r, indexing='ij')      # z fastest in C order
+    d = np.sqrt((oz * dz) ** 2 + (oy * dy) ** 2 + (ox * dx) ** 2).ravel().astype(np.float32)
+    with np.errstate(divide='ignore'):
+        w = (1.0 / d).astype(np.float32)
+    w = w / np.sum(w[~np.isinf(w)])
+    return w[~np.isinf(w)].astype(np.float32)

@@ -140,6 +140,8 @@ class projectorClass:
     Quad = False
     Huber = False
     huber_delta = 1.
+    # GGMRF prior (GGMRF_p / q / c below)
+    GGMRF = False
     # median root prior (proj.py MRP, med_no_norm)
     MRP = False
     med_no_norm = False

@@ -308,11 +308,12 @@ def reconstructions_main(options):
     nlm = bool(getattr(options, 'NLM', False))
     mrp = bool(getattr(options, 'MRP', False))
     tvp = bool(getattr(options, 'TV', False)) and not options.PDHG   # TV as a prior of the MAP algorithms
-    n_priors = int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp)
+    ggmrf = bool(getattr(options, 'GGMRF', False))
+    n_priors = int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp) + int(ggmrf)
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
         raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM, '
-                                  'options.MRP or options.TV')
+                                  'options.MRP, options.TV or options.GGMRF')
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
         raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
@@ -378,7 +379,16 @@ def reconstructions_main(options):
                    (_native.OMB_PRIOR_NLM if nlm else
                     (_native.OMB_PRIOR_MRP if mrp else
                      (_native.OMB_PRIOR_TV if tvp else
-                      (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER)))))
+                      (_native.OMB_PRIOR_GGMRF if ggmrf else
+                       (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))))))
+        if ggmrf:
+            from . import priors
+            gw = torch.from_numpy(priors.ggmrf_weights(options)).to(dev)
+            keep.append(gw)
+            p.ggmrf_weights = ctypes.c_void_p(gw.data_ptr())
+            p.prior_g[0], p.prior_g[1], p.prior_g[2] = int(options.Ndx), int(options.Ndy), int(options.Ndz)
+            p.ggmrf[0], p.ggmrf[1], p.ggmrf[2] = (float(options.GGMRF_p), float(options.GGMRF_q),
+                                                 float(options.GGMRF_c))
         if mrp:
             # the median window is Ndx / Ndy / Ndz (priors.h:371-375)
             p.prior_g[0], p.prior_g[1], p.prior_g[2] = int(options.Ndx), int(options.Ndy), int(options.Ndz)

@@ -164,3 +164,30 @@ def padded_symmetric(u, shape, m):
     mx, my, mz = (int(v) for v in m)
     U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
     return np.ascontiguousarray(np.pad(U, ((mz, mz), (my, my), (mx, mx)), mode='symmetric').ravel())
+
+
+def ggmrf_gradient(u, shape, s, weights, p, q, c, beta):
+    """GGMRF gradient (GGMRFKernel, auxKernels.cl:878-980) in FP64, edge-clamped
+    neighbours, weights in the kernel's order (x outermost, z fastest)."""
+    nx, ny, nz = shape
+    sx, sy, sz = (int(v) for v in s)
+    U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
+    P = np.pad(U, ((sz, sz), (sy, sy), (sx, sx)), mode='edge')
+    cpq = c ** (p - q)
+    pqc = (p - q) / c ** (p - q)
+    out = np.zeros_like(U)
+    uu = 0
+    for i in range(-sx, sx + 1):
+        for j in range(-sy, sy + 1):
+            for k in range(-sz, sz + 1):
+                if i == 0 and j == 0 and k == 0:
+                    continue
+                d = U - P[sz + k:sz + k + nz, sy + j:sy + j + ny, sx + i:sx + i + nx]
+                a = np.abs(d)
+                dcpq = np.abs(d / c) ** (p - q)
+                dpq = 1.0 + dcpq
+                with np.errstate(divide='ignore', invalid='ignore'):
+                    t = weights[uu] * (a ** (p - 1.0) / dpq) * (p - pqc * ((dcpq * cpq) / dpq)) * np.sign(d)
+                out += np.where(d != 0.0, t, 0.0)
+                uu += 1
+    return (beta * out).ravel()

@@ -134,6 +134,15 @@ def prior_weight_fixture(proj):
         prepass.huberWeights(o)
         out["huber_" + tag] = np.asarray(o.weights_huber, dtype=np.float32)
         out["weights_" + tag] = w
+    # GGMRF: the branch of computeWeights for it and quadWeights with options.GGMRF set
+    o = apply(proj.projectorClass(), CONFIGS["pet_mini"])
+    o.addProjector()
+    o.Ndx = o.Ndy = o.Ndz = 1
+    o.weights = np.empty(0, dtype=np.float32)
+    o.GGMRF = True
+    prepass.computeWeights(o, True)
+    prepass.quadWeights(o, True)
+    out["ggmrf_111"] = np.asarray(o.weights_quad, dtype=np.float32)
     np.savez_compressed(os.path.join(HERE, "priorw_pet_mini.npz"), **out)
     print("priorw_pet_mini", {k: v.shape for k, v in out.items()})
 
@@ -195,6 +204,9 @@ def main():
         return
     if sys.argv[1:] == ["nlm"]:
         nlm_fixture()
+        return
+    if sys.argv[1:] == ["priorw"]:
+        prior_weight_fixture(reference_projector())
         return
     proj = reference_projector()
     volume_fixture()

@@ -1,6 +1,8 @@
-"""Median root prior: the median pinned against the reference's CPU
-medianFilter3D (oracle/_ref, MRP.h), the CUDA gradient against the
-restatement, and OSL-OSEM with MRP."""
+"""Local priors: the median root prior (its median pinned against the
+reference's CPU medianFilter3D, oracle/_ref MRP.h), the TV prior of the MAP
+algorithms and GGMRF (weights pinned against the reference's prepass,
+golden priorw_pet_mini.npz): CUDA gradients against the restatements and
+OSL-OSEM / BSREM with each prior."""
 import ctypes
 
 import numpy as np
@@ -124,3 +126,60 @@ def test_builtin_with_tv_prior(cuda, method):
         ref = orc.relaxed(g, ys, np.ones(g.n_img), 2, "BSREM", lam=lam, prior_grad=grad)
     x = out.ravel(order='F')
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+
+
+def test_ggmrf_weights_match_reference():
+    from conftest import make_options
+    from omega_b200 import priors
+    import os
+    f = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "priorw_pet_mini.npz"))
+    o = make_options("pet_mini")
+    o.Ndx = o.Ndy = o.Ndz = 1
+    assert np.array_equal(priors.ggmrf_weights(o), f["ggmrf_111"])
+
+
+@pytest.mark.gpu
+def test_ggmrf_kernel_matches_restatement(cuda):
+    import torch
+    from omega_b200 import _native
+    from omega_b200.reconstruction import _stream
+    rng = np.random.default_rng(5)
+    n = int(np.prod(SHAPE))
+    u = np.round(rng.uniform(0.5, 1.5, n), 2).astype(np.float32)     # equal neighbours: the d = 0 skip
+    w = rng.uniform(0.01, 0.1, 26).astype(np.float32)
+    U, W = torch.tensor(u, device=cuda), torch.tensor(w, device=cuda)
+    out = torch.full((n,), 0.5, device=cuda)
+    _native.call("omb_ggmrf_gradient", ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(out.data_ptr()), *SHAPE,
+                 1, 1, 1, ctypes.c_void_p(W.data_ptr()), 2.0, 1.5, 0.05, 0.3, _stream(cuda))
+    want = 0.5 + io.ggmrf_gradient(u.astype(np.float64), SHAPE, (1, 1, 1), w.astype(np.float64), 2.0, 1.5, 0.05, 0.3)
+    assert orc.rel_l2(out.cpu().numpy() - 0.5, want - 0.5) < 2e-5
+
+
+@pytest.mark.gpu
+def test_builtin_osl_osem_with_ggmrf(cuda):
+    from conftest import make_options
+    from omega_b200 import priors
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(10)
+    full = make_options("pet_mini")
+    full.subsets, full.subsetType = 1, 8
+    full.addProjector()
+    y = rng.poisson(orc.forward(orc.Geometry(full), rng.uniform(0.5, 2.0, g.n_img), 0) * 200).astype(np.float32) / 200
+    o.SinM = y.copy()
+    o.OSL_OSEM = True
+    o.GGMRF = True
+    o.GGMRF_p, o.GGMRF_q, o.GGMRF_c = 2.0, 1.5, 0.05
+    o.beta = 0.005
+    o.Niter = 2
+    out, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    shape = (g.nx, g.ny, g.nz)
+    w = priors.ggmrf_weights(o).astype(np.float64)
+    ref = orc.osem(g, ys, np.ones(g.n_img), 2,
+                   prior_grad=lambda v: io.ggmrf_gradient(v, shape, (1, 1, 1), w, 2.0, 1.5, 0.05, 0.005))
+    x = out.ravel(order='F')
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    assert orc.rel_l2(ref, orc.osem(g, ys, np.ones(g.n_img), 2)) > 1e-4
