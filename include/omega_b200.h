@@ -314,7 +314,8 @@ typedef enum omb_prior {
     OMB_PRIOR_NLM = 4,      /* options.NLM (with NLTV / NLM_MRP / NLRD / NLLange / NLGGMRF): omb_nlm_gradient */
     OMB_PRIOR_MRP = 5,      /* options.MRP: omb_mrp_gradient over the prior_g window (Ndx, Ndy, Ndz) */
     OMB_PRIOR_TV = 6,       /* options.TV with a MAP algorithm other than PDHG: omb_tv_gradient, tv_smoothing */
-    OMB_PRIOR_GGMRF = 7     /* options.GGMRF: omb_ggmrf_gradient over prior_g with ggmrf_weights and ggmrf[3] */
+    OMB_PRIOR_GGMRF = 7,    /* options.GGMRF: omb_ggmrf_gradient over prior_g with ggmrf_weights and ggmrf[3] */
+    OMB_PRIOR_HYPERBOLIC = 8/* options.hyperbolic: omb_hyperbolic_gradient over prior_g with hyper_weights */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -355,6 +356,8 @@ typedef struct omb_recon_params {
                                  (rhs * x / D), see omb_precond_image */
     int32_t mrp_no_norm;      /* MRP: options.med_no_norm */
     const float *ggmrf_weights;/* GGMRF: device, the neighbours' weights (centre left out, z fastest) */
+    const float *hyper_weights;/* hyperbolic: device, options.weights_quad (centre left out, x fastest) */
+    float hyper_delta;        /* hyperbolic: options.hyperbolicDelta */
 } omb_recon_params;
 
 /*
@@ -392,6 +395,15 @@ int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t
  */
 int omb_ggmrf_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t sx, int32_t sy,
                        int32_t sz, const float *weights, float p, float q, float c, float beta, void *stream);
+
+/*
+ * Hyperbolic prior gradient (hyperbolicKernel, auxKernels.cl:1591-1688; the
+ * image read clamped to its edges): grad += beta * sum_k w_k t / delta /
+ * sqrt(t^2 + 1), t = (u_j - u_k) / delta, neighbours z outermost, x fastest,
+ * `weights` (device) the quadratic prior's normalised weights.
+ */
+int omb_hyperbolic_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t sx, int32_t sy,
+                            int32_t sz, const float *weights, float delta, float beta, void *stream);
 
 /*
  * Median root prior gradient (priors.h:4-25, medianFilter3D auxKernels.cl:

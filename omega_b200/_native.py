@@ -118,6 +118,8 @@ class ReconParams(ctypes.Structure):
         ("precond", ctypes.c_int32),
         ("mrp_no_norm", ctypes.c_int32),
         ("ggmrf_weights", ctypes.c_void_p),
+        ("hyper_weights", ctypes.c_void_p),
+        ("hyper_delta", ctypes.c_float),
     ]
 
 
@@ -138,6 +140,7 @@ OMB_PRIOR_NLM = 4
 OMB_PRIOR_MRP = 5
 OMB_PRIOR_TV = 6
 OMB_PRIOR_GGMRF = 7
+OMB_PRIOR_HYPERBOLIC = 8
 
 
 class Tuning(ctypes.Structure):
@@ -223,6 +226,9 @@ EXPORTS = [
     ("omb_precond_image", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_void_p]),
+    ("omb_hyperbolic_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                               ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                               ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_void_p]),
     ("omb_ggmrf_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                           ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,

@@ -343,3 +343,52 @@ extern "C" int omb_ggmrf_gradient(const float *u, float *grad, int32_t nx, int32
     OMB_LAUNCH_CHECK("GGMRF gradient launch");
     return OMB_OK;
 }
+
+namespace omb {
+
+// Hyperbolic prior (hyperbolicKernel, auxKernels.cl:1591-1688; the image read
+// clamped to its edges): grad += beta * sum_k w_k t_k / delta / sqrt(t_k^2 + 1),
+// t_k = (u_j - u_k) / delta, over the neighbours z outermost, x fastest.
+__global__ void k_hyperbolic_gradient(const float *__restrict__ u, float *__restrict__ grad, int nx, int ny, int nz,
+                                      int sx, int sy, int sz, const float *__restrict__ w, float delta, float beta) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const int64_t nxy = (int64_t)nx * ny;
+    const int64_t n = x + (int64_t)y * nx + (int64_t)z * nxy;
+    const float uj = __ldg(u + n);
+    const float inv = 1.f / delta;
+    float out = 0.f;
+    int uu = 0;
+    for (int k = -sz; k <= sz; ++k)
+        for (int j = -sy; j <= sy; ++j)
+            for (int i = -sx; i <= sx; ++i) {
+                if (i == 0 && j == 0 && k == 0) continue;
+                const float uk =
+                    __ldg(u + clampi(x + i, nx) + (int64_t)clampi(y + j, ny) * nx + (int64_t)clampi(z + k, nz) * nxy);
+                const float t = (uj - uk) * inv;
+                out += t * inv * rsqrtf(t * t + 1.f) * __ldg(w + uu++);
+            }
+    grad[n] += beta * out;
+}
+
+}  // namespace omb
+
+extern "C" int omb_hyperbolic_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t sx,
+                                       int32_t sy, int32_t sz, const float *weights, float delta, float beta,
+                                       void *stream) {
+    using namespace omb;
+    if (!u || !grad || !weights) return set_error(OMB_ERR_INVALID, "u/grad/weights pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    if (sx < 0 || sy < 0 || sz < 0 || sx > 8 || sy > 8 || sz > 8)
+        return set_error(OMB_ERR_INVALID, "hyperbolic prior window 0..8");
+    if (!(delta > 0.f)) return set_error(OMB_ERR_INVALID, "the hyperbolic prior needs delta > 0");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    k_hyperbolic_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, sx, sy, sz, weights, delta,
+                                                                     beta);
+    OMB_LAUNCH_CHECK("hyperbolic gradient launch");
+    return OMB_OK;
+}

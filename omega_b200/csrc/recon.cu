@@ -91,10 +91,12 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         const bool sub_prior = alg == OMB_RECON_MBSREM || (pkma && p->prior != 0);
         const bool need_prior = osl || map || sub_prior;
         const bool no_sens = ramla || pkma || mb;
-        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_GGMRF))
+        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_HYPERBOLIC))
             return set_error(OMB_ERR_INVALID, "unknown prior");
         if (need_prior && (p->prior == OMB_PRIOR_QUAD || p->prior == OMB_PRIOR_HUBER) && !p->prior_window)
             return set_error(OMB_ERR_INVALID, "the quadratic / Huber prior needs its window");
+        if (need_prior && p->prior == OMB_PRIOR_HYPERBOLIC && !p->hyper_weights)
+            return set_error(OMB_ERR_INVALID, "the hyperbolic prior needs its weights");
         if (need_prior && p->prior == OMB_PRIOR_GGMRF && !p->ggmrf_weights)
             return set_error(OMB_ERR_INVALID, "the GGMRF prior needs its weights");
         if (need_prior && p->prior == OMB_PRIOR_NLM && !p->nlm_gaussian)
@@ -158,6 +160,9 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                 return set_error(OMB_ERR_CUDA, "clearing the prior gradient failed");
             if (p->prior == OMB_PRIOR_RDP)
                 return omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
+            if (p->prior == OMB_PRIOR_HYPERBOLIC)
+                return omb_hyperbolic_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1],
+                                               p->prior_g[2], p->hyper_weights, p->hyper_delta, p->beta, stream);
             if (p->prior == OMB_PRIOR_GGMRF)
                 return omb_ggmrf_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1], p->prior_g[2],
                                           p->ggmrf_weights, p->ggmrf[0], p->ggmrf[1], p->ggmrf[2], p->beta, stream);

@@ -140,8 +140,10 @@ class projectorClass:
     Quad = False
     Huber = False
     huber_delta = 1.
-    # GGMRF prior (GGMRF_p / q / c below)
+    # GGMRF prior (GGMRF_p / q / c below); hyperbolic prior (proj.py:361)
     GGMRF = False
+    hyperbolic = False
+    hyperbolicDelta = 1.
     # median root prior (proj.py MRP, med_no_norm)
     MRP = False
     med_no_norm = False

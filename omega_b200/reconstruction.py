@@ -309,11 +309,13 @@ def reconstructions_main(options):
     mrp = bool(getattr(options, 'MRP', False))
     tvp = bool(getattr(options, 'TV', False)) and not options.PDHG   # TV as a prior of the MAP algorithms
     ggmrf = bool(getattr(options, 'GGMRF', False))
-    n_priors = int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp) + int(ggmrf)
+    hyper = bool(getattr(options, 'hyperbolic', False))
+    n_priors = (int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp) + int(ggmrf) +
+                int(hyper))
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
         raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM, '
-                                  'options.MRP, options.TV or options.GGMRF')
+                                  'options.MRP, options.TV, options.GGMRF or options.hyperbolic')
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
         raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
@@ -380,7 +382,19 @@ def reconstructions_main(options):
                     (_native.OMB_PRIOR_MRP if mrp else
                      (_native.OMB_PRIOR_TV if tvp else
                       (_native.OMB_PRIOR_GGMRF if ggmrf else
-                       (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))))))
+                       (_native.OMB_PRIOR_HYPERBOLIC if hyper else
+                        (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER)))))))
+        if hyper:
+            # the quadratic prior's normalised weights and hyperbolicDelta (libHeader.h:1159-1162)
+            from . import priors
+            w = np.asarray(options.weights, dtype=np.float32) if np.size(options.weights) else \
+                priors.neighbourhood_weights(options)
+            wq = priors.normalised_weights(w) if not np.size(options.weights) else w[~np.isinf(w)]
+            hw = torch.from_numpy(np.ascontiguousarray(wq, dtype=np.float32)).to(dev)
+            keep.append(hw)
+            p.hyper_weights = ctypes.c_void_p(hw.data_ptr())
+            p.hyper_delta = float(getattr(options, 'hyperbolicDelta', 1.0))
+            p.prior_g[0], p.prior_g[1], p.prior_g[2] = int(options.Ndx), int(options.Ndy), int(options.Ndz)
         if ggmrf:
             from . import priors
             gw = torch.from_numpy(priors.ggmrf_weights(options)).to(dev)

@@ -191,3 +191,23 @@ def ggmrf_gradient(u, shape, s, weights, p, q, c, beta):
                 out += np.where(d != 0.0, t, 0.0)
                 uu += 1
     return (beta * out).ravel()
+
+
+def hyperbolic_gradient(u, shape, s, weights, delta, beta):
+    """Hyperbolic prior gradient (hyperbolicKernel, auxKernels.cl:1591-1688) in
+    FP64, edge-clamped neighbours, weights z outermost, x fastest."""
+    nx, ny, nz = shape
+    sx, sy, sz = (int(v) for v in s)
+    U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
+    P = np.pad(U, ((sz, sz), (sy, sy), (sx, sx)), mode='edge')
+    out = np.zeros_like(U)
+    uu = 0
+    for k in range(-sz, sz + 1):
+        for j in range(-sy, sy + 1):
+            for i in range(-sx, sx + 1):
+                if i == 0 and j == 0 and k == 0:
+                    continue
+                t = (U - P[sz + k:sz + k + nz, sy + j:sy + j + ny, sx + i:sx + i + nx]) / delta
+                out += t / delta / np.sqrt(t * t + 1.0) * weights[uu]
+                uu += 1
+    return (beta * out).ravel()

@@ -183,3 +183,48 @@ def test_builtin_osl_osem_with_ggmrf(cuda):
     x = out.ravel(order='F')
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
     assert orc.rel_l2(ref, orc.osem(g, ys, np.ones(g.n_img), 2)) > 1e-4
+
+
+@pytest.mark.gpu
+def test_builtin_bsrem_with_hyperbolic(cuda):
+    import torch
+    from conftest import make_options
+    from omega_b200 import _native, priors
+    from omega_b200 import reconstruction as rec
+    from omega_b200.reconstruction import _stream
+    # the kernel alone
+    rng = np.random.default_rng(12)
+    n = int(np.prod(SHAPE))
+    u = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    w = rng.uniform(0.01, 0.1, 26).astype(np.float32)
+    U, W = torch.tensor(u, device=cuda), torch.tensor(w, device=cuda)
+    out = torch.full((n,), 0.5, device=cuda)
+    _native.call("omb_hyperbolic_gradient", ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(out.data_ptr()), *SHAPE,
+                 1, 1, 1, ctypes.c_void_p(W.data_ptr()), 0.2, 0.3, _stream(cuda))
+    want = 0.5 + io.hyperbolic_gradient(u.astype(np.float64), SHAPE, (1, 1, 1), w.astype(np.float64), 0.2, 0.3)
+    assert orc.rel_l2(out.cpu().numpy() - 0.5, want - 0.5) < 1e-5
+    # BSREM with it
+    o = make_options("pet_mini")
+    g = orc.Geometry(o)
+    full = make_options("pet_mini")
+    full.subsets, full.subsetType = 1, 8
+    full.addProjector()
+    y = rng.poisson(orc.forward(orc.Geometry(full), rng.uniform(0.5, 2.0, g.n_img), 0) * 200).astype(np.float32) / 200
+    o.SinM = y.copy()
+    o.BSREM = True
+    o.hyperbolic = True
+    o.hyperbolicDelta = 0.1
+    o.beta = 0.05
+    o.Niter = 2
+    lam = np.array([0.2, 0.12], np.float32)
+    o.lambdaN = lam
+    res, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    shape = (g.nx, g.ny, g.nz)
+    wq = priors.normalised_weights(priors.neighbourhood_weights(o)).astype(np.float64)
+    ref = orc.relaxed(g, ys, np.ones(g.n_img), 2, "BSREM", lam=lam,
+                      prior_grad=lambda v: io.hyperbolic_gradient(v, shape, (1, 1, 1), wq, 0.1, 0.05))
+    x = res.ravel(order='F')
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    assert orc.rel_l2(ref, orc.relaxed(g, ys, np.ones(g.n_img), 2, "RAMLA", lam=lam)) > 1e-4
