@@ -315,7 +315,8 @@ typedef enum omb_prior {
     OMB_PRIOR_MRP = 5,      /* options.MRP: omb_mrp_gradient over the prior_g window (Ndx, Ndy, Ndz) */
     OMB_PRIOR_TV = 6,       /* options.TV with a MAP algorithm other than PDHG: omb_tv_gradient, tv_smoothing */
     OMB_PRIOR_GGMRF = 7,    /* options.GGMRF: omb_ggmrf_gradient over prior_g with ggmrf_weights and ggmrf[3] */
-    OMB_PRIOR_HYPERBOLIC = 8/* options.hyperbolic: omb_hyperbolic_gradient over prior_g with hyper_weights */
+    OMB_PRIOR_HYPERBOLIC = 8,/* options.hyperbolic: omb_hyperbolic_gradient over prior_g with hyper_weights */
+    OMB_PRIOR_WMEAN = 9     /* options.weighted_mean, mean_type 1-3: omb_wmean_gradient over prior_g */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -358,6 +359,9 @@ typedef struct omb_recon_params {
     const float *ggmrf_weights;/* GGMRF: device, the neighbours' weights (centre left out, z fastest) */
     const float *hyper_weights;/* hyperbolic: device, options.weights_quad (centre left out, x fastest) */
     float hyper_delta;        /* hyperbolic: options.hyperbolicDelta */
+    const float *wmean_weights;/* weighted mean: device, options.weighted_weights (x fastest) */
+    int32_t wmean_type;       /* weighted mean: options.mean_type (1 arithmetic, 2 harmonic, 3 geometric); the
+                                 normalisation switch is mrp_no_norm (options.med_no_norm) */
 } omb_recon_params;
 
 /*
@@ -404,6 +408,16 @@ int omb_ggmrf_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int3
  */
 int omb_hyperbolic_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t sx, int32_t sy,
                             int32_t sz, const float *weights, float delta, float beta, void *stream);
+
+/*
+ * Weighted-mean prior gradient, mean types 1-3 (priors.h:99-160): m = the
+ * weighted arithmetic / harmonic / geometric mean of the mirrored
+ * (2mx+1)(2my+1)(2mz+1) window (weights / wsum applied as a convolution);
+ * grad += beta * (u - m) / (m + epps), or beta * (u - m) with no_norm.
+ */
+int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx, int32_t my,
+                       int32_t mz, const float *weights, float wsum, int32_t mean_type, float epps, float beta,
+                       int32_t no_norm, void *stream);
 
 /*
  * Median root prior gradient (priors.h:4-25, medianFilter3D auxKernels.cl:

@@ -120,6 +120,8 @@ class ReconParams(ctypes.Structure):
         ("ggmrf_weights", ctypes.c_void_p),
         ("hyper_weights", ctypes.c_void_p),
         ("hyper_delta", ctypes.c_float),
+        ("wmean_weights", ctypes.c_void_p),
+        ("wmean_type", ctypes.c_int32),
     ]
 
 
@@ -141,6 +143,7 @@ OMB_PRIOR_MRP = 5
 OMB_PRIOR_TV = 6
 OMB_PRIOR_GGMRF = 7
 OMB_PRIOR_HYPERBOLIC = 8
+OMB_PRIOR_WMEAN = 9
 
 
 class Tuning(ctypes.Structure):
@@ -226,6 +229,10 @@ EXPORTS = [
     ("omb_precond_image", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_map_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_void_p]),
+    ("omb_wmean_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_void_p, ctypes.c_float, ctypes.c_int32, ctypes.c_float,
+                                          ctypes.c_float, ctypes.c_int32, ctypes.c_void_p]),
     ("omb_hyperbolic_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                                ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_void_p]),

@@ -392,3 +392,56 @@ extern "C" int omb_hyperbolic_gradient(const float *u, float *grad, int32_t nx, 
     OMB_LAUNCH_CHECK("hyperbolic gradient launch");
     return OMB_OK;
 }
+
+namespace omb {
+
+// Weighted-mean prior, mean types 1-3 (Weighted_mean, priors.h:99-160 for
+// types 1-3): m = the weighted arithmetic (1), harmonic (2) or geometric (3)
+// mean of the (2mx+1)(2my+1)(2mz+1) window of u mirrored at its faces, the
+// weights w (x fastest) applied as a convolution (af::convolve3: the weight
+// of offset -o multiplies u(x + o)) and divided by wsum;
+// grad += beta * (u - m) / (m + epps), or beta * (u - m) with no_norm.
+__global__ void k_wmean_gradient(const float *__restrict__ u, float *__restrict__ grad, int nx, int ny, int nz, int mx,
+                                 int my, int mz, const float *__restrict__ w, float wsum, int mean_type, float epps,
+                                 float beta, int no_norm) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const int64_t nxy = (int64_t)nx * ny;
+    const int wx = 2 * mx + 1, wy = 2 * my + 1;
+    float acc = 0.f;
+    for (int k = -mz; k <= mz; ++k)
+        for (int j = -my; j <= my; ++j)
+            for (int i = -mx; i <= mx; ++i) {
+                const float v = __ldg(u + mirror(x + i, nx) + (int64_t)mirror(y + j, ny) * nx +
+                                      (int64_t)mirror(z + k, nz) * nxy);
+                const float wk = __ldg(w + (mx - i) + (my - j) * wx + (mz - k) * wx * wy) / wsum;
+                acc += wk * (mean_type == 2 ? 1.f / v : (mean_type == 3 ? logf(v) : v));
+            }
+    const float m = mean_type == 2 ? 1.f / acc : (mean_type == 3 ? expf(acc) : acc);
+    const int64_t n = x + (int64_t)y * nx + (int64_t)z * nxy;
+    const float d = __ldg(u + n) - m;
+    grad[n] += beta * (no_norm ? d : d / (m + epps));
+}
+
+}  // namespace omb
+
+extern "C" int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx,
+                                  int32_t my, int32_t mz, const float *weights, float wsum, int32_t mean_type,
+                                  float epps, float beta, int32_t no_norm, void *stream) {
+    using namespace omb;
+    if (!u || !grad || !weights) return set_error(OMB_ERR_INVALID, "u/grad/weights pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    if (mean_type < 1 || mean_type > 3) return set_error(OMB_ERR_UNSUPPORTED, "weighted mean types 1-3 are built");
+    if (mx < 0 || my < 0 || mz < 0 || mx > nx || my > ny || mz > nz)
+        return set_error(OMB_ERR_INVALID, "weighted mean window must fit one mirror of the image");
+    if (!(wsum != 0.f)) return set_error(OMB_ERR_INVALID, "weighted mean weights sum to 0");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    k_wmean_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, mx, my, mz, weights, wsum,
+                                                                mean_type, epps, beta, no_norm);
+    OMB_LAUNCH_CHECK("weighted mean gradient launch");
+    return OMB_OK;
+}

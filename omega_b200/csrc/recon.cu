@@ -91,10 +91,12 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         const bool sub_prior = alg == OMB_RECON_MBSREM || (pkma && p->prior != 0);
         const bool need_prior = osl || map || sub_prior;
         const bool no_sens = ramla || pkma || mb;
-        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_HYPERBOLIC))
+        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_WMEAN))
             return set_error(OMB_ERR_INVALID, "unknown prior");
         if (need_prior && (p->prior == OMB_PRIOR_QUAD || p->prior == OMB_PRIOR_HUBER) && !p->prior_window)
             return set_error(OMB_ERR_INVALID, "the quadratic / Huber prior needs its window");
+        if (need_prior && p->prior == OMB_PRIOR_WMEAN && !p->wmean_weights)
+            return set_error(OMB_ERR_INVALID, "the weighted mean prior needs its weights");
         if (need_prior && p->prior == OMB_PRIOR_HYPERBOLIC && !p->hyper_weights)
             return set_error(OMB_ERR_INVALID, "the hyperbolic prior needs its weights");
         if (need_prior && p->prior == OMB_PRIOR_GGMRF && !p->ggmrf_weights)
@@ -160,6 +162,9 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                 return set_error(OMB_ERR_CUDA, "clearing the prior gradient failed");
             if (p->prior == OMB_PRIOR_RDP)
                 return omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
+            if (p->prior == OMB_PRIOR_WMEAN)
+                return omb_wmean_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1], p->prior_g[2],
+                                          p->wmean_weights, 1.f, p->wmean_type, epps, p->beta, p->mrp_no_norm, stream);
             if (p->prior == OMB_PRIOR_HYPERBOLIC)
                 return omb_hyperbolic_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1],
                                                p->prior_g[2], p->hyper_weights, p->hyper_delta, p->beta, stream);

@@ -126,3 +126,17 @@ def ggmrf_weights(options):
         w = (1.0 / d).astype(np.float32)
     w = w / np.sum(w[~np.isinf(w)])
     return w[~np.isinf(w)].astype(np.float32)
+
+
+def weighted_mean_weights(options):
+    """weightedWeights (prepass.py:754-774): sqrt(2) * FOVa_x / Nx times the
+    distance weights, the centre set to weighted_center_weight, normalised to
+    sum 1; x fastest, float32.  options.weighted_weights when given."""
+    w = np.asarray(getattr(options, 'weighted_weights', np.empty(0)), dtype=np.float32).ravel(order='F')
+    if w.size == 0:
+        # float32 pitch, then FP64 (the reference's sqrt(2) is a float64 scalar) until the final cast
+        dist = np.float32(np.ravel(options.FOVa_x)[0]) / np.float32(np.ravel(options.Nx)[0])
+        w = np.sqrt(2.) * np.float64(dist) * neighbourhood_weights(options).astype(np.float64)
+        w[np.isinf(w)] = float(getattr(options, 'weighted_center_weight', 2.))
+        w = w / np.sum(w)
+    return np.ascontiguousarray(w, dtype=np.float32)

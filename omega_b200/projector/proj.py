@@ -144,6 +144,11 @@ class projectorClass:
     GGMRF = False
     hyperbolic = False
     hyperbolicDelta = 1.
+    # weighted-mean prior (proj.py:97, 160, 316)
+    weighted_mean = False
+    weighted_weights = np.empty(0, dtype=np.float32)
+    weighted_center_weight = 2.
+    mean_type = 4
     # median root prior (proj.py MRP, med_no_norm)
     MRP = False
     med_no_norm = False

@@ -310,12 +310,14 @@ def reconstructions_main(options):
     tvp = bool(getattr(options, 'TV', False)) and not options.PDHG   # TV as a prior of the MAP algorithms
     ggmrf = bool(getattr(options, 'GGMRF', False))
     hyper = bool(getattr(options, 'hyperbolic', False))
+    wmean = bool(getattr(options, 'weighted_mean', False))
     n_priors = (int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp) + int(ggmrf) +
-                int(hyper))
+                int(hyper) + int(wmean))
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
         raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM, '
-                                  'options.MRP, options.TV, options.GGMRF or options.hyperbolic')
+                                  'options.MRP, options.TV, options.GGMRF, options.hyperbolic or '
+                                  'options.weighted_mean')
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
         raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
@@ -383,7 +385,20 @@ def reconstructions_main(options):
                      (_native.OMB_PRIOR_TV if tvp else
                       (_native.OMB_PRIOR_GGMRF if ggmrf else
                        (_native.OMB_PRIOR_HYPERBOLIC if hyper else
-                        (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER)))))))
+                        (_native.OMB_PRIOR_WMEAN if wmean else
+                         (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))))))))
+        if wmean:
+            from . import priors
+            mt = int(getattr(options, 'mean_type', 4))
+            if mt not in (1, 2, 3):
+                raise ValueError('weighted_mean is built for mean_type 1 (arithmetic), 2 (harmonic) and 3 '
+                                 '(geometric)')
+            ww = torch.from_numpy(priors.weighted_mean_weights(options)).to(dev)
+            keep.append(ww)
+            p.wmean_weights = ctypes.c_void_p(ww.data_ptr())
+            p.wmean_type = mt
+            p.mrp_no_norm = 1 if getattr(options, 'med_no_norm', False) else 0
+            p.prior_g[0], p.prior_g[1], p.prior_g[2] = int(options.Ndx), int(options.Ndy), int(options.Ndz)
         if hyper:
             # the quadratic prior's normalised weights and hyperbolicDelta (libHeader.h:1159-1162)
             from . import priors

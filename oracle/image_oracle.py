@@ -211,3 +211,23 @@ def hyperbolic_gradient(u, shape, s, weights, delta, beta):
                 out += t / delta / np.sqrt(t * t + 1.0) * weights[uu]
                 uu += 1
     return (beta * out).ravel()
+
+
+def wmean_gradient(u, shape, m, weights, mean_type, beta, epps, no_norm=False):
+    """Weighted-mean prior gradient, types 1-3 (priors.h:99-160) in FP64: the
+    weighted arithmetic / harmonic / geometric mean of the symmetric-padded
+    window, weights applied as a convolution (flipped)."""
+    nx, ny, nz = shape
+    mx, my, mz = (int(v) for v in m)
+    U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
+    P = np.pad(U, ((mz, mz), (my, my), (mx, mx)), mode='symmetric')
+    W = np.asarray(weights, dtype=np.float64).reshape((2 * mz + 1, 2 * my + 1, 2 * mx + 1))
+    f = {1: lambda a: a, 2: lambda a: 1.0 / a, 3: np.log}[mean_type]
+    acc = np.zeros_like(U)
+    for k in range(-mz, mz + 1):
+        for j in range(-my, my + 1):
+            for i in range(-mx, mx + 1):
+                acc += W[mz - k, my - j, mx - i] * f(P[mz + k:mz + k + nz, my + j:my + j + ny, mx + i:mx + i + nx])
+    mean = {1: lambda a: a, 2: lambda a: 1.0 / a, 3: np.exp}[mean_type](acc)
+    d = U - mean
+    return (beta * (d if no_norm else d / (mean + epps))).ravel()

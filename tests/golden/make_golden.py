@@ -143,6 +143,16 @@ def prior_weight_fixture(proj):
     prepass.computeWeights(o, True)
     prepass.quadWeights(o, True)
     out["ggmrf_111"] = np.asarray(o.weights_quad, dtype=np.float32)
+    # weighted mean: weightedWeights on the distance weights
+    o = apply(proj.projectorClass(), CONFIGS["pet_mini"])
+    o.addProjector()
+    o.Ndx = o.Ndy = o.Ndz = 1
+    o.weights = np.empty(0, dtype=np.float32)
+    o.GGMRF = False
+    prepass.computeWeights(o, False)
+    o.weighted_weights = np.empty(0, dtype=np.float32)
+    prepass.weightedWeights(o)
+    out["wmean_111"] = np.asarray(o.weighted_weights, dtype=np.float32).ravel(order='F')
     np.savez_compressed(os.path.join(HERE, "priorw_pet_mini.npz"), **out)
     print("priorw_pet_mini", {k: v.shape for k, v in out.items()})
 

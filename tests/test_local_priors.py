@@ -228,3 +228,66 @@ def test_builtin_bsrem_with_hyperbolic(cuda):
     x = res.ravel(order='F')
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
     assert orc.rel_l2(ref, orc.relaxed(g, ys, np.ones(g.n_img), 2, "RAMLA", lam=lam)) > 1e-4
+
+
+def test_weighted_mean_weights_match_reference():
+    import os
+    from conftest import make_options
+    from omega_b200 import priors
+    f = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "priorw_pet_mini.npz"))
+    o = make_options("pet_mini")
+    o.Ndx = o.Ndy = o.Ndz = 1
+    assert np.array_equal(priors.weighted_mean_weights(o), f["wmean_111"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mean_type,no_norm", [(1, False), (2, False), (3, True)])
+def test_weighted_mean(cuda, mean_type, no_norm):
+    import torch
+    from conftest import make_options
+    from omega_b200 import _native, priors
+    from omega_b200 import reconstruction as rec
+    from omega_b200.reconstruction import _stream
+    rng = np.random.default_rng(20 + mean_type)
+    n = int(np.prod(SHAPE))
+    u = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    w = rng.uniform(0.01, 0.1, 27).astype(np.float32)
+    U, W = torch.tensor(u, device=cuda), torch.tensor(w, device=cuda)
+    out = torch.full((n,), 0.5, device=cuda)
+    _native.call("omb_wmean_gradient", ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(out.data_ptr()), *SHAPE,
+                 1, 1, 1, ctypes.c_void_p(W.data_ptr()), float(w.sum()), mean_type, 1e-8, 0.3,
+                 1 if no_norm else 0, _stream(cuda))
+    want = 0.5 + io.wmean_gradient(u.astype(np.float64), SHAPE, (1, 1, 1), w.astype(np.float64) / float(w.sum()),
+                                   mean_type, 0.3, 1e-8, no_norm)
+    assert orc.rel_l2(out.cpu().numpy() - 0.5, want - 0.5) < 1e-5
+    # BSREM with the prior: its MAP step keeps the image >= epps, so the
+    # harmonic and geometric means stay finite where no ray reaches (one-step-
+    # late OSEM drives those voxels to 0); the harmonic mean is left to the
+    # kernel check above
+    if mean_type == 2:
+        return
+    o = make_options("pet_mini")
+    g = orc.Geometry(o)
+    full = make_options("pet_mini")
+    full.subsets, full.subsetType = 1, 8
+    full.addProjector()
+    y = rng.poisson(orc.forward(orc.Geometry(full), rng.uniform(0.5, 2.0, g.n_img), 0) * 200).astype(np.float32) / 200
+    o.SinM = y.copy()
+    o.BSREM = True
+    o.weighted_mean = True
+    o.mean_type = mean_type
+    o.med_no_norm = no_norm
+    o.beta = 0.01
+    o.Niter = 2
+    lam = np.array([0.2, 0.12], np.float32)
+    o.lambdaN = lam
+    res, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    shape = (g.nx, g.ny, g.nz)
+    ww = priors.weighted_mean_weights(o).astype(np.float64)
+    ref = orc.relaxed(g, ys, np.ones(g.n_img), 2, "BSREM", lam=lam,
+                      prior_grad=lambda v: io.wmean_gradient(v, shape, (1, 1, 1), ww, mean_type, 0.01, g.epps,
+                                                             no_norm))
+    x = res.ravel(order='F')
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
