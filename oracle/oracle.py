@@ -147,7 +147,10 @@ class Geometry:
         self.n_meas = np.asarray(o.nMeas, dtype=np.int64).ravel()
         self.xy = np.ascontiguousarray(np.asarray(o.x, dtype=np.float32).ravel())
         self.z = np.ascontiguousarray(np.asarray(o.z, dtype=np.float32).ravel())
-        self.pitch = (float(o.dPitchX), float(o.dPitchY))
+        # CT: the detector pitch as the kernels receive it, a float32 scalar
+        # (projfunctions.py passes cp.float32(dPitchX / dPitchY))
+        self.pitch = (float(np.float32(o.dPitchX)), float(np.float32(o.dPitchY))) if self.ct else \
+            (float(o.dPitchX), float(o.dPitchY))
         self.global_factor = float(o.global_factor)
         self.epps = float(o.epps)
         self.nbins = int(o.TOF_bins_used) if o.TOF else 1
@@ -155,7 +158,8 @@ class Geometry:
         self.tofc = np.ascontiguousarray(np.asarray(o.TOFCenter, dtype=np.float64).ravel()) if o.TOF else \
             np.zeros(1, dtype=np.float64)
         # projector type 4: sampling length and the CT backprojection weight
-        self.dL = float(o.dL)
+        # the sampling length as the kernels receive it, a float32 scalar
+        self.dL = float(np.float32(o.dL))
         self.kerroin = float(np.ravel(o.kerroin)[0]) if np.size(o.kerroin) else 0.0
         # PET multi-ray: rays per LOR over the crystal pitches (dPitchX
         # transaxially, dPitchY axially, as the reference's kernels take them)

@@ -1,0 +1,261 @@
+"""TEST INFRASTRUCTURE ONLY: the reference's own GPU kernels, run on the host.
+
+Loads ``oracle/_ref/libref_cl_<variant>_{d,f}.so`` (built by oracle/Makefile
+from OMEGA's source/opencl kernels through ``cl_host_shim.h`` and
+``ref_cl_wrap.cpp``) and calls them on the arrays an addProjector()-ed
+projector object holds, exactly as omegatomo/projector/projfunctions.py hands
+them to the CUDA kernels: the same subset slices of ``x`` / ``z``, the same
+float32 scalars (voxel grid, dScale / dSize, dL, kerroin, bmax = b + N d).
+
+``precision="d"`` runs the kernels in FP64 with exact texture weights: the
+pin of the FP64 restatements in bdd_oracle.c, interp_oracle.c and oracle.py.
+``precision="f"`` runs them in FP32 with the 8-bit texture weights of the
+reference's GPU path (``frac_bits=8``), to state how far the reference's own
+GPU arithmetic is from the FP64 answer.
+
+Only tests/ import this module; it needs the OMEGA sources at build time, so
+tests that use it skip when oracle/_ref was not built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+_libs = {}
+_D = ctypes.c_double
+_I = ctypes.c_int
+_LL = ctypes.c_longlong
+_P = ctypes.POINTER(ctypes.c_double)
+
+
+def available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libref_cl_bdd_fp_d.so"))
+
+
+def _lib(variant, precision):
+    key = (variant, precision)
+    if key not in _libs:
+        path = os.path.join(REF_DIR, f"libref_cl_{variant}_{precision}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (make -C oracle OMEGA_REFERENCE=...)")
+        L = ctypes.CDLL(path)
+        if hasattr(L, "refcl_bdd_fp"):
+            L.refcl_bdd_fp.argtypes = [_I, _I, _D, _D, _I, _I, _I] + [_D] * 11 + [_P, _P, _LL, _P, _I, _P]
+        if hasattr(L, "refcl_bdd_bp"):
+            L.refcl_bdd_bp.argtypes = [_I, _I, _D, _D, _I, _I, _I] + [_D] * 11 + [_P, _P, _LL, _P, _I, _I, _P, _P]
+        if hasattr(L, "refcl_interp"):
+            L.refcl_interp.argtypes = [_I, _I, _D, _D, _D, _D, _P, _D, _I, _I, _I] + [_D] * 9 + \
+                [_P, _LL, _P, _LL, _I, _P, _P, _P, _I]
+        if hasattr(L, "refcl_interp_ct_bp"):
+            L.refcl_interp_ct_bp.argtypes = [_I, _I, _D, _D, _I, _I, _I] + [_D] * 7 + [_P, _P, _LL, _P, _I, _I, _P,
+                                                                                        _P]
+        if hasattr(L, "refcl_tv_gradient"):
+            L.refcl_tv_gradient.argtypes = [_I, _I, _I, _P, _D, _D, _D, _P]
+            L.refcl_pdhg_update.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D, _D, _I]
+        _libs[key] = L
+    return _libs[key]
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def _f32(v):
+    return float(np.float32(np.ravel(v)[0]))
+
+
+def _frac(precision):
+    return 0 if precision == "d" else 8
+
+
+def _scales(o, exact):
+    """The scale scalars the kernels receive.  The reference hands them over
+    as float32 (coordinates.py:209-269 rounds them, projfunctions.py passes
+    cp.float32); ``exact`` gives the unrounded FP64 values of the same
+    formulas, which isolates the algorithm from that input rounding."""
+    d = [np.float64(np.ravel(v)[0]) for v in (o.dx, o.dy, o.dz)]
+    N = [int(np.ravel(v)[0]) for v in (o.Nx, o.Ny, o.Nz)]
+    if not exact:
+        out = {k: _f32(getattr(o, k)) for k in ("dScaleX4", "dScaleY4", "dScaleZ4")}
+        if o.CT and int(o.projector_type) in (5, 15, 45, 54, 51):
+            out.update({k: _f32(getattr(o, k)) for k in ("dScaleX", "dScaleY", "dScaleZ", "dSizeX", "dSizeY")})
+        return out
+    out = {"dScaleX4": 1.0 / (d[0] * N[0]), "dScaleY4": 1.0 / (d[1] * N[1]), "dScaleZ4": 1.0 / (d[2] * N[2]),
+           "dScaleX": 1.0 / (d[0] * (N[0] + 1)), "dScaleY": 1.0 / (d[1] * (N[1] + 1)),
+           "dScaleZ": 1.0 / (d[2] * (N[2] + 1)), "dSizeX": 1.0 / (d[0] * N[0]), "dSizeY": 1.0 / (d[1] * N[1])}
+    return out
+
+
+class RefCT:
+    """Cone-beam geometry of a CT projector object (types 4 and 5)."""
+
+    def __init__(self, o, exact_inputs=False):
+        self.sc = _scales(o, exact_inputs)
+        self.n_rows, self.n_cols = int(o.nRowsD), int(o.nColsD)
+        self.pitch = (_f32(o.dPitchX), _f32(o.dPitchY))
+        self.N = tuple(int(np.ravel(v)[0]) for v in (o.Nx, o.Ny, o.Nz))
+        self.b = tuple(_f32(v) for v in (o.bx, o.by, o.bz))
+        self.d = tuple(_f32(v) for v in (o.dx, o.dy, o.dz))
+        self.n_meas = np.asarray(o.nMeas, dtype=np.int64).ravel()
+        self.n_proj = int(o.nProjections)
+        self.xyz = np.asarray(o.x, dtype=np.float32).ravel().astype(np.float64)
+        self.uv = np.asarray(o.z, dtype=np.float32).ravel().astype(np.float64)
+        self.o = o
+
+    @property
+    def n_img(self):
+        return self.N[0] * self.N[1] * self.N[2]
+
+    def span(self, subset):
+        if subset < 0:
+            return 0, self.n_proj
+        return int(self.n_meas[subset]), int(self.n_meas[subset + 1] - self.n_meas[subset])
+
+    def geom(self, subset):
+        p0, n = self.span(subset)
+        return (np.ascontiguousarray(self.xyz[6 * p0:6 * (p0 + n)]), np.ascontiguousarray(self.uv[2 * p0:2 * (p0 + n)]),
+                n)
+
+    # -- projector type 5 ------------------------------------------------------
+    def bdd_forward(self, image, subset=-1, precision="d"):
+        o = self.o
+        xyz, uv, n = self.geom(subset)
+        img = np.ascontiguousarray(image, dtype=np.float64).ravel()
+        y = np.zeros(self.n_rows * self.n_cols * n)
+        _lib("bdd_fp", precision).refcl_bdd_fp(
+            self.n_rows, self.n_cols, *self.pitch, *self.N, *self.b, self.sc["dSizeX"], self.sc["dSizeY"], *self.d,
+            self.sc["dScaleX"], self.sc["dScaleY"], self.sc["dScaleZ"], _dp(xyz), _dp(uv), n, _dp(img), _frac(precision),
+            _dp(y))
+        return y
+
+    def bdd_backward(self, y, subset=-1, sens=False, precision="d"):
+        o = self.o
+        xyz, uv, n = self.geom(subset)
+        yy = np.ascontiguousarray(y, dtype=np.float64).ravel()
+        img = np.zeros(self.n_img)
+        s = np.zeros(self.n_img) if sens else None
+        _lib("bdd_bp", precision).refcl_bdd_bp(
+            self.n_rows, self.n_cols, *self.pitch, *self.N, *self.b, *self.d, self.sc["dScaleX"], self.sc["dScaleY"],
+            self.sc["dScaleZ"], _f32(o.dSizeXBP), _f32(o.dSizeZBP), _dp(xyz), _dp(uv), n, _dp(yy), 0 if sens else 1,
+            _frac(precision), _dp(img), _dp(s))
+        return (img, s) if sens else img
+
+    # -- projector type 4 (CT) ---------------------------------------------------
+    def interp_forward(self, image, subset=-1, precision="d"):
+        o = self.o
+        xyz, uv, n = self.geom(subset)
+        img = np.ascontiguousarray(image, dtype=np.float64).ravel()
+        y = np.zeros(self.n_rows * self.n_cols * n)
+        bmax = [_f32(np.float64(b) + N * np.float64(d)) for b, N, d in
+                zip((np.ravel(o.bx)[0], np.ravel(o.by)[0], np.ravel(o.bz)[0]), self.N,
+                    (np.ravel(o.dx)[0], np.ravel(o.dy)[0], np.ravel(o.dz)[0]))]
+        _lib("i4_ct_fp", precision).refcl_interp(
+            self.n_rows, self.n_cols, *self.pitch, _f32(o.dL), _f32(o.global_factor), None, 0.0, *self.N, *self.b,
+            *bmax, self.sc["dScaleX4"], self.sc["dScaleY4"], self.sc["dScaleZ4"], _dp(xyz), xyz.size, _dp(uv), n,
+            _frac(precision), _dp(img), _dp(y), None, 1)
+        return y
+
+    def interp_backward(self, y, subset=-1, sens=False, precision="d"):
+        o = self.o
+        xyz, uv, n = self.geom(subset)
+        yy = np.ascontiguousarray(y, dtype=np.float64).ravel()
+        img = np.zeros(self.n_img)
+        s = np.zeros(self.n_img) if sens else None
+        _lib("i4_ct_bp", precision).refcl_interp_ct_bp(
+            self.n_rows, self.n_cols, *self.pitch, *self.N, *self.b, *self.d, _f32(np.ravel(o.kerroin)[0]), _dp(xyz),
+            _dp(uv), n, _dp(yy), 0 if sens else 1, _frac(precision), _dp(img), _dp(s))
+        return (img, s) if sens else img
+
+
+class RefPET:
+    """PET sinogram geometry of a projector object (type 4, whole-sinogram
+    subsets: subset types >= 8 or one subset)."""
+
+    def __init__(self, o, exact_inputs=False):
+        self.sc = _scales(o, exact_inputs)
+        self.o = o
+        self.n_rows, self.n_cols = int(o.Ndist), int(o.Nang)
+        self.pitch = (_f32(o.dPitchX), _f32(o.dPitchY))
+        self.N = tuple(int(np.ravel(v)[0]) for v in (o.Nx, o.Ny, o.Nz))
+        self.b = tuple(_f32(v) for v in (o.bx, o.by, o.bz))
+        self.n_meas = np.asarray(o.nMeas, dtype=np.int64).ravel()
+        self.n_proj = int(o.NSinos) if int(o.subsets) == 1 else int(self.n_meas[-1])
+        self.xyz = np.asarray(o.x, dtype=np.float32).ravel().astype(np.float64)
+        self.uv = np.asarray(o.z, dtype=np.float32).ravel().astype(np.float64)
+        self.nbins = int(o.TOF_bins_used) if o.TOF else 1
+        tofc = np.asarray(o.TOFCenter, dtype=np.float64).ravel()
+        self.tofc = (tofc if exact_inputs else tofc.astype(np.float32).astype(np.float64)) if o.TOF else None
+        self.sigma_x = (float(o.sigma_x) if exact_inputs else _f32(o.sigma_x)) if o.TOF else 0.0
+        if int(o.subsets) > 1 and int(o.subsetType) < 8:
+            raise ValueError("measurement-level subsets are not wired into the host-compiled reference")
+
+    @property
+    def n_img(self):
+        return self.N[0] * self.N[1] * self.N[2]
+
+    def _variant(self, fp):
+        kind = "fp" if fp else "bp"
+        return f"i4_pet_{kind}_nb1" if self.nbins == 1 else f"i4_pet_{kind}_tof{self.nbins}"
+
+    def _call(self, fp, subset, precision, img, meas, sens):
+        o = self.o
+        p0 = 0 if subset < 0 else int(self.n_meas[subset])
+        n = self.n_proj if subset < 0 else int(self.n_meas[subset + 1] - self.n_meas[subset])
+        uv = np.ascontiguousarray(self.uv[2 * p0:2 * (p0 + n)])
+        bmax = [_f32(np.float64(np.ravel(b)[0]) + N * np.float64(np.ravel(d)[0])) for b, N, d in
+                zip((o.bx, o.by, o.bz), self.N, (o.dx, o.dy, o.dz))]
+        _lib(self._variant(fp), precision).refcl_interp(
+            self.n_rows, self.n_cols, *self.pitch, _f32(o.dL), _f32(o.global_factor), _dp(self.tofc), self.sigma_x,
+            *self.N, *self.b, *bmax, self.sc["dScaleX4"], self.sc["dScaleY4"], self.sc["dScaleZ4"], _dp(self.xyz),
+            self.xyz.size, _dp(uv), n, _frac(precision), _dp(img), _dp(meas), _dp(sens), 0 if sens is not None else 1)
+        return n
+
+    def rays(self, subset):
+        n = self.n_proj if subset < 0 else int(self.n_meas[subset + 1] - self.n_meas[subset])
+        return self.n_rows * self.n_cols * n
+
+    def interp_forward(self, image, subset=-1, precision="d"):
+        img = np.ascontiguousarray(image, dtype=np.float64).ravel()
+        y = np.zeros(self.rays(subset) * self.nbins)
+        self._call(True, subset, precision, img, y, None)
+        return y
+
+    def interp_backward(self, y, subset=-1, sens=False, precision="d"):
+        yy = np.ascontiguousarray(y, dtype=np.float64).ravel()
+        img = np.zeros(self.n_img)
+        s = np.zeros(self.n_img) if sens else None
+        self._call(False, subset, precision, img, yy, s)
+        return (img, s) if sens else img
+
+
+def _scalar(v, exact):
+    return float(v) if exact else float(np.float32(v))
+
+
+def tv_gradient(u, shape, smooth, beta, precision="d", sigma=1.0, exact_inputs=False):
+    """auxKernels.cl TVKernel (plain TV, texture reads): grad += beta * dTV(u)
+    with smoothing ``smooth``; the scalars go in as float32 like the
+    reference's launch unless ``exact_inputs``."""
+    nx, ny, nz = shape
+    uu = np.ascontiguousarray(u, dtype=np.float64).ravel()
+    g = np.zeros(uu.size)
+    _lib("aux", precision).refcl_tv_gradient(nx, ny, nz, _dp(uu), _scalar(sigma, exact_inputs),
+                                             _scalar(smooth, exact_inputs), _scalar(beta, exact_inputs), _dp(g))
+    return g
+
+
+def pdhg_update(im, rhs, u, shape, tau, theta=1.0, eps=1e-5, positivity=True, precision="d", exact_inputs=False):
+    """auxKernels.cl PDHGUpdate (no subsets); returns the new (im, u)."""
+    nx, ny, nz = shape
+    a = np.ascontiguousarray(im, dtype=np.float64).ravel().copy()
+    b = np.ascontiguousarray(u, dtype=np.float64).ravel().copy()
+    r = np.ascontiguousarray(rhs, dtype=np.float64).ravel()
+    _lib("aux", precision).refcl_pdhg_update(nx, ny, nz, _dp(a), _dp(r), _dp(b), _scalar(eps, exact_inputs),
+                                             _scalar(theta, exact_inputs), _scalar(tau, exact_inputs),
+                                             int(positivity))
+    return a, b

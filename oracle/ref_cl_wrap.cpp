@@ -1,0 +1,350 @@
+/*
+ * TEST INFRASTRUCTURE ONLY -- drivers that run OMEGA's own GPU kernel
+ * sources on the CPU, as the pinned oracle of projector types 4 and 5, the
+ * TV gradient and the PDHG image update.  Built by oracle/Makefile into
+ * oracle/_ref/ (one shared object per kernel variant); nothing in the product
+ * loads them.
+ *
+ * This file is compiled once per variant.  The variant macro selects which
+ * reference source is included and which driver is exported; the kernel's
+ * own feature macros are the ones omegatomo/projector/init.py:250-442 passes
+ * for that case (CUDA, PYTHON, USEGLOBAL, USEIMAGES, USEMAD, TOTLENGTH, CT or
+ * PET, FP or BP, PROJ5 / PTYPE4 / BP4 with NVOXELS*, TOF with NBINS) and are
+ * given on the compiler's command line by the Makefile.
+ *
+ *   REFCL_BDD_FP     projectorType5.cl:64-333   projectorType5Forward
+ *   REFCL_BDD_BP     projectorType5.cl:381-757  projectorType5Backward (GEOM5)
+ *   REFCL_INTERP_FP  projectorType4.cl:84-683   projectorType4Forward (PET or CT, FP)
+ *   REFCL_INTERP_BP  projectorType4.cl:84-683   projectorType4Forward (PET, BP, float atomics)
+ *   REFCL_INTERP_CTBP projectorType4.cl:718-1100 projectorType4Backward (BP4)
+ *   REFCL_AUX        auxKernels.cl:1733-1990    TVKernel (TVGRAD, texture reads)
+ *                    auxKernels.cl:2033-2062    PDHGUpdate (PDHG, no subsets)
+ *
+ * The host-side inputs the reference builds before a launch are restated
+ * here so that each kernel receives exactly what the Python projector hands
+ * it: the two image summed-area tables (projfunctions.py:203-238), the
+ * measurement summed-area table (projfunctions.py:869-878), the per-projection
+ * GEOM5 constants (computeGeom5, init.py:6-37) and the texture objects with
+ * their filter and addressing modes (projfunctions.py:215-238, 266-290, 969-1003).
+ *
+ * OMB_REAL = double runs the kernels in FP64 with exact texture weights (the
+ * oracle mode); OMB_REAL = float with frac_bits = 8 reproduces the
+ * reference's single-precision GPU arithmetic and 8-bit texture weights.
+ */
+#include "cl_host_shim.h"
+
+#include <stdlib.h>
+
+#include <vector>
+
+#if OMB_FP64
+#define float double
+#endif
+#include "general_opencl_functions.h"
+#if defined(REFCL_BDD_FP) || defined(REFCL_BDD_BP)
+#include "projectorType5.cl"
+#elif defined(REFCL_INTERP_FP) || defined(REFCL_INTERP_BP) || defined(REFCL_INTERP_CTBP)
+#include "projectorType4.cl"
+#elif defined(REFCL_AUX)
+#include "auxKernels.cl"
+#endif
+#if OMB_FP64
+#undef float
+#endif
+
+#define REFCL_EXPORT extern "C" __attribute__((visibility("default")))
+
+typedef std::vector<omb_real> rvec;
+
+static rvec to_real(const double *p, size_t n) {
+    rvec v(n);
+    for (size_t i = 0; i < n; ++i) v[i] = (omb_real)p[i];
+    return v;
+}
+
+static void from_real(const rvec &v, double *p) {
+    for (size_t i = 0; i < v.size(); ++i) p[i] = (double)v[i];
+}
+
+static void set_item(unsigned x, unsigned y, unsigned z) {
+    blockIdx = make_uint3(x, y, z);
+    threadIdx = make_uint3(0, 0, 0);
+    blockDim = make_uint3(1, 1, 1);
+}
+
+static omb_tex make_tex(const rvec &data, int w, int h, int d, int linear, int normalized, int frac_bits) {
+    omb_tex t;
+    t.data = data.data();
+    t.w = w;
+    t.h = h;
+    t.d = d;
+    t.linear = linear;
+    t.normalized = normalized;
+    t.frac_bits = frac_bits;
+    return t;
+}
+
+REFCL_EXPORT int refcl_precision(void) { return (int)sizeof(omb_real); }
+
+#if defined(REFCL_BDD_FP)
+/* Forward projection of `n_proj` cone-beam projections.  img: Nx*Ny*Nz,
+ * x fastest; xyz: 6 per projection (source, panel centre); uv: 2 per
+ * projection; out: n_rows*n_cols*n_proj, rows fastest (accumulated into). */
+REFCL_EXPORT int refcl_bdd_fp(int n_rows, int n_cols, double pitch_x, double pitch_y, int nx, int ny, int nz,
+                              double bx, double by, double bz, double size_x, double size_y, double dx, double dy,
+                              double dz, double scale_x, double scale_y, double scale_z, const double *xyz,
+                              const double *uv, long long n_proj, const double *img, int frac_bits, double *out) {
+    /* The SAT over (x, z) of every y slice: (Nx+1) x (Nz+1) x Ny, x fastest,
+     * node (i, k) = sum of img[a, j, c] for a < i, c < k (projfunctions.py:231-238). */
+    const size_t W1 = (size_t)nx + 1, H = (size_t)nz + 1;
+    rvec satY(W1 * H * (size_t)ny, (omb_real)0);
+    for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k)
+            for (int i = 0; i < nx; ++i)
+                satY[((size_t)j * H + k + 1) * W1 + i + 1] = (omb_real)img[i + (size_t)nx * (j + (size_t)ny * k)];
+    for (int j = 0; j < ny; ++j)       /* cumsum along x (axis 0) */
+        for (size_t k = 0; k < H; ++k)
+            for (size_t i = 1; i < W1; ++i) satY[((size_t)j * H + k) * W1 + i] += satY[((size_t)j * H + k) * W1 + i - 1];
+    for (int j = 0; j < ny; ++j)       /* then along z (axis 1) */
+        for (size_t k = 1; k < H; ++k)
+            for (size_t i = 0; i < W1; ++i) satY[((size_t)j * H + k) * W1 + i] += satY[((size_t)j * H + k - 1) * W1 + i];
+    /* The SAT over (y, z) of every x slice: (Ny+1) x (Nz+1) x Nx, y fastest
+     * (projfunctions.py:203-214). */
+    const size_t W2 = (size_t)ny + 1;
+    rvec satX(W2 * H * (size_t)nx, (omb_real)0);
+    for (int i = 0; i < nx; ++i)
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                satX[((size_t)i * H + k + 1) * W2 + j + 1] = (omb_real)img[i + (size_t)nx * (j + (size_t)ny * k)];
+    for (int i = 0; i < nx; ++i)
+        for (size_t k = 0; k < H; ++k)
+            for (size_t j = 1; j < W2; ++j) satX[((size_t)i * H + k) * W2 + j] += satX[((size_t)i * H + k) * W2 + j - 1];
+    for (int i = 0; i < nx; ++i)
+        for (size_t k = 1; k < H; ++k)
+            for (size_t j = 0; j < W2; ++j) satX[((size_t)i * H + k) * W2 + j] += satX[((size_t)i * H + k - 1) * W2 + j];
+    const omb_tex texY = make_tex(satY, (int)W1, (int)H, ny, 1, 1, frac_bits);
+    const omb_tex texX = make_tex(satX, (int)W2, (int)H, nx, 1, 1, frac_bits);
+    rvec g = to_real(xyz, (size_t)n_proj * 6), d_uv = to_real(uv, (size_t)n_proj * 2);
+    rvec y((size_t)n_rows * n_cols * n_proj, (omb_real)0);
+    const int gy = (n_cols + NVOXELSFP - 1) / NVOXELSFP;
+#pragma omp parallel for schedule(dynamic)
+    for (long long p = 0; p < n_proj; ++p)
+        for (int c = 0; c < gy; ++c)
+            for (int r = 0; r < n_rows; ++r) {
+                set_item((unsigned)r, (unsigned)c, (unsigned)p);
+                projectorType5Forward((unsigned)n_rows, (unsigned)n_cols, (omb_real)pitch_x, (omb_real)pitch_y,
+                                      (unsigned)nx, (unsigned)ny, (unsigned)nz, (omb_real)bx, (omb_real)by,
+                                      (omb_real)bz, (omb_real)size_x, (omb_real)size_y, (omb_real)dx, (omb_real)dy,
+                                      (omb_real)dz, (omb_real)scale_x, (omb_real)scale_y, (omb_real)scale_z,
+                                      g.data(), d_uv.data(), &texY, &texX, y.data(), n_proj);
+            }
+    for (size_t i = 0; i < y.size(); ++i) out[i] += (double)y[i];
+    return 0;
+}
+#endif
+
+#if defined(REFCL_BDD_BP)
+/* Backprojection of `n_proj` projections into an Nx*Ny*Nz image (x fastest).
+ * y: n_rows*n_cols*n_proj, rows fastest.  img and (no_norm == 0) sens are
+ * overwritten, as the kernel stores rather than accumulates. */
+REFCL_EXPORT int refcl_bdd_bp(int n_rows, int n_cols, double pitch_x, double pitch_y, int nx, int ny, int nz,
+                              double bx, double by, double bz, double dx, double dy, double dz, double scale_x,
+                              double scale_y, double scale_z, double size_x_bp, double size_z_bp, const double *xyz,
+                              const double *uv, long long n_proj, const double *y, int no_norm, int frac_bits,
+                              double *img, double *sens) {
+    /* computeGeom5 (init.py:6-37): 16 values per projection. */
+    rvec geom((size_t)n_proj * 16);
+    const omb_real indX = (omb_real)n_rows / (omb_real)2, indY = (omb_real)n_cols / (omb_real)2;
+    for (long long p = 0; p < n_proj; ++p) {
+        const double *q = xyz + 6 * p;
+        const float3 s = make_float3((omb_real)q[0], (omb_real)q[1], (omb_real)q[2]);
+        const float3 d = make_float3((omb_real)q[3], (omb_real)q[4], (omb_real)q[5]);
+        const float3 apuX = make_float3((omb_real)uv[2 * p] * indX, (omb_real)uv[2 * p + 1] * indX, (omb_real)0);
+        const float3 apuY = make_float3((omb_real)0, (omb_real)0, indY * (omb_real)pitch_y);
+        const float3 d3 = make_float3(d.x - apuX.x - apuY.x, d.y - apuX.y - apuY.y, d.z - apuX.z - apuY.z);
+        const float3 d2 = make_float3(apuX.x - apuY.x, apuX.y - apuY.y, apuX.z - apuY.z);
+        const omb_real nX = omb_sqrt(apuX.x * apuX.x + apuX.y * apuX.y + apuX.z * apuX.z);
+        const omb_real nY = omb_sqrt(apuY.x * apuY.x + apuY.y * apuY.y + apuY.z * apuY.z);
+        const float3 e = make_float3(d3.x - d.x, d3.y - d.y, d3.z - d.z);
+        const float3 cp = make_float3(d2.y * e.z - d2.z * e.y, d2.z * e.x - d2.x * e.z, d2.x * e.y - d2.y * e.x);
+        const omb_real up = cp.x * (s.x - d.x) + cp.y * (s.y - d.y) + cp.z * (s.z - d.z);
+        omb_real *o = geom.data() + 16 * p;
+        const omb_real v[16] = {s.x,          s.y,          s.z,          d3.x, d3.y, d3.z, apuX.x / nX, apuX.y / nX,
+                                apuX.z / nX, apuY.x / nY, apuY.y / nY, apuY.z / nY, cp.x, cp.y, cp.z, up};
+        memcpy(o, v, sizeof(v));
+    }
+    /* Measurement SAT (projfunctions.py:869-878): (n_rows+1) x (n_cols+1) x
+     * n_proj, rows fastest, cumulative along rows then columns. */
+    const size_t W = (size_t)n_rows + 1, H = (size_t)n_cols + 1;
+    rvec sat(W * H * (size_t)n_proj, (omb_real)0);
+    for (long long p = 0; p < n_proj; ++p)
+        for (int c = 0; c < n_cols; ++c)
+            for (int r = 0; r < n_rows; ++r)
+                sat[((size_t)p * H + c + 1) * W + r + 1] = (omb_real)y[r + (size_t)n_rows * (c + (size_t)n_cols * p)];
+    for (long long p = 0; p < n_proj; ++p)
+        for (size_t c = 0; c < H; ++c)
+            for (size_t r = 1; r < W; ++r) sat[((size_t)p * H + c) * W + r] += sat[((size_t)p * H + c) * W + r - 1];
+    for (long long p = 0; p < n_proj; ++p)
+        for (size_t c = 1; c < H; ++c)
+            for (size_t r = 0; r < W; ++r) sat[((size_t)p * H + c) * W + r] += sat[((size_t)p * H + c - 1) * W + r];
+    const omb_tex tex = make_tex(sat, (int)W, (int)H, (int)n_proj, 1, 1, frac_bits);
+    rvec g = to_real(xyz, (size_t)n_proj * 6), d_uv = to_real(uv, (size_t)n_proj * 2);
+    const size_t N = (size_t)nx * ny * nz;
+    rvec out(N, (omb_real)0), wsum(N, (omb_real)0);
+    const int gz = (nz + NVOXELS5 - 1) / NVOXELS5;
+#pragma omp parallel for schedule(dynamic)
+    for (int k = 0; k < gz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                projectorType5Backward((unsigned)n_rows, (unsigned)n_cols, (omb_real)pitch_x, (omb_real)pitch_y,
+                                       (unsigned)nx, (unsigned)ny, (unsigned)nz, (omb_real)bx, (omb_real)by,
+                                       (omb_real)bz, (omb_real)dx, (omb_real)dy, (omb_real)dz, (omb_real)scale_x,
+                                       (omb_real)scale_y, (omb_real)scale_z, (omb_real)size_x_bp,
+                                       (omb_real)size_z_bp, g.data(), d_uv.data(), geom.data(), &tex, out.data(),
+                                       wsum.data(), (unsigned char)no_norm, n_proj, 0);
+            }
+    from_real(out, img);
+    if (no_norm == 0 && sens) from_real(wsum, sens);
+    return 0;
+}
+#endif
+
+#if defined(REFCL_INTERP_FP) || defined(REFCL_INTERP_BP)
+/* Ray-driven type-4 projection of one call: for PET, n_rows x n_cols bins of
+ * `n_proj` sinograms (xyz: 4 per bin of the whole sinogram, uv: 2 per
+ * sinogram of this call); for CT, n_proj projections (xyz: 6, uv: 2 per
+ * projection).  The image is a linear-filtered, normalized, clamp-to-edge
+ * texture (projfunctions.py:266-290); bmax = b + N d and the scales
+ * dScale4 = 1 / (d N) are passed as the reference passes them.
+ * FP: meas (n_rows*n_cols*n_proj*NBINS, bins outermost) is accumulated into.
+ * BP: meas is read, img and (no_norm == 0) sens are accumulated into. */
+REFCL_EXPORT int refcl_interp(int n_rows, int n_cols, double pitch_x, double pitch_y, double dL, double global_factor,
+                              const double *tof_centers, double sigma_x, int nx, int ny, int nz, double bx, double by,
+                              double bz, double bmax_x, double bmax_y, double bmax_z, double scale_x, double scale_y,
+                              double scale_z, const double *xyz, long long n_xyz, const double *uv, long long n_proj,
+                              int frac_bits, double *img, double *meas, double *sens, int no_norm) {
+    (void)tof_centers;
+    (void)sigma_x;
+    (void)sens;
+    (void)no_norm;
+    (void)frac_bits;
+    const size_t N = (size_t)nx * ny * nz;
+    const unsigned long long m_size = (unsigned long long)n_rows * n_cols * (unsigned long long)n_proj;
+    rvec g = to_real(xyz, (size_t)n_xyz), d_uv = to_real(uv, (size_t)n_proj * 2);
+#ifdef TOF
+    rvec tc = to_real(tof_centers, NBINS);
+#endif
+#if defined(REFCL_INTERP_FP)
+    rvec im = to_real(img, N);
+    const omb_tex tex = make_tex(im, nx, ny, nz, 1, 1, frac_bits);
+    rvec y(m_size * NBINS, (omb_real)0);
+#define REFCL_IMG_ARG &tex
+#define REFCL_OUT_ARG y.data()
+#else
+    rvec y = to_real(meas, m_size * NBINS);
+    rvec out(N, (omb_real)0), wsum(N, (omb_real)0);
+#define REFCL_IMG_ARG y.data()
+#define REFCL_OUT_ARG out.data()
+#endif
+#if defined(REFCL_INTERP_FP)
+#pragma omp parallel for schedule(dynamic)
+#endif
+    for (long long p = 0; p < n_proj; ++p)
+        for (int c = 0; c < n_cols; ++c)
+            for (int r = 0; r < n_rows; ++r) {
+                set_item((unsigned)r, (unsigned)c, (unsigned)p);
+                projectorType4Forward((unsigned)n_rows, (unsigned)n_cols, (omb_real)pitch_x, (omb_real)pitch_y,
+                                      (omb_real)dL, (omb_real)global_factor,
+#ifdef TOF
+                                      tc.data(), (omb_real)sigma_x,
+#endif
+                                      (unsigned)nx, (unsigned)ny, (unsigned)nz, (omb_real)bx, (omb_real)by,
+                                      (omb_real)bz, (omb_real)bmax_x, (omb_real)bmax_y, (omb_real)bmax_z,
+                                      (omb_real)scale_x, (omb_real)scale_y, (omb_real)scale_z, REFCL_IMG_ARG,
+                                      REFCL_OUT_ARG, g.data(), d_uv.data(), n_proj,
+#if defined(REFCL_INTERP_BP)
+                                      wsum.data(),
+#endif
+                                      (unsigned char)no_norm, m_size, 0u, 0);
+            }
+#if defined(REFCL_INTERP_FP)
+    for (size_t i = 0; i < y.size(); ++i) meas[i] += (double)y[i];
+#else
+    for (size_t i = 0; i < N; ++i) img[i] += (double)out[i];
+    if (no_norm == 0 && sens)
+        for (size_t i = 0; i < N; ++i) sens[i] += (double)wsum[i];
+#endif
+    return 0;
+}
+#endif
+
+#if defined(REFCL_INTERP_CTBP)
+/* Voxel-driven type-4 CT backprojection of n_proj projections: the
+ * measurement is a linear-filtered, normalized, clamp-to-edge texture of
+ * n_rows x n_cols x n_proj (projfunctions.py:969-980); img and
+ * (no_norm == 0) sens are overwritten. */
+REFCL_EXPORT int refcl_interp_ct_bp(int n_rows, int n_cols, double pitch_x, double pitch_y, int nx, int ny, int nz,
+                                    double bx, double by, double bz, double dx, double dy, double dz, double kerroin,
+                                    const double *xyz, const double *uv, long long n_proj, const double *y, int no_norm,
+                                    int frac_bits, double *img, double *sens) {
+    rvec meas = to_real(y, (size_t)n_rows * n_cols * n_proj);
+    const omb_tex tex = make_tex(meas, n_rows, n_cols, (int)n_proj, 1, 1, frac_bits);
+    rvec g = to_real(xyz, (size_t)n_proj * 6), d_uv = to_real(uv, (size_t)n_proj * 2);
+    const size_t N = (size_t)nx * ny * nz;
+    rvec out(N, (omb_real)0), wsum(N, (omb_real)0);
+    const int gz = (nz + NVOXELS - 1) / NVOXELS;
+#pragma omp parallel for schedule(dynamic)
+    for (int k = 0; k < gz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                projectorType4Backward((unsigned)n_rows, (unsigned)n_cols, (omb_real)pitch_x, (omb_real)pitch_y,
+                                       (unsigned)nx, (unsigned)ny, (unsigned)nz, (omb_real)bx, (omb_real)by,
+                                       (omb_real)bz, (omb_real)dx, (omb_real)dy, (omb_real)dz, (omb_real)kerroin,
+                                       &tex, out.data(), g.data(), d_uv.data(), wsum.data(), (unsigned char)no_norm,
+                                       n_proj, 0);
+            }
+    from_real(out, img);
+    if (no_norm == 0 && sens) from_real(wsum, sens);
+    return 0;
+}
+#endif
+
+#if defined(REFCL_AUX)
+/* TVKernel with texture reads (nearest point, unnormalized, clamp to edge):
+ * grad += beta * dTV(u) with smoothing `epps` (the reference's TVsmoothing). */
+REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, double sigma, double epps, double beta,
+                                   double *grad) {
+    const size_t N = (size_t)nx * ny * nz;
+    rvec uu = to_real(u, N), g = to_real(grad, N);
+    const omb_tex tex = make_tex(uu, nx, ny, nz, 0, 0, 0);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                TVKernel(g.data(), &tex, nx, ny, nz, nx, ny, nz, (omb_real)sigma, (omb_real)epps, (omb_real)beta);
+            }
+    from_real(g, grad);
+    return 0;
+}
+
+/* PDHGUpdate without subsets: u -= tau * rhs (clamped at epps when
+ * positivity is enforced), im = u + theta (u - u_prev). */
+REFCL_EXPORT int refcl_pdhg_update(int nx, int ny, int nz, double *im, const double *rhs, double *u, double epps,
+                                   double theta, double tau, int positivity) {
+    const size_t N = (size_t)nx * ny * nz;
+    rvec a = to_real(im, N), r = to_real(rhs, N), b = to_real(u, N);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                PDHGUpdate(a.data(), r.data(), b.data(), make_int3(nx, ny, nz), (omb_real)epps, (omb_real)theta,
+                           (omb_real)tau, (unsigned char)positivity);
+            }
+    from_real(a, im);
+    from_real(b, u);
+    return 0;
+}
+#endif

@@ -67,6 +67,14 @@ CONFIGS["ct_fine5"] = dict(CT=True, nRowsD=24, nColsD=20, nProjections=30, dPitc
                            FOVa_y=32., axial_fov=24., projector_type=5, subsets=1, subsetType=8, Niter=1,
                            verbose=0, angles=np.linspace(0, 2 * np.pi, 30, endpoint=False).astype(np.float32),
                            SinM=np.zeros((24, 20, 30), dtype=np.float32))
+# four of the 360 views (0, 91, 182 and 273 degrees) of the cone-beam CT
+# benchmark geometry: 512 x 512 panel of 0.4 mm pixels, SOD 500 / SDD 1000 mm,
+# 256^3 volume of 0.25 mm voxels (every voxel footprint lies on the panel)
+_CFG1_ANGLES = np.linspace(0, 2 * np.pi, 360, endpoint=False).astype(np.float32)[[0, 91, 182, 273]]
+CONFIGS["ct_cfg1_4v"] = dict(CT=True, nRowsD=512, nColsD=512, nProjections=4, dPitchX=0.4, dPitchY=0.4,
+                             sourceToCRot=500., sourceToDetector=1000., Nx=256, Ny=256, Nz=256, FOVa_x=64.,
+                             FOVa_y=64., axial_fov=64., projector_type=5, subsets=1, subsetType=8, Niter=1,
+                             verbose=0, angles=_CFG1_ANGLES, SinM=np.zeros((512, 512, 4), dtype=np.float32))
 # TOF width so that the bins cover the FOV diagonal: 7 bins of 85 mm / (c/2) seconds
 CONFIGS["pet_mini_tof"]["TOF_width"] = 85.0 / (2.99792458e11 / 2.)
 # projector type 4 (interpolation): PET, PET with TOF, PET with a sampling

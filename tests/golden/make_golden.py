@@ -1,11 +1,11 @@
 """Generates the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container that holds the OMEGA sources (default /root/reference, or
-$OMEGA_REFERENCE):
+Run where the OMEGA sources are, with $OMEGA_REFERENCE naming their root:
 
-    python tests/golden/make_golden.py            # everything
+    OMEGA_REFERENCE=<checkout> python tests/golden/make_golden.py   # everything
     python tests/golden/make_golden.py volumes    # the type-3 tables only
     python tests/golden/make_golden.py nlm        # the NLM patch weights only
+    python tests/golden/make_golden.py geom NAME  # one geometry fixture
 
 For every option set in configs.py it imports the reference's own Python
 projector surface (omegatomo.projector.proj.projectorClass), runs its
@@ -24,7 +24,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("OMEGA_REFERENCE", "/root/reference")
+REF = os.environ.get("OMEGA_REFERENCE", "")
 sys.path.insert(0, HERE)
 from configs import CONFIGS, GEOMETRY_KEYS, SCALAR_KEYS, SCALE_KEYS, _pet, apply  # noqa: E402
 
@@ -37,6 +37,8 @@ CONFIGS_EXTRA = {
 
 
 def reference_projector():
+    if not REF:
+        sys.exit("set OMEGA_REFERENCE to the root of an OMEGA checkout (the directory holding source/Python)")
     sys.path.insert(0, os.path.join(REF, "source", "Python"))
     from omegatomo.projector import proj
     return proj
@@ -217,6 +219,12 @@ def main():
         return
     if sys.argv[1:] == ["priorw"]:
         prior_weight_fixture(reference_projector())
+        return
+    if sys.argv[1:2] == ["geom"]:
+        proj = reference_projector()
+        for name in sys.argv[2:]:
+            _, g = geometry(proj, CONFIGS[name])
+            np.savez_compressed(os.path.join(HERE, f"geom_{name}.npz"), **g)
         return
     proj = reference_projector()
     volume_fixture()

@@ -1,0 +1,204 @@
+"""The FP64 restatements of projector types 4 and 5, the TV gradient and the
+PDHG update against the reference's own kernel sources run on the host.
+
+oracle/_ref/libref_cl_*.so are OMEGA's projectorType5.cl, projectorType4.cl
+and auxKernels.cl compiled unchanged with g++ through oracle/cl_host_shim.h
+(built by oracle/Makefile when the OMEGA sources are given).  In FP64 with
+exact texture weights and unrounded scale scalars they compute the
+reference's algorithm without its single-precision rounding, and the
+restatements the GPU kernels are tested against must equal them to rounding.
+The same kernels in FP32 with 8-bit texture weights (the reference's GPU
+arithmetic) are compared too, to state the reference's own error.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+sys.path.insert(0, os.path.dirname(HERE))
+
+from configs import CONFIGS, apply  # noqa: E402
+from oracle import oracle as orc  # noqa: E402
+from oracle import ref_cl  # noqa: E402
+
+pytestmark = pytest.mark.skipif(not ref_cl.available(), reason="oracle/_ref not built (needs the OMEGA sources)")
+
+# restatement vs reference, both FP64 with the same inputs
+PIN = 1e-11
+
+
+def _proj(name, **extra):
+    from omega_b200.projector import proj
+    o = apply(proj.projectorClass(), dict(CONFIGS[name], **extra))
+    o.addProjector()
+    return o
+
+
+# ---------------------------------------------------------------------------
+# projector type 5 (branchless distance-driven)
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("name", ["ct_mini5", "ct_fine5", "ct_cfg1_4v"])
+def test_bdd_forward_pinned(name):
+    o = _proj(name)
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(11)
+    x = rng.uniform(0.0, 0.02, g.n_img)
+    ours = orc.bdd_forward(g, x, -1)
+    ref = ref_cl.RefCT(o, exact_inputs=True).bdd_forward(x, -1)
+    assert orc.rel_l2(ours, ref) < PIN
+    # with the float32 scale scalars the reference's launch passes
+    ref32in = ref_cl.RefCT(o).bdd_forward(x, -1)
+    assert orc.rel_l2(ours, ref32in) < 1e-6
+    if name != "ct_cfg1_4v":
+        # the reference's own GPU arithmetic (FP32, 8-bit texture weights)
+        gpu_like = ref_cl.RefCT(o).bdd_forward(x, -1, precision="f")
+        assert orc.rel_l2(gpu_like, ref) < 5e-3
+
+
+@pytest.mark.parametrize("name", ["ct_fine5", "ct_cfg1_4v"])
+def test_bdd_backward_pinned(name):
+    """Panels that cover every voxel footprint: image and sensitivity equal."""
+    o = _proj(name)
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(12)
+    y = rng.uniform(0.0, 1.0, g.rays(-1))
+    ours, sens = orc.bdd_backward(g, y, -1, sens=True)
+    ref, rsens = ref_cl.RefCT(o, exact_inputs=True).bdd_backward(y, -1, sens=True)
+    assert orc.rel_l2(ours, ref) < PIN
+    assert orc.rel_l2(sens, rsens) < PIN
+
+
+def test_bdd_backward_off_panel():
+    """ct_mini5's panel does not cover the volume: footprints beyond the far
+    panel edge read the clamped last summed-area node four times, and the
+    reference's `apu != 0` test then sees the rounding residue of
+    A + D - C - B, so it adds those views to the sensitivity (and a residue to
+    the image).  The restatement counts them as zero, as exact arithmetic
+    does: the images agree to rounding, and the reference's sensitivity only
+    ever has extra views."""
+    o = _proj("ct_mini5")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(13)
+    y = rng.uniform(0.0, 1.0, g.rays(-1))
+    ours, sens = orc.bdd_backward(g, y, -1, sens=True)
+    ref, rsens = ref_cl.RefCT(o, exact_inputs=True).bdd_backward(y, -1, sens=True)
+    assert orc.rel_l2(ours, ref) < PIN
+    assert np.all(rsens >= sens - 1e-9 * sens.max())
+    assert np.count_nonzero(rsens > sens + 1e-9 * sens.max()) > 0
+
+
+# ---------------------------------------------------------------------------
+# projector type 4 (interpolation)
+# ---------------------------------------------------------------------------
+
+# A FOV that is not a multiple of the crystal pitch: no sample of the PET
+# type-4 backprojection falls exactly on a voxel face.
+OFFSET_FOV = dict(FOVa_x=180.37, FOVa_y=180.37, axial_fov=33.71)
+
+
+@pytest.mark.parametrize("name,extra", [("pet_mini4", {}), ("pet_mini4", OFFSET_FOV),
+                                        ("pet_mini4_tof", OFFSET_FOV), ("ct_mini4", {})])
+def test_interp_forward_pinned(name, extra):
+    o = _proj(name, **extra)
+    g = orc.Geometry(o)
+    R = ref_cl.RefCT(o, exact_inputs=True) if o.CT else ref_cl.RefPET(o, exact_inputs=True)
+    rng = np.random.default_rng(14)
+    x = rng.uniform(0.5, 1.5, g.n_img)
+    for s in (0, 1):
+        ours = orc.interp_forward(g, x, s)
+        assert orc.rel_l2(ours, R.interp_forward(x, s)) < PIN
+        gpu_like = (ref_cl.RefCT(o) if o.CT else ref_cl.RefPET(o)).interp_forward(x, s, precision="f")
+        assert orc.rel_l2(gpu_like, ours) < 5e-3
+
+
+@pytest.mark.parametrize("name,extra", [("pet_mini4", OFFSET_FOV), ("pet_mini4_tof", OFFSET_FOV), ("ct_mini4", {})])
+def test_interp_backward_pinned(name, extra):
+    o = _proj(name, **extra)
+    g = orc.Geometry(o)
+    R = ref_cl.RefCT(o, exact_inputs=True) if o.CT else ref_cl.RefPET(o, exact_inputs=True)
+    rng = np.random.default_rng(15)
+    for s in (0, 1):
+        y = rng.uniform(0.0, 1.0, R.interp_forward(np.zeros(g.n_img), s).size)
+        back = orc.interp_ct_backward if o.CT else orc.interp_backward
+        ours, sens = back(g, y, s, sens=True)
+        ref, rsens = R.interp_backward(y, s, sens=True)
+        assert orc.rel_l2(ours, ref) < PIN
+        assert orc.rel_l2(sens, rsens) < PIN
+
+
+def test_interp_backward_face_samples():
+    """With a FOV of whole crystal pitches, axis-parallel PET rays sample
+    exactly on voxel faces and the nearest-voxel choice floor(p N) is decided
+    by rounding: the reference's own FP32 and FP64 runs differ there by a few
+    1e-3, and the restatement (FP64 decision) sits within that spread."""
+    o = _proj("pet_mini4")
+    g = orc.Geometry(o)
+    R = ref_cl.RefPET(o, exact_inputs=True)
+    rng = np.random.default_rng(16)
+    y = rng.uniform(0.0, 1.0, g.rays(0))
+    ours = orc.interp_backward(g, y, 0)
+    ref64 = R.interp_backward(y, 0)
+    ref32 = ref_cl.RefPET(o).interp_backward(y, 0, precision="f")
+    spread = orc.rel_l2(ref32, ref64)
+    assert 1e-4 < spread < 1e-2
+    assert orc.rel_l2(ours, ref64) < 2 * spread
+
+
+# ---------------------------------------------------------------------------
+# TV gradient and PDHG update
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("shape", [(17, 13, 9), (32, 32, 24)])
+@pytest.mark.parametrize("smooth", [1e-2, 1e-4])
+def test_tv_gradient_pinned(shape, smooth):
+    rng = np.random.default_rng(17)
+    u = rng.uniform(0.0, 1.0, int(np.prod(shape)))
+    ours = orc.tv_gradient(u, shape, smooth, 0.7)
+    ref = ref_cl.tv_gradient(u, shape, smooth, 0.7, exact_inputs=True)
+    assert orc.rel_l2(ours, ref) < 1e-13
+    ref32 = ref_cl.tv_gradient(u, shape, smooth, 0.7, precision="f")
+    assert orc.rel_l2(ours, ref32) < 1e-5
+
+
+def test_pdhg_update_pinned():
+    """One PDHG primal step of the restatement (oracle.pdhg_tv's update) equals
+    auxKernels.cl PDHGUpdate, with the clamp active on part of the image."""
+    shape = (20, 18, 7)
+    rng = np.random.default_rng(18)
+    n = int(np.prod(shape))
+    im, u = rng.uniform(0, 1, n), rng.uniform(0, 1, n)
+    rhs = rng.normal(0, 2, n)
+    tau, theta, eps = 0.3, 1.0, 1e-5
+    u_new = np.maximum(eps, u - tau * rhs)
+    x_new = u_new + theta * (u_new - u)
+    assert np.any(u - tau * rhs < eps)
+    ref_x, ref_u = ref_cl.pdhg_update(im, rhs, u, shape, tau, theta, eps, exact_inputs=True)
+    assert orc.rel_l2(x_new, ref_x) < 1e-15
+    assert orc.rel_l2(u_new, ref_u) < 1e-15
+
+
+def test_pdhg_iteration_pinned():
+    """Two PDHG+TV iterations of oracle.pdhg_tv against the same loop built
+    from the reference's kernels: its type-5 projector pair, TVKernel and
+    PDHGUpdate (dual step computeForwardProject.h:227-316)."""
+    o = _proj("ct_fine5")
+    g = orc.Geometry(o)
+    R = ref_cl.RefCT(o, exact_inputs=True)
+    shape = (g.nx, g.ny, g.nz)
+    rng = np.random.default_rng(19)
+    truth = rng.uniform(0.0, 0.02, g.n_img)
+    y = orc.bdd_forward(g, truth, -1)
+    x0 = np.full(g.n_img, 1e-3)
+    tau, beta, smooth, sigma = 1e-4, 0.01, 1e-4, 1.0
+    ours = orc.pdhg_tv(g, y, x0, 2, tau, beta, smooth, sigma=sigma)
+    x, u = x0.copy(), x0.copy()
+    p = np.zeros(g.rays(-1))
+    for _ in range(2):
+        p = (p + sigma * (R.bdd_forward(x, -1) - y)) / (1.0 + sigma)
+        rhs = R.bdd_backward(p, -1) + ref_cl.tv_gradient(x, shape, smooth, beta, exact_inputs=True)
+        x, u = ref_cl.pdhg_update(x, rhs, u, shape, tau, 1.0, 1e-5, exact_inputs=True)
+    assert orc.rel_l2(ours, x) < PIN
