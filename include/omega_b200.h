@@ -636,15 +636,18 @@ size_t omb_reduce_workspace_bytes(int64_t n);
  * allocation-free form of omb_backward(..., OMB_BP_FIXED64, ...) and gives
  * the same result.
  * No handle: `desc` is the same descriptor as for omb_create, except that
- * desc->xy, desc->z and desc->tof_centers are DEVICE pointers (n_meas stays
- * a host array).  y, image and sens (may be NULL) are device buffers; image
- * and sens are overwritten.  Images above OMB_NOALLOC_MAX_VOXELS voxels are
+ * the per-ray geometry is already on the device: desc->xy, desc->z and
+ * desc->tof_centers are DEVICE pointers, while desc->n_meas stays a HOST
+ * array (it is read on the host to size the launch).  y, image and sens (may
+ * be NULL) are device buffers; image and sens are overwritten.  Images above OMB_NOALLOC_MAX_VOXELS voxels are
  * rejected with OMB_ERR_UNSUPPORTED.
  * The scratch array is shared by all calls and keeps the last call's
  * contents (each call clears what it uses); calls that overlap on the GPU
  * (different streams or threads on one device) race on it.  The first call
  * on each device looks up the array's device address (cudaGetSymbolAddress)
- * and caches it; make that first call before any stream capture.
+ * and caches it; make that first call before any stream capture.  The
+ * cached address belongs to the device's primary context: calls after
+ * cudaDeviceReset on that device are not supported.
  */
 int omb_backward_fixed64_noalloc(const omb_geometry_desc *desc, int32_t subset, const float *y, float *image,
                                  float *sens, void *stream);

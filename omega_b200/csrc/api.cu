@@ -41,6 +41,7 @@ struct omb_handle {
     unsigned long long *d_acc = nullptr;  // 2 * N int64 accumulators (fixed-point BP)
     float *d_imgT = nullptr;              // y-fastest image copy (type-5 forward projection)
     BddProj *d_bddp = nullptr;            // per-projection maps (type-5 backprojection)
+    BddMap64 *d_bddm64 = nullptr;         // the same maps in FP64 (re-based per block by the type-5 backprojection)
     int64_t n_img = 0;
     Tuning tune{};
     int read_mode = OMB_READ_FP32;        // image precision of the type-1/4 forward projections
@@ -87,8 +88,9 @@ static void attach_interleave(omb_handle *h, Frames &f, cudaStream_t s) {
 // same vectors the reference's computeGeom5 uses (omegatomo/projector/
 // init.py:6-37): panel corner d3 = d - apuX - apuY, unit axes along apuX and
 // apuY, plane normal cross(apuX - apuY, -apuX - apuY).
-static std::vector<BddProj> bdd_maps(const omb_geometry_desc &d) {
+static std::vector<BddProj> bdd_maps(const omb_geometry_desc &d, std::vector<BddMap64> *maps64 = nullptr) {
     std::vector<BddProj> out((size_t)d.n_proj);
+    if (maps64) maps64->assign((size_t)d.n_proj, BddMap64{});
     const double nr2 = (double)d.n_rows_d / 2.0, nc2 = (double)d.n_cols_d / 2.0;
     for (int64_t p = 0; p < d.n_proj; ++p) {
         const float *q = d.xy + p * 6;
@@ -124,6 +126,16 @@ static std::vector<BddProj> bdd_maps(const omb_geometry_desc &d) {
         }
         P.au0 = (float)(-dot(cu, s) / ((double)d.dpitch_x * D0));
         P.av0 = (float)(-dot(cv, s) / ((double)d.dpitch_y * D0));
+        if (maps64) {
+            BddMap64 &M = (*maps64)[(size_t)p];
+            for (int k = 0; k < 3; ++k) {
+                M.au[k] = cu[k] / ((double)d.dpitch_x * D0);
+                M.av[k] = cv[k] / ((double)d.dpitch_y * D0);
+                M.c[k] = n[k] / D0;
+            }
+            M.au0 = -dot(cu, s) / ((double)d.dpitch_x * D0);
+            M.av0 = -dot(cv, s) / ((double)d.dpitch_y * D0);
+        }
         P.ysl = fabs(s[0]) <= fabs(s[1]);
         P.spos = P.ysl ? (s[1] > 0.0) : (s[0] > 0.0);
         const double dms[3] = {dd[0] - s[0], dd[1] - s[1], dd[2] - s[2]};
@@ -480,10 +492,14 @@ int omb_create(const omb_geometry_desc *desc, omb_handle **out) {
             return fail(cuda_fail(e, "cudaMalloc type-5 image copy"));
     }
     if (desc->bp_type == 5 || (desc->bp_type == 4 && desc->modality == OMB_CT_PANEL)) {
-        std::vector<BddProj> maps = bdd_maps(*desc);
-        if ((e = cudaMalloc(&h->d_bddp, maps.size() * sizeof(BddProj))) != cudaSuccess)
+        std::vector<BddMap64> maps64;
+        std::vector<BddProj> maps = bdd_maps(*desc, &maps64);
+        if ((e = cudaMalloc(&h->d_bddp, maps.size() * sizeof(BddProj))) != cudaSuccess ||
+            (e = cudaMalloc(&h->d_bddm64, maps64.size() * sizeof(BddMap64))) != cudaSuccess)
             return fail(cuda_fail(e, "cudaMalloc type-5 projection maps"));
-        if ((e = cudaMemcpy(h->d_bddp, maps.data(), maps.size() * sizeof(BddProj), cudaMemcpyHostToDevice)) != cudaSuccess)
+        if ((e = cudaMemcpy(h->d_bddp, maps.data(), maps.size() * sizeof(BddProj), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(h->d_bddm64, maps64.data(), maps64.size() * sizeof(BddMap64), cudaMemcpyHostToDevice)) !=
+                cudaSuccess)
             return fail(cuda_fail(e, "upload type-5 projection maps"));
     }
     if (desc->fixed64_workspace) {
@@ -530,6 +546,7 @@ int omb_destroy(omb_handle *h) {
     cudaFree(h->d_acc);
     cudaFree(h->d_imgT);
     cudaFree(h->d_bddp);
+    cudaFree(h->d_bddm64);
     cudaFree(h->d_img16);
     cudaFree(h->d_ilv);
     cudaFree(h->d_w);
@@ -606,8 +623,8 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
     if (h->desc.bp_type == 5) {
         if (mode != OMB_BP_FLOAT_ATOMIC)
             return set_error(OMB_ERR_UNSUPPORTED, "the type-5 backprojection is a gather; it has no fixed-point mode");
-        return bdd_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y, image, sens,
-                            h->tune, s);
+        return bdd_backward(h->grid, h->d_bddp + rs.proj0, h->d_bddm64 + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y,
+                            image, sens, h->tune, s);
     }
     if (h->desc.bp_type == 4 && h->desc.modality == OMB_CT_PANEL) {
         if (mode != OMB_BP_FLOAT_ATOMIC)

@@ -140,22 +140,30 @@ __global__ void k_transpose_xy(const float *__restrict__ in, float *__restrict__
 // m = floor(v): two shared-memory reads per voxel instead of a walk over its
 // detector pixels.
 template <int kBpZ, bool SENS, bool FULL, int kBpThreads>
-__global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
-                                                       int64_t nproj, const float *__restrict__ y,
-                                                       float *__restrict__ img, float *__restrict__ sens) {
+__global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, const BddMap64 *__restrict__ pm, int nr, int nc,
+                         int64_t nproj, const float *__restrict__ y, float *__restrict__ img,
+                         float *__restrict__ sens) {
     constexpr int kBpCols = bp_slots(kBpZ);
     __shared__ float2 pref[kBpCols][kBpThreads];  // (P_m, RS_m) of column cA + m
+    __shared__ BddMapR smap[2];                   // the projection's map re-based to this block (double-buffered)
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = blockIdx.x * blockDim.x, j0 = blockIdx.y * blockDim.y;
+    const int i = i0 + threadIdx.x;
+    const int j = j0 + threadIdx.y;
     const int kz0 = blockIdx.z * kBpZ;
-    if (i >= g.nx || j >= g.ny || kz0 >= g.nz) return;
-    const int nzt = FULL ? kBpZ : min(kBpZ, g.nz - kz0);  // FULL: nz is a multiple of kBpZ
+    const bool active = i < g.nx && j < g.ny && kz0 < g.nz;
+    const int nzt = FULL ? kBpZ : max(min(kBpZ, g.nz - kz0), 0);  // FULL: nz is a multiple of kBpZ
+    // voxel centre relative to the block corner p0 (exact for grid steps)
+    const float rx0 = ((float)(i - i0) + 0.5f) * g.dx;
+    const float ry0 = ((float)(j - j0) + 0.5f) * g.dy;
+    const float rz0 = 0.5f * g.dz;
     const float qx = fmaf((float)i, g.dx, g.bx + 0.5f * g.dx);
     const float qy = fmaf((float)j, g.dy, g.by + 0.5f * g.dy);
     const float qz0 = fmaf((float)kz0, g.dz, g.bz + 0.5f * g.dz);
     const float hx = 0.5f * g.dx, hy = 0.5f * g.dy, hz = 0.5f * g.dz;
-    const float fnr = (float)nr, fnc = (float)nc;
+    // block corner (FP64), for the re-based maps
+    const double p0x = (double)g.bx + (double)i0 * g.dx, p0y = (double)g.by + (double)j0 * g.dy;
+    const double p0z = (double)g.bz + (double)kz0 * g.dz;
     float temp[kBpZ], wsum[kBpZ];
 #pragma unroll
     for (int t = 0; t < kBpZ; ++t) {
@@ -163,39 +171,34 @@ __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
         wsum[t] = 0.f;
     }
     for (int64_t p = 0; p < nproj; ++p) {
-        const BddProj P = pj[p];
-        float lx, ly, rx, ry;
-        const float sgn = P.spos ? 1.f : -1.f;
-        if (P.ysl) {
-            lx = qx - sgn * hx; rx = qx + sgn * hx; ly = qy; ry = qy;
-        } else {
-            lx = qx; rx = qx; ly = qy + sgn * hy; ry = qy - sgn * hy;
+        // one thread re-bases the map to the block, with the pixel origin the
+        // TMA-staged kernel gives a block of the same shape (the lowest row /
+        // column its 8 corners reach), so both compute the same numbers
+        if (tid == 0) {
+            const BddProj P = pj[p];
+            float umin = 3.4e38f, vmin = 3.4e38f;
+            for (int q = 0; q < 8; ++q) {
+                const float cx = g.bx + (float)((q & 1) ? min(i0 + (int)blockDim.x, g.nx) : i0) * g.dx;
+                const float cy = g.by + (float)((q & 2) ? min(j0 + (int)blockDim.y, g.ny) : j0) * g.dy;
+                const float cz = g.bz + (float)((q & 4) ? min(kz0 + kBpZ, g.nz) : kz0) * g.dz;
+                const float2 uv = bdd_corner_uv(P, cx, cy, cz);
+                umin = fminf(umin, uv.x);
+                vmin = fminf(vmin, uv.y);
+            }
+            const int2 org = bdd_block_origin(umin, vmin, nr, nc);
+            bdd_rebase(smap[p & 1], pm[p], P, p0x, p0y, p0z, org.x, org.y);
         }
-        // z-independent parts (P.c[2] == 0 and P.au[2] == 0 for these panels)
-        const float dl = 1.f / fmaf(P.c[0], lx, fmaf(P.c[1], ly, fmaf(P.c[2], qz0, 1.f)));
-        const float dr = 1.f / fmaf(P.c[0], rx, fmaf(P.c[1], ry, fmaf(P.c[2], qz0, 1.f)));
-        const float ul = fmaf(P.au[0], lx, fmaf(P.au[1], ly, fmaf(P.au[2], qz0, P.au0))) * dl;
-        const float ur = fmaf(P.au[0], rx, fmaf(P.au[1], ry, fmaf(P.au[2], qz0, P.au0))) * dr;
-        const float ua = fmaxf(fminf(ul, ur), 0.f), ub = fminf(fmaxf(ul, ur), fnr);
-        if (!(ub > ua)) continue;
-        const int r0 = (int)ua;  // ua >= 0: truncation is floor
-        const Seg seg = make_seg(ua, ub, r0, min((int)ceilf(ub), nr) - 1 - r0);
-        // v of the two corners of voxel t: linear in t
-        const float vl0 = fmaf(P.av[0], lx, fmaf(P.av[1], ly, fmaf(P.av[2], qz0 - hz, P.av0))) * dl;
-        const float vr0 = fmaf(P.av[0], rx, fmaf(P.av[1], ry, fmaf(P.av[2], qz0 + hz, P.av0))) * dr;
-        const float svl = P.av[2] * g.dz * dl, svr = P.av[2] * g.dz * dr;
-        const float tl = (float)(nzt - 1);
-        const float vA = fmaxf(fminf(fminf(vl0, vr0), fminf(fmaf(tl, svl, vl0), fmaf(tl, svr, vr0))), 0.f);
-        const float vB = fminf(fmaxf(fmaxf(vl0, vr0), fmaxf(fmaf(tl, svl, vl0), fmaf(tl, svr, vr0))), fnc);
-        if (!(vB > vA)) continue;
-        // kerroin = d * |v| / |v_axis|, v = voxel centre - source
-        const float vx = qx - P.s[0], vy = qy - P.s[1];
-        const float axy = vx * vx + vy * vy;
-        const float kscale = P.ysl ? __fdividef(g.dy, fabsf(vy)) : __fdividef(g.dx, fabsf(vx));
-        const float *yp = y + p * (int64_t)nr * nc + r0;
+        __syncthreads();
+        if (!active) continue;
+        const BddMapR M = smap[p & 1];
+        BpFootprint F;
+        if (!bdd_bp_footprint(M, rx0, ry0, rz0, hx, hy, hz, qx, qy, g, nr, nc, nzt, F)) continue;
+        const Seg &seg = F.seg;
+        const int r0 = F.r0, cA = F.cA, ncols = F.ncols;
+        const float V0 = F.V0, vl0 = F.vl0, vr0 = F.vr0, svl = F.svl, svr = F.svr, vA = F.vA, vB = F.vB;
+        const float axy = F.axy, kscale = F.kscale;
+        const float *yp = y + p * (int64_t)nr * nc + (int64_t)M.o.y * nr + M.o.x + r0;
 #define col_sum(c) seg_sum(seg, yp + (int64_t)(c) * nr)
-        const int cA = (int)vA;
-        const int ncols = min((int)ceilf(vB), nc) - cA;
         if (ncols <= kBpCols) {
             float acc = 0.f;
 #pragma unroll 4
@@ -210,14 +213,14 @@ __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
             for (int t = 0; t < kBpZ; ++t) {
                 if (FULL || t < nzt) {
                     const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
-                    // clamp to [vA, vB] (inside [0, nc]); an empty footprint gives va == vb
+                    // clamp to [vA, vB] (inside the panel); an empty footprint gives va == vb
                     const float qa = fminf(fmaxf(fminf(vlt, vrt), vA), vB) - fA;
                     const float qb = fminf(fmaxf(fmaxf(vlt, vrt), vA), vB) - fA;
                     const int ma = min((int)qa, mmax), mb = min((int)qb, mmax);
                     const float2 ea = pref[ma][tid], eb = pref[mb][tid];
                     const float apu = fmaf(qb - (float)mb, eb.y, eb.x) - fmaf(qa - (float)ma, ea.y, ea.x);
                     if (apu != 0.f) {
-                        const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
+                        const float vz = fmaf((float)t, g.dz, qz0) - M.s.z;
                         const float q2 = fmaf(vz, vz, axy);
                         const float ker = kscale * (q2 * rsqrtf(q2));
                         temp[t] = fmaf(apu, ker, temp[t]);
@@ -230,16 +233,16 @@ __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
 #pragma unroll
             for (int t = 0; t < kBpZ; ++t) {
                 const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
-                const float va = fmaxf(fminf(vlt, vrt), 0.f), vb = fminf(fmaxf(vlt, vrt), fnc);
+                const float va = fmaxf(fminf(vlt, vrt), -V0), vb = fminf(fmaxf(vlt, vrt), (float)nc - V0);
                 if ((FULL || t < nzt) && vb > va) {
-                    const int c0 = (int)va, c1 = min((int)ceilf(vb), nc) - 1;
+                    const int c0 = (int)floorf(va), c1 = min((int)ceilf(vb), nc - M.o.y) - 1;
                     float apu = 0.f;
                     for (int c = c0; c <= c1; ++c) {
                         const float ov = fminf(vb, (float)(c + 1)) - fmaxf(va, (float)c);
                         apu = fmaf(ov, col_sum(c), apu);
                     }
                     if (apu != 0.f) {
-                        const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
+                        const float vz = fmaf((float)t, g.dz, qz0) - M.s.z;
                         const float q2 = fmaf(vz, vz, axy);
                         const float ker = kscale * (q2 * rsqrtf(q2));
                         temp[t] = fmaf(apu, ker, temp[t]);
@@ -250,6 +253,7 @@ __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, int nr, int nc,
         }
 #undef col_sum
     }
+    if (!active) return;
     int64_t n = i + (int64_t)j * g.nx + (int64_t)kz0 * g.nx * g.ny;
 #pragma unroll
     for (int t = 0; t < kBpZ; ++t) {
@@ -272,28 +276,30 @@ static void launch_fp(const Grid &g, const float *xy, const float *uv, int nr, i
 }
 
 template <int Z, int T>
-static void launch_bp_t(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                        float *sens, cudaStream_t st) {
+static void launch_bp_t(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
+                        const float *y, float *img, float *sens, cudaStream_t st) {
     dim3 block(32, T / 32);
     dim3 grid((g.nx + 31) / 32, (g.ny + block.y - 1) / block.y, (g.nz + Z - 1) / Z);
     const bool full = g.nz % Z == 0;
     if (sens && full)
-        k_bdd_bp<Z, true, true, T><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+        k_bdd_bp<Z, true, true, T><<<grid, block, 0, st>>>(g, pj, pm, nr, nc, nproj, y, img, sens);
     else if (sens)
-        k_bdd_bp<Z, true, false, T><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+        k_bdd_bp<Z, true, false, T><<<grid, block, 0, st>>>(g, pj, pm, nr, nc, nproj, y, img, sens);
     else if (full)
-        k_bdd_bp<Z, false, true, T><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+        k_bdd_bp<Z, false, true, T><<<grid, block, 0, st>>>(g, pj, pm, nr, nc, nproj, y, img, sens);
     else
-        k_bdd_bp<Z, false, false, T><<<grid, block, 0, st>>>(g, pj, nr, nc, nproj, y, img, sens);
+        k_bdd_bp<Z, false, false, T><<<grid, block, 0, st>>>(g, pj, pm, nr, nc, nproj, y, img, sens);
 }
 
 template <int Z>
-static void launch_bp(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                      float *sens, int rows, cudaStream_t st) {
-    if (rows == 4)
-        launch_bp_t<Z, 128>(g, pj, nr, nc, nproj, y, img, sens, st);
+static void launch_bp(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
+                      const float *y, float *img, float *sens, int rows, cudaStream_t st) {
+    // 16 voxels along z: the prefix slots of 256 threads would exceed 48 KB
+    // of static shared memory, so that shape runs 128-thread blocks
+    if (rows == 4 || Z == 16)
+        launch_bp_t<Z, 128>(g, pj, pm, nr, nc, nproj, y, img, sens, st);
     else
-        launch_bp_t<Z, 256>(g, pj, nr, nc, nproj, y, img, sens, st);
+        launch_bp_t<Z < 16 ? Z : 8, 256>(g, pj, pm, nr, nc, nproj, y, img, sens, st);
 }
 
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
@@ -313,16 +319,16 @@ int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc,
     return OMB_OK;
 }
 
-int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                 float *sens, const Tuning &tn, cudaStream_t st) {
+int bdd_backward(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj, const float *y,
+                 float *img, float *sens, const Tuning &tn, cudaStream_t st) {
     if (g.nz > 65535 * 4) return set_error(OMB_ERR_UNSUPPORTED, "too many slices");
     if (tn.bdd_bp_staged && tn.bdd_bp_z == 8 && bdd_bp_tma_supported(nr, y))
-        return bdd_backward_tma(g, pj, nr, nc, nproj, y, img, sens, st);
+        return bdd_backward_tma(g, pj, pm, nr, nc, nproj, y, img, sens, st);
     const int rows = tn.bdd_bp_rows;
     switch (tn.bdd_bp_z) {
-        case 4: launch_bp<4>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;
-        case 16: launch_bp<16>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;
-        default: launch_bp<8>(g, pj, nr, nc, nproj, y, img, sens, rows, st); break;
+        case 4: launch_bp<4>(g, pj, pm, nr, nc, nproj, y, img, sens, rows, st); break;
+        case 16: launch_bp<16>(g, pj, pm, nr, nc, nproj, y, img, sens, rows, st); break;
+        default: launch_bp<8>(g, pj, pm, nr, nc, nproj, y, img, sens, rows, st); break;
     }
     OMB_LAUNCH_CHECK("bdd backward launch");
     return OMB_OK;

@@ -124,6 +124,61 @@ __device__ __forceinline__ float seg_sum(const Seg &s, const float *__restrict__
 // the per-voxel path (about 1.25 columns per voxel at magnification 2)
 __host__ __device__ constexpr int bp_slots(int kBpZ) { return kBpZ + kBpZ / 2 + (kBpZ < 16 ? 4 : 0); }
 
+// One voxel column's footprint on one projection for the backprojection:
+// rows [ua, ub] (shared by the column's voxels: u does not depend on z for
+// these panels) with their weights `seg`, the columns [vA, vB] the whole run
+// of nzt voxels covers, and the per-voxel column edges v = v0 + t s (left and
+// right corner).  Coordinates are relative to the re-based map's pixel origin
+// (U0, V0); (rx0, ry0, rz0) is the first voxel's centre relative to the
+// block corner, (qx, qy) its world x and y.  False when the footprint misses
+// the panel.
+struct BpFootprint {
+    Seg seg;
+    int r0, cA, ncols;
+    float U0, V0;
+    float vl0, vr0, svl, svr, vmin, vmax, vA, vB;
+    float axy, kscale;
+};
+
+__device__ __forceinline__ bool bdd_bp_footprint(const BddMapR &M, float rx0, float ry0, float rz0, float hx, float hy,
+                                                 float hz, float qx, float qy, const Grid &g, int nr, int nc, int nzt,
+                                                 BpFootprint &F) {
+    F.U0 = M.s.w;
+    F.V0 = (float)M.o.y;
+    float lx, ly, rx, ry;
+    const float sgn = M.o.w ? 1.f : -1.f;
+    if (M.o.z) {
+        lx = rx0 - sgn * hx; rx = rx0 + sgn * hx; ly = ry0; ry = ry0;
+    } else {
+        lx = rx0; rx = rx0; ly = ry0 + sgn * hy; ry = ry0 - sgn * hy;
+    }
+    const float dl = 1.f / fmaf(M.c.x, lx, fmaf(M.c.y, ly, fmaf(M.c.z, rz0, M.c.w)));
+    const float dr = 1.f / fmaf(M.c.x, rx, fmaf(M.c.y, ry, fmaf(M.c.z, rz0, M.c.w)));
+    const float ul = fmaf(M.u.x, lx, fmaf(M.u.y, ly, fmaf(M.u.z, rz0, M.u.w))) * dl;
+    const float ur = fmaf(M.u.x, rx, fmaf(M.u.y, ry, fmaf(M.u.z, rz0, M.u.w))) * dr;
+    const float ua = fmaxf(fminf(ul, ur), -F.U0), ub = fminf(fmaxf(ul, ur), (float)nr - F.U0);
+    if (!(ub > ua)) return false;
+    F.r0 = (int)floorf(ua);
+    F.seg = make_seg(ua, ub, F.r0, min((int)ceilf(ub), nr - M.o.x) - 1 - F.r0);
+    F.vl0 = fmaf(M.v.x, lx, fmaf(M.v.y, ly, fmaf(M.v.z, rz0 - hz, M.v.w))) * dl;
+    F.vr0 = fmaf(M.v.x, rx, fmaf(M.v.y, ry, fmaf(M.v.z, rz0 + hz, M.v.w))) * dr;
+    F.svl = M.v.z * g.dz * dl;
+    F.svr = M.v.z * g.dz * dr;
+    const float tl = (float)(nzt - 1);
+    F.vmin = fminf(fminf(F.vl0, F.vr0), fminf(fmaf(tl, F.svl, F.vl0), fmaf(tl, F.svr, F.vr0)));
+    F.vmax = fmaxf(fmaxf(F.vl0, F.vr0), fmaxf(fmaf(tl, F.svl, F.vl0), fmaf(tl, F.svr, F.vr0)));
+    F.vA = fmaxf(F.vmin, -F.V0);
+    F.vB = fminf(F.vmax, (float)nc - F.V0);
+    if (!(F.vB > F.vA)) return false;
+    // kerroin = d * |v| / |v_axis|, v = voxel centre - source
+    const float vx = qx - M.s.x, vy = qy - M.s.y;
+    F.axy = vx * vx + vy * vy;
+    F.kscale = M.o.z ? __fdividef(g.dy, fabsf(vy)) : __fdividef(g.dx, fabsf(vx));
+    F.cA = (int)floorf(F.vA);
+    F.ncols = min((int)ceilf(F.vB), nc - M.o.y) - F.cA;
+    return true;
+}
+
 // seg_sum over a run staged in shared memory (plain loads, same arithmetic).
 __device__ __forceinline__ float seg_sum_shared(const Seg &s, const float *p) {
     float acc = fmaf(s.w2, p[s.o2], fmaf(s.w1, p[s.o1], s.w0 * p[0]));

@@ -263,16 +263,17 @@ constexpr int kStages = 4;
 struct Shared {
     alignas(128) float box[kStages][kStageFloats];
     alignas(8) uint64_t full[kStages];
-    int2 origin[kStages];  // (row, column) of the box's first element
+    BddMapR map[kStages];  // the stage's map re-based to this block; (U0, V0) = the box's first element
     float2 pref[kSlots][kThreads];
 };
 
 }  // namespace bb
 
 template <bool SENS, bool FULL>
-__global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_constant__ CUtensorMap map_y, Grid g, const BddProj *__restrict__ pj,
-                             int nr, int nc, int64_t nproj, const float *__restrict__ y, float *__restrict__ img,
-                             float *__restrict__ sens) {
+__global__ void __launch_bounds__(bb::kThreads, 6)
+    k_bdd_bp_tma(const __grid_constant__ CUtensorMap map_y, Grid g, const BddProj *__restrict__ pj,
+                 const BddMap64 *__restrict__ pm, int nr, int nc, int64_t nproj, const float *__restrict__ y,
+                 float *__restrict__ img, float *__restrict__ sens) {
     using namespace bb;
     constexpr int kBpZ = kZ;
     __shared__ Shared sh;
@@ -294,23 +295,23 @@ __global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_con
     const float cx = g.bx + (float)((lane & 1) ? min((int)blockIdx.x * 32 + 32, g.nx) : (int)blockIdx.x * 32) * g.dx;
     const float cy = g.by + (float)((lane & 2) ? min((int)blockIdx.y * 4 + 4, g.ny) : (int)blockIdx.y * 4) * g.dy;
     const float cz = g.bz + (float)((lane & 4) ? min(kz0 + kBpZ, g.nz) : kz0) * g.dz;
+    const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 4;
+    const double p0x = (double)g.bx + (double)i0 * g.dx, p0y = (double)g.by + (double)j0 * g.dy;
+    const double p0z = (double)g.bz + (double)kz0 * g.dz;
     // loads the box of projection pn into stage s (a whole warp; lane 0 issues)
     auto produce = [&](int64_t pn, int s) {
         const BddProj P = pj[pn];
-        const float den = 1.f / fmaf(P.c[0], cx, fmaf(P.c[1], cy, fmaf(P.c[2], cz, 1.f)));
-        float u = fmaf(P.au[0], cx, fmaf(P.au[1], cy, fmaf(P.au[2], cz, P.au0))) * den;
-        float v = fmaf(P.av[0], cx, fmaf(P.av[1], cy, fmaf(P.av[2], cz, P.av0))) * den;
+        float2 uv = bdd_corner_uv(P, cx, cy, cz);
 #pragma unroll
         for (int o = 1; o < 8; o <<= 1) {
-            u = fminf(u, __shfl_xor_sync(0xffffffffu, u, o));
-            v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+            uv.x = fminf(uv.x, __shfl_xor_sync(0xffffffffu, uv.x, o));
+            uv.y = fminf(uv.y, __shfl_xor_sync(0xffffffffu, uv.y, o));
         }
         if (lane == 0) {
-            int r = (int)floorf(fmaxf(u - 1.f, 0.f));
-            r = min(r, nr - 1) & ~3;
-            int c = (int)floorf(fmaxf(v - 1.f, 0.f));
-            c = min(c, nc - 1);
-            sh.origin[s] = make_int2(r, c);
+            const int2 org = bdd_block_origin(uv.x, uv.y, nr, nc);
+            // the map re-based to the block corner with the box origin as pixel
+            // origin (FP64), published to the consumers by the arrive below
+            bdd_rebase(sh.map[s], pm[pn], P, p0x, p0y, p0z, org.x, org.y);
             const uint32_t bar = bt::smem_u32(&sh.full[s]);
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
                          "r"((uint32_t)(kRW * kCW * sizeof(float)))
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_con
             asm volatile(
                 "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
                 "%4}], [%5];\n" ::"r"(bt::smem_u32(sh.box[s])),
-                "l"(reinterpret_cast<uint64_t>(&map_y)), "r"(r), "r"(c), "r"((int)pn), "r"(bar)
+                "l"(reinterpret_cast<uint64_t>(&map_y)), "r"(org.x), "r"(org.y), "r"((int)pn), "r"(bar)
                 : "memory");
         }
     };
@@ -326,6 +327,10 @@ __global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_con
         for (int s = 0; s < kStages && s < nproj; ++s) produce(s, s);
 
     const int nzt = FULL ? kBpZ : min(kBpZ, g.nz - kz0);
+    // voxel centre relative to the block corner (exact for grid steps)
+    const float rx0 = ((float)(i - i0) + 0.5f) * g.dx;
+    const float ry0 = ((float)(j - j0) + 0.5f) * g.dy;
+    const float rz0 = 0.5f * g.dz;
     const float qx = fmaf((float)i, g.dx, g.bx + 0.5f * g.dx);
     const float qy = fmaf((float)j, g.dy, g.by + 0.5f * g.dy);
     const float qz0 = fmaf((float)kz0, g.dz, g.bz + 0.5f * g.dz);
@@ -346,42 +351,19 @@ __global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_con
         }
         do {
             if (!active) break;
-            const BddProj P = pj[p];
-            float lx, ly, rx, ry;
-            const float sgn = P.spos ? 1.f : -1.f;
-            if (P.ysl) {
-                lx = qx - sgn * hx; rx = qx + sgn * hx; ly = qy; ry = qy;
-            } else {
-                lx = qx; rx = qx; ly = qy + sgn * hy; ry = qy - sgn * hy;
-            }
-            const float dl = 1.f / fmaf(P.c[0], lx, fmaf(P.c[1], ly, fmaf(P.c[2], qz0, 1.f)));
-            const float dr = 1.f / fmaf(P.c[0], rx, fmaf(P.c[1], ry, fmaf(P.c[2], qz0, 1.f)));
-            const float ul = fmaf(P.au[0], lx, fmaf(P.au[1], ly, fmaf(P.au[2], qz0, P.au0))) * dl;
-            const float ur = fmaf(P.au[0], rx, fmaf(P.au[1], ry, fmaf(P.au[2], qz0, P.au0))) * dr;
-            const float ua = fmaxf(fminf(ul, ur), 0.f), ub = fminf(fmaxf(ul, ur), fnr);
-            if (!(ub > ua)) break;
-            const int r0 = (int)ua;
-            const Seg seg = make_seg(ua, ub, r0, min((int)ceilf(ub), nr) - 1 - r0);
-            const float vl0 = fmaf(P.av[0], lx, fmaf(P.av[1], ly, fmaf(P.av[2], qz0 - hz, P.av0))) * dl;
-            const float vr0 = fmaf(P.av[0], rx, fmaf(P.av[1], ry, fmaf(P.av[2], qz0 + hz, P.av0))) * dr;
-            const float svl = P.av[2] * g.dz * dl, svr = P.av[2] * g.dz * dr;
-            const float tl = (float)(nzt - 1);
-            const float vmin = fminf(fminf(vl0, vr0), fminf(fmaf(tl, svl, vl0), fmaf(tl, svr, vr0)));
-            const float vmax = fmaxf(fmaxf(vl0, vr0), fmaxf(fmaf(tl, svl, vl0), fmaf(tl, svr, vr0)));
-            const float vA = fmaxf(vmin, 0.f);
-            const float vB = fminf(vmax, fnc);
-            if (!(vB > vA)) break;
-            const float vx = qx - P.s[0], vy = qy - P.s[1];
-            const float axy = vx * vx + vy * vy;
-            const float kscale = P.ysl ? __fdividef(g.dy, fabsf(vy)) : __fdividef(g.dx, fabsf(vx));
-            const int cA = (int)vA;
-            const int ncols = min((int)ceilf(vB), nc) - cA;
-            const int2 o = sh.origin[s];
-            const bool staged = r0 >= o.x && r0 + seg.n < o.x + kRW && cA >= o.y && cA + ncols <= o.y + kCW;
+            // u, v below are relative to the box origin (U0, V0)
+            const BddMapR M = sh.map[s];
+            BpFootprint F;
+            if (!bdd_bp_footprint(M, rx0, ry0, rz0, hx, hy, hz, qx, qy, g, nr, nc, nzt, F)) break;
+            const Seg &seg = F.seg;
+            const int r0 = F.r0, cA = F.cA, ncols = F.ncols;
+            const float V0 = F.V0, vl0 = F.vl0, vr0 = F.vr0, svl = F.svl, svr = F.svr, vA = F.vA, vB = F.vB;
+            const float vmin = F.vmin, vmax = F.vmax, axy = F.axy, kscale = F.kscale;
+            const bool staged = r0 >= 0 && r0 + seg.n < kRW && cA >= 0 && cA + ncols <= kCW;
             if (ncols <= kSlots) {
                 float acc = 0.f;
                 if (staged && seg.n <= 2) {
-                    const float *q = sh.box[s] + (cA - o.y) * kRW + (r0 - o.x);
+                    const float *q = sh.box[s] + cA * kRW + r0;
 #pragma unroll 4
                     for (int m = 0; m < ncols; ++m) {
                         const float rs = fmaf(seg.w2, q[seg.o2], fmaf(seg.w1, q[seg.o1], seg.w0 * q[0]));
@@ -390,7 +372,7 @@ __global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_con
                         q += kRW;
                     }
                 } else {
-                    const float *yp = y + p * (int64_t)nr * nc + r0;
+                    const float *yp = y + p * (int64_t)nr * nc + (int64_t)M.o.y * nr + M.o.x + r0;
 #pragma unroll 4
                     for (int m = 0; m < ncols; ++m) {
                         const float rs = seg_sum(seg, yp + (int64_t)(cA + m) * nr);
@@ -401,7 +383,7 @@ __global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_con
                 const float fA = (float)cA;
                 const int mmax = ncols - 1;
                 // inside the panel the clamps to [vA, vB] below are identities
-                const bool inside = vmin >= 0.f && vmax <= fnc;
+                const bool inside = vmin >= -V0 && vmax <= fnc - V0;
 #pragma unroll
                 for (int t = 0; t < kBpZ; ++t) {
                     if (FULL || t < nzt) {
@@ -413,7 +395,7 @@ __global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_con
                         const float2 ea = sh.pref[ma][tid], eb = sh.pref[mb][tid];
                         const float apu = fmaf(qb - (float)mb, eb.y, eb.x) - fmaf(qa - (float)ma, ea.y, ea.x);
                         if (apu != 0.f) {
-                            const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
+                            const float vz = fmaf((float)t, g.dz, qz0) - M.s.z;
                             const float q2 = fmaf(vz, vz, axy);
                             const float ker = kscale * (q2 * rsqrtf(q2));
                             temp[t] = fmaf(apu, ker, temp[t]);
@@ -422,20 +404,20 @@ __global__ void __launch_bounds__(bb::kThreads, 6) k_bdd_bp_tma(const __grid_con
                     }
                 }
             } else {
-                const float *yp = y + p * (int64_t)nr * nc + r0;
+                const float *yp = y + p * (int64_t)nr * nc + (int64_t)M.o.y * nr + M.o.x + r0;
 #pragma unroll
                 for (int t = 0; t < kBpZ; ++t) {
                     const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
-                    const float va = fmaxf(fminf(vlt, vrt), 0.f), vb = fminf(fmaxf(vlt, vrt), fnc);
+                    const float va = fmaxf(fminf(vlt, vrt), -V0), vb = fminf(fmaxf(vlt, vrt), fnc - V0);
                     if ((FULL || t < nzt) && vb > va) {
-                        const int c0 = (int)va, c1 = min((int)ceilf(vb), nc) - 1;
+                        const int c0 = (int)floorf(va), c1 = min((int)ceilf(vb), nc - M.o.y) - 1;
                         float apu = 0.f;
                         for (int c = c0; c <= c1; ++c) {
                             const float ov = fminf(vb, (float)(c + 1)) - fmaxf(va, (float)c);
                             apu = fmaf(ov, seg_sum(seg, yp + (int64_t)c * nr), apu);
                         }
                         if (apu != 0.f) {
-                            const float vz = fmaf((float)t, g.dz, qz0) - P.s[2];
+                            const float vz = fmaf((float)t, g.dz, qz0) - M.s.z;
                             const float q2 = fmaf(vz, vz, axy);
                             const float ker = kscale * (q2 * rsqrtf(q2));
                             temp[t] = fmaf(apu, ker, temp[t]);
@@ -514,8 +496,8 @@ bool bdd_bp_tma_supported(int nr, const float *y) {
     return nr % 4 == 0 && ((uintptr_t)y & 15) == 0 && encode_fn() != nullptr;
 }
 
-int bdd_backward_tma(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                     float *sens, cudaStream_t st) {
+int bdd_backward_tma(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
+                     const float *y, float *img, float *sens, cudaStream_t st) {
     if (nproj <= 0) return OMB_OK;
     auto fn = encode_fn();
     CUtensorMap m_y;
@@ -531,13 +513,13 @@ int bdd_backward_tma(const Grid &g, const BddProj *pj, int nr, int nc, int64_t n
     dim3 grid((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + bb::kZ - 1) / bb::kZ);
     const bool full = g.nz % bb::kZ == 0;
     if (sens && full)
-        k_bdd_bp_tma<true, true><<<grid, block, 0, st>>>(m_y, g, pj, nr, nc, nproj, y, img, sens);
+        k_bdd_bp_tma<true, true><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
     else if (sens)
-        k_bdd_bp_tma<true, false><<<grid, block, 0, st>>>(m_y, g, pj, nr, nc, nproj, y, img, sens);
+        k_bdd_bp_tma<true, false><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
     else if (full)
-        k_bdd_bp_tma<false, true><<<grid, block, 0, st>>>(m_y, g, pj, nr, nc, nproj, y, img, sens);
+        k_bdd_bp_tma<false, true><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
     else
-        k_bdd_bp_tma<false, false><<<grid, block, 0, st>>>(m_y, g, pj, nr, nc, nproj, y, img, sens);
+        k_bdd_bp_tma<false, false><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
     OMB_LAUNCH_CHECK("type-5 TMA backward launch");
     return OMB_OK;
 }

@@ -120,6 +120,72 @@ struct BddProj {
     float pad[3];
 };
 
+// The same map in FP64 (the values BddProj rounds), for re-basing it to one
+// thread block: evaluated in FP32 at pixel coordinates of several hundred the
+// map carries ~3e-5 pixels of rounding, which moves a backprojection by
+// ~1e-5 relative L2 at 512^2 panels; re-based it carries ~2e-6.
+struct BddMap64 {
+    double au[3], au0;
+    double av[3], av0;
+    double c[3], pad;
+};
+
+// A projection's map re-based to one block of voxels: with d = q - p0 (p0 a
+// corner of the block) and integer pixel origins (U0, V0),
+//   u - U0 = (au . d + nu0) / (c . d + d0),  v - V0 = (av . d + nv0) / (c . d + d0),
+// coefficients rounded to FP32 from FP64.  Also carries what the voxel loop
+// needs of BddProj (source, slice orientation) so it reads no global memory.
+// Laid out as 16-byte vectors so a thread reads it with five vector loads:
+//   u = (au.x, au.y, au.z, nu0), v = (av.x, av.y, av.z, nv0),
+//   c = (c.x, c.y, c.z, d0), s = (source x, y, z, float(U0)),
+//   o = (U0, V0, ysl, spos).
+struct alignas(16) BddMapR {
+    float4 u, v, c, s;
+    int4 o;
+};
+
+// Re-bases M to the block corner p0 with pixel origins (U0, V0), in FP64.
+__device__ __forceinline__ void bdd_rebase(BddMapR &R, const BddMap64 &M, const BddProj &P, double p0x, double p0y,
+                                           double p0z, int U0, int V0) {
+    const double D0 = fma(M.c[0], p0x, fma(M.c[1], p0y, fma(M.c[2], p0z, 1.0)));
+    const double Nu = fma(M.au[0], p0x, fma(M.au[1], p0y, fma(M.au[2], p0z, M.au0)));
+    const double Nv = fma(M.av[0], p0x, fma(M.av[1], p0y, fma(M.av[2], p0z, M.av0)));
+    const double u0 = (double)U0, v0 = (double)V0;
+    R.u = make_float4((float)(M.au[0] - u0 * M.c[0]), (float)(M.au[1] - u0 * M.c[1]), (float)(M.au[2] - u0 * M.c[2]),
+                      (float)(Nu - u0 * D0));
+    R.v = make_float4((float)(M.av[0] - v0 * M.c[0]), (float)(M.av[1] - v0 * M.c[1]), (float)(M.av[2] - v0 * M.c[2]),
+                      (float)(Nv - v0 * D0));
+    R.c = make_float4((float)M.c[0], (float)M.c[1], (float)M.c[2], (float)D0);
+    R.s = make_float4(P.s[0], P.s[1], P.s[2], (float)U0);
+    R.o = make_int4(U0, V0, P.ysl, P.spos);
+}
+
+// Pixel origin of a block's re-based map: the lowest row / column the
+// float map sends any of the block's 8 corners to, minus one, clamped into
+// the panel, the row rounded down to a multiple of 4 (the staged kernel's
+// detector box starts there; the box load needs a 16-byte aligned start).
+__device__ __forceinline__ int2 bdd_block_origin(float umin, float vmin, int nr, int nc) {
+    int r = (int)floorf(fmaxf(umin - 1.f, 0.f));
+    r = min(r, nr - 1) & ~3;
+    int c = (int)floorf(fmaxf(vmin - 1.f, 0.f));
+    c = min(c, nc - 1);
+    return make_int2(r, c);
+}
+
+// The float map at one corner of a block (the staged kernel's box corners).
+__device__ __forceinline__ float2 bdd_corner_uv(const BddProj &P, float cx, float cy, float cz) {
+    const float den = 1.f / fmaf(P.c[0], cx, fmaf(P.c[1], cy, fmaf(P.c[2], cz, 1.f)));
+    return make_float2(fmaf(P.au[0], cx, fmaf(P.au[1], cy, fmaf(P.au[2], cz, P.au0))) * den,
+                       fmaf(P.av[0], cx, fmaf(P.av[1], cy, fmaf(P.av[2], cz, P.av0))) * den);
+}
+
+// Pixel coordinates (u, v) of world point p under M, FP64.
+__device__ __forceinline__ void bdd_map_at(const BddMap64 &M, double px, double py, double pz, double &u, double &v) {
+    const double D = fma(M.c[0], px, fma(M.c[1], py, fma(M.c[2], pz, 1.0)));
+    u = fma(M.au[0], px, fma(M.au[1], py, fma(M.au[2], pz, M.au0))) / D;
+    v = fma(M.av[0], px, fma(M.av[1], py, fma(M.av[2], pz, M.av0))) / D;
+}
+
 // Launch shapes the autotuner chooses between (per handle).
 struct Tuning {
     int siddon_blocks_per_sm = 8;   // grid-stride grid of the Siddon kernels: blocks per SM

@@ -99,12 +99,12 @@ int bdd_forward_tma(const Grid &g, const float *xy, const float *uv, int nr, int
                     int64_t nproj, const float *img, const float *imgT, float *y, cudaStream_t st);
 // Device error word of the bounded waits (1 after a wait ran out; reset when read), < 0 on failure.
 int take_device_error();
-int bdd_backward(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                 float *sens, const Tuning &tn, cudaStream_t st);
+int bdd_backward(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj, const float *y,
+                 float *img, float *sens, const Tuning &tn, cudaStream_t st);
 // The same backprojection with per-projection detector boxes staged by TMA (8 voxels along z per thread).
 bool bdd_bp_tma_supported(int nr, const float *y);
-int bdd_backward_tma(const Grid &g, const BddProj *pj, int nr, int nc, int64_t nproj, const float *y, float *img,
-                     float *sens, cudaStream_t st);
+int bdd_backward_tma(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
+                     const float *y, float *img, float *sens, cudaStream_t st);
 
 // Projector type 4 (interpolation), PET and CT.
 int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img,

@@ -438,6 +438,8 @@ extern "C" int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32
     if (mx < 0 || my < 0 || mz < 0 || mx > nx || my > ny || mz > nz)
         return set_error(OMB_ERR_INVALID, "weighted mean window must fit one mirror of the image");
     if (!(wsum != 0.f)) return set_error(OMB_ERR_INVALID, "weighted mean weights sum to 0");
+    // the reference takes a 2-D path for one slice (no z window)
+    if (nz == 1 && mz > 0) return set_error(OMB_ERR_INVALID, "weighted mean of a single slice needs mz = 0");
     dim3 block(32, 8);
     dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
     k_wmean_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, mx, my, mz, weights, wsum,

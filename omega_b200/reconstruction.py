@@ -326,6 +326,13 @@ def reconstructions_main(options):
         raise ValueError(method + ' is built for PET data')
     if options.PDHG and not options.TV:
         raise ValueError('PDHG is built with the TV prior (options.TV = True)')
+    if getattr(options, 'TV', False):
+        # the reference compiles other TV gradients for these settings
+        # (ProjectorClass.h:900-918: TVtype 4 SATV, 6 TVW1, anatomical TV)
+        if int(getattr(options, 'TVtype', 1)) not in (1, 2, 3):
+            raise ValueError('TV is built for TVtype 1, 2 and 3 (the plain TV gradient)')
+        if getattr(options, 'TV_use_anatomical', False):
+            raise ValueError('anatomical TV (TV_use_anatomical) is not built')
     sin = np.asarray(options.SinM, dtype=np.float32)
     if options.CT and not options.usingLinearizedData:
         if options.flat <= 0:

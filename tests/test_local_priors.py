@@ -240,6 +240,48 @@ def test_weighted_mean_weights_match_reference():
     assert np.array_equal(priors.weighted_mean_weights(o), f["wmean_111"])
 
 
+def test_weighted_mean_user_weights_are_normalised():
+    """Weights given in options.weighted_weights are divided by their sum, as
+    Weighted_mean (priors.h:103) divides by af::sum of the weights."""
+    from conftest import make_options
+    from omega_b200 import priors
+    o = make_options("pet_mini")
+    o.Ndx = o.Ndy = o.Ndz = 1
+    w = np.arange(1, 28, dtype=np.float32)
+    o.weighted_weights = w
+    got = priors.weighted_mean_weights(o)
+    assert abs(float(got.sum()) - 1.0) < 1e-6
+    assert np.allclose(got, w / w.sum(), rtol=1e-6)
+    o.weighted_weights = np.zeros(27, np.float32)
+    with pytest.raises(ValueError, match="sum to 0"):
+        priors.weighted_mean_weights(o)
+
+
+def test_weighted_mean_single_slice_needs_flat_window():
+    """One slice: the reference takes its 2-D path (no z window), so a z
+    window is rejected before any launch."""
+    from omega_b200 import _native
+    st = _native.lib().omb_wmean_gradient(ctypes.c_void_p(16), ctypes.c_void_p(16), 8, 8, 1, 1, 1, 1,
+                                          ctypes.c_void_p(16), ctypes.c_float(1.0), 1, ctypes.c_float(1e-8),
+                                          ctypes.c_float(0.1), 0, None)
+    assert st != 0
+    assert "single slice" in _native.lib().omb_last_error().decode()
+
+
+@pytest.mark.parametrize("attrs", [dict(TVtype=4), dict(TVtype=6), dict(TV_use_anatomical=True)])
+def test_tv_variants_not_built_are_rejected(attrs):
+    from conftest import make_options
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    o.SinM = np.ones(int(o.Ndist) * int(o.Nang) * int(o.NSinos), np.float32)
+    o.OSL_OSEM = True
+    o.TV = True
+    for k, v in attrs.items():
+        setattr(o, k, v)
+    with pytest.raises(ValueError, match="TV"):
+        rec.reconstructions_main(o)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("mean_type,no_norm", [(1, False), (2, False), (3, True)])
 def test_weighted_mean(cuda, mean_type, no_norm):
