@@ -48,7 +48,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM bytes (read + write) per launch from ncu captures, scaled to the full
-# workload by rays; see profiles/ for the captures they come from.
+# workload by rays where the capture was smaller; see profiles/ for the
+# captures they come from.
 PROFILED_TRAFFIC = {
     # DRAM bytes read + written per launch, from the ncu captures summarised
     # in profiles/: bdd_cbct_capture.md (36-view capture x 10) and
@@ -57,6 +58,8 @@ PROFILED_TRAFFIC = {
     ("cbct", "bdd_bp"): 3.87e8,
     ("dynpet", "siddon_fp"): 3.81e8,
     ("dynpet", "siddon_bp"): 4.77e8,
+    # interp_tof_capture.md: one subset's forward launch (16 per step)
+    ("interp_tof", "interp_fp"): 5.60e6,
 }
 # What bounds each kernel instead of HBM (the volumes and images are
 # L2-resident, so DRAM moves a few per cent of the cache-less bytes): the
@@ -66,6 +69,7 @@ PROFILED_LIMITER = {
     ("cbct", "bdd_bp"): {"issue_active_pct": 74.2, "sm_throughput_pct": 73.8, "dram_pct": 0.2},
     ("dynpet", "siddon_fp"): {"issue_active_pct": 66.5, "l1tex_pct": 92.0, "dram_pct": 1.0},
     ("dynpet", "siddon_bp"): {"issue_active_pct": 44.4, "lts_pct": 65.9, "dram_pct": 1.0},
+    ("interp_tof", "interp_fp"): {"issue_active_pct": 84.9, "sm_throughput_pct": 78.6, "dram_pct": 0.01},
 }
 FALLBACK_HBM_GBS = 6650.0
 
@@ -77,12 +81,15 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="cbct",
-                   choices=["cbct", "cbct_small", "dynpet", "dynpet_small", "fanbeam64", "fanbeam64_small"])
+                   choices=["cbct", "cbct_small", "dynpet", "dynpet_small", "fanbeam64", "fanbeam64_small",
+                            "interp_tof", "interp_tof_small"])
     p.add_argument("--frames", type=int, default=None)
     p.add_argument("--views", type=int, default=None,
                    help="cbct: number of projections (fewer than 360 only for short profiling captures)")
     p.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain OSEM time-to-logL leg")
+    p.add_argument("--no-legs", action="store_true",
+                   help="skip the Siddon dynamic-PET and type-4 TOF legs of the default line")
     p.add_argument("--tuning", default=None,
                    help="fixed launch shapes instead of the autotuner, e.g. bdd_fp_columns=16,bdd_bp_zrun=8")
     return p.parse_args()
@@ -141,6 +148,63 @@ def dynamic_images(o, frames, seed=2024):
         flat = reg.ravel(order="F")
         imgs += np.outer(tac, flat).astype(np.float32)
     return imgs
+
+
+def tof_pet_options(small=False, **extra):
+    """The precision workload: 672 crystals x 55 rings (42 blocks of 16, ring
+    diameter 856 mm), 400 radial x 336 angles x 109 span-3 sinograms with 15
+    TOF bins of 200 ps FWHM covering +-424 mm (the FOV diagonal), a
+    200 x 200 x 109 image over 600 x 600 x 436 mm, projector type 4, 16
+    subsets.  ``small``: 11 rings, 22 sinograms, 100 x 100 x 21 image."""
+    from omega_b200.projector import geometry as geo
+    from omega_b200.projector import proj
+    c = 2.99792458e11  # mm/s
+    rings, nz, nx = (11, 21, 100) if small else (55, 109, 200)
+    o = proj.projectorClass()
+    o.blocks_per_ring, o.cryst_per_block, o.cryst_per_block_axial, o.linear_multip = 42, 16, rings, 1
+    o.rings = rings
+    o.det_per_ring = o.det_w_pseudo = 672
+    o.diameter = 856.
+    o.cr_p = math.pi * 856. / 672.
+    o.cr_pz = 4.0
+    o.FOVa_x = o.FOVa_y = 600.
+    o.axial_fov = 436. * nz / 109.
+    o.Nx = o.Ny = nx
+    o.Nz = nz
+    o.span, o.ring_difference = 3, rings - 1
+    o.Ndist, o.Nang = (400, 336) if not small else (200, 168)
+    o.NSinos = nz
+    o.TotSinos = int(np.sum(geo.default_segment_table(rings, 3, rings - 1, nz)))
+    o.TOF_bins = o.TOF_bins_used = 15
+    o.TOF_FWHM = 200e-12
+    o.TOF_width = 848.0 / 15 / (c / 2)
+    o.projector_type = 4
+    o.subsets, o.subsetType = 16, 8
+    o.verbose = 0
+    for k, v in extra.items():
+        setattr(o, k, v)
+    o.addProjector()
+    return o
+
+
+def tof_phantom(o, seed=7):
+    """Seeded anthropomorphic-style ellipsoid phantom: elliptic body, two
+    lung-like cold ellipsoids, a warm organ and hot lesions."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = int(o.Nx[0]), int(o.Ny[0]), int(o.Nz[0])
+    xs = (np.arange(nx) + 0.5) * float(o.dx[0]) + float(o.bx[0])
+    ys = (np.arange(ny) + 0.5) * float(o.dy[0]) + float(o.by[0])
+    zs = (np.arange(nz) + 0.5) * float(o.dz[0]) + float(o.bz[0])
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    img = 1.0 * ((X / 220.) ** 2 + (Y / 150.) ** 2 < 1)
+    for sx in (-90., 90.):
+        img[((X - sx) / 60.) ** 2 + (Y / 80.) ** 2 + (Z / 150.) ** 2 < 1] = 0.3
+    img[((X - 30.) / 70.) ** 2 + ((Y + 40.) / 50.) ** 2 + ((Z + 60.) / 80.) ** 2 < 1] = 2.0
+    for _ in range(6):
+        c = rng.uniform(-100, 100, 3)
+        r = rng.uniform(6, 15)
+        img[((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) < r * r] = 6.0
+    return img.ravel(order="F").astype(np.float32)
 
 
 # ---------------------------------------------------------------------------
@@ -387,12 +451,30 @@ def e2e_time(args, world, dev, step_host):
     return total
 
 
-def roofline(name, nbytes, duration, traffic_key):
+def roofline(name, model_bytes, duration, traffic_key, compulsory_bytes=None, launches=1):
+    """HBM roofline of the dominant kernel.  ``achieved`` / ``frac`` count the
+    DRAM bytes the kernel really moves per call: the ncu dram__bytes of one
+    launch (profiles/, scaled to the full workload as the summary states)
+    times the launches of the timed phase, over its event-timed duration.
+    ``model_*`` keep the survey's cache-less byte model (every tap a DRAM
+    access, above 1 when taps hit on chip) and ``compulsory_*`` the bytes any
+    implementation must move (inputs and outputs once)."""
     peak, src = measured_peak()
-    achieved = nbytes / duration / 1e9
-    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": src, "algorithmic_bytes": nbytes,
-            "traffic": PROFILED_TRAFFIC.get(traffic_key), "limiter": PROFILED_LIMITER.get(traffic_key)}
+    traffic = PROFILED_TRAFFIC.get(traffic_key)
+    out = {"bound": "hbm", "kernel": name, "peak": peak, "unit": "GB/s", "peak_source": src,
+           "model_bytes": model_bytes, "model_achieved": model_bytes / duration / 1e9,
+           "model_frac": model_bytes / duration / 1e9 / peak, "limiter": PROFILED_LIMITER.get(traffic_key)}
+    if traffic is not None:
+        achieved = traffic * launches / duration / 1e9
+        out.update({"achieved": achieved, "frac": achieved / peak, "traffic": traffic,
+                    "basis": f"DRAM bytes ncu counted per launch x {launches} launch(es) / event-timed phase"})
+    else:
+        out.update({"achieved": out["model_achieved"], "frac": out["model_frac"], "traffic": None,
+                    "basis": "no ncu capture of this workload: cache-less byte model"})
+    if compulsory_bytes is not None:
+        out["compulsory_bytes"] = compulsory_bytes
+        out["compulsory_frac"] = compulsory_bytes / duration / 1e9 / peak
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -449,9 +531,13 @@ def learned_time_to_logl(studies=8, timing_studies=4):
             "continuation_iterations_median": summary["k_median"], "continuation_iterations_max": summary["k_max"],
             "plain_20_iterations_ms": summary["plain_ms_median"], "warm_start_ms": summary["warm_ms_median"],
             "time_ratio": summary["time_ratio_median"],
+            "timed_continuation_iterations": summary["timed_continuation"],
+            "timed_studies": summary["timed_studies"], "timed_reached_plain_L20": summary["timed_reached_L20"],
             "rel_l2_warm_vs_plain20": summary["rel_l2_warm_vs_plain20_median"],
-            "setup": "384 crystals x 32 rings, 128x128x63 image, 16 subsets, 1e7-1e8 counts; warm start = 2 OSEM "
-                     "iterations + BF16 U-Net + OSEM until the plain 20-iteration logL; CUDA events per study",
+            "setup": "384 crystals x 32 rings, 128x128x63 image, 16 subsets, 1e7-1e8 counts; timed warm path = 2 "
+                     "OSEM iterations + BF16 U-Net + a fixed 4 OSEM iterations + the log-likelihood check, the "
+                     "same for every study (no per-study stop count); plain = 20 iterations; CUDA events per "
+                     "study",
             "weights": "omega_b200/weights/warmstart_pet128.npz (5000 training studies)"}
 
 
@@ -533,13 +619,11 @@ def run_cbct(args, rank, world, dev):
     bp_bytes = n * nproj * 16 + n * 4
     mean_fp, mean_bp = t_fp / K, t_bp / K
     if mean_bp >= mean_fp:
-        rl = roofline("bdd_bp", bp_bytes, mean_bp, (args.workload, "bdd_bp"))
+        rl = roofline("bdd_bp", bp_bytes, mean_bp, (args.workload, "bdd_bp"), (n + m) * 4)
     else:
-        rl = roofline("bdd_fp", fp_bytes, mean_fp, (args.workload, "bdd_fp"))
+        rl = roofline("bdd_fp", fp_bytes, mean_fp, (args.workload, "bdd_fp"), (n + m) * 4)
     rl["model"] = ("cache-less tap bytes: FP = rays x (slices x 4 taps x 4 B + 4 B out); BP = voxels x views x "
-                   "4 taps x 4 B + 4 B out. The 67 MB volume is L2-resident, so the taps are served on chip; "
-                   "traffic is the DRAM bytes ncu counted")
-    rl["compulsory_bytes"] = (n + m) * 4
+                   "4 taps x 4 B + 4 B out. The 67 MB volume is L2-resident, so the taps are served on chip")
     panel = int(o.nRowsD)
     line = {
         "metric": "proj+backproj rays/s", "value": value, "unit": "rays/s", "n_gpus": world,
@@ -661,10 +745,12 @@ def run_dynpet(args, rank, world, dev):
     fp_bytes = frames * (4 * sum_np + 32 * m)
     bp_bytes = frames * (8 * sum_np + 28 * m)
     mean_fp, mean_bp = t_fp / K, t_bp / K
+    comp = frames * (n + m) * 4
     if mean_bp >= mean_fp:
-        rl = roofline("siddon_bp", bp_bytes, mean_bp, (args.workload, "siddon_bp"))
+        rl = roofline("siddon_bp", bp_bytes, mean_bp, (args.workload, "siddon_bp"), comp)
     else:
-        rl = roofline("siddon_fp", fp_bytes, mean_fp, (args.workload, "siddon_fp"))
+        rl = roofline("siddon_fp", fp_bytes, mean_fp, (args.workload, "siddon_fp"), comp)
+    rl["model"] = "cache-less: FP = frames x sum_rays (4 Np + 32) B; BP = frames x sum_rays (8 Np + 28) B"
     line = {
         "metric": "proj+backproj rays/s", "value": ray_frames * K * world / total, "unit": "rays/s",
         "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * total / K,
@@ -777,9 +863,9 @@ def run_fanbeam(args, rank, world, dev):
     fp_bytes = 4 * npx + 32 * nmeas
     bp_bytes = 8 * npx + 28 * nmeas
     if mean_bp >= mean_fp:
-        rl = roofline("batch_siddon_bp", bp_bytes, mean_bp, (args.workload, "bp"))
+        rl = roofline("batch_siddon_bp", bp_bytes, mean_bp, (args.workload, "bp"), (nimg + nmeas) * 4)
     else:
-        rl = roofline("batch_siddon_fp", fp_bytes, mean_fp, (args.workload, "fp"))
+        rl = roofline("batch_siddon_fp", fp_bytes, mean_fp, (args.workload, "fp"), (nimg + nmeas) * 4)
     line = {
         "metric": "proj+backproj rays/s", "value": nmeas * K * world / total, "unit": "rays/s", "n_gpus": world,
         "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * total / K, "higher_is_better": True,
@@ -813,6 +899,161 @@ def run_fanbeam(args, rank, world, dev):
         except Exception as e:
             line["cpu_baseline"] = {"error": str(e)}
     return line
+
+
+# ---------------------------------------------------------------------------
+# our arm: the precision workload, projector type 4 with 15 TOF bins
+# ---------------------------------------------------------------------------
+
+def interp_model_bytes(o, nbins):
+    """Cache-less bytes of the type-4 forward projection, sum over rays of
+    32 nSteps + 8 NB + 24 (8 texels per trilinear sample), with nSteps per
+    ray as projectorType4.cl:467-482 counts them (FP64 here), and its
+    backprojection, sum of 8 nSteps + 28 (nearest-voxel atomics)."""
+    xy = np.asarray(o.x, dtype=np.float64).reshape(-1, 4)
+    z = np.asarray(o.z, dtype=np.float64).reshape(-1, 2)
+    b = np.array([float(o.bx[0]), float(o.by[0]), float(o.bz[0])])
+    bmax = b + np.array([int(o.Nx[0]) * float(o.dx[0]), int(o.Ny[0]) * float(o.dy[0]), int(o.Nz[0]) * float(o.dz[0])])
+    dL = float(np.float32(o.dL))
+    steps = 0
+    for k in range(z.shape[0]):
+        s = np.stack([xy[:, 0], xy[:, 1], np.full(len(xy), z[k, 0])], 1)
+        d = np.stack([xy[:, 2], xy[:, 3], np.full(len(xy), z[k, 1])], 1)
+        v = d - s
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t1, t2 = (b - s) / v, (bmax - s) / v
+        t0 = np.nanmax(np.minimum(t1, t2), 1)
+        te = np.nanmin(np.maximum(t1, t2), 1)
+        L = np.linalg.norm(v, axis=1)
+        ok = te > t0
+        steps += int(np.sum(np.floor((te[ok] - t0[ok]) / (dL / L[ok])) + 1))
+    rays = xy.shape[0] * z.shape[0]
+    return steps, 32 * steps + (8 * nbins + 24) * rays, 8 * steps + 28 * rays
+
+
+def run_interp_tof(args, rank, world, dev):
+    import torch
+    from omega_b200 import _native
+    small = args.workload == "interp_tof_small"
+    o = tof_pet_options(small, imageReadPrecision="bf16", use_64bit_atomics=True)
+    o.initProj()
+    h = o._handle
+    n = int(o.N[0])
+    S = int(o.subsets)
+    nb = int(o.TOF_bins_used)
+    ms = [o.measurementCount(s) for s in range(S)]      # all TOF bins
+    offs = np.concatenate([[0], np.cumsum(ms)]).astype(np.int64)
+    x_host = tof_phantom(o)
+    x = torch.from_numpy(x_host).to(dev)
+    y = torch.empty(int(offs[-1]), device=dev)
+    back = torch.empty(n, device=dev)
+    sp = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+    def P(t, off=0):
+        return ctypes.c_void_p(t.data_ptr() + 4 * int(off))
+
+    def step(tm):
+        tm.mark()
+        for s in range(S):
+            _native.call("omb_forward", h, s, P(x), P(y, offs[s]), sp)
+        tm.mark()
+        for s in range(S):
+            _native.call("omb_backward", h, s, P(y, offs[s]), P(back), None, 0, sp)
+        tm.mark()
+
+    tuning = choose_tuning(o, args, 1)
+    tot, clk, wall = run_timed(args, world, dev, step, 2)
+    t_fp, t_bp = tot
+
+    # the int64 fixed-point backprojection of the same step, timed apart,
+    # and checked bit-identical run to run
+    def step64(tm):
+        tm.mark()
+        for s in range(S):
+            _native.call("omb_backward", h, s, P(y, offs[s]), P(back), None, 1, sp)
+        tm.mark()
+
+    t64, _, _ = run_timed(args, world, dev, step64, 1)
+    first = back.clone()
+    step64(Timed(torch.cuda.current_stream(dev)))
+    torch.cuda.synchronize()
+    int64_identical = bool(torch.equal(first.view(torch.int32), back.view(torch.int32)))
+
+    h_in = torch.from_numpy(x_host).pin_memory()
+    h_out = torch.empty(n, dtype=torch.float32).pin_memory()
+
+    class _NoMarks:
+        def mark(self):
+            pass
+
+    def step_host():
+        x.copy_(h_in, non_blocking=True)
+        step(_NoMarks())
+        h_out.copy_(back, non_blocking=True)
+
+    e2e_total = e2e_time(args, world, dev, step_host)
+    if rank != 0:
+        return None
+    K = args.steps
+    lors = int(offs[-1]) // nb
+    total = t_fp + t_bp
+    mean_fp, mean_bp = t_fp / K, t_bp / K
+    steps_total, fp_bytes, bp_bytes = interp_model_bytes(o, nb)
+    comp = (n + int(offs[-1])) * 4
+    if mean_bp >= mean_fp:
+        rl = roofline("interp_bp", bp_bytes, mean_bp, (args.workload, "interp_bp"), comp, launches=S)
+    else:
+        rl = roofline("interp_fp", fp_bytes, mean_fp, (args.workload, "interp_fp"), comp, launches=S)
+    rl["model"] = ("cache-less: FP = sum_rays (32 nSteps + 8 NB + 24) B (8 texels per trilinear sample); "
+                   "BP = sum_rays (8 nSteps + 28) B (nearest-voxel atomics)")
+    line = {
+        "metric": "proj+backproj rays/s", "value": lors * K * world / total, "unit": "rays/s", "n_gpus": world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * total / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (bf16 image reads in the forward projection)",
+        "data": "synthetic (seeded anthropomorphic-style ellipsoid phantom)",
+        "config": {"workload": ("3-D TOF PET, 672 crystals x 55 rings, 400x336x109 sinograms x 15 TOF bins "
+                                "(200 ps FWHM), 200x200x109 image, interpolation projector (type 4), BF16 image "
+                                "reads, FP32 accumulation, all 16 subsets forward then back per step")
+                   if not small else "3-D TOF PET small (11 rings) for profiling",
+                   "lors_per_step": lors, "bins_per_step": int(offs[-1]), "tof_bins": nb, "samples_per_step": steps_total,
+                   "subsets": S, "tuning": tuning, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (%.0f MB of TOF sinograms) plus a 256 MB L2 flush between steps"
+                         % (int(offs[-1]) * 4 / 1e6)},
+        "fp_ms": 1e3 * mean_fp, "bp_ms": 1e3 * mean_bp, "bp_int64_ms": 1e3 * t64[0] / K,
+        "int64_bit_identical": int64_identical, "bins_per_s": int(offs[-1]) * K * world / total,
+        "roofline": rl,
+        "e2e": {"value": lors * K * world / e2e_total, "unit": "rays/s", "h2d_bytes_per_step": n * 4,
+                "d2h_bytes_per_step": n * 4},
+        "gpu_launches": 2 * S * K, "clocks": clk, "wall_s": wall,
+    }
+    if not args.no_baseline and world == 1:
+        try:
+            v, sample = interp_cpu_rate(small, x_host, 10.0)
+            line["cpu_baseline"] = {"value": v, "unit": "rays/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                    "sample": sample + "; FP64 restatement (OpenMP forward, one-thread atomic "
+                                              "backprojection) pinned to the reference's projectorType4.cl; the "
+                                              f"reference has no CPU type-4 projector; host CPU {cpu_model()}"}
+        except Exception as e:
+            line["cpu_baseline"] = {"error": str(e)}
+    return line
+
+
+def interp_cpu_rate(small, image, seconds):
+    """FP64 restatement of the type-4 TOF pair on one sinogram of the same
+    scanner, repeated for at least `seconds`."""
+    from oracle import oracle as orc
+    o = tof_pet_options(small, subsets=int(22 if small else 109))
+    g = orc.Geometry(o)
+    rays = g.rays(0)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        yy = orc.interp_forward(g, image, 0)
+        orc.interp_backward(g, yy, 0)
+        done += rays
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return done / el, f"one sinogram ({rays} LORs x {g.nbins} TOF bins) per FP+BP pair, {done // rays} pairs in {el:.1f} s"
 
 
 # ---------------------------------------------------------------------------
@@ -901,9 +1142,26 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-    run = run_cbct if args.workload.startswith("cbct") else (
-        run_fanbeam if args.workload.startswith("fanbeam") else run_dynpet)
+    runs = {"cbct": run_cbct, "fanbeam": run_fanbeam, "dynpet": run_dynpet, "interp_tof": run_interp_tof}
+    run = next(f for k, f in runs.items() if args.workload.startswith(k))
     line = run(args, rank, world, dev)
+    if args.workload == "cbct" and world == 1 and not args.no_legs:
+        # the other projectors of the path, each timed the same way: improved
+        # Siddon (dynamic PET) and interpolation with TOF (precision workload)
+        import copy
+
+        import torch
+        legs = {}
+        for name, wl, fn in (("siddon_dynpet", "dynpet", run_dynpet), ("interp_tof", "interp_tof", run_interp_tof)):
+            torch.cuda.empty_cache()
+            a = copy.copy(args)
+            a.workload = wl
+            a.tuning = None
+            try:
+                legs[name] = fn(a, rank, world, dev)
+            except Exception as e:  # a leg must not hide the headline number
+                legs[name] = {"error": f"{type(e).__name__}: {e}"}
+        line["legs"] = legs
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

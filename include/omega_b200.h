@@ -63,8 +63,13 @@ typedef enum omb_read_precision {
 } omb_read_precision;
 
 typedef enum omb_bp_mode {
-    OMB_BP_FLOAT_ATOMIC = 0, /* float32 atomics (the reference's CUDA path) */
-    OMB_BP_FIXED64 = 1       /* int64 fixed point, bit-identical run to run (the reference's OpenCL -DATOMIC path) */
+    OMB_BP_FLOAT_ATOMIC = 0, /* float32 atomics (the reference's CUDA path); projector type 5: the reference's
+                                voxel-driven gather (projectorType5Backward) */
+    OMB_BP_FIXED64 = 1,      /* int64 fixed point, bit-identical run to run (the reference's OpenCL -DATOMIC path);
+                                projector type 5: the ray-driven scatter below with int64 atomics */
+    OMB_BP_RAY = 2           /* projector type 5: the ray-driven scatter form, the exact adjoint of the forward
+                                projection (projectorType5Forward), float atomics; other types: as
+                                OMB_BP_FLOAT_ATOMIC (their backprojections are ray-driven already) */
 } omb_bp_mode;
 
 /*
@@ -172,7 +177,11 @@ int omb_forward_frames(omb_handle *h, int32_t subset, int32_t n_frames, const fl
  * image = A_s^T * y, and sens = A_s^T * 1 when `sens` is not NULL (the
  * reference's no_norm == 0 pass).  Both outputs are overwritten.
  * mode: omb_bp_mode; OMB_BP_FIXED64 needs a handle created with
- * fixed64_workspace != 0.
+ * fixed64_workspace != 0.  Projector type 5 has two backprojectors: the
+ * voxel-driven gather of the reference (OMB_BP_FLOAT_ATOMIC; not the exact
+ * adjoint of the forward projection) and the ray-driven scatter
+ * (OMB_BP_RAY, or OMB_BP_FIXED64 for its deterministic int64 form), which
+ * is.
  * Replaces projfunctions.py:735-1095 (backwardProjection) and
  * ProjectorClass.h:3893 (backwardProjection); kernels restate
  * projectorType123.cl (-DBP, rhs() general_opencl_functions.h:1212-1275),

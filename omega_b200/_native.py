@@ -23,6 +23,7 @@ OMB_READ_FP32 = 0
 OMB_READ_BF16 = 1
 OMB_BP_FLOAT_ATOMIC = 0
 OMB_BP_FIXED64 = 1
+OMB_BP_RAY = 2
 
 _c_float_p = ctypes.POINTER(ctypes.c_float)
 _c_i64_p = ctypes.POINTER(ctypes.c_int64)

@@ -612,7 +612,8 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
                  void *stream) {
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
     if (!image || !y) return set_error(OMB_ERR_INVALID, "image/y pointer is NULL");
-    if (mode != OMB_BP_FLOAT_ATOMIC && mode != OMB_BP_FIXED64) return set_error(OMB_ERR_INVALID, "unknown backprojection mode");
+    if (mode != OMB_BP_FLOAT_ATOMIC && mode != OMB_BP_FIXED64 && mode != OMB_BP_RAY)
+        return set_error(OMB_ERR_INVALID, "unknown backprojection mode");
     if (mode == OMB_BP_FIXED64 && !h->d_acc)
         return set_error(OMB_ERR_INVALID, "fixed-point backprojection needs a handle created with fixed64_workspace");
     RaySet rs{};
@@ -621,14 +622,29 @@ int omb_backward(omb_handle *h, int32_t subset, const float *y, float *image, fl
     cudaStream_t s = (cudaStream_t)stream;
     const size_t nb = h->n_img * sizeof(float);
     if (h->desc.bp_type == 5) {
-        if (mode != OMB_BP_FLOAT_ATOMIC)
-            return set_error(OMB_ERR_UNSUPPORTED, "the type-5 backprojection is a gather; it has no fixed-point mode");
-        return bdd_backward(h->grid, h->d_bddp + rs.proj0, h->d_bddm64 + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, y,
-                            image, sens, h->tune, s);
+        if (mode == OMB_BP_FLOAT_ATOMIC)
+            return bdd_backward(h->grid, h->d_bddp + rs.proj0, h->d_bddm64 + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj,
+                                y, image, sens, h->tune, s);
+        // ray-driven scatter: the exact adjoint of the forward projection
+        if (mode == OMB_BP_FIXED64) {
+            unsigned long long *acc = h->d_acc, *acc_s = sens ? h->d_acc + h->n_img : nullptr;
+            OMB_CUDA_TRY(cudaMemsetAsync(h->d_acc, 0, (sens ? 2 : 1) * h->n_img * sizeof(unsigned long long), s));
+            st = bdd_backward_ray(h->grid, rs.xy, rs.z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj, y,
+                                  nullptr, nullptr, acc, acc_s, s);
+            if (st != OMB_OK) return st;
+            st = fixed_to_float(acc, image, h->n_img, s);
+            if (st == OMB_OK && sens) st = fixed_to_float(acc_s, sens, h->n_img, s);
+            return st;
+        }
+        OMB_CUDA_TRY(cudaMemsetAsync(image, 0, nb, s));
+        if (sens) OMB_CUDA_TRY(cudaMemsetAsync(sens, 0, nb, s));
+        return bdd_backward_ray(h->grid, rs.xy, rs.z, rs.n_rows, rs.n_cols, rs.pitch_y, rs.proj0, rs.n_proj, y, image,
+                                sens, nullptr, nullptr, s);
     }
     if (h->desc.bp_type == 4 && h->desc.modality == OMB_CT_PANEL) {
         if (mode != OMB_BP_FLOAT_ATOMIC)
-            return set_error(OMB_ERR_UNSUPPORTED, "the type-4 CT backprojection is a gather; it has no fixed-point mode");
+            return set_error(OMB_ERR_UNSUPPORTED, "the type-4 CT backprojection is a gather; it has no fixed-point "
+                                                  "or ray-driven mode");
         return interp_ct_backward(h->grid, h->d_bddp + rs.proj0, rs.n_rows, rs.n_cols, rs.n_proj, h->desc.kerroin, y,
                                   image, sens, s);
     }

@@ -101,6 +101,12 @@ int bdd_forward_tma(const Grid &g, const float *xy, const float *uv, int nr, int
 int take_device_error();
 int bdd_backward(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj, const float *y,
                  float *img, float *sens, const Tuning &tn, cudaStream_t st);
+// Ray-driven (scatter) type-5 backprojection, the exact adjoint of the forward
+// projection: float atomics into img / sens (zeroed by the caller), or int64
+// fixed-point atomics into acc / acc_s (when acc is not NULL).
+int bdd_backward_ray(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
+                     int64_t nproj, const float *y, float *img, float *sens, unsigned long long *acc,
+                     unsigned long long *acc_s, cudaStream_t st);
 // The same backprojection with per-projection detector boxes staged by TMA (8 voxels along z per thread).
 bool bdd_bp_tma_supported(int nr, const float *y);
 int bdd_backward_tma(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,

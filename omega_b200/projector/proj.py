@@ -17,6 +17,12 @@ Differences from the reference surface:
  * ``use_64bit_atomics = True`` selects the bit-deterministic int64
    fixed-point backprojection on CUDA (the reference only offers it on
    OpenCL and forces it off on CUDA, init.py:251-254);
+ * ``bddRayBackprojection = True`` (projector type 5) backprojects with the
+   ray-driven scatter, the exact adjoint of the forward projection, instead
+   of the reference's voxel-driven gather; ``bddRayBackprojection = 'int64'``
+   takes the same scatter in int64 fixed point, bit-identical run to run
+   (the reference clears ``use_64bit_atomics`` for CT types 4 and 5, whose
+   gathers have no fixed-point form);
  * with TOF the forward projection returns all bins of the subset
    ([bin0 rays, bin1 rays, ...]); the reference's Python path sizes the output
    for one bin only.
@@ -225,6 +231,7 @@ class projectorClass:
     use_psf = False
     use_64bit_atomics = False
     use_32bit_atomics = False
+    bddRayBackprojection = False
     global_factor = 1.
     epps = 1e-5
     # Subsets / reconstruction
@@ -707,7 +714,7 @@ class projectorClass:
             d.d_size5[0], d.d_size5[1] = float(self.dSizeX[0]), float(self.dSizeY[0])
             d.d_scale5[0], d.d_scale5[1], d.d_scale5[2] = (float(self.dScaleX[0]), float(self.dScaleY[0]),
                                                            float(self.dScaleZ[0]))
-        d.fixed64_workspace = 1 if self.use_64bit_atomics else 0
+        d.fixed64_workspace = 1 if (self.use_64bit_atomics or self.bddRayBackprojection == 'int64') else 0
         if not self.CT:
             d.n_rays_xy = int(self.n_rays_transaxial)
             d.n_rays_z = int(self.n_rays_axial)
@@ -910,7 +917,9 @@ class projectorClass:
         f = torch.empty(n, dtype=torch.float32, device=y.device)
         s = torch.empty(n, dtype=torch.float32, device=y.device) if sens else None
         stream = torch.cuda.current_stream(y.device).cuda_stream
-        mode = _native.OMB_BP_FIXED64 if self.use_64bit_atomics else _native.OMB_BP_FLOAT_ATOMIC
+        ray = self.bddRayBackprojection
+        mode = _native.OMB_BP_FIXED64 if (self.use_64bit_atomics or ray == 'int64') else (
+            _native.OMB_BP_RAY if ray else _native.OMB_BP_FLOAT_ATOMIC)
         _native.call("omb_backward", self._handle, int(subset), ctypes.c_void_p(y.data_ptr()),
                      ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(s.data_ptr() if s is not None else 0),
                      int(mode), ctypes.c_void_p(stream))

@@ -262,3 +262,97 @@ int oracle_bdd_bp(const oracle_ct *g, const double *y, double *img, double *sens
     free(sat);
     return 0;
 }
+
+/* Ray-driven (scatter) backprojection: the exact adjoint of oracle_bdd_fp.
+ * Every ray's forward weight kerroin / area times the clamped overlap of its
+ * footprint with voxel (i, k) of slice jj -- the quantity the summed-area
+ * difference integrates -- carries y[ray] back onto that voxel.  The
+ * 8-column groups share their first column's geometry exactly as in the
+ * forward projection (projectorType5.cl:166-174).  img is overwritten;
+ * sens (when not NULL) receives A^T 1. */
+static double overlap(double a, double b, double lo, double hi) {
+    const double l = a > lo ? a : lo, h = b < hi ? b : hi;
+    return h > l ? h - l : 0.0;
+}
+
+int oracle_bdd_bp_ray(const oracle_ct *g, const double *y, double *img, double *sens) {
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const size_t N = (size_t)nx * ny * nz;
+    for (size_t n = 0; n < N; ++n) {
+        img[n] = 0.0;
+        if (sens) sens[n] = 0.0;
+    }
+    const int nr = g->n_rows, nc = g->n_cols, groups = (nc + 7) / 8;
+    for (int64_t p = 0; p < g->n_proj; ++p) {
+        for (int cg = 0; cg < groups; ++cg) {
+            const int64_t gp = g->proj0 + p;
+            const float *q = g->xy + gp * 6;
+            const d3 s = {q[0], q[1], q[2]};
+            const d3 dc = {q[3], q[4], q[5]};
+            const double ux = g->uv[gp * 2], uy = g->uv[gp * 2 + 1];
+            const int c0 = cg * 8;
+            const int maxzz = nc - c0 < 8 ? nc - c0 : 8;
+            for (int r = 0; r < nr; ++r) {
+                const double ia = (double)r - (double)nr / 2.0 + 0.5;
+                const double ib = (double)c0 - (double)nc / 2.0 + 0.5;
+                const d3 d = {dc.x + ia * ux, dc.y + ia * uy, dc.z + ib * g->pitch_y};
+                const d3 dR = {d.x - 0.5 * ux, d.y - 0.5 * uy, d.z};
+                const d3 dL = {d.x + 0.5 * ux, d.y + 0.5 * uy, d.z};
+                const d3 dU = {d.x, d.y, d.z + 0.5 * g->pitch_y};
+                const d3 dD = {d.x, d.y, d.z - 0.5 * g->pitch_y};
+                const d3 dsv = sub(d, s);
+                const double L = len3(dsv);
+                double kerroin = g->dx * g->dy * g->dz;
+                const double apuZ = g->bz - s.z - g->dz / 2.0;
+                const int ysl = fabs(s.x) <= fabs(s.y);
+                double P0, P1, Z0, Z1, apuL, apuV, dlat, dsl;
+                int nsl, nlat;
+                if (ysl) {
+                    P0 = (dL.x - s.x) / (dL.y - s.y); P1 = (dR.x - s.x) / (dR.y - s.y);
+                    Z0 = (dU.z - s.z) / (dU.y - s.y); Z1 = (dD.z - s.z) / (dD.y - s.y);
+                    kerroin /= fabs(dsv.y / L);
+                    apuL = g->bx - s.x - g->dx / 2.0; apuV = g->by - s.y;
+                    dlat = g->dx; dsl = g->dy; nsl = ny; nlat = nx;
+                } else {
+                    P0 = (dL.y - s.y) / (dL.x - s.x); P1 = (dR.y - s.y) / (dR.x - s.x);
+                    Z0 = (dU.z - s.z) / (dU.x - s.x); Z1 = (dD.z - s.z) / (dD.x - s.x);
+                    kerroin /= fabs(dsv.x / L);
+                    apuL = g->by - s.y - g->dy / 2.0; apuV = g->bx - s.x;
+                    dlat = g->dy; dsl = g->dx; nsl = nx; nlat = ny;
+                }
+                const int64_t yidx = r + (int64_t)c0 * nr + p * (int64_t)nr * nc;
+                for (int jj = 0; jj < nsl; ++jj) {
+                    const double v = (jj + 0.5) * dsl + apuV;
+                    const double a0 = v * P0 - apuL, a1 = v * P1 - apuL;
+                    const double z0 = v * Z0 - apuZ, z1 = v * Z1 - apuZ;
+                    const double xl = fmin(a0, a1), xr = fmax(a0, a1);
+                    const double zu = fmin(z0, z1), zd = fmax(z0, z1);
+                    const double area = fabs((xl - xr) * (zu - zd));
+                    const double w = zd - zu;
+                    /* voxel-edge coordinates of the footprint */
+                    const double el = xl / dlat - 0.5, er = xr / dlat - 0.5;
+                    const int ia0 = (int)floor(fmax(el, 0.0)), ia1 = (int)ceil(fmin(er, (double)nlat));
+                    for (int zz = 0; zz < maxzz; ++zz) {
+                        const double yv = y[yidx + (int64_t)zz * nr];
+                        const double eu = (zu + zz * w) / g->dz - 0.5, ed = (zd + zz * w) / g->dz - 0.5;
+                        const int k0 = (int)floor(fmax(eu, 0.0)), k1 = (int)ceil(fmin(ed, (double)nz));
+                        for (int k = k0; k < k1; ++k) {
+                            const double oz = overlap(eu, ed, (double)k, (double)k + 1.0);
+                            if (oz <= 0.0) continue;
+                            for (int i = ia0; i < ia1; ++i) {
+                                const double ox = overlap(el, er, (double)i, (double)i + 1.0);
+                                if (ox <= 0.0) continue;
+                                const double wt = kerroin * ox * oz / area;
+                                const size_t n = ysl ? (size_t)i + (size_t)jj * nx + (size_t)k * nx * ny
+                                                     : (size_t)jj + (size_t)i * nx + (size_t)k * nx * ny;
+                                img[n] += wt * yv;
+                                if (sens) sens[n] += wt;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    return 0;
+}

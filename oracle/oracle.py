@@ -93,6 +93,7 @@ def lib():
         C = ctypes.POINTER(OracleCT)
         L.oracle_bdd_fp.argtypes = [C, P, P]
         L.oracle_bdd_bp.argtypes = [C, P, P, P]
+        L.oracle_bdd_bp_ray.argtypes = [C, P, P, P]
         L.oracle_orth_fp.argtypes = [G, P, P]
         L.oracle_orth_bp.argtypes = [G, P, P, P]
         L.oracle_interp_fp.argtypes = [G, ctypes.c_double, P, P]
@@ -619,6 +620,18 @@ def bdd_backward(geom: Geometry, y, subset, sens=False):
     s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
     if lib().oracle_bdd_bp(ctypes.byref(g), _dp(yy), _dp(img), _dp(s)) != 0:
         raise MemoryError("oracle_bdd_bp")
+    return (img, s) if sens else img
+
+
+def bdd_backward_ray(geom: Geometry, y, subset, sens=False):
+    """FP64 ray-driven distance-driven backprojection: the exact adjoint of
+    bdd_forward (and its A^T 1)."""
+    yy = np.ascontiguousarray(y, dtype=np.float64).ravel()
+    g = _ct_struct(geom, subset)
+    img = np.zeros(geom.n_img, dtype=np.float64)
+    s = np.zeros(geom.n_img, dtype=np.float64) if sens else None
+    if lib().oracle_bdd_bp_ray(ctypes.byref(g), _dp(yy), _dp(img), _dp(s)) != 0:
+        raise MemoryError("oracle_bdd_bp_ray")
     return (img, s) if sens else img
 
 

@@ -58,14 +58,14 @@ def cbct(cuda):
     y = np.random.default_rng(8).uniform(0.0, 2.0, g.rays(0))
     ref_fp = orc.bdd_forward(g, x, 0)
     ref_bp, ref_sens = orc.bdd_backward(g, y, 0, sens=True)
-    return o, x, y, ref_fp, ref_bp, ref_sens
+    return o, x, y, ref_fp, ref_bp, ref_sens, g
 
 
 @pytest.mark.parametrize("staged", [1, 0])
 @pytest.mark.parametrize("columns", [8, 16])
 def test_cbct_full_geometry_forward(cuda, cbct, staged, columns):
     from omega_b200 import _native
-    o, x, _, ref_fp, _, _ = cbct
+    o, x, _, ref_fp, _, _, _ = cbct
     o.tuning = {"bdd_fp_staged": staged, "bdd_fp_columns": columns}
     y = o.forwardProject(_t(x, cuda), 0).cpu().numpy()
     assert _native.lib().omb_take_device_error() == 0
@@ -75,12 +75,30 @@ def test_cbct_full_geometry_forward(cuda, cbct, staged, columns):
 @pytest.mark.parametrize("staged", [1, 0])
 def test_cbct_full_geometry_backward(cuda, cbct, staged):
     from omega_b200 import _native
-    o, _, y, _, ref_bp, ref_sens = cbct
+    o, _, y, _, ref_bp, ref_sens, _ = cbct
     o.tuning = {"bdd_bp_staged": staged}
     img, sens = o.backwardProject(_t(y, cuda), 0, sens=True)
     assert _native.lib().omb_take_device_error() == 0
     assert orc.rel_l2(img.cpu().numpy(), ref_bp) < TOL
     assert orc.rel_l2(sens.cpu().numpy(), ref_sens) < TOL
+
+
+def test_cbct_full_geometry_ray_backward(cuda, cbct):
+    """The ray-driven scatter backprojection (float atomics) at the benchmark
+    geometry against the FP64 adjoint of the forward projection."""
+    import ctypes
+
+    import torch
+    from omega_b200 import _native
+    o, _, y, _, _, _, g = cbct
+    ref = orc.bdd_backward_ray(g, y, 0)
+    yd = _t(y, cuda)
+    img = torch.empty(g.n_img, device=cuda)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _native.call("omb_backward", o._handle, 0, ctypes.c_void_p(yd.data_ptr()), ctypes.c_void_p(img.data_ptr()),
+                 None, _native.OMB_BP_RAY, st)
+    assert orc.rel_l2(img.cpu().numpy(), ref) < TOL
+    assert _native.lib().omb_take_device_error() == 0
 
 
 @pytest.mark.parametrize("layout", [0, 1])
