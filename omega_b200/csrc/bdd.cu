@@ -57,17 +57,23 @@ __global__ void k_bdd_fp(Grid g, const float *__restrict__ xy, const float *__re
     for (int c = 0; c < kColsPerThread; ++c) temp[c] = 0.f;
 
     const int zmax = g.nz - 1;
-    for (int j = 0; j < nsl; ++j) {
+    // only the slices where the group's footprint can meet the volume
+    SliceRange range = slice_range_empty();
+    slice_range_add(range, b.xa0, b.xa1, b.xb0, b.xb1, b.za0, b.za1, b.zb0, b.zb1, nsl, nlat, g.nz,
+                    (float)kColsPerThread);
+    const int2 jr = slice_range_bounds(range);
+    for (int j = jr.x; j <= jr.y; ++j) {
         const float fj = (float)j;
         const float xa = fmaf(fj, b.xa1, b.xa0), xb = fmaf(fj, b.xb1, b.xb0);
         const float za = fmaf(fj, b.za1, b.za0), zb = fmaf(fj, b.zb1, b.zb0);
         const float el = fminf(xa, xb), er = fmaxf(xa, xb);
         const float zu = fminf(za, zb);
         const float w = fabsf(fmaf(fj, b.dz1, b.dz0));
-        const float inv_area = 1.f / (fabsf(fmaf(fj, b.dw1, b.dw0)) * dlat * w * g.dz);
-        // lateral overlap range (clamped to the slice)
+        // lateral overlap range (clamped to the slice); a run of columns wholly
+        // above or below the volume integrates to exactly zero
         const float cl = fmaxf(el, 0.f), cr = fminf(er, flat);
-        if (!(cr > cl)) continue;
+        if (!(cr > cl) || !(zu < fz) || !(fmaf((float)kColsPerThread, w, zu) > 0.f)) continue;
+        const float inv_area = 1.f / (fabsf(fmaf(fj, b.dw1, b.dw0)) * dlat * w * g.dz);
         const int i0 = (int)cl;  // cl >= 0: truncation is floor
         const Seg seg = make_seg(cl, cr, i0, min((int)ceilf(cr), nlat) - 1 - i0);
         const float *slice = vol + (int64_t)j * sl_stride + i0;
@@ -99,6 +105,115 @@ __global__ void k_bdd_fp(Grid g, const float *__restrict__ xy, const float *__re
 #pragma unroll
     for (int c = 0; c < kColsPerThread; ++c)
         if (c < ncol) y[idx + (int64_t)c * nr] = temp[c] * (c < 8 ? b.kerroin : kerroin8);
+}
+
+// Ray-driven (scatter) backprojection: the exact adjoint of k_bdd_fp<8>.
+// Same thread layout and footprint walk as the forward projection; where the
+// forward sums the lateral row integrals of the rows a column's axial range
+// [b_c, b_c+1] crosses, weighted by the overlap lengths, the adjoint collects
+// for every crossed row k the measurement-weighted overlaps
+//   A(k) = kerroin * sum_c y_c * |[b_c, b_c+1] n [k, k+1]|
+// and adds A(k) * w_i / area to the voxels i of the lateral run.  Float
+// atomics, or (FIXED) int64 atomics of round-toward-zero(v * 1e11): the sum
+// of integers does not depend on the order the atomics land in, so the
+// fixed-point image is bit-identical run to run.  SENS adds A^T 1.
+template <bool FIXED, bool SENS>
+__global__ void k_bdd_bp_ray(Grid g, const float *__restrict__ xy, const float *__restrict__ uv, int nr, int nc,
+                             float pitch_y, int64_t proj0, int64_t nproj, const float *__restrict__ y,
+                             float *__restrict__ img, float *__restrict__ sens, unsigned long long *__restrict__ acc,
+                             unsigned long long *__restrict__ acc_s) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cg = blockIdx.y * blockDim.y + threadIdx.y;
+    const int64_t p = blockIdx.z;
+    const int c0 = cg * 8;
+    if (r >= nr || c0 >= nc || p >= nproj) return;
+    const int ncol = min(8, nc - c0);
+    const int64_t idx = r + (int64_t)c0 * nr + p * (int64_t)nr * nc;
+    float yv[8];
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        yv[c] = c < ncol ? __ldg(y + idx + (int64_t)c * nr) : 0.f;
+        any |= yv[c] != 0.f;
+    }
+    if (!SENS && !any) return;
+    const BddRay b = bdd_ray_setup(g, xy, uv, proj0 + p, r, c0, nr, nc, pitch_y);
+    const int nsl = b.ysl ? g.ny : g.nx;
+    const int nlat = b.ysl ? g.nx : g.ny;
+    // slices along y: lateral = x; slices along x: lateral = y (x-fastest image)
+    const int64_t lat_stride = b.ysl ? 1 : g.nx;
+    const int64_t sl_stride = b.ysl ? g.nx : 1;
+    const int64_t z_stride = (int64_t)g.nx * g.ny;
+    const float flat = (float)nlat, fz = (float)g.nz;
+    const float dlat = b.ysl ? g.dx : g.dy;
+    const int zmax = g.nz - 1;
+    const float ker = b.kerroin;
+    SliceRange range = slice_range_empty();
+    slice_range_add(range, b.xa0, b.xa1, b.xb0, b.xb1, b.za0, b.za1, b.zb0, b.zb1, nsl, nlat, g.nz, 8.f);
+    const int2 jr = slice_range_bounds(range);
+
+    for (int j = jr.x; j <= jr.y; ++j) {
+        const float fj = (float)j;
+        const float xa = fmaf(fj, b.xa1, b.xa0), xb = fmaf(fj, b.xb1, b.xb0);
+        const float za = fmaf(fj, b.za1, b.za0), zb = fmaf(fj, b.zb1, b.zb0);
+        const float el = fminf(xa, xb), er = fmaxf(xa, xb);
+        const float zu = fminf(za, zb);
+        const float w = fabsf(fmaf(fj, b.dz1, b.dz0));
+        const float cl = fmaxf(el, 0.f), cr = fminf(er, flat);
+        if (!(cr > cl) || !(zu < fz) || !(fmaf(8.f, w, zu) > 0.f)) continue;
+        const float inv_area = 1.f / (fabsf(fmaf(fj, b.dw1, b.dw0)) * dlat * w * g.dz);
+        const int i0 = (int)cl;
+        const Seg seg = make_seg(cl, cr, i0, min((int)ceilf(cr), nlat) - 1 - i0);
+        const int64_t base = (int64_t)j * sl_stride + (int64_t)i0 * lat_stride;
+        const float scale = ker * inv_area;
+        // the row's accumulated weight goes to the lateral run's voxels
+        auto flush = [&](int k, float A, float As) {
+            const int64_t row = base + (int64_t)k * z_stride;
+            for (int e = 0; e <= seg.n; ++e) {
+                const float we = e == 0 ? seg.w0 : (e == 1 ? seg.w1 : (e == 2 ? seg.w2 :
+                                 fminf(seg.hi, (float)(seg.base + e + 1)) - (float)(seg.base + e)));
+                const int64_t off = row + (int64_t)e * lat_stride;
+                const float v = A * scale * we;
+                if (FIXED) {
+                    if (v != 0.f) atomicAdd(acc + off, (unsigned long long)(long long)((double)v * kFixedScale));
+                    if (SENS) {
+                        const float vs = As * scale * we;
+                        if (vs != 0.f) atomicAdd(acc_s + off, (unsigned long long)(long long)((double)vs * kFixedScale));
+                    }
+                } else {
+                    if (v != 0.f) atomicAdd(img + off, v);
+                    if (SENS) {
+                        const float vs = As * scale * we;
+                        if (vs != 0.f) atomicAdd(sens + off, vs);
+                    }
+                }
+            }
+        };
+        float bz = fminf(fmaxf(zu, 0.f), fz);
+        int kc = min((int)bz, zmax);
+        float prev = bz, A = 0.f, As = 0.f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float bzn = fminf(fmaxf(fmaf((float)(c + 1), w, zu), 0.f), fz);
+            const int kn = min((int)bzn, zmax);
+            const float one = c < ncol ? 1.f : 0.f;
+            while (kc < kn) {
+                const float len = (float)(kc + 1) - prev;
+                A = fmaf(yv[c], len, A);
+                if (SENS) As = fmaf(one, len, As);
+                flush(kc, A, As);
+                A = 0.f;
+                As = 0.f;
+                ++kc;
+                prev = (float)kc;
+            }
+            const float len = bzn - prev;
+            A = fmaf(yv[c], len, A);
+            if (SENS) As = fmaf(one, len, As);
+            prev = bzn;
+        }
+        flush(kc, A, As);
+    }
 }
 
 // y-fastest copy of an x-fastest volume (per z slice, a 2-D transpose).
@@ -316,6 +431,32 @@ int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc,
         default: launch_fp<8>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, tn.bdd_fp_rows, st); break;
     }
     OMB_LAUNCH_CHECK("bdd forward launch");
+    return OMB_OK;
+}
+
+int bdd_backward_ray(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
+                     int64_t nproj, const float *y, float *img, float *sens, unsigned long long *acc,
+                     unsigned long long *acc_s, cudaStream_t st) {
+    if (nproj <= 0) return OMB_OK;
+    if (nproj > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 projections in one call");
+    const int groups = (nc + 7) / 8;
+    dim3 block(32, 4);
+    dim3 grid((nr + 31) / 32, (groups + 3) / 4, (unsigned)nproj);
+    if (acc) {
+        if (acc_s)
+            k_bdd_bp_ray<true, true><<<grid, block, 0, st>>>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, y, img, sens,
+                                                              acc, acc_s);
+        else
+            k_bdd_bp_ray<true, false><<<grid, block, 0, st>>>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, y, img, sens,
+                                                               acc, acc_s);
+    } else if (sens) {
+        k_bdd_bp_ray<false, true><<<grid, block, 0, st>>>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, y, img, sens,
+                                                           acc, acc_s);
+    } else {
+        k_bdd_bp_ray<false, false><<<grid, block, 0, st>>>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, y, img, sens,
+                                                            acc, acc_s);
+    }
+    OMB_LAUNCH_CHECK("type-5 ray-driven backward launch");
     return OMB_OK;
 }
 

@@ -76,6 +76,74 @@ __device__ __forceinline__ BddRay bdd_ray_setup(const Grid &g, const float *__re
     return b;
 }
 
+// Slices [lo, hi] outside which a group of rays cannot meet the volume: a
+// forward-projection thread (one ray group) or a CTA (the union of its
+// corner ray groups) loops over these slices only.  The slices where a ray
+// group's footprint meets the volume satisfy four conditions, each the union
+// of half-lines in j (the footprint edges are linear in the slice index):
+//   lateral  min(xa, xb) < nlat  and  max(xa, xb) > 0,
+//   axial    min(za, zb) < nz    and  the group's top > 0, where the top of
+//            C columns is zu + C|zb - za|, bounded by C zb - (C-1) za or
+//            C za - (C-1) zb.
+// Each condition's solution set is replaced by the hull of its half-lines
+// (one slice of margin at each end) and the hulls are intersected: a superset
+// of the true slices, so skipping the others changes no result -- outside
+// them every column's footprint integral is exactly zero.
+struct SliceHull {
+    int lo, hi;  // hull of the half-lines added so far; lo > hi: empty
+};
+
+// adds {j in [0, nsl-1] : a + b j > c} to the hull
+__device__ __forceinline__ void slice_halfline(SliceHull &h, float a, float b, float c, int nsl) {
+    int lo = 0, hi = nsl - 1;
+    if (fabsf(b) * (float)nsl <= 1e-6f * (fabsf(a) + fabsf(c) + 1.f)) {
+        if (!(a > c - 1e-4f * (fabsf(c) + 1.f))) return;  // constant and false
+    } else {
+        const float js = (c - a) / b;
+        if (b > 0.f) {
+            if (js >= (float)nsl) return;
+            lo = max((int)floorf(js) - 1, 0);
+        } else {
+            if (js < 0.f) return;
+            hi = min((int)ceilf(js) + 1, nsl - 1);
+        }
+    }
+    if (lo > hi) return;
+    h.lo = min(h.lo, lo);
+    h.hi = max(h.hi, hi);
+}
+
+// The four condition hulls of one ray group (edges e(j) = e0 + j e1 in voxel
+// units, as BddRay holds them), accumulated over several groups.
+struct SliceRange {
+    SliceHull lat_lo, lat_hi, ax_lo, ax_hi;
+};
+
+__device__ __forceinline__ SliceRange slice_range_empty() {
+    SliceRange r;
+    r.lat_lo = r.lat_hi = r.ax_lo = r.ax_hi = SliceHull{1 << 30, -1};
+    return r;
+}
+
+__device__ __forceinline__ void slice_range_add(SliceRange &r, float xa0, float xa1, float xb0, float xb1, float za0,
+                                                float za1, float zb0, float zb1, int nsl, int nlat, int nz,
+                                                float C) {
+    slice_halfline(r.lat_lo, -xa0, -xa1, -(float)nlat, nsl);
+    slice_halfline(r.lat_lo, -xb0, -xb1, -(float)nlat, nsl);
+    slice_halfline(r.lat_hi, xa0, xa1, 0.f, nsl);
+    slice_halfline(r.lat_hi, xb0, xb1, 0.f, nsl);
+    slice_halfline(r.ax_lo, -za0, -za1, -(float)nz, nsl);
+    slice_halfline(r.ax_lo, -zb0, -zb1, -(float)nz, nsl);
+    slice_halfline(r.ax_hi, C * zb0 - (C - 1.f) * za0, C * zb1 - (C - 1.f) * za1, 0.f, nsl);
+    slice_halfline(r.ax_hi, C * za0 - (C - 1.f) * zb0, C * za1 - (C - 1.f) * zb1, 0.f, nsl);
+}
+
+// [lo, hi] of the slices to visit (lo > hi: none)
+__device__ __forceinline__ int2 slice_range_bounds(const SliceRange &r) {
+    return make_int2(max(max(r.lat_lo.lo, r.lat_hi.lo), max(r.ax_lo.lo, r.ax_hi.lo)),
+                     min(min(r.lat_lo.hi, r.lat_hi.hi), min(r.ax_lo.hi, r.ax_hi.hi)));
+}
+
 // The forward weight dx*dy*dz / |u_axis| of the ray through pixel (r, c).
 __device__ __forceinline__ float bdd_kerroin(const Grid &g, const float *__restrict__ xy,
                                              const float *__restrict__ uv, int64_t gp, int r, int c, int nr, int nc,

@@ -66,6 +66,7 @@ struct Shared {
     alignas(8) uint64_t full[kStages];
     int2 origin[kStages];  // (lateral, z) voxel of the box's first element
     Corner corner[4];
+    int2 slices;           // [first, last] slice the CTA's rays can meet
 };
 
 // Box of slice j covering the four corner rays' footprints (lateral start
@@ -126,6 +127,18 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
     const int nsl = ysl ? g.ny : g.nx;
     const int nlat = ysl ? g.nx : g.ny;
     const CUtensorMap *map = ysl ? &map_img : &map_imgT;
+    // the slices any of the CTA's ray groups can meet (the hull over its
+    // corner groups); outside them every footprint integral is zero
+    if (tid == 0) {
+        SliceRange range = slice_range_empty();
+        for (int q = 0; q < 4; ++q) {
+            const Corner &c = sh.corner[q];
+            slice_range_add(range, c.xa0, c.xa1, c.xb0, c.xb1, c.za0, c.za1, c.zb0, c.zb1, nsl, nlat, g.nz, 8.f);
+        }
+        sh.slices = slice_range_bounds(range);
+    }
+    __syncthreads();
+    const int j_lo = sh.slices.x, j_hi = sh.slices.y;
 
     // loads slice jn into stage s (one thread)
     auto issue = [&](int jn, int s) {
@@ -142,7 +155,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
             : "memory");
     };
     if (tid == 0)
-        for (int s = 0; s < kStages && s < nsl; ++s) issue(s, s);
+        for (int s = 0; s < kStages && j_lo + s <= j_hi; ++s) issue(j_lo + s, s);
 
     BddRay b{};
     float kerroin = 0.f;
@@ -160,9 +173,10 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
     for (int c = 0; c < 8; ++c) temp[c] = 0.f;
     int tries = kWaitTries;
 
-    for (int j = 0; j < nsl; ++j) {
-        const int s = j % kStages;
-        if (!mbar_wait(smem_u32(&sh.full[s]), (uint32_t)((j / kStages) & 1), tries)) {
+    for (int j = j_lo; j <= j_hi; ++j) {
+        const int t = j - j_lo;  // position in the ring's sequence
+        const int s = t % kStages;
+        if (!mbar_wait(smem_u32(&sh.full[s]), (uint32_t)((t / kStages) & 1), tries)) {
             atomicExch(&g_device_error, 1);
             tries = kWaitTriesAfterFailure;
         }
@@ -173,7 +187,8 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
         const float zu = fminf(za, zb);
         const float w = fabsf(fmaf(fj, b.dz1, b.dz0));
         const float cl = fmaxf(el, 0.f), cr = fminf(er, flat);
-        if (active && cr > cl) {
+        // a run of columns wholly above or below the volume integrates to zero
+        if (active && cr > cl && zu < fz && fmaf(8.f, w, zu) > 0.f) {
             const float inv_area = 1.f / (fabsf(fmaf(fj, b.dw1, b.dw0)) * dlat * w * g.dz);
             const int i0 = (int)cl;
             const Seg seg = make_seg(cl, cr, i0, min((int)ceilf(cr), nlat) - 1 - i0);
@@ -229,7 +244,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
             }
         }
         __syncthreads();  // stage s is free again
-        if (threadIdx.x == 0 && threadIdx.y == j % kRB && j + kStages < nsl) issue(j + kStages, s);
+        if (threadIdx.x == 0 && threadIdx.y == t % kRB && j + kStages <= j_hi) issue(j + kStages, s);
     }
     if (!active) return;
     const int ncol = min(8, nc - c0);
