@@ -274,11 +274,15 @@ constexpr int kRW = 52;                            // detector rows of a box (mu
 constexpr int kCW = kSlots + 4;                    // detector columns of a box
 constexpr int kStageFloats = (kRW * kCW + 31) / 32 * 32;  // 128-byte aligned stages
 constexpr int kStages = 4;
+constexpr int kChunk = 16;  // views whose re-based maps the CTA prepares together
 
 struct Shared {
     alignas(128) float box[kStages][kStageFloats];
     alignas(8) uint64_t full[kStages];
-    BddMapR map[kStages];  // the stage's map re-based to this block; (U0, V0) = the box's first element
+    // the maps of a chunk of views re-based to this block, (U0, V0) = the
+    // view's box origin; two chunks alternate (the one being consumed and
+    // the next, prepared once per kChunk views by all threads)
+    BddMapR map[2][kChunk];
     float2 pref[kSlots][kThreads];
 };
 
@@ -306,39 +310,49 @@ __global__ void __launch_bounds__(bb::kThreads, 6)
     }
     __syncthreads();
 
-    // corner `lane & 7` of the CTA's voxel block (edges of its voxels)
-    const float cx = g.bx + (float)((lane & 1) ? min((int)blockIdx.x * 32 + 32, g.nx) : (int)blockIdx.x * 32) * g.dx;
-    const float cy = g.by + (float)((lane & 2) ? min((int)blockIdx.y * 4 + 4, g.ny) : (int)blockIdx.y * 4) * g.dy;
-    const float cz = g.bz + (float)((lane & 4) ? min(kz0 + kBpZ, g.nz) : kz0) * g.dz;
+    // corner `tid & 7` of the CTA's voxel block (edges of its voxels)
+    const int q8 = tid & 7;
+    const float cx = g.bx + (float)((q8 & 1) ? min((int)blockIdx.x * 32 + 32, g.nx) : (int)blockIdx.x * 32) * g.dx;
+    const float cy = g.by + (float)((q8 & 2) ? min((int)blockIdx.y * 4 + 4, g.ny) : (int)blockIdx.y * 4) * g.dy;
+    const float cz = g.bz + (float)((q8 & 4) ? min(kz0 + kBpZ, g.nz) : kz0) * g.dz;
     const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 4;
     const double p0x = (double)g.bx + (double)i0 * g.dx, p0y = (double)g.by + (double)j0 * g.dy;
     const double p0z = (double)g.bz + (double)kz0 * g.dz;
-    // loads the box of projection pn into stage s (a whole warp; lane 0 issues)
-    auto produce = [&](int64_t pn, int s) {
-        const BddProj P = pj[pn];
+    // prepares the re-based maps of views [kChunk c, kChunk (c + 1)): thread
+    // 8v + q projects corner q of the block with view v's float map, the 8
+    // corners' minimum gives the box origin, and thread 8v re-bases the FP64
+    // map to it.  All threads of the CTA take part (warp-uniform shuffles).
+    auto prepare = [&](int64_t c) {
+        const int64_t pv = c * kChunk + (tid >> 3);
+        const bool have = pv < nproj;
+        const BddProj P = pj[have ? pv : 0];
         float2 uv = bdd_corner_uv(P, cx, cy, cz);
 #pragma unroll
         for (int o = 1; o < 8; o <<= 1) {
             uv.x = fminf(uv.x, __shfl_xor_sync(0xffffffffu, uv.x, o));
             uv.y = fminf(uv.y, __shfl_xor_sync(0xffffffffu, uv.y, o));
         }
-        if (lane == 0) {
+        if (have && q8 == 0) {
             const int2 org = bdd_block_origin(uv.x, uv.y, nr, nc);
-            // the map re-based to the block corner with the box origin as pixel
-            // origin (FP64), published to the consumers by the arrive below
-            bdd_rebase(sh.map[s], pm[pn], P, p0x, p0y, p0z, org.x, org.y);
-            const uint32_t bar = bt::smem_u32(&sh.full[s]);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
-                         "r"((uint32_t)(kRW * kCW * sizeof(float)))
-                         : "memory");
-            asm volatile(
-                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
-                "%4}], [%5];\n" ::"r"(bt::smem_u32(sh.box[s])),
-                "l"(reinterpret_cast<uint64_t>(&map_y)), "r"(org.x), "r"(org.y), "r"((int)pn), "r"(bar)
-                : "memory");
+            bdd_rebase(sh.map[c & 1][tid >> 3], pm[pv], P, p0x, p0y, p0z, org.x, org.y);
         }
     };
-    if (threadIdx.y == 0)
+    // loads the detector box of projection pn into stage s (one thread)
+    auto produce = [&](int64_t pn, int s) {
+        const BddMapR &M = sh.map[(pn / kChunk) & 1][pn % kChunk];
+        const uint32_t bar = bt::smem_u32(&sh.full[s]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
+                     "r"((uint32_t)(kRW * kCW * sizeof(float)))
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+            "%4}], [%5];\n" ::"r"(bt::smem_u32(sh.box[s])),
+            "l"(reinterpret_cast<uint64_t>(&map_y)), "r"(M.o.x), "r"(M.o.y), "r"((int)pn), "r"(bar)
+            : "memory");
+    };
+    prepare(0);
+    __syncthreads();
+    if (tid == 0)
         for (int s = 0; s < kStages && s < nproj; ++s) produce(s, s);
 
     const int nzt = FULL ? kBpZ : min(kBpZ, g.nz - kz0);
@@ -360,6 +374,9 @@ __global__ void __launch_bounds__(bb::kThreads, 6)
     int tries = bt::kWaitTries;
     for (int64_t p = 0; p < nproj; ++p) {
         const int s = (int)(p % kStages);
+        // the next chunk's maps, kChunk views ahead of their first use (the
+        // buffer held the previous chunk, all of whose views are done)
+        if (p % kChunk == 0 && p + kChunk < nproj) prepare(p / kChunk + 1);
         if (!bt::mbar_wait(bt::smem_u32(&sh.full[s]), (uint32_t)((p / kStages) & 1), tries)) {
             atomicExch(&g_device_error, 1);
             tries = bt::kWaitTriesAfterFailure;
@@ -367,7 +384,7 @@ __global__ void __launch_bounds__(bb::kThreads, 6)
         do {
             if (!active) break;
             // u, v below are relative to the box origin (U0, V0)
-            const BddMapR M = sh.map[s];
+            const BddMapR M = sh.map[(p / kChunk) & 1][p % kChunk];
             BpFootprint F;
             if (!bdd_bp_footprint(M, rx0, ry0, rz0, hx, hy, hz, qx, qy, g, nr, nc, nzt, F)) break;
             const Seg &seg = F.seg;
@@ -443,7 +460,7 @@ __global__ void __launch_bounds__(bb::kThreads, 6)
             }
         } while (false);
         __syncthreads();  // stage s is free again
-        if (threadIdx.y == (int)(p % 4) && p + kStages < nproj) produce(p + kStages, s);
+        if (lane == 0 && threadIdx.y == (int)(p % 4) && p + kStages < nproj) produce(p + kStages, s);
     }
     if (!active) return;
     int64_t n = i + (int64_t)j * g.nx + (int64_t)kz0 * g.nx * g.ny;
