@@ -371,6 +371,12 @@ typedef struct omb_recon_params {
     const float *wmean_weights;/* weighted mean: device, options.weighted_weights (x fastest) */
     int32_t wmean_type;       /* weighted mean: options.mean_type (1 arithmetic, 2 harmonic, 3 geometric); the
                                  normalisation switch is mrp_no_norm (options.med_no_norm) */
+    int32_t tv_variant;       /* OMB_PRIOR_TV and PDHG: omb_tv_variant (0: the plain TV) */
+    float tv_sigma;           /* OMB_PRIOR_TV and PDHG: options.SATVPhi (SATV, weighted TV) */
+    float tv_c;               /* OMB_PRIOR_TV and PDHG: options.C (anatomical type 2) or options.eta (type 5,
+                                 APLS) */
+    const float *tv_ref;      /* OMB_PRIOR_TV and PDHG: device reference image / tensor of the anatomical
+                                 variants (OMB_TV_ANAT1 and above), NULL otherwise */
 } omb_recon_params;
 
 /*
@@ -391,6 +397,15 @@ int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *y, const fl
 int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const float *sens,
                    const float *du, float *work_meas, float *work_img, void *stream);
 
+typedef enum omb_tv_variant {
+    OMB_TV_PLAIN = 0,  /* TVtype 1-3 without a reference image: the plain smoothed TV */
+    OMB_TV_SATV = 1,   /* TVtype 4 (SATV), sigma = options.SATVPhi */
+    OMB_TV_W1 = 2,     /* TVtype 6 (weighted TV, TVW1), sigma = options.SATVPhi */
+    OMB_TV_ANAT1 = 3,  /* TV_use_anatomical, TVtype 1: ref = the 9-channel tensor (9 images, channel 3 r + c) */
+    OMB_TV_ANAT2 = 4,  /* TV_use_anatomical, TVtype 2: ref = the reference image, C = options.C */
+    OMB_TV_APLS = 5    /* TV_use_anatomical TVtype 5, and APLS: ref = the reference image, C = options.eta */
+} omb_tv_variant;
+
 /*
  * Smoothed TV gradient (priors.h:404-409, TVKernel auxKernels.cl:1733-1990,
  * plain TV; neighbours outside the image read the edge voxel): grad += beta *
@@ -398,6 +413,17 @@ int omb_osl_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
  */
 int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float beta, float smooth,
                     void *stream);
+
+/*
+ * The TV gradients of the other TV settings (TVKernel built with -DSATV,
+ * -DTVW1, -DANATOMICAL1/2/3; ProjectorClass.h:900-918, functions.hpp:
+ * 1096-1113): grad += beta * dTV_variant(u), smoothing `smooth`
+ * (TVsmoothing, APLSsmoothing for APLS); `ref` (device) the reference image
+ * or tensor of the anatomical variants, NULL otherwise.  OMB_TV_PLAIN is
+ * omb_tv_gradient.
+ */
+int omb_tv_gradient_ex(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float beta, float smooth,
+                       int32_t variant, float sigma, float C, const float *ref, void *stream);
 
 /*
  * GGMRF prior gradient (GGMRFKernel, auxKernels.cl:878-980; the image read

@@ -123,6 +123,10 @@ class ReconParams(ctypes.Structure):
         ("hyper_delta", ctypes.c_float),
         ("wmean_weights", ctypes.c_void_p),
         ("wmean_type", ctypes.c_int32),
+        ("tv_variant", ctypes.c_int32),
+        ("tv_sigma", ctypes.c_float),
+        ("tv_c", ctypes.c_float),
+        ("tv_ref", ctypes.c_void_p),
     ]
 
 
@@ -142,6 +146,7 @@ OMB_PRIOR_HUBER = 3
 OMB_PRIOR_NLM = 4
 OMB_PRIOR_MRP = 5
 OMB_PRIOR_TV = 6
+OMB_TV_PLAIN, OMB_TV_SATV, OMB_TV_W1, OMB_TV_ANAT1, OMB_TV_ANAT2, OMB_TV_APLS = range(6)
 OMB_PRIOR_GGMRF = 7
 OMB_PRIOR_HYPERBOLIC = 8
 OMB_PRIOR_WMEAN = 9
@@ -243,6 +248,9 @@ EXPORTS = [
                                           ctypes.c_float, ctypes.c_void_p]),
     ("omb_tv_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_void_p]),
+    ("omb_tv_gradient_ex", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                          ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_mrp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p]),

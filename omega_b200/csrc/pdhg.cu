@@ -182,3 +182,178 @@ extern "C" int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t 
     OMB_LAUNCH_CHECK("TV gradient launch");
     return OMB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// The other TV gradients the reference compiles into TVKernel
+// (auxKernels.cl:1733-1990), selected by TVtype / TV_use_anatomical / APLS
+// (ProjectorClass.h:900-918, functions.hpp:1096-1113):
+//   OMB_TV_SATV   TVtype 4 (SATV): per axis and side, d = u - neighbour,
+//                 a = d / (|d| + epps); grad += beta sum (a - a / (|d| / sigma + 1))
+//   OMB_TV_W1     TVtype 6 (TVW1): the plain TV's forward and backward
+//                 differences weighted by exp(-(d / sigma)^2) per component
+//   OMB_TV_ANAT1  anatomical TVtype 1: the quadratic forms of the 9-channel
+//                 tensor S (prepass assembleS) on the same differences
+//   OMB_TV_ANAT2  anatomical TVtype 2: the forward term's norm adds
+//                 C |forward differences of the reference image S|^2
+//   OMB_TV_APLS   anatomical TVtype 5 and APLS (C = eta): asymmetric parallel
+//                 level sets with the reference image's normalised gradient
+// The image is read edge-clamped (the texture path); S is read as zero past
+// the last voxel (its buffer path).  The formulas keep the reference's own
+// choices, e.g. TVW1's backward-z term weighted by w3.y and APLS's norms
+// built from the raw reference gradient.
+// ---------------------------------------------------------------------------
+namespace omb {
+namespace tvv {
+
+struct Nb {
+    float c, px, py, pz, mx, my, mz, uix, uiy, ujx, ujy, ukx, uky;
+};
+
+__device__ __forceinline__ Nb gather(const float *__restrict__ u, int i, int j, int k, int nx, int ny, int nz) {
+    Nb b;
+    b.c = tv_at(u, i, j, k, nx, ny, nz);
+    b.px = tv_at(u, i + 1, j, k, nx, ny, nz);
+    b.py = tv_at(u, i, j + 1, k, nx, ny, nz);
+    b.pz = tv_at(u, i, j, k + 1, nx, ny, nz);
+    b.mx = tv_at(u, i - 1, j, k, nx, ny, nz);
+    b.my = tv_at(u, i, j - 1, k, nx, ny, nz);
+    b.mz = tv_at(u, i, j, k - 1, nx, ny, nz);
+    b.uix = tv_at(u, i - 1, j + 1, k, nx, ny, nz);
+    b.uiy = tv_at(u, i - 1, j, k + 1, nx, ny, nz);
+    b.ujx = tv_at(u, i + 1, j - 1, k, nx, ny, nz);
+    b.ujy = tv_at(u, i, j - 1, k + 1, nx, ny, nz);
+    b.ukx = tv_at(u, i + 1, j, k - 1, nx, ny, nz);
+    b.uky = tv_at(u, i, j + 1, k - 1, nx, ny, nz);
+    return b;
+}
+
+__device__ __forceinline__ float wnorm(float a, float b, float c, float wa, float wb, float wc, float eps) {
+    return sqrtf(wa * a * a + wb * b * b + wc * c * c + eps);
+}
+
+__device__ __forceinline__ float w_of(float d, float sigma) {
+    const float t = d / sigma;
+    return __expf(-t * t);
+}
+
+}  // namespace tvv
+
+template <int V>
+__global__ void __launch_bounds__(256) k_tv_variant(const float *__restrict__ u, const float *__restrict__ S,
+                                                    float *__restrict__ grad, int nx, int ny, int nz, float beta,
+                                                    float eps, float sigma, float C) {
+    using namespace tvv;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nx || j >= ny || k >= nz) return;
+    const int64_t nxy = (int64_t)nx * ny;
+    const int64_t n = i + (int64_t)j * nx + (int64_t)k * nxy;
+    const Nb b = gather(u, i, j, k, nx, ny, nz);
+    // the backward-difference triples of the plain TV (u1, u2, u3)
+    const float a1x = b.c - b.mx, a1y = b.uix - b.mx, a1z = b.uiy - b.mx;
+    const float a2x = b.ujx - b.my, a2y = b.c - b.my, a2z = b.ujy - b.my;
+    const float a3x = b.ukx - b.mz, a3y = b.uky - b.mz, a3z = b.c - b.mz;
+    float g;
+    if (V == OMB_TV_SATV) {
+        const float d[6] = {b.c - b.px, b.c - b.mx, b.c - b.py, b.c - b.my, b.c - b.pz, b.c - b.mz};
+        g = 0.f;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const float ad = fabsf(d[q]);
+            const float a = d[q] / (ad + eps);
+            g += a - a / (ad / sigma + 1.f);
+        }
+    } else if (V == OMB_TV_W1) {
+        const float fx = b.px - b.c, fy = b.py - b.c, fz = b.pz - b.c;
+        const float w4x = w_of(fx, sigma), w4y = w_of(fy, sigma), w4z = w_of(fz, sigma);
+        const float w1x = w_of(a1x, sigma), w1y = w_of(a1y, sigma), w1z = w_of(a1z, sigma);
+        const float w2x = w_of(a2x, sigma), w2y = w_of(a2y, sigma), w2z = w_of(a2z, sigma);
+        const float w3x = w_of(a3x, sigma), w3y = w_of(a3y, sigma), w3z = w_of(a3z, sigma);
+        g = -(w4x * fx + w4y * fy + w4z * fz) / wnorm(fx, fy, fz, w4x, w4y, w4z, eps) +
+            w1x * (b.c - b.mx) / wnorm(a1x, a1y, a1z, w1x, w1y, w1z, eps) +
+            w2y * (b.c - b.my) / wnorm(a2x, a2y, a2z, w2x, w2y, w2z, eps) +
+            w3y * (b.c - b.mz) / wnorm(a3x, a3y, a3z, w3x, w3y, w3z, eps);
+    } else if (V == OMB_TV_ANAT1) {
+        const int64_t N = nxy * nz;
+        float s[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) s[q] = __ldg(S + n + q * N);
+        auto pv = [&](float x, float y, float z) {
+            return sqrtf(x * x * s[0] + y * y * s[4] + z * z * s[8] + (s[1] + s[3]) * x * y + (s[2] + s[6]) * x * z +
+                         (s[5] + s[7]) * y * z + eps);
+        };
+        const float vx = b.px - b.c, vy = b.py - b.c, vz = b.pz - b.c;
+        const float dx = s[0] * 2.f * (b.c - b.mx) + (s[3] + s[1]) * a1y + (s[2] + s[6]) * a1z;
+        const float dy = s[4] * 2.f * (b.c - b.my) + (s[5] + s[7]) * a2z + (s[3] + s[1]) * a2x;
+        const float dz = s[8] * 2.f * (b.c - b.mz) + (s[6] + s[2]) * a3x + (s[5] + s[7]) * a3y;
+        const float d = (s[1] + s[2] + s[3] + s[6]) * vx + (s[1] + s[3] + s[5] + s[7]) * vy +
+                        (s[2] + s[5] + s[6] + s[7]) * vz + 2.f * (s[0] * vx + s[4] * vy + s[8] * vz);
+        g = 0.5f * (d / pv(vx, vy, vz) + dx / pv(a1x, a1y, a1z) + dy / pv(a2x, a2y, a2z) + dz / pv(a3x, a3y, a3z));
+    } else {
+        // anatomical types 2 and 5: forward differences of the reference image
+        const float r0 = __ldg(S + n);
+        const float rx = i < nx - 1 ? __ldg(S + n + 1) : 0.f;
+        const float ry = j < ny - 1 ? __ldg(S + n + nx) : 0.f;
+        const float rz = k < nz - 1 ? __ldg(S + n + nxy) : 0.f;
+        const float fx = b.px - b.c, fy = b.py - b.c, fz = b.pz - b.c;
+        if (V == OMB_TV_ANAT2) {
+            const float sx = rx - r0, sy = ry - r0, sz = rz - r0;
+            const float p0 = sqrtf(fx * fx + fy * fy + fz * fz + C * (sx * sx + sy * sy + sz * sz) + eps);
+            g = (3.f * b.c - b.px - b.py - b.pz) / p0 + (b.c - b.mx) / wnorm(a1x, a1y, a1z, 1.f, 1.f, 1.f, eps) +
+                (b.c - b.my) / wnorm(a2x, a2y, a2z, 1.f, 1.f, 1.f, eps) +
+                (b.c - b.mz) / wnorm(a3x, a3y, a3z, 1.f, 1.f, 1.f, eps) + 1e-7f;
+        } else {
+            float ex = rx - r0, ey = ry - r0, ez = rz - r0;
+            const float en = sqrtf(ex * ex + ey * ey + ez * ez + C * C);
+            ex /= en;
+            ey /= en;
+            ez /= en;
+            const float apuR = rx * fx + ry * fy + rz * fz;
+            const float p0 = sqrtf(fx * fx + fy * fy + fz * fz - apuR * apuR + eps);
+            auto pr = [&](float x, float y, float z) {
+                const float rr = rx * x + ry * y + rz * z;
+                return sqrtf(x * x + y * y + z * z + rr * rr + eps);
+            };
+            const float e1 = ex * a1x + ey * a1y + ez * a1z;
+            const float e2 = ex * a2x + ey * a2y + ez * a2z;
+            const float e3 = ex * a3x + ey * a3y + ez * a3z;
+            const float ec = ex * (b.c - b.px) + ey * (b.c - b.py) + ez * (b.c - b.pz);
+            g = 0.5f * ((6.f * b.c - 2.f * (b.px + b.py + b.pz) + 2.f * ec * (ex + ey + ez)) / p0 +
+                        2.f * (a1x - ex * e1) / pr(a1x, a1y, a1z) + 2.f * (a2y - ey * e2) / pr(a2x, a2y, a2z) +
+                        2.f * (a3z - ez * e3) / pr(a3x, a3y, a3z) + 1e-7f);
+        }
+    }
+    grad[n] += beta * g;
+}
+
+}  // namespace omb
+
+extern "C" int omb_tv_gradient_ex(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float beta,
+                                  float smooth, int32_t variant, float sigma, float C, const float *ref,
+                                  void *stream) {
+    using namespace omb;
+    if (variant == OMB_TV_PLAIN) return omb_tv_gradient(u, grad, nx, ny, nz, beta, smooth, stream);
+    if (!u || !grad) return set_error(OMB_ERR_INVALID, "u/grad pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    if (variant < OMB_TV_SATV || variant > OMB_TV_APLS) return set_error(OMB_ERR_INVALID, "unknown TV variant");
+    if (variant >= OMB_TV_ANAT1 && !ref)
+        return set_error(OMB_ERR_INVALID, "anatomical TV and APLS need the reference image (or tensor)");
+    if ((variant == OMB_TV_SATV || variant == OMB_TV_W1) && !(sigma != 0.f))
+        return set_error(OMB_ERR_INVALID, "SATV and weighted TV need a nonzero sigma (SATVPhi)");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    cudaStream_t st = (cudaStream_t)stream;
+#define OMB_TV_LAUNCH(V) k_tv_variant<V><<<grid, block, 0, st>>>(u, ref, grad, nx, ny, nz, beta, smooth, sigma, C)
+    switch (variant) {
+        case OMB_TV_SATV: OMB_TV_LAUNCH(OMB_TV_SATV); break;
+        case OMB_TV_W1: OMB_TV_LAUNCH(OMB_TV_W1); break;
+        case OMB_TV_ANAT1: OMB_TV_LAUNCH(OMB_TV_ANAT1); break;
+        case OMB_TV_ANAT2: OMB_TV_LAUNCH(OMB_TV_ANAT2); break;
+        default: OMB_TV_LAUNCH(OMB_TV_APLS); break;
+    }
+#undef OMB_TV_LAUNCH
+    OMB_LAUNCH_CHECK("TV variant gradient launch");
+    return OMB_OK;
+}

@@ -80,6 +80,12 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
     const bool graph = p->use_graph != 0;
     int st = OMB_OK;
     const int alg = p->algorithm;
+    if (alg == OMB_RECON_PDHG_TV || p->prior == OMB_PRIOR_TV) {
+        if (p->tv_variant < OMB_TV_PLAIN || p->tv_variant > OMB_TV_APLS)
+            return set_error(OMB_ERR_INVALID, "unknown TV variant");
+        if (p->tv_variant >= OMB_TV_ANAT1 && !p->tv_ref)
+            return set_error(OMB_ERR_INVALID, "anatomical TV and APLS need tv_ref");
+    }
     if (alg >= OMB_RECON_OSEM && alg <= OMB_RECON_MBSREM && alg != OMB_RECON_PDHG_TV) {
         const bool osl = alg == OMB_RECON_OSL_OSEM;
         const bool map = alg == OMB_RECON_BSREM || alg == OMB_RECON_ROSEM_MAP;  // MAP step once per iteration
@@ -172,7 +178,8 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                 return omb_ggmrf_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1], p->prior_g[2],
                                           p->ggmrf_weights, p->ggmrf[0], p->ggmrf[1], p->ggmrf[2], p->beta, stream);
             if (p->prior == OMB_PRIOR_TV)
-                return omb_tv_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->beta, p->tv_smoothing, stream);
+                return omb_tv_gradient_ex(x_out, du.f(), g.nx, g.ny, g.nz, p->beta, p->tv_smoothing, p->tv_variant,
+                                          p->tv_sigma, p->tv_c, p->tv_ref, stream);
             if (p->prior == OMB_PRIOR_MRP)
                 return omb_mrp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1], p->prior_g[2],
                                         epps, p->beta, p->mrp_no_norm, stream);
@@ -224,6 +231,7 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
     } else if (p->algorithm == OMB_RECON_PDHG_TV) {
         const int64_t m_all = omb_measurement_count(h, -1);  // one subset: all measurements
         if (m_all < 0) return -1;
+        const Grid g = handle_grid(h);
         DevBuf xn, u, pd, wm, wi, work;
         if ((st = alloc(xn, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(u, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
@@ -255,19 +263,32 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         p->tau_used = tau;
         OMB_CUDA_TRY(cudaMemcpyAsync(u.p, x_out, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
         OMB_CUDA_TRY(cudaMemsetAsync(pd.p, 0, (size_t)m_all * sizeof(float), s));
+        // one iteration; the plain TV gradient is fused into the primal step,
+        // the other TV gradients are added to A^T p before it
+        auto one = [&](float *xa, float *xb) {
+            if (p->tv_variant == OMB_TV_PLAIN)
+                return omb_pdhg_iteration(h, xa, xb, u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
+                                          p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
+            int e = omb_forward(h, -1, xa, wm.f(), stream);
+            if (e == OMB_OK) e = omb_pdhg_dual(pd.f(), wm.f(), y, m_all, p->sigma, stream);
+            if (e == OMB_OK) e = omb_backward(h, -1, pd.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC, stream);
+            if (e == OMB_OK)
+                e = omb_tv_gradient_ex(xa, wi.f(), g.nx, g.ny, g.nz, p->beta, p->tv_smoothing, p->tv_variant,
+                                       p->tv_sigma, p->tv_c, p->tv_ref, stream);
+            if (e == OMB_OK)
+                e = omb_pdhg_primal(h, xa, wi.f(), u.f(), xb, tau, p->theta, 0.f, p->tv_smoothing, p->positivity,
+                                    stream);
+            return e;
+        };
         // two iterations per repetition keep x_out / xn in place for graph replays
         auto two = [&]() {
-            int e = omb_pdhg_iteration(h, x_out, xn.f(), u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
-                                       p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
-            if (e == OMB_OK)
-                e = omb_pdhg_iteration(h, xn.f(), x_out, u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
-                                       p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
+            int e = one(x_out, xn.f());
+            if (e == OMB_OK) e = one(xn.f(), x_out);
             return e;
         };
         st = repeat(p->n_iter / 2, graph, s, two);
         if (st == OMB_OK && p->n_iter % 2) {
-            st = omb_pdhg_iteration(h, x_out, xn.f(), u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
-                                    p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
+            st = one(x_out, xn.f());
             if (st == OMB_OK)
                 OMB_CUDA_TRY(cudaMemcpyAsync(x_out, xn.p, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
         }

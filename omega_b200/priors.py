@@ -147,3 +147,91 @@ def weighted_mean_weights(options):
         w[np.isinf(w)] = float(getattr(options, 'weighted_center_weight', 2.))
         w = w / np.sum(w)
     return np.ascontiguousarray(w, dtype=np.float32)
+
+
+def tv_anatomical_tensor(ref, Nx, Ny, Nz, T):
+    """The weighting tensor of anatomical TV type 1 (prepass.py:509-533,
+    assembleS): per voxel B = I - (1 - gamma) nu nu^T, nu the unit vector of
+    the reference image's negated forward differences (ordered y, x, z as the
+    reference stacks them, zero past the last voxel), gamma = exp(-|d|^2 /
+    T^2), B = I where the differences vanish.  Returns the 9 channels
+    B[r, c] (channel 3 r + c), each an image with x fastest, concatenated:
+    float32, 9 Nx Ny Nz values, as options.s holds them (prepass.py:570-580)."""
+    a = np.asarray(ref, dtype=np.float32).reshape((Nx, Ny, Nz), order='F')
+    dy = np.zeros_like(a)
+    dx = np.zeros_like(a)
+    dz = np.zeros_like(a)
+    dy[:, :-1, :] = a[:, :-1, :] - a[:, 1:, :]
+    dx[:-1, :, :] = a[:-1, :, :] - a[1:, :, :]
+    dz[:, :, :-1] = a[:, :, :-1] - a[:, :, 1:]
+    d = [v.ravel(order='F') for v in (dy, dx, dz)]
+    norm = np.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+    gamma = np.exp(-(norm * norm) / np.float32(T * T))
+    nz = norm > 0
+    safe = np.where(nz, norm, np.float32(1.0))
+    nu = [np.where(nz, v / safe, np.float32(0.0)) for v in d]
+    one_minus = np.float32(1.0) - gamma
+    out = np.empty((9, norm.size), dtype=np.float32)
+    for r in range(3):
+        for c in range(3):
+            # float32 (1 - gamma) (nu_r nu_c), subtracted from the identity in FP64
+            prod = np.where(nz, one_minus * (nu[r] * nu[c]), np.float32(0.0))
+            out[3 * r + c] = float(r == c) - prod.astype(np.float64)
+    return out.ravel()
+
+
+def _reference_image(img, n, what, normalise):
+    r = np.asarray(img, dtype=np.float32)
+    if r.size != n:
+        raise ValueError(what + ' must have the size of the image (Nx * Ny * Nz values)')
+    r = r.ravel(order='F') if r.ndim > 1 else r.ravel()
+    if normalise:
+        # min-max normalised to [0, 1] in float32 (prepass.py:564-566)
+        r = r - np.min(r)
+        top = np.max(r)
+        if not top > 0:
+            raise ValueError(what + ' is constant')
+        r = r / top
+    return np.ascontiguousarray(r, dtype=np.float32)
+
+
+def tv_setup(options, apls=False):
+    """The TV gradient the reference builds for the TV options (ProjectorClass.h:
+    900-918 kernel choice, functions.hpp:1096-1113 scalars, libHeader.h:1108-
+    1124 and 1232-1245 option reads): returns (variant, sigma, C, smoothing,
+    reference array or None) with variant an omb_tv_variant.
+
+    Without TV_use_anatomical: TVtype 4 is SATV and 6 the weighted TV, both
+    with sigma = SATVPhi; other types are the plain TV.  With it, the
+    reference image TV_referenceImage is min-max normalised and TVtype 1
+    weights the differences with the tensor of tv_anatomical_tensor (options.T),
+    TVtype 2 adds C |grad ref|^2 (options.C), TVtype 5 is APLS with C =
+    options.eta; other types are the plain TV.  options.APLS (apls=True) is
+    APLS with the unnormalised APLS_ref_image, C = eta and the smoothing
+    APLSsmoothing.  Reference images are arrays of Nx * Ny * Nz values (the
+    reference's file loading and resizing are not part of this path)."""
+    Nx, Ny, Nz = (int(np.ravel(getattr(options, k))[0]) for k in ('Nx', 'Ny', 'Nz'))
+    n = Nx * Ny * Nz
+    smooth = float(getattr(options, 'TVsmoothing', 1e-2))
+    if apls:
+        ref = _reference_image(options.APLS_ref_image, n, 'APLS_ref_image', False)
+        return (_native.OMB_TV_APLS, 0.0, float(getattr(options, 'eta', 1e-5)),
+                float(getattr(options, 'APLSsmoothing', 1e-5)), ref)
+    tvtype = int(getattr(options, 'TVtype', 1))
+    if not getattr(options, 'TV_use_anatomical', False):
+        phi = float(getattr(options, 'SATVPhi', 1.0))
+        if tvtype == 4:
+            return _native.OMB_TV_SATV, phi, 0.0, smooth, None
+        if tvtype == 6:
+            return _native.OMB_TV_W1, phi, 0.0, smooth, None
+        return _native.OMB_TV_PLAIN, 0.0, 0.0, smooth, None
+    if tvtype not in (1, 2, 5):
+        return _native.OMB_TV_PLAIN, 0.0, 0.0, smooth, None
+    ref = _reference_image(options.TV_referenceImage, n, 'TV_referenceImage', True)
+    if tvtype == 1:
+        if getattr(options, 'T', None) is None:
+            raise ValueError('anatomical TV type 1 needs options.T')
+        return _native.OMB_TV_ANAT1, 0.0, 0.0, smooth, tv_anatomical_tensor(ref, Nx, Ny, Nz, float(options.T))
+    if tvtype == 2:
+        return _native.OMB_TV_ANAT2, 0.0, float(getattr(options, 'C', 1.0)), smooth, ref
+    return _native.OMB_TV_APLS, 0.0, float(getattr(options, 'eta', 1e-5)), smooth, ref

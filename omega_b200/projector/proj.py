@@ -184,6 +184,19 @@ class projectorClass:
     MAP = False
     beta = 0.
     TVsmoothing = 1e-4
+    # TV variants (proj.py:316-328, 410, 440-441 of the reference): TVtype 4
+    # SATV and 6 weighted TV with SATVPhi; TV_use_anatomical with the
+    # reference image TV_referenceImage, TVtype 1 (tensor, T), 2 (C) or 5
+    # (eta); the APLS prior with APLS_ref_image, eta and APLSsmoothing
+    TV_use_anatomical = False
+    TVtype = 1
+    C = 1.
+    SATVPhi = 1.
+    eta = 1e-5
+    APLSsmoothing = 1e-5
+    APLS = False
+    APLS_ref_image = np.empty(0, dtype=np.float32)
+    TV_referenceImage = np.empty(0, dtype=np.float32)
     tauCP = 0.
     sigmaCP = 1.
     thetaCP = 1.

@@ -284,11 +284,14 @@ def reconstructions_main(options):
     the compiled omegaMain entry) for the algorithms of this path:
     options.OSEM, options.ROSEM, options.RAMLA, options.MRAMLA and options.PKMA
     (PET; PKMA takes a prior when one is set), options.OSL_OSEM,
-    options.BSREM, options.ROSEM_MAP and options.MBSREM with options.RDP,
-    options.Quad or options.Huber (PET, MAP; Ndx/Ndy/Ndz neighbourhood weights
-    as the reference forms them; relaxation options.lambdaN, PKMA momentum
+    options.BSREM, options.ROSEM_MAP and options.MBSREM with one prior
+    (options.RDP, Quad, Huber, NLM, MRP, TV, APLS, GGMRF, hyperbolic or
+    weighted_mean; PET, MAP; Ndx/Ndy/Ndz neighbourhood weights as the
+    reference forms them; relaxation options.lambdaN, PKMA momentum
     options.alpha_PKMA, MRAMLA / MBSREM bound options.U) or options.PDHG with
-    options.TV, options.Niter iterations from options.x0, run natively by
+    options.TV (TV, SATV, weighted and anatomical TV by options.TVtype and
+    options.TV_use_anatomical, priors.tv_setup), options.Niter iterations
+    from options.x0, run natively by
     omb_reconstruct.  CT data are linearised as log(flat / SinM) first
     (prepass.py:22-36; flat = max(SinM) when options.flat <= 0), negative PET
     counts set to 0.  Returns (image of shape (Nx, Ny, Nz, 1) in Fortran
@@ -311,12 +314,13 @@ def reconstructions_main(options):
     ggmrf = bool(getattr(options, 'GGMRF', False))
     hyper = bool(getattr(options, 'hyperbolic', False))
     wmean = bool(getattr(options, 'weighted_mean', False))
+    apls = bool(getattr(options, 'APLS', False)) and not options.PDHG   # the APLS prior: TVKernel's APLS form
     n_priors = (int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp) + int(ggmrf) +
-                int(hyper) + int(wmean))
+                int(hyper) + int(wmean) + int(apls))
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
         raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM, '
-                                  'options.MRP, options.TV, options.GGMRF, options.hyperbolic or '
+                                  'options.MRP, options.TV, options.APLS, options.GGMRF, options.hyperbolic or '
                                   'options.weighted_mean')
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
@@ -326,13 +330,11 @@ def reconstructions_main(options):
         raise ValueError(method + ' is built for PET data')
     if options.PDHG and not options.TV:
         raise ValueError('PDHG is built with the TV prior (options.TV = True)')
-    if getattr(options, 'TV', False):
-        # the reference compiles other TV gradients for these settings
-        # (ProjectorClass.h:900-918: TVtype 4 SATV, 6 TVW1, anatomical TV)
-        if int(getattr(options, 'TVtype', 1)) not in (1, 2, 3):
-            raise ValueError('TV is built for TVtype 1, 2 and 3 (the plain TV gradient)')
-        if getattr(options, 'TV_use_anatomical', False):
-            raise ValueError('anatomical TV (TV_use_anatomical) is not built')
+    tv_set = None
+    if (prior and (tvp or apls)) or options.PDHG:
+        # the TV gradient variant of the TV / APLS options (ProjectorClass.h:900-918)
+        from . import priors
+        tv_set = priors.tv_setup(options, apls=apls)
     sin = np.asarray(options.SinM, dtype=np.float32)
     if options.CT and not options.usingLinearizedData:
         if options.flat <= 0:
@@ -389,7 +391,7 @@ def reconstructions_main(options):
         p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
                    (_native.OMB_PRIOR_NLM if nlm else
                     (_native.OMB_PRIOR_MRP if mrp else
-                     (_native.OMB_PRIOR_TV if tvp else
+                     (_native.OMB_PRIOR_TV if (tvp or apls) else
                       (_native.OMB_PRIOR_GGMRF if ggmrf else
                        (_native.OMB_PRIOR_HYPERBOLIC if hyper else
                         (_native.OMB_PRIOR_WMEAN if wmean else
@@ -465,6 +467,12 @@ def reconstructions_main(options):
     p.n_iter = int(options.Niter)
     p.beta = float(options.beta)
     p.tv_smoothing = float(options.TVsmoothing)
+    if tv_set is not None:
+        p.tv_variant, p.tv_sigma, p.tv_c, p.tv_smoothing, tv_ref = tv_set
+        if tv_ref is not None:
+            rt = torch.from_numpy(tv_ref).to(dev)
+            keep.append(rt)
+            p.tv_ref = ctypes.c_void_p(rt.data_ptr())
     p.tau = float(np.ravel(options.tauCP)[0]) if np.size(options.tauCP) else 0.0
     p.sigma = float(np.ravel(options.sigmaCP)[0])
     p.theta = float(np.ravel(options.thetaCP)[0])

@@ -231,3 +231,133 @@ def wmean_gradient(u, shape, m, weights, mean_type, beta, epps, no_norm=False):
     mean = {1: lambda a: a, 2: lambda a: 1.0 / a, 3: np.exp}[mean_type](acc)
     d = U - mean
     return (beta * (d if no_norm else d / (mean + epps))).ravel()
+
+
+# ---------------------------------------------------------------------------
+# TV gradient variants of TVKernel (auxKernels.cl:1733-1990): the image read
+# edge-clamped (the texture path), the anatomical reference S read as zero
+# beyond the image (its buffer path).  variant: 'satv' (TVtype 4), 'tvw1'
+# (TVtype 6), 'anat1' (anatomical TVtype 1, S = the 9 tensor channels),
+# 'anat2' (anatomical TVtype 2, S = the reference image, weight C), 'apls'
+# (anatomical TVtype 5 and APLS, S = the reference image, C = eta).
+# ---------------------------------------------------------------------------
+
+def _clamped(U, dx, dy, dz):
+    nx, ny, nz = U.shape
+    ix = np.clip(np.arange(nx) + dx, 0, nx - 1)
+    iy = np.clip(np.arange(ny) + dy, 0, ny - 1)
+    iz = np.clip(np.arange(nz) + dz, 0, nz - 1)
+    return U[ix][:, iy][:, :, iz]
+
+
+def _zero_beyond(S, dx, dy, dz):
+    """S shifted by +1 along one axis with zero past the last voxel."""
+    out = np.zeros_like(S)
+    if dx:
+        out[:-1] = S[1:]
+    elif dy:
+        out[:, :-1] = S[:, 1:]
+    else:
+        out[:, :, :-1] = S[:, :, 1:]
+    return out
+
+
+def tv_gradient_variant(u, shape, variant, smooth, beta, sigma=1.0, C=0.0, S=None):
+    nx, ny, nz = shape
+    U = np.asarray(u, dtype=np.float64).reshape(shape, order='F')
+    c = U
+    P = [_clamped(U, 1, 0, 0), _clamped(U, 0, 1, 0), _clamped(U, 0, 0, 1)]
+    M = [_clamped(U, -1, 0, 0), _clamped(U, 0, -1, 0), _clamped(U, 0, 0, -1)]
+    ui = (_clamped(U, -1, 1, 0), _clamped(U, -1, 0, 1))
+    uj = (_clamped(U, 1, -1, 0), _clamped(U, 0, -1, 1))
+    uk = (_clamped(U, 1, 0, -1), _clamped(U, 0, 1, -1))
+    u1 = (c - M[0], ui[0] - M[0], ui[1] - M[0])
+    u2 = (uj[0] - M[1], c - M[1], uj[1] - M[1])
+    u3 = (uk[0] - M[2], uk[1] - M[2], c - M[2])
+
+    def sq(v, w=(1.0, 1.0, 1.0)):
+        return np.sqrt(w[0] * v[0] ** 2 + w[1] * v[1] ** 2 + w[2] * v[2] ** 2 + smooth)
+
+    if variant == 'satv':
+        g = 0.0
+        for a in range(3):
+            for nb in (P[a], M[a]):
+                d = c - nb
+                ua = d / (np.abs(d) + smooth)
+                g = g + ua - ua / (np.abs(d) / sigma + 1.0)
+        return (beta * g).ravel(order='F')
+    if variant == 'tvw1':
+        u4 = (P[0] - c, P[1] - c, P[2] - c)
+
+        def wts(v):
+            return tuple(np.exp(-(x / sigma) ** 2) for x in v)
+        w4, w1, w2, w3 = wts(u4), wts(u1), wts(u2), wts(u3)
+        g = (-(w4[0] * u4[0] + w4[1] * u4[1] + w4[2] * u4[2]) / sq(u4, w4) + w1[0] * (c - M[0]) / sq(u1, w1)
+             + w2[1] * (c - M[1]) / sq(u2, w2) + w3[1] * (c - M[2]) / sq(u3, w3))
+        return (beta * g).ravel(order='F')
+    if variant == 'anat1':
+        s = [np.asarray(S, dtype=np.float64)[k * nx * ny * nz:(k + 1) * nx * ny * nz].reshape(shape, order='F')
+             for k in range(9)]
+
+        def pv(v):
+            return np.sqrt(v[0] ** 2 * s[0] + v[1] ** 2 * s[4] + v[2] ** 2 * s[8] + (s[1] + s[3]) * v[0] * v[1]
+                           + (s[2] + s[6]) * v[0] * v[2] + (s[5] + s[7]) * v[1] * v[2] + smooth)
+        val = (P[0] - c, P[1] - c, P[2] - c)
+        dx = s[0] * 2 * (c - M[0]) + (s[3] + s[1]) * u1[1] + (s[2] + s[6]) * u1[2]
+        dy = s[4] * 2 * (c - M[1]) + (s[5] + s[7]) * u2[2] + (s[3] + s[1]) * u2[0]
+        dz = s[8] * 2 * (c - M[2]) + (s[6] + s[2]) * u3[0] + (s[5] + s[7]) * u3[1]
+        d = ((s[1] + s[2] + s[3] + s[6]) * val[0] + (s[1] + s[3] + s[5] + s[7]) * val[1]
+             + (s[2] + s[5] + s[6] + s[7]) * val[2] + 2 * (s[0] * val[0] + s[4] * val[1] + s[8] * val[2]))
+        g = 0.5 * (d / pv(val) + dx / pv(u1) + dy / pv(u2) + dz / pv(u3))
+        return (beta * g).ravel(order='F')
+    R = np.asarray(S, dtype=np.float64).reshape(shape, order='F')
+    Rp = (_zero_beyond(R, 1, 0, 0), _zero_beyond(R, 0, 1, 0), _zero_beyond(R, 0, 0, 1))
+    apu = (P[0] - c, P[1] - c, P[2] - c)
+    if variant == 'anat2':
+        aS = (Rp[0] - R, Rp[1] - R, Rp[2] - R)
+        p0 = np.sqrt(apu[0] ** 2 + apu[1] ** 2 + apu[2] ** 2 + C * (aS[0] ** 2 + aS[1] ** 2 + aS[2] ** 2) + smooth)
+        g = ((3 * c - P[0] - P[1] - P[2]) / p0 + (c - M[0]) / sq(u1) + (c - M[1]) / sq(u2) + (c - M[2]) / sq(u3)
+             + 1e-7)
+        return (beta * g).ravel(order='F')
+    if variant == 'apls':
+        e = (Rp[0] - R, Rp[1] - R, Rp[2] - R)
+        en = np.sqrt(e[0] ** 2 + e[1] ** 2 + e[2] ** 2 + C * C)
+        e = (e[0] / en, e[1] / en, e[2] / en)
+        apuR = Rp[0] * apu[0] + Rp[1] * apu[1] + Rp[2] * apu[2]
+        p0 = np.sqrt(apu[0] ** 2 + apu[1] ** 2 + apu[2] ** 2 - apuR ** 2 + smooth)
+
+        def pr(v):
+            r = Rp[0] * v[0] + Rp[1] * v[1] + Rp[2] * v[2]
+            return np.sqrt(v[0] ** 2 + v[1] ** 2 + v[2] ** 2 + r * r + smooth)
+
+        def edot(v):
+            return e[0] * v[0] + e[1] * v[1] + e[2] * v[2]
+        g = 0.5 * ((6 * c - 2 * (P[0] + P[1] + P[2]) + 2 * edot((c - P[0], c - P[1], c - P[2])) * (e[0] + e[1] + e[2]))
+                   / p0 + 2 * (u1[0] - e[0] * edot(u1)) / pr(u1) + 2 * (u2[1] - e[1] * edot(u2)) / pr(u2)
+                   + 2 * (u3[2] - e[2] * edot(u3)) / pr(u3) + 1e-7)
+        return (beta * g).ravel(order='F')
+    raise ValueError(variant)
+
+
+def tv_anatomical_tensor(ref, shape, T):
+    """The 9 channels of the anatomical TV type-1 weighting (prepass.py:496-
+    533, assembleS): per voxel B = I - (1 - gamma) nu nu^T with nu the unit
+    forward-difference gradient of the reference image and gamma =
+    exp(-|grad|^2 / T^2); channels k = 3 row + col, each an image (x fastest)."""
+    nx, ny, nz = shape
+    a = np.asarray(ref, dtype=np.float32).reshape(shape, order='F')
+    f = np.concatenate((-np.diff(a, axis=1), np.zeros((nx, 1, nz), np.float32)), axis=1).ravel('F')
+    g = np.concatenate((-np.diff(a, axis=0), np.zeros((1, ny, nz), np.float32)), axis=0).ravel('F')
+    h = np.concatenate((-np.diff(a, axis=2), np.zeros((nx, ny, 1), np.float32)), axis=2).ravel('F')
+    gv = np.vstack((f, g, h))
+    gn = np.linalg.norm(gv, axis=0)
+    gamma = np.exp(-gn ** 2 / (T ** 2))
+    out = np.empty((9, gn.size), dtype=np.float32)
+    eye = np.eye(3)
+    nu = np.where(gn > 0, gv / np.where(gn > 0, gn, 1.0), 0.0)
+    for r in range(3):
+        for col in range(3):
+            # float32 (1 - gamma) times the float32 outer product, then the
+            # FP64 subtraction from the identity, stored as float32
+            out[3 * r + col] = (eye[r, col] - np.where(gn > 0, (np.float32(1.0) - gamma) * (nu[r] * nu[col]), 0.0))
+    return out.ravel()

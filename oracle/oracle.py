@@ -682,9 +682,10 @@ def power_method(geom: Geometry, n_iter, seed=0, x0=None):
 
 
 def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1.0, eps=1e-5,
-            positivity=True):
+            positivity=True, tv_grad=None):
     """PDHG with a TV-gradient term, one subset (computeForwardProject.h:227-316,
-    algorithms.h:329-420, auxKernels.cl:2034-2062), in FP64."""
+    algorithms.h:329-420, auxKernels.cl:2034-2062), in FP64.  tv_grad(x), when
+    given, replaces the plain TV term beta * dTV(x) (the other TVKernel forms)."""
     shape = (geom.nx, geom.ny, geom.nz)
     x = np.asarray(x0, dtype=np.float64).copy()
     u = x.copy()
@@ -693,7 +694,7 @@ def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1
     for _ in range(n_iter):
         res = bdd_forward(geom, x, -1) - yy
         p = (p + sigma * res) / (1.0 + sigma)
-        rhs = bdd_backward(geom, p, -1) + tv_gradient(x, shape, smooth, beta)
+        rhs = bdd_backward(geom, p, -1) + (tv_gradient(x, shape, smooth, beta) if tv_grad is None else tv_grad(x))
         u_prev = u.copy()
         u = u - tau * rhs
         if positivity:

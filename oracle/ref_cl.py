@@ -56,7 +56,10 @@ def _lib(variant, precision):
                                                                                         _P]
         if hasattr(L, "refcl_tv_gradient"):
             L.refcl_tv_gradient.argtypes = [_I, _I, _I, _P, _D, _D, _D, _P]
+        if hasattr(L, "refcl_pdhg_update"):
             L.refcl_pdhg_update.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D, _D, _I]
+        if hasattr(L, "refcl_tv_gradient_ex"):
+            L.refcl_tv_gradient_ex.argtypes = [_I, _I, _I, _P, _D, _D, _D, _D, _P, _P]
         _libs[key] = L
     return _libs[key]
 
@@ -259,3 +262,21 @@ def pdhg_update(im, rhs, u, shape, tau, theta=1.0, eps=1e-5, positivity=True, pr
                                              _scalar(theta, exact_inputs), _scalar(tau, exact_inputs),
                                              int(positivity))
     return a, b
+
+
+_TV_LIB = {"satv": "aux_satv", "tvw1": "aux_tvw1", "anat1": "aux_anat1", "anat2": "aux_anat2", "apls": "aux_anat3"}
+
+
+def tv_gradient_variant(u, shape, variant, smooth, beta, sigma=1.0, C=0.0, S=None, precision="d",
+                        exact_inputs=False):
+    """TVKernel built with the variant's macro (-DSATV, -DTVW1,
+    -DANATOMICAL1/2/3): grad += beta * dTV(u); S the reference image (the 9
+    tensor channels for 'anat1')."""
+    nx, ny, nz = shape
+    uu = np.ascontiguousarray(u, dtype=np.float64).ravel()
+    g = np.zeros(uu.size)
+    ss = None if S is None else np.ascontiguousarray(S, dtype=np.float64).ravel()
+    _lib(_TV_LIB[variant], precision).refcl_tv_gradient_ex(
+        nx, ny, nz, _dp(uu), _scalar(sigma, exact_inputs), _scalar(smooth, exact_inputs), _scalar(beta, exact_inputs),
+        _scalar(C, exact_inputs), _dp(ss), _dp(g))
+    return g

@@ -312,6 +312,7 @@ REFCL_EXPORT int refcl_interp_ct_bp(int n_rows, int n_cols, double pitch_x, doub
 #endif
 
 #if defined(REFCL_AUX)
+#if !defined(ANATOMICAL1) && !defined(ANATOMICAL2) && !defined(ANATOMICAL3)
 /* TVKernel with texture reads (nearest point, unnormalized, clamp to edge):
  * grad += beta * dTV(u) with smoothing `epps` (the reference's TVsmoothing). */
 REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, double sigma, double epps, double beta,
@@ -325,6 +326,46 @@ REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, doub
             for (int i = 0; i < nx; ++i) {
                 set_item((unsigned)i, (unsigned)j, (unsigned)k);
                 TVKernel(g.data(), &tex, nx, ny, nz, nx, ny, nz, (omb_real)sigma, (omb_real)epps, (omb_real)beta);
+            }
+    from_real(g, grad);
+    return 0;
+}
+#endif
+
+/* TVKernel in the variant the build selected (-DSATV, -DTVW1,
+ * -DANATOMICAL1/2/3): S is the reference image (or, ANATOMICAL1, the nine
+ * tensor channels), C the anatomical weight (options.C, or eta for
+ * ANATOMICAL3). */
+REFCL_EXPORT int refcl_tv_gradient_ex(int nx, int ny, int nz, const double *u, double sigma, double epps, double beta,
+                                      double C, const double *S, double *grad) {
+    const size_t N = (size_t)nx * ny * nz;
+    rvec uu = to_real(u, N), g = to_real(grad, N);
+#if defined(ANATOMICAL1) || defined(ANATOMICAL2) || defined(ANATOMICAL3)
+    rvec ss = to_real(S, N * (
+#if defined(ANATOMICAL1)
+                                  9
+#else
+                                  1
+#endif
+                                  ));
+#else
+    (void)S;
+    (void)C;
+#endif
+    const omb_tex tex = make_tex(uu, nx, ny, nz, 0, 0, 0);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                TVKernel(g.data(), &tex, nx, ny, nz, nx, ny, nz, (omb_real)sigma, (omb_real)epps, (omb_real)beta
+#if defined(ANATOMICAL2) || defined(ANATOMICAL3)
+                         , (omb_real)C
+#endif
+#if defined(ANATOMICAL1) || defined(ANATOMICAL2) || defined(ANATOMICAL3)
+                         , ss.data()
+#endif
+                );
             }
     from_real(g, grad);
     return 0;

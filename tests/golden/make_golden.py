@@ -5,6 +5,7 @@ Run where the OMEGA sources are, with $OMEGA_REFERENCE naming their root:
     OMEGA_REFERENCE=<checkout> python tests/golden/make_golden.py   # everything
     python tests/golden/make_golden.py volumes    # the type-3 tables only
     python tests/golden/make_golden.py nlm        # the NLM patch weights only
+    python tests/golden/make_golden.py tv         # the anatomical TV preparation only
     python tests/golden/make_golden.py geom NAME  # one geometry fixture
 
 For every option set in configs.py it imports the reference's own Python
@@ -206,6 +207,46 @@ def nlm_fixture():
     print("nlm_gauss", {k: v.shape for k, v in out.items()})
 
 
+def tv_fixture():
+    """The reference's anatomical TV preparation (prepass.py TVPrepass): the
+    min-max normalised reference image (TVtype 2) and the 9-channel weighting
+    tensor of TVtype 1 (assembleS), for a seeded 7 x 6 x 5 reference image
+    with a constant block (zero gradients), stored in tv_anat.npz.  Its
+    image resize is never reached (the image has the reconstruction's size),
+    so a stand-in skimage module satisfies the import."""
+    import importlib.util
+    import types
+    for name in ("skimage", "skimage.transform"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.modules["skimage.transform"].resize = None
+    spec = importlib.util.spec_from_file_location(
+        "omega_prepass", os.path.join(REF, "source", "Python", "omegatomo", "reconstruction", "prepass.py"))
+    prepass = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(prepass)
+
+    class Opt:
+        pass
+    rng = np.random.default_rng(77)
+    shape = (7, 6, 5)
+    img = rng.uniform(2.0, 9.0, shape).astype(np.float32)
+    img[1:4, 1:4, 1:3] = 5.0
+    img = np.asfortranarray(img)
+    out = {"ref": img}
+    for tvtype, T in ((1, 0.3), (2, 0.3), (1, 2.0)):
+        o = Opt()
+        o.Nx, o.Ny, o.Nz = (np.array([v], dtype=np.uint32) for v in shape)
+        o.TV_use_anatomical = True
+        o.TVtype = tvtype
+        o.T = T
+        o.TV_referenceImage = img.copy(order="F")
+        prepass.TVPrepass(o)
+        if tvtype == 1:
+            out[f"s_T{T}"] = np.asarray(o.s, dtype=np.float32)
+        out["ref_norm"] = np.asarray(o.TV_referenceImage, dtype=np.float32)
+    np.savez_compressed(os.path.join(HERE, "tv_anat.npz"), **out)
+    print("tv_anat", {k: v.shape for k, v in out.items()})
+
+
 # type-3 table cases: tube radius, voxel radius (before scaling), voxel size (dx, dy, dz)
 VOLUME_CASES = {"a": (1.0, 1.0, (2.0, 2.0, 2.5)), "b": (2.5, 1.0, (1.5, 1.5, 1.5))}
 
@@ -216,6 +257,9 @@ def main():
         return
     if sys.argv[1:] == ["nlm"]:
         nlm_fixture()
+        return
+    if sys.argv[1:] == ["tv"]:
+        tv_fixture()
         return
     if sys.argv[1:] == ["priorw"]:
         prior_weight_fixture(reference_projector())
@@ -229,6 +273,7 @@ def main():
     proj = reference_projector()
     volume_fixture()
     nlm_fixture()
+    tv_fixture()
     psf_fixture(proj)
     prior_weight_fixture(proj)
     allc = dict(CONFIGS)

@@ -268,18 +268,189 @@ def test_weighted_mean_single_slice_needs_flat_window():
     assert "single slice" in _native.lib().omb_last_error().decode()
 
 
-@pytest.mark.parametrize("attrs", [dict(TVtype=4), dict(TVtype=6), dict(TV_use_anatomical=True)])
-def test_tv_variants_not_built_are_rejected(attrs):
+def _tv_golden():
+    import os
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tv_anat.npz"))
+
+
+class _TVOpts:
+    Nx, Ny, Nz = 7, 6, 5
+    TVsmoothing = 1e-3
+    SATVPhi = 0.4
+    C = 0.7
+    eta = 0.02
+    APLSsmoothing = 1e-4
+    TV_use_anatomical = False
+    TVtype = 1
+
+
+def test_tv_setup_matches_reference_prepass():
+    """The anatomical TV preparation equals the reference's own TVPrepass
+    output bit for bit (tests/golden/tv_anat.npz): the min-max normalised
+    reference image and the TVtype-1 tensor for two T; the other TV settings
+    pick the reference's kernel form (ProjectorClass.h:900-918) and scalars
+    (functions.hpp:1096-1113)."""
+    from omega_b200 import _native, priors
+    f = _tv_golden()
+    o = _TVOpts()
+    assert priors.tv_setup(o)[0] == _native.OMB_TV_PLAIN
+    o.TVtype = 4
+    assert priors.tv_setup(o) == (_native.OMB_TV_SATV, pytest.approx(0.4), 0.0, pytest.approx(1e-3), None)
+    o.TVtype = 6
+    assert priors.tv_setup(o)[:2] == (_native.OMB_TV_W1, pytest.approx(0.4))
+    o.TV_use_anatomical = True
+    o.TV_referenceImage = f["ref"]
+    assert priors.tv_setup(o)[0] == _native.OMB_TV_PLAIN   # TVtype 6 with a reference: the plain kernel
+    for T in (0.3, 2.0):
+        o.TVtype, o.T = 1, T
+        v, _, _, _, s = priors.tv_setup(o)
+        assert v == _native.OMB_TV_ANAT1 and np.array_equal(s, f["s_T" + str(T)])
+    o.TVtype = 2
+    v, _, c, _, r = priors.tv_setup(o)
+    assert v == _native.OMB_TV_ANAT2 and c == pytest.approx(0.7) and np.array_equal(r, f["ref_norm"])
+    o.TVtype = 5
+    v, _, c, sm, r = priors.tv_setup(o)
+    assert v == _native.OMB_TV_APLS and c == pytest.approx(0.02) and sm == pytest.approx(1e-3)
+    assert np.array_equal(r, f["ref_norm"])
+    # the APLS prior: the raw reference image, eta and APLSsmoothing
+    o.APLS_ref_image = f["ref"]
+    v, _, c, sm, r = priors.tv_setup(o, apls=True)
+    assert v == _native.OMB_TV_APLS and sm == pytest.approx(1e-4)
+    assert np.array_equal(r, f["ref"].ravel(order="F"))
+
+
+def test_tv_setup_rejects_bad_reference_images():
+    from omega_b200 import priors
+    o = _TVOpts()
+    o.TV_use_anatomical, o.TVtype = True, 2
+    o.TV_referenceImage = np.ones(10, np.float32)
+    with pytest.raises(ValueError, match="size of the image"):
+        priors.tv_setup(o)
+    o.TV_referenceImage = np.ones(7 * 6 * 5, np.float32)
+    with pytest.raises(ValueError, match="constant"):
+        priors.tv_setup(o)
+    o.TV_referenceImage = _tv_golden()["ref"]
+    o.TVtype = 1
+    with pytest.raises(ValueError, match="options.T"):
+        priors.tv_setup(o)
+
+
+def test_tv_variant_entry_validates_arguments():
+    from omega_b200 import _native
+    L = _native.lib()
+    p = ctypes.c_void_p(16)
+    f = ctypes.c_float
+    # anatomical variants need the reference; SATV a nonzero sigma; unknown variants are refused
+    assert L.omb_tv_gradient_ex(p, p, 8, 8, 4, f(1), f(1e-3), _native.OMB_TV_ANAT2, f(1), f(1), None, None) != 0
+    assert "reference" in L.omb_last_error().decode()
+    assert L.omb_tv_gradient_ex(p, p, 8, 8, 4, f(1), f(1e-3), _native.OMB_TV_SATV, f(0), f(0), None, None) != 0
+    assert "sigma" in L.omb_last_error().decode()
+    assert L.omb_tv_gradient_ex(p, p, 8, 8, 4, f(1), f(1e-3), 9, f(1), f(0), None, None) != 0
+
+
+_TV_VARIANTS = {"satv": "OMB_TV_SATV", "tvw1": "OMB_TV_W1", "anat1": "OMB_TV_ANAT1", "anat2": "OMB_TV_ANAT2",
+                "apls": "OMB_TV_APLS"}
+
+
+def _tv_variant_inputs(variant, shape, seed):
+    rng = np.random.default_rng(seed)
+    n = int(np.prod(shape))
+    u = rng.uniform(0.2, 1.0, n).astype(np.float32)
+    ref = rng.uniform(0.0, 1.0, n).astype(np.float32)
+    if variant == "anat1":
+        from omega_b200 import priors
+        S = priors.tv_anatomical_tensor(ref, *shape, 0.5)
+    elif variant == "apls":
+        S = 0.5 * ref     # keeps |d|^2 - (r . d)^2 + smooth positive
+    elif variant == "anat2":
+        S = ref
+    else:
+        S = None
+    sigma, C = 0.3, (0.4 if variant == "anat2" else 0.05)
+    return u, S, sigma, C
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", list(_TV_VARIANTS))
+def test_tv_variant_kernels_match_oracle(cuda, variant):
+    """omb_tv_gradient_ex against the FP64 restatement of the TVKernel forms
+    (pinned to the reference's kernel by test_refcl_pin), accumulating into
+    an existing gradient."""
+    import torch
+    from omega_b200 import _native
+    from omega_b200.reconstruction import _stream
+    u, S, sigma, C = _tv_variant_inputs(variant, SHAPE, 61)
+    n = u.size
+    U = torch.tensor(u, device=cuda)
+    R = torch.tensor(S, device=cuda) if S is not None else None
+    out = torch.full((n,), 0.5, device=cuda)
+    _native.call("omb_tv_gradient_ex", ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(out.data_ptr()), *SHAPE,
+                 0.8, 1e-3, getattr(_native, _TV_VARIANTS[variant]), sigma, C,
+                 ctypes.c_void_p(R.data_ptr() if R is not None else 0), _stream(cuda))
+    want = io.tv_gradient_variant(u.astype(np.float64), SHAPE, variant, 1e-3, 0.8, sigma=sigma, C=C,
+                                  S=None if S is None else S.astype(np.float64))
+    assert orc.rel_l2(out.cpu().numpy() - 0.5, want) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["satv", "tvw1", "anat1", "anat2", "anat5", "apls_prior"])
+def test_builtin_osl_osem_tv_variants(cuda, case):
+    """One-step-late OSEM with each TV setting through the built-in entry,
+    against the FP64 OSEM with the restated gradient."""
     from conftest import make_options
+    from omega_b200 import priors
     from omega_b200 import reconstruction as rec
     o = make_options("pet_mini")
-    o.SinM = np.ones(int(o.Ndist) * int(o.Nang) * int(o.NSinos), np.float32)
+    g = orc.Geometry(o)
+    shape = (g.nx, g.ny, g.nz)
+    rng = np.random.default_rng(71)
+    full = make_options("pet_mini")
+    full.subsets, full.subsetType = 1, 8
+    full.addProjector()
+    truth = rng.uniform(0.5, 2.0, g.n_img)
+    y = rng.poisson(orc.forward(orc.Geometry(full), truth, 0) * 200).astype(np.float32) / 200
+    o.SinM = y.copy()
     o.OSL_OSEM = True
-    o.TV = True
-    for k, v in attrs.items():
-        setattr(o, k, v)
-    with pytest.raises(ValueError, match="TV"):
-        rec.reconstructions_main(o)
+    o.TVsmoothing = 1e-2
+    o.beta = 0.002
+    o.Niter = 2
+    ref_img = (truth + rng.uniform(0, 0.3, g.n_img)).astype(np.float32)
+    if case == "apls_prior":
+        o.APLS = True
+        o.APLS_ref_image = 0.02 * ref_img
+        o.APLSsmoothing = 1e-2
+        o.eta = 0.1
+    else:
+        o.TV = True
+        o.SATVPhi = 0.5
+        if case in ("satv", "tvw1"):
+            o.TVtype = 4 if case == "satv" else 6
+        else:
+            o.TV_use_anatomical = True
+            o.TV_referenceImage = ref_img
+            if case == "anat5":
+                # APLS reads the raw (normalised) reference values into
+                # sqrt(|d|^2 - (r . d)^2 + smooth), as TVKernel does: values
+                # up to 0.3 keep it real; the maximum sits in voxel 0, which
+                # is no voxel's forward neighbour
+                ref5 = 0.3 * rng.uniform(0.0, 1.0, g.n_img).astype(np.float32)
+                ref5[0] = 1.0
+                o.TV_referenceImage = ref5
+            o.TVtype = {"anat1": 1, "anat2": 2, "anat5": 5}[case]
+            o.T, o.C, o.eta = 0.5, 0.3, 0.05
+    variant, sigma, C, smooth, S = priors.tv_setup(o, apls=case == "apls_prior")
+    name = {1: "satv", 2: "tvw1", 3: "anat1", 4: "anat2", 5: "apls"}[int(variant)]
+    out, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    S64 = None if S is None else S.astype(np.float64)
+
+    def grad(v):
+        return io.tv_gradient_variant(v, shape, name, smooth, 0.002, sigma=sigma, C=C, S=S64)
+    want = orc.osem(g, ys, np.ones(g.n_img), 2, prior_grad=grad)
+    x = out.ravel(order='F')
+    assert np.all(np.isfinite(x))
+    assert orc.rel_l2(x, want) < 5e-5, orc.rel_l2(x, want)
 
 
 @pytest.mark.gpu

@@ -202,3 +202,25 @@ def test_pdhg_iteration_pinned():
         rhs = R.bdd_backward(p, -1) + ref_cl.tv_gradient(x, shape, smooth, beta, exact_inputs=True)
         x, u = ref_cl.pdhg_update(x, rhs, u, shape, tau, 1.0, 1e-5, exact_inputs=True)
     assert orc.rel_l2(ours, x) < PIN
+
+
+@pytest.mark.parametrize("variant", ["satv", "tvw1", "anat1", "anat2", "apls"])
+def test_tv_variants_pinned(variant):
+    """The TV gradients of the other TV settings (TVtype 4 and 6, anatomical
+    TVtype 1, 2 and 5, APLS) against TVKernel compiled with the variant's
+    macro."""
+    from oracle import image_oracle as io
+    shape = (15, 12, 9)
+    rng = np.random.default_rng(51)
+    n = int(np.prod(shape))
+    u = rng.uniform(0.2, 1.0, n)
+    ref = rng.uniform(0.0, 1.0, n)
+    # APLS reads the reference image's raw values into sqrt(|d|^2 - (r . d)^2
+    # + smooth): reference values below 1 keep it real (above, the reference
+    # kernel itself returns NaN)
+    S = io.tv_anatomical_tensor(ref, shape, 0.5).astype(np.float64) if variant == "anat1" else \
+        (ref if variant == "anat2" else (0.5 * ref if variant == "apls" else None))
+    kw = dict(sigma=0.3, C=0.4 if variant == "anat2" else 0.05, S=S)
+    ours = io.tv_gradient_variant(u, shape, variant, 1e-3, 0.8, **kw)
+    theirs = ref_cl.tv_gradient_variant(u, shape, variant, 1e-3, 0.8, exact_inputs=True, **kw)
+    assert orc.rel_l2(ours, theirs) < 1e-12
