@@ -342,6 +342,19 @@ def check(fn_name, status):
         raise NativeError(fn_name, status, msg)
 
 
+def check_device(what):
+    """Reads and clears the device error word of the staged type-5 kernels
+    (synchronises the device).  A nonzero word means a bounded wait on a
+    staged copy ran out: the results of the calls since the last read are
+    void, and this raises NativeError."""
+    v = lib().omb_take_device_error()
+    if v < 0:
+        check("omb_take_device_error", v)
+    if v:
+        raise NativeError(what, v, "a staged kernel's bounded wait ran out; the results since the last check "
+                                   "are void")
+
+
 def call(fn_name, *args):
     """Calls an int-returning entry point and raises NativeError on failure."""
     st = getattr(lib(), fn_name)(*args)

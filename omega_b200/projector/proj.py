@@ -13,7 +13,8 @@ Differences from the reference surface:
  * every call is stream-ordered on ``torch.cuda.current_stream()``; nothing
    synchronises (the reference synchronises after each call,
    projfunctions.py:435-436) -- ``.cpu()`` or ``torch.cuda.synchronize()`` is
-   the caller's sync point;
+   the caller's sync point (projector type 5 synchronises after each call to
+   read the staged kernels' error word unless ``checkDeviceErrors = False``);
  * ``use_64bit_atomics = True`` selects the bit-deterministic int64
    fixed-point backprojection on CUDA (the reference only offers it on
    OpenCL and forces it off on CUDA, init.py:251-254);
@@ -245,6 +246,11 @@ class projectorClass:
     use_64bit_atomics = False
     use_32bit_atomics = False
     bddRayBackprojection = False
+    # type 5: read the staged kernels' device error word after every
+    # projection (a device synchronisation) and raise when a bounded wait ran
+    # out; False leaves the calls asynchronous and the check to the caller
+    # (omega_b200._native.check_device)
+    checkDeviceErrors = True
     global_factor = 1.
     epps = 1e-5
     # Subsets / reconstruction
@@ -915,7 +921,12 @@ class projectorClass:
         stream = torch.cuda.current_stream(f.device).cuda_stream
         _native.call("omb_forward", self._handle, int(subset), ctypes.c_void_p(f.data_ptr()),
                      ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(stream))
+        self._check_staged("omb_forward")
         return y
+
+    def _check_staged(self, what):
+        if int(np.ravel(self.projector_type)[0]) == 5 and self.checkDeviceErrors:
+            _native.check_device(what)
 
     def backwardProject(self, y, subset=-1, sens=False):
         """f = A_subset^T y (projfunctions.py:735).  With ``sens=True`` also
@@ -936,6 +947,7 @@ class projectorClass:
         _native.call("omb_backward", self._handle, int(subset), ctypes.c_void_p(y.data_ptr()),
                      ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(s.data_ptr() if s is not None else 0),
                      int(mode), ctypes.c_void_p(stream))
+        self._check_staged("omb_backward")
         if self.use_psf:
             f = self._psf(f)
             s = self._psf(s) if sens else None

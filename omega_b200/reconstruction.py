@@ -88,6 +88,7 @@ class PDHG:
             for _ in range(n_iter):
                 self._step(self.x, self.x_next)
                 self.x, self.x_next = self.x_next, self.x
+            self.o._check_staged("PDHG.iterate")
             return self.x
         if self.graph is None:
             # one graph holds two iterations (x -> x_next -> x), so the
@@ -108,6 +109,7 @@ class PDHG:
         if n_iter % 2:
             self._step(self.x, self.x_next)
             self.x, self.x_next = self.x_next, self.x
+        self.o._check_staged("PDHG.iterate")
         return self.x
 
 
@@ -480,6 +482,7 @@ def reconstructions_main(options):
     p.positivity = 1 if options.enforcePositivity else 0
     p.use_graph = 1 if getattr(options, 'use_graph', True) else 0
     _native.call("omb_reconstruct", options._handle, ctypes.byref(p), _ptr(y), _ptr(x0), _ptr(x), _stream(dev))
+    options._check_staged("omb_reconstruct")
     options.tau_used = p.tau_used
     out = x.cpu().numpy().reshape((int(np.ravel(options.Nx)[0]), int(np.ravel(options.Ny)[0]),
                                    int(np.ravel(options.Nz)[0]), 1), order='F')

@@ -352,10 +352,13 @@ _TV_VARIANTS = {"satv": "OMB_TV_SATV", "tvw1": "OMB_TV_W1", "anat1": "OMB_TV_ANA
                 "apls": "OMB_TV_APLS"}
 
 
-def _tv_variant_inputs(variant, shape, seed):
+def _tv_variant_inputs(variant, shape, seed, wide=False):
     rng = np.random.default_rng(seed)
     n = int(np.prod(shape))
     u = rng.uniform(0.2, 1.0, n).astype(np.float32)
+    if wide:
+        # an iterate's range: zeros beside values up to 25
+        u = (25.0 * u * (rng.uniform(0, 1, n) > 0.2)).astype(np.float32)
     ref = rng.uniform(0.0, 1.0, n).astype(np.float32)
     if variant == "anat1":
         from omega_b200 import priors
@@ -371,15 +374,16 @@ def _tv_variant_inputs(variant, shape, seed):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("wide", [False, True])
 @pytest.mark.parametrize("variant", list(_TV_VARIANTS))
-def test_tv_variant_kernels_match_oracle(cuda, variant):
+def test_tv_variant_kernels_match_oracle(cuda, variant, wide):
     """omb_tv_gradient_ex against the FP64 restatement of the TVKernel forms
     (pinned to the reference's kernel by test_refcl_pin), accumulating into
     an existing gradient."""
     import torch
     from omega_b200 import _native
     from omega_b200.reconstruction import _stream
-    u, S, sigma, C = _tv_variant_inputs(variant, SHAPE, 61)
+    u, S, sigma, C = _tv_variant_inputs(variant, SHAPE, 61, wide)
     n = u.size
     U = torch.tensor(u, device=cuda)
     R = torch.tensor(S, device=cuda) if S is not None else None
@@ -389,7 +393,8 @@ def test_tv_variant_kernels_match_oracle(cuda, variant):
                  ctypes.c_void_p(R.data_ptr() if R is not None else 0), _stream(cuda))
     want = io.tv_gradient_variant(u.astype(np.float64), SHAPE, variant, 1e-3, 0.8, sigma=sigma, C=C,
                                   S=None if S is None else S.astype(np.float64))
-    assert orc.rel_l2(out.cpu().numpy() - 0.5, want) < 1e-5
+    got = out.cpu().numpy() - 0.5
+    assert orc.rel_l2(got, want) < 1e-5, (orc.rel_l2(got, want), np.abs(got - want).max(), np.abs(want).max())
 
 
 @pytest.mark.gpu
@@ -412,7 +417,12 @@ def test_builtin_osl_osem_tv_variants(cuda, case):
     o.SinM = y.copy()
     o.OSL_OSEM = True
     o.TVsmoothing = 1e-2
-    o.beta = 0.002
+    # small enough that sens + beta dTV stays away from 0 in every reached
+    # voxel (at 2e-3 FP32 rounding alone moves the result by 5e-5); the
+    # weighted TV's backward-z term (its w3.y weighting) reaches 100 times
+    # the plain gradient, so it takes a tenth of that
+    beta = 2e-5 if case == "tvw1" else 2e-4
+    o.beta = beta
     o.Niter = 2
     ref_img = (truth + rng.uniform(0, 0.3, g.n_img)).astype(np.float32)
     if case == "apls_prior":
@@ -446,11 +456,14 @@ def test_builtin_osl_osem_tv_variants(cuda, case):
     S64 = None if S is None else S.astype(np.float64)
 
     def grad(v):
-        return io.tv_gradient_variant(v, shape, name, smooth, 0.002, sigma=sigma, C=C, S=S64)
+        return io.tv_gradient_variant(v, shape, name, smooth, beta, sigma=sigma, C=C, S=S64)
     want = orc.osem(g, ys, np.ones(g.n_img), 2, prior_grad=grad)
     x = out.ravel(order='F')
     assert np.all(np.isfinite(x))
     assert orc.rel_l2(x, want) < 5e-5, orc.rel_l2(x, want)
+    # the variant reached the kernel: the plain TV gives another image
+    plain = orc.osem(g, ys, np.ones(g.n_img), 2, prior_grad=lambda v: orc.tv_gradient(v, shape, smooth, beta))
+    assert orc.rel_l2(x, plain) > 1e-3
 
 
 @pytest.mark.gpu
