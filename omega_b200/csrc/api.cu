@@ -1185,8 +1185,9 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
     }
     if (e == cudaSuccess && st == OMB_OK && h->desc.bp_type == 5) {
         float best_ms = 3.4e38f;
-        // (voxels along z, warps per block, staged); the staged kernel has 8 voxels and 4 warps
-        const int shapes[7][3] = {{4, 4, 0}, {4, 8, 0}, {8, 4, 0}, {8, 8, 0}, {16, 4, 0}, {16, 8, 0}, {8, 4, 1}};
+        // (voxels along z, warps per block, staged); the staged kernel has 8 or 16 voxels and 4 warps
+        const int shapes[8][3] = {{4, 4, 0}, {4, 8, 0}, {8, 4, 0}, {8, 8, 0}, {16, 4, 0}, {16, 8, 0}, {8, 4, 1},
+                                  {16, 4, 1}};
         for (const auto &sh : shapes) {
             h->tune = best;
             h->tune.bdd_bp_z = sh[0];

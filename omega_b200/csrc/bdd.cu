@@ -310,7 +310,7 @@ __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, const BddMap64 
         if (!bdd_bp_footprint(M, rx0, ry0, rz0, hx, hy, hz, qx, qy, g, nr, nc, nzt, F)) continue;
         const Seg &seg = F.seg;
         const int r0 = F.r0, cA = F.cA, ncols = F.ncols;
-        const float V0 = F.V0, vl0 = F.vl0, vr0 = F.vr0, svl = F.svl, svr = F.svr, vA = F.vA, vB = F.vB;
+        const float V0 = F.V0, vl0 = F.vl0, vr0 = F.vr0, svl = F.svl, svr = F.svr;
         const float axy = F.axy, kscale = F.kscale;
         const float *yp = y + p * (int64_t)nr * nc + (int64_t)M.o.y * nr + M.o.x + r0;
 #define col_sum(c) seg_sum(seg, yp + (int64_t)(c) * nr)
@@ -322,27 +322,7 @@ __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, const BddMap64 
                 pref[m][tid] = make_float2(acc, rs);
                 acc += rs;
             }
-            const float fA = (float)cA;
-            const int mmax = ncols - 1;
-#pragma unroll
-            for (int t = 0; t < kBpZ; ++t) {
-                if (FULL || t < nzt) {
-                    const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
-                    // clamp to [vA, vB] (inside the panel); an empty footprint gives va == vb
-                    const float qa = fminf(fmaxf(fminf(vlt, vrt), vA), vB) - fA;
-                    const float qb = fminf(fmaxf(fmaxf(vlt, vrt), vA), vB) - fA;
-                    const int ma = min((int)qa, mmax), mb = min((int)qb, mmax);
-                    const float2 ea = pref[ma][tid], eb = pref[mb][tid];
-                    const float apu = fmaf(qb - (float)mb, eb.y, eb.x) - fmaf(qa - (float)ma, ea.y, ea.x);
-                    if (apu != 0.f) {
-                        const float vz = fmaf((float)t, g.dz, qz0) - M.s.z;
-                        const float q2 = fmaf(vz, vz, axy);
-                        const float ker = kscale * (q2 * rsqrtf(q2));
-                        temp[t] = fmaf(apu, ker, temp[t]);
-                        if (SENS) wsum[t] += ker;
-                    }
-                }
-            }
+            bp_voxels<kBpZ, SENS, FULL, kBpThreads>(F, &pref[0][tid], nzt, nc, qz0 - M.s.z, g.dz, temp, wsum);
         } else {
             // footprints wider than the slot array: per voxel, walk its columns
 #pragma unroll
@@ -463,8 +443,8 @@ int bdd_backward_ray(const Grid &g, const float *xy, const float *uv, int nr, in
 int bdd_backward(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj, const float *y,
                  float *img, float *sens, const Tuning &tn, cudaStream_t st) {
     if (g.nz > 65535 * 4) return set_error(OMB_ERR_UNSUPPORTED, "too many slices");
-    if (tn.bdd_bp_staged && tn.bdd_bp_z == 8 && bdd_bp_tma_supported(nr, y))
-        return bdd_backward_tma(g, pj, pm, nr, nc, nproj, y, img, sens, st);
+    if (tn.bdd_bp_staged && (tn.bdd_bp_z == 8 || tn.bdd_bp_z == 16) && bdd_bp_tma_supported(nr, y))
+        return bdd_backward_tma(g, pj, pm, nr, nc, nproj, y, img, sens, tn.bdd_bp_z, st);
     const int rows = tn.bdd_bp_rows;
     switch (tn.bdd_bp_z) {
         case 4: launch_bp<4>(g, pj, pm, nr, nc, nproj, y, img, sens, rows, st); break;

@@ -247,6 +247,75 @@ __device__ __forceinline__ bool bdd_bp_footprint(const BddMapR &M, float rx0, fl
     return true;
 }
 
+// The voxels of one column on one projection, from the column prefix sums
+// pc[m * STRIDE] = (sum of row sums of columns cA .. cA + m - 1, row sum of
+// column cA + m), m < ncols: voxel t covers the detector columns between its
+// edges a_t = vl0 + t svl and b_t = vr0 + t svr (relative to column cA, as
+// fractional column positions), and its value is the prefix difference
+// P(max) - P(min), P linear inside a column.  IN: every edge lies on the panel
+// (no clamp to [vA, vB]); CR: the two edge lines cross inside the run (the
+// lower edge is taken per voxel).  Shared by the staged and unstaged kernels,
+// which therefore compute the same numbers.
+template <int KZ, bool SENS, bool FULL, int STRIDE, bool IN, bool CR>
+__device__ __forceinline__ void bp_voxel_run(const float2 *__restrict__ pc, int nzt, int mmax, float a0, float sa,
+                                             float b0, float sb, float vAr, float vBr, float vz0, float dz, float axy,
+                                             float kscale, float *temp, float *wsum) {
+#pragma unroll
+    for (int t = 0; t < KZ; ++t) {
+        if (FULL || t < nzt) {
+            const float at = fmaf((float)t, sa, a0), bt = fmaf((float)t, sb, b0);
+            float lo = CR ? fminf(at, bt) : at, hi = CR ? fmaxf(at, bt) : bt;
+            if (!IN) {
+                lo = fminf(fmaxf(lo, vAr), vBr);
+                hi = fminf(fmaxf(hi, vAr), vBr);
+            }
+            const int ma = min((int)lo, mmax), mb = min((int)hi, mmax);
+            const float2 ea = pc[ma * STRIDE], eb = pc[mb * STRIDE];
+            const float apu = fmaf(hi - (float)mb, eb.y, eb.x) - fmaf(lo - (float)ma, ea.y, ea.x);
+            if (apu != 0.f) {
+                const float vz = fmaf((float)t, dz, vz0);
+                const float q2 = fmaf(vz, vz, axy);
+                const float ker = kscale * (q2 * rsqrtf(q2));
+                temp[t] = fmaf(apu, ker, temp[t]);
+                if (SENS) wsum[t] += ker;
+            }
+        }
+    }
+}
+
+template <int KZ, bool SENS, bool FULL, int STRIDE>
+__device__ __forceinline__ void bp_voxels(const BpFootprint &F, const float2 *__restrict__ pc, int nzt, int nc,
+                                          float vz0, float dz, float *temp, float *wsum) {
+    const float fA = (float)F.cA;
+    const int mmax = F.ncols - 1;
+    float a0 = F.vl0 - fA, b0 = F.vr0 - fA, sa = F.svl, sb = F.svr;
+    const float tl = (float)((FULL ? KZ : nzt) - 1);
+    const float aL = fmaf(tl, sa, a0), bL = fmaf(tl, sb, b0);
+    const bool cross = (a0 <= b0) != (aL <= bL);
+    if (!cross && b0 < a0) {
+        // the right-corner edge is the lower one throughout
+        float u = a0;
+        a0 = b0;
+        b0 = u;
+        u = sa;
+        sa = sb;
+        sb = u;
+    }
+    const bool in = F.vmin >= -F.V0 && F.vmax <= (float)nc - F.V0;
+    const float vAr = F.vA - fA, vBr = F.vB - fA;
+    if (!cross) {
+        if (in)
+            bp_voxel_run<KZ, SENS, FULL, STRIDE, true, false>(pc, nzt, mmax, a0, sa, b0, sb, vAr, vBr, vz0, dz, F.axy,
+                                                             F.kscale, temp, wsum);
+        else
+            bp_voxel_run<KZ, SENS, FULL, STRIDE, false, false>(pc, nzt, mmax, a0, sa, b0, sb, vAr, vBr, vz0, dz,
+                                                              F.axy, F.kscale, temp, wsum);
+    } else {
+        bp_voxel_run<KZ, SENS, FULL, STRIDE, false, true>(pc, nzt, mmax, a0, sa, b0, sb, vAr, vBr, vz0, dz, F.axy,
+                                                         F.kscale, temp, wsum);
+    }
+}
+
 // seg_sum over a run staged in shared memory (plain loads, same arithmetic).
 __device__ __forceinline__ float seg_sum_shared(const Seg &s, const float *p) {
     float acc = fmaf(s.w2, p[s.o2], fmaf(s.w1, p[s.o1], s.w0 * p[0]));

@@ -267,35 +267,43 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
 // ---------------------------------------------------------------------------
 namespace bb {
 
-constexpr int kZ = 8;                              // voxels along z per thread
-constexpr int kThreads = 128;                      // 32 x 4 voxel columns
-constexpr int kSlots = bp_slots(kZ);               // prefix-sum slots per thread
-constexpr int kRW = 52;                            // detector rows of a box (multiple of 4)
-constexpr int kCW = kSlots + 4;                    // detector columns of a box
-constexpr int kStageFloats = (kRW * kCW + 31) / 32 * 32;  // 128-byte aligned stages
-constexpr int kStages = 4;
-constexpr int kChunk = 16;  // views whose re-based maps the CTA prepares together
+constexpr int kThreads = 128;  // 32 x 4 voxel columns
+constexpr int kRW = 52;        // detector rows of a box (multiple of 4)
+constexpr int kChunk = 16;     // views whose re-based maps the CTA prepares together
 
+// KZ voxels along z per thread (8 or 16)
+template <int KZ>
+struct Cfg {
+    static constexpr int kSlots = bp_slots(KZ);  // prefix-sum slots per thread
+    static constexpr int kCW = kSlots + 4;       // detector columns of a box
+    static constexpr int kStageFloats = (kRW * kCW + 31) / 32 * 32;  // 128-byte aligned stages
+    // the static shared memory stays below 48 KB: 4 stages at 8 voxels, 3 at 16
+    static constexpr int kStages = KZ == 8 ? 4 : 3;
+    static constexpr int kMinBlocks = KZ == 8 ? 6 : 5;
+};
+
+template <int KZ>
 struct Shared {
-    alignas(128) float box[kStages][kStageFloats];
-    alignas(8) uint64_t full[kStages];
+    alignas(128) float box[Cfg<KZ>::kStages][Cfg<KZ>::kStageFloats];
+    alignas(8) uint64_t full[Cfg<KZ>::kStages];
     // the maps of a chunk of views re-based to this block, (U0, V0) = the
     // view's box origin; two chunks alternate (the one being consumed and
     // the next, prepared once per kChunk views by all threads)
     BddMapR map[2][kChunk];
-    float2 pref[kSlots][kThreads];
+    float2 pref[Cfg<KZ>::kSlots][kThreads];
 };
 
 }  // namespace bb
 
-template <bool SENS, bool FULL>
-__global__ void __launch_bounds__(bb::kThreads, 6)
+template <int KZ, bool SENS, bool FULL>
+__global__ void __launch_bounds__(bb::kThreads, bb::Cfg<KZ>::kMinBlocks)
     k_bdd_bp_tma(const __grid_constant__ CUtensorMap map_y, Grid g, const BddProj *__restrict__ pj,
                  const BddMap64 *__restrict__ pm, int nr, int nc, int64_t nproj, const float *__restrict__ y,
                  float *__restrict__ img, float *__restrict__ sens) {
     using namespace bb;
-    constexpr int kBpZ = kZ;
-    __shared__ Shared sh;
+    constexpr int kBpZ = KZ;
+    constexpr int kSlots = Cfg<KZ>::kSlots, kCW = Cfg<KZ>::kCW, kStages = Cfg<KZ>::kStages;
+    __shared__ Shared<KZ> sh;
     const int tid = threadIdx.x + threadIdx.y * 32;
     const int lane = threadIdx.x;
     const int i = blockIdx.x * 32 + threadIdx.x;
@@ -364,7 +372,7 @@ __global__ void __launch_bounds__(bb::kThreads, 6)
     const float qy = fmaf((float)j, g.dy, g.by + 0.5f * g.dy);
     const float qz0 = fmaf((float)kz0, g.dz, g.bz + 0.5f * g.dz);
     const float hx = 0.5f * g.dx, hy = 0.5f * g.dy, hz = 0.5f * g.dz;
-    const float fnr = (float)nr, fnc = (float)nc;
+    const float fnc = (float)nc;
     float temp[kBpZ], wsum[kBpZ];
 #pragma unroll
     for (int t = 0; t < kBpZ; ++t) {
@@ -389,8 +397,8 @@ __global__ void __launch_bounds__(bb::kThreads, 6)
             if (!bdd_bp_footprint(M, rx0, ry0, rz0, hx, hy, hz, qx, qy, g, nr, nc, nzt, F)) break;
             const Seg &seg = F.seg;
             const int r0 = F.r0, cA = F.cA, ncols = F.ncols;
-            const float V0 = F.V0, vl0 = F.vl0, vr0 = F.vr0, svl = F.svl, svr = F.svr, vA = F.vA, vB = F.vB;
-            const float vmin = F.vmin, vmax = F.vmax, axy = F.axy, kscale = F.kscale;
+            const float V0 = F.V0, vl0 = F.vl0, vr0 = F.vr0, svl = F.svl, svr = F.svr;
+            const float axy = F.axy, kscale = F.kscale;
             const bool staged = r0 >= 0 && r0 + seg.n < kRW && cA >= 0 && cA + ncols <= kCW;
             if (ncols <= kSlots) {
                 float acc = 0.f;
@@ -412,29 +420,7 @@ __global__ void __launch_bounds__(bb::kThreads, 6)
                         acc += rs;
                     }
                 }
-                const float fA = (float)cA;
-                const int mmax = ncols - 1;
-                // inside the panel the clamps to [vA, vB] below are identities
-                const bool inside = vmin >= -V0 && vmax <= fnc - V0;
-#pragma unroll
-                for (int t = 0; t < kBpZ; ++t) {
-                    if (FULL || t < nzt) {
-                        const float vlt = fmaf((float)t, svl, vl0), vrt = fmaf((float)t, svr, vr0);
-                        const float lo = fminf(vlt, vrt), hi = fmaxf(vlt, vrt);
-                        const float qa = (inside ? lo : fminf(fmaxf(lo, vA), vB)) - fA;
-                        const float qb = (inside ? hi : fminf(fmaxf(hi, vA), vB)) - fA;
-                        const int ma = min((int)qa, mmax), mb = min((int)qb, mmax);
-                        const float2 ea = sh.pref[ma][tid], eb = sh.pref[mb][tid];
-                        const float apu = fmaf(qb - (float)mb, eb.y, eb.x) - fmaf(qa - (float)ma, ea.y, ea.x);
-                        if (apu != 0.f) {
-                            const float vz = fmaf((float)t, g.dz, qz0) - M.s.z;
-                            const float q2 = fmaf(vz, vz, axy);
-                            const float ker = kscale * (q2 * rsqrtf(q2));
-                            temp[t] = fmaf(apu, ker, temp[t]);
-                            if (SENS) wsum[t] += ker;
-                        }
-                    }
-                }
+                bp_voxels<kBpZ, SENS, FULL, kThreads>(F, &sh.pref[0][tid], nzt, nc, qz0 - M.s.z, g.dz, temp, wsum);
             } else {
                 const float *yp = y + p * (int64_t)nr * nc + (int64_t)M.o.y * nr + M.o.x + r0;
 #pragma unroll
@@ -528,32 +514,40 @@ bool bdd_bp_tma_supported(int nr, const float *y) {
     return nr % 4 == 0 && ((uintptr_t)y & 15) == 0 && encode_fn() != nullptr;
 }
 
-int bdd_backward_tma(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
-                     const float *y, float *img, float *sens, cudaStream_t st) {
-    if (nproj <= 0) return OMB_OK;
+template <int KZ>
+static int launch_bp_tma(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
+                         const float *y, float *img, float *sens, cudaStream_t st) {
     auto fn = encode_fn();
     CUtensorMap m_y;
     const cuuint64_t dims[3] = {(cuuint64_t)nr, (cuuint64_t)nc, (cuuint64_t)nproj};
     const cuuint64_t strides[2] = {(cuuint64_t)nr * sizeof(float), (cuuint64_t)nr * nc * sizeof(float)};
-    const cuuint32_t box[3] = {(cuuint32_t)bb::kRW, (cuuint32_t)bb::kCW, 1u};
+    const cuuint32_t box[3] = {(cuuint32_t)bb::kRW, (cuuint32_t)bb::Cfg<KZ>::kCW, 1u};
     const cuuint32_t estr[3] = {1u, 1u, 1u};
     if (!fn || fn(&m_y, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(y), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return set_error(OMB_ERR_CUDA, "cuTensorMapEncodeTiled failed for the type-5 projection map");
     dim3 block(32, 4);
-    dim3 grid((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + bb::kZ - 1) / bb::kZ);
-    const bool full = g.nz % bb::kZ == 0;
+    dim3 grid((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + KZ - 1) / KZ);
+    const bool full = g.nz % KZ == 0;
     if (sens && full)
-        k_bdd_bp_tma<true, true><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
+        k_bdd_bp_tma<KZ, true, true><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
     else if (sens)
-        k_bdd_bp_tma<true, false><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
+        k_bdd_bp_tma<KZ, true, false><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
     else if (full)
-        k_bdd_bp_tma<false, true><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
+        k_bdd_bp_tma<KZ, false, true><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
     else
-        k_bdd_bp_tma<false, false><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
+        k_bdd_bp_tma<KZ, false, false><<<grid, block, 0, st>>>(m_y, g, pj, pm, nr, nc, nproj, y, img, sens);
     OMB_LAUNCH_CHECK("type-5 TMA backward launch");
     return OMB_OK;
+}
+
+int bdd_backward_tma(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
+                     const float *y, float *img, float *sens, int kz, cudaStream_t st) {
+    if (nproj <= 0) return OMB_OK;
+    if (kz == 16) return launch_bp_tma<16>(g, pj, pm, nr, nc, nproj, y, img, sens, st);
+    if (kz == 8) return launch_bp_tma<8>(g, pj, pm, nr, nc, nproj, y, img, sens, st);
+    return set_error(OMB_ERR_INVALID, "the staged type-5 backprojection takes runs of 8 or 16 voxels");
 }
 
 int take_device_error() {

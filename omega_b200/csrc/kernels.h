@@ -107,10 +107,11 @@ int bdd_backward(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, i
 int bdd_backward_ray(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
                      int64_t nproj, const float *y, float *img, float *sens, unsigned long long *acc,
                      unsigned long long *acc_s, cudaStream_t st);
-// The same backprojection with per-projection detector boxes staged by TMA (8 voxels along z per thread).
+// The same backprojection with per-projection detector boxes staged by TMA (kz = 8 or 16 voxels along z per
+// thread; the same numbers as bdd_backward with bdd_bp_z = kz).
 bool bdd_bp_tma_supported(int nr, const float *y);
 int bdd_backward_tma(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
-                     const float *y, float *img, float *sens, cudaStream_t st);
+                     const float *y, float *img, float *sens, int kz, cudaStream_t st);
 
 // Projector type 4 (interpolation), PET and CT.
 int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img,

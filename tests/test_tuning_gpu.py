@@ -51,8 +51,9 @@ def test_bdd_every_shape_matches_oracle(cuda, name):
     # staging the image / detector boxes in shared memory changes where the
     # data are read from, not the arithmetic
     assert np.array_equal(fps[(8, 4, 1)].view(np.uint32), fps[(8, 4, 0)].view(np.uint32))
-    for a, b in zip(bps[(8, 4, 1)], bps[(8, 4, 0)]):
-        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    for z in (8, 16):
+        for a, b in zip(bps[(z, 4, 1)], bps[(z, 4, 0)]):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), z
 
 
 def test_siddon_every_shape_matches_oracle(cuda):
