@@ -316,10 +316,11 @@ __global__ void k_bdd_bp(Grid g, const BddProj *__restrict__ pj, const BddMap64 
 #define col_sum(c) seg_sum(seg, yp + (int64_t)(c) * nr)
         if (ncols <= kBpCols) {
             float acc = 0.f;
-#pragma unroll 4
-            for (int m = 0; m < ncols; ++m) {
+#pragma unroll
+            for (int m = 0; m < kBpCols; ++m) {
+                if (m >= ncols) break;
                 const float rs = col_sum(cA + m);
-                pref[m][tid] = make_float2(acc, rs);
+                pref[m][tid] = bp_prefix_node(acc, rs, m);
                 acc += rs;
             }
             bp_voxels<kBpZ, SENS, FULL, kBpThreads>(F, &pref[0][tid], nzt, nc, qz0 - M.s.z, g.dz, temp, wsum);

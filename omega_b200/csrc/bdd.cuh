@@ -247,12 +247,18 @@ __device__ __forceinline__ bool bdd_bp_footprint(const BddMapR &M, float rx0, fl
     return true;
 }
 
-// The voxels of one column on one projection, from the column prefix sums
-// pc[m * STRIDE] = (sum of row sums of columns cA .. cA + m - 1, row sum of
-// column cA + m), m < ncols: voxel t covers the detector columns between its
-// edges a_t = vl0 + t svl and b_t = vr0 + t svr (relative to column cA, as
-// fractional column positions), and its value is the prefix difference
-// P(max) - P(min), P linear inside a column.  IN: every edge lies on the panel
+// Node m of a column prefix: the prefix P(x) = (sum of the row sums of the
+// columns before m) + (x - m) rs_m for x in [m, m + 1] (x relative to the
+// first column), stored as its intercept and slope, P(x) = B_m + x rs_m.
+__device__ __forceinline__ float2 bp_prefix_node(float acc, float rs, int m) {
+    return make_float2(fmaf(-(float)m, rs, acc), rs);
+}
+
+// The voxels of one column on one projection, from the prefix nodes
+// pc[m * STRIDE] (bp_prefix_node), m < ncols: voxel t covers the detector
+// columns between its edges a_t = vl0 + t svl and b_t = vr0 + t svr
+// (relative to column cA, as fractional column positions), and its value is
+// the prefix difference P(max) - P(min).  IN: every edge lies on the panel
 // (no clamp to [vA, vB]); CR: the two edge lines cross inside the run (the
 // lower edge is taken per voxel).  Shared by the staged and unstaged kernels,
 // which therefore compute the same numbers.
@@ -271,7 +277,7 @@ __device__ __forceinline__ void bp_voxel_run(const float2 *__restrict__ pc, int 
             }
             const int ma = min((int)lo, mmax), mb = min((int)hi, mmax);
             const float2 ea = pc[ma * STRIDE], eb = pc[mb * STRIDE];
-            const float apu = fmaf(hi - (float)mb, eb.y, eb.x) - fmaf(lo - (float)ma, ea.y, ea.x);
+            const float apu = fmaf(hi, eb.y, eb.x) - fmaf(lo, ea.y, ea.x);
             if (apu != 0.f) {
                 const float vz = fmaf((float)t, dz, vz0);
                 const float q2 = fmaf(vz, vz, axy);

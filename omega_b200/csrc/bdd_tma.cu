@@ -402,21 +402,24 @@ __global__ void __launch_bounds__(bb::kThreads, bb::Cfg<KZ>::kMinBlocks)
             const bool staged = r0 >= 0 && r0 + seg.n < kRW && cA >= 0 && cA + ncols <= kCW;
             if (ncols <= kSlots) {
                 float acc = 0.f;
+                float2 *pw = &sh.pref[0][tid];
                 if (staged && seg.n <= 2) {
-                    const float *q = sh.box[s] + cA * kRW + r0;
-#pragma unroll 4
-                    for (int m = 0; m < ncols; ++m) {
-                        const float rs = fmaf(seg.w2, q[seg.o2], fmaf(seg.w1, q[seg.o1], seg.w0 * q[0]));
-                        sh.pref[m][tid] = make_float2(acc, rs);
+                    const float *q0 = sh.box[s] + cA * kRW + r0;
+                    const float *q1 = q0 + seg.o1, *q2 = q0 + seg.o2;
+#pragma unroll
+                    for (int m = 0; m < kSlots; ++m) {
+                        if (m >= ncols) break;
+                        const float rs = fmaf(seg.w2, q2[m * kRW], fmaf(seg.w1, q1[m * kRW], seg.w0 * q0[m * kRW]));
+                        pw[m * kThreads] = bp_prefix_node(acc, rs, m);
                         acc += rs;
-                        q += kRW;
                     }
                 } else {
                     const float *yp = y + p * (int64_t)nr * nc + (int64_t)M.o.y * nr + M.o.x + r0;
-#pragma unroll 4
-                    for (int m = 0; m < ncols; ++m) {
+#pragma unroll
+                    for (int m = 0; m < kSlots; ++m) {
+                        if (m >= ncols) break;
                         const float rs = seg_sum(seg, yp + (int64_t)(cA + m) * nr);
-                        sh.pref[m][tid] = make_float2(acc, rs);
+                        pw[m * kThreads] = bp_prefix_node(acc, rs, m);
                         acc += rs;
                     }
                 }
