@@ -54,8 +54,8 @@ PROFILED_TRAFFIC = {
     # DRAM bytes read + written per launch, from the ncu captures summarised
     # in profiles/: bdd_cbct_capture.md (36-view capture x 10) and
     # siddon_dynpet_launches.md (full-size capture)
-    ("cbct", "bdd_fp"): 9.40e9,
-    ("cbct", "bdd_bp"): 3.87e8,
+    ("cbct", "bdd_fp"): 9.46e9,
+    ("cbct", "bdd_bp"): 3.76e8,
     ("dynpet", "siddon_fp"): 3.81e8,
     ("dynpet", "siddon_bp"): 4.77e8,
     # interp_tof_capture.md: one subset's forward launch (16 per step)
@@ -65,8 +65,8 @@ PROFILED_TRAFFIC = {
 # L2-resident, so DRAM moves a few per cent of the cache-less bytes): the
 # issue-active and SM-throughput percentages of the same ncu captures.
 PROFILED_LIMITER = {
-    ("cbct", "bdd_fp"): {"issue_active_pct": 83.0, "sm_throughput_pct": 79.7, "dram_pct": 5.2},
-    ("cbct", "bdd_bp"): {"issue_active_pct": 74.2, "sm_throughput_pct": 73.8, "dram_pct": 0.2},
+    ("cbct", "bdd_fp"): {"issue_active_pct": 80.4, "sm_throughput_pct": 75.5, "dram_pct": 7.6},
+    ("cbct", "bdd_bp"): {"issue_active_pct": 72.9, "sm_throughput_pct": 71.8, "dram_pct": 0.35},
     ("dynpet", "siddon_fp"): {"issue_active_pct": 66.5, "l1tex_pct": 92.0, "dram_pct": 1.0},
     ("dynpet", "siddon_bp"): {"issue_active_pct": 44.4, "lts_pct": 65.9, "dram_pct": 1.0},
     ("interp_tof", "interp_fp"): {"issue_active_pct": 84.9, "sm_throughput_pct": 78.6, "dram_pct": 0.01},
