@@ -609,6 +609,18 @@ def run_cbct(args, rank, world, dev):
         h_out.copy_(b, non_blocking=True)
 
     e2e_total = e2e_time(args, world, dev, step_host)
+
+    # the ray-driven (scatter) backprojection of the same dual variable, the
+    # exact adjoint of the forward projection, timed beside the gather
+    ray_ms = []
+    for it in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _native.call("omb_backward", h, -1, P(p), P(wi), None, _native.OMB_BP_RAY, sp)
+        e1.record(stream)
+        e1.synchronize()
+        if it:
+            ray_ms.append(e0.elapsed_time(e1))
     if rank != 0:
         return None
     K = args.steps
@@ -640,6 +652,9 @@ def run_cbct(args, rank, world, dev):
                          % (m * 4 / 1e6)},
         "fp_ms": 1e3 * mean_fp, "bp_ms": 1e3 * mean_bp, "dual_ms": 1e3 * t_dual / K,
         "primal_tv_ms": 1e3 * t_primal / K, "tau": tau,
+        "bp_ray": {"ms": statistics.median(ray_ms),
+                   "what": "ray-driven scatter backprojection (float atomics), the exact adjoint of the forward "
+                           "projection, of the same data; not part of the step"},
         "roofline": rl,
         "e2e": {"value": m * K * world / e2e_total, "unit": "rays/s", "h2d_bytes_per_step": n * 4,
                 "d2h_bytes_per_step": n * 4},
