@@ -325,7 +325,7 @@ typedef enum omb_prior {
     OMB_PRIOR_TV = 6,       /* options.TV with a MAP algorithm other than PDHG: omb_tv_gradient, tv_smoothing */
     OMB_PRIOR_GGMRF = 7,    /* options.GGMRF: omb_ggmrf_gradient over prior_g with ggmrf_weights and ggmrf[3] */
     OMB_PRIOR_HYPERBOLIC = 8,/* options.hyperbolic: omb_hyperbolic_gradient over prior_g with hyper_weights */
-    OMB_PRIOR_WMEAN = 9     /* options.weighted_mean, mean_type 1-3: omb_wmean_gradient over prior_g */
+    OMB_PRIOR_WMEAN = 9     /* options.weighted_mean, mean_type 1-6: omb_wmean_gradient over prior_g */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -369,7 +369,8 @@ typedef struct omb_recon_params {
     const float *hyper_weights;/* hyperbolic: device, options.weights_quad (centre left out, x fastest) */
     float hyper_delta;        /* hyperbolic: options.hyperbolicDelta */
     const float *wmean_weights;/* weighted mean: device, options.weighted_weights (x fastest) */
-    int32_t wmean_type;       /* weighted mean: options.mean_type (1 arithmetic, 2 harmonic, 3 geometric); the
+    int32_t wmean_type;       /* weighted mean: options.mean_type (1-3 arithmetic, harmonic, geometric; 4-6 their
+                                 neighbourhood forms, see omb_wmean_gradient); the
                                  normalisation switch is mrp_no_norm (options.med_no_norm) */
     int32_t tv_variant;       /* OMB_PRIOR_TV and PDHG: omb_tv_variant (0: the plain TV) */
     float tv_sigma;           /* OMB_PRIOR_TV and PDHG: options.SATVPhi (SATV, weighted TV) */
@@ -377,6 +378,8 @@ typedef struct omb_recon_params {
                                  APLS) */
     const float *tv_ref;      /* OMB_PRIOR_TV and PDHG: device reference image / tensor of the anatomical
                                  variants (OMB_TV_ANAT1 and above), NULL otherwise */
+    float wmean_wsum;         /* weighted mean: the sum of wmean_weights (the means divide the weights by it;
+                                 types 4-6 also weight their sum by the raw weights); <= 0: 1 */
 } omb_recon_params;
 
 /*
@@ -445,10 +448,17 @@ int omb_hyperbolic_gradient(const float *u, float *grad, int32_t nx, int32_t ny,
                             int32_t sz, const float *weights, float delta, float beta, void *stream);
 
 /*
- * Weighted-mean prior gradient, mean types 1-3 (priors.h:99-160): m = the
+ * Weighted-mean prior gradient (priors.h:99-210).  Types 1-3: m = the
  * weighted arithmetic / harmonic / geometric mean of the mirrored
  * (2mx+1)(2my+1)(2mz+1) window (weights / wsum applied as a convolution);
  * grad += beta * (u - m) / (m + epps), or beta * (u - m) with no_norm.
+ * Types 4-6 (the same three means, mirrored twice as far, taken at every
+ * voxel's neighbours too): grad += beta * sum_d w_d g(u, M(x + d)) over the
+ * window's offsets d (raw weights, x fastest) with g = log(max(u / M,
+ * 1e-6)) (4), (u' - M) / u' - ((u' - M) / (sqrt(2) u'))^2 (5), 1 - M / u'
+ * (6), u' = max(u, 1e-6); no_norm and epps do not apply.  Types 4-6 need
+ * 2 mx <= nx (likewise y, z) and take an (nx+2mx)(ny+2my)(nz+2mz)-float
+ * scratch image with cudaMallocAsync on `stream`.
  */
 int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx, int32_t my,
                        int32_t mz, const float *weights, float wsum, int32_t mean_type, float epps, float beta,

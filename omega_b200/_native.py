@@ -127,6 +127,7 @@ class ReconParams(ctypes.Structure):
         ("tv_sigma", ctypes.c_float),
         ("tv_c", ctypes.c_float),
         ("tv_ref", ctypes.c_void_p),
+        ("wmean_wsum", ctypes.c_float),
     ]
 
 

@@ -425,6 +425,73 @@ __global__ void k_wmean_gradient(const float *__restrict__ u, float *__restrict_
     grad[n] += beta * (no_norm ? d : d / (m + epps));
 }
 
+// Mean types 4-6, first pass: the weighted mean M over the image grown by
+// (mx, my, mz) on every side (the means of the neighbours of border voxels),
+// from the image mirrored twice as far; M(c) for c = the original
+// coordinate, stored at c + (mx, my, mz) in an (nx+2mx)(ny+2my)(nz+2mz) grid.
+__global__ void k_wmean_ext(const float *__restrict__ u, float *__restrict__ mext, int nx, int ny, int nz, int mx,
+                            int my, int mz, const float *__restrict__ w, float wsum, int mean_type) {
+    const int ex = nx + 2 * mx, ey = ny + 2 * my;
+    const int xe = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ye = blockIdx.y * blockDim.y + threadIdx.y;
+    const int ze = blockIdx.z;
+    if (xe >= ex || ye >= ey) return;
+    const int x = xe - mx, y = ye - my, z = ze - mz;
+    const int64_t nxy = (int64_t)nx * ny;
+    const int wx = 2 * mx + 1, wy = 2 * my + 1;
+    float acc = 0.f;
+    for (int k = -mz; k <= mz; ++k)
+        for (int j = -my; j <= my; ++j)
+            for (int i = -mx; i <= mx; ++i) {
+                const float v = __ldg(u + mirror(x + i, nx) + (int64_t)mirror(y + j, ny) * nx +
+                                      (int64_t)mirror(z + k, nz) * nxy);
+                const float wk = __ldg(w + (mx - i) + (my - j) * wx + (mz - k) * wx * wy) / wsum;
+                acc += wk * (mean_type == 5 ? 1.f / v : (mean_type == 6 ? logf(v) : v));
+            }
+    mext[xe + (int64_t)ye * ex + (int64_t)ze * ex * ey] =
+        mean_type == 5 ? 1.f / acc : (mean_type == 6 ? expf(acc) : acc);
+}
+
+// Second pass (priors.h:125-210): per voxel the sum over the window's
+// offsets d of w_d g(u, M(x + d)), the raw weights paired with the offsets
+// in x-fastest order: type 4 log(max(u / M, 1e-6)); type 5, with u' =
+// max(u, 1e-6), (u' - M) / u' - ((u' - M) / (sqrt(2) u'))^2; type 6
+// 1 - M / u'.
+__global__ void k_wmean_grad46(const float *__restrict__ u, const float *__restrict__ mext, float *__restrict__ grad,
+                               int nx, int ny, int nz, int mx, int my, int mz, const float *__restrict__ w,
+                               int mean_type, float beta) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const int ex = nx + 2 * mx, ey = ny + 2 * my;
+    const int wx = 2 * mx + 1, wy = 2 * my + 1;
+    const int64_t n = x + (int64_t)y * nx + (int64_t)z * nx * ny;
+    const float uv = __ldg(u + n);
+    const float ut = fmaxf(uv, 1e-6f);
+    const float s2 = sqrtf(2.f) * ut;
+    float acc = 0.f;
+    for (int l = 0; l < 2 * mz + 1; ++l)
+        for (int k = 0; k < wy; ++k)
+            for (int h = 0; h < wx; ++h) {
+                // offset (h - mx, k - my, l - mz): extended index (x + h, y + k, z + l)
+                const float M = __ldg(mext + (x + h) + (int64_t)(y + k) * ex + (int64_t)(z + l) * ex * ey);
+                const float wk = __ldg(w + h + k * wx + l * wx * wy);
+                float g;
+                if (mean_type == 4) {
+                    g = logf(fmaxf(uv / M, 1e-6f));
+                } else if (mean_type == 5) {
+                    const float d = ut - M;
+                    const float r = d / s2;
+                    g = d / ut - r * r;
+                } else {
+                    g = 1.f - M / ut;
+                }
+                acc += g * wk;
+            }
+    grad[n] += beta * acc;
+}
+
 }  // namespace omb
 
 extern "C" int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx,
@@ -434,16 +501,39 @@ extern "C" int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32
     if (!u || !grad || !weights) return set_error(OMB_ERR_INVALID, "u/grad/weights pointer is NULL");
     if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
     if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
-    if (mean_type < 1 || mean_type > 3) return set_error(OMB_ERR_UNSUPPORTED, "weighted mean types 1-3 are built");
+    if (mean_type < 1 || mean_type > 6) return set_error(OMB_ERR_INVALID, "weighted mean type must be 1-6");
     if (mx < 0 || my < 0 || mz < 0 || mx > nx || my > ny || mz > nz)
         return set_error(OMB_ERR_INVALID, "weighted mean window must fit one mirror of the image");
+    // types 4-6 read the image mirrored twice the window's reach
+    if (mean_type >= 4 && (2 * mx > nx || 2 * my > ny || 2 * mz > nz))
+        return set_error(OMB_ERR_INVALID, "weighted mean types 4-6 need twice the window within one mirror");
     if (!(wsum != 0.f)) return set_error(OMB_ERR_INVALID, "weighted mean weights sum to 0");
     // the reference takes a 2-D path for one slice (no z window)
     if (nz == 1 && mz > 0) return set_error(OMB_ERR_INVALID, "weighted mean of a single slice needs mz = 0");
     dim3 block(32, 8);
     dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
-    k_wmean_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, mx, my, mz, weights, wsum,
-                                                                mean_type, epps, beta, no_norm);
-    OMB_LAUNCH_CHECK("weighted mean gradient launch");
+    if (mean_type <= 3) {
+        k_wmean_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, mx, my, mz, weights, wsum,
+                                                                    mean_type, epps, beta, no_norm);
+        OMB_LAUNCH_CHECK("weighted mean gradient launch");
+        return OMB_OK;
+    }
+    const cudaStream_t st = (cudaStream_t)stream;
+    const int ex = nx + 2 * mx, ey = ny + 2 * my, ez = nz + 2 * mz;
+    if (ez > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    float *mext = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void **>(&mext), (size_t)ex * ey * ez * sizeof(float), st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(OMB_ERR_CUDA, "allocating the weighted means of types 4-6 failed");
+    }
+    dim3 gext((ex + 31) / 32, (ey + 7) / 8, ez);
+    k_wmean_ext<<<gext, block, 0, st>>>(u, mext, nx, ny, nz, mx, my, mz, weights, wsum, mean_type);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        k_wmean_grad46<<<grid, block, 0, st>>>(u, mext, grad, nx, ny, nz, mx, my, mz, weights, mean_type, beta);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(mext, st);
+    if (e != cudaSuccess) return set_error(OMB_ERR_CUDA, "weighted mean (types 4-6) launch failed");
     return OMB_OK;
 }

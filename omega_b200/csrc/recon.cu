@@ -170,7 +170,8 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                 return omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
             if (p->prior == OMB_PRIOR_WMEAN)
                 return omb_wmean_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1], p->prior_g[2],
-                                          p->wmean_weights, 1.f, p->wmean_type, epps, p->beta, p->mrp_no_norm, stream);
+                                          p->wmean_weights, p->wmean_wsum > 0.f ? p->wmean_wsum : 1.f, p->wmean_type, epps,
+                                          p->beta, p->mrp_no_norm, stream);
             if (p->prior == OMB_PRIOR_HYPERBOLIC)
                 return omb_hyperbolic_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1],
                                                p->prior_g[2], p->hyper_weights, p->hyper_delta, p->beta, stream);

@@ -129,17 +129,16 @@ def ggmrf_weights(options):
 
 
 def weighted_mean_weights(options):
-    """weightedWeights (prepass.py:754-774): sqrt(2) * FOVa_x / Nx times the
+    """The weighted-mean prior's weights, x fastest, float32: options.weighted_weights
+    when given, as given (Weighted_mean, priors.h:103, divides them by their
+    sum for the means and uses them raw in the sums of types 4-6), else
+    weightedWeights (prepass.py:754-774): sqrt(2) * FOVa_x / Nx times the
     distance weights, the centre set to weighted_center_weight, normalised to
-    sum 1; x fastest, float32.  options.weighted_weights when given, divided
-    by their sum (Weighted_mean, priors.h:103, divides by af::sum of the
-    weights it is given)."""
+    sum 1.  Raises when the weights sum to 0."""
     w = np.asarray(getattr(options, 'weighted_weights', np.empty(0)), dtype=np.float32).ravel(order='F')
     if w.size:
-        total = float(np.sum(w, dtype=np.float32))
-        if total == 0.0:
+        if float(np.sum(w, dtype=np.float32)) == 0.0:
             raise ValueError('weighted_weights sum to 0')
-        w = w.astype(np.float64) / total
     else:
         # float32 pitch, then FP64 (the reference's sqrt(2) is a float64 scalar) until the final cast
         dist = np.float32(np.ravel(options.FOVa_x)[0]) / np.float32(np.ravel(options.Nx)[0])

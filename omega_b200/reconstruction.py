@@ -309,6 +309,9 @@ def reconstructions_main(options):
     if len(chosen) > 1:
         raise ValueError('Select one reconstruction method (' + ', '.join(list(_PET_METHODS) + ['PDHG']) + ')')
     method = chosen[0]
+    if bool(getattr(options, 'L', False)) or bool(getattr(options, 'FMH', False)):
+        # the reference's Python path has no weights for these filters (prepass.py:1021-1022)
+        raise ValueError('L-filter and FMH-filter are not yet implemented!')
     quad, huber = bool(getattr(options, 'Quad', False)), bool(getattr(options, 'Huber', False))
     nlm = bool(getattr(options, 'NLM', False))
     mrp = bool(getattr(options, 'MRP', False))
@@ -401,12 +404,13 @@ def reconstructions_main(options):
         if wmean:
             from . import priors
             mt = int(getattr(options, 'mean_type', 4))
-            if mt not in (1, 2, 3):
-                raise ValueError('weighted_mean is built for mean_type 1 (arithmetic), 2 (harmonic) and 3 '
-                                 '(geometric)')
-            ww = torch.from_numpy(priors.weighted_mean_weights(options)).to(dev)
+            if mt not in (1, 2, 3, 4, 5, 6):
+                raise ValueError('mean_type must be 1-6')
+            w = priors.weighted_mean_weights(options)
+            ww = torch.from_numpy(w).to(dev)
             keep.append(ww)
             p.wmean_weights = ctypes.c_void_p(ww.data_ptr())
+            p.wmean_wsum = float(np.sum(w, dtype=np.float32))
             p.wmean_type = mt
             p.mrp_no_norm = 1 if getattr(options, 'med_no_norm', False) else 0
             p.prior_g[0], p.prior_g[1], p.prior_g[2] = int(options.Ndx), int(options.Ndy), int(options.Ndz)

@@ -233,6 +233,50 @@ def wmean_gradient(u, shape, m, weights, mean_type, beta, epps, no_norm=False):
     return (beta * (d if no_norm else d / (mean + epps))).ravel()
 
 
+def wmean_gradient46(u, shape, m, weights, mean_type, beta):
+    """Weighted-mean prior gradient, types 4-6 (priors.h:125-210) in FP64.
+    The image is mirrored by twice the window (functions.hpp:216-260 with
+    2 Ndx ...), the weighted arithmetic / harmonic / geometric mean M (the
+    weights divided by their sum, applied as a convolution) is taken over
+    the image grown by the window on every side, and each voxel sums
+    w_d g(u, M(x + d)) over the window's offsets d with the raw weights in
+    x-fastest order: g = log(max(u / M, 1e-6)) (type 4); with u' = max(u,
+    1e-6), (u' - M) / u' - ((u' - M) / (sqrt(2) u'))^2 (type 5), 1 - M / u'
+    (type 6)."""
+    nx, ny, nz = shape
+    mx, my, mz = (int(v) for v in m)
+    U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
+    P = np.pad(U, ((2 * mz, 2 * mz), (2 * my, 2 * my), (2 * mx, 2 * mx)), mode='symmetric')
+    W = np.asarray(weights, dtype=np.float64).reshape((2 * mz + 1, 2 * my + 1, 2 * mx + 1))
+    Wn = W / W.sum()
+    f = {4: lambda a: a, 5: lambda a: 1.0 / a, 6: np.log}[mean_type]
+    ez, ey, ex = nz + 2 * mz, ny + 2 * my, nx + 2 * mx
+    acc = np.zeros((ez, ey, ex))
+    with np.errstate(divide='ignore'):
+        FP = f(P)
+    for k in range(-mz, mz + 1):
+        for j in range(-my, my + 1):
+            for i in range(-mx, mx + 1):
+                acc += Wn[mz - k, my - j, mx - i] * FP[mz + k:mz + k + ez, my + j:my + j + ey, mx + i:mx + i + ex]
+    with np.errstate(divide='ignore'):
+        M = {4: lambda a: a, 5: lambda a: 1.0 / a, 6: np.exp}[mean_type](acc)
+    ut = np.maximum(U, 1e-6)
+    g = np.zeros_like(U)
+    for l in range(2 * mz + 1):
+        for k in range(2 * my + 1):
+            for h in range(2 * mx + 1):
+                Md = M[l:l + nz, k:k + ny, h:h + nx]
+                if mean_type == 4:
+                    with np.errstate(divide='ignore'):
+                        t = np.log(np.maximum(U / Md, 1e-6))
+                elif mean_type == 5:
+                    t = (ut - Md) / ut - ((ut - Md) / (np.sqrt(2.0) * ut)) ** 2
+                else:
+                    t = 1.0 - Md / ut
+                g += W[l, k, h] * t
+    return (beta * g).ravel()
+
+
 # ---------------------------------------------------------------------------
 # TV gradient variants of TVKernel (auxKernels.cl:1733-1990): the image read
 # edge-clamped (the texture path), the anatomical reference S read as zero

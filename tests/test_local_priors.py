@@ -240,21 +240,82 @@ def test_weighted_mean_weights_match_reference():
     assert np.array_equal(priors.weighted_mean_weights(o), f["wmean_111"])
 
 
-def test_weighted_mean_user_weights_are_normalised():
-    """Weights given in options.weighted_weights are divided by their sum, as
-    Weighted_mean (priors.h:103) divides by af::sum of the weights."""
+def test_weighted_mean_user_weights_keep_their_sum():
+    """Weights given in options.weighted_weights are passed as given, with
+    their sum beside them: Weighted_mean (priors.h:103) divides them by
+    af::sum of the weights for the means and uses them raw in the sums of
+    types 4-6."""
     from conftest import make_options
     from omega_b200 import priors
     o = make_options("pet_mini")
     o.Ndx = o.Ndy = o.Ndz = 1
     w = np.arange(1, 28, dtype=np.float32)
     o.weighted_weights = w
-    got = priors.weighted_mean_weights(o)
-    assert abs(float(got.sum()) - 1.0) < 1e-6
-    assert np.allclose(got, w / w.sum(), rtol=1e-6)
+    assert np.array_equal(priors.weighted_mean_weights(o), w)
     o.weighted_weights = np.zeros(27, np.float32)
     with pytest.raises(ValueError, match="sum to 0"):
         priors.weighted_mean_weights(o)
+
+
+def test_wmean46_oracle_follows_the_reference_steps():
+    """The types 4-6 restatement against the reference's ArrayFire steps
+    written out literally (priors.h:125-210): pad by twice the window
+    (symmetric, functions.hpp:216-260), convolve the padded image with the
+    normalised weights (zero outside, same size), crop to the image grown by
+    the window, then sum w_d g over the shifted means."""
+    from scipy import ndimage
+    rng = np.random.default_rng(3)
+    shape = (9, 8, 7)
+    nx, ny, nz = shape
+    u = rng.uniform(0.2, 1.5, nx * ny * nz)
+    w = rng.uniform(0.1, 1.0, 27)
+    for mt in (4, 5, 6):
+        ours = io.wmean_gradient46(u, shape, (1, 1, 1), w, mt, 1.0)
+        U = u.reshape(shape, order='F')
+        padd = np.pad(U, 2, mode='symmetric')
+        W = w.reshape((3, 3, 3), order='F')
+        f = {4: lambda a: a, 5: lambda a: 1 / a, 6: np.log}[mt]
+        fi = {4: lambda a: a, 5: lambda a: 1 / a, 6: np.exp}[mt]
+        M = fi(ndimage.convolve(f(padd), W / W.sum(), mode='constant', cval=0.0))[1:nx + 3, 1:ny + 3, 1:nz + 3]
+        g = np.zeros_like(U)
+        ut = np.maximum(U, 1e-6)
+        for ll in range(3):
+            for kk in range(3):
+                for hh in range(3):
+                    Md = M[hh:hh + nx, kk:kk + ny, ll:ll + nz]
+                    if mt == 4:
+                        t = np.log(np.maximum(U / Md, 1e-6))
+                    elif mt == 5:
+                        t = (ut - Md) / ut - ((ut - Md) / (np.sqrt(2) * ut)) ** 2
+                    else:
+                        t = 1 - Md / ut
+                    g += W[hh, kk, ll] * t
+        assert np.abs(g.ravel(order='F') - ours).max() < 1e-12 * np.abs(ours).max()
+
+
+@pytest.mark.parametrize("flag", ["L", "FMH"])
+def test_l_filter_and_fmh_raise_as_the_reference(flag):
+    """The reference's Python path raises for the L-filter and FMH priors
+    (prepass.py:1021-1022: their weights are built only by the MATLAB
+    prepass); the built-in entry raises the same error before any launch."""
+    from conftest import make_options
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    o.SinM = np.ones(int(o.Ndist) * int(o.Nang) * int(o.NSinos), np.float32)
+    o.OSL_OSEM = True
+    setattr(o, flag, True)
+    with pytest.raises(ValueError, match="not yet implemented"):
+        rec.reconstructions_main(o)
+
+
+def test_wmean46_rejects_windows_beyond_one_mirror():
+    from omega_b200 import _native
+    L = _native.lib()
+    p = ctypes.c_void_p(16)
+    f = ctypes.c_float
+    assert L.omb_wmean_gradient(p, p, 8, 8, 3, 1, 1, 2, p, f(1.0), 4, f(1e-8), f(0.1), 0, None) != 0
+    assert "twice the window" in L.omb_last_error().decode()
+    assert L.omb_wmean_gradient(p, p, 8, 8, 3, 1, 1, 1, p, f(1.0), 7, f(1e-8), f(0.1), 0, None) != 0
 
 
 def test_weighted_mean_single_slice_needs_flat_window():
@@ -464,6 +525,54 @@ def test_builtin_osl_osem_tv_variants(cuda, case):
     # the variant reached the kernel: the plain TV gives another image
     plain = orc.osem(g, ys, np.ones(g.n_img), 2, prior_grad=lambda v: orc.tv_gradient(v, shape, smooth, beta))
     assert orc.rel_l2(x, plain) > 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mean_type", [4, 5, 6])
+def test_weighted_mean_types_4_to_6(cuda, mean_type):
+    """Kernel = restatement (weights not summing to 1), then BSREM with the
+    prior through the built-in entry = the FP64 loop."""
+    import torch
+    from conftest import make_options
+    from omega_b200 import _native, priors
+    from omega_b200 import reconstruction as rec
+    from omega_b200.reconstruction import _stream
+    rng = np.random.default_rng(30 + mean_type)
+    n = int(np.prod(SHAPE))
+    u = rng.uniform(0.3, 1.7, n).astype(np.float32)
+    w = rng.uniform(0.05, 0.3, 27).astype(np.float32)
+    U, W = torch.tensor(u, device=cuda), torch.tensor(w, device=cuda)
+    out = torch.full((n,), 0.5, device=cuda)
+    _native.call("omb_wmean_gradient", ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(out.data_ptr()), *SHAPE,
+                 1, 1, 1, ctypes.c_void_p(W.data_ptr()), float(np.sum(w, dtype=np.float32)), mean_type, 1e-8, 0.3, 0,
+                 _stream(cuda))
+    want = io.wmean_gradient46(u.astype(np.float64), SHAPE, (1, 1, 1), w.astype(np.float64), mean_type, 0.3)
+    got = out.cpu().numpy() - 0.5
+    assert orc.rel_l2(got, want) < 1e-5, orc.rel_l2(got, want)
+    o = make_options("pet_mini")
+    g = orc.Geometry(o)
+    full = make_options("pet_mini")
+    full.subsets, full.subsetType = 1, 8
+    full.addProjector()
+    y = rng.poisson(orc.forward(orc.Geometry(full), rng.uniform(0.5, 2.0, g.n_img), 0) * 200).astype(np.float32) / 200
+    o.SinM = y.copy()
+    o.BSREM = True
+    o.weighted_mean = True
+    o.mean_type = mean_type
+    o.beta = 0.01
+    o.Niter = 2
+    lam = np.array([0.2, 0.12], np.float32)
+    o.lambdaN = lam
+    res, _ = rec.reconstructions_main(o)
+    m = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
+    shape = (g.nx, g.ny, g.nz)
+    ww = priors.weighted_mean_weights(o).astype(np.float64)
+    ref = orc.relaxed(g, ys, np.ones(g.n_img), 2, "BSREM", lam=lam,
+                      prior_grad=lambda v: io.wmean_gradient46(v, shape, (1, 1, 1), ww, mean_type, 0.01))
+    x = res.ravel(order='F')
+    assert np.all(np.isfinite(x))
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
 
 
 @pytest.mark.gpu
