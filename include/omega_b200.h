@@ -380,6 +380,12 @@ typedef struct omb_recon_params {
                                  variants (OMB_TV_ANAT1 and above), NULL otherwise */
     float wmean_wsum;         /* weighted mean: the sum of wmean_weights (the means divide the weights by it;
                                  types 4-6 also weight their sum by the raw weights); <= 0: 1 */
+    int32_t tv_prox;          /* PDHG: nonzero = proximal TV (options.ProxTV: a dual TV variable projected onto
+                                 the beta ball, omb_proxtv_dual / omb_proxtv_divergence) instead of the TV
+                                 gradient */
+    float sigma2;             /* PDHG with proximal TV: the TV dual step (options.sigma2CP) */
+    int32_t l2_ball;          /* PDHG with proximal TV: options.useL2Ball (1: L2 ball, 0: max-norm ball) */
+    int32_t diff_type;        /* PDHG with proximal TV: options.derivativeType (0 forward, 1 backward differences) */
 } omb_recon_params;
 
 /*
@@ -416,6 +422,23 @@ typedef enum omb_tv_variant {
  */
 int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float beta, float smooth,
                     void *stream);
+
+/*
+ * Proximal TV of the PDHG loop (priors.h:261-281; ProxTVGradient, ProxTVq,
+ * ProxTVDivergence auxKernels.cl:1141-1343).  q (device) holds 3 images
+ * (x, y, z components, x fastest), zero before the first iteration.
+ *   omb_proxtv_dual:       q <- P(q + sigma2 D x), D the forward differences
+ *                          (diff_type 0; -x at the last voxel) or backward
+ *                          ones (1; x at the first), P the projection onto the
+ *                          per-voxel ball of radius alpha (options.beta):
+ *                          L2 (l2_ball != 0) or max norm;
+ *   omb_proxtv_divergence: rhs -= div q (backward differences for
+ *                          diff_type 0, forward for 1), before the primal step.
+ */
+int omb_proxtv_dual(const float *x, float *q, int32_t nx, int32_t ny, int32_t nz, float sigma2, float alpha,
+                    int32_t l2_ball, int32_t diff_type, void *stream);
+int omb_proxtv_divergence(const float *q, float *rhs, int32_t nx, int32_t ny, int32_t nz, int32_t diff_type,
+                          void *stream);
 
 /*
  * The TV gradients of the other TV settings (TVKernel built with -DSATV,

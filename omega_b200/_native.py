@@ -128,6 +128,10 @@ class ReconParams(ctypes.Structure):
         ("tv_c", ctypes.c_float),
         ("tv_ref", ctypes.c_void_p),
         ("wmean_wsum", ctypes.c_float),
+        ("tv_prox", ctypes.c_int32),
+        ("sigma2", ctypes.c_float),
+        ("l2_ball", ctypes.c_int32),
+        ("diff_type", ctypes.c_int32),
     ]
 
 
@@ -252,6 +256,11 @@ EXPORTS = [
     ("omb_tv_gradient_ex", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                           ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
                                           ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_proxtv_dual", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_void_p]),
+    ("omb_proxtv_divergence", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     ("omb_mrp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p]),

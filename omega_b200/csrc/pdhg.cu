@@ -357,3 +357,109 @@ extern "C" int omb_tv_gradient_ex(const float *u, float *grad, int32_t nx, int32
     OMB_LAUNCH_CHECK("TV variant gradient launch");
     return OMB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Proximal TV of the PDHG loop (priors.h:261-281; ProxTVGradient, ProxTVq,
+// ProxTVDivergence auxKernels.cl:1141-1343).  The dual variable q holds three
+// images (x, y, z components).  One step: q <- P_alpha(q + sigma2 D x), D the
+// forward differences (DT 0; the last voxel's difference is -x) or the
+// backward ones (DT 1; the first voxel's is x), P the projection onto the
+// per-voxel L2 ball of radius alpha (L2) or the max-norm ball; then the
+// primal right-hand side takes rhs -= div q, the sum of the backward (DT 0)
+// or forward (DT 1) differences of the components.
+// ---------------------------------------------------------------------------
+namespace omb {
+
+template <int DT, bool L2>
+__global__ void __launch_bounds__(256) k_proxtv_dual(const float *__restrict__ x, float *__restrict__ q, int nx, int ny,
+                                                     int nz, float sigma2, float alpha) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nx || j >= ny || k >= nz) return;
+    const int64_t nxy = (int64_t)nx * ny, N = nxy * nz;
+    const int64_t n = i + (int64_t)j * nx + (int64_t)k * nxy;
+    const float c = __ldg(x + n);
+    float gx, gy, gz;
+    if (DT == 0) {
+        gx = i < nx - 1 ? __ldg(x + n + 1) - c : -c;
+        gy = j < ny - 1 ? __ldg(x + n + nx) - c : -c;
+        gz = k < nz - 1 ? __ldg(x + n + nxy) - c : -c;
+    } else {
+        gx = i > 0 ? c - __ldg(x + n - 1) : c;
+        gy = j > 0 ? c - __ldg(x + n - nx) : c;
+        gz = k > 0 ? c - __ldg(x + n - nxy) : c;
+    }
+    // the scaled difference rounded before the addition, as the reference's kernel
+    const float ax = q[n] + __fmul_rn(gx, sigma2);
+    const float ay = q[n + N] + __fmul_rn(gy, sigma2);
+    const float az = q[n + 2 * N] + __fmul_rn(gz, sigma2);
+    const float scale = L2 ? fmaxf(1.f, sqrtf(ax * ax + ay * ay + az * az) / alpha)
+                           : fmaxf(fmaxf(fabsf(az), fmaxf(fabsf(ax), fabsf(ay))) / alpha, 1.f);
+    q[n] = ax / scale;
+    q[n + N] = ay / scale;
+    q[n + 2 * N] = az / scale;
+}
+
+template <int DT>
+__global__ void __launch_bounds__(256) k_proxtv_div(const float *__restrict__ q, float *__restrict__ rhs, int nx, int ny,
+                                                    int nz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nx || j >= ny || k >= nz) return;
+    const int64_t nxy = (int64_t)nx * ny, N = nxy * nz;
+    const int64_t n = i + (int64_t)j * nx + (int64_t)k * nxy;
+    const float *qx = q, *qy = q + N, *qz = q + 2 * N;
+    float d = 0.f;
+    if (DT == 0) {
+        d += i > 0 ? __ldg(qx + n) - __ldg(qx + n - 1) : __ldg(qx + n);
+        d += j > 0 ? __ldg(qy + n) - __ldg(qy + n - nx) : __ldg(qy + n);
+        d += k > 0 ? __ldg(qz + n) - __ldg(qz + n - nxy) : __ldg(qz + n);
+    } else {
+        d += i < nx - 1 ? __ldg(qx + n + 1) - __ldg(qx + n) : -__ldg(qx + n);
+        d += j < ny - 1 ? __ldg(qy + n + nx) - __ldg(qy + n) : -__ldg(qy + n);
+        d += k < nz - 1 ? __ldg(qz + n + nxy) - __ldg(qz + n) : -__ldg(qz + n);
+    }
+    rhs[n] -= d;
+}
+
+}  // namespace omb
+
+extern "C" int omb_proxtv_dual(const float *x, float *q, int32_t nx, int32_t ny, int32_t nz, float sigma2, float alpha,
+                               int32_t l2_ball, int32_t diff_type, void *stream) {
+    using namespace omb;
+    if (!x || !q) return set_error(OMB_ERR_INVALID, "x/q pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    if (diff_type != 0 && diff_type != 1) return set_error(OMB_ERR_INVALID, "diff_type must be 0 or 1");
+    if (!(alpha > 0.f)) return set_error(OMB_ERR_INVALID, "the proximal TV weight (beta) must be positive");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (diff_type == 0) {
+        if (l2_ball) k_proxtv_dual<0, true><<<grid, block, 0, st>>>(x, q, nx, ny, nz, sigma2, alpha);
+        else k_proxtv_dual<0, false><<<grid, block, 0, st>>>(x, q, nx, ny, nz, sigma2, alpha);
+    } else {
+        if (l2_ball) k_proxtv_dual<1, true><<<grid, block, 0, st>>>(x, q, nx, ny, nz, sigma2, alpha);
+        else k_proxtv_dual<1, false><<<grid, block, 0, st>>>(x, q, nx, ny, nz, sigma2, alpha);
+    }
+    OMB_LAUNCH_CHECK("proximal TV dual launch");
+    return OMB_OK;
+}
+
+extern "C" int omb_proxtv_divergence(const float *q, float *rhs, int32_t nx, int32_t ny, int32_t nz, int32_t diff_type,
+                                     void *stream) {
+    using namespace omb;
+    if (!q || !rhs) return set_error(OMB_ERR_INVALID, "q/rhs pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    if (diff_type != 0 && diff_type != 1) return set_error(OMB_ERR_INVALID, "diff_type must be 0 or 1");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (diff_type == 0) k_proxtv_div<0><<<grid, block, 0, st>>>(q, rhs, nx, ny, nz);
+    else k_proxtv_div<1><<<grid, block, 0, st>>>(q, rhs, nx, ny, nz);
+    OMB_LAUNCH_CHECK("proximal TV divergence launch");
+    return OMB_OK;
+}

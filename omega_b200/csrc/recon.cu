@@ -80,6 +80,10 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
     const bool graph = p->use_graph != 0;
     int st = OMB_OK;
     const int alg = p->algorithm;
+    if (alg == OMB_RECON_PDHG_TV && p->tv_prox) {
+        if (!(p->beta > 0.f)) return set_error(OMB_ERR_INVALID, "proximal TV needs beta > 0");
+        if (p->diff_type != 0 && p->diff_type != 1) return set_error(OMB_ERR_INVALID, "diff_type must be 0 or 1");
+    }
     if (alg == OMB_RECON_PDHG_TV || p->prior == OMB_PRIOR_TV) {
         if (p->tv_variant < OMB_TV_PLAIN || p->tv_variant > OMB_TV_APLS)
             return set_error(OMB_ERR_INVALID, "unknown TV variant");
@@ -233,12 +237,17 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         const int64_t m_all = omb_measurement_count(h, -1);  // one subset: all measurements
         if (m_all < 0) return -1;
         const Grid g = handle_grid(h);
-        DevBuf xn, u, pd, wm, wi, work;
+        DevBuf xn, u, pd, wm, wi, work, q;
         if ((st = alloc(xn, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(u, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(pd, (size_t)m_all * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(wm, (size_t)m_all * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(wi, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        if (p->tv_prox) {
+            // the proximal TV's dual variable, three images starting at zero
+            if ((st = alloc(q, 3 * (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+            OMB_CUDA_TRY(cudaMemsetAsync(q.p, 0, 3 * (size_t)n * sizeof(float), s));
+        }
         float tau = p->tau;
         if (!(tau > 0.f)) {
             // |N(0,1)| start normalised to unit length (functions.hpp:2430-2437)
@@ -267,6 +276,20 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         // one iteration; the plain TV gradient is fused into the primal step,
         // the other TV gradients are added to A^T p before it
         auto one = [&](float *xa, float *xb) {
+            if (p->tv_prox) {
+                // priors.h:261-281 between the backprojection and the primal step
+                int e = omb_forward(h, -1, xa, wm.f(), stream);
+                if (e == OMB_OK) e = omb_pdhg_dual(pd.f(), wm.f(), y, m_all, p->sigma, stream);
+                if (e == OMB_OK) e = omb_backward(h, -1, pd.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC, stream);
+                if (e == OMB_OK)
+                    e = omb_proxtv_dual(xa, q.f(), g.nx, g.ny, g.nz, p->sigma2, p->beta, p->l2_ball, p->diff_type,
+                                        stream);
+                if (e == OMB_OK) e = omb_proxtv_divergence(q.f(), wi.f(), g.nx, g.ny, g.nz, p->diff_type, stream);
+                if (e == OMB_OK)
+                    e = omb_pdhg_primal(h, xa, wi.f(), u.f(), xb, tau, p->theta, 0.f, p->tv_smoothing, p->positivity,
+                                        stream);
+                return e;
+            }
             if (p->tv_variant == OMB_TV_PLAIN)
                 return omb_pdhg_iteration(h, xa, xb, u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
                                           p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);

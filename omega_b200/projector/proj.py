@@ -198,6 +198,12 @@ class projectorClass:
     APLS = False
     APLS_ref_image = np.empty(0, dtype=np.float32)
     TV_referenceImage = np.empty(0, dtype=np.float32)
+    # proximal TV with PDHG (proj.py:119, 274, 353, 415 of the reference):
+    # the TV dual step, L2 or max-norm ball, forward / backward differences
+    ProxTV = False
+    sigma2CP = 1.
+    useL2Ball = True
+    derivativeType = 0
     tauCP = 0.
     sigmaCP = 1.
     thetaCP = 1.

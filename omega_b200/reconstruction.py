@@ -333,10 +333,16 @@ def reconstructions_main(options):
                          'epsilon_mramla is not built)')
     if method != 'PDHG' and options.CT:
         raise ValueError(method + ' is built for PET data')
-    if options.PDHG and not options.TV:
-        raise ValueError('PDHG is built with the TV prior (options.TV = True)')
+    prox = bool(getattr(options, 'ProxTV', False))
+    if options.PDHG and not (options.TV or prox):
+        raise ValueError('PDHG is built with the TV prior (options.TV = True) or the proximal TV (options.ProxTV = '
+                         'True)')
+    if options.PDHG and options.TV and prox:
+        raise ValueError('Select one of options.TV and options.ProxTV')
+    if prox and not options.PDHG:
+        raise ValueError('options.ProxTV is built for PDHG')
     tv_set = None
-    if (prior and (tvp or apls)) or options.PDHG:
+    if (prior and (tvp or apls)) or (options.PDHG and options.TV):
         # the TV gradient variant of the TV / APLS options (ProjectorClass.h:900-918)
         from . import priors
         tv_set = priors.tv_setup(options, apls=apls)
@@ -473,6 +479,17 @@ def reconstructions_main(options):
     p.n_iter = int(options.Niter)
     p.beta = float(options.beta)
     p.tv_smoothing = float(options.TVsmoothing)
+    if options.PDHG and prox:
+        # the proximal TV of the PDHG loop: dual step options.sigma2CP, the
+        # beta ball (L2 or max norm), forward or backward differences
+        p.tv_prox = 1
+        p.sigma2 = float(np.ravel(getattr(options, 'sigma2CP', 1.0))[0])
+        p.l2_ball = 1 if getattr(options, 'useL2Ball', True) else 0
+        p.diff_type = int(getattr(options, 'derivativeType', 0))
+        if p.diff_type not in (0, 1):
+            raise ValueError('derivativeType must be 0 or 1')
+        if not float(options.beta) > 0:
+            raise ValueError('options.ProxTV needs options.beta > 0')
     if tv_set is not None:
         p.tv_variant, p.tv_sigma, p.tv_c, p.tv_smoothing, tv_ref = tv_set
         if tv_ref is not None:

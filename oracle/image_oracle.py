@@ -278,6 +278,67 @@ def wmean_gradient46(u, shape, m, weights, mean_type, beta):
 
 
 # ---------------------------------------------------------------------------
+# Proximal TV of the PDHG loop (priors.h:261-281; auxKernels.cl:1141-1343
+# ProxTVq, ProxTVDivergence, ProxTVGradient): the image differences with
+# zero beyond the grid, the dual variable q = (qx, qy, qz) projected onto the
+# alpha ball, its negative divergence added to the primal right-hand side.
+# ---------------------------------------------------------------------------
+
+def _diff(U, axis, forward):
+    """Forward (next - this; the last voxel gives -this) or backward (this -
+    previous; the first voxel gives this) difference along one axis of an
+    (x, y, z) array."""
+    out = np.empty_like(U)
+    if forward:
+        sl_a = [slice(None)] * 3
+        sl_b = [slice(None)] * 3
+        sl_a[axis] = slice(0, -1)
+        sl_b[axis] = slice(1, None)
+        out[tuple(sl_a)] = U[tuple(sl_b)] - U[tuple(sl_a)]
+        last = [slice(None)] * 3
+        last[axis] = slice(-1, None)
+        out[tuple(last)] = -U[tuple(last)]
+    else:
+        sl_a = [slice(None)] * 3
+        sl_b = [slice(None)] * 3
+        sl_a[axis] = slice(1, None)
+        sl_b[axis] = slice(0, -1)
+        out[tuple(sl_a)] = U[tuple(sl_a)] - U[tuple(sl_b)]
+        first = [slice(None)] * 3
+        first[axis] = slice(0, 1)
+        out[tuple(first)] = U[tuple(first)]
+    return out
+
+
+def proxtv_dual(x, q, shape, sigma2, alpha, l2=True, diff_type=0):
+    """q <- P_alpha(q + sigma2 D x): D the forward differences (diff_type 0)
+    or the backward ones (1); P the projection onto the per-voxel L2 ball of
+    radius alpha (l2) or onto the max-norm ball.  q is (3, N), x fastest."""
+    X = np.asarray(x, dtype=np.float64).reshape(shape, order='F')
+    Qa = np.asarray(q, dtype=np.float64).reshape(3, -1)
+    Q = np.stack([Qa[a].reshape(shape, order='F') for a in range(3)])
+    g = np.stack([_diff(X, a, diff_type == 0) for a in range(3)])
+    Qn = Q + sigma2 * g
+    if l2:
+        scale = np.maximum(1.0, np.sqrt((Qn ** 2).sum(axis=0)) / alpha)
+    else:
+        scale = np.maximum(np.abs(Qn).max(axis=0) / alpha, 1.0)
+    Qn = Qn / scale
+    return np.stack([Qn[a].ravel(order='F') for a in range(3)])
+
+
+def proxtv_divergence(q, shape, diff_type=0):
+    """The term ProxTVDivergence subtracts from the right-hand side: the sum
+    over the axes of the backward differences of q (diff_type 0, the
+    adjoint of the forward differences up to sign) or the forward ones (1)."""
+    out = np.zeros(shape)
+    for a in range(3):
+        Q = np.asarray(q[a], dtype=np.float64).reshape(shape, order='F')
+        out += _diff(Q, a, diff_type != 0)
+    return out.ravel(order='F')
+
+
+# ---------------------------------------------------------------------------
 # TV gradient variants of TVKernel (auxKernels.cl:1733-1990): the image read
 # edge-clamped (the texture path), the anatomical reference S read as zero
 # beyond the image (its buffer path).  variant: 'satv' (TVtype 4), 'tvw1'

@@ -682,19 +682,27 @@ def power_method(geom: Geometry, n_iter, seed=0, x0=None):
 
 
 def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1.0, eps=1e-5,
-            positivity=True, tv_grad=None):
+            positivity=True, tv_grad=None, prox=None):
     """PDHG with a TV-gradient term, one subset (computeForwardProject.h:227-316,
     algorithms.h:329-420, auxKernels.cl:2034-2062), in FP64.  tv_grad(x), when
-    given, replaces the plain TV term beta * dTV(x) (the other TVKernel forms)."""
+    given, replaces the plain TV term beta * dTV(x) (the other TVKernel forms).
+    prox = dict(sigma2=..., l2=..., diff_type=...): the proximal TV instead
+    (priors.h:261-281), a dual variable q on the beta ball, rhs -= div q."""
+    from oracle import image_oracle as io
     shape = (geom.nx, geom.ny, geom.nz)
     x = np.asarray(x0, dtype=np.float64).copy()
     u = x.copy()
     p = np.zeros(geom.rays(-1), dtype=np.float64)
+    q = np.zeros((3, geom.n_img))
     yy = np.asarray(y, dtype=np.float64)
     for _ in range(n_iter):
         res = bdd_forward(geom, x, -1) - yy
         p = (p + sigma * res) / (1.0 + sigma)
-        rhs = bdd_backward(geom, p, -1) + (tv_gradient(x, shape, smooth, beta) if tv_grad is None else tv_grad(x))
+        if prox is not None:
+            q = io.proxtv_dual(x, q, shape, prox["sigma2"], beta, prox.get("l2", True), prox.get("diff_type", 0))
+            rhs = bdd_backward(geom, p, -1) - io.proxtv_divergence(q, shape, prox.get("diff_type", 0))
+        else:
+            rhs = bdd_backward(geom, p, -1) + (tv_gradient(x, shape, smooth, beta) if tv_grad is None else tv_grad(x))
         u_prev = u.copy()
         u = u - tau * rhs
         if positivity:

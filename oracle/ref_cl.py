@@ -60,6 +60,8 @@ def _lib(variant, precision):
             L.refcl_pdhg_update.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D, _D, _I]
         if hasattr(L, "refcl_tv_gradient_ex"):
             L.refcl_tv_gradient_ex.argtypes = [_I, _I, _I, _P, _D, _D, _D, _D, _P, _P]
+        if hasattr(L, "refcl_proxtv"):
+            L.refcl_proxtv.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D]
         _libs[key] = L
     return _libs[key]
 
@@ -280,3 +282,17 @@ def tv_gradient_variant(u, shape, variant, smooth, beta, sigma=1.0, C=0.0, S=Non
         nx, ny, nz, _dp(uu), _scalar(sigma, exact_inputs), _scalar(smooth, exact_inputs), _scalar(beta, exact_inputs),
         _scalar(C, exact_inputs), _dp(ss), _dp(g))
     return g
+
+
+def proxtv_step(x, q, rhs, shape, sigma2, alpha, l2=True, diff_type=0, precision="d", exact_inputs=False):
+    """One proximal-TV step with the reference's kernels (ProxTVGradient,
+    ProxTVq, ProxTVDivergence built with -DPROXTV, -DL2 for the L2 ball,
+    -DDIFFTYPE=1 for backward differences): returns (q, rhs) updated."""
+    nx, ny, nz = shape
+    lib = "aux_proxtv_" + ("l2" if l2 else "max") + ("_d1" if diff_type == 1 else "")
+    xx = np.ascontiguousarray(x, dtype=np.float64).ravel()
+    qq = np.ascontiguousarray(q, dtype=np.float64).ravel().copy()
+    rr = np.ascontiguousarray(rhs, dtype=np.float64).ravel().copy()
+    _lib(lib, precision).refcl_proxtv(nx, ny, nz, _dp(xx), _dp(qq), _dp(rr), _scalar(sigma2, exact_inputs),
+                                      _scalar(alpha, exact_inputs))
+    return qq.reshape(3, -1), rr

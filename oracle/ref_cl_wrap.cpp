@@ -332,6 +332,41 @@ REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, doub
 }
 #endif
 
+#if defined(PROXTV)
+/* One proximal-TV step of the PDHG loop (priors.h:261-281): ProxTVGradient
+ * (q += sigma2 * the image differences), ProxTVq (q onto the alpha ball: L2
+ * with -DL2, else the max norm), ProxTVDivergence (rhs -= the divergence of
+ * q).  q: 3 images (qx, qy, qz), x fastest; updated in place, as is rhs. */
+REFCL_EXPORT int refcl_proxtv(int nx, int ny, int nz, const double *im, double *q, double *rhs, double sigma2,
+                              double alpha) {
+    const size_t N = (size_t)nx * ny * nz;
+    rvec I = to_real(im, N), QX = to_real(q, N), QY = to_real(q + N, N), QZ = to_real(q + 2 * N, N);
+    rvec R = to_real(rhs, N);
+    const int3 Nn = make_int3(nx, ny, nz);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                ProxTVGradient(Nn, Nn, I.data(), QX.data(), QY.data(), QZ.data(), (omb_real)sigma2);
+            }
+    for (size_t v = 0; v < N; ++v) {
+        set_item((unsigned)v, 0u, 0u);
+        ProxTVq(QX.data(), QY.data(), QZ.data(), (omb_real)alpha);
+    }
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                ProxTVDivergence(Nn, Nn, QX.data(), QY.data(), QZ.data(), R.data());
+            }
+    from_real(QX, q);
+    from_real(QY, q + N);
+    from_real(QZ, q + 2 * N);
+    from_real(R, rhs);
+    return 0;
+}
+#endif
+
 /* TVKernel in the variant the build selected (-DSATV, -DTVW1,
  * -DANATOMICAL1/2/3): S is the reference image (or, ANATOMICAL1, the nine
  * tensor channels), C the anatomical weight (options.C, or eta for

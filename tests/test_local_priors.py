@@ -308,6 +308,29 @@ def test_l_filter_and_fmh_raise_as_the_reference(flag):
         rec.reconstructions_main(o)
 
 
+def test_proxtv_entry_points_validate_arguments():
+    from omega_b200 import _native
+    L = _native.lib()
+    p = ctypes.c_void_p(16)
+    f = ctypes.c_float
+    assert L.omb_proxtv_dual(p, p, 8, 8, 4, f(0.5), f(0.0), 1, 0, None) != 0
+    assert "beta" in L.omb_last_error().decode()
+    assert L.omb_proxtv_dual(p, p, 8, 8, 4, f(0.5), f(0.1), 1, 2, None) != 0
+    assert L.omb_proxtv_divergence(p, p, 8, 8, 4, 3, None) != 0
+    assert "diff_type" in L.omb_last_error().decode()
+
+
+def test_proxtv_needs_pdhg():
+    from conftest import make_options
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    o.SinM = np.ones(int(o.Ndist) * int(o.Nang) * int(o.NSinos), np.float32)
+    o.OSEM = True
+    o.ProxTV = True
+    with pytest.raises(ValueError, match="built for PDHG"):
+        rec.reconstructions_main(o)
+
+
 def test_wmean46_rejects_windows_beyond_one_mirror():
     from omega_b200 import _native
     L = _native.lib()

@@ -224,3 +224,53 @@ def test_tv_variants_pinned(variant):
     ours = io.tv_gradient_variant(u, shape, variant, 1e-3, 0.8, **kw)
     theirs = ref_cl.tv_gradient_variant(u, shape, variant, 1e-3, 0.8, exact_inputs=True, **kw)
     assert orc.rel_l2(ours, theirs) < 1e-12
+
+
+@pytest.mark.parametrize("l2,diff_type", [(True, 0), (False, 0), (True, 1)])
+def test_proxtv_pinned(l2, diff_type):
+    """The proximal TV step (image_oracle.proxtv_dual / proxtv_divergence)
+    against ProxTVGradient, ProxTVq and ProxTVDivergence compiled with -DPROXTV
+    (-DL2 for the L2 ball, -DDIFFTYPE=1 for backward differences), with the
+    ball projection active on part of the image."""
+    from oracle import image_oracle as io
+    shape = (11, 9, 7)
+    rng = np.random.default_rng(52)
+    n = int(np.prod(shape))
+    x = rng.uniform(0.0, 1.0, n)
+    q = rng.normal(0.0, 0.3, (3, n))
+    rhs = rng.normal(0.0, 1.0, n)
+    q_ref, rhs_ref = ref_cl.proxtv_step(x, q, rhs, shape, 0.7, 0.25, l2, diff_type, exact_inputs=True)
+    ours = io.proxtv_dual(x, q, shape, 0.7, 0.25, l2, diff_type)
+    assert np.abs(ours - q_ref).max() <= 1e-13 * np.abs(q_ref).max()
+    r = rhs - io.proxtv_divergence(ours, shape, diff_type)
+    assert np.abs(r - rhs_ref).max() <= 1e-13 * np.abs(rhs_ref).max()
+    # the projection changed some voxels
+    raw = q + 0.7 * np.stack([io._diff(x.reshape(shape, order='F'), a, diff_type == 0).ravel(order='F')
+                              for a in range(3)])
+    assert np.count_nonzero(np.abs(raw - ours).max(axis=0) > 1e-12) > n // 10
+
+
+def test_pdhg_proxtv_iteration_pinned():
+    """Two PDHG iterations with the proximal TV (oracle.pdhg_tv(prox=...))
+    against the same loop built from the reference's kernels: the type-5
+    projector pair, ProxTVGradient / ProxTVq / ProxTVDivergence and
+    PDHGUpdate."""
+    o = _proj("ct_fine5")
+    g = orc.Geometry(o)
+    R = ref_cl.RefCT(o, exact_inputs=True)
+    shape = (g.nx, g.ny, g.nz)
+    rng = np.random.default_rng(53)
+    truth = rng.uniform(0.0, 0.02, g.n_img)
+    y = orc.bdd_forward(g, truth, -1)
+    x0 = np.full(g.n_img, 1e-3)
+    tau, beta, sigma, sigma2 = 1e-4, 0.01, 1.0, 0.5
+    ours = orc.pdhg_tv(g, y, x0, 2, tau, beta, 1e-4, sigma=sigma, prox=dict(sigma2=sigma2, l2=True, diff_type=0))
+    x, u = x0.copy(), x0.copy()
+    p = np.zeros(g.rays(-1))
+    q = np.zeros((3, g.n_img))
+    for _ in range(2):
+        p = (p + sigma * (R.bdd_forward(x, -1) - y)) / (1.0 + sigma)
+        rhs = R.bdd_backward(p, -1)
+        q, rhs = ref_cl.proxtv_step(x, q, rhs, shape, sigma2, beta, True, 0, exact_inputs=True)
+        x, u = ref_cl.pdhg_update(x, rhs, u, shape, tau, 1.0, 1e-5, exact_inputs=True)
+    assert orc.rel_l2(ours, x) < PIN
