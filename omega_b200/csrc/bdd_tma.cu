@@ -201,7 +201,31 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
             // (0.99: margin for rounding), so each column crosses at most one
             // new row -- straight-line code, no loops.
             const bool staged = i0 >= o.x && i0 + seg.n < o.x + kBW && kc >= o.y && k_end < o.y + kBZ;
-            if (staged && seg.n <= 2 && w < 0.99f) {
+            if (staged && seg.n <= 2 && w < 0.99f && zu >= 0.f && fmaf(8.f, w, zu) < fz) {
+                // the same, with the run inside the volume: the clamps of the
+                // column edges to [0, nz] and of the row to nz - 1 are identities
+                const float *q = sh.box[s] + (kc - o.y) * kBW + (i0 - o.x);
+                const float *q1 = q + seg.o1, *q2 = q + seg.o2;
+                float R = fmaf(seg.w2, *q2, fmaf(seg.w1, *q1, seg.w0 * q[0]));
+                float S = 0.f;
+                float Cprev = (bz - (float)kc) * R;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    bz = fmaf((float)(c + 1), w, zu);
+                    const int kn = (int)bz;
+                    if (kc < kn) {
+                        S += R;
+                        ++kc;
+                        q += kBW;
+                        q1 += kBW;
+                        q2 += kBW;
+                        R = fmaf(seg.w2, *q2, fmaf(seg.w1, *q1, seg.w0 * q[0]));
+                    }
+                    const float C = fmaf(bz - (float)kc, R, S);
+                    temp[c] = fmaf(C - Cprev, inv_area, temp[c]);
+                    Cprev = C;
+                }
+            } else if (staged && seg.n <= 2 && w < 0.99f) {
                 const float *q = sh.box[s] + (kc - o.y) * kBW + (i0 - o.x);
                 float R = fmaf(seg.w2, q[seg.o2], fmaf(seg.w1, q[seg.o1], seg.w0 * q[0]));
                 float S = 0.f;

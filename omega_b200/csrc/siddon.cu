@@ -150,16 +150,32 @@ __global__ void __launch_bounds__(kBlock) k_siddon_bp_ilv(Grid g, RaySet rs, flo
     y += f0 * y_stride;
     float4 *im = reinterpret_cast<float4 *>(img + (int64_t)blockIdx.y * n_img * FB);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.m_size; r += stride) {
+    // the next ray's measurements and end points are loaded before this
+    // ray's walk, so their latency hides behind it
+    int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float axn[FB];
+    Ray rayn{};
+    if (r < rs.m_size) {
+#pragma unroll
+        for (int f = 0; f < FB; ++f) axn[f] = f < nf ? __ldg(y + f * y_stride + r) : 0.f;
+        rayn = load_ray(rs, r);
+    }
+    for (; r < rs.m_size; r += stride) {
         float ax[FB];
         bool any = false;
 #pragma unroll
         for (int f = 0; f < FB; ++f) {
-            ax[f] = f < nf ? __ldg(y + f * y_stride + r) : 0.f;
+            ax[f] = axn[f];
             any |= ax[f] != 0.f;
         }
+        const Ray ray = rayn;
+        const int64_t rn = r + stride;
+        if (rn < rs.m_size) {
+#pragma unroll
+            for (int f = 0; f < FB; ++f) axn[f] = f < nf ? __ldg(y + f * y_stride + rn) : 0.f;
+            rayn = load_ray(rs, rn);
+        }
         if (!any) continue;  // adds only zeros
-        const Ray ray = load_ray(rs, r);
         const float gfr = pet && (rs.w || rs.mu) ? gf * ray_correction(g, rs, ray, r) : gf;
         float temp = 0.f;
         siddon_walk<1>(g, ray, pet, gfr, tof, temp, [&](int64_t ind, float ele, const float *, float) {

@@ -55,10 +55,20 @@ __device__ __forceinline__ Ray load_ray(const RaySet &rs, int64_t r) {
     int64_t ix, iy, iz;
     if (rs.stype == 0) {
         const int64_t nbin = (int64_t)rs.n_rows * rs.n_cols;
-        iz = r / nbin;
-        const int64_t b = r - iz * nbin;
-        iy = b / rs.n_rows;
-        ix = b - iy * rs.n_rows;
+        if (r <= 0x7fffffff && nbin <= 0x7fffffff) {
+            // 32-bit division (the 64-bit one is a long software routine)
+            const unsigned ru = (unsigned)r, nb = (unsigned)nbin;
+            const unsigned z32 = ru / nb, b = ru - z32 * nb;
+            const unsigned y32 = b / (unsigned)rs.n_rows;
+            iz = z32;
+            iy = y32;
+            ix = b - y32 * (unsigned)rs.n_rows;
+        } else {
+            iz = r / nbin;
+            const int64_t b = r - iz * nbin;
+            iy = b / rs.n_rows;
+            ix = b - iy * rs.n_rows;
+        }
         iz += rs.proj0;
     } else {
         // Measurement-level subsets (general_opencl_functions.h:914-940):
