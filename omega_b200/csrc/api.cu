@@ -1163,8 +1163,8 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
     }
     if (e == cudaSuccess && st == OMB_OK && h->desc.fp_type == 5) {
         float best_ms = 3.4e38f;
-        // (columns, warps per block, staged); the staged kernel has 8 columns and 4 warps
-        const int shapes[5][3] = {{8, 4, 0}, {8, 8, 0}, {16, 4, 0}, {16, 8, 0}, {8, 4, 1}};
+        // (columns, warps per block, staged); the staged kernel has 8 or 16 columns per thread, 32 per CTA
+        const int shapes[6][3] = {{8, 4, 0}, {8, 8, 0}, {16, 4, 0}, {16, 8, 0}, {8, 4, 1}, {16, 4, 1}};
         for (const auto &sh : shapes) {
             h->tune = best;
             h->tune.bdd_fp_cols = sh[0];

@@ -405,8 +405,8 @@ int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc,
     dim3 tg((g.nx + 31) / 32, (g.ny + 31) / 32, g.nz);
     k_transpose_xy<<<tg, dim3(32, 8), 0, st>>>(img, imgT, g.nx, g.ny, g.nz);
     OMB_LAUNCH_CHECK("transpose launch");
-    if (tn.bdd_fp_staged && tn.bdd_fp_cols == 8 && bdd_fp_tma_supported(g, img, imgT))
-        return bdd_forward_tma(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, st);
+    if (tn.bdd_fp_staged && (tn.bdd_fp_cols == 8 || tn.bdd_fp_cols == 16) && bdd_fp_tma_supported(g, img, imgT))
+        return bdd_forward_tma(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, tn.bdd_fp_cols, st);
     switch (tn.bdd_fp_cols) {
         case 16: launch_fp<16>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, tn.bdd_fp_rows, st); break;
         default: launch_fp<8>(g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y, tn.bdd_fp_rows, st); break;

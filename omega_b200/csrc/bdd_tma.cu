@@ -34,7 +34,7 @@ namespace bt {
 constexpr int kBW = 40;       // lateral voxels of a staged box (x multiple of 4: 16-byte aligned starts)
 constexpr int kBZ = 36;       // voxel rows (z) of a staged box
 constexpr int kStages = 4;    // ring depth
-constexpr int kRB = 4;        // warps per CTA = groups of 8 columns
+constexpr int kCTACols = 32;  // detector columns of a CTA (kCTACols / C warps of C-column groups)
 constexpr int kBoxFloats = kBW * kBZ;
 constexpr int kWaitTries = 1 << 22;
 constexpr int kWaitTriesAfterFailure = 64;
@@ -91,26 +91,29 @@ __device__ __forceinline__ int2 slice_box(const Shared &sh, int j, int nlat, int
 
 }  // namespace bt
 
+template <int C>
 __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const __grid_constant__ CUtensorMap map_imgT,
                              Grid g, const float *__restrict__ xy, const float *__restrict__ uv, int nr, int nc,
                              float pitch_y, int64_t proj0, int64_t nproj, const float *__restrict__ img,
                              const float *__restrict__ imgT, float *__restrict__ y) {
     using namespace bt;
+    constexpr int kRB = kCTACols / C;  // warps per CTA
+    constexpr float kC = (float)C;
     __shared__ Shared sh;
     const int tid = threadIdx.x + threadIdx.y * 32;
     const int r = blockIdx.x * 32 + threadIdx.x;
     const int cg = blockIdx.y * kRB + threadIdx.y;
     const int64_t p = blockIdx.z;
-    const int c0 = cg * 8;
+    const int c0 = cg * C;
     const bool active = r < nr && c0 < nc && p < nproj;
-    const int n_groups = (nc + 7) / 8;
+    const int n_groups = (nc + C - 1) / C;
 
     // corner rays: first/last active row x first/last active column group
     if (tid < 4) {
         const int r_last = min(blockIdx.x * 32 + 31, nr - 1);
         const int g_last = min((int)blockIdx.y * kRB + kRB - 1, n_groups - 1);
         const int rr = (tid & 1) ? r_last : (int)blockIdx.x * 32;
-        const int cc = ((tid & 2) ? g_last : (int)blockIdx.y * kRB) * 8;
+        const int cc = ((tid & 2) ? g_last : (int)blockIdx.y * kRB) * C;
         const BddRay b = bdd_ray_setup(g, xy, uv, proj0 + p, rr, cc, nr, nc, pitch_y);
         sh.corner[tid] = Corner{b.xa0, b.xa1, b.xb0, b.xb1, b.za0, b.za1, b.zb0, b.zb1, b.dz0, b.dz1};
         if (tid == 0) {
@@ -133,7 +136,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
         SliceRange range = slice_range_empty();
         for (int q = 0; q < 4; ++q) {
             const Corner &c = sh.corner[q];
-            slice_range_add(range, c.xa0, c.xa1, c.xb0, c.xb1, c.za0, c.za1, c.zb0, c.zb1, nsl, nlat, g.nz, 8.f);
+            slice_range_add(range, c.xa0, c.xa1, c.xb0, c.xb1, c.za0, c.za1, c.zb0, c.zb1, nsl, nlat, g.nz, kC);
         }
         sh.slices = slice_range_bounds(range);
     }
@@ -158,19 +161,21 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
         for (int s = 0; s < kStages && j_lo + s <= j_hi; ++s) issue(j_lo + s, s);
 
     BddRay b{};
-    float kerroin = 0.f;
+    float kerroin = 0.f, kerroin8 = 0.f;
     if (active) {
         b = bdd_ray_setup(g, xy, uv, proj0 + p, r, c0, nr, nc, pitch_y);
         kerroin = b.kerroin;
+        // the weight belongs to groups of 8 columns (projectorType5.cl:166-174)
+        if (C > 8 && c0 + 8 < nc) kerroin8 = bdd_kerroin(g, xy, uv, proj0 + p, r, c0 + 8, nr, nc, pitch_y, b.ysl);
     }
     const int64_t z_stride = (int64_t)g.nx * g.ny;
     const float *__restrict__ vol = ysl ? img : imgT;
     const float flat = (float)nlat, fz = (float)g.nz;
     const float dlat = ysl ? g.dx : g.dy;
     const int zmax = g.nz - 1;
-    float temp[8];
+    float temp[C];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) temp[c] = 0.f;
+    for (int c = 0; c < C; ++c) temp[c] = 0.f;
     int tries = kWaitTries;
 
     for (int j = j_lo; j <= j_hi; ++j) {
@@ -188,20 +193,20 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
         const float w = fabsf(fmaf(fj, b.dz1, b.dz0));
         const float cl = fmaxf(el, 0.f), cr = fminf(er, flat);
         // a run of columns wholly above or below the volume integrates to zero
-        if (active && cr > cl && zu < fz && fmaf(8.f, w, zu) > 0.f) {
+        if (active && cr > cl && zu < fz && fmaf(kC, w, zu) > 0.f) {
             const float inv_area = 1.f / (fabsf(fmaf(fj, b.dw1, b.dw0)) * dlat * w * g.dz);
             const int i0 = (int)cl;
             const Seg seg = make_seg(cl, cr, i0, min((int)ceilf(cr), nlat) - 1 - i0);
             float bz = fminf(fmaxf(zu, 0.f), fz);
             int kc = min((int)bz, zmax);
-            const int k_end = min((int)fminf(fmaxf(fmaf(8.f, w, zu), 0.f), fz), zmax);
+            const int k_end = min((int)fminf(fmaxf(fmaf(kC, w, zu), 0.f), fz), zmax);
             const int2 o = sh.origin[s];
             // Fast path: the run lies in the staged box, spans at most 3
             // voxels (no tail loop) and a column is narrower than a voxel row
             // (0.99: margin for rounding), so each column crosses at most one
             // new row -- straight-line code, no loops.
             const bool staged = i0 >= o.x && i0 + seg.n < o.x + kBW && kc >= o.y && k_end < o.y + kBZ;
-            if (staged && seg.n <= 2 && w < 0.99f && zu >= 0.f && fmaf(8.f, w, zu) < fz) {
+            if (staged && seg.n <= 2 && w < 0.99f && zu >= 0.f && fmaf(kC, w, zu) < fz) {
                 // the same, with the run inside the volume: the clamps of the
                 // column edges to [0, nz] and of the row to nz - 1 are identities
                 const float *q = sh.box[s] + (kc - o.y) * kBW + (i0 - o.x);
@@ -210,7 +215,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
                 float S = 0.f;
                 float Cprev = (bz - (float)kc) * R;
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
+                for (int c = 0; c < C; ++c) {
                     bz = fmaf((float)(c + 1), w, zu);
                     const int kn = (int)bz;
                     if (kc < kn) {
@@ -231,7 +236,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
                 float S = 0.f;
                 float Cprev = (bz - (float)kc) * R;
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
+                for (int c = 0; c < C; ++c) {
                     bz = fminf(fmaxf(fmaf((float)(c + 1), w, zu), 0.f), fz);
                     const int kn = min((int)bz, zmax);
                     if (kc < kn) {
@@ -253,7 +258,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
                 float S = 0.f;
                 float Cprev = (bz - (float)kc) * R;
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
+                for (int c = 0; c < C; ++c) {
                     bz = fminf(fmaxf(fmaf((float)(c + 1), w, zu), 0.f), fz);
                     const int kn = min((int)bz, zmax);
                     while (kc < kn) {
@@ -271,11 +276,11 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
         if (threadIdx.x == 0 && threadIdx.y == t % kRB && j + kStages <= j_hi) issue(j + kStages, s);
     }
     if (!active) return;
-    const int ncol = min(8, nc - c0);
+    const int ncol = min(C, nc - c0);
     const int64_t idx = r + (int64_t)c0 * nr + p * (int64_t)nr * nc;
 #pragma unroll
-    for (int c = 0; c < 8; ++c)
-        if (c < ncol) y[idx + (int64_t)c * nr] = temp[c] * kerroin;
+    for (int c = 0; c < C; ++c)
+        if (c < ncol) y[idx + (int64_t)c * nr] = temp[c] * (c < 8 ? kerroin : kerroin8);
 }
 
 // ---------------------------------------------------------------------------
@@ -525,14 +530,19 @@ bool bdd_fp_tma_supported(const Grid &g, const float *img, const float *imgT) {
 }
 
 int bdd_forward_tma(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
-                    int64_t nproj, const float *img, const float *imgT, float *y, cudaStream_t st) {
+                    int64_t nproj, const float *img, const float *imgT, float *y, int cols, cudaStream_t st) {
     CUtensorMap m_img, m_imgT;
     if (!encode_volume(m_img, img, g.nx, g.ny, g.nz) || !encode_volume(m_imgT, imgT, g.ny, g.nx, g.nz))
         return set_error(OMB_ERR_CUDA, "cuTensorMapEncodeTiled failed for the type-5 image maps");
-    const int groups = (nc + 7) / 8;
-    dim3 block(32, bt::kRB);
-    dim3 grid((nr + 31) / 32, (groups + bt::kRB - 1) / bt::kRB, (unsigned)nproj);
-    k_bdd_fp_tma<<<grid, block, 0, st>>>(m_img, m_imgT, g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y);
+    const int C = cols == 16 ? 16 : 8;
+    const int rb = bt::kCTACols / C;
+    const int groups = (nc + C - 1) / C;
+    dim3 block(32, rb);
+    dim3 grid((nr + 31) / 32, (groups + rb - 1) / rb, (unsigned)nproj);
+    if (C == 16)
+        k_bdd_fp_tma<16><<<grid, block, 0, st>>>(m_img, m_imgT, g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y);
+    else
+        k_bdd_fp_tma<8><<<grid, block, 0, st>>>(m_img, m_imgT, g, xy, uv, nr, nc, pitch_y, proj0, nproj, img, imgT, y);
     OMB_LAUNCH_CHECK("type-5 TMA forward launch");
     return OMB_OK;
 }

@@ -93,10 +93,11 @@ int multiray_backward(const Grid &g, const RaySet &rs, const Tof &tof, float gf,
 // Projector type 5 (branchless distance-driven), CT.
 int bdd_forward(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
                 int64_t nproj, const float *img, float *imgT, float *y, const Tuning &tn, cudaStream_t st);
-// The same projection with per-slice image boxes staged by TMA (8 columns per thread).
+// The same projection with per-slice image boxes staged by TMA (cols = 8 or 16 columns per thread; the same
+// numbers as bdd_forward with bdd_fp_cols = cols).
 bool bdd_fp_tma_supported(const Grid &g, const float *img, const float *imgT);
 int bdd_forward_tma(const Grid &g, const float *xy, const float *uv, int nr, int nc, float pitch_y, int64_t proj0,
-                    int64_t nproj, const float *img, const float *imgT, float *y, cudaStream_t st);
+                    int64_t nproj, const float *img, const float *imgT, float *y, int cols, cudaStream_t st);
 // Device error word of the bounded waits (1 after a wait ran out; reset when read), < 0 on failure.
 int take_device_error();
 int bdd_backward(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj, const float *y,

@@ -35,7 +35,7 @@ def test_bdd_every_shape_matches_oracle(cuda, name):
     ref_bp, ref_s = orc.bdd_backward(g, y, 0, sens=True)
     from omega_b200 import _native
     shapes = [(c, z, r, 0) for c, z, r in itertools.product([8, 16], [4, 8, 16], [4, 8])]
-    shapes += [(8, z, 4, 1) for z in (4, 8, 16)]
+    shapes += [(8, z, 4, 1) for z in (4, 8, 16)] + [(16, 16, 4, 1)]
     fps, bps = {}, {}
     for cols, zrun, rows, staged in shapes:
         o.tuning = {"bdd_fp_columns": cols, "bdd_bp_zrun": zrun, "bdd_fp_block_rows": rows,
@@ -50,7 +50,8 @@ def test_bdd_every_shape_matches_oracle(cuda, name):
     assert _native.call("omb_take_device_error") == 0
     # staging the image / detector boxes in shared memory changes where the
     # data are read from, not the arithmetic
-    assert np.array_equal(fps[(8, 4, 1)].view(np.uint32), fps[(8, 4, 0)].view(np.uint32))
+    for c in (8, 16):
+        assert np.array_equal(fps[(c, 4, 1)].view(np.uint32), fps[(c, 4, 0)].view(np.uint32)), c
     for z in (8, 16):
         for a, b in zip(bps[(z, 4, 1)], bps[(z, 4, 0)]):
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), z
