@@ -274,8 +274,16 @@ typedef struct omb_tuning {
                                         with bdd_fp_columns = 8; needs Nx, Ny multiples of 4) */
     int32_t bdd_bp_staged;           /* 0, 1 (default 1): type-5 backprojection with each CTA's
                                         per-projection detector boxes staged in shared memory by TMA
-                                        (applies with bdd_bp_zrun = 8; needs a row count that is a
+                                        (applies with bdd_bp_zrun = 8 or 16; needs a row count that is a
                                         multiple of 4) */
+    int32_t siddon_bp_matrix;        /* 0, 1 (default 0): type-1 non-TOF backprojections of measurements
+                                        through a transposed system matrix kept on the handle (per subset:
+                                        for every voxel the weights of the rays crossing it, 8 bytes a
+                                        crossing), built by the first such call on a subset (that call
+                                        synchronises its stream and must not be captured into a CUDA
+                                        graph); one thread per voxel, no atomics, the sums in ray order:
+                                        bit-identical call to call.  Sensitivity images keep the
+                                        ray-driven kernels */
 } omb_tuning;
 
 /*

@@ -171,6 +171,7 @@ class Tuning(ctypes.Structure):
         ("siddon_fp_steps", ctypes.c_int32),
         ("bdd_fp_staged", ctypes.c_int32),
         ("bdd_bp_staged", ctypes.c_int32),
+        ("siddon_bp_matrix", ctypes.c_int32),
     ]
 
     def as_dict(self):

@@ -47,6 +47,9 @@ struct omb_handle {
     int read_mode = OMB_READ_FP32;        // image precision of the type-1/4 forward projections
     __nv_bfloat16 *d_img16 = nullptr;     // BF16 image copies (read_mode == OMB_READ_BF16)
     int img16_frames = 0;                 // frames d_img16 holds
+    std::vector<SysMat> sysmats;          // type-1 transposed system matrices, one per subset used
+    float *d_ym = nullptr;                // ray-major measurement scratch of the system-matrix backprojection
+    int64_t ym_floats = 0;
     float *d_ilv = nullptr;               // voxel-interleaved frame scratch (type-1 frame batches)
     int64_t ilv_floats = 0;               // its capacity
     float *d_w = nullptr;                 // PET: multiplicative weight per measurement (all subsets), or NULL
@@ -405,6 +408,34 @@ static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, fl
         }
         return OMB_OK;
     }
+    if (h->tune.siddon_bp_matrix && h->tof.nbins == 1 && !sens && f.meas && f.img) {
+        // the subset's transposed system matrix, built by its first call
+        SysMat *sm = nullptr;
+        for (auto &x : h->sysmats)
+            if (x.proj0 == rs.proj0 && x.m_size == rs.m_size && x.cur_subset == rs.cur_subset) sm = &x;
+        if (!sm) {
+            SysMat nm;
+            if (sysmat_build(h->grid, rs, h->desc.global_factor, nm, s) != OMB_OK) return -1;
+            h->sysmats.push_back(nm);
+            sm = &h->sysmats.back();
+        }
+        const int fb = f.n >= 8 ? 8 : (f.n >= 4 ? 4 : 1);
+        if (fb > 1 && (int64_t)fb * rs.m_size > h->ym_floats) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+                return set_error(OMB_ERR_INVALID, "the system-matrix backprojection scratch grows on a call outside "
+                                                  "CUDA-graph capture (run one call first)");
+            float *p = nullptr;
+            if (cudaMalloc(&p, (size_t)fb * rs.m_size * sizeof(float)) != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(OMB_ERR_CUDA, "allocating the system-matrix backprojection scratch failed");
+            }
+            if (h->d_ym) h->retired.push_back(h->d_ym);
+            h->d_ym = p;
+            h->ym_floats = (int64_t)fb * rs.m_size;
+        }
+        return sysmat_backward(h->grid, *sm, f, rs.m_size, h->d_ym, h->ym_floats, s);
+    }
     if (!sens && f.meas && f.img) attach_interleave(h, f, s);
     return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, sens, h->tune, s);
 }
@@ -553,6 +584,8 @@ int omb_destroy(omb_handle *h) {
     cudaFree(h->d_mu);
     cudaFree(h->d_rand);
     cudaFree(h->d_vol);
+    for (auto &m : h->sysmats) sysmat_free(m);
+    cudaFree(h->d_ym);
     for (void *p : h->retired) cudaFree(p);
     if (prev != h->device) cudaSetDevice(prev);
     delete h;
@@ -959,6 +992,7 @@ static int tuning_from(const omb_tuning *in, Tuning &t) {
     if (!one_of(in->siddon_fp_steps, {1, 2, 4})) return set_error(OMB_ERR_INVALID, "siddon_fp_steps must be 1, 2 or 4");
     if (!one_of(in->bdd_fp_staged, {0, 1}) || !one_of(in->bdd_bp_staged, {0, 1}))
         return set_error(OMB_ERR_INVALID, "bdd_fp_staged and bdd_bp_staged must be 0 or 1");
+    if (!one_of(in->siddon_bp_matrix, {0, 1})) return set_error(OMB_ERR_INVALID, "siddon_bp_matrix must be 0 or 1");
     t.siddon_blocks_per_sm = in->siddon_blocks_per_sm;
     t.siddon_frames = in->siddon_frames_per_walk;
     t.bdd_fp_cols = in->bdd_fp_columns;
@@ -969,6 +1003,7 @@ static int tuning_from(const omb_tuning *in, Tuning &t) {
     t.siddon_fp_steps = in->siddon_fp_steps;
     t.bdd_fp_staged = in->bdd_fp_staged;
     t.bdd_bp_staged = in->bdd_bp_staged;
+    t.siddon_bp_matrix = in->siddon_bp_matrix;
     return OMB_OK;
 }
 
@@ -984,10 +1019,20 @@ static void tuning_to(const Tuning &t, omb_tuning *out) {
     out->siddon_fp_steps = t.siddon_fp_steps;
     out->bdd_fp_staged = t.bdd_fp_staged;
     out->bdd_bp_staged = t.bdd_bp_staged;
+    out->siddon_bp_matrix = t.siddon_bp_matrix;
 }
 
 int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weights, const float *atten_image,
                         int64_t n_atten, void *stream) {
+    // the system matrices fold the corrections into their weights (retired,
+    // not freed: a captured graph may still address them)
+    if (h) {
+        for (auto &m : h->sysmats) {
+            h->retired.push_back(m.off);
+            h->retired.push_back(m.ent);
+        }
+        h->sysmats.clear();
+    }
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
     if ((meas_weights || atten_image) && h->desc.modality == OMB_CT_PANEL)
         return set_error(OMB_ERR_UNSUPPORTED, "corrections apply to PET data");
@@ -1159,6 +1204,30 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
                 best_ms = a;
                 best.siddon_fp_steps = k;
             }
+        }
+    }
+    // then the type-1 non-TOF backprojection through the resident transposed
+    // system matrix, when its 8 bytes a crossing fit in half the free memory
+    if (e == cudaSuccess && st == OMB_OK && h->desc.bp_type == 1 && h->desc.tof_bins == 1 &&
+        h->desc.n_rays_xy * h->desc.n_rays_z <= 1) {
+        int64_t crossings = 0;
+        size_t free_b = 0, total_b = 0;
+        if (omb_intersection_count(h, -1, &crossings, stream) == OMB_OK && cudaStreamSynchronize(s) == cudaSuccess &&
+            cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+            (double)crossings * 8.0 + 8.0 * (double)m * 4.0 < 0.5 * (double)free_b) {
+            h->tune = best;
+            h->tune.siddon_bp_matrix = 0;
+            const float b0 = timed(bwd);
+            h->tune.siddon_bp_matrix = 1;
+            const float b1 = timed(bwd);
+            if (b0 < 0.f || b1 < 0.f) st = -1;
+            else best.siddon_bp_matrix = b1 < b0 ? 1 : 0;
+            if (!best.siddon_bp_matrix) {
+                for (auto &x : h->sysmats) sysmat_free(x);
+                h->sysmats.clear();
+            }
+        } else {
+            cudaGetLastError();
         }
     }
     if (e == cudaSuccess && st == OMB_OK && h->desc.fp_type == 5) {

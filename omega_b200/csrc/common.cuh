@@ -197,7 +197,8 @@ struct Tuning {
     int siddon_layout = 1;          // frame batches: 0 = frame-major reads/atomics, 1 = voxel-interleaved
     int siddon_fp_steps = 4;        // non-TOF forward walks: crossings gathered per batched step (1, 2, 4)
     int bdd_fp_staged = 1;          // type-5 forward: image boxes staged by TMA (with 8 columns per thread)
-    int bdd_bp_staged = 1;          // type-5 backward: detector boxes staged by TMA (with 8 voxels per thread)
+    int bdd_bp_staged = 1;          // type-5 backward: detector boxes staged by TMA (with 8 or 16 voxels per thread)
+    int siddon_bp_matrix = 0;       // type-1 non-TOF backprojection through a resident transposed system matrix
 };
 
 // Read-only image load as float from an FP32 or BF16 array.

@@ -114,6 +114,24 @@ bool bdd_bp_tma_supported(int nr, const float *y);
 int bdd_backward_tma(const Grid &g, const BddProj *pj, const BddMap64 *pm, int nr, int nc, int64_t nproj,
                      const float *y, float *img, float *sens, int kz, cudaStream_t st);
 
+// Resident transposed system matrix of the type-1 non-TOF projector for one subset (sysmat.cu): for each
+// voxel the (ray, weight) pairs of the rays crossing it, in ray order; off[v] .. off[v + 1] index ent.
+struct SysMat {
+    int64_t proj0 = 0, m_size = 0;
+    int cur_subset = 0;
+    int64_t *off = nullptr;
+    uint2 *ent = nullptr;  // (launch-local ray index, weight bits)
+    int64_t nnz = 0;
+};
+// Builds sm for the rays of rs (the walk and weights of the ray-driven backprojection); synchronises `st`
+// and refuses to run while `st` is captured into a CUDA graph.
+int sysmat_build(const Grid &g, const RaySet &rs, float gf, SysMat &sm, cudaStream_t st);
+void sysmat_free(SysMat &sm);
+// Backprojection of fr.n frames through sm (images overwritten); ym: ray-major scratch of at least
+// 8 * m floats (4 * m for 4..7 frames; unused for fewer).
+int sysmat_backward(const Grid &g, const SysMat &sm, const Frames &fr, int64_t m, float *ym, int64_t ym_floats,
+                    cudaStream_t st);
+
 // Projector type 4 (interpolation), PET and CT.
 int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img,
                    const __nv_bfloat16 *img16, float *y, const Tuning &tn, cudaStream_t st);

@@ -233,3 +233,66 @@ def test_intersection_count_matches_oracle(cuda):
                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     ref = orc.intersections(g, 1)
     assert abs(n.value - ref) <= 1e-4 * ref
+
+
+@pytest.mark.parametrize("name", ["pet_mini", "pet_stype1", "pet_stype4", "pet_odd_span1"])
+def test_system_matrix_backprojection(cuda, name):
+    """Backprojections through the resident transposed system matrix
+    (siddon_bp_matrix = 1) against the FP64 oracle and the ray-driven
+    atomics, for every subset, frame batches of 1, 5 (4 + 1) and 11 (8 + 3)
+    frames, and bit-identical call to call."""
+    import ctypes
+
+    import torch
+    from omega_b200 import _native
+    o = _init(name)
+    g = orc.Geometry(o)
+    n = int(o.N[0])
+    rng = np.random.default_rng(7)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for s in range(g.n_subsets):
+        m = o.measurementCount(s)
+        for nf in (1, 5, 11):
+            ys = _t(rng.uniform(0.0, 2.0, (nf, m)), cuda)
+            outs = []
+            for mat in (0, 1, 1):
+                o.tuning = {"siddon_bp_matrix": mat}
+                back = torch.empty((nf, n), device=cuda)
+                _native.call("omb_backward_frames", o._handle, s, nf, ctypes.c_void_p(ys.data_ptr()), m,
+                             ctypes.c_void_p(back.data_ptr()), n, st)
+                outs.append(back.cpu().numpy())
+            assert np.array_equal(outs[1].view(np.uint32), outs[2].view(np.uint32))
+            for f in range(nf):
+                assert orc.rel_l2(outs[1][f], outs[0][f]) < 1e-6, (s, nf, f)
+            ref = orc.backward(g, ys[nf - 1].cpu().numpy().astype(np.float64), s)
+            assert orc.rel_l2(outs[1][nf - 1], ref) < TOL
+
+
+def test_system_matrix_backprojection_with_corrections(cuda):
+    """Corrections set after a matrix was built replace it (the weights fold
+    them in): the backprojection follows the new corrections."""
+    import ctypes
+
+    import torch
+    from omega_b200 import _native
+    o = _init("pet_mini")
+    g = orc.Geometry(o)
+    n = int(o.N[0])
+    m = o.measurementCount(-1)
+    rng = np.random.default_rng(8)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    y = _t(rng.uniform(0.0, 2.0, m), cuda)
+
+    def bp(mat):
+        o.tuning = {"siddon_bp_matrix": mat}
+        b = torch.empty(n, device=cuda)
+        _native.call("omb_backward", o._handle, -1, ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(b.data_ptr()),
+                     None, 0, st)
+        return b.cpu().numpy()
+    plain = bp(1)
+    n_all = o.measurementCount(-1)
+    w = rng.uniform(0.5, 1.5, n_all).astype(np.float32)
+    _native.call("omb_set_corrections", o._handle, w.ctypes.data_as(ctypes.c_void_p), w.size, None, 0, None)
+    corr = bp(1)
+    assert orc.rel_l2(corr, bp(0)) < 1e-6
+    assert orc.rel_l2(corr, plain) > 1e-3
