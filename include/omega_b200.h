@@ -371,7 +371,8 @@ typedef struct omb_recon_params {
     int32_t nlm_adaptive;     /* options.NLAdaptive */
     float nlm_adaptive_s;     /* options.NLAdaptiveConstant */
     int32_t precond;          /* PKMA / MRAMLA / MBSREM image preconditioner: 0 none, 1 type 0 (rhs / D), 2 type 1
-                                 (rhs * x / D), see omb_precond_image */
+                                 (rhs * x / D), 3 type 2 (rhs * max(x, max(1e-5, precond_ref)) / D), see
+                                 omb_precond_image */
     int32_t mrp_no_norm;      /* MRP: options.med_no_norm */
     const float *ggmrf_weights;/* GGMRF: device, the neighbours' weights (centre left out, z fastest) */
     const float *hyper_weights;/* hyperbolic: device, options.weights_quad (centre left out, x fastest) */
@@ -393,7 +394,22 @@ typedef struct omb_recon_params {
                                  gradient */
     float sigma2;             /* PDHG with proximal TV: the TV dual step (options.sigma2CP) */
     int32_t l2_ball;          /* PDHG with proximal TV: options.useL2Ball (1: L2 ball, 0: max-norm ball) */
-    int32_t diff_type;        /* PDHG with proximal TV: options.derivativeType (0 forward, 1 backward differences) */
+    int32_t diff_type;        /* options.derivativeType: PDHG with proximal TV (0 forward, 1 backward
+                                 differences) and the gradient image preconditioner (0, 1, or 2 central) */
+    const float *precond_ref; /* PKMA / MRAMLA / MBSREM, precond = 3 (options.precondTypeImage[2]): device
+                                 reference image (options.referenceImage) */
+    const float *precond_alpha;/* PKMA / MRAMLA / MBSREM, options.precondTypeImage[3]: host, n_iter * n_subsets
+                                 values (options.alphaPrecond) the gradient is multiplied by, or NULL */
+    int32_t precond_grad;     /* options.precondTypeImage[4]: gradient-based preconditioner (functions.hpp:
+                                 2036-2054), recomputed in sub-iterations grad_iters[0] .. grad_iters[1] and
+                                 applied from grad_iters[0] on */
+    float grad_v[2];          /* options.gradV1, gradV2: its bounds */
+    int32_t grad_iters[2];    /* options.gradInitIter, gradLastIter (sub-iteration counts) */
+    int32_t precond_curv;     /* options.precondTypeImage[6]: curvature preconditioner dP = sum over the
+                                 subsets of S / A_s^T (A_s 1 / y_s) (reconstructionAF.h:600-650) */
+    int32_t precond_meas;     /* options.precondTypeMeas[0]: the ratio divided by A_s 1 (zeros -> 1) */
+    int32_t pkma_relax;       /* PKMA: bit 0 options.computeRelaxationParameters (lam from the norms of the
+                                 image and the gradient, algorithms.h:155-187), bit 1 options.relaxationScaling */
 } omb_recon_params;
 
 /*

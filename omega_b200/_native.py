@@ -132,6 +132,14 @@ class ReconParams(ctypes.Structure):
         ("sigma2", ctypes.c_float),
         ("l2_ball", ctypes.c_int32),
         ("diff_type", ctypes.c_int32),
+        ("precond_ref", ctypes.c_void_p),
+        ("precond_alpha", ctypes.c_void_p),
+        ("precond_grad", ctypes.c_int32),
+        ("grad_v", ctypes.c_float * 2),
+        ("grad_iters", ctypes.c_int32 * 2),
+        ("precond_curv", ctypes.c_int32),
+        ("precond_meas", ctypes.c_int32),
+        ("pkma_relax", ctypes.c_int32),
     ]
 
 

@@ -824,9 +824,35 @@ int relaxed_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
     st = ratio_shift(y_subset, work_meas, m, h->d_rand ? h->d_rand + subset_ray0(h, rs, subset) : nullptr,
                      rs.m_size, eps, shift, sign, s);
     if (st != OMB_OK) return st;
+    // measurement preconditioner type 0: the ratio over A 1 (computeForwardProject.h:149, 183;
+    // functions.hpp:2156-2166)
+    if (a.meas_m && (st = div_inplace(work_meas, a.meas_m, m, s)) != OMB_OK) return st;
     OMB_CUDA_TRY(cudaMemsetAsync(work_img, 0, h->n_img * sizeof(float), s));
     st = rays_backward(h, rs, one_frame_bp(h, work_meas, work_img, rs.m_size), nullptr, s);
     if (st != OMB_OK) return st;
+    if ((a.kind == kPkma || a.kind == kMbsrem) && (a.ext_on || a.auto_relax || a.relax_scaling)) {
+        // the gradient preconditioned in place, then (PKMA) the relaxation from the norms
+        PrecondExt p = a.ext;
+        p.fold = a.kind == kMbsrem ? 1 : 0;
+        p.upper = a.upper;
+        if (p.gradF && (st = precond_gradient(image, a.gradF, h->grid, p, a.work, s)) != OMB_OK) return st;
+        if ((st = precond_apply(work_img, a.du, image, h->n_img, p, s)) != OMB_OK) return st;
+        if (a.kind == kPkma && (a.auto_relax || a.relax_scaling)) {
+            if (!a.lam.lam || !a.lam.iter || !a.work)
+                return set_error(OMB_ERR_INVALID, "PKMA relaxation needs the device schedule and workspace");
+            double *w1 = a.work + precond_workspace_bytes() / sizeof(double);
+            double *w2 = w1 + dot_workspace_bytes() / sizeof(double);
+            const size_t off = dot_workspace_bytes() / sizeof(double) - 2;
+            if ((st = dot2(image, work_img, h->n_img, w1, s)) != OMB_OK) return st;  // x.g, g.g
+            if ((st = dot2(work_img, image, h->n_img, w2, s)) != OMB_OK) return st;  // g.x, x.x
+            if ((st = pkma_relax(const_cast<float *>(a.lam.lam), a.lam.iter, p.sub, w1 + off, w2 + off,
+                                 a.auto_relax, a.relax_scaling, s)) != OMB_OK)
+                return st;
+        }
+        if (a.kind == kPkma)
+            return pkma_update(image, work_img, nullptr, h->n_img, a.lam, a.alpha, eps, a.positivity, nullptr, 0, s);
+        return mbsrem_update(image, work_img, nullptr, h->n_img, a.lam, eps, a.upper, a.positivity, nullptr, 0, s);
+    }
     switch (a.kind) {
         case kRosem: return rosem_update(image, a.sens, work_img, h->n_img, a.lam, s);
         case kRamla: return bsrem_update(image, work_img, h->n_img, a.lam, eps, a.positivity, s);

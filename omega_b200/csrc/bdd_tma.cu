@@ -91,29 +91,29 @@ __device__ __forceinline__ int2 slice_box(const Shared &sh, int j, int nlat, int
 
 }  // namespace bt
 
-template <int C>
+template <int NC>
 __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const __grid_constant__ CUtensorMap map_imgT,
                              Grid g, const float *__restrict__ xy, const float *__restrict__ uv, int nr, int nc,
                              float pitch_y, int64_t proj0, int64_t nproj, const float *__restrict__ img,
                              const float *__restrict__ imgT, float *__restrict__ y) {
     using namespace bt;
-    constexpr int kRB = kCTACols / C;  // warps per CTA
-    constexpr float kC = (float)C;
+    constexpr int kRB = kCTACols / NC;  // warps per CTA
+    constexpr float kC = (float)NC;
     __shared__ Shared sh;
     const int tid = threadIdx.x + threadIdx.y * 32;
     const int r = blockIdx.x * 32 + threadIdx.x;
     const int cg = blockIdx.y * kRB + threadIdx.y;
     const int64_t p = blockIdx.z;
-    const int c0 = cg * C;
+    const int c0 = cg * NC;
     const bool active = r < nr && c0 < nc && p < nproj;
-    const int n_groups = (nc + C - 1) / C;
+    const int n_groups = (nc + NC - 1) / NC;
 
     // corner rays: first/last active row x first/last active column group
     if (tid < 4) {
         const int r_last = min(blockIdx.x * 32 + 31, nr - 1);
         const int g_last = min((int)blockIdx.y * kRB + kRB - 1, n_groups - 1);
         const int rr = (tid & 1) ? r_last : (int)blockIdx.x * 32;
-        const int cc = ((tid & 2) ? g_last : (int)blockIdx.y * kRB) * C;
+        const int cc = ((tid & 2) ? g_last : (int)blockIdx.y * kRB) * NC;
         const BddRay b = bdd_ray_setup(g, xy, uv, proj0 + p, rr, cc, nr, nc, pitch_y);
         sh.corner[tid] = Corner{b.xa0, b.xa1, b.xb0, b.xb1, b.za0, b.za1, b.zb0, b.zb1, b.dz0, b.dz1};
         if (tid == 0) {
@@ -166,16 +166,16 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
         b = bdd_ray_setup(g, xy, uv, proj0 + p, r, c0, nr, nc, pitch_y);
         kerroin = b.kerroin;
         // the weight belongs to groups of 8 columns (projectorType5.cl:166-174)
-        if (C > 8 && c0 + 8 < nc) kerroin8 = bdd_kerroin(g, xy, uv, proj0 + p, r, c0 + 8, nr, nc, pitch_y, b.ysl);
+        if (NC > 8 && c0 + 8 < nc) kerroin8 = bdd_kerroin(g, xy, uv, proj0 + p, r, c0 + 8, nr, nc, pitch_y, b.ysl);
     }
     const int64_t z_stride = (int64_t)g.nx * g.ny;
     const float *__restrict__ vol = ysl ? img : imgT;
     const float flat = (float)nlat, fz = (float)g.nz;
     const float dlat = ysl ? g.dx : g.dy;
     const int zmax = g.nz - 1;
-    float temp[C];
+    float temp[NC];
 #pragma unroll
-    for (int c = 0; c < C; ++c) temp[c] = 0.f;
+    for (int c = 0; c < NC; ++c) temp[c] = 0.f;
     int tries = kWaitTries;
 
     for (int j = j_lo; j <= j_hi; ++j) {
@@ -215,7 +215,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
                 float S = 0.f;
                 float Cprev = (bz - (float)kc) * R;
 #pragma unroll
-                for (int c = 0; c < C; ++c) {
+                for (int c = 0; c < NC; ++c) {
                     bz = fmaf((float)(c + 1), w, zu);
                     const int kn = (int)bz;
                     if (kc < kn) {
@@ -236,7 +236,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
                 float S = 0.f;
                 float Cprev = (bz - (float)kc) * R;
 #pragma unroll
-                for (int c = 0; c < C; ++c) {
+                for (int c = 0; c < NC; ++c) {
                     bz = fminf(fmaxf(fmaf((float)(c + 1), w, zu), 0.f), fz);
                     const int kn = min((int)bz, zmax);
                     if (kc < kn) {
@@ -258,7 +258,7 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
                 float S = 0.f;
                 float Cprev = (bz - (float)kc) * R;
 #pragma unroll
-                for (int c = 0; c < C; ++c) {
+                for (int c = 0; c < NC; ++c) {
                     bz = fminf(fmaxf(fmaf((float)(c + 1), w, zu), 0.f), fz);
                     const int kn = min((int)bz, zmax);
                     while (kc < kn) {
@@ -276,10 +276,10 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
         if (threadIdx.x == 0 && threadIdx.y == t % kRB && j + kStages <= j_hi) issue(j + kStages, s);
     }
     if (!active) return;
-    const int ncol = min(C, nc - c0);
+    const int ncol = min(NC, nc - c0);
     const int64_t idx = r + (int64_t)c0 * nr + p * (int64_t)nr * nc;
 #pragma unroll
-    for (int c = 0; c < C; ++c)
+    for (int c = 0; c < NC; ++c)
         if (c < ncol) y[idx + (int64_t)c * nr] = temp[c] * (c < 8 ? kerroin : kerroin8);
 }
 

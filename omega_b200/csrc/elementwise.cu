@@ -410,3 +410,237 @@ int loglik(const float *y, const float *fp, int64_t n, float epps, double *out_h
 }
 
 }  // namespace omb
+
+// ---------------------------------------------------------------------------
+// The other image preconditioners of PKMA / MRAMLA / MBSREM and PKMA's
+// automatic relaxation (applyImagePreconditioning functions.hpp:2057-2106,
+// gradientPreconditioner :2036-2054, computeGradient :2016-2035; PKMA
+// algorithms.h:151-212).  The gradient g = rhs + dU is multiplied, in the
+// reference's order, by the type-4 image gradF (from sub-iteration grad_init
+// on), the type-3 value alpha[k], the types 0 / 1 / 2 factor (1 / D, xp / D,
+// max(xp, max(1e-5, ref)) / D) and the type-6 image dP; xp is the image, for
+// MBSREM folded to U - x where x >= U / 2.
+// ---------------------------------------------------------------------------
+namespace omb {
+namespace {
+
+__global__ void k_precond_apply(float *__restrict__ g, const float *__restrict__ du, const float *__restrict__ img,
+                                int64_t n, PrecondExt p) {
+    const int kk = *p.it * p.n_sub + p.sub;
+    const bool grad = p.gradF && kk >= p.grad_init;
+    const float al = p.alpha ? p.alpha[kk] : 1.f;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float x = img[i];
+        const float xp = p.fold && x >= p.upper / 2.f ? p.upper - x : x;
+        float v = du ? g[i] + __ldg(du + i) : g[i];
+        if (grad) v *= __ldg(p.gradF + i);
+        if (p.alpha) v *= al;
+        if (p.mode == 1) v /= __ldg(p.dd + i);
+        else if (p.mode == 2) v *= xp / __ldg(p.dd + i);
+        else if (p.mode == 3) v *= fmaxf(xp, fmaxf(1e-5f, __ldg(p.ref + i))) / __ldg(p.dd + i);
+        if (p.dP) v *= __ldg(p.dP + i);
+        g[i] = v;
+    }
+}
+
+// deterministic FP64 sum in two passes (partials per block, then one block)
+constexpr int kSumBlocks = 296;
+
+// type-4 window check: sub-iteration k in [init, last]
+__device__ __forceinline__ bool grad_window(const PrecondExt &p) {
+    const int kk = *p.it * p.n_sub + p.sub;
+    return kk >= p.grad_init && kk <= p.grad_last;
+}
+
+__device__ __forceinline__ float folded(const float *img, int64_t i, const PrecondExt &p) {
+    const float x = img[i];
+    return p.fold && x >= p.upper / 2.f ? p.upper - x : x;
+}
+
+// sum of the folded image (which = 0) or of gradF (which = 1) over the image
+__global__ void k_grad_sum(const float *__restrict__ img, const float *__restrict__ f, int64_t n, PrecondExt p,
+                           int which, double *__restrict__ part) {
+    if (!grad_window(p)) return;
+    __shared__ double sh[8];
+    double acc = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        acc += which ? (double)__ldg(f + i) : (double)folded(img, i, p);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_grad_fold(double *__restrict__ part, int nb, PrecondExt p, double *__restrict__ out) {
+    if (!grad_window(p)) return;
+    double t = 0.0;
+    for (int b = (int)threadIdx.x; b < nb; b += 32) t += part[b];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) *out = t;
+}
+
+// one axis of computeGradient: forward (0), backward (1) or central (2)
+// difference of the folded image at voxel (i along an axis of length len,
+// neighbours at +-step)
+__device__ __forceinline__ float axis_diff(const float *img, int64_t n0, int i, int len, int64_t step, int type,
+                                           const PrecondExt &p) {
+    const float c = folded(img, n0, p);
+    if (type == 0) return i < len - 1 ? folded(img, n0 + step, p) - c : -c;
+    if (type == 1) return i > 0 ? folded(img, n0 - step, p) - c : -c;
+    if (len < 2) return 0.f;
+    if (i == 0) return folded(img, n0 + step, p) - c;
+    if (i == len - 1) return c - folded(img, n0 - step, p);
+    return (folded(img, n0 + step, p) - folded(img, n0 - step, p)) * 0.5f;
+}
+
+// f = max(1e-5, |grad xp| / mean(xp)) into gradF
+__global__ void k_grad_norm(const float *__restrict__ img, float *__restrict__ f, Grid g, PrecondExt p,
+                            const double *__restrict__ sum_x) {
+    if (!grad_window(p)) return;
+    const int64_t nxy = (int64_t)g.nx * g.ny, n = nxy * g.nz;
+    const float mean = (float)(*sum_x / (double)n);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        const int k = (int)(v / nxy), j = (int)((v - k * nxy) / g.nx), i = (int)(v - k * nxy - (int64_t)j * g.nx);
+        const float a = axis_diff(img, v, i, g.nx, 1, p.deriv_type, p);
+        const float b = axis_diff(img, v, j, g.ny, g.nx, p.deriv_type, p);
+        const float c = axis_diff(img, v, k, g.nz, nxy, p.deriv_type, p);
+        f[v] = fmaxf(1e-5f, sqrtf(a * a + b * b + c * c) / mean);
+    }
+}
+
+// gradF = min(V2, max(V1, mean(f) / f))
+__global__ void k_grad_finish(float *__restrict__ f, int64_t n, PrecondExt p, const double *__restrict__ sum_f) {
+    if (!grad_window(p)) return;
+    const float mean = (float)(*sum_f / (double)n);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        f[v] = fminf(p.grad_v2, fmaxf(p.grad_v1, mean / f[v]));
+}
+
+// PKMA's relaxation (algorithms.h:155-197) from ||x||^2 and ||g||^2:
+// first sub-iteration lam[0] = ||x|| / ||g|| / 4; first sub-iteration of
+// iteration it > 0: lam[it] = lam[it - 1] / (it / 35 + 1); with scaling,
+// q = ||x|| / (lam ||g||) and lam *= q / 1.5 when 0 < q < 1.5.
+__global__ void k_pkma_relax(float *__restrict__ lam, const int *__restrict__ it, int sub, const double *xg_gg,
+                             const double *gx_xx, int compute, int scaling) {
+    const int t = *it;
+    const double gn = sqrt(xg_gg[1]), xn = sqrt(gx_xx[1]);
+    if (compute) {
+        if (t == 0 && sub == 0) lam[0] = (float)(xn / gn) * .25f;
+        else if (t > 0 && sub == 0) lam[t] = lam[t - 1] * (1.f / ((float)t / 35.f + 1.f));
+    }
+    if (scaling) {
+        const float q = (float)(xn / (gn * (double)lam[t]));
+        if (q < 1.5f && q > 0.f) lam[t] *= q / 1.5f;
+    }
+}
+
+__global__ void k_div_inplace(float *__restrict__ a, const float *__restrict__ b, int64_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) a[i] /= __ldg(b + i);
+}
+
+// E / y where y > 0, else 0 (the type-6 measurement image, reconstructionAF.h:600-616)
+__global__ void k_curv_meas(float *__restrict__ e, const float *__restrict__ y, int64_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float yv = __ldg(y + i);
+        e[i] = yv > 0.f ? e[i] / yv : 0.f;
+    }
+}
+
+// dP (+)= S / rhs; finish: NaN / Inf -> 1 (reconstructionAF.h:637-650)
+__global__ void k_curv_acc(float *__restrict__ dp, const float *__restrict__ rhs, int64_t n, float S, int first) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float v = S / __ldg(rhs + i);
+        dp[i] = first ? v : dp[i] + v;
+    }
+}
+
+__global__ void k_curv_finish(float *__restrict__ dp, int64_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (isnan(dp[i]) || isinf(dp[i])) dp[i] = 1.f;
+}
+
+// zeros of M -> 1 (reconstructionAF.h:861)
+__global__ void k_zero_to_one(float *__restrict__ a, int64_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (a[i] == 0.f) a[i] = 1.f;
+}
+
+}  // namespace
+
+size_t precond_workspace_bytes() { return (size_t)(kSumBlocks + 2) * sizeof(double); }
+
+int precond_apply(float *g, const float *du, const float *img, int64_t n, const PrecondExt &p, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_precond_apply<<<grid_for(n, 4), kBlock, 0, st>>>(g, du, img, n, p);
+    OMB_LAUNCH_CHECK("image preconditioner launch");
+    return OMB_OK;
+}
+
+int precond_gradient(const float *img, float *gradF, const Grid &g, const PrecondExt &p, double *work,
+                     cudaStream_t st) {
+    const int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    double *part = work, *sx = work + kSumBlocks, *sf = work + kSumBlocks + 1;
+    k_grad_sum<<<kSumBlocks, kBlock, 0, st>>>(img, nullptr, n, p, 0, part);
+    k_grad_fold<<<1, 32, 0, st>>>(part, kSumBlocks, p, sx);
+    k_grad_norm<<<grid_for(n, 4), kBlock, 0, st>>>(img, gradF, g, p, sx);
+    k_grad_sum<<<kSumBlocks, kBlock, 0, st>>>(img, gradF, n, p, 1, part);
+    k_grad_fold<<<1, 32, 0, st>>>(part, kSumBlocks, p, sf);
+    k_grad_finish<<<grid_for(n, 4), kBlock, 0, st>>>(gradF, n, p, sf);
+    OMB_LAUNCH_CHECK("gradient preconditioner launch");
+    return OMB_OK;
+}
+
+int pkma_relax(float *lam, const int *it, int sub, const double *xg_gg, const double *gx_xx, bool compute,
+               bool scaling, cudaStream_t st) {
+    k_pkma_relax<<<1, 1, 0, st>>>(lam, it, sub, xg_gg, gx_xx, compute ? 1 : 0, scaling ? 1 : 0);
+    OMB_LAUNCH_CHECK("PKMA relaxation launch");
+    return OMB_OK;
+}
+
+int div_inplace(float *a, const float *b, int64_t n, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_div_inplace<<<grid_for(n, 4), kBlock, 0, st>>>(a, b, n);
+    OMB_LAUNCH_CHECK("division launch");
+    return OMB_OK;
+}
+
+int curv_meas(float *e, const float *y, int64_t n, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_curv_meas<<<grid_for(n, 4), kBlock, 0, st>>>(e, y, n);
+    OMB_LAUNCH_CHECK("curvature preconditioner launch");
+    return OMB_OK;
+}
+
+int curv_acc(float *dp, const float *rhs, int64_t n, int subsets, bool first, cudaStream_t st) {
+    k_curv_acc<<<grid_for(n, 4), kBlock, 0, st>>>(dp, rhs, n, (float)subsets, first ? 1 : 0);
+    OMB_LAUNCH_CHECK("curvature preconditioner launch");
+    return OMB_OK;
+}
+
+int curv_finish(float *dp, int64_t n, cudaStream_t st) {
+    k_curv_finish<<<grid_for(n, 4), kBlock, 0, st>>>(dp, n);
+    OMB_LAUNCH_CHECK("curvature preconditioner launch");
+    return OMB_OK;
+}
+
+int zero_to_one(float *a, int64_t n, cudaStream_t st) {
+    if (n <= 0) return OMB_OK;
+    k_zero_to_one<<<grid_for(n, 4), kBlock, 0, st>>>(a, n);
+    OMB_LAUNCH_CHECK("measurement preconditioner launch");
+    return OMB_OK;
+}
+
+}  // namespace omb

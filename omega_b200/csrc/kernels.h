@@ -64,6 +64,23 @@ int map_step(float *img, const float *du, int64_t n, Relax lam, float epps, cuda
 int relax_advance(int *iter, cudaStream_t st);
 // The relaxed sub-iterations of a handle.
 enum RelaxedKind { kRosem = 0, kRamla = 1, kPkma = 2, kMbsrem = 3 };
+// The other image preconditioners of PKMA / MRAMLA / MBSREM (elementwise.cu): the gradient times the type-4
+// image gradF (from sub-iteration grad_init on), the type-3 value alpha[k], the types 0 / 1 / 2 factor
+// (mode 1: 1 / D, 2: xp / D, 3: max(xp, max(1e-5, ref)) / D) and the type-6 image dP; k = *it * n_sub + sub,
+// xp the image (folded to U - x where x >= U / 2 when fold).
+struct PrecondExt {
+    int mode = 0;
+    const float *dd = nullptr, *ref = nullptr;
+    const float *gradF = nullptr;
+    int grad_init = 0, grad_last = 0, deriv_type = 0;
+    float grad_v1 = 0.5f, grad_v2 = 2.5f;
+    const float *alpha = nullptr;
+    const float *dP = nullptr;
+    const int *it = nullptr;
+    int n_sub = 1, sub = 0;
+    int fold = 0;
+    float upper = 10000.f;
+};
 struct RelaxedArgs {
     int kind = kRosem;
     const float *sens = nullptr;   // ROSEM
@@ -74,9 +91,31 @@ struct RelaxedArgs {
     bool positivity = true;
     const float *precond_d = nullptr;  // PKMA / MBSREM: D of the image preconditioner
     int precond = 0;               // 0 none, 1 g / D (type 0), 2 g * x / D (type 1)
+    // the other preconditioners (when ext_on): applied by precond_apply before the update, which then
+    // takes the gradient as it is
+    bool ext_on = false;
+    PrecondExt ext;
+    float *gradF = nullptr;        // type-4 image, recomputed in its window
+    double *work = nullptr;        // precond_workspace_bytes() + 2 dot2 workspaces (type 4, relaxation)
+    const float *meas_m = nullptr; // measurement preconditioner type 0: the subset's A 1 (zeros -> 1), or NULL
+    bool auto_relax = false, relax_scaling = false;  // PKMA: lam from the norms (needs lam.lam)
 };
 int relaxed_subset(omb_handle *h, int32_t subset, float *image, const float *y_subset, const RelaxedArgs &a,
                    float *work_meas, float *work_img, cudaStream_t st);
+
+int precond_apply(float *g, const float *du, const float *img, int64_t n, const PrecondExt &p, cudaStream_t st);
+// Type 4: recomputes gradF from img when the sub-iteration lies in [grad_init, grad_last] (device-side check).
+size_t precond_workspace_bytes();
+int precond_gradient(const float *img, float *gradF, const Grid &g, const PrecondExt &p, double *work,
+                     cudaStream_t st);
+// PKMA's automatic relaxation / relaxation scaling of lam[*it] from dot2 results (x.g, g.g) and (g.x, x.x).
+int pkma_relax(float *lam, const int *it, int sub, const double *xg_gg, const double *gx_xx, bool compute,
+               bool scaling, cudaStream_t st);
+int div_inplace(float *a, const float *b, int64_t n, cudaStream_t st);
+int curv_meas(float *e, const float *y, int64_t n, cudaStream_t st);
+int curv_acc(float *dp, const float *rhs, int64_t n, int subsets, bool first, cudaStream_t st);
+int curv_finish(float *dp, int64_t n, cudaStream_t st);
+int zero_to_one(float *a, int64_t n, cudaStream_t st);
 
 // Projector types 2 / 3 (PET), one frame.
 int orth_forward(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof, float gf, const float *img, float *y,

@@ -157,12 +157,71 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         const float upper = p->upper_bound > 0.f ? p->upper_bound : 10000.f;
         // PKMA / MBSREM image preconditioner: D once, before the iterations
         DevBuf pd;
-        if (p->precond < 0 || p->precond > 2 || (p->precond && !(pkma || mb)))
-            return set_error(OMB_ERR_INVALID, "image preconditioners 1 and 2 are for PKMA / MRAMLA / MBSREM");
+        if (p->precond < 0 || p->precond > 3 || (p->precond && !(pkma || mb)))
+            return set_error(OMB_ERR_INVALID, "image preconditioners 1 to 3 are for PKMA / MRAMLA / MBSREM");
+        const bool ext = p->precond == 3 || p->precond_alpha || p->precond_grad || p->precond_curv;
+        if ((ext || p->precond_meas) && !(pkma || mb))
+            return set_error(OMB_ERR_INVALID, "the image and measurement preconditioners are for PKMA / MRAMLA / MBSREM");
+        if (p->pkma_relax && !pkma) return set_error(OMB_ERR_INVALID, "the relaxation parameters are PKMA's");
+        if (p->precond == 3 && !p->precond_ref)
+            return set_error(OMB_ERR_INVALID, "image preconditioner type 2 needs precond_ref");
+        if (p->precond_grad && (p->diff_type < 0 || p->diff_type > 2))
+            return set_error(OMB_ERR_INVALID, "diff_type must be 0, 1 or 2");
         if (p->precond) {
             if ((st = alloc(pd, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
             if ((st = omb_precond_image(h, pd.f(), wi.f(), stream)) != OMB_OK) return st;
         }
+        // the other preconditioners (functions.hpp:2057-2106, reconstructionAF.h:600-650, 827-861) and the
+        // PKMA relaxation's workspace
+        DevBuf ones, gradF, dP, alpha_d, meas_m, pwork;
+        if (p->precond_curv || p->precond_meas) {
+            if ((st = alloc(ones, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+            OMB_CUDA_TRY(cudaMemsetAsync(ones.p, 0, (size_t)n * sizeof(float), s));
+            if ((st = zero_to_one(ones.f(), n, s)) != OMB_OK) return st;  // an image of ones
+        }
+        if (p->precond_meas) {
+            // A_s 1 of every subset, in subset order like y
+            if ((st = alloc(meas_m, (size_t)off[n_subsets] * sizeof(float), s)) != OMB_OK) return st;
+            for (int s_ = 0; s_ < n_subsets && st == OMB_OK; ++s_)
+                st = omb_forward(h, s_, ones.f(), meas_m.f() + off[s_], stream);
+            if (st == OMB_OK) st = zero_to_one(meas_m.f(), off[n_subsets], s);
+            if (st != OMB_OK) return st;
+        }
+        if (p->precond_curv) {
+            if ((st = alloc(dP, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+            for (int s_ = 0; s_ < n_subsets && st == OMB_OK; ++s_) {
+                const int64_t ms = off[s_ + 1] - off[s_];
+                st = omb_forward(h, s_, ones.f(), wm.f(), stream);
+                if (st == OMB_OK) st = curv_meas(wm.f(), y + off[s_], ms, s);
+                if (st == OMB_OK) st = omb_backward(h, s_, wm.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC, stream);
+                if (st == OMB_OK) st = curv_acc(dP.f(), wi.f(), n, n_subsets, s_ == 0, s);
+            }
+            if (st == OMB_OK) st = curv_finish(dP.f(), n, s);
+            if (st != OMB_OK) return st;
+        }
+        if (p->precond_grad && (st = alloc(gradF, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        if (p->precond_alpha) {
+            const size_t na = (size_t)p->n_iter * n_subsets;
+            if ((st = alloc(alpha_d, na * sizeof(float), s)) != OMB_OK) return st;
+            OMB_CUDA_TRY(cudaMemcpyAsync(alpha_d.p, p->precond_alpha, na * sizeof(float), cudaMemcpyHostToDevice, s));
+        }
+        if ((ext || p->pkma_relax) &&
+            (st = alloc(pwork, precond_workspace_bytes() + 2 * dot_workspace_bytes(), s)) != OMB_OK)
+            return st;
+        PrecondExt pe;
+        pe.mode = p->precond;
+        pe.dd = p->precond ? pd.f() : nullptr;
+        pe.ref = p->precond_ref;
+        pe.gradF = p->precond_grad ? gradF.f() : nullptr;
+        pe.grad_init = p->grad_iters[0];
+        pe.grad_last = p->grad_iters[1];
+        pe.deriv_type = p->diff_type;
+        pe.grad_v1 = p->grad_v[0];
+        pe.grad_v2 = p->grad_v[1];
+        pe.alpha = p->precond_alpha ? alpha_d.f() : nullptr;
+        pe.dP = p->precond_curv ? dP.f() : nullptr;
+        pe.it = rl.iter;
+        pe.n_sub = n_subsets;
         for (int s_ = 0; s_ < n_subsets && !no_sens && st == OMB_OK; ++s_)
             st = omb_sensitivity(h, s_, sens.f() + s_ * n, stream);
         if (st != OMB_OK) return st;
@@ -216,8 +275,17 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                     ra.alpha.subset = s_;
                     ra.upper = upper;
                     ra.positivity = p->positivity != 0;
-                    ra.precond = p->precond;
-                    ra.precond_d = p->precond ? pd.f() : nullptr;
+                    // with the other preconditioners on, precond_apply takes types 0-2 as well
+                    ra.precond = ext ? 0 : p->precond;
+                    ra.precond_d = p->precond && !ext ? pd.f() : nullptr;
+                    ra.ext_on = ext;
+                    ra.ext = pe;
+                    ra.ext.sub = s_;
+                    ra.gradF = p->precond_grad ? gradF.f() : nullptr;
+                    ra.work = static_cast<double *>(pwork.p);
+                    ra.meas_m = p->precond_meas ? meas_m.f() + off[s_] : nullptr;
+                    ra.auto_relax = (p->pkma_relax & 1) != 0;
+                    ra.relax_scaling = (p->pkma_relax & 2) != 0;
                     if (sub_prior) {
                         e = prior_grad();
                         ra.du = du.f();

@@ -140,6 +140,18 @@ class projectorClass:
     delta_PKMA = 100.
     U = 0.
     precondTypeImage = np.full((7, 1), False)
+    precondTypeMeas = np.full((2, 1), False)
+    # image preconditioner options (proj.py:107, 276-279, 362-363, 439 of the
+    # reference): type 2's reference image, type 3's per-sub-iteration values,
+    # type 4's bounds and window; PKMA's automatic relaxation
+    referenceImage = np.empty(0, dtype=np.float32)
+    alphaPrecond = np.empty(0, dtype=np.float32)
+    gradV1 = 0.5
+    gradV2 = 2.5
+    gradInitIter = 1
+    gradLastIter = 1
+    computeRelaxationParameters = False
+    relaxationScaling = False
     PDHG = False
     TV = False
     RDP = False

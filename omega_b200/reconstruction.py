@@ -281,6 +281,20 @@ def momentum(options):
     return np.ascontiguousarray(a[:n], dtype=np.float32)
 
 
+def _check_preconditioners(options):
+    """The preconditioner selections the built-in loop takes (before any
+    device work): at most one of the image types 0-2; the filtering-based
+    image (5) and measurement (1) preconditioners are not built."""
+    pt_im = np.ravel(np.asarray(getattr(options, 'precondTypeImage', np.zeros(7, dtype=bool)), dtype=bool))
+    pt_meas = np.ravel(np.asarray(getattr(options, 'precondTypeMeas', np.zeros(2, dtype=bool)), dtype=bool))
+    if int(np.count_nonzero(pt_im[:3])) > 1:
+        raise ValueError('Only one of the image preconditioners 0-2 can be selected')
+    if pt_im.size > 5 and pt_im[5]:
+        raise ValueError('The filtering-based image preconditioner (type 5) is not built')
+    if pt_meas.size > 1 and pt_meas[1]:
+        raise ValueError('The filtering-based measurement preconditioner (type 1) is not built')
+
+
 def reconstructions_main(options):
     """The built-in reconstruction (omegatomo/reconstruction/recomain.py:427-725,
     the compiled omegaMain entry) for the algorithms of this path:
@@ -327,6 +341,8 @@ def reconstructions_main(options):
         raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM, '
                                   'options.MRP, options.TV, options.APLS, options.GGMRF, options.hyperbolic or '
                                   'options.weighted_mean')
+    if method in ('PKMA', 'MRAMLA', 'MBSREM'):
+        _check_preconditioners(options)
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
         raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
@@ -387,17 +403,44 @@ def reconstructions_main(options):
     if method in ('MRAMLA', 'MBSREM'):
         u = float(getattr(options, 'U', 0.))
         p.upper_bound = u if u > 0 else 10000.
-    # image preconditioners of PKMA / MRAMLA / MBSREM: types 0 (rhs / D) and 1
-    # (rhs * x / D) of options.precondTypeImage; other algorithms ignore them,
-    # as the reference does (proj.py:1079-1082)
+    # image preconditioners of PKMA / MRAMLA / MBSREM (options.precondTypeImage, functions.hpp:2057-2106:
+    # 0 rhs / D, 1 rhs x / D, 2 rhs max(x, ref) / D, 3 alphaPrecond, 4 gradient-based, 6 curvature) and
+    # the measurement preconditioner type 0 (options.precondTypeMeas[0], the ratio over A 1); other
+    # algorithms ignore them, as the reference does (proj.py:1079-1082)
     pt_im = np.ravel(np.asarray(getattr(options, 'precondTypeImage', np.zeros(7, dtype=bool)), dtype=bool))
-    if method in ('PKMA', 'MRAMLA', 'MBSREM') and pt_im.size and pt_im.any():
-        if pt_im.size > 2 and pt_im[2:].any():
-            raise ValueError('Image preconditioners other than types 0 and 1 are not built')
-        if pt_im[0] and pt_im.size > 1 and pt_im[1]:
-            raise ValueError('Only one of the image preconditioners 0-2 can be selected')
-        p.precond = 1 if pt_im[0] else 2
+    pt_meas = np.ravel(np.asarray(getattr(options, 'precondTypeMeas', np.zeros(2, dtype=bool)), dtype=bool))
     keep = []
+    if method in ('PKMA', 'MRAMLA', 'MBSREM'):
+        def on(k):
+            return pt_im.size > k and bool(pt_im[k])
+        p.precond = 1 if on(0) else (2 if on(1) else (3 if on(2) else 0))
+        if on(2):
+            ref = np.asarray(getattr(options, 'referenceImage', np.empty(0)), dtype=np.float32)
+            if ref.size != n:
+                raise ValueError('Image preconditioner type 2 needs options.referenceImage of the image size')
+            rt = torch.from_numpy(np.ascontiguousarray(ref.ravel(order='F'))).to(dev)
+            keep.append(rt)
+            p.precond_ref = ctypes.c_void_p(rt.data_ptr())
+        alpha_pre = None
+        if on(3):
+            alpha_pre = np.ascontiguousarray(np.ravel(getattr(options, 'alphaPrecond', np.empty(0))), dtype=np.float32)
+            if alpha_pre.size < int(options.Niter) * S:
+                raise ValueError('Image preconditioner type 3 needs options.alphaPrecond with Niter * subsets values')
+            p.precond_alpha = ctypes.c_void_p(alpha_pre.ctypes.data)
+        if on(4):
+            p.precond_grad = 1
+            p.grad_v[0] = float(getattr(options, 'gradV1', 0.5))
+            p.grad_v[1] = float(getattr(options, 'gradV2', 2.5))
+            p.grad_iters[0] = int(getattr(options, 'gradInitIter', 1))
+            p.grad_iters[1] = int(getattr(options, 'gradLastIter', 1))
+            p.diff_type = int(getattr(options, 'derivativeType', 0))
+        if on(6):
+            p.precond_curv = 1
+        if pt_meas.size and pt_meas[0]:
+            p.precond_meas = 1
+    if method == 'PKMA':
+        p.pkma_relax = (1 if getattr(options, 'computeRelaxationParameters', False) else 0) | \
+            (2 if getattr(options, 'relaxationScaling', False) else 0)
     if prior:
         p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
                    (_native.OMB_PRIOR_NLM if nlm else

@@ -356,8 +356,34 @@ def precond_image(geom: Geometry, backward=None):
     return np.where(d == 0.0, 1.0, d)
 
 
+def _grad_precond(xp, shape, diff_type, v1, v2):
+    """gradientPreconditioner (functions.hpp:2016-2054): f = max(1e-5,
+    |grad xp| / mean(xp)), gradF = min(v2, max(v1, mean(f) / f));
+    computeGradient's forward (0), backward (1) or central (2) differences."""
+    X = np.asarray(xp, dtype=np.float64).reshape(shape, order='F')
+    comps = []
+    for a in range(3):
+        Xa = np.moveaxis(X, a, 0)
+        d = np.empty_like(Xa)
+        if diff_type == 0:
+            d[:-1] = Xa[1:] - Xa[:-1]
+            d[-1] = -Xa[-1]
+        elif diff_type == 1:
+            d[1:] = Xa[:-1] - Xa[1:]
+            d[0] = -Xa[0]
+        else:
+            d[1:-1] = (Xa[2:] - Xa[:-2]) * 0.5
+            d[0] = Xa[1] - Xa[0]
+            d[-1] = Xa[-1] - Xa[-2]
+        comps.append(np.moveaxis(d, 0, a))
+    f = np.maximum(1e-5, np.sqrt(comps[0] ** 2 + comps[1] ** 2 + comps[2] ** 2) / X.mean())
+    f = f.mean() / f
+    return np.minimum(v2, np.maximum(v1, f)).ravel(order='F')
+
+
 def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None, backward=None, randoms=None,
-            prior_grad=None, positivity=True, alpha=None, upper=10000.0, precond=0):
+            prior_grad=None, positivity=True, alpha=None, upper=10000.0, precond=0, ref=None, alpha_precond=None,
+            grad_precond=None, curv_precond=False, meas_precond=False, auto_relax=False, relax_scaling=False):
     """Restated relaxed loops in FP64 (kind: "ROSEM", "RAMLA", "BSREM",
     "ROSEM_MAP", "PKMA", "MRAMLA", "MBSREM"); returns the image after n_iter
     iterations.
@@ -376,7 +402,16 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
     auxKernels.cl:2011-2022): x + lam (A^T (y / (fp + epps [+ r]) - 1)
     [+ dU]), max(epps, .) with positivity, values >= U set to U - epps.
     precond (PKMA / MRAMLA / MBSREM, functions.hpp:2057-2106): 1 divides the
-    gradient by D, 2 multiplies it by x / D (MBSREM: U - x where x >= U / 2)."""
+    gradient by D, 2 multiplies it by x / D (MBSREM: U - x where x >= U / 2),
+    3 by max(x, max(1e-5, ref)) / D.  Before it the gradient is multiplied by
+    the type-4 image (grad_precond = dict(v1, v2, init, last, diff_type):
+    recomputed from the (folded) image in sub-iterations init..last, applied
+    from init on) and by alpha_precond[k] (type 3); after it by the type-6
+    image dP = sum_s S / A_s^T (A_s 1 / y_s) (curv_precond).  meas_precond
+    divides the ratio by A_s 1 (zeros -> 1).  PKMA with auto_relax: lam[0] =
+    ||x|| / ||g|| / 4 at the first sub-iteration, lam[it] = lam[it - 1] /
+    (it / 35 + 1) at each later iteration's first; relax_scaling: q = ||x|| /
+    (lam ||g||), lam *= q / 1.5 when 0 < q < 1.5 (algorithms.h:151-197)."""
     fwd = forward or globals()["forward"]
     bwd = backward or globals()["backward"]
     lam = np.asarray(default_relaxation(n_iter) if lam is None else lam, dtype=np.float32)
@@ -389,14 +424,35 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
     x = np.asarray(x0, dtype=np.float64).copy()
     eps = geom.epps
     D = precond_image(geom, bwd) if precond else None
+    shape = (geom.nx, geom.ny, geom.nz)
+    lam = np.asarray(lam, dtype=np.float64).copy()
+    ones = np.ones(geom.n_img)
+    M = None
+    if meas_precond:
+        M = []
+        for s in range(S):
+            mv = fwd(geom, ones, s)
+            mv[mv == 0] = 1.0
+            M.append(mv)
+    dP = None
+    if curv_precond:
+        dP = np.zeros(geom.n_img)
+        for s in range(S):
+            E = fwd(geom, ones, s)
+            ys = np.asarray(y_subsets[s], dtype=np.float64)
+            EE = np.where(ys > 0, E / np.where(ys > 0, ys, 1.0), 0.0)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                dP = dP + S / bwd(geom, EE, s)
+        dP[~np.isfinite(dP)] = 1.0
+    gradF = None
     sens = []
     if kind in ("ROSEM", "ROSEM_MAP"):
         for s in range(S):
             _, sv = bwd(geom, None, s, sens=True)
             sens.append(np.maximum(sv, eps))
     for it in range(n_iter):
-        lm = float(lam[it])
         for s in range(S):
+            lm = float(lam[it])
             du = prior_grad(x) if additive and prior_grad is not None else None
             fp = fwd(geom, x, s) + eps
             if randoms is not None:
@@ -408,14 +464,40 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
             elif ramla or kind in ("MRAMLA", "MBSREM"):
                 r = r - 1.0
             r[~np.isfinite(r)] = eps
+            if M is not None:
+                r = r / M[s]
             rhs = bwd(geom, r, s)
             if du is not None:
                 rhs = rhs + du
+            xp = np.where(x >= upper / 2.0, upper - x, x) if kind in ("MRAMLA", "MBSREM") else x
+            kk = it * S + s
+            if grad_precond is not None and kk >= grad_precond["init"]:
+                if kk <= grad_precond["last"]:
+                    gradF = _grad_precond(xp, shape, grad_precond.get("diff_type", 0), grad_precond["v1"],
+                                          grad_precond["v2"])
+                rhs = rhs * gradF
+            if alpha_precond is not None:
+                rhs = rhs * float(alpha_precond[kk])
             if precond == 1:
                 rhs = rhs / D
             elif precond == 2:
-                xp = np.where(x >= upper / 2.0, upper - x, x) if kind in ("MRAMLA", "MBSREM") else x
                 rhs = rhs * (xp / D)
+            elif precond == 3:
+                rhs = rhs * (np.maximum(xp, np.maximum(1e-5, ref)) / D)
+            if dP is not None:
+                rhs = rhs * dP
+            if kind == "PKMA" and (auto_relax or relax_scaling):
+                xn, gn = np.linalg.norm(x), np.linalg.norm(rhs)
+                if auto_relax:
+                    if it == 0 and s == 0:
+                        lam[0] = np.float32(xn / gn) * np.float32(0.25)
+                    elif it > 0 and s == 0:
+                        lam[it] = np.float32(lam[it - 1]) * np.float32(1.0 / (it / 35.0 + 1.0))
+                if relax_scaling:
+                    q = np.float32(xn / (gn * lam[it]))
+                    if 0 < q < 1.5:
+                        lam[it] = np.float32(lam[it]) * np.float32(q / 1.5)
+                lm = float(lam[it])
             if kind == "PKMA":
                 a = float(alpha[it * S + s])
                 xa = x - lm * rhs

@@ -404,3 +404,72 @@ def test_builtin_preconditioned_matches_oracle(cuda, method, mode):
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
     plain = orc.relaxed(g, ys, np.ones(g.n_img), 3, method, lam=np.float32(lam), prior_grad=grad)
     assert orc.rel_l2(ref, plain) > 1e-3
+
+
+def _other_precond_case(case, g, rng):
+    """(options, oracle keyword arguments, method, relaxation) of one of the
+    other preconditioners; the relaxation keeps each run well-conditioned."""
+    S = g.n_subsets
+    n_iter = 3
+    if case == "type2":
+        ref = rng.uniform(0.5, 1.5, g.n_img).astype(np.float32)
+        return (dict(precondTypeImage=np.array([0, 0, 1, 0, 0, 0, 0], bool), referenceImage=ref),
+                dict(precond=3, ref=ref.astype(np.float64)), "PKMA", [0.6, 0.4, 0.3])
+    if case == "type3":
+        a = rng.uniform(0.5, 1.0, n_iter * S).astype(np.float32)
+        return (dict(precondTypeImage=np.array([0, 0, 0, 1, 0, 0, 0], bool), alphaPrecond=a),
+                dict(alpha_precond=a), "PKMA", [0.3, 0.2, 0.15])
+    if case == "type4":
+        return (dict(precondTypeImage=np.array([0, 0, 0, 0, 1, 0, 0], bool), gradV1=0.5, gradV2=2.5, gradInitIter=2,
+                     gradLastIter=5, derivativeType=2),
+                dict(grad_precond=dict(v1=0.5, v2=2.5, init=2, last=5, diff_type=2)), "PKMA", [0.3, 0.2, 0.15])
+    if case == "type0+4":
+        return (dict(precondTypeImage=np.array([1, 0, 0, 0, 1, 0, 0], bool), gradInitIter=1, gradLastIter=1,
+                     derivativeType=0),
+                dict(precond=1, grad_precond=dict(v1=0.5, v2=2.5, init=1, last=1, diff_type=0)), "MRAMLA",
+                [0.3, 0.2, 0.15])
+    if case == "type6":
+        return (dict(precondTypeImage=np.array([0, 0, 0, 0, 0, 0, 1], bool), U=5.0),
+                dict(curv_precond=True, upper=5.0), "MRAMLA", [0.02, 0.012, 0.008])
+    if case == "meas0":
+        return (dict(precondTypeMeas=np.array([1, 0], bool)), dict(meas_precond=True), "PKMA", [0.3, 0.2, 0.15])
+    if case == "relax":
+        return (dict(computeRelaxationParameters=True, relaxationScaling=True),
+                dict(auto_relax=True, relax_scaling=True), "PKMA", [0.3, 0.2, 0.15])
+    raise KeyError(case)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["type2", "type3", "type4", "type0+4", "type6", "meas0", "relax"])
+def test_builtin_other_preconditioners(cuda, case):
+    """Image preconditioners 2, 3, 4 and 6, the measurement preconditioner 0
+    and PKMA's automatic relaxation through the built-in entry against the
+    FP64 loop; each changes the result."""
+    o, g = _pet("pet_mini", 42)
+    rng = np.random.default_rng(43)
+    opts, kw, method, lam = _other_precond_case(case, g, rng)
+    x = _run_builtin(o, method, 3, lam=lam, **opts)
+    ys = _subset_measurements(o, g)
+    upper = kw.pop("upper", 10000.0)
+    ref = orc.relaxed(g, ys, np.ones(g.n_img), 3, method, lam=np.float32(lam), upper=upper, **kw)
+    assert np.all(np.isfinite(x))
+    assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+    plain = orc.relaxed(g, ys, np.ones(g.n_img), 3, method, lam=np.float32(lam), upper=upper)
+    assert orc.rel_l2(ref, plain) > 1e-3
+
+
+def test_other_preconditioners_validate():
+    """Rejected selections raise before any device work."""
+    o, g = _pet("pet_mini", 44)
+    from omega_b200 import reconstruction as rec
+    o.PKMA = True
+    o.precondTypeImage = np.array([0, 0, 0, 0, 0, 1, 0], bool)
+    with pytest.raises(ValueError, match="type 5"):
+        rec.reconstructions_main(o)
+    o.precondTypeImage = np.array([1, 1, 0, 0, 0, 0, 0], bool)
+    with pytest.raises(ValueError, match="Only one"):
+        rec.reconstructions_main(o)
+    o.precondTypeImage = np.zeros(7, bool)
+    o.precondTypeMeas = np.array([0, 1], bool)
+    with pytest.raises(ValueError, match="measurement preconditioner"):
+        rec.reconstructions_main(o)
