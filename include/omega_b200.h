@@ -410,6 +410,16 @@ typedef struct omb_recon_params {
     int32_t precond_meas;     /* options.precondTypeMeas[0]: the ratio divided by A_s 1 (zeros -> 1) */
     int32_t pkma_relax;       /* PKMA: bit 0 options.computeRelaxationParameters (lam from the norms of the
                                  image and the gradient, algorithms.h:155-187), bit 1 options.relaxationScaling */
+    const float *filter_h;    /* PDHG, options.precondTypeMeas[1]: device, filter_nf taps h = ifft(filter) of the
+                                 filtering-based measurement preconditioner (see omb_row_filter), or NULL */
+    const float *filter_hinv; /* the taps of 1 / (1 + sigma filter) (the dual step's inverse filter; needed when
+                                 filter_iters > 0) */
+    int32_t filter_nf;        /* the filters' length Nf (a power of two >= filter_rows) */
+    int32_t filter_rows;      /* detector rows per filtered column (nRowsD) */
+    int32_t filter_iters;     /* options.filteringIterations: the iterations that filter (0: all, with the plain
+                                 dual step) */
+    float tau_filt;           /* options.tauCPFilt: the primal step while filtering; <= 0: 1 / the power-method
+                                 eigenvalue of A^T F A */
 } omb_recon_params;
 
 /*
@@ -446,6 +456,17 @@ typedef enum omb_tv_variant {
  */
 int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float beta, float smooth,
                     void *stream);
+
+/*
+ * Detector-row filter of the filtering-based measurement preconditioner
+ * (applyMeasPreconditioning functions.hpp:2109-2166, filtering :1882-1902):
+ * every column of n_rows values (rows fastest; n_cols columns) zero-padded
+ * to nf, filtered by a real even filter in the Fourier domain and cut back:
+ * out[i] = sum_j h[(i - j) mod nf] in[j], h = ifft(filter) (device, nf
+ * taps).  in and out (device) must differ; n_rows <= 2048, nf >= n_rows.
+ */
+int omb_row_filter(const float *in, float *out, int32_t n_rows, int64_t n_cols, const float *h, int32_t nf,
+                   void *stream);
 
 /*
  * Proximal TV of the PDHG loop (priors.h:261-281; ProxTVGradient, ProxTVq,

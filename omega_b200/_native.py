@@ -140,6 +140,12 @@ class ReconParams(ctypes.Structure):
         ("precond_curv", ctypes.c_int32),
         ("precond_meas", ctypes.c_int32),
         ("pkma_relax", ctypes.c_int32),
+        ("filter_h", ctypes.c_void_p),
+        ("filter_hinv", ctypes.c_void_p),
+        ("filter_nf", ctypes.c_int32),
+        ("filter_rows", ctypes.c_int32),
+        ("filter_iters", ctypes.c_int32),
+        ("tau_filt", ctypes.c_float),
     ]
 
 
@@ -265,6 +271,8 @@ EXPORTS = [
     ("omb_tv_gradient_ex", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                           ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
                                           ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]),
+    ("omb_row_filter", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64,
+                                      ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     ("omb_proxtv_dual", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_void_p]),

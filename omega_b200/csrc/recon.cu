@@ -316,10 +316,24 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             if ((st = alloc(q, 3 * (size_t)n * sizeof(float), s)) != OMB_OK) return st;
             OMB_CUDA_TRY(cudaMemsetAsync(q.p, 0, 3 * (size_t)n * sizeof(float), s));
         }
-        float tau = p->tau;
-        if (!(tau > 0.f)) {
-            // |N(0,1)| start normalised to unit length (functions.hpp:2430-2437)
-            if ((st = alloc(work, omb_power_workspace_bytes(), s)) != OMB_OK) return st;
+        // the filtering-based measurement preconditioner (functions.hpp:2109-2166, computeForwardProject.h:
+        // 21-45, 253-298): the residual filtered along the detector rows with h; while k < K the dual step is
+        // p = (I + sigma F)^-1 (p + sigma F r) (the inverse filter hinv), afterwards the plain one without
+        // filtering; with K = 0 every residual is filtered and the dual step stays the plain one
+        const bool filt = p->filter_h != nullptr;
+        const int K = p->filter_iters;
+        DevBuf wf;
+        if (filt) {
+            if (p->filter_rows < 1 || m_all % p->filter_rows != 0)
+                return set_error(OMB_ERR_INVALID, "filter_rows must divide the measurement count");
+            if (K > 0 && !p->filter_hinv) return set_error(OMB_ERR_INVALID, "filtering iterations need filter_hinv");
+            if ((st = alloc(wf, (size_t)m_all * sizeof(float), s)) != OMB_OK) return st;
+        }
+        const int64_t fcols = filt ? m_all / p->filter_rows : 0;
+        // power method (functions.hpp:2417-2540): x <- A^T (F) A x from an |N(0,1)| start normalised to unit
+        // length (2430-2437); L = x . A^T (F) A x / x . x at the last step
+        auto power = [&](bool use_filter, double &L) -> int {
+            if (!work.p && (st = alloc(work, omb_power_workspace_bytes(), s)) != OMB_OK) return st;
             std::vector<float> v((size_t)n);
             std::mt19937 rng(1u);
             std::normal_distribution<float> nd(0.f, 1.f);
@@ -331,58 +345,122 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             const float inv = (float)(1.0 / std::sqrt(norm));
             for (auto &a : v) a *= inv;
             OMB_CUDA_TRY(cudaMemcpyAsync(xn.p, v.data(), (size_t)n * sizeof(float), cudaMemcpyHostToDevice, s));
+            if (!use_filter) {
+                const int e = omb_power_method(h, p->power_iterations > 0 ? p->power_iterations : 20, xn.f(), wm.f(),
+                                               wi.f(), work.p, &L, stream);
+                return e;
+            }
+            double *wl = static_cast<double *>(work.p);
+            double *wn = wl + dot_workspace_bytes() / sizeof(double);
+            const int iters = p->power_iterations > 0 ? p->power_iterations : 20;
+            int e = OMB_OK;
+            for (int it = 0; it < iters && e == OMB_OK; ++it) {
+                e = omb_forward(h, -1, xn.f(), wm.f(), stream);
+                if (e == OMB_OK) e = circ_filter(wm.f(), wf.f(), p->filter_rows, fcols, p->filter_h, p->filter_nf, s);
+                if (e == OMB_OK) e = omb_backward(h, -1, wf.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC, stream);
+                if (e == OMB_OK && it == iters - 1) e = dot2(wi.f(), xn.f(), n, wl, s);
+                if (e == OMB_OK) e = dot2(wi.f(), wi.f(), n, wn, s);
+                if (e == OMB_OK) e = normalize_into(xn.f(), wi.f(), n, wn + dot_workspace_bytes() / sizeof(double) - 2, s);
+            }
+            if (e != OMB_OK) return e;
+            double d[2];
+            OMB_CUDA_TRY(cudaMemcpyAsync(d, wl + dot_workspace_bytes() / sizeof(double) - 2, sizeof(d),
+                                         cudaMemcpyDeviceToHost, s));
+            OMB_CUDA_TRY(cudaStreamSynchronize(s));
+            L = d[0] / d[1];
+            return OMB_OK;
+        };
+        float tau = p->tau;      // the step without filtering
+        float tau_f = 0.f;       // the step while filtering
+        if (filt) {
+            tau_f = p->tau_filt;
+            if (!(tau_f > 0.f)) {
+                double L = 0.0;
+                if ((st = power(true, L)) != OMB_OK) return st;
+                if (!(L > 0.0)) return set_error(OMB_ERR_INVALID, "power method gave a non-positive eigenvalue");
+                tau_f = (float)(1.0 / L);
+            }
+            if (!(tau > 0.f) && K > 0 && K < p->n_iter) {
+                double L = 0.0;
+                if ((st = power(false, L)) != OMB_OK) return st;
+                if (!(L > 0.0)) return set_error(OMB_ERR_INVALID, "power method gave a non-positive eigenvalue");
+                tau = (float)(1.0 / L);
+            }
+        } else if (!(tau > 0.f)) {
             double L = 0.0;
-            st = omb_power_method(h, p->power_iterations > 0 ? p->power_iterations : 20, xn.f(), wm.f(), wi.f(),
-                                  work.p, &L, stream);
-            if (st != OMB_OK) return st;
+            if ((st = power(false, L)) != OMB_OK) return st;
             if (!(L > 0.0)) return set_error(OMB_ERR_INVALID, "power method gave a non-positive eigenvalue");
             tau = (float)(1.0 / L);
         }
-        p->tau_used = tau;
+        p->tau_used = filt ? tau_f : tau;
         OMB_CUDA_TRY(cudaMemcpyAsync(u.p, x_out, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
         OMB_CUDA_TRY(cudaMemsetAsync(pd.p, 0, (size_t)m_all * sizeof(float), s));
-        // one iteration; the plain TV gradient is fused into the primal step,
-        // the other TV gradients are added to A^T p before it
-        auto one = [&](float *xa, float *xb) {
-            if (p->tv_prox) {
-                // priors.h:261-281 between the backprojection and the primal step
-                int e = omb_forward(h, -1, xa, wm.f(), stream);
-                if (e == OMB_OK) e = omb_pdhg_dual(pd.f(), wm.f(), y, m_all, p->sigma, stream);
-                if (e == OMB_OK) e = omb_backward(h, -1, pd.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC, stream);
-                if (e == OMB_OK)
-                    e = omb_proxtv_dual(xa, q.f(), g.nx, g.ny, g.nz, p->sigma2, p->beta, p->l2_ball, p->diff_type,
-                                        stream);
-                if (e == OMB_OK) e = omb_proxtv_divergence(q.f(), wi.f(), g.nx, g.ny, g.nz, p->diff_type, stream);
-                if (e == OMB_OK)
-                    e = omb_pdhg_primal(h, xa, wi.f(), u.f(), xb, tau, p->theta, 0.f, p->tv_smoothing, p->positivity,
-                                        stream);
-                return e;
-            }
-            if (p->tv_variant == OMB_TV_PLAIN)
-                return omb_pdhg_iteration(h, xa, xb, u.f(), pd.f(), y, tau, p->sigma, p->theta, p->beta,
+        // one iteration with steps tau_k, sig_k; fmode 0 no filtering, 1 filtered residual and the plain dual
+        // step, 2 filtered residual and the inverse-filtered dual step.  The plain TV gradient is fused into
+        // the primal step when nothing else comes between; the other TV terms are added to A^T p before it
+        auto one = [&](float *xa, float *xb, float tau_k, float sig_k, int fmode) {
+            if (fmode == 0 && !p->tv_prox && p->tv_variant == OMB_TV_PLAIN)
+                return omb_pdhg_iteration(h, xa, xb, u.f(), pd.f(), y, tau_k, sig_k, p->theta, p->beta,
                                           p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
             int e = omb_forward(h, -1, xa, wm.f(), stream);
-            if (e == OMB_OK) e = omb_pdhg_dual(pd.f(), wm.f(), y, m_all, p->sigma, stream);
+            if (e == OMB_OK && fmode == 0) e = omb_pdhg_dual(pd.f(), wm.f(), y, m_all, sig_k, stream);
+            if (e == OMB_OK && fmode > 0) {
+                e = meas_residual(wm.f(), y, m_all, s);
+                if (e == OMB_OK) e = circ_filter(wm.f(), wf.f(), p->filter_rows, fcols, p->filter_h, p->filter_nf, s);
+                if (e == OMB_OK && fmode == 1) e = dual_step(pd.f(), wf.f(), pd.f(), m_all, sig_k, true, s);
+                if (e == OMB_OK && fmode == 2) e = dual_step(pd.f(), wf.f(), wm.f(), m_all, sig_k, false, s);
+                if (e == OMB_OK && fmode == 2)
+                    e = circ_filter(wm.f(), pd.f(), p->filter_rows, fcols, p->filter_hinv, p->filter_nf, s);
+            }
             if (e == OMB_OK) e = omb_backward(h, -1, pd.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC, stream);
-            if (e == OMB_OK)
+            if (e == OMB_OK && p->tv_prox) {
+                // priors.h:261-281 between the backprojection and the primal step
+                e = omb_proxtv_dual(xa, q.f(), g.nx, g.ny, g.nz, p->sigma2, p->beta, p->l2_ball, p->diff_type, stream);
+                if (e == OMB_OK) e = omb_proxtv_divergence(q.f(), wi.f(), g.nx, g.ny, g.nz, p->diff_type, stream);
+            } else if (e == OMB_OK) {
                 e = omb_tv_gradient_ex(xa, wi.f(), g.nx, g.ny, g.nz, p->beta, p->tv_smoothing, p->tv_variant,
                                        p->tv_sigma, p->tv_c, p->tv_ref, stream);
+            }
             if (e == OMB_OK)
-                e = omb_pdhg_primal(h, xa, wi.f(), u.f(), xb, tau, p->theta, 0.f, p->tv_smoothing, p->positivity,
+                e = omb_pdhg_primal(h, xa, wi.f(), u.f(), xb, tau_k, p->theta, 0.f, p->tv_smoothing, p->positivity,
                                     stream);
             return e;
         };
-        // two iterations per repetition keep x_out / xn in place for graph replays
-        auto two = [&]() {
-            int e = one(x_out, xn.f());
-            if (e == OMB_OK) e = one(xn.f(), x_out);
-            return e;
-        };
-        st = repeat(p->n_iter / 2, graph, s, two);
-        if (st == OMB_OK && p->n_iter % 2) {
-            st = one(x_out, xn.f());
-            if (st == OMB_OK)
-                OMB_CUDA_TRY(cudaMemcpyAsync(x_out, xn.p, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        if (!filt) {
+            // two iterations per repetition keep x_out / xn in place for graph replays
+            auto two = [&]() {
+                int e = one(x_out, xn.f(), tau, p->sigma, 0);
+                if (e == OMB_OK) e = one(xn.f(), x_out, tau, p->sigma, 0);
+                return e;
+            };
+            st = repeat(p->n_iter / 2, graph, s, two);
+            if (st == OMB_OK && p->n_iter % 2) {
+                st = one(x_out, xn.f(), tau, p->sigma, 0);
+                if (st == OMB_OK)
+                    OMB_CUDA_TRY(cudaMemcpyAsync(x_out, xn.p, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+            }
+        } else {
+            // the filter schedule changes at iteration K: eager iterations, host-side schedule
+            float tau_k = tau_f, sig_k = p->sigma;
+            float *xa = x_out, *xb = xn.f();
+            for (int k = 0; k < p->n_iter && st == OMB_OK; ++k) {
+                if (K > 0 && k == K) {
+                    // computeForwardProject.h:22-35: the steps without filtering from here on
+                    if (sig_k == 1.f) {
+                        tau_k = tau;
+                    } else if (sig_k == tau_k) {
+                        tau_k = tau;
+                        sig_k = tau;
+                    } else {
+                        sig_k = tau;
+                    }
+                }
+                const int fmode = K > 0 ? (k < K ? 2 : 0) : 1;
+                st = one(xa, xb, tau_k, sig_k, fmode);
+                std::swap(xa, xb);
+            }
+            if (st == OMB_OK && xa != x_out)
+                OMB_CUDA_TRY(cudaMemcpyAsync(x_out, xa, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
         }
     } else {
         return set_error(OMB_ERR_INVALID, "unknown reconstruction algorithm");

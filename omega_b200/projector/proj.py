@@ -152,6 +152,13 @@ class projectorClass:
     gradLastIter = 1
     computeRelaxationParameters = False
     relaxationScaling = False
+    # the filtering-based measurement preconditioner of PDHG (proj.py:116,
+    # 123, 170-171, 269 of the reference)
+    filterWindow = "hamming"
+    cutoffFrequency = 1.
+    normalFilterSigma = 0.25
+    filteringIterations = 0
+    tauCPFilt = 0.
     PDHG = False
     TV = False
     RDP = False

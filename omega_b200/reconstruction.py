@@ -295,6 +295,19 @@ def _check_preconditioners(options):
         raise ValueError('The filtering-based measurement preconditioner (type 1) is not built')
 
 
+def _check_pdhg_preconditioners(options):
+    """PDHG takes the filtering-based measurement preconditioner; its image
+    and diagonal measurement preconditioners are not built."""
+    pt_im = np.ravel(np.asarray(getattr(options, 'precondTypeImage', np.zeros(7, dtype=bool)), dtype=bool))
+    pt_meas = np.ravel(np.asarray(getattr(options, 'precondTypeMeas', np.zeros(2, dtype=bool)), dtype=bool))
+    if pt_im.any():
+        raise ValueError('Image preconditioners are built for PKMA / MRAMLA / MBSREM, not PDHG')
+    if pt_meas.size and pt_meas[0]:
+        raise ValueError('The diagonal measurement preconditioner (type 0) is built for PKMA / MRAMLA / MBSREM')
+    if pt_meas.size > 1 and pt_meas[1] and int(options.subsets) > 1 and int(options.subsetType) < 8:
+        raise ValueError('The filtering-based preconditioner needs whole projections per subset (subsetType >= 8)')
+
+
 def reconstructions_main(options):
     """The built-in reconstruction (omegatomo/reconstruction/recomain.py:427-725,
     the compiled omegaMain entry) for the algorithms of this path:
@@ -343,6 +356,8 @@ def reconstructions_main(options):
                                   'options.weighted_mean')
     if method in ('PKMA', 'MRAMLA', 'MBSREM'):
         _check_preconditioners(options)
+    if method == 'PDHG':
+        _check_pdhg_preconditioners(options)
     if method in ('MRAMLA', 'MBSREM') and getattr(options, 'randoms_correction', False) and \
             np.size(getattr(options, 'SinDelayed', [])) and not np.all(np.asarray(options.SinDelayed) > 0):
         raise ValueError(method + ' with randoms is built for positive randoms (the zero-randoms bound '
@@ -522,6 +537,26 @@ def reconstructions_main(options):
     p.n_iter = int(options.Niter)
     p.beta = float(options.beta)
     p.tv_smoothing = float(options.TVsmoothing)
+    if options.PDHG:
+        # the filtering-based measurement preconditioner (precondTypeMeas[1], prepass.py:1121-1136,
+        # functions.hpp:2109-2166); PDHG's other preconditioners are not built
+        pt_meas_p = np.ravel(np.asarray(getattr(options, 'precondTypeMeas', np.zeros(2, dtype=bool)), dtype=bool))
+        if pt_meas_p.size > 1 and pt_meas_p[1]:
+            from . import filters
+            nr = int(np.ravel(options.nRowsD)[0]) if options.CT else int(np.ravel(options.Ndist)[0])
+            sig = float(np.ravel(options.sigmaCP)[0])
+            nf, _, _, fh, fhinv = filters.pdhg_row_filters(nr, sig, getattr(options, 'filterWindow', 'hamming'),
+                                                           float(getattr(options, 'cutoffFrequency', 1.0)),
+                                                           float(getattr(options, 'normalFilterSigma', 0.25)))
+            th = torch.from_numpy(fh).to(dev)
+            thi = torch.from_numpy(fhinv).to(dev)
+            keep.extend([th, thi])
+            p.filter_h = ctypes.c_void_p(th.data_ptr())
+            p.filter_hinv = ctypes.c_void_p(thi.data_ptr())
+            p.filter_nf = nf
+            p.filter_rows = nr
+            p.filter_iters = int(getattr(options, 'filteringIterations', 0))
+            p.tau_filt = float(np.ravel(getattr(options, 'tauCPFilt', 0.0))[0])
     if options.PDHG and prox:
         # the proximal TV of the PDHG loop: dual step options.sigma2CP, the
         # beta ball (L2 or max norm), forward or backward differences

@@ -763,13 +763,30 @@ def power_method(geom: Geometry, n_iter, seed=0, x0=None):
     return L
 
 
+def row_filter_fft(v, rows, nf, filt, inverse=False):
+    """filtering / filteringInverse (functions.hpp:1882-1952) in FP64: each
+    column of `rows` values zero-padded to nf, its FFT multiplied (divided)
+    by the real filter, transformed back, the real part cut to `rows`."""
+    V = np.asarray(v, dtype=np.float64).reshape(-1, rows).T
+    F = np.fft.fft(V, n=nf, axis=0)
+    f = np.asarray(filt, dtype=np.float64)[:, None]
+    F = F / f if inverse else F * f
+    return np.real(np.fft.ifft(F, axis=0))[:rows].T.ravel()
+
+
 def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1.0, eps=1e-5,
-            positivity=True, tv_grad=None, prox=None):
+            positivity=True, tv_grad=None, prox=None, meas_filter=None):
     """PDHG with a TV-gradient term, one subset (computeForwardProject.h:227-316,
     algorithms.h:329-420, auxKernels.cl:2034-2062), in FP64.  tv_grad(x), when
     given, replaces the plain TV term beta * dTV(x) (the other TVKernel forms).
     prox = dict(sigma2=..., l2=..., diff_type=...): the proximal TV instead
-    (priors.h:261-281), a dual variable q on the beta ball, rhs -= div q."""
+    (priors.h:261-281), a dual variable q on the beta ball, rhs -= div q.
+    meas_filter = dict(filter0, ffilter, nf, rows, K, tau2): the filtering-based
+    measurement preconditioner (computeForwardProject.h:21-45, 253-298): the
+    residual filtered by filter0; for k < K the dual step (p + sigma F r)
+    divided by ffilter in the Fourier domain, from k = K on the plain dual
+    step without filtering and the primal step tau2 (K = 0: every residual
+    filtered, plain dual step)."""
     from oracle import image_oracle as io
     shape = (geom.nx, geom.ny, geom.nz)
     x = np.asarray(x0, dtype=np.float64).copy()
@@ -777,9 +794,19 @@ def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1
     p = np.zeros(geom.rays(-1), dtype=np.float64)
     q = np.zeros((3, geom.n_img))
     yy = np.asarray(y, dtype=np.float64)
-    for _ in range(n_iter):
+    for k in range(n_iter):
         res = bdd_forward(geom, x, -1) - yy
-        p = (p + sigma * res) / (1.0 + sigma)
+        mf = meas_filter
+        if mf is not None and mf["K"] > 0 and k == mf["K"]:
+            tau = mf["tau2"]
+        if mf is not None and (mf["K"] == 0 or k < mf["K"]):
+            r = row_filter_fft(res, mf["rows"], mf["nf"], mf["filter0"])
+            if mf["K"] == 0:
+                p = (p + sigma * r) / (1.0 + sigma)
+            else:
+                p = row_filter_fft(p + sigma * r, mf["rows"], mf["nf"], mf["ffilter"], inverse=True)
+        else:
+            p = (p + sigma * res) / (1.0 + sigma)
         if prox is not None:
             q = io.proxtv_dual(x, q, shape, prox["sigma2"], beta, prox.get("l2", True), prox.get("diff_type", 0))
             rhs = bdd_backward(geom, p, -1) - io.proxtv_divergence(q, shape, prox.get("diff_type", 0))

@@ -6,6 +6,7 @@ Run where the OMEGA sources are, with $OMEGA_REFERENCE naming their root:
     python tests/golden/make_golden.py volumes    # the type-3 tables only
     python tests/golden/make_golden.py nlm        # the NLM patch weights only
     python tests/golden/make_golden.py tv         # the anatomical TV preparation only
+    python tests/golden/make_golden.py ramp       # the measurement filters only
     python tests/golden/make_golden.py geom NAME  # one geometry fixture
 
 For every option set in configs.py it imports the reference's own Python
@@ -247,6 +248,24 @@ def tv_fixture():
     print("tv_anat", {k: v.shape for k, v in out.items()})
 
 
+def ramp_fixture():
+    """The reference's rampFilt (omegatomo/reconstruction/rampfilt.py) for
+    every window, two cut-offs and even / odd lengths, stored in
+    ramp_filters.npz (key window_c_N)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "omega_rampfilt", os.path.join(REF, "source", "Python", "omegatomo", "reconstruction", "rampfilt.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    out = {}
+    for window in ("hamming", "hann", "blackman", "nuttal", "gaussian", "shepp-logan", "cosine", "parzen", "none"):
+        for c in (1.0, 0.8):
+            for N in (512, 64, 101):
+                out[f"{window}_{c}_{N}"] = np.asarray(mod.rampFilt(N, window, c, 0.25))
+    np.savez_compressed(os.path.join(HERE, "ramp_filters.npz"), **out)
+    print("ramp_filters", len(out))
+
+
 # type-3 table cases: tube radius, voxel radius (before scaling), voxel size (dx, dy, dz)
 VOLUME_CASES = {"a": (1.0, 1.0, (2.0, 2.0, 2.5)), "b": (2.5, 1.0, (1.5, 1.5, 1.5))}
 
@@ -257,6 +276,9 @@ def main():
         return
     if sys.argv[1:] == ["nlm"]:
         nlm_fixture()
+        return
+    if sys.argv[1:] == ["ramp"]:
+        ramp_fixture()
         return
     if sys.argv[1:] == ["tv"]:
         tv_fixture()
@@ -274,6 +296,7 @@ def main():
     volume_fixture()
     nlm_fixture()
     tv_fixture()
+    ramp_fixture()
     psf_fixture(proj)
     prior_weight_fixture(proj)
     allc = dict(CONFIGS)

@@ -174,6 +174,72 @@ def test_builtin_pdhg_ct_proxtv(cuda):
     assert orc.rel_l2(plain, ref) > 1e-2
 
 
+@pytest.mark.parametrize("rows,window", [(100, "hann"), (512, "hamming"), (37, "parzen")])
+def test_row_filter_kernel(cuda, rows, window):
+    """omb_row_filter (circular convolution with the taps) against the
+    reference's Fourier-domain filtering restated in FP64."""
+    import ctypes
+
+    import torch
+    from omega_b200 import _native, filters
+    from omega_b200.reconstruction import _stream
+    nf, f0, ff, h, hinv = filters.pdhg_row_filters(rows, 1.0, window)
+    rng = np.random.default_rng(rows)
+    v = rng.normal(size=rows * 203).astype(np.float32)
+    V, H, HI = (torch.tensor(a, device=cuda) for a in (v, h, hinv))
+    out = torch.empty_like(V)
+    for taps, filt, inv in ((H, f0, False), (HI, ff, True)):
+        _native.call("omb_row_filter", ctypes.c_void_p(V.data_ptr()), ctypes.c_void_p(out.data_ptr()), rows, 203,
+                     ctypes.c_void_p(taps.data_ptr()), nf, _stream(cuda))
+        want = orc.row_filter_fft(v, rows, nf, filt, inverse=inv)
+        assert orc.rel_l2(out.cpu().numpy(), want) < 1e-6, orc.rel_l2(out.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("K", [2, 0])
+def test_builtin_pdhg_ct_measurement_filter(cuda, K):
+    """PDHG + TV with the filtering-based measurement preconditioner
+    (precondTypeMeas[1]): K filtering iterations with the inverse-filtered
+    dual step, then the plain steps with tauCP; K = 0 filters every
+    residual."""
+    from omega_b200 import filters
+    from omega_b200 import reconstruction as rec
+    o = make_options("ct_mini5")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(6)
+    truth = rng.uniform(0.0, 0.02, g.n_img)
+    counts = 1e4 * np.exp(-orc.bdd_forward(g, truth, -1))
+    o.SinM = rng.poisson(counts).astype(np.float32) + 1
+    o.PDHG = True
+    o.TV = True
+    o.beta = 0.05
+    o.Niter = 5
+    o.x0 = np.zeros(g.n_img, dtype=np.float32)
+    o.precondTypeMeas = np.array([False, True])
+    o.filteringIterations = K
+    o.filterWindow = "hann"
+    # the step after the filtering iterations: 1 / the FP64 power-method eigenvalue of A^T A
+    xv = np.abs(rng.normal(size=g.n_img))
+    xv /= np.linalg.norm(xv)
+    for _ in range(20):
+        bv = orc.bdd_backward(g, orc.bdd_forward(g, xv, -1), -1)
+        L = float(bv @ xv / (xv @ xv))
+        xv = bv / np.linalg.norm(bv)
+    tau2 = float(np.float32(1.0 / L))
+    o.tauCP = tau2
+    out, _ = rec.reconstructions_mainCT(o)
+    tau_f = o.tau_used
+    assert tau_f > 0
+    y = np.asarray(o.SinM, dtype=np.float32).ravel(order='F')
+    nr = int(o.nRowsD)
+    nf, f0, ff, _, _ = filters.pdhg_row_filters(nr, 1.0, "hann")
+    mf = dict(filter0=f0, ffilter=ff, nf=nf, rows=nr, K=K, tau2=tau2)
+    ref = orc.pdhg_tv(g, y.astype(np.float64), np.zeros(g.n_img), 5, tau_f, 0.05, 1e-4, meas_filter=mf)
+    x = out.ravel(order='F')
+    assert orc.rel_l2(x, ref) < 1e-4, orc.rel_l2(x, ref)
+    plain = orc.pdhg_tv(g, y.astype(np.float64), np.zeros(g.n_img), 5, tau_f, 0.05, 1e-4)
+    assert orc.rel_l2(plain, ref) > 1e-3
+
+
 def test_builtin_osl_osem_rdp_matches_oracle(cuda):
     from omega_b200 import reconstruction as rec
     from oracle import image_oracle as io

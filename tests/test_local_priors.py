@@ -649,3 +649,39 @@ def test_weighted_mean(cuda, mean_type, no_norm):
                                                              no_norm))
     x = res.ravel(order='F')
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
+
+
+def test_ramp_filters_match_reference():
+    """omega_b200.filters.ramp_filter = the reference's rampFilt bit for bit
+    (tests/golden/ramp_filters.npz: every window, two cut-offs, even and odd
+    lengths), and the row filter's taps reproduce the Fourier-domain
+    filtering of the reference (filtering / filteringInverse)."""
+    import os
+    from omega_b200 import filters
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ramp_filters.npz"))
+    for k in g.files:
+        w, c, N = k.rsplit("_", 2)
+        ours = filters.ramp_filter(int(N), w, float(c), 0.25)
+        assert ours.dtype == g[k].dtype and np.array_equal(ours, g[k]), k
+    nf, f0, ff, h, hinv = filters.pdhg_row_filters(100, 0.7, "hann")
+    assert nf == 128 and f0[0] == np.float32(1e-6)
+    rng = np.random.default_rng(2)
+    v = rng.normal(size=100 * 5)
+    cols = v.reshape(-1, 100)
+    for taps, filt, inv in ((h, f0, False), (hinv, ff, True)):
+        direct = np.array([[np.dot(taps.astype(np.float64)[(i - np.arange(100)) % nf], col) for i in range(100)]
+                           for col in cols]).ravel()
+        fft = orc.row_filter_fft(v, 100, nf, filt, inverse=inv)
+        assert np.abs(direct - fft).max() < 1e-7 * np.abs(fft).max()
+
+
+def test_pdhg_preconditioner_selection_is_checked():
+    from conftest import make_options
+    from omega_b200 import reconstruction as rec
+    o = make_options("ct_mini5")
+    o.SinM = np.ones(int(o.nRowsD) * int(o.nColsD) * int(o.nProjections), np.float32)
+    o.PDHG = True
+    o.TV = True
+    o.precondTypeImage = np.array([1, 0, 0, 0, 0, 0, 0], bool)
+    with pytest.raises(ValueError, match="not PDHG"):
+        rec.reconstructions_mainCT(o)
