@@ -420,6 +420,11 @@ typedef struct omb_recon_params {
                                  dual step) */
     float tau_filt;           /* options.tauCPFilt: the primal step while filtering; <= 0: 1 / the power-method
                                  eigenvalue of A^T F A */
+    int32_t tgv;              /* PDHG: options.TGV, the proximal TGV (omb_proxtgv_step) in place of the TV term:
+                                 0 off, 1 3-D (TGVZ), 2 2-D (options.use2DTGV); the dual step divides by
+                                 1 + sigma beta (computeForwardProject.h:295-298) and the filter by sigma beta */
+    float alpha0_tgv;         /* options.alpha0TGV: the first-order ball (q) */
+    float alpha1_tgv;         /* options.alpha1TGV: the second-order ball (r) */
 } omb_recon_params;
 
 /*
@@ -484,6 +489,25 @@ int omb_proxtv_dual(const float *x, float *q, int32_t nx, int32_t ny, int32_t nz
                     int32_t l2_ball, int32_t diff_type, void *stream);
 int omb_proxtv_divergence(const float *q, float *rhs, int32_t nx, int32_t ny, int32_t nz, int32_t diff_type,
                           void *stream);
+
+/*
+ * One proximal TGV step of the PDHG loop (priors.h:284-313; ProxTVGradient
+ * with PROXTGV, ProxTVq, ProxTVDivergence, ProxTGVSymmDeriv, ProxTGVq,
+ * ProxTGVDivergence auxKernels.cl:1141-1560; forward differences, the only
+ * form the reference's kernels build):
+ *   q <- P_alpha0(q + sigma2 (D x - v)),   rhs -= div q,
+ *   r <- P_alpha1(r + sigma2 E v),         E v the symmetric derivative,
+ *   v1 = v + tau (q + div_sym r),          v <- v1 + theta (v1 - v).
+ * three_d != 0: v holds 3 images, r 6 (rxx, ryy, rzz, rxy, rxz, ryz);
+ * three_d == 0 (use2DTGV): v 2 images, r 3 (rxx, ryy, rxy), and the z
+ * difference of x enters q without a v term.  q holds 3 images.  All
+ * device, x fastest, zero before the first iteration.  The balls are
+ * per-voxel L2 (off-diagonal terms of r counted twice; l2_ball != 0) or
+ * max-norm.
+ */
+int omb_proxtgv_step(const float *x, float *q, float *r, float *v, float *rhs, int32_t nx, int32_t ny, int32_t nz,
+                     float sigma2, float alpha0, float alpha1, float theta, float tau, int32_t l2_ball, int32_t three_d,
+                     void *stream);
 
 /*
  * The TV gradients of the other TV settings (TVKernel built with -DSATV,

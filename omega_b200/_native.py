@@ -146,6 +146,9 @@ class ReconParams(ctypes.Structure):
         ("filter_rows", ctypes.c_int32),
         ("filter_iters", ctypes.c_int32),
         ("tau_filt", ctypes.c_float),
+        ("tgv", ctypes.c_int32),
+        ("alpha0_tgv", ctypes.c_float),
+        ("alpha1_tgv", ctypes.c_float),
     ]
 
 
@@ -278,6 +281,10 @@ EXPORTS = [
                                        ctypes.c_void_p]),
     ("omb_proxtv_divergence", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    ("omb_proxtgv_step", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                                        ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_void_p]),
     ("omb_mrp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p]),

@@ -107,13 +107,14 @@ __global__ void k_meas_residual(float *__restrict__ fp, const float *__restrict_
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) fp[i] -= __ldg(y + i);
 }
 
-// out = p + sigma r, divided by 1 + sigma when `divide`
+// out = (p + sigma r) / denom (denom 1: no division)
 __global__ void k_dual_step(const float *__restrict__ p, const float *__restrict__ r, float *__restrict__ out, int64_t n,
-                            float sigma, int divide) {
+                            float sigma, float denom) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const bool divide = denom != 1.f;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float v = p[i] + sigma * __ldg(r + i);
-        out[i] = divide ? v / (1.f + sigma) : v;
+        out[i] = divide ? v / denom : v;
     }
 }
 
@@ -126,9 +127,9 @@ int meas_residual(float *fp, const float *y, int64_t n, cudaStream_t st) {
     return OMB_OK;
 }
 
-int dual_step(const float *p, const float *r, float *out, int64_t n, float sigma, bool divide, cudaStream_t st) {
+int dual_step(const float *p, const float *r, float *out, int64_t n, float sigma, float denom, cudaStream_t st) {
     if (n <= 0) return OMB_OK;
-    k_dual_step<<<grid_for(n, 4), kBlock, 0, st>>>(p, r, out, n, sigma, divide ? 1 : 0);
+    k_dual_step<<<grid_for(n, 4), kBlock, 0, st>>>(p, r, out, n, sigma, denom);
     OMB_LAUNCH_CHECK("dual step launch");
     return OMB_OK;
 }

@@ -172,10 +172,10 @@ int sysmat_backward(const Grid &g, const SysMat &sm, const Frames &fr, int64_t m
                     cudaStream_t st);
 
 // Detector-row filtering (filter.cu): out = the circular convolution (length nf) of each column of nr rows with
-// h; the measurement residual fp -= y; the dual step out = p + sigma r (divided by 1 + sigma when divide).
+// h; the measurement residual fp -= y; the dual step out = (p + sigma r) / denom (denom 1: no division).
 int circ_filter(const float *in, float *out, int nr, int64_t ncols, const float *h, int nf, cudaStream_t st);
 int meas_residual(float *fp, const float *y, int64_t n, cudaStream_t st);
-int dual_step(const float *p, const float *r, float *out, int64_t n, float sigma, bool divide, cudaStream_t st);
+int dual_step(const float *p, const float *r, float *out, int64_t n, float sigma, float denom, cudaStream_t st);
 
 // Projector type 4 (interpolation), PET and CT.
 int interp_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, float dL, const float *img,

@@ -463,3 +463,141 @@ extern "C" int omb_proxtv_divergence(const float *q, float *rhs, int32_t nx, int
     OMB_LAUNCH_CHECK("proximal TV divergence launch");
     return OMB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Proximal TGV of the PDHG loop (options.TGV; priors.h:284-313; ProxTVGradient
+// with PROXTGV, ProxTVq, ProxTVDivergence, ProxTGVSymmDeriv, ProxTGVq,
+// ProxTGVDivergence auxKernels.cl:1141-1560; forward differences):
+//   q <- P_a0(q + sigma2 (D x - v)),  rhs -= div q,
+//   r <- P_a1(r + sigma2 E v),  v1 = v + tau (q + div_sym r),  v <- v1 + theta (v1 - v).
+// Z3: 3-D (v 3 images, r = (rxx, ryy, rzz, rxy, rxz, ryz)); else 2-D (v 2
+// images, r = (rxx, ryy, rxy); the z difference of x enters q without v).
+// ---------------------------------------------------------------------------
+namespace omb {
+namespace {
+
+// forward difference of a (zero beyond the last voxel) at n along a stride
+__device__ __forceinline__ float fwd_diff(const float *a, int64_t n, bool last, int64_t step) {
+    const float c = __ldg(a + n);
+    return last ? -c : __ldg(a + n + step) - c;
+}
+
+// backward difference (zero before the first voxel)
+__device__ __forceinline__ float bwd_diff(const float *a, int64_t n, bool first, int64_t step) {
+    const float c = __ldg(a + n);
+    return first ? c : c - __ldg(a + n - step);
+}
+
+template <bool L2, bool Z3>
+__global__ void __launch_bounds__(256) k_tgv_q(const float *__restrict__ x, const float *__restrict__ v,
+                                               float *__restrict__ q, int nx, int ny, int nz, float sigma2,
+                                               float alpha) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= nx || j >= ny || k >= nz) return;
+    const int64_t nxy = (int64_t)nx * ny, N = nxy * nz, n = i + (int64_t)j * nx + (int64_t)k * nxy;
+    const float gx = fwd_diff(x, n, i == nx - 1, 1) - __ldg(v + n);
+    const float gy = fwd_diff(x, n, j == ny - 1, nx) - __ldg(v + N + n);
+    const float gz = Z3 ? fwd_diff(x, n, k == nz - 1, nxy) - __ldg(v + 2 * N + n) : fwd_diff(x, n, k == nz - 1, nxy);
+    const float ax = q[n] + __fmul_rn(gx, sigma2), ay = q[n + N] + __fmul_rn(gy, sigma2);
+    const float az = q[n + 2 * N] + __fmul_rn(gz, sigma2);
+    const float scale = L2 ? fmaxf(1.f, sqrtf(ax * ax + ay * ay + az * az) / alpha)
+                           : fmaxf(fmaxf(fabsf(az), fmaxf(fabsf(ax), fabsf(ay))) / alpha, 1.f);
+    q[n] = ax / scale;
+    q[n + N] = ay / scale;
+    q[n + 2 * N] = az / scale;
+}
+
+template <bool L2, bool Z3>
+__global__ void __launch_bounds__(256) k_tgv_r(const float *__restrict__ v, float *__restrict__ r, int nx, int ny,
+                                               int nz, float sigma2, float alpha) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= nx || j >= ny || k >= nz) return;
+    const int64_t nxy = (int64_t)nx * ny, N = nxy * nz, n = i + (int64_t)j * nx + (int64_t)k * nxy;
+    const bool lx = i == nx - 1, ly = j == ny - 1, lz = k == nz - 1;
+    const float *vx = v, *vy = v + N, *vz = v + 2 * N;
+    const float h = __fmul_rn(sigma2, .5f);
+    if (Z3) {
+        float d[6];
+        d[0] = r[n] + __fmul_rn(fwd_diff(vx, n, lx, 1), sigma2);
+        d[1] = r[n + N] + __fmul_rn(fwd_diff(vy, n, ly, nx), sigma2);
+        d[2] = r[n + 2 * N] + __fmul_rn(fwd_diff(vz, n, lz, nxy), sigma2);
+        d[3] = r[n + 3 * N] + __fmul_rn(fwd_diff(vx, n, ly, nx) + fwd_diff(vy, n, lx, 1), h);
+        d[4] = r[n + 4 * N] + __fmul_rn(fwd_diff(vx, n, lz, nxy) + fwd_diff(vz, n, lx, 1), h);
+        d[5] = r[n + 5 * N] + __fmul_rn(fwd_diff(vy, n, lz, nxy) + fwd_diff(vz, n, ly, nx), h);
+        const float scale =
+            L2 ? fmaxf(1.f, sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2] +
+                                  2.f * (d[3] * d[3]) + 2.f * (d[4] * d[4]) + 2.f * (d[5] * d[5])) / alpha)
+               : fmaxf(fmaxf(fabsf(d[5]), fmaxf(fabsf(d[4]), fmaxf(fabsf(d[3]), fmaxf(fabsf(d[2]),
+                                                                                       fmaxf(fabsf(d[0]), fabsf(d[1])))))) /
+                           alpha,
+                       1.f);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) r[n + c * N] = d[c] / scale;
+    } else {
+        float d[3];
+        d[0] = r[n] + __fmul_rn(fwd_diff(vx, n, lx, 1), sigma2);
+        d[1] = r[n + N] + __fmul_rn(fwd_diff(vy, n, ly, nx), sigma2);
+        d[2] = r[n + 2 * N] + __fmul_rn(fwd_diff(vx, n, ly, nx) + fwd_diff(vy, n, lx, 1), h);
+        const float scale = L2 ? fmaxf(1.f, sqrtf(d[0] * d[0] + d[1] * d[1] + 2.f * (d[2] * d[2])) / alpha)
+                               : fmaxf(fmaxf(fabsf(d[2]), fmaxf(fabsf(d[0]), fabsf(d[1]))) / alpha, 1.f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) r[n + c * N] = d[c] / scale;
+    }
+}
+
+template <bool Z3>
+__global__ void __launch_bounds__(256) k_tgv_v(const float *__restrict__ r, const float *__restrict__ q,
+                                               float *__restrict__ v, int nx, int ny, int nz, float theta, float tau) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= nx || j >= ny || k >= nz) return;
+    const int64_t nxy = (int64_t)nx * ny, N = nxy * nz, n = i + (int64_t)j * nx + (int64_t)k * nxy;
+    const bool fx = i == 0, fy = j == 0, fz = k == 0;
+    float dv[3];
+    if (Z3) {
+        dv[0] = bwd_diff(r, n, fx, 1) + bwd_diff(r + 3 * N, n, fy, nx) + bwd_diff(r + 4 * N, n, fz, nxy);
+        dv[1] = bwd_diff(r + N, n, fy, nx) + bwd_diff(r + 3 * N, n, fx, 1) + bwd_diff(r + 5 * N, n, fz, nxy);
+        dv[2] = bwd_diff(r + 2 * N, n, fz, nxy) + bwd_diff(r + 4 * N, n, fx, 1) + bwd_diff(r + 5 * N, n, fy, nx);
+    } else {
+        dv[0] = bwd_diff(r, n, fx, 1) + bwd_diff(r + 2 * N, n, fy, nx);
+        dv[1] = bwd_diff(r + N, n, fy, nx) + bwd_diff(r + 2 * N, n, fx, 1);
+    }
+#pragma unroll
+    for (int c = 0; c < (Z3 ? 3 : 2); ++c) {
+        const float vo = v[n + c * N];
+        const float v1 = fmaf(tau, __ldg(q + n + c * N) + dv[c], vo);
+        v[n + c * N] = fmaf(theta, v1 - vo, v1);
+    }
+}
+
+}  // namespace
+}  // namespace omb
+
+extern "C" int omb_proxtgv_step(const float *x, float *q, float *r, float *v, float *rhs, int32_t nx, int32_t ny,
+                                int32_t nz, float sigma2, float alpha0, float alpha1, float theta, float tau,
+                                int32_t l2_ball, int32_t three_d, void *stream) {
+    using namespace omb;
+    if (!x || !q || !r || !v || !rhs) return set_error(OMB_ERR_INVALID, "NULL pointer passed to omb_proxtgv_step");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    if (!(alpha0 > 0.f) || !(alpha1 > 0.f)) return set_error(OMB_ERR_INVALID, "the TGV weights alpha0, alpha1 must be positive");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    cudaStream_t st = (cudaStream_t)stream;
+#define OMB_TGV(L, Z)                                                                         \
+    k_tgv_q<L, Z><<<grid, block, 0, st>>>(x, v, q, nx, ny, nz, sigma2, alpha0);               \
+    k_proxtv_div<0><<<grid, block, 0, st>>>(q, rhs, nx, ny, nz);                              \
+    k_tgv_r<L, Z><<<grid, block, 0, st>>>(v, r, nx, ny, nz, sigma2, alpha1);                  \
+    k_tgv_v<Z><<<grid, block, 0, st>>>(r, q, v, nx, ny, nz, theta, tau);
+    if (l2_ball && three_d) {
+        OMB_TGV(true, true)
+    } else if (l2_ball) {
+        OMB_TGV(true, false)
+    } else if (three_d) {
+        OMB_TGV(false, true)
+    } else {
+        OMB_TGV(false, false)
+    }
+#undef OMB_TGV
+    OMB_LAUNCH_CHECK("proximal TGV launch");
+    return OMB_OK;
+}

@@ -84,6 +84,15 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         if (!(p->beta > 0.f)) return set_error(OMB_ERR_INVALID, "proximal TV needs beta > 0");
         if (p->diff_type != 0 && p->diff_type != 1) return set_error(OMB_ERR_INVALID, "diff_type must be 0 or 1");
     }
+    if (alg == OMB_RECON_PDHG_TV && p->tgv) {
+        if (p->tgv != 1 && p->tgv != 2) return set_error(OMB_ERR_INVALID, "tgv must be 0, 1 (3-D) or 2 (2-D)");
+        if (p->tv_prox) return set_error(OMB_ERR_INVALID, "proximal TV and TGV exclude each other");
+        if (!(p->alpha0_tgv > 0.f) || !(p->alpha1_tgv > 0.f))
+            return set_error(OMB_ERR_INVALID, "TGV needs alpha0_tgv > 0 and alpha1_tgv > 0");
+        if (p->diff_type != 0)
+            return set_error(OMB_ERR_UNSUPPORTED, "TGV is built with forward differences only (diff_type 0)");
+        if (!(p->beta >= 0.f)) return set_error(OMB_ERR_INVALID, "TGV needs beta >= 0");
+    }
     if (alg == OMB_RECON_PDHG_TV || p->prior == OMB_PRIOR_TV) {
         if (p->tv_variant < OMB_TV_PLAIN || p->tv_variant > OMB_TV_APLS)
             return set_error(OMB_ERR_INVALID, "unknown TV variant");
@@ -305,7 +314,7 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         const int64_t m_all = omb_measurement_count(h, -1);  // one subset: all measurements
         if (m_all < 0) return -1;
         const Grid g = handle_grid(h);
-        DevBuf xn, u, pd, wm, wi, work, q;
+        DevBuf xn, u, pd, wm, wi, work, q, tr, tv;
         if ((st = alloc(xn, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(u, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
         if ((st = alloc(pd, (size_t)m_all * sizeof(float), s)) != OMB_OK) return st;
@@ -315,6 +324,17 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             // the proximal TV's dual variable, three images starting at zero
             if ((st = alloc(q, 3 * (size_t)n * sizeof(float), s)) != OMB_OK) return st;
             OMB_CUDA_TRY(cudaMemsetAsync(q.p, 0, 3 * (size_t)n * sizeof(float), s));
+        }
+        const bool tgv = p->tgv != 0;
+        if (tgv) {
+            // the TGV variables (functions.hpp:2936-2952): q 3 images, r 6 (3-D) or 3 (2-D), v 3 or 2, all zero
+            const size_t nr = p->tgv == 1 ? 6 : 3, nv = p->tgv == 1 ? 3 : 2;
+            if ((st = alloc(q, 3 * (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+            if ((st = alloc(tr, nr * (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+            if ((st = alloc(tv, nv * (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+            OMB_CUDA_TRY(cudaMemsetAsync(q.p, 0, 3 * (size_t)n * sizeof(float), s));
+            OMB_CUDA_TRY(cudaMemsetAsync(tr.p, 0, nr * (size_t)n * sizeof(float), s));
+            OMB_CUDA_TRY(cudaMemsetAsync(tv.p, 0, nv * (size_t)n * sizeof(float), s));
         }
         // the filtering-based measurement preconditioner (functions.hpp:2109-2166, computeForwardProject.h:
         // 21-45, 253-298): the residual filtered along the detector rows with h; while k < K the dual step is
@@ -398,22 +418,32 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         // one iteration with steps tau_k, sig_k; fmode 0 no filtering, 1 filtered residual and the plain dual
         // step, 2 filtered residual and the inverse-filtered dual step.  The plain TV gradient is fused into
         // the primal step when nothing else comes between; the other TV terms are added to A^T p before it
+        // the plain dual step divides by 1 + sigma, by 1 + sigma beta with TGV (computeForwardProject.h:295-303)
         auto one = [&](float *xa, float *xb, float tau_k, float sig_k, int fmode) {
-            if (fmode == 0 && !p->tv_prox && p->tv_variant == OMB_TV_PLAIN)
+            if (fmode == 0 && !p->tv_prox && !tgv && p->tv_variant == OMB_TV_PLAIN)
                 return omb_pdhg_iteration(h, xa, xb, u.f(), pd.f(), y, tau_k, sig_k, p->theta, p->beta,
                                           p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
+            const float denom = tgv ? 1.f + sig_k * p->beta : 1.f + sig_k;
             int e = omb_forward(h, -1, xa, wm.f(), stream);
-            if (e == OMB_OK && fmode == 0) e = omb_pdhg_dual(pd.f(), wm.f(), y, m_all, sig_k, stream);
+            if (e == OMB_OK && fmode == 0 && !tgv) e = omb_pdhg_dual(pd.f(), wm.f(), y, m_all, sig_k, stream);
+            if (e == OMB_OK && fmode == 0 && tgv) {
+                e = meas_residual(wm.f(), y, m_all, s);
+                if (e == OMB_OK) e = dual_step(pd.f(), wm.f(), pd.f(), m_all, sig_k, denom, s);
+            }
             if (e == OMB_OK && fmode > 0) {
                 e = meas_residual(wm.f(), y, m_all, s);
                 if (e == OMB_OK) e = circ_filter(wm.f(), wf.f(), p->filter_rows, fcols, p->filter_h, p->filter_nf, s);
-                if (e == OMB_OK && fmode == 1) e = dual_step(pd.f(), wf.f(), pd.f(), m_all, sig_k, true, s);
-                if (e == OMB_OK && fmode == 2) e = dual_step(pd.f(), wf.f(), wm.f(), m_all, sig_k, false, s);
+                if (e == OMB_OK && fmode == 1) e = dual_step(pd.f(), wf.f(), pd.f(), m_all, sig_k, denom, s);
+                if (e == OMB_OK && fmode == 2) e = dual_step(pd.f(), wf.f(), wm.f(), m_all, sig_k, 1.f, s);
                 if (e == OMB_OK && fmode == 2)
                     e = circ_filter(wm.f(), pd.f(), p->filter_rows, fcols, p->filter_hinv, p->filter_nf, s);
             }
             if (e == OMB_OK) e = omb_backward(h, -1, pd.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC, stream);
-            if (e == OMB_OK && p->tv_prox) {
+            if (e == OMB_OK && tgv) {
+                // priors.h:284-313: theta = thetaCP, tau the current primal step
+                e = omb_proxtgv_step(xa, q.f(), tr.f(), tv.f(), wi.f(), g.nx, g.ny, g.nz, p->sigma2, p->alpha0_tgv,
+                                     p->alpha1_tgv, p->theta, tau_k, p->l2_ball, p->tgv == 1, stream);
+            } else if (e == OMB_OK && p->tv_prox) {
                 // priors.h:261-281 between the backprojection and the primal step
                 e = omb_proxtv_dual(xa, q.f(), g.nx, g.ny, g.nz, p->sigma2, p->beta, p->l2_ball, p->diff_type, stream);
                 if (e == OMB_OK) e = omb_proxtv_divergence(q.f(), wi.f(), g.nx, g.ny, g.nz, p->diff_type, stream);

@@ -223,6 +223,12 @@ class projectorClass:
     sigma2CP = 1.
     useL2Ball = True
     derivativeType = 0
+    # TGV with PDHG (proj.py:351-352, 360, 411 of the reference): the
+    # first- and second-order ball radii, 2-D TGV (no z component of v)
+    TGV = False
+    alpha0TGV = 0.
+    alpha1TGV = 0.
+    use2DTGV = False
     tauCP = 0.
     sigmaCP = 1.
     thetaCP = 1.

@@ -365,13 +365,22 @@ def reconstructions_main(options):
     if method != 'PDHG' and options.CT:
         raise ValueError(method + ' is built for PET data')
     prox = bool(getattr(options, 'ProxTV', False))
-    if options.PDHG and not (options.TV or prox):
-        raise ValueError('PDHG is built with the TV prior (options.TV = True) or the proximal TV (options.ProxTV = '
-                         'True)')
-    if options.PDHG and options.TV and prox:
-        raise ValueError('Select one of options.TV and options.ProxTV')
+    tgv = bool(getattr(options, 'TGV', False))
+    if options.PDHG and not (options.TV or prox or tgv):
+        raise ValueError('PDHG is built with the TV prior (options.TV = True), the proximal TV (options.ProxTV = '
+                         'True) or TGV (options.TGV = True)')
+    if options.PDHG and int(bool(options.TV)) + int(prox) + int(tgv) > 1:
+        raise ValueError('Select one of options.TV, options.ProxTV and options.TGV')
     if prox and not options.PDHG:
         raise ValueError('options.ProxTV is built for PDHG')
+    if tgv and not options.PDHG:
+        raise ValueError('options.TGV is built for PDHG')
+    if tgv:
+        if not (float(getattr(options, 'alpha0TGV', 0.)) > 0 and float(getattr(options, 'alpha1TGV', 0.)) > 0):
+            raise ValueError('options.TGV needs options.alpha0TGV > 0 and options.alpha1TGV > 0')
+        if int(getattr(options, 'derivativeType', 0)) != 0:
+            # the reference's ProxTGVSymmDeriv does not compile with DIFFTYPE 1 (auxKernels.cl:1422)
+            raise ValueError('options.TGV is built with forward differences (derivativeType 0)')
     tv_set = None
     if (prior and (tvp or apls)) or (options.PDHG and options.TV):
         # the TV gradient variant of the TV / APLS options (ProjectorClass.h:900-918)
@@ -545,6 +554,9 @@ def reconstructions_main(options):
             from . import filters
             nr = int(np.ravel(options.nRowsD)[0]) if options.CT else int(np.ravel(options.Ndist)[0])
             sig = float(np.ravel(options.sigmaCP)[0])
+            if tgv:
+                # the inverse filter's sigma times beta with TGV (prepass.py:1133-1134)
+                sig *= float(options.beta)
             nf, _, _, fh, fhinv = filters.pdhg_row_filters(nr, sig, getattr(options, 'filterWindow', 'hamming'),
                                                            float(getattr(options, 'cutoffFrequency', 1.0)),
                                                            float(getattr(options, 'normalFilterSigma', 0.25)))
@@ -568,6 +580,16 @@ def reconstructions_main(options):
             raise ValueError('derivativeType must be 0 or 1')
         if not float(options.beta) > 0:
             raise ValueError('options.ProxTV needs options.beta > 0')
+    if options.PDHG and tgv:
+        # TGV of the PDHG loop (priors.h:284-313): the balls alpha0TGV,
+        # alpha1TGV, the dual step sigma2CP; the data dual divides by
+        # 1 + sigma beta
+        p.tgv = 2 if bool(getattr(options, 'use2DTGV', False)) else 1
+        p.alpha0_tgv = float(options.alpha0TGV)
+        p.alpha1_tgv = float(options.alpha1TGV)
+        p.sigma2 = float(np.ravel(getattr(options, 'sigma2CP', 1.0))[0])
+        p.l2_ball = 1 if getattr(options, 'useL2Ball', True) else 0
+        p.diff_type = 0
     if tv_set is not None:
         p.tv_variant, p.tv_sigma, p.tv_c, p.tv_smoothing, tv_ref = tv_set
         if tv_ref is not None:

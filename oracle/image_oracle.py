@@ -338,6 +338,75 @@ def proxtv_divergence(q, shape, diff_type=0):
     return out.ravel(order='F')
 
 
+def proxtgv_step(x, q, r, v, rhs, shape, sigma2, alpha0, alpha1, theta, tau, l2=True, three_d=True):
+    """One proximal TGV step of the PDHG loop (priors.h:284-313; ProxTVGradient
+    with PROXTGV, ProxTVq, ProxTVDivergence, ProxTGVSymmDeriv, ProxTGVq,
+    ProxTGVDivergence auxKernels.cl:1141-1560, forward differences):
+      q <- P_alpha0(q + sigma2 (D x - v)),  rhs <- rhs - div q,
+      r <- P_alpha1(r + sigma2 E v),
+      v1 = v + tau (q + div_sym r),  v <- v1 + theta (v1 - v).
+    3-D (three_d): v = (vx, vy, vz), r = (rxx, ryy, rzz, rxy, rxz, ryz);
+    2-D (use2DTGV): v = (vx, vy), r = (rxx, ryy, rxy), and the z difference
+    of x enters q without a v term.  P: the per-voxel L2 ball (off-diagonal
+    terms counted twice) or the max-norm ball.  Arrays (k, N), x fastest;
+    returns (q, r, v, rhs)."""
+    def img(a):
+        return np.asarray(a, dtype=np.float64).reshape(shape, order='F')
+
+    def flat(a):
+        return a.ravel(order='F')
+    X = img(x)
+    Q = [img(a) for a in np.asarray(q, dtype=np.float64).reshape(3, -1)]
+    nr = 6 if three_d else 3
+    nv = 3 if three_d else 2
+    R = [img(a) for a in np.asarray(r, dtype=np.float64).reshape(nr, -1)]
+    V = [img(a) for a in np.asarray(v, dtype=np.float64).reshape(nv, -1)]
+    # TV part with v
+    g = [_diff(X, a, True) for a in range(3)]
+    for a in range(nv):
+        g[a] = g[a] - V[a]
+    Qn = [Q[a] + sigma2 * g[a] for a in range(3)]
+    nq = np.sqrt(Qn[0] ** 2 + Qn[1] ** 2 + Qn[2] ** 2) if l2 else np.maximum(np.abs(Qn[2]), np.maximum(np.abs(Qn[0]), np.abs(Qn[1])))
+    sq = np.maximum(1.0, nq / alpha0)
+    Qn = [a / sq for a in Qn]
+    div = sum(_diff(Qn[a], a, False) for a in range(3))
+    rhs_n = np.asarray(rhs, dtype=np.float64) - flat(div)
+    # symmetric derivative of v
+    if three_d:
+        E = [_diff(V[0], 0, True), _diff(V[1], 1, True), _diff(V[2], 2, True),
+             0.5 * (_diff(V[0], 1, True) + _diff(V[1], 0, True)),
+             0.5 * (_diff(V[0], 2, True) + _diff(V[2], 0, True)),
+             0.5 * (_diff(V[1], 2, True) + _diff(V[2], 1, True))]
+    else:
+        E = [_diff(V[0], 0, True), _diff(V[1], 1, True), 0.5 * (_diff(V[0], 1, True) + _diff(V[1], 0, True))]
+    Rn = [R[k] + sigma2 * E[k] for k in range(nr)]
+    if three_d:
+        dg, od = Rn[:3], Rn[3:]
+    else:
+        dg, od = Rn[:2] + [np.zeros_like(Rn[0])], Rn[2:] + [np.zeros_like(Rn[0])] * 2
+    if l2:
+        nrm = np.sqrt(dg[0] ** 2 + dg[1] ** 2 + dg[2] ** 2 + 2 * (od[0] ** 2 + od[1] ** 2 + od[2] ** 2))
+        sr = np.maximum(1.0, nrm / alpha1)
+    else:
+        m = np.maximum(np.abs(od[2]), np.maximum(np.abs(od[1]), np.maximum(np.abs(od[0]), np.maximum(
+            np.abs(dg[2]), np.maximum(np.abs(dg[0]), np.abs(dg[1]))))))
+        sr = np.maximum(m / alpha1, 1.0)
+    Rn = [a / sr for a in Rn]
+    # v update with the divergence of the symmetric tensor
+    if three_d:
+        dv = [_diff(Rn[0], 0, False) + _diff(Rn[3], 1, False) + _diff(Rn[4], 2, False),
+              _diff(Rn[1], 1, False) + _diff(Rn[3], 0, False) + _diff(Rn[5], 2, False),
+              _diff(Rn[2], 2, False) + _diff(Rn[4], 0, False) + _diff(Rn[5], 1, False)]
+    else:
+        dv = [_diff(Rn[0], 0, False) + _diff(Rn[2], 1, False), _diff(Rn[1], 1, False) + _diff(Rn[2], 0, False)]
+    Vn = []
+    for a in range(nv):
+        v1 = V[a] + tau * (Qn[a] + dv[a])
+        Vn.append(v1 + theta * (v1 - V[a]))
+    return (np.stack([flat(a) for a in Qn]), np.stack([flat(a) for a in Rn]), np.stack([flat(a) for a in Vn]),
+            rhs_n)
+
+
 # ---------------------------------------------------------------------------
 # TV gradient variants of TVKernel (auxKernels.cl:1733-1990): the image read
 # edge-clamped (the texture path), the anatomical reference S read as zero

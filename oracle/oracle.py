@@ -775,7 +775,7 @@ def row_filter_fft(v, rows, nf, filt, inverse=False):
 
 
 def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1.0, eps=1e-5,
-            positivity=True, tv_grad=None, prox=None, meas_filter=None):
+            positivity=True, tv_grad=None, prox=None, meas_filter=None, tgv=None):
     """PDHG with a TV-gradient term, one subset (computeForwardProject.h:227-316,
     algorithms.h:329-420, auxKernels.cl:2034-2062), in FP64.  tv_grad(x), when
     given, replaces the plain TV term beta * dTV(x) (the other TVKernel forms).
@@ -786,13 +786,22 @@ def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1
     residual filtered by filter0; for k < K the dual step (p + sigma F r)
     divided by ffilter in the Fourier domain, from k = K on the plain dual
     step without filtering and the primal step tau2 (K = 0: every residual
-    filtered, plain dual step)."""
+    filtered, plain dual step).  tgv = dict(alpha0, alpha1, sigma2, l2,
+    three_d): TGV instead of the TV term (priors.h:284-313,
+    image_oracle.proxtgv_step with theta and the current tau), the plain
+    dual step divided by 1 + sigma beta (computeForwardProject.h:295-298;
+    with meas_filter, its ffilter built from sigma beta)."""
     from oracle import image_oracle as io
     shape = (geom.nx, geom.ny, geom.nz)
     x = np.asarray(x0, dtype=np.float64).copy()
     u = x.copy()
     p = np.zeros(geom.rays(-1), dtype=np.float64)
     q = np.zeros((3, geom.n_img))
+    if tgv is not None:
+        three_d = tgv.get("three_d", True)
+        r_t = np.zeros((6 if three_d else 3, geom.n_img))
+        v_t = np.zeros((3 if three_d else 2, geom.n_img))
+    den = 1.0 + sigma * (beta if tgv is not None else 1.0)
     yy = np.asarray(y, dtype=np.float64)
     for k in range(n_iter):
         res = bdd_forward(geom, x, -1) - yy
@@ -802,12 +811,16 @@ def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1
         if mf is not None and (mf["K"] == 0 or k < mf["K"]):
             r = row_filter_fft(res, mf["rows"], mf["nf"], mf["filter0"])
             if mf["K"] == 0:
-                p = (p + sigma * r) / (1.0 + sigma)
+                p = (p + sigma * r) / den
             else:
                 p = row_filter_fft(p + sigma * r, mf["rows"], mf["nf"], mf["ffilter"], inverse=True)
         else:
-            p = (p + sigma * res) / (1.0 + sigma)
-        if prox is not None:
+            p = (p + sigma * res) / den
+        if tgv is not None:
+            q, r_t, v_t, rhs = io.proxtgv_step(x, q, r_t, v_t, bdd_backward(geom, p, -1), shape, tgv["sigma2"],
+                                               tgv["alpha0"], tgv["alpha1"], theta, tau, tgv.get("l2", True),
+                                               three_d)
+        elif prox is not None:
             q = io.proxtv_dual(x, q, shape, prox["sigma2"], beta, prox.get("l2", True), prox.get("diff_type", 0))
             rhs = bdd_backward(geom, p, -1) - io.proxtv_divergence(q, shape, prox.get("diff_type", 0))
         else:

@@ -62,6 +62,8 @@ def _lib(variant, precision):
             L.refcl_tv_gradient_ex.argtypes = [_I, _I, _I, _P, _D, _D, _D, _D, _P, _P]
         if hasattr(L, "refcl_proxtv"):
             L.refcl_proxtv.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D]
+        if hasattr(L, "refcl_proxtgv"):
+            L.refcl_proxtgv.argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _D, _D, _D, _D, _D]
         _libs[key] = L
     return _libs[key]
 
@@ -296,3 +298,20 @@ def proxtv_step(x, q, rhs, shape, sigma2, alpha, l2=True, diff_type=0, precision
     _lib(lib, precision).refcl_proxtv(nx, ny, nz, _dp(xx), _dp(qq), _dp(rr), _scalar(sigma2, exact_inputs),
                                       _scalar(alpha, exact_inputs))
     return qq.reshape(3, -1), rr
+
+
+def proxtgv_step(x, q, r, v, rhs, shape, sigma2, alpha0, alpha1, theta, tau, l2=True, three_d=True, precision="d",
+                 exact_inputs=False):
+    """One proximal TGV step with the reference's kernels (-DPROXTV -DPROXTGV,
+    -DTGVZ for 3-D, -DL2 for the L2 balls): returns (q, r, v, rhs)."""
+    nx, ny, nz = shape
+    lib = "aux_proxtgv" + ("" if three_d else "2d") + ("_l2" if l2 else "_max")
+    xx = np.ascontiguousarray(x, dtype=np.float64).ravel()
+    qq = np.ascontiguousarray(q, dtype=np.float64).ravel().copy()
+    rr = np.ascontiguousarray(r, dtype=np.float64).ravel().copy()
+    vv = np.ascontiguousarray(v, dtype=np.float64).ravel().copy()
+    hh = np.ascontiguousarray(rhs, dtype=np.float64).ravel().copy()
+    e = exact_inputs
+    _lib(lib, precision).refcl_proxtgv(nx, ny, nz, _dp(xx), _dp(qq), _dp(rr), _dp(vv), _dp(hh), _scalar(sigma2, e),
+                                       _scalar(alpha0, e), _scalar(alpha1, e), _scalar(theta, e), _scalar(tau, e))
+    return qq.reshape(3, -1), rr.reshape(6 if three_d else 3, -1), vv.reshape(3 if three_d else 2, -1), hh

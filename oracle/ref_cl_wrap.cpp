@@ -332,7 +332,7 @@ REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, doub
 }
 #endif
 
-#if defined(PROXTV)
+#if defined(PROXTV) && !defined(PROXTGV)
 /* One proximal-TV step of the PDHG loop (priors.h:261-281): ProxTVGradient
  * (q += sigma2 * the image differences), ProxTVq (q onto the alpha ball: L2
  * with -DL2, else the max norm), ProxTVDivergence (rhs -= the divergence of
@@ -362,6 +362,73 @@ REFCL_EXPORT int refcl_proxtv(int nx, int ny, int nz, const double *im, double *
     from_real(QX, q);
     from_real(QY, q + N);
     from_real(QZ, q + 2 * N);
+    from_real(R, rhs);
+    return 0;
+}
+#endif
+
+#if defined(PROXTGV)
+/* One proximal TGV step (priors.h:284-313): ProxTVGradient with v, ProxTVq
+ * (alpha0), ProxTVDivergence (rhs), ProxTGVSymmDeriv, ProxTGVq (alpha1),
+ * ProxTGVDivergence (theta, tau).  q: 3 images; r: 6 (TGVZ) or 3; v: 3 or 2;
+ * all updated in place, as is rhs. */
+REFCL_EXPORT int refcl_proxtgv(int nx, int ny, int nz, const double *im, double *q, double *r, double *v, double *rhs,
+                               double sigma2, double alpha0, double alpha1, double theta, double tau) {
+    const size_t N = (size_t)nx * ny * nz;
+#if defined(TGVZ)
+    const int NR = 6, NV = 3;
+#else
+    const int NR = 3, NV = 2;
+#endif
+    rvec I = to_real(im, N), R = to_real(rhs, N);
+    rvec Q[3], RR[6], VV[3];
+    for (int k = 0; k < 3; ++k) Q[k] = to_real(q + k * N, N);
+    for (int k = 0; k < NR; ++k) RR[k] = to_real(r + k * N, N);
+    for (int k = 0; k < NV; ++k) VV[k] = to_real(v + k * N, N);
+    const int3 Nn = make_int3(nx, ny, nz);
+    auto each = [&](auto &&f) {
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                    f();
+                }
+    };
+#if defined(TGVZ)
+    each([&] { ProxTVGradient(Nn, Nn, I.data(), Q[0].data(), Q[1].data(), Q[2].data(), (omb_real)sigma2,
+                              VV[0].data(), VV[1].data(), VV[2].data()); });
+#else
+    each([&] { ProxTVGradient(Nn, Nn, I.data(), Q[0].data(), Q[1].data(), Q[2].data(), (omb_real)sigma2,
+                              VV[0].data(), VV[1].data()); });
+#endif
+    for (size_t x = 0; x < N; ++x) {
+        set_item((unsigned)x, 0u, 0u);
+        ProxTVq(Q[0].data(), Q[1].data(), Q[2].data(), (omb_real)alpha0);
+    }
+    each([&] { ProxTVDivergence(Nn, Nn, Q[0].data(), Q[1].data(), Q[2].data(), R.data()); });
+#if defined(TGVZ)
+    each([&] { ProxTGVSymmDeriv(Nn, Nn, VV[0].data(), VV[1].data(), VV[2].data(), RR[0].data(), RR[1].data(),
+                                RR[2].data(), RR[3].data(), RR[4].data(), RR[5].data(), (omb_real)sigma2); });
+    for (size_t x = 0; x < N; ++x) {
+        set_item((unsigned)x, 0u, 0u);
+        ProxTGVq(RR[0].data(), RR[1].data(), RR[2].data(), RR[3].data(), RR[4].data(), RR[5].data(), (omb_real)alpha1);
+    }
+    each([&] { ProxTGVDivergence(Nn, Nn, RR[0].data(), RR[1].data(), RR[2].data(), RR[3].data(), RR[4].data(),
+                                 RR[5].data(), VV[0].data(), VV[1].data(), VV[2].data(), Q[0].data(), Q[1].data(),
+                                 Q[2].data(), (omb_real)theta, (omb_real)tau); });
+#else
+    each([&] { ProxTGVSymmDeriv(Nn, Nn, VV[0].data(), VV[1].data(), RR[0].data(), RR[1].data(), RR[2].data(),
+                                (omb_real)sigma2); });
+    for (size_t x = 0; x < N; ++x) {
+        set_item((unsigned)x, 0u, 0u);
+        ProxTGVq(RR[0].data(), RR[1].data(), RR[2].data(), (omb_real)alpha1);
+    }
+    each([&] { ProxTGVDivergence(Nn, Nn, RR[0].data(), RR[1].data(), RR[2].data(), VV[0].data(), VV[1].data(),
+                                 Q[0].data(), Q[1].data(), Q[2].data(), (omb_real)theta, (omb_real)tau); });
+#endif
+    for (int k = 0; k < 3; ++k) from_real(Q[k], q + k * N);
+    for (int k = 0; k < NR; ++k) from_real(RR[k], r + k * N);
+    for (int k = 0; k < NV; ++k) from_real(VV[k], v + k * N);
     from_real(R, rhs);
     return 0;
 }

@@ -174,6 +174,80 @@ def test_builtin_pdhg_ct_proxtv(cuda):
     assert orc.rel_l2(plain, ref) > 1e-2
 
 
+@pytest.mark.parametrize("l2,three_d", [(True, True), (False, True), (True, False), (False, False)])
+def test_proxtgv_kernel_matches_oracle(cuda, l2, three_d):
+    """omb_proxtgv_step against the restatement (pinned to the reference's
+    six TGV kernels), both balls active on part of the image."""
+    import ctypes
+
+    import torch
+    from omega_b200 import _native
+    from omega_b200.reconstruction import _stream
+    from oracle import image_oracle as io
+    shape = (37, 19, 11)
+    n = int(np.prod(shape))
+    nr, nv = (6, 3) if three_d else (3, 2)
+    rng = np.random.default_rng(63)
+    x = rng.uniform(0.0, 1.0, n).astype(np.float32)
+    q = rng.normal(0.0, 0.3, (3, n)).astype(np.float32)
+    r = rng.normal(0.0, 0.2, (nr, n)).astype(np.float32)
+    v = rng.normal(0.0, 0.2, (nv, n)).astype(np.float32)
+    rhs = rng.normal(0.0, 1.0, n).astype(np.float32)
+    X, Q, R, V, H = (torch.tensor(a, device=cuda) for a in (x, q, r, v, rhs))
+    _native.call("omb_proxtgv_step", *(ctypes.c_void_p(t.data_ptr()) for t in (X, Q, R, V, H)), *shape, 0.7, 0.3,
+                 0.2, 0.9, 0.05, 1 if l2 else 0, 1 if three_d else 0, _stream(cuda))
+    want = io.proxtgv_step(*(a.astype(np.float64) for a in (x, q, r, v, rhs)), shape, 0.7, 0.3, 0.2, 0.9, 0.05,
+                           l2=l2, three_d=three_d)
+    for got, w in zip((Q, R, V, H), want):
+        assert orc.rel_l2(got.cpu().numpy().ravel(), w.ravel()) < 1e-6, orc.rel_l2(got.cpu().numpy().ravel(),
+                                                                                    w.ravel())
+
+
+@pytest.mark.parametrize("use2d,K", [(False, None), (True, None), (False, 2)])
+def test_builtin_pdhg_ct_tgv(cuda, use2d, K):
+    """PDHG with TGV (options.TGV; 3-D or use2DTGV) through the built-in
+    entry against the FP64 loop; with K, also the filtering-based
+    measurement preconditioner, whose inverse filter takes sigma beta."""
+    from omega_b200 import filters
+    from omega_b200 import reconstruction as rec
+    o = make_options("ct_mini5")
+    g = orc.Geometry(o)
+    rng = np.random.default_rng(7)
+    truth = rng.uniform(0.0, 0.02, g.n_img)
+    counts = 1e4 * np.exp(-orc.bdd_forward(g, truth, -1))
+    o.SinM = rng.poisson(counts).astype(np.float32) + 1
+    o.PDHG = True
+    o.TGV = True
+    o.use2DTGV = use2d
+    # balls and the dual step large enough that TGV moves the image by ~13 %
+    o.alpha0TGV = 5.0
+    o.alpha1TGV = 10.0
+    o.sigma2CP = 1000.0
+    beta = 1.0 if K is None else 2.0
+    o.beta = beta
+    o.Niter = 5
+    o.x0 = np.zeros(g.n_img, dtype=np.float32)
+    mf = None
+    if K is not None:
+        o.precondTypeMeas = np.array([False, True])
+        o.filteringIterations = K
+        o.filterWindow = "hann"
+        o.tauCP = 2e-5
+    out, _ = rec.reconstructions_mainCT(o)
+    tau = o.tau_used
+    y = np.asarray(o.SinM, dtype=np.float32).ravel(order='F').astype(np.float64)
+    if K is not None:
+        nr = int(o.nRowsD)
+        nf, f0, ff, _, _ = filters.pdhg_row_filters(nr, beta, "hann")
+        mf = dict(filter0=f0, ffilter=ff, nf=nf, rows=nr, K=K, tau2=float(np.float32(2e-5)))
+    tg = dict(alpha0=5.0, alpha1=10.0, sigma2=1000.0, l2=True, three_d=not use2d)
+    ref = orc.pdhg_tv(g, y, np.zeros(g.n_img), 5, tau, beta, 1e-4, tgv=tg, meas_filter=mf)
+    x = out.ravel(order='F')
+    assert orc.rel_l2(x, ref) < 1e-4, orc.rel_l2(x, ref)
+    plain = orc.pdhg_tv(g, y, np.zeros(g.n_img), 5, tau, 0.0, 1e-4, meas_filter=mf)
+    assert orc.rel_l2(plain, ref) > 1e-2
+
+
 @pytest.mark.parametrize("rows,window", [(100, "hann"), (512, "hamming"), (37, "parzen")])
 def test_row_filter_kernel(cuda, rows, window):
     """omb_row_filter (circular convolution with the taps) against the

@@ -331,6 +331,44 @@ def test_proxtv_needs_pdhg():
         rec.reconstructions_main(o)
 
 
+def test_proxtgv_entry_point_validates_arguments():
+    from omega_b200 import _native
+    L = _native.lib()
+    p = ctypes.c_void_p(16)
+    f = ctypes.c_float
+    assert L.omb_proxtgv_step(p, p, p, p, p, 8, 8, 4, f(0.5), f(0.0), f(0.1), f(1.0), f(0.01), 1, 1, None) != 0
+    assert "alpha0" in L.omb_last_error().decode()
+    assert L.omb_proxtgv_step(p, p, p, p, None, 8, 8, 4, f(0.5), f(0.1), f(0.1), f(1.0), f(0.01), 1, 1, None) != 0
+    assert "NULL" in L.omb_last_error().decode()
+
+
+@pytest.mark.parametrize("case,match", [
+    ("osem", "built for PDHG"), ("alpha", "alpha0TGV"), ("difftype", "forward differences"),
+    ("both", "Select one")])
+def test_tgv_option_checks(case, match):
+    """options.TGV: PDHG only, positive balls, forward differences (the
+    reference's backward-difference TGV kernels do not compile), one TV
+    form at a time; all raised before the projector is set up."""
+    from conftest import make_options
+    from omega_b200 import reconstruction as rec
+    o = make_options("pet_mini")
+    o.SinM = np.ones(int(o.Ndist) * int(o.Nang) * int(o.NSinos), np.float32)
+    o.TGV = True
+    o.alpha0TGV, o.alpha1TGV = 1.0, 1.0
+    if case == "osem":
+        o.OSEM = True
+    else:
+        o.PDHG = True
+    if case == "alpha":
+        o.alpha1TGV = 0.0
+    if case == "difftype":
+        o.derivativeType = 1
+    if case == "both":
+        o.ProxTV = True
+    with pytest.raises(ValueError, match=match):
+        rec.reconstructions_main(o)
+
+
 def test_wmean46_rejects_windows_beyond_one_mirror():
     from omega_b200 import _native
     L = _native.lib()

@@ -274,3 +274,69 @@ def test_pdhg_proxtv_iteration_pinned():
         q, rhs = ref_cl.proxtv_step(x, q, rhs, shape, sigma2, beta, True, 0, exact_inputs=True)
         x, u = ref_cl.pdhg_update(x, rhs, u, shape, tau, 1.0, 1e-5, exact_inputs=True)
     assert orc.rel_l2(ours, x) < PIN
+
+
+@pytest.mark.parametrize("l2,three_d", [(True, True), (False, True), (True, False)])
+def test_proxtgv_pinned(l2, three_d):
+    """One proximal TGV step (image_oracle.proxtgv_step) against
+    ProxTVGradient, ProxTVq, ProxTVDivergence, ProxTGVSymmDeriv, ProxTGVq and
+    ProxTGVDivergence compiled with -DPROXTV -DPROXTGV (-DTGVZ for 3-D, -DL2
+    for the L2 balls), with both ball projections active on part of the
+    image."""
+    from oracle import image_oracle as io
+    shape = (10, 9, 7)
+    rng = np.random.default_rng(61)
+    n = int(np.prod(shape))
+    nr, nv = (6, 3) if three_d else (3, 2)
+    x = rng.uniform(0.0, 1.0, n)
+    q = rng.normal(0.0, 0.3, (3, n))
+    r = rng.normal(0.0, 0.2, (nr, n))
+    v = rng.normal(0.0, 0.2, (nv, n))
+    rhs = rng.normal(0.0, 1.0, n)
+    args = (shape, 0.7, 0.3, 0.2, 0.9, 0.05)
+    theirs = ref_cl.proxtgv_step(x, q, r, v, rhs, *args, l2=l2, three_d=three_d, exact_inputs=True)
+    ours = io.proxtgv_step(x, q, r, v, rhs, *args, l2=l2, three_d=three_d)
+    for a, b in zip(ours, theirs):
+        assert np.abs(a - b).max() <= 1e-13 * max(np.abs(b).max(), 1.0)
+    # the projections changed part of q and of r
+    q_raw = q + 0.7 * (np.stack([io._diff(x.reshape(shape, order='F'), a, True).ravel(order='F') for a in range(3)])
+                       - np.vstack([v, np.zeros((3 - nv, n))]))
+    assert np.count_nonzero(np.abs(q_raw - ours[0]).max(axis=0) > 1e-12) > n // 10
+    rr = ours[1]
+    nd = 3 if three_d else 2
+    if l2:
+        norm = np.sqrt((rr[:nd] ** 2).sum(axis=0) + 2 * (rr[nd:] ** 2).sum(axis=0))
+    else:
+        norm = np.abs(rr).max(axis=0)
+    on_ball = np.abs(norm - 0.2) < 1e-12
+    assert n // 10 < np.count_nonzero(on_ball) < n
+
+
+def test_pdhg_tgv_iteration_pinned():
+    """Two PDHG iterations with TGV (oracle.pdhg_tv(tgv=...)) against the same
+    loop built from the reference's kernels: the type-5 projector pair, the
+    dual step divided by 1 + sigma beta, the six TGV kernels and
+    PDHGUpdate."""
+    o = _proj("ct_fine5")
+    g = orc.Geometry(o)
+    R = ref_cl.RefCT(o, exact_inputs=True)
+    shape = (g.nx, g.ny, g.nz)
+    rng = np.random.default_rng(62)
+    truth = rng.uniform(0.0, 0.02, g.n_img)
+    y = orc.bdd_forward(g, truth, -1)
+    x0 = np.full(g.n_img, 1e-3)
+    tau, beta, sigma, sigma2, a0, a1 = 1e-4, 0.5, 1.0, 0.5, 0.01, 0.02
+    ours = orc.pdhg_tv(g, y, x0, 2, tau, beta, 1e-4, sigma=sigma,
+                       tgv=dict(alpha0=a0, alpha1=a1, sigma2=sigma2, l2=True, three_d=True))
+    x, u = x0.copy(), x0.copy()
+    p = np.zeros(g.rays(-1))
+    q = np.zeros((3, g.n_img))
+    r = np.zeros((6, g.n_img))
+    v = np.zeros((3, g.n_img))
+    for _ in range(2):
+        p = (p + sigma * (R.bdd_forward(x, -1) - y)) / (1.0 + sigma * beta)
+        rhs = R.bdd_backward(p, -1)
+        q, r, v, rhs = ref_cl.proxtgv_step(x, q, r, v, rhs, shape, sigma2, a0, a1, 1.0, tau, True, True,
+                                           exact_inputs=True)
+        x, u = ref_cl.pdhg_update(x, rhs, u, shape, tau, 1.0, 1e-5, exact_inputs=True)
+    assert orc.rel_l2(ours, x) < PIN
