@@ -425,6 +425,14 @@ typedef struct omb_recon_params {
                                  1 + sigma beta (computeForwardProject.h:295-298) and the filter by sigma beta */
     float alpha0_tgv;         /* options.alpha0TGV: the first-order ball (q) */
     float alpha1_tgv;         /* options.alpha1TGV: the second-order ball (r) */
+    const float *img_filter_h;/* options.precondTypeImage[5] (PKMA / MRAMLA / MBSREM, PDHG): device, the 1-D taps
+                                 of the filtering-based image preconditioner (see omb_image_filter), or NULL;
+                                 applied last in the image preconditioning of sub-iterations k < filter_iters
+                                 (filter_iters 0: k = 0 only); PDHG switches its step to tau (the power method
+                                 without the filter) at k = filter_iters */
+    int32_t img_filter_nf;    /* its length Nf (a power of two >= nx, ny) */
+    float tau_used2;          /* out: PDHG with a filtering preconditioner, the primal step from iteration
+                                 filter_iters on (0 when the run never switches) */
 } omb_recon_params;
 
 /*
@@ -472,6 +480,18 @@ int omb_tv_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t
  */
 int omb_row_filter(const float *in, float *out, int32_t n_rows, int64_t n_cols, const float *h, int32_t nf,
                    void *stream);
+
+/*
+ * The filtering-based image preconditioner (filtering2D functions.hpp:
+ * 1908-1932, applied by applyImagePreconditioning :2093-2099): every slice of
+ * g (device, nx x ny x nz, x fastest) zero-padded to nf x nf, multiplied in the
+ * Fourier domain by the separable filter F = f f^T / max(f f^T) and cut back
+ * to nx x ny; computed as the circular convolution of the x lines, then the y
+ * lines, with h = real(ifft(f)) / sqrt(max(f f^T)) (device, nf taps).  tmp
+ * (device, one image) is scratch; g is filtered in place.  nx, ny <= nf <= 2048.
+ */
+int omb_image_filter(float *g, float *tmp, int32_t nx, int32_t ny, int32_t nz, const float *h, int32_t nf,
+                     void *stream);
 
 /*
  * Proximal TV of the PDHG loop (priors.h:261-281; ProxTVGradient, ProxTVq,

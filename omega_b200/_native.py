@@ -149,6 +149,9 @@ class ReconParams(ctypes.Structure):
         ("tgv", ctypes.c_int32),
         ("alpha0_tgv", ctypes.c_float),
         ("alpha1_tgv", ctypes.c_float),
+        ("img_filter_h", ctypes.c_void_p),
+        ("img_filter_nf", ctypes.c_int32),
+        ("tau_used2", ctypes.c_float),
     ]
 
 
@@ -276,6 +279,8 @@ EXPORTS = [
                                           ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_row_filter", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64,
                                       ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    ("omb_image_filter", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     ("omb_proxtv_dual", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_void_p]),

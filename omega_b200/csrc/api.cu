@@ -837,6 +837,18 @@ int relaxed_subset(omb_handle *h, int32_t subset, float *image, const float *y_s
         p.upper = a.upper;
         if (p.gradF && (st = precond_gradient(image, a.gradF, h->grid, p, a.work, s)) != OMB_OK) return st;
         if ((st = precond_apply(work_img, a.du, image, h->n_img, p, s)) != OMB_OK) return st;
+        if (p.filt_h) {
+            // type 5 last (functions.hpp:2093-2099), in the filtering sub-iterations only
+            FilterGate gt;
+            gt.it = p.it;
+            gt.n_sub = p.n_sub;
+            gt.sub = p.sub;
+            gt.K = p.filt_K;
+            if (!p.filt_tmp || !p.it) return set_error(OMB_ERR_INVALID, "the image filter needs its scratch and counter");
+            if ((st = image_filter(work_img, p.filt_tmp, h->grid.nx, h->grid.ny, h->grid.nz, p.filt_h, p.filt_nf, gt, s)) !=
+                OMB_OK)
+                return st;
+        }
         if (a.kind == kPkma && (a.auto_relax || a.relax_scaling)) {
             if (!a.lam.lam || !a.lam.iter || !a.work)
                 return set_error(OMB_ERR_INVALID, "PKMA relaxation needs the device schedule and workspace");

@@ -6,6 +6,12 @@
 // convolution of the zero-padded column with h = ifft(filter) (real, even),
 // computed here directly: out[i] = sum_{j < nr} h[(i - j) mod Nf] x[j].
 //
+// The same kernel filters the image lines of the filtering-based image
+// preconditioner (filtering2D functions.hpp:1908-1932: every slice
+// zero-padded to Nf x Nf, multiplied by the separable filter f f^T / max,
+// cut back): x lines, then y lines, each a circular convolution with the
+// 1-D taps scaled by 1 / sqrt(max).
+//
 // A CTA takes 16 columns: their nr x 16 values and the 2 nr - 1 taps
 // e[k] = h[(k - nr + 1) mod Nf] are staged in shared memory; a thread owns 8
 // consecutive rows x 4 columns and walks j with a sliding window of 8 taps in
@@ -21,8 +27,25 @@ constexpr int kR = 8;      // rows per thread
 constexpr int kC = 4;      // columns per thread
 constexpr int kXS = 20;    // row stride of the staged columns (16-byte aligned, fewer bank conflicts)
 
-__global__ void k_circ_filter(const float *__restrict__ in, float *__restrict__ out, int nr, int64_t ncols,
-                              const float *__restrict__ h, int nf) {
+// Where element (row r, column c) of the filtered data lies: (c % cdim) * cs0 + (c / cdim) * cs1 + r * rs.
+// Detector columns: rs = 1, cs0 = rows, cdim = columns.  Image x lines: rs = 1, cs0 = nx, cdim = ny nz.
+// Image y lines: rs = nx, cs0 = 1, cdim = nx, cs1 = nx ny.
+struct Lines {
+    int64_t rs, cs0, cs1, cdim;
+    __device__ __forceinline__ int64_t at(int64_t c, int r) const { return (c % cdim) * cs0 + (c / cdim) * cs1 + r * rs; }
+};
+
+// the gate of a filter inside a replayed loop: active in sub-iteration kk = *it * n_sub + sub when kk < K
+// (K > 0) or kk == 0 (K == 0); always active without a counter
+__device__ __forceinline__ bool gate_open(const FilterGate &g) {
+    if (!g.it) return true;
+    const int kk = *g.it * g.n_sub + g.sub;
+    return g.K > 0 ? kk < g.K : kk == 0;
+}
+
+__global__ void k_circ_filter(const float *__restrict__ in, float *__restrict__ out, int nr, int64_t ncols, Lines L,
+                              const float *__restrict__ h, int nf, FilterGate gate) {
+    if (!gate_open(gate)) return;
     extern __shared__ float smem[];
     float *x = smem;                     // [nr][kXS]
     float *e = smem + (size_t)nr * kXS;  // [2 nr - 1] (+ kR padding)
@@ -33,10 +56,20 @@ __global__ void k_circ_filter(const float *__restrict__ in, float *__restrict__ 
         const int d = k - (nr - 1);  // i - j
         e[k] = k < 2 * nr - 1 ? __ldg(h + ((d % nf) + nf) % nf) : 0.f;
     }
-    for (int k = tid; k < nr * kCols; k += nt) {
-        const int c = k / nr, r = k - c * nr;
-        const int64_t col = col0 + c;
-        x[r * kXS + c] = col < ncols ? __ldg(in + col * nr + r) : 0.f;
+    if (L.rs == 1) {
+        // rows contiguous: consecutive threads take consecutive rows
+        for (int k = tid; k < nr * kCols; k += nt) {
+            const int c = k / nr, r = k - c * nr;
+            const int64_t col = col0 + c;
+            x[r * kXS + c] = col < ncols ? __ldg(in + L.at(col, r)) : 0.f;
+        }
+    } else {
+        // columns contiguous: consecutive threads take consecutive columns
+        for (int k = tid; k < nr * kCols; k += nt) {
+            const int r = k / kCols, c = k - r * kCols;
+            const int64_t col = col0 + c;
+            x[r * kXS + c] = col < ncols ? __ldg(in + L.at(col, r)) : 0.f;
+        }
     }
     __syncthreads();
     const int c0 = threadIdx.x * kC;
@@ -71,13 +104,15 @@ __global__ void k_circ_filter(const float *__restrict__ in, float *__restrict__ 
         if (col >= ncols) continue;
 #pragma unroll
         for (int r = 0; r < kR; ++r)
-            if (i0 + r < nr) out[col * nr + i0 + r] = acc[r][c];
+            if (i0 + r < nr) out[L.at(col, i0 + r)] = acc[r][c];
     }
 }
 
 }  // namespace
 
-int circ_filter(const float *in, float *out, int nr, int64_t ncols, const float *h, int nf, cudaStream_t st) {
+namespace {
+int launch_lines(const float *in, float *out, int nr, int64_t ncols, const Lines &L, const float *h, int nf,
+                 const FilterGate &gate, cudaStream_t st) {
     if (nr < 1 || nr > 2048 || nf < nr) return set_error(OMB_ERR_INVALID, "row filter: 1 <= rows <= 2048 and Nf >= rows");
     if (ncols <= 0) return OMB_OK;
     const size_t smem = ((size_t)nr * kXS + 2 * (size_t)nr - 1 + kR) * sizeof(float);
@@ -85,9 +120,28 @@ int circ_filter(const float *in, float *out, int nr, int64_t ncols, const float 
         return set_error(OMB_ERR_CUDA, "row filter: shared memory attribute failed");
     dim3 block(kCols / kC, (nr + kR - 1) / kR);
     dim3 grid((unsigned)((ncols + kCols - 1) / kCols));
-    k_circ_filter<<<grid, block, smem, st>>>(in, out, nr, ncols, h, nf);
+    k_circ_filter<<<grid, block, smem, st>>>(in, out, nr, ncols, L, h, nf, gate);
     OMB_LAUNCH_CHECK("row filter launch");
     return OMB_OK;
+}
+}  // namespace
+
+int circ_filter(const float *in, float *out, int nr, int64_t ncols, const float *h, int nf, cudaStream_t st) {
+    Lines L{1, nr, 0, ncols > 0 ? ncols : 1};
+    return launch_lines(in, out, nr, ncols, L, h, nf, FilterGate{}, st);
+}
+
+int image_filter(float *g, float *tmp, int nx, int ny, int nz, const float *h, int nf, const FilterGate &gate,
+                 cudaStream_t st) {
+    if (nx > nf || ny > nf) return set_error(OMB_ERR_INVALID, "image filter: Nf must cover the image's x and y size");
+    const int64_t nxy = (int64_t)nx * ny;
+    // x lines into tmp, then y lines of tmp back into g (the separable 2-D filter, slice by slice)
+    const int64_t nyz = (int64_t)ny * nz;
+    Lines Lx{1, nx, 0, nyz};
+    int e = launch_lines(g, tmp, nx, nyz, Lx, h, nf, gate, st);
+    Lines Ly{nx, 1, nxy, nx};
+    if (e == OMB_OK) e = launch_lines(tmp, g, ny, (int64_t)nx * nz, Ly, h, nf, gate, st);
+    return e;
 }
 
 }  // namespace omb
@@ -97,6 +151,14 @@ extern "C" int omb_row_filter(const float *in, float *out, int32_t n_rows, int64
     if (!in || !out || !h) return omb::set_error(OMB_ERR_INVALID, "NULL pointer passed to omb_row_filter");
     if (in == out) return omb::set_error(OMB_ERR_INVALID, "omb_row_filter: in and out must differ");
     return omb::circ_filter(in, out, n_rows, n_cols, h, nf, (cudaStream_t)stream);
+}
+
+extern "C" int omb_image_filter(float *g, float *tmp, int32_t nx, int32_t ny, int32_t nz, const float *h, int32_t nf,
+                                void *stream) {
+    if (!g || !tmp || !h) return omb::set_error(OMB_ERR_INVALID, "NULL pointer passed to omb_image_filter");
+    if (g == tmp) return omb::set_error(OMB_ERR_INVALID, "omb_image_filter: g and tmp must differ");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return omb::set_error(OMB_ERR_INVALID, "image size must be positive");
+    return omb::image_filter(g, tmp, nx, ny, nz, h, nf, omb::FilterGate{}, (cudaStream_t)stream);
 }
 
 namespace omb {

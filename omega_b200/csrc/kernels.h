@@ -80,6 +80,10 @@ struct PrecondExt {
     int n_sub = 1, sub = 0;
     int fold = 0;
     float upper = 10000.f;
+    // type 5: the image filter's taps (or NULL), length, filtering sub-iterations and scratch image
+    const float *filt_h = nullptr;
+    int filt_nf = 0, filt_K = 0;
+    float *filt_tmp = nullptr;
 };
 struct RelaxedArgs {
     int kind = kRosem;
@@ -174,6 +178,15 @@ int sysmat_backward(const Grid &g, const SysMat &sm, const Frames &fr, int64_t m
 // Detector-row filtering (filter.cu): out = the circular convolution (length nf) of each column of nr rows with
 // h; the measurement residual fp -= y; the dual step out = (p + sigma r) / denom (denom 1: no division).
 int circ_filter(const float *in, float *out, int nr, int64_t ncols, const float *h, int nf, cudaStream_t st);
+// The filtering-based image preconditioner: g (nx x ny x nz) filtered slice by slice with the separable
+// circular filter h (x lines into tmp, then y lines back into g); with a gate counter, only in the
+// sub-iterations kk = *it * n_sub + sub < K (K > 0) or kk == 0 (K == 0), g untouched otherwise.
+struct FilterGate {
+    const int *it = nullptr;
+    int n_sub = 1, sub = 0, K = 0;
+};
+int image_filter(float *g, float *tmp, int nx, int ny, int nz, const float *h, int nf, const FilterGate &gate,
+                 cudaStream_t st);
 int meas_residual(float *fp, const float *y, int64_t n, cudaStream_t st);
 int dual_step(const float *p, const float *r, float *out, int64_t n, float sigma, float denom, cudaStream_t st);
 

@@ -168,7 +168,8 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         DevBuf pd;
         if (p->precond < 0 || p->precond > 3 || (p->precond && !(pkma || mb)))
             return set_error(OMB_ERR_INVALID, "image preconditioners 1 to 3 are for PKMA / MRAMLA / MBSREM");
-        const bool ext = p->precond == 3 || p->precond_alpha || p->precond_grad || p->precond_curv;
+        const bool ifilt = p->img_filter_h != nullptr;
+        const bool ext = p->precond == 3 || p->precond_alpha || p->precond_grad || p->precond_curv || ifilt;
         if ((ext || p->precond_meas) && !(pkma || mb))
             return set_error(OMB_ERR_INVALID, "the image and measurement preconditioners are for PKMA / MRAMLA / MBSREM");
         if (p->pkma_relax && !pkma) return set_error(OMB_ERR_INVALID, "the relaxation parameters are PKMA's");
@@ -182,7 +183,12 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         }
         // the other preconditioners (functions.hpp:2057-2106, reconstructionAF.h:600-650, 827-861) and the
         // PKMA relaxation's workspace
-        DevBuf ones, gradF, dP, alpha_d, meas_m, pwork;
+        DevBuf ones, gradF, dP, alpha_d, meas_m, pwork, ftmp;
+        if (ifilt) {
+            if (p->img_filter_nf < g.nx || p->img_filter_nf < g.ny || p->img_filter_nf > 2048)
+                return set_error(OMB_ERR_INVALID, "img_filter_nf must cover nx and ny (at most 2048)");
+            if ((st = alloc(ftmp, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        }
         if (p->precond_curv || p->precond_meas) {
             if ((st = alloc(ones, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
             OMB_CUDA_TRY(cudaMemsetAsync(ones.p, 0, (size_t)n * sizeof(float), s));
@@ -231,6 +237,10 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         pe.dP = p->precond_curv ? dP.f() : nullptr;
         pe.it = rl.iter;
         pe.n_sub = n_subsets;
+        pe.filt_h = p->img_filter_h;
+        pe.filt_nf = p->img_filter_nf;
+        pe.filt_K = p->filter_iters;
+        pe.filt_tmp = ifilt ? ftmp.f() : nullptr;
         for (int s_ = 0; s_ < n_subsets && !no_sens && st == OMB_OK; ++s_)
             st = omb_sensitivity(h, s_, sens.f() + s_ * n, stream);
         if (st != OMB_OK) return st;
@@ -341,8 +351,17 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         // p = (I + sigma F)^-1 (p + sigma F r) (the inverse filter hinv), afterwards the plain one without
         // filtering; with K = 0 every residual is filtered and the dual step stays the plain one
         const bool filt = p->filter_h != nullptr;
+        // the filtering-based image preconditioner (functions.hpp:2093-2099, subiterStep.h:28-45): A^T p plus the
+        // TV term filtered before the primal step in iterations k < K (K = 0: k = 0 only)
+        const bool ifilt = p->img_filter_h != nullptr;
+        if (filt && ifilt) return set_error(OMB_ERR_UNSUPPORTED, "one filtering-based preconditioner at a time");
         const int K = p->filter_iters;
-        DevBuf wf;
+        DevBuf wf, ftmp;
+        if (ifilt) {
+            if (p->img_filter_nf < g.nx || p->img_filter_nf < g.ny || p->img_filter_nf > 2048)
+                return set_error(OMB_ERR_INVALID, "img_filter_nf must cover nx and ny (at most 2048)");
+            if ((st = alloc(ftmp, (size_t)n * sizeof(float), s)) != OMB_OK) return st;
+        }
         if (filt) {
             if (p->filter_rows < 1 || m_all % p->filter_rows != 0)
                 return set_error(OMB_ERR_INVALID, "filter_rows must divide the measurement count");
@@ -351,7 +370,8 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         }
         const int64_t fcols = filt ? m_all / p->filter_rows : 0;
         // power method (functions.hpp:2417-2540): x <- A^T (F) A x from an |N(0,1)| start normalised to unit
-        // length (2430-2437); L = x . A^T (F) A x / x . x at the last step
+        // length (2430-2437); L = x . A^T (F) A x / x . x at the last step.  With the image filter P:
+        // x <- P A^T A x in the power iterations it <= K (applyImagePreconditioning's kk <= filterIter)
         auto power = [&](bool use_filter, double &L) -> int {
             if (!work.p && (st = alloc(work, omb_power_workspace_bytes(), s)) != OMB_OK) return st;
             std::vector<float> v((size_t)n);
@@ -376,8 +396,13 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             int e = OMB_OK;
             for (int it = 0; it < iters && e == OMB_OK; ++it) {
                 e = omb_forward(h, -1, xn.f(), wm.f(), stream);
-                if (e == OMB_OK) e = circ_filter(wm.f(), wf.f(), p->filter_rows, fcols, p->filter_h, p->filter_nf, s);
-                if (e == OMB_OK) e = omb_backward(h, -1, wf.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC, stream);
+                if (e == OMB_OK && filt)
+                    e = circ_filter(wm.f(), wf.f(), p->filter_rows, fcols, p->filter_h, p->filter_nf, s);
+                if (e == OMB_OK) e = omb_backward(h, -1, filt ? wf.f() : wm.f(), wi.f(), nullptr, OMB_BP_FLOAT_ATOMIC,
+                                                  stream);
+                if (e == OMB_OK && ifilt && it <= K)
+                    e = image_filter(wi.f(), ftmp.f(), g.nx, g.ny, g.nz, p->img_filter_h, p->img_filter_nf,
+                                     FilterGate{}, s);
                 if (e == OMB_OK && it == iters - 1) e = dot2(wi.f(), xn.f(), n, wl, s);
                 if (e == OMB_OK) e = dot2(wi.f(), wi.f(), n, wn, s);
                 if (e == OMB_OK) e = normalize_into(xn.f(), wi.f(), n, wn + dot_workspace_bytes() / sizeof(double) - 2, s);
@@ -406,21 +431,38 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                 if (!(L > 0.0)) return set_error(OMB_ERR_INVALID, "power method gave a non-positive eigenvalue");
                 tau = (float)(1.0 / L);
             }
+        } else if (ifilt) {
+            // libHeader.h:1356-1361: tauCP is the step while filtering; the one after K comes from the power
+            // method without the filter (functions.hpp:2696-2886)
+            tau_f = p->tau;
+            if (!(tau_f > 0.f)) {
+                double L = 0.0;
+                if ((st = power(true, L)) != OMB_OK) return st;
+                if (!(L > 0.0)) return set_error(OMB_ERR_INVALID, "power method gave a non-positive eigenvalue");
+                tau_f = (float)(1.0 / L);
+            }
+            if (K > 0 && K < p->n_iter) {
+                double L = 0.0;
+                if ((st = power(false, L)) != OMB_OK) return st;
+                if (!(L > 0.0)) return set_error(OMB_ERR_INVALID, "power method gave a non-positive eigenvalue");
+                tau = (float)(1.0 / L);
+            }
         } else if (!(tau > 0.f)) {
             double L = 0.0;
             if ((st = power(false, L)) != OMB_OK) return st;
             if (!(L > 0.0)) return set_error(OMB_ERR_INVALID, "power method gave a non-positive eigenvalue");
             tau = (float)(1.0 / L);
         }
-        p->tau_used = filt ? tau_f : tau;
+        p->tau_used = filt || ifilt ? tau_f : tau;
+        p->tau_used2 = (filt || ifilt) && K > 0 && K < p->n_iter ? tau : 0.f;
         OMB_CUDA_TRY(cudaMemcpyAsync(u.p, x_out, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
         OMB_CUDA_TRY(cudaMemsetAsync(pd.p, 0, (size_t)m_all * sizeof(float), s));
         // one iteration with steps tau_k, sig_k; fmode 0 no filtering, 1 filtered residual and the plain dual
         // step, 2 filtered residual and the inverse-filtered dual step.  The plain TV gradient is fused into
         // the primal step when nothing else comes between; the other TV terms are added to A^T p before it
         // the plain dual step divides by 1 + sigma, by 1 + sigma beta with TGV (computeForwardProject.h:295-303)
-        auto one = [&](float *xa, float *xb, float tau_k, float sig_k, int fmode) {
-            if (fmode == 0 && !p->tv_prox && !tgv && p->tv_variant == OMB_TV_PLAIN)
+        auto one = [&](float *xa, float *xb, float tau_k, float sig_k, int fmode, bool imgf) {
+            if (fmode == 0 && !imgf && !p->tv_prox && !tgv && p->tv_variant == OMB_TV_PLAIN)
                 return omb_pdhg_iteration(h, xa, xb, u.f(), pd.f(), y, tau_k, sig_k, p->theta, p->beta,
                                           p->tv_smoothing, p->positivity, wm.f(), wi.f(), stream);
             const float denom = tgv ? 1.f + sig_k * p->beta : 1.f + sig_k;
@@ -451,21 +493,24 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                 e = omb_tv_gradient_ex(xa, wi.f(), g.nx, g.ny, g.nz, p->beta, p->tv_smoothing, p->tv_variant,
                                        p->tv_sigma, p->tv_c, p->tv_ref, stream);
             }
+            if (e == OMB_OK && imgf)
+                e = image_filter(wi.f(), ftmp.f(), g.nx, g.ny, g.nz, p->img_filter_h, p->img_filter_nf, FilterGate{},
+                                 s);
             if (e == OMB_OK)
                 e = omb_pdhg_primal(h, xa, wi.f(), u.f(), xb, tau_k, p->theta, 0.f, p->tv_smoothing, p->positivity,
                                     stream);
             return e;
         };
-        if (!filt) {
+        if (!filt && !ifilt) {
             // two iterations per repetition keep x_out / xn in place for graph replays
             auto two = [&]() {
-                int e = one(x_out, xn.f(), tau, p->sigma, 0);
-                if (e == OMB_OK) e = one(xn.f(), x_out, tau, p->sigma, 0);
+                int e = one(x_out, xn.f(), tau, p->sigma, 0, false);
+                if (e == OMB_OK) e = one(xn.f(), x_out, tau, p->sigma, 0, false);
                 return e;
             };
             st = repeat(p->n_iter / 2, graph, s, two);
             if (st == OMB_OK && p->n_iter % 2) {
-                st = one(x_out, xn.f(), tau, p->sigma, 0);
+                st = one(x_out, xn.f(), tau, p->sigma, 0, false);
                 if (st == OMB_OK)
                     OMB_CUDA_TRY(cudaMemcpyAsync(x_out, xn.p, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, s));
             }
@@ -485,8 +530,9 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
                         sig_k = tau;
                     }
                 }
-                const int fmode = K > 0 ? (k < K ? 2 : 0) : 1;
-                st = one(xa, xb, tau_k, sig_k, fmode);
+                const int fmode = !filt ? 0 : (K > 0 ? (k < K ? 2 : 0) : 1);
+                const bool imgf = ifilt && (K > 0 ? k < K : k == 0);
+                st = one(xa, xb, tau_k, sig_k, fmode, imgf);
                 std::swap(xa, xb);
             }
             if (st == OMB_OK && xa != x_out)

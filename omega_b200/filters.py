@@ -9,6 +9,17 @@ power of two at or above the detector rows, filter0 = rampFilt with its zero
 frequency set to 1e-6, and the dual step's 1 + sigma filter0.  The kernels
 filter by circular convolution, so both are returned as their real
 time-domain taps (ifft).
+
+``image_filter_2d`` builds the filter of the filtering-based image
+preconditioner (options.precondTypeImage[5]): Nf = 2^ceil(log2 Nx)
+(prepass.py:1106-1109) and F = f f^T / max(f f^T), f = rampFilt(Nf, ...),
+the 2-D filter rampFilt.m:65-69 forms.  The reference's Python rampFilt with
+use2D (rampfilt.py:55-58) tiles the 1-D array into one row of Nf^2 values and
+builds an (Nf^2, Nf^2) product whose first Nf^2 values -- all the library
+reads as its Nf x Nf filter (libHeader.h:1059) -- are f[0] f = 0, so through
+that path the preconditioner zeroes the gradient; the filter here is the
+MATLAB path's.  F is separable, so the kernels apply it as two 1-D
+convolutions with the taps real(ifft(f)) / sqrt(max(f f^T)).
 """
 from __future__ import annotations
 
@@ -73,3 +84,19 @@ def pdhg_row_filters(n_rows, sigma, window="hamming", c=1.0, fsigma=0.25):
     h = np.real(np.fft.ifft(filter0.astype(np.float64))).astype(np.float32)
     hinv = np.real(np.fft.ifft(1.0 / ffilter.astype(np.float64))).astype(np.float32)
     return nf, filter0, ffilter, h, hinv
+
+
+def image_filter_2d(nx, window="hamming", c=1.0, fsigma=0.25):
+    """(Nf, F, h): Nf the power of two at or above nx, F the Nf x Nf float32
+    filter f f^T / max(f f^T) with f = rampFilt(Nf, window, c, fsigma), and h
+    the float32 1-D taps real(ifft(f)) / sqrt(max(f f^T)) whose separable
+    circular convolution applies F."""
+    nf = int(2 ** np.ceil(np.log2(int(nx))))
+    f = ramp_filter(nf, window, c, fsigma).astype(np.float32)
+    ff = np.outer(f, f).astype(np.float32)
+    m = float(ff.max())
+    if not m > 0:
+        raise ValueError('the image filter is zero everywhere')
+    F = (ff / np.float32(m)).astype(np.float32)
+    h = (np.real(np.fft.ifft(f.astype(np.float64))) / np.sqrt(m)).astype(np.float32)
+    return nf, F, h

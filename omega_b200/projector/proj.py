@@ -152,13 +152,16 @@ class projectorClass:
     gradLastIter = 1
     computeRelaxationParameters = False
     relaxationScaling = False
-    # the filtering-based measurement preconditioner of PDHG (proj.py:116,
-    # 123, 170-171, 269 of the reference)
+    # the filtering-based measurement (PDHG) and image preconditioners
+    # (proj.py:104, 116, 123, 170-171, 269 of the reference): window, cut-off,
+    # filtering sub-iterations, PDHG's step while filtering, the relaxation
+    # while filtering
     filterWindow = "hamming"
     cutoffFrequency = 1.
     normalFilterSigma = 0.25
     filteringIterations = 0
     tauCPFilt = 0.
+    lambdaFiltered = np.empty(0, dtype=np.float32)
     PDHG = False
     TV = False
     RDP = False

@@ -284,24 +284,68 @@ def momentum(options):
 def _check_preconditioners(options):
     """The preconditioner selections the built-in loop takes (before any
     device work): at most one of the image types 0-2; the filtering-based
-    image (5) and measurement (1) preconditioners are not built."""
+    measurement preconditioner (1) is built for PDHG only."""
     pt_im = np.ravel(np.asarray(getattr(options, 'precondTypeImage', np.zeros(7, dtype=bool)), dtype=bool))
     pt_meas = np.ravel(np.asarray(getattr(options, 'precondTypeMeas', np.zeros(2, dtype=bool)), dtype=bool))
     if int(np.count_nonzero(pt_im[:3])) > 1:
         raise ValueError('Only one of the image preconditioners 0-2 can be selected')
     if pt_im.size > 5 and pt_im[5]:
-        raise ValueError('The filtering-based image preconditioner (type 5) is not built')
+        _check_image_filter(options)
+        _filtered_relaxation(options, relaxation(options), int(getattr(options, 'filteringIterations', 0)),
+                             int(options.subsets))
     if pt_meas.size > 1 and pt_meas[1]:
         raise ValueError('The filtering-based measurement preconditioner (type 1) is not built')
 
 
+def _filtered_relaxation(options, lam, K, S):
+    """The per-iteration relaxation with the filtering-based image
+    preconditioner: options.lambdaFiltered (options.lambdaN when it is empty,
+    or of another size with K < Niter * subsets) in the iterations whose
+    sub-iterations all filter, lambdaN from sub-iteration K on; K = 0 or
+    K >= Niter * subsets never switches.  A switch inside an iteration needs
+    equal values there."""
+    n = int(options.Niter)
+    lf = np.asarray(getattr(options, 'lambdaFiltered', np.empty(0)), dtype=np.float32).ravel()
+    lam_n = np.asarray(options.lambdaN, dtype=np.float32).ravel()
+    if (lf.size != lam_n.size and K < S * n) or lf.size == 0:
+        lf = lam_n
+    if lf.size < n:
+        raise ValueError('options.lambdaFiltered needs at least Niter values')
+    out = lf[:n].astype(np.float32).copy()
+    if 0 < K < S * n:
+        for i in range(n):
+            if i * S >= K:
+                out[i] = lam[i]
+            elif (i + 1) * S > K and lf[i] != lam[i]:
+                raise ValueError('options.lambdaFiltered differing from lambdaN needs filteringIterations to be a '
+                                 'multiple of subsets')
+    options.lambdaFiltered = lf
+    return np.ascontiguousarray(out, dtype=np.float32)
+
+
+def _check_image_filter(options):
+    """The filtering-based image preconditioner filters whole slices: Nf (the
+    power of two at or above Nx) must cover Ny too."""
+    nx, ny = int(np.ravel(options.Nx)[0]), int(np.ravel(options.Ny)[0])
+    nf = int(2 ** np.ceil(np.log2(nx)))
+    if ny > nf:
+        raise ValueError('The filtering-based image preconditioner needs Ny <= 2^ceil(log2(Nx))')
+    if nf > 2048:
+        raise ValueError('The filtering-based image preconditioner is built for Nx <= 2048')
+
+
 def _check_pdhg_preconditioners(options):
-    """PDHG takes the filtering-based measurement preconditioner; its image
-    and diagonal measurement preconditioners are not built."""
+    """PDHG takes the filtering-based measurement (type 1) or image (type 5)
+    preconditioner, one at a time; its other image and diagonal measurement
+    preconditioners are not built."""
     pt_im = np.ravel(np.asarray(getattr(options, 'precondTypeImage', np.zeros(7, dtype=bool)), dtype=bool))
     pt_meas = np.ravel(np.asarray(getattr(options, 'precondTypeMeas', np.zeros(2, dtype=bool)), dtype=bool))
-    if pt_im.any():
-        raise ValueError('Image preconditioners are built for PKMA / MRAMLA / MBSREM, not PDHG')
+    if pt_im[:5].any() or (pt_im.size > 6 and pt_im[6]):
+        raise ValueError('Image preconditioners 0-4 and 6 are built for PKMA / MRAMLA / MBSREM, not PDHG')
+    if pt_im.size > 5 and pt_im[5]:
+        _check_image_filter(options)
+        if pt_meas.size > 1 and pt_meas[1]:
+            raise ValueError('Select one of the filtering-based preconditioners (image type 5, measurement type 1)')
     if pt_meas.size and pt_meas[0]:
         raise ValueError('The diagonal measurement preconditioner (type 0) is built for PKMA / MRAMLA / MBSREM')
     if pt_meas.size > 1 and pt_meas[1] and int(options.subsets) > 1 and int(options.subsetType) < 8:
@@ -460,6 +504,22 @@ def reconstructions_main(options):
             p.diff_type = int(getattr(options, 'derivativeType', 0))
         if on(6):
             p.precond_curv = 1
+        if on(5):
+            # the filtering-based image preconditioner and its relaxation schedule (functions.hpp:2093-2099,
+            # subiterStep.h:28-45, libHeader.h:1335-1338, prepass.py:1154-1156): lambdaFiltered in the
+            # filtering sub-iterations, lambdaN from sub-iteration K on (never when K = 0)
+            from . import filters
+            nf, _, fh = filters.image_filter_2d(int(np.ravel(options.Nx)[0]), getattr(options, 'filterWindow', 'hamming'),
+                                                 float(getattr(options, 'cutoffFrequency', 1.0)),
+                                                 float(getattr(options, 'normalFilterSigma', 0.25)))
+            th = torch.from_numpy(fh).to(dev)
+            keep.append(th)
+            p.img_filter_h = ctypes.c_void_p(th.data_ptr())
+            p.img_filter_nf = nf
+            K = int(getattr(options, 'filteringIterations', 0))
+            p.filter_iters = K
+            lam = _filtered_relaxation(options, lam, K, S)
+            p.relaxation = ctypes.c_void_p(lam.ctypes.data)
         if pt_meas.size and pt_meas[0]:
             p.precond_meas = 1
     if method == 'PKMA':
@@ -569,6 +629,19 @@ def reconstructions_main(options):
             p.filter_rows = nr
             p.filter_iters = int(getattr(options, 'filteringIterations', 0))
             p.tau_filt = float(np.ravel(getattr(options, 'tauCPFilt', 0.0))[0])
+        pt_im_p = np.ravel(np.asarray(getattr(options, 'precondTypeImage', np.zeros(7, dtype=bool)), dtype=bool))
+        if pt_im_p.size > 5 and pt_im_p[5]:
+            # the filtering-based image preconditioner: A^T p plus the TV term filtered in iterations
+            # k < filteringIterations, tauCP the step while filtering
+            from . import filters
+            nf, _, fh = filters.image_filter_2d(int(np.ravel(options.Nx)[0]), getattr(options, 'filterWindow', 'hamming'),
+                                                 float(getattr(options, 'cutoffFrequency', 1.0)),
+                                                 float(getattr(options, 'normalFilterSigma', 0.25)))
+            th = torch.from_numpy(fh).to(dev)
+            keep.append(th)
+            p.img_filter_h = ctypes.c_void_p(th.data_ptr())
+            p.img_filter_nf = nf
+            p.filter_iters = int(getattr(options, 'filteringIterations', 0))
     if options.PDHG and prox:
         # the proximal TV of the PDHG loop: dual step options.sigma2CP, the
         # beta ball (L2 or max norm), forward or backward differences
@@ -605,6 +678,7 @@ def reconstructions_main(options):
     _native.call("omb_reconstruct", options._handle, ctypes.byref(p), _ptr(y), _ptr(x0), _ptr(x), _stream(dev))
     options._check_staged("omb_reconstruct")
     options.tau_used = p.tau_used
+    options.tau_used2 = p.tau_used2
     out = x.cpu().numpy().reshape((int(np.ravel(options.Nx)[0]), int(np.ravel(options.Ny)[0]),
                                    int(np.ravel(options.Nz)[0]), 1), order='F')
     return out, np.empty(0, dtype=np.float32)

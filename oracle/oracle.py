@@ -383,7 +383,8 @@ def _grad_precond(xp, shape, diff_type, v1, v2):
 
 def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None, backward=None, randoms=None,
             prior_grad=None, positivity=True, alpha=None, upper=10000.0, precond=0, ref=None, alpha_precond=None,
-            grad_precond=None, curv_precond=False, meas_precond=False, auto_relax=False, relax_scaling=False):
+            grad_precond=None, curv_precond=False, meas_precond=False, auto_relax=False, relax_scaling=False,
+            img_filter=None, lam_filtered=None):
     """Restated relaxed loops in FP64 (kind: "ROSEM", "RAMLA", "BSREM",
     "ROSEM_MAP", "PKMA", "MRAMLA", "MBSREM"); returns the image after n_iter
     iterations.
@@ -411,7 +412,11 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
     divides the ratio by A_s 1 (zeros -> 1).  PKMA with auto_relax: lam[0] =
     ||x|| / ||g|| / 4 at the first sub-iteration, lam[it] = lam[it - 1] /
     (it / 35 + 1) at each later iteration's first; relax_scaling: q = ||x|| /
-    (lam ||g||), lam *= q / 1.5 when 0 < q < 1.5 (algorithms.h:151-197)."""
+    (lam ||g||), lam *= q / 1.5 when 0 < q < 1.5 (algorithms.h:151-197).
+    img_filter = dict(nf, F, K): the filtering-based image preconditioner last
+    (functions.hpp:2093-2099, image_filter_fft) in sub-iterations kk < K
+    (K = 0: kk = 0 only, subiterStep.h:28-45); lam_filtered: the relaxation
+    until sub-iteration K (never switched for K = 0), lam from K on."""
     fwd = forward or globals()["forward"]
     bwd = backward or globals()["backward"]
     lam = np.asarray(default_relaxation(n_iter) if lam is None else lam, dtype=np.float32)
@@ -453,6 +458,9 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
     for it in range(n_iter):
         for s in range(S):
             lm = float(lam[it])
+            if img_filter is not None and lam_filtered is not None and \
+                    not (img_filter["K"] > 0 and it * S + s >= img_filter["K"]):
+                lm = float(lam_filtered[it])
             du = prior_grad(x) if additive and prior_grad is not None else None
             fp = fwd(geom, x, s) + eps
             if randoms is not None:
@@ -486,6 +494,8 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
                 rhs = rhs * (np.maximum(xp, np.maximum(1e-5, ref)) / D)
             if dP is not None:
                 rhs = rhs * dP
+            if img_filter is not None and (kk < img_filter["K"] if img_filter["K"] > 0 else kk == 0):
+                rhs = image_filter_fft(rhs, shape, img_filter["nf"], img_filter["F"])
             if kind == "PKMA" and (auto_relax or relax_scaling):
                 xn, gn = np.linalg.norm(x), np.linalg.norm(rhs)
                 if auto_relax:
@@ -774,8 +784,18 @@ def row_filter_fft(v, rows, nf, filt, inverse=False):
     return np.real(np.fft.ifft(F, axis=0))[:rows].T.ravel()
 
 
+def image_filter_fft(g, shape, nf, F):
+    """filtering2D (functions.hpp:1908-1932) in FP64: every slice of g
+    zero-padded to nf x nf, its 2-D FFT multiplied by the real filter F,
+    transformed back, the real part cut to nx x ny."""
+    nx, ny, _ = shape
+    G = np.asarray(g, dtype=np.float64).reshape(shape, order='F')
+    T = np.fft.fft2(G, s=(nf, nf), axes=(0, 1)) * np.asarray(F, dtype=np.float64)[:, :, None]
+    return np.real(np.fft.ifft2(T, axes=(0, 1)))[:nx, :ny, :].ravel(order='F')
+
+
 def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1.0, eps=1e-5,
-            positivity=True, tv_grad=None, prox=None, meas_filter=None, tgv=None):
+            positivity=True, tv_grad=None, prox=None, meas_filter=None, tgv=None, img_filter=None):
     """PDHG with a TV-gradient term, one subset (computeForwardProject.h:227-316,
     algorithms.h:329-420, auxKernels.cl:2034-2062), in FP64.  tv_grad(x), when
     given, replaces the plain TV term beta * dTV(x) (the other TVKernel forms).
@@ -790,7 +810,10 @@ def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1
     three_d): TGV instead of the TV term (priors.h:284-313,
     image_oracle.proxtgv_step with theta and the current tau), the plain
     dual step divided by 1 + sigma beta (computeForwardProject.h:295-298;
-    with meas_filter, its ffilter built from sigma beta)."""
+    with meas_filter, its ffilter built from sigma beta).  img_filter =
+    dict(nf, F, K, tau2): the filtering-based image preconditioner, A^T p plus
+    the TV term filtered (image_filter_fft) in iterations k < K (K = 0: k = 0
+    only) and the primal step tau2 from k = K on (subiterStep.h:28-45)."""
     from oracle import image_oracle as io
     shape = (geom.nx, geom.ny, geom.nz)
     x = np.asarray(x0, dtype=np.float64).copy()
@@ -808,6 +831,8 @@ def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1
         mf = meas_filter
         if mf is not None and mf["K"] > 0 and k == mf["K"]:
             tau = mf["tau2"]
+        if img_filter is not None and img_filter["K"] > 0 and k == img_filter["K"]:
+            tau = img_filter["tau2"]
         if mf is not None and (mf["K"] == 0 or k < mf["K"]):
             r = row_filter_fft(res, mf["rows"], mf["nf"], mf["filter0"])
             if mf["K"] == 0:
@@ -825,6 +850,8 @@ def pdhg_tv(geom: Geometry, y, x0, n_iter, tau, beta, smooth, sigma=1.0, theta=1
             rhs = bdd_backward(geom, p, -1) - io.proxtv_divergence(q, shape, prox.get("diff_type", 0))
         else:
             rhs = bdd_backward(geom, p, -1) + (tv_gradient(x, shape, smooth, beta) if tv_grad is None else tv_grad(x))
+        if img_filter is not None and (k < img_filter["K"] if img_filter["K"] > 0 else k == 0):
+            rhs = image_filter_fft(rhs, shape, img_filter["nf"], img_filter["F"])
         u_prev = u.copy()
         u = u - tau * rhs
         if positivity:

@@ -262,6 +262,12 @@ def ramp_fixture():
         for c in (1.0, 0.8):
             for N in (512, 64, 101):
                 out[f"{window}_{c}_{N}"] = np.asarray(mod.rampFilt(N, window, c, 0.25))
+    # the 2-D form (use2D) of the image preconditioner: its shape and the
+    # first N^2 values, which the library reads as the N x N filter
+    for N in (16, 32):
+        f2 = np.asarray(mod.rampFilt(N, "hamming", 1.0, 0.25, True))
+        out[f"use2D_shape_{N}"] = np.asarray(f2.shape)
+        out[f"use2D_first_{N}"] = np.ascontiguousarray(f2).ravel()[:N * N].copy()
     np.savez_compressed(os.path.join(HERE, "ramp_filters.npz"), **out)
     print("ramp_filters", len(out))
 

@@ -436,14 +436,27 @@ def _other_precond_case(case, g, rng):
     if case == "relax":
         return (dict(computeRelaxationParameters=True, relaxationScaling=True),
                 dict(auto_relax=True, relax_scaling=True), "PKMA", [0.3, 0.2, 0.15])
+    if case in ("type5", "type5k0", "type5mramla"):
+        # the filtering-based image preconditioner: one filtered iteration with its own relaxation, or
+        # (K = 0) the first sub-iteration only with lambdaFiltered = lambdaN throughout
+        from omega_b200 import filters
+        nf, F, _ = filters.image_filter_2d(g.nx, "hann")
+        K = 0 if case == "type5k0" else S
+        lf = None if case == "type5k0" else np.array([0.05, 0.04, 0.03], np.float32)
+        opts = dict(precondTypeImage=np.array([0, 0, 0, 0, 0, 1, 0], bool), filteringIterations=K, filterWindow="hann")
+        if lf is not None:
+            opts["lambdaFiltered"] = lf
+        return (opts, dict(img_filter=dict(nf=nf, F=F, K=K), lam_filtered=lf),
+                "MRAMLA" if case == "type5mramla" else "PKMA", [0.3, 0.2, 0.15])
     raise KeyError(case)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["type2", "type3", "type4", "type0+4", "type6", "meas0", "relax"])
+@pytest.mark.parametrize("case", ["type2", "type3", "type4", "type0+4", "type6", "meas0", "relax", "type5", "type5k0",
+                                  "type5mramla"])
 def test_builtin_other_preconditioners(cuda, case):
-    """Image preconditioners 2, 3, 4 and 6, the measurement preconditioner 0
-    and PKMA's automatic relaxation through the built-in entry against the
+    """Image preconditioners 2, 3, 4, 5 and 6, the measurement preconditioner
+    0 and PKMA's automatic relaxation through the built-in entry against the
     FP64 loop; each changes the result."""
     o, g = _pet("pet_mini", 42)
     rng = np.random.default_rng(43)
@@ -464,8 +477,17 @@ def test_other_preconditioners_validate():
     from omega_b200 import reconstruction as rec
     o.PKMA = True
     o.precondTypeImage = np.array([0, 0, 0, 0, 0, 1, 0], bool)
-    with pytest.raises(ValueError, match="type 5"):
+    o.filteringIterations = 3
+    o.Niter = 2
+    o.lambdaN = np.array([1., .5], np.float32)
+    o.lambdaFiltered = np.array([.3, .2], np.float32)
+    with pytest.raises(ValueError, match="multiple of subsets"):
         rec.reconstructions_main(o)
+    nx = int(np.ravel(o.Nx)[0])
+    o.Ny = 2 * nx + 1
+    with pytest.raises(ValueError, match="Ny <="):
+        rec.reconstructions_main(o)
+    o.Ny = nx
     o.precondTypeImage = np.array([1, 1, 0, 0, 0, 0, 0], bool)
     with pytest.raises(ValueError, match="Only one"):
         rec.reconstructions_main(o)
