@@ -46,6 +46,16 @@ int omb_unet_take_error(int32_t *out_host);
 int omb_unet_conv_wgrad(int32_t cin, int32_t cout, const void *in, const void *dz, float *dw, int32_t X, int32_t Y,
                         int32_t Z, int32_t B, void *stream);
 
+/*
+ * The same weight gradient on the tensor cores (tcgen05.mma, the voxels as
+ * the reduction dimension, 128 rows of (tap, ci) x cout per CTA accumulated in
+ * tensor memory, FP32 atomics into dw), for the shapes omb_unet_conv_tc
+ * builds.  Its waits are bounded like omb_unet_conv_tc's (flag read by
+ * omb_unet_take_error).
+ */
+int omb_unet_conv_wgrad_tc(int32_t cin, int32_t cout, const void *in, const void *dz, float *dw, int32_t X,
+                           int32_t Y, int32_t Z, int32_t B, void *stream);
+
 /* db[c] += sum_v dz[v][c], c in {16, 32, 64}. */
 int omb_unet_bias_grad(int32_t c, const void *dz, float *db, int64_t nvox, void *stream);
 

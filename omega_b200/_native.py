@@ -327,6 +327,7 @@ EXPORTS = [
     ("omb_unet_conv_tc", ctypes.c_int, [_i32, _i32, _v, _v, _v, _v, _v, _i32, _i32, _i32, _i32, _i32, _v]),
     ("omb_unet_take_error", ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     ("omb_unet_conv_wgrad", ctypes.c_int, [_i32, _i32, _v, _v, _v, _i32, _i32, _i32, _i32, _v]),
+    ("omb_unet_conv_wgrad_tc", ctypes.c_int, [_i32, _i32, _v, _v, _v, _i32, _i32, _i32, _i32, _v]),
     ("omb_unet_bias_grad", ctypes.c_int, [_i32, _v, _v, _i64, _v]),
     ("omb_unet_flip_weights", ctypes.c_int, [_v, _v, _i32, _i32, _v]),
     ("omb_unet_avgpool", ctypes.c_int, [_v, _v, _i32, _i32, _i32, _i32, _i32, _i32, _v]),

@@ -13,7 +13,9 @@
 // epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes
 // 32w..32w+31 = voxels 32w..), adds the bias, applies the ReLU or the mask
 // and stores BF16.  Every mbarrier wait is bounded; on a timeout the CTA
-// raises the error flag read by omb_unet_take_error().
+// raises the error flag read by omb_unet_take_error().  The weight gradient
+// (k_conv3d_wgrad_tc, below) runs on the same instructions with the voxels
+// as the reduction dimension.
 #include <cuda_bf16.h>
 
 #include "kernels.h"
@@ -272,6 +274,189 @@ int unet_conv_tc(int cin, int cout, const void *in, const void *w, const float *
                                               " is not built");
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradient on the tensor cores.  dW[tap][co][ci] = sum_v dz[v][co]
+// in[v + off(tap)][ci] is a GEMM with the voxels as its K dimension:
+// D[m][co] = sum_v A[m][v] B[co][v], the rows m = tap * CIN + ci of all 27
+// taps taken 128 at a time (grid.y), B = dz.  A CTA reduces `per_cta`
+// voxels (grid.x) in stages of 32 (two K = 16 instructions) and adds its
+// 128 x COUT partial sums to dW with FP32 atomics.  Both operands are staged
+// MN-major (the transpose bits of the instruction descriptor): 8 consecutive
+// rows of A are 8 consecutive channels of one tap-shifted input voxel and 8
+// consecutive rows of B 8 output channels of one dz voxel, so every 16-byte
+// global load lands as one 16-byte row of a core matrix (8 voxels x 16
+// bytes).  Core matrix (row group g, voxel group k) lies at g * 256 + k *
+// 128 bytes: a row-group stride of 256 (SBO) and a voxel-group stride of 128
+// (LBO), the same address map as the K-major operands of the forward kernel,
+// so the MMA reads stay inside each 128-row x 16-voxel sub-tile.
+// ---------------------------------------------------------------------------
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_conv3d_wgrad_tc(const __nv_bfloat16 *__restrict__ in,
+                                                         const __nv_bfloat16 *__restrict__ dz,
+                                                         float *__restrict__ dw, int X, int Y, int Z, int64_t nvox,
+                                                         int per_cta) {
+    static_assert(CIN % 8 == 0 && COUT % 16 == 0 && COUT <= 128, "channel counts");
+    constexpr int MROWS = 27 * CIN;
+    constexpr int KV = 32;                       // voxels per stage
+    constexpr int A_SUB = tc::kM * 16 * 2;       // one K = 16 sub-tile of A (bytes)
+    constexpr int B_SUB = COUT * 16 * 2;         // of B
+    constexpr int NG = COUT / 8;                 // 8-channel groups of B
+    constexpr int TMEM_COLS = COUT <= 32 ? 32 : (COUT <= 64 ? 64 : 128);
+    __shared__ __align__(1024) uint8_t sA[2][2 * A_SUB];
+    __shared__ __align__(1024) uint8_t sB[2][2 * B_SUB];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ short4 vc[2][KV];  // (x, y, z, inside) of each staged voxel
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        tc::mbar_init(tc::smem_u32(&bars[0]), 1);
+        tc::mbar_init(tc::smem_u32(&bars[1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(tc::smem_u32(&tmem_base)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const int m0 = blockIdx.y * tc::kM;
+    // this thread's A row group (the same in every stage): tap, first channel and the tap's voxel offset
+    const int ga = tid & 15, ma = m0 + ga * 8;
+    const bool arow = ma < MROWS;
+    const int tapa = arow ? ma / CIN : 0, cia = arow ? ma - tapa * CIN : 0;
+    const int ddx = tapa % 3 - 1, ddy = (tapa / 3) % 3 - 1, ddz = tapa / 9 - 1;
+    const int64_t doff = ((int64_t)ddz * Y + ddy) * X + ddx;
+    const int64_t v_begin = (int64_t)blockIdx.x * per_cta;
+    const int64_t v_end = min(v_begin + (int64_t)per_cta, nvox);
+    const int nst = (int)((v_end - v_begin + KV - 1) / KV);
+    // A and B both MN-major (transpose bits 15 and 16)
+    const uint32_t idesc = tc::instr_desc(COUT) | (1u << 15) | (1u << 16);
+    // (x, y, z) of voxel v0 + k of a stage, in 32-bit arithmetic (the launch keeps nvox below 2^31)
+    auto coords = [&](int st_idx, int buf) {
+        if (tid < KV) {
+            const int64_t v = v_begin + (int64_t)st_idx * KV + tid;
+            short4 c = make_short4(0, 0, 0, 0);
+            if (v < v_end) {
+                int q = (int)v;
+                c.x = (short)(q % X);
+                q /= X;
+                c.y = (short)(q % Y);
+                q /= Y;
+                c.z = (short)(q % Z);
+                c.w = 1;
+            }
+            vc[buf][tid] = c;
+        }
+    };
+    int issued = 0;
+    bool ok = true;
+    if (nst > 0) coords(0, 0);
+    for (int ks = 0; ks < nst; ++ks) {
+        const int s = ks & 1;
+        if (ks >= 2) {
+            if (!tc::mbar_wait(tc::smem_u32(&bars[s]), (uint32_t)((ks >> 1) - 1) & 1u)) ok = false;
+        }
+        if (!__syncthreads_and(ok)) {
+            ok = false;
+            break;
+        }
+        if (ks + 1 < nst) coords(ks + 1, s ^ 1);  // read after the next barrier
+        const int64_t v0 = v_begin + (int64_t)ks * KV;
+        // A: 32 voxels x 16 row groups, 4 per thread (the voxel k = idx / 16, this thread's row group ga); the
+        // voxel coordinates come from the table the previous step filled
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = (tid >> 4) + 8 * j;
+            const short4 c = vc[s][k];
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (arow && c.w) {
+                const int xs = c.x + ddx, ys = c.y + ddy, zs = c.z + ddz;
+                if (xs >= 0 && xs < X && ys >= 0 && ys < Y && zs >= 0 && zs < Z)
+                    val = __ldg(reinterpret_cast<const uint4 *>(in + (v0 + k + doff) * CIN + cia));
+            }
+            const int kk = k & 15;
+            *reinterpret_cast<uint4 *>(sA[s] + (k >> 4) * A_SUB + ga * tc::kCoreGroup + (kk >> 3) * tc::kKHalf +
+                                       (kk & 7) * 16) = val;
+        }
+        // B: 32 voxels x NG channel groups
+        for (int idx = tid; idx < KV * NG; idx += 128) {
+            const int k = idx / NG, g = idx - k * NG;
+            const int64_t v = v0 + k;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (v < v_end) val = __ldg(reinterpret_cast<const uint4 *>(dz + v * COUT + g * 8));
+            const int kk = k & 15;
+            *reinterpret_cast<uint4 *>(sB[s] + (k >> 4) * B_SUB + g * tc::kCoreGroup + (kk >> 3) * tc::kKHalf +
+                                       (kk & 7) * 16) = val;
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+            for (int sub = 0; sub < 2; ++sub)
+                tc::mma_issue(tmem, tc::smem_desc(tc::smem_u32(sA[s] + sub * A_SUB)),
+                              tc::smem_desc(tc::smem_u32(sB[s] + sub * B_SUB)), idesc, (ks > 0 || sub > 0) ? 1u : 0u);
+            tc::mma_commit(tc::smem_u32(&bars[s]));
+        }
+        issued = ks + 1;
+    }
+    if (ok && nst > 0) {
+        const int last = nst - 1;
+        if (!tc::mbar_wait(tc::smem_u32(&bars[last & 1]), (uint32_t)(last >> 1) & 1u)) ok = false;
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(&g_unet_error, 1);
+        if (issued > 0) tc::mbar_wait(tc::smem_u32(&bars[(issued - 1) & 1]), (uint32_t)((issued - 1) >> 1) & 1u);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (ok && nst > 0) {
+        // row m of D = TMEM lane m: warp w holds rows 32w..32w+31
+        const int m = m0 + warp * 32 + lane;
+        const bool mrow = m < MROWS;
+        const int tap = mrow ? m / CIN : 0, ci = mrow ? m - tap * CIN : 0;
+        float *d = dw + (int64_t)tap * COUT * CIN + ci;
+#pragma unroll
+        for (int c0 = 0; c0 < COUT; c0 += 16) {
+            float acc[16];
+            tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, acc);
+            if (mrow) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) atomicAdd(d + (c0 + i) * CIN, acc[i]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
+int unet_conv_wgrad_tc(int cin, int cout, const void *in, const void *dz, float *dw, int X, int Y, int Z, int B,
+                       cudaStream_t st) {
+    if (X <= 0 || Y <= 0 || Z <= 0 || B <= 0) return set_error(OMB_ERR_INVALID, "bad conv volume");
+    const int64_t nvox = (int64_t)X * Y * Z * B;
+    const int per_cta = 32 * 256;  // voxels per CTA (a multiple of the 32-voxel stage)
+    const int64_t chunks = (nvox + per_cta - 1) / per_cta;
+    if (nvox > 2147483647 || X > 32767 || Y > 32767 || Z > 32767)
+        return set_error(OMB_ERR_UNSUPPORTED, "wgrad volume too large (2^31 voxels, 32767 per axis)");
+    const auto *i = static_cast<const __nv_bfloat16 *>(in), *d = static_cast<const __nv_bfloat16 *>(dz);
+#define X(ci, co)                                                                                             \
+    if (cin == ci && cout == co) {                                                                            \
+        dim3 grid((unsigned)chunks, (unsigned)((27 * ci + tc::kM - 1) / tc::kM));                              \
+        k_conv3d_wgrad_tc<ci, co><<<grid, 128, 0, st>>>(i, d, dw, X, Y, Z, nvox, per_cta);                     \
+        OMB_LAUNCH_CHECK("tcgen05 wgrad launch");                                                             \
+        return OMB_OK;                                                                                        \
+    }
+    OMB_TC_SHAPES(X)
+#undef X
+    return set_error(OMB_ERR_UNSUPPORTED, "wgrad shape " + std::to_string(cin) + "->" + std::to_string(cout) +
+                                              " is not built");
+}
+
 }  // namespace omb
 
 extern "C" {
@@ -280,6 +465,12 @@ int omb_unet_conv_tc(int32_t cin, int32_t cout, const void *in, const void *w, c
                      const void *relu_mask, int32_t relu, int32_t X, int32_t Y, int32_t Z, int32_t B, void *stream) {
     if (!in || !w || !out) return omb::set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_unet_conv_tc");
     return omb::unet_conv_tc(cin, cout, in, w, bias, out, relu_mask, relu, X, Y, Z, B, (cudaStream_t)stream);
+}
+
+int omb_unet_conv_wgrad_tc(int32_t cin, int32_t cout, const void *in, const void *dz, float *dw, int32_t X,
+                           int32_t Y, int32_t Z, int32_t B, void *stream) {
+    if (!in || !dz || !dw) return omb::set_error(OMB_ERR_INVALID, "NULL buffer passed to omb_unet_conv_wgrad_tc");
+    return omb::unet_conv_wgrad_tc(cin, cout, in, dz, dw, X, Y, Z, B, (cudaStream_t)stream);
 }
 
 int omb_unet_take_error(int32_t *out_host) {

@@ -48,6 +48,9 @@ class UNet3D:
     # "omb_unet_conv_tc" (tcgen05, accumulator in tensor memory) or
     # "omb_unet_conv" (warp-level mma.sync)
     conv_entry = "omb_unet_conv_tc"
+    # weight gradients: "omb_unet_conv_wgrad" (mma.sync, the faster of the two on
+    # every built shape) or "omb_unet_conv_wgrad_tc" (tcgen05)
+    wgrad_entry = "omb_unet_conv_wgrad"
 
     def __init__(self, X, Y, Zs, batch, device, seed=0):
         import torch
@@ -185,7 +188,7 @@ class UNet3D:
         X, Y, Z = self._dims(level)
         st = self._stream()
         p = self.params[i]
-        _native.call("omb_unet_conv_wgrad", ci, co, _p(src), _p(dz), _p(p["gw"]), X, Y, Z, self.B, st)
+        _native.call(self.wgrad_entry, ci, co, _p(src), _p(dz), _p(p["gw"]), X, Y, Z, self.B, st)
         _native.call("omb_unet_bias_grad", co, _p(dz), _p(p["gb"]), X * Y * Z * self.B, st)
 
     def _dgrad(self, i, dz, dst, level, mask):

@@ -53,3 +53,30 @@ def test_tc_conv_matches_oracle(cuda, ci, co):
     flag = ctypes.c_int32(-1)
     _native.call("omb_unet_take_error", ctypes.byref(flag))
     assert flag.value == 0
+
+
+@pytest.mark.parametrize("ci,co", SHAPES)
+def test_tc_wgrad_matches_oracle(cuda, ci, co):
+    """omb_unet_conv_wgrad_tc (tcgen05, the voxels as the reduction
+    dimension) against the FP64 weight gradient and the mma.sync kernel, on
+    a volume whose voxel count leaves partial stages and CTAs."""
+    import torch
+    from oracle import unet_oracle as uo
+    from omega_b200 import _native
+    st = ctypes.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
+    rng = np.random.default_rng(ci * 7 + co)
+    B, Z, Y, X = 2, 7, 9, 70          # 8820 voxels: 2 CTAs of 8192, a partial last stage
+    x = uo.bf16(rng.normal(0, 1, (B, Z, Y, X, ci)))
+    dz = uo.bf16(rng.normal(0, 1, (B, Z, Y, X, co)))
+    xt, dzt = _bf(x, cuda), _bf(dz, cuda)
+    dw = torch.zeros(27 * co * ci, device=cuda)
+    _native.call("omb_unet_conv_wgrad_tc", ci, co, P(xt), P(dzt), P(dw), X, Y, Z, B, st)
+    ref = uo.conv3d_wgrad(x, dz)
+    got = dw.cpu().numpy().reshape(ref.shape)
+    assert _rel(got, ref) < 1e-5, _rel(got, ref)
+    dw2 = torch.zeros_like(dw)
+    _native.call("omb_unet_conv_wgrad", ci, co, P(xt), P(dzt), P(dw2), X, Y, Z, B, st)
+    assert _rel(got, dw2.cpu().numpy().reshape(ref.shape)) < 1e-5
+    flag = ctypes.c_int32(-1)
+    _native.call("omb_unet_take_error", ctypes.byref(flag))
+    assert flag.value == 0
