@@ -403,8 +403,11 @@ __device__ bool orth_trace(const Grid &g, const Orth &o, const Ray &ray, float g
     return true;
 }
 
+// Register caps: 64 per thread for the forward projection (8 CTAs, 32 warps per SM) and 80 for the
+// backprojection (6 CTAs); the tracer is latency-bound on dependent FP64 arithmetic, and the extra warps
+// hide more of it than the spills to the stack cost.
 template <int NB>
-__global__ void __launch_bounds__(kBlockO) k_orth_fp(Grid g, RaySet rs, Orth o, Tof tof, float gf, const float *img,
+__global__ void __launch_bounds__(kBlockO, 8) k_orth_fp(Grid g, RaySet rs, Orth o, Tof tof, float gf, const float *img,
                                                      float *y) {
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rs.m_size) return;
@@ -428,7 +431,7 @@ __global__ void __launch_bounds__(kBlockO) k_orth_fp(Grid g, RaySet rs, Orth o, 
 }
 
 template <int NB>
-__global__ void __launch_bounds__(kBlockO) k_orth_bp(Grid g, RaySet rs, Orth o, Tof tof, float gf, const float *y,
+__global__ void __launch_bounds__(kBlockO, 6) k_orth_bp(Grid g, RaySet rs, Orth o, Tof tof, float gf, const float *y,
                                                      float *img, float *sens) {
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rs.m_size) return;
