@@ -333,7 +333,8 @@ typedef enum omb_prior {
     OMB_PRIOR_TV = 6,       /* options.TV with a MAP algorithm other than PDHG: omb_tv_gradient, tv_smoothing */
     OMB_PRIOR_GGMRF = 7,    /* options.GGMRF: omb_ggmrf_gradient over prior_g with ggmrf_weights and ggmrf[3] */
     OMB_PRIOR_HYPERBOLIC = 8,/* options.hyperbolic: omb_hyperbolic_gradient over prior_g with hyper_weights */
-    OMB_PRIOR_WMEAN = 9     /* options.weighted_mean, mean_type 1-6: omb_wmean_gradient over prior_g */
+    OMB_PRIOR_WMEAN = 9,    /* options.weighted_mean, mean_type 1-6: omb_wmean_gradient over prior_g */
+    OMB_PRIOR_AD = 10       /* options.AD: omb_ad_gradient with ad_dt, ad_k, ad_niter, ad_flux, ad_diffusion */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -433,6 +434,12 @@ typedef struct omb_recon_params {
     int32_t img_filter_nf;    /* its length Nf (a power of two >= nx, ny) */
     float tau_used2;          /* out: PDHG with a filtering preconditioner, the primal step from iteration
                                  filter_iters on (0 when the run never switches) */
+    float ad_dt;              /* OMB_PRIOR_AD: options.TimeStepAD */
+    float ad_k;               /* OMB_PRIOR_AD: options.KAD (conductance) */
+    int32_t ad_niter;         /* OMB_PRIOR_AD: options.NiterAD */
+    int32_t ad_flux;          /* OMB_PRIOR_AD: options.FluxType (1 exponential, 2 quadratic) */
+    int32_t ad_diffusion;     /* OMB_PRIOR_AD: options.DiffusionType (1 gradient, 2 modified curvature); the
+                                 normalisation switch is mrp_no_norm (options.med_no_norm) */
 } omb_recon_params;
 
 /*
@@ -584,6 +591,20 @@ int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int3
  */
 int omb_mrp_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx, int32_t my,
                      int32_t mz, float epps, float beta, int32_t no_norm, void *stream);
+
+/*
+ * Anisotropic-diffusion prior gradient (priors.h:226-237): grad += beta *
+ * (u - AD(u)) / (AD(u) + epps) (no_norm: beta * (u - AD(u))), AD = `niter`
+ * steps of 2-D diffusion of every slice (edges replicated) with time step dt
+ * and conductance k: flux 1 exponential exp(-g^2 / k^2), 2 quadratic
+ * 1 / (1 + g^2 / k^2); diffusion 1 gradient (Perona-Malik), 2 modified
+ * curvature.  The reference calls ArrayFire's anisotropicDiffusion here; this
+ * restates the published schemes (ArrayFire's own code is not part of the
+ * reference).  Allocates two scratch images stream-ordered.
+ */
+int omb_ad_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float dt, float k,
+                    int32_t niter, int32_t flux, int32_t diffusion, float epps, float beta, int32_t no_norm,
+                    void *stream);
 
 /*
  * Non-local regulariser gradient (the NLM kernel, auxKernels.cl:297-620, the

@@ -152,6 +152,11 @@ class ReconParams(ctypes.Structure):
         ("img_filter_h", ctypes.c_void_p),
         ("img_filter_nf", ctypes.c_int32),
         ("tau_used2", ctypes.c_float),
+        ("ad_dt", ctypes.c_float),
+        ("ad_k", ctypes.c_float),
+        ("ad_niter", ctypes.c_int32),
+        ("ad_flux", ctypes.c_int32),
+        ("ad_diffusion", ctypes.c_int32),
     ]
 
 
@@ -175,6 +180,7 @@ OMB_TV_PLAIN, OMB_TV_SATV, OMB_TV_W1, OMB_TV_ANAT1, OMB_TV_ANAT2, OMB_TV_APLS = 
 OMB_PRIOR_GGMRF = 7
 OMB_PRIOR_HYPERBOLIC = 8
 OMB_PRIOR_WMEAN = 9
+OMB_PRIOR_AD = 10
 
 
 class Tuning(ctypes.Structure):
@@ -290,6 +296,10 @@ EXPORTS = [
                                         ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
                                         ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_void_p]),
+    ("omb_ad_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                       ctypes.c_void_p]),
     ("omb_mrp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p]),

@@ -226,6 +226,15 @@ class projectorClass:
     sigma2CP = 1.
     useL2Ball = True
     derivativeType = 0
+    # the anisotropic-diffusion prior (proj.py:325-326, 334, 340-341 of the
+    # reference): flux 1 exponential / 2 quadratic, diffusion 1 gradient /
+    # 2 modified curvature, iterations, time step, conductance
+    AD = False
+    FluxType = 1
+    DiffusionType = 2
+    NiterAD = 1
+    TimeStepAD = 1.
+    KAD = 1.
     # TGV with PDHG (proj.py:351-352, 360, 411 of the reference): the
     # first- and second-order ball radii, 2-D TGV (no z component of v)
     TGV = False

@@ -391,13 +391,19 @@ def reconstructions_main(options):
     hyper = bool(getattr(options, 'hyperbolic', False))
     wmean = bool(getattr(options, 'weighted_mean', False))
     apls = bool(getattr(options, 'APLS', False)) and not options.PDHG   # the APLS prior: TVKernel's APLS form
+    ad = bool(getattr(options, 'AD', False))
     n_priors = (int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp) + int(ggmrf) +
-                int(hyper) + int(wmean) + int(apls))
+                int(hyper) + int(wmean) + int(apls) + int(ad))
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
         raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM, '
-                                  'options.MRP, options.TV, options.APLS, options.GGMRF, options.hyperbolic or '
-                                  'options.weighted_mean')
+                                  'options.MRP, options.TV, options.APLS, options.GGMRF, options.hyperbolic, '
+                                  'options.weighted_mean or options.AD')
+    if prior and ad:
+        if int(getattr(options, 'NiterAD', 1)) < 1 or not float(getattr(options, 'KAD', 1.)) > 0:
+            raise ValueError('options.AD needs NiterAD >= 1 and KAD > 0')
+        if int(getattr(options, 'FluxType', 1)) not in (1, 2) or int(getattr(options, 'DiffusionType', 2)) not in (1, 2):
+            raise ValueError('options.FluxType and options.DiffusionType must be 1 or 2')
     if method in ('PKMA', 'MRAMLA', 'MBSREM'):
         _check_preconditioners(options)
     if method == 'PDHG':
@@ -526,7 +532,8 @@ def reconstructions_main(options):
         p.pkma_relax = (1 if getattr(options, 'computeRelaxationParameters', False) else 0) | \
             (2 if getattr(options, 'relaxationScaling', False) else 0)
     if prior:
-        p.prior = (_native.OMB_PRIOR_RDP if options.RDP else
+        p.prior = (_native.OMB_PRIOR_AD if ad else
+                   _native.OMB_PRIOR_RDP if options.RDP else
                    (_native.OMB_PRIOR_NLM if nlm else
                     (_native.OMB_PRIOR_MRP if mrp else
                      (_native.OMB_PRIOR_TV if (tvp or apls) else
@@ -534,6 +541,15 @@ def reconstructions_main(options):
                        (_native.OMB_PRIOR_HYPERBOLIC if hyper else
                         (_native.OMB_PRIOR_WMEAN if wmean else
                          (_native.OMB_PRIOR_QUAD if quad else _native.OMB_PRIOR_HUBER))))))))
+        if ad:
+            # the AD prior (priors.h:226-237, libHeader.h:1212-1232): time step, conductance, iterations,
+            # flux 1 exponential / 2 quadratic, diffusion 1 gradient / 2 modified curvature
+            p.ad_dt = float(getattr(options, 'TimeStepAD', 1.))
+            p.ad_k = float(getattr(options, 'KAD', 1.))
+            p.ad_niter = int(getattr(options, 'NiterAD', 1))
+            p.ad_flux = int(getattr(options, 'FluxType', 1))
+            p.ad_diffusion = int(getattr(options, 'DiffusionType', 2))
+            p.mrp_no_norm = 1 if getattr(options, 'med_no_norm', False) else 0
         if wmean:
             from . import priors
             mt = int(getattr(options, 'mean_type', 4))
