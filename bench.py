@@ -57,7 +57,7 @@ PROFILED_TRAFFIC = {
     ("cbct", "bdd_fp"): 9.46e9,
     ("cbct", "bdd_bp"): 3.76e8,
     ("dynpet", "siddon_fp"): 3.81e8,
-    ("dynpet", "siddon_bp"): 4.77e8,
+    ("dynpet", "siddon_bp"): 6.59e9,   # 3 launches of k_sm_bp_sl (8 frames each) per call
     # interp_tof_capture.md: one subset's forward launch (16 per step)
     ("interp_tof", "interp_fp"): 5.60e6,
 }
@@ -68,7 +68,7 @@ PROFILED_LIMITER = {
     ("cbct", "bdd_fp"): {"issue_active_pct": 80.4, "sm_throughput_pct": 75.5, "dram_pct": 7.6},
     ("cbct", "bdd_bp"): {"issue_active_pct": 72.9, "sm_throughput_pct": 71.8, "dram_pct": 0.35},
     ("dynpet", "siddon_fp"): {"issue_active_pct": 66.5, "l1tex_pct": 92.0, "dram_pct": 1.0},
-    ("dynpet", "siddon_bp"): {"issue_active_pct": 44.4, "lts_pct": 65.9, "dram_pct": 1.0},
+    ("dynpet", "siddon_bp"): {"issue_active_pct": 10.7, "l1tex_pct": 94.0, "dram_pct": 21.8},
     ("interp_tof", "interp_fp"): {"issue_active_pct": 84.9, "sm_throughput_pct": 78.6, "dram_pct": 0.01},
 }
 FALLBACK_HBM_GBS = 6650.0

@@ -1068,6 +1068,8 @@ int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weig
         for (auto &m : h->sysmats) {
             h->retired.push_back(m.off);
             h->retired.push_back(m.ent);
+            h->retired.push_back(m.soff);
+            h->retired.push_back(m.sent);
         }
         h->sysmats.clear();
     }

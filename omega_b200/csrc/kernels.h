@@ -163,8 +163,12 @@ struct SysMat {
     int64_t proj0 = 0, m_size = 0;
     int cur_subset = 0;
     int64_t *off = nullptr;
-    uint2 *ent = nullptr;  // (launch-local ray index, weight bits)
+    uint2 *ent = nullptr;  // (launch-local ray index, weight bits), voxel-major lists
     int64_t nnz = 0;
+    // sliced copy (when it fits): slices of 32 consecutive voxels, entry k of the slice's voxel l at
+    // soff[slice] + 32 k + l; the voxel-major lists are released once it is built
+    int64_t *soff = nullptr;
+    uint2 *sent = nullptr;
 };
 // Builds sm for the rays of rs (the walk and weights of the ray-driven backprojection); synchronises `st`
 // and refuses to run while `st` is captured into a CUDA graph.

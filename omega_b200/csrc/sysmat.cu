@@ -15,6 +15,12 @@
 // gathered 8 (or 4) at a time from a ray-major copy of the measurements
 // (32 bytes a ray), so a crossing costs one 8-byte matrix read and one
 // 32-byte gather for 8 frames.
+//
+// After the build the lists are re-laid in slices of 32 consecutive voxels
+// (one warp's voxels): entry k of every voxel of a slice side by side, so a
+// warp reads its 32 matrix entries of step k as one 256-byte run instead of
+// 32 scattered 8-byte reads.  Each voxel still sums its own list in ray
+// order, so the result is the same bit for bit.
 #include "common.cuh"
 #include "kernels.h"
 #include "siddon.cuh"
@@ -128,13 +134,64 @@ __global__ void __launch_bounds__(kBlock) k_sm_bp(const int64_t *__restrict__ of
     }
 }
 
+// the voxel-major lists re-laid in slices of 32 voxels (entry k of voxel l at soff[s] + 32 k + l)
+__global__ void k_sm_slice(const int64_t *__restrict__ off, const uint2 *__restrict__ ent,
+                           const int64_t *__restrict__ soff, uint2 *__restrict__ sent, int64_t n_img) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_img; v += stride) {
+        const int64_t a = off[v], n = off[v + 1] - a;
+        uint2 *d = sent + soff[v >> 5] + (v & 31);
+        for (int64_t k = 0; k < n; ++k) d[k * 32] = ent[a + k];
+    }
+}
+
+// k_sm_bp on the sliced lists: the grid-stride loop keeps a warp on the 32 voxels of one slice
+template <int FB>
+__global__ void __launch_bounds__(kBlock) k_sm_bp_sl(const int64_t *__restrict__ off, const int64_t *__restrict__ soff,
+                                                     const uint2 *__restrict__ sent, const float *__restrict__ y,
+                                                     int64_t n_img, float *__restrict__ img, int64_t img_stride, int nf) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n_img; v += stride) {
+        float acc[FB];
+#pragma unroll
+        for (int f = 0; f < FB; ++f) acc[f] = 0.f;
+        const int64_t n = __ldg(off + v + 1) - __ldg(off + v);
+        const uint2 *e0 = sent + __ldg(soff + (v >> 5)) + (v & 31);
+#pragma unroll 4
+        for (int64_t k = 0; k < n; ++k) {
+            const uint2 e = __ldg(e0 + k * 32);
+            const float w = __uint_as_float(e.y);
+            if (FB == 1) {
+                acc[0] = fmaf(__ldg(y + e.x), w, acc[0]);
+            } else {
+                const float4 *p = reinterpret_cast<const float4 *>(y) + (int64_t)e.x * (FB / 4);
+#pragma unroll
+                for (int q = 0; q < FB / 4; ++q) {
+                    const float4 t = __ldg(p + q);
+                    acc[4 * q] = fmaf(t.x, w, acc[4 * q]);
+                    acc[4 * q + 1] = fmaf(t.y, w, acc[4 * q + 1]);
+                    acc[4 * q + 2] = fmaf(t.z, w, acc[4 * q + 2]);
+                    acc[4 * q + 3] = fmaf(t.w, w, acc[4 * q + 3]);
+                }
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < FB; ++f)
+            if (f < nf) img[f * img_stride + v] = acc[f];
+    }
+}
+
 }  // namespace
 
 void sysmat_free(SysMat &sm) {
     if (sm.off) cudaFree(sm.off);
     if (sm.ent) cudaFree(sm.ent);
+    if (sm.soff) cudaFree(sm.soff);
+    if (sm.sent) cudaFree(sm.sent);
     sm.off = nullptr;
     sm.ent = nullptr;
+    sm.soff = nullptr;
+    sm.sent = nullptr;
     sm.nnz = 0;
 }
 
@@ -177,6 +234,37 @@ int sysmat_build(const Grid &g, const RaySet &rs, float gf, SysMat &sm, cudaStre
         sysmat_free(sm);
         return set_error(OMB_ERR_CUDA, std::string("system matrix build failed: ") + cudaGetErrorString(e));
     }
+    // the sliced copy: each slice as long as its longest list; kept only when it fits beside the lists
+    {
+        const int64_t n_sl = (n_img + 31) / 32;
+        std::vector<int64_t> hs((size_t)n_sl + 1);
+        hs[0] = 0;
+        for (int64_t s_ = 0; s_ < n_sl; ++s_) {
+            unsigned mx = 0;
+            for (int64_t v = s_ * 32; v < n_img && v < s_ * 32 + 32; ++v) mx = hc[v] > mx ? hc[v] : mx;
+            hs[s_ + 1] = hs[s_] + 32 * (int64_t)mx;
+        }
+        const int64_t tot = hs[n_sl];
+        if (cudaMalloc(reinterpret_cast<void **>(&sm.soff), (size_t)(n_sl + 1) * sizeof(int64_t)) == cudaSuccess &&
+            cudaMalloc(reinterpret_cast<void **>(&sm.sent), (size_t)(tot > 0 ? tot : 1) * sizeof(uint2)) ==
+                cudaSuccess) {
+            cudaMemcpyAsync(sm.soff, hs.data(), (size_t)(n_sl + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+            k_sm_slice<<<grid_for(n_img), kBlock, 0, st>>>(sm.off, sm.ent, sm.soff, sm.sent, n_img);
+            const cudaError_t e2 = cudaStreamSynchronize(st);
+            if (e2 != cudaSuccess) {
+                sysmat_free(sm);
+                return set_error(OMB_ERR_CUDA, std::string("system matrix slicing failed: ") + cudaGetErrorString(e2));
+            }
+            cudaFree(sm.ent);
+            sm.ent = nullptr;
+        } else {
+            // not enough memory for the copy: keep the lists
+            cudaGetLastError();
+            if (sm.soff) cudaFree(sm.soff);
+            sm.soff = nullptr;
+            sm.sent = nullptr;
+        }
+    }
     sm.nnz = nnz;
     sm.proj0 = rs.proj0;
     sm.m_size = rs.m_size;
@@ -194,14 +282,27 @@ int sysmat_backward(const Grid &g, const SysMat &sm, const Frames &fr, int64_t m
         const int nf = fr.n - f0 < fb ? fr.n - f0 : fb;
         const float *meas = fr.meas + f0 * fr.meas_stride;
         float *img = fr.img + f0 * fr.img_stride;
+        const bool sl = sm.sent != nullptr;
         if (fb == 8) {
             k_meas_to_raymajor<8><<<grid_for(m, 4), kBlock, 0, st>>>(meas, fr.meas_stride, nf, m, ym);
-            k_sm_bp<8><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.ent, ym, n_img, img, fr.img_stride, nf);
+            if (sl)
+                k_sm_bp_sl<8><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.soff, sm.sent, ym, n_img, img,
+                                                                     fr.img_stride, nf);
+            else
+                k_sm_bp<8><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.ent, ym, n_img, img, fr.img_stride, nf);
         } else if (fb == 4) {
             k_meas_to_raymajor<4><<<grid_for(m, 4), kBlock, 0, st>>>(meas, fr.meas_stride, nf, m, ym);
-            k_sm_bp<4><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.ent, ym, n_img, img, fr.img_stride, nf);
+            if (sl)
+                k_sm_bp_sl<4><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.soff, sm.sent, ym, n_img, img,
+                                                                     fr.img_stride, nf);
+            else
+                k_sm_bp<4><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.ent, ym, n_img, img, fr.img_stride, nf);
         } else {
-            k_sm_bp<1><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.ent, meas, n_img, img, fr.img_stride, 1);
+            if (sl)
+                k_sm_bp_sl<1><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.soff, sm.sent, meas, n_img, img,
+                                                                     fr.img_stride, 1);
+            else
+                k_sm_bp<1><<<grid_for(n_img, 8), kBlock, 0, st>>>(sm.off, sm.ent, meas, n_img, img, fr.img_stride, 1);
         }
         OMB_LAUNCH_CHECK("system matrix backprojection launch");
     }
