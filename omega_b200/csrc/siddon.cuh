@@ -292,21 +292,19 @@ __device__ __forceinline__ bool pre_loop_3d(const Grid &g, D3 s, D3 d, D3 diff, 
 template <int NB>
 __device__ __forceinline__ float tof_weights(const Tof &tof, float ddsign, float element, float D, float *w) {
     const float dX = element / 3.f;  // TRAPZ_BINS - 1
-    const float sdX = dX * ddsign;
+    // the trapezoid points in units of sigma: a_tr = (D - c) / sigma - tr * beta (the last one at the element's
+    // end), and the normalisation sigma_coef * dX applied once to the weighted sum of the four Gaussians
+    const float beta = dX * ddsign * tof.sigma_inv;
+    const float aend = element * ddsign * tof.sigma_inv;
+    const float scale = tof.sigma_coef * dX;
     float sum = 0.f;
 #pragma unroll
     for (int to = 0; to < NB; ++to) {
-        const float c = __ldg(tof.centers + to);
-        float a = (D - c) * tof.sigma_inv;
-        float out = tof.sigma_coef * __expf(-0.5f * a * a);
-#pragma unroll
-        for (int tr = 1; tr < 3; ++tr) {
-            a = (fmaf(-sdX, (float)tr, D) - c) * tof.sigma_inv;
-            out += tof.sigma_coef * __expf(-0.5f * a * a) * 2.f;
-        }
-        a = (fmaf(-element, ddsign, D) - c) * tof.sigma_inv;
-        out += tof.sigma_coef * __expf(-0.5f * a * a);
-        w[to] = out * dX;
+        const float a0 = (D - __ldg(tof.centers + to)) * tof.sigma_inv;
+        const float a1 = a0 - beta, a2 = fmaf(-2.f, beta, a0), a3 = a0 - aend;
+        const float e0 = __expf(a0 * (-0.5f * a0)), e1 = __expf(a1 * (-0.5f * a1));
+        const float e2 = __expf(a2 * (-0.5f * a2)), e3 = __expf(a3 * (-0.5f * a3));
+        w[to] = ((e0 + e3) + 2.f * (e1 + e2)) * scale;
         sum += w[to];
     }
     if (sum < tof.epps) sum = tof.epps;
