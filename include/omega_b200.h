@@ -440,6 +440,8 @@ typedef struct omb_recon_params {
     int32_t ad_flux;          /* OMB_PRIOR_AD: options.FluxType (1 exponential, 2 quadratic) */
     int32_t ad_diffusion;     /* OMB_PRIOR_AD: options.DiffusionType (1 gradient, 2 modified curvature); the
                                  normalisation switch is mrp_no_norm (options.med_no_norm) */
+    int32_t rdp_edge;         /* OMB_PRIOR_RDP: 1 neighbours outside the image clamped to the edge voxel (options.useImages,
+                                 the reference's default), 0 read as 0 (see omb_rdp_gradient_ex) */
 } omb_recon_params;
 
 /*
@@ -697,6 +699,17 @@ int omb_psf_convolve(const float *in, float *out, int32_t nx, int32_t ny, int32_
  */
 int omb_rdp_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float gamma, float epps,
                      float beta, void *stream);
+
+/*
+ * The same with the edge rule chosen: edge 0 reads neighbours outside the
+ * image as 0 (omb_rdp_gradient; the reference's buffer path and its
+ * util/priors.py RDP), 1 clamps them to the edge voxel (the reference's
+ * built-in reconstruction with options.useImages, its default: the prior
+ * reads the image through a clamp-to-edge texture, ProjectorClass.h:
+ * 6574-6576, samplerRDP auxKernels.cl:653).
+ */
+int omb_rdp_gradient_ex(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float gamma, float epps,
+                        float beta, int32_t edge, void *stream);
 
 /*
  * PET corrections of the projector type-1 forward and backward projections

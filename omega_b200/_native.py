@@ -157,6 +157,7 @@ class ReconParams(ctypes.Structure):
         ("ad_niter", ctypes.c_int32),
         ("ad_flux", ctypes.c_int32),
         ("ad_diffusion", ctypes.c_int32),
+        ("rdp_edge", ctypes.c_int32),
     ]
 
 
@@ -315,6 +316,9 @@ EXPORTS = [
     ("omb_rdp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                         ctypes.c_void_p]),
+    ("omb_rdp_gradient_ex", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                        ctypes.c_int32, ctypes.c_void_p]),
     ("omb_reconstruct", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ReconParams), ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_void_p]),
     ("omb_set_randoms", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),

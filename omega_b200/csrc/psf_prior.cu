@@ -48,6 +48,11 @@ __device__ __forceinline__ float rdp_term(float uj, float uk, float gamma, float
     return d * (gamma * fabsf(d) + uj + 3.f * uk + epps * epps) / (div * div + epps);
 }
 
+// CLAMP: a neighbour outside the image reads the edge voxel (the clamp-to-edge
+// texture of the reference's built-in path with useImages, ProjectorClass.h:
+// 6574-6576; samplerRDP auxKernels.cl:653), else 0 (its buffer path, and the
+// border-addressed texture of util/priors.py:143-146)
+template <bool CLAMP>
 __global__ void k_rdp_gradient(const float *__restrict__ u, float *__restrict__ grad, int nx, int ny, int nz,
                                float gamma, float epps, float beta) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -57,9 +62,10 @@ __global__ void k_rdp_gradient(const float *__restrict__ u, float *__restrict__ 
     const int64_t nxy = (int64_t)nx * ny;
     const int64_t n = x + (int64_t)y * nx + z * nxy;
     const float uj = __ldg(u + n);
-    const float xp = x < nx - 1 ? __ldg(u + n + 1) : 0.f, xm = x > 0 ? __ldg(u + n - 1) : 0.f;
-    const float yp = y < ny - 1 ? __ldg(u + n + nx) : 0.f, ym = y > 0 ? __ldg(u + n - nx) : 0.f;
-    const float zp = z < nz - 1 ? __ldg(u + n + nxy) : 0.f, zm = z > 0 ? __ldg(u + n - nxy) : 0.f;
+    const float e = CLAMP ? uj : 0.f;
+    const float xp = x < nx - 1 ? __ldg(u + n + 1) : e, xm = x > 0 ? __ldg(u + n - 1) : e;
+    const float yp = y < ny - 1 ? __ldg(u + n + nx) : e, ym = y > 0 ? __ldg(u + n - nx) : e;
+    const float zp = z < nz - 1 ? __ldg(u + n + nxy) : e, zm = z > 0 ? __ldg(u + n - nxy) : e;
     // the reference sums the +1 and -1 neighbours as the two halves of a float2
     float a = rdp_term(uj, xp, gamma, epps) + rdp_term(uj, yp, gamma, epps) + rdp_term(uj, zp, gamma, epps);
     float b = rdp_term(uj, xm, gamma, epps) + rdp_term(uj, ym, gamma, epps) + rdp_term(uj, zm, gamma, epps);
@@ -94,7 +100,21 @@ extern "C" int omb_rdp_gradient(const float *u, float *grad, int32_t nx, int32_t
     if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
     dim3 block(32, 8);
     dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
-    k_rdp_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, gamma, epps, beta);
+    k_rdp_gradient<false><<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, gamma, epps, beta);
+    OMB_LAUNCH_CHECK("RDP gradient launch");
+    return OMB_OK;
+}
+
+extern "C" int omb_rdp_gradient_ex(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, float gamma,
+                                   float epps, float beta, int32_t edge, void *stream) {
+    if (edge != 0 && edge != 1) return set_error(OMB_ERR_INVALID, "edge must be 0 (zero) or 1 (clamp)");
+    if (!u || !grad) return set_error(OMB_ERR_INVALID, "u/grad pointer is NULL");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    if (edge) k_rdp_gradient<true><<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, gamma, epps, beta);
+    else k_rdp_gradient<false><<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, gamma, epps, beta);
     OMB_LAUNCH_CHECK("RDP gradient launch");
     return OMB_OK;
 }

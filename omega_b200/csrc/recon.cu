@@ -249,7 +249,8 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             if (cudaMemsetAsync(du.p, 0, (size_t)n * sizeof(float), s) != cudaSuccess)
                 return set_error(OMB_ERR_CUDA, "clearing the prior gradient failed");
             if (p->prior == OMB_PRIOR_RDP)
-                return omb_rdp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, stream);
+                return omb_rdp_gradient_ex(x_out, du.f(), g.nx, g.ny, g.nz, p->rdp_gamma, epps, p->beta, p->rdp_edge,
+                                           stream);
             if (p->prior == OMB_PRIOR_WMEAN)
                 return omb_wmean_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1], p->prior_g[2],
                                           p->wmean_weights, p->wmean_wsum > 0.f ? p->wmean_wsum : 1.f, p->wmean_type, epps,

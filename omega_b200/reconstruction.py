@@ -465,6 +465,9 @@ def reconstructions_main(options):
     p = _native.ReconParams(struct_size=ctypes.sizeof(_native.ReconParams))
     p.algorithm = _PET_METHODS.get(method, _native.OMB_RECON_PDHG_TV)
     p.rdp_gamma = float(getattr(options, 'RDP_gamma', 1.0))
+    # RDP neighbours outside the image: clamped to the edge with options.useImages (the reference's default
+    # texture reads), 0 without
+    p.rdp_edge = 1 if getattr(options, 'useImages', True) else 0
     window = None
     lam = None
     mom = None

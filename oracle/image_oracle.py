@@ -5,8 +5,10 @@ steps around the projectors, for the parity tests:
   the window applied at every voxel with the image mirrored at its faces
   (edge voxel repeated: index -1 reads 0, N reads N-1);
 * rdp_gradient: RDPKernel (auxKernels.cl:664-872), 6-neighbour form,
-  neighbours outside the image 0 (the CUDA border addressing of the
-  reference's PyTorch/CuPy path, util/priors.py:178-181);
+  neighbours outside the image 0 (the border-addressed texture of the
+  reference's PyTorch/CuPy path, util/priors.py:143-146, and its buffer
+  path) or clamped to the edge (the texture of its built-in path with
+  useImages), both pinned to the kernel compiled on the host;
 * nlm_gradient: the non-local kernels NLM (auxKernels.cl:297-620) with the
   image read clamped to its edges (the texture sampler of the reference's
   kernel path), and, with cpu_mode, the reference CPU function NLMFunc
@@ -34,10 +36,13 @@ def psf_convolve(img, shape, window, g):
     return out.ravel(order='F')
 
 
-def rdp_gradient(u, shape, gamma, beta, epps=1e-8):
+def rdp_gradient(u, shape, gamma, beta, epps=1e-8, clamp=False):
+    """beta * dRDP(u)/du, 6 neighbours; outside the image 0, or (clamp) the
+    edge voxel, the clamp-to-edge texture of the reference's built-in path
+    (useImages)."""
     nx, ny, nz = shape
     a = np.asarray(u, dtype=np.float64).reshape((nx, ny, nz), order='F')
-    p = np.pad(a, 1, mode='constant')
+    p = np.pad(a, 1, mode='edge' if clamp else 'constant')
 
     def term(k):
         d = a - k

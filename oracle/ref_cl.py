@@ -62,6 +62,8 @@ def _lib(variant, precision):
             L.refcl_tv_gradient_ex.argtypes = [_I, _I, _I, _P, _D, _D, _D, _D, _P, _P]
         if hasattr(L, "refcl_proxtv"):
             L.refcl_proxtv.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D]
+        if hasattr(L, "refcl_rdp"):
+            L.refcl_rdp.argtypes = [_I, _I, _I, _P, _D, _D, _D, _P]
         if hasattr(L, "refcl_proxtgv"):
             L.refcl_proxtgv.argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _D, _D, _D, _D, _D]
         _libs[key] = L
@@ -315,3 +317,15 @@ def proxtgv_step(x, q, r, v, rhs, shape, sigma2, alpha0, alpha1, theta, tau, l2=
     _lib(lib, precision).refcl_proxtgv(nx, ny, nz, _dp(xx), _dp(qq), _dp(rr), _dp(vv), _dp(hh), _scalar(sigma2, e),
                                        _scalar(alpha0, e), _scalar(alpha1, e), _scalar(theta, e), _scalar(tau, e))
     return qq.reshape(3, -1), rr.reshape(6 if three_d else 3, -1), vv.reshape(3 if three_d else 2, -1), hh
+
+
+def rdp_gradient(u, shape, gamma, epps, beta, images=True, precision="d", exact_inputs=False):
+    """RDPKernel of the reference (-DRDP; images: the clamp-to-edge texture,
+    else the buffer): beta * dRDP(u), flat, x fastest."""
+    nx, ny, nz = shape
+    uu = np.ascontiguousarray(u, dtype=np.float64).ravel()
+    g = np.zeros(uu.size)
+    e = exact_inputs
+    _lib("aux_rdp" if images else "aux_rdp_buf", precision).refcl_rdp(
+        nx, ny, nz, _dp(uu), _scalar(gamma, e), _scalar(epps, e), _scalar(beta, e), _dp(g))
+    return g

@@ -312,7 +312,7 @@ REFCL_EXPORT int refcl_interp_ct_bp(int n_rows, int n_cols, double pitch_x, doub
 #endif
 
 #if defined(REFCL_AUX)
-#if !defined(ANATOMICAL1) && !defined(ANATOMICAL2) && !defined(ANATOMICAL3)
+#if !defined(ANATOMICAL1) && !defined(ANATOMICAL2) && !defined(ANATOMICAL3) && defined(USEIMAGES)
 /* TVKernel with texture reads (nearest point, unnormalized, clamp to edge):
  * grad += beta * dTV(u) with smoothing `epps` (the reference's TVsmoothing). */
 REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, double sigma, double epps, double beta,
@@ -326,6 +326,34 @@ REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, doub
             for (int i = 0; i < nx; ++i) {
                 set_item((unsigned)i, (unsigned)j, (unsigned)k);
                 TVKernel(g.data(), &tex, nx, ny, nz, nx, ny, nz, (omb_real)sigma, (omb_real)epps, (omb_real)beta);
+            }
+    from_real(g, grad);
+    return 0;
+}
+#endif
+
+#ifdef RDP
+/* RDPKernel (auxKernels.cl:650-875, the 6-neighbour form): grad += beta *
+ * dRDP(u); built with USEIMAGES the image is read through the shim's
+ * clamp-to-edge texture, without it from the buffer (0 outside). */
+REFCL_EXPORT int refcl_rdp(int nx, int ny, int nz, const double *u, double gamma, double epps, double beta,
+                           double *grad) {
+    const size_t N = (size_t)nx * ny * nz;
+    rvec uu = to_real(u, N), g = to_real(grad, N);
+#ifdef USEIMAGES
+    const omb_tex tex = make_tex(uu, nx, ny, nz, 0, 0, 0);
+#endif
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+#ifdef USEIMAGES
+                RDPKernel(g.data(), &tex, nx, ny, nz, nx, ny, nz, (omb_real)gamma, (omb_real)epps, (omb_real)beta);
+#else
+                RDPKernel(g.data(), uu.data(), nx, ny, nz, nx, ny, nz, (omb_real)gamma, (omb_real)epps,
+                          (omb_real)beta);
+#endif
             }
     from_real(g, grad);
     return 0;
@@ -434,6 +462,7 @@ REFCL_EXPORT int refcl_proxtgv(int nx, int ny, int nz, const double *im, double 
 }
 #endif
 
+#ifdef USEIMAGES
 /* TVKernel in the variant the build selected (-DSATV, -DTVW1,
  * -DANATOMICAL1/2/3): S is the reference image (or, ANATOMICAL1, the nine
  * tensor channels), C the anatomical weight (options.C, or eta for
@@ -472,6 +501,7 @@ REFCL_EXPORT int refcl_tv_gradient_ex(int nx, int ny, int nz, const double *u, d
     from_real(g, grad);
     return 0;
 }
+#endif
 
 /* PDHGUpdate without subsets: u -= tau * rhs (clamped at epps when
  * positivity is enforced), im = u + theta (u - u_prev). */

@@ -390,7 +390,7 @@ def test_builtin_osl_osem_rdp_matches_oracle(cuda):
     ys = [np.asarray(o.subsetMeasurements(m, s), dtype=np.float64) for s in range(g.n_subsets)]
     shape = (g.nx, g.ny, g.nz)
     ref = orc.osem(g, ys, np.ones(g.n_img), 2,
-                   prior_grad=lambda x: io.rdp_gradient(x, shape, 2.0, 0.002, g.epps))
+                   prior_grad=lambda x: io.rdp_gradient(x, shape, 2.0, 0.002, g.epps, clamp=True))
     plain = orc.osem(g, ys, np.ones(g.n_img), 2)
     x = out.ravel(order='F')
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)

@@ -121,6 +121,12 @@ def test_psf_and_rdp_kernels_match_restatements(cuda):
     u[::17] = 0.0
     grad = priors.RDP(_t(u, cuda), *shape, gamma=2.0, beta=0.3).cpu().numpy()
     assert orc.rel_l2(grad, io.rdp_gradient(u, shape, 2.0, 0.3)) < 1e-5
+    # the built-in loop's edge rule: neighbours outside the image clamped to the edge voxel
+    U2 = _t(u, cuda)
+    g2 = torch.zeros_like(U2)
+    _native.call("omb_rdp_gradient_ex", ctypes.c_void_p(U2.data_ptr()), ctypes.c_void_p(g2.data_ptr()), *shape, 2.0,
+                 1e-8, 0.3, 1, st)
+    assert orc.rel_l2(g2.cpu().numpy(), io.rdp_gradient(u, shape, 2.0, 0.3, clamp=True)) < 1e-5
     with pytest.raises(_native.NativeError):
         _native.call("omb_psf_convolve", ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(U.data_ptr()), *shape,
                      ctypes.c_void_p(W.data_ptr()), *g, st)

@@ -340,3 +340,20 @@ def test_pdhg_tgv_iteration_pinned():
                                            exact_inputs=True)
         x, u = ref_cl.pdhg_update(x, rhs, u, shape, tau, 1.0, 1e-5, exact_inputs=True)
     assert orc.rel_l2(ours, x) < PIN
+
+
+
+@pytest.mark.parametrize("images", [True, False])
+def test_rdp_pinned(images):
+    """image_oracle.rdp_gradient against RDPKernel compiled with -DRDP: the
+    clamp-to-edge texture (USEIMAGES, the reference's built-in default) and
+    the buffer path (0 outside), exactly; the two edge rules differ."""
+    from oracle import image_oracle as io
+    shape = (11, 9, 7)
+    rng = np.random.default_rng(71)
+    u = rng.uniform(0.0, 2.0, int(np.prod(shape)))
+    u[::13] = 0.0
+    theirs = ref_cl.rdp_gradient(u, shape, 2.0, 1e-8, 0.3, images=images, exact_inputs=True)
+    ours = io.rdp_gradient(u, shape, 2.0, 0.3, 1e-8, clamp=images)
+    assert np.abs(ours - theirs).max() <= 1e-14 * np.abs(theirs).max()
+    assert orc.rel_l2(io.rdp_gradient(u, shape, 2.0, 0.3, 1e-8, clamp=not images), theirs) > 1e-2

@@ -166,14 +166,18 @@ def test_builtin_ramla_matches_oracle(cuda, name, graph):
 
 
 @pytest.mark.gpu
-def test_builtin_bsrem_rdp_matches_oracle(cuda):
+@pytest.mark.parametrize("images", [True, False])
+def test_builtin_bsrem_rdp_matches_oracle(cuda, images):
+    """BSREM with RDP; with options.useImages (the default) the prior's
+    neighbours outside the image are the edge voxel, without it 0, as the
+    reference's texture and buffer paths read them."""
     o, g = _pet("pet_mini", 23)
     lam = [0.2, 0.12, 0.08]
-    x = _run_builtin(o, "BSREM", 3, lam=lam, RDP=True, RDP_gamma=2.0, beta=0.05)
+    x = _run_builtin(o, "BSREM", 3, lam=lam, RDP=True, RDP_gamma=2.0, beta=0.05, useImages=images)
     shape = (g.nx, g.ny, g.nz)
     ys = _subset_measurements(o, g)
     ref = orc.relaxed(g, ys, np.ones(g.n_img), 3, "BSREM", lam=np.float32(lam),
-                      prior_grad=lambda v: io.rdp_gradient(v, shape, 2.0, 0.05, g.epps))
+                      prior_grad=lambda v: io.rdp_gradient(v, shape, 2.0, 0.05, g.epps, clamp=images))
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
     plain = orc.relaxed(g, ys, np.ones(g.n_img), 3, "RAMLA", lam=np.float32(lam))
     assert orc.rel_l2(ref, plain) > 1e-3  # the prior changes the result
@@ -222,7 +226,8 @@ def test_custom_loop_entries_match_builtin(cuda):
             _native.call("omb_ramla_subset", o._handle, s, _ptr(x), _ptr(ys[s]), float(lam[it]), 1, _ptr(wm),
                          _ptr(wi), st)
         du.zero_()
-        _native.call("omb_rdp_gradient", _ptr(x), _ptr(du), g.nx, g.ny, g.nz, 2.0, float(g.epps), 0.05, st)
+        # the built-in loop clamps the prior's neighbours to the edge (options.useImages, the default)
+        _native.call("omb_rdp_gradient_ex", _ptr(x), _ptr(du), g.nx, g.ny, g.nz, 2.0, float(g.epps), 0.05, 1, st)
         _native.call("omb_map_step", _ptr(x), _ptr(du), ctypes.c_int64(g.n_img), float(lam[it]), float(g.epps), st)
     assert orc.rel_l2(x.cpu().numpy(), built) < 1e-6
     # ROSEM sub-iterations by hand against the built-in ROSEM
@@ -306,7 +311,7 @@ def test_builtin_pkma_with_rdp_matches_oracle(cuda):
     shape = (g.nx, g.ny, g.nz)
     ys = _subset_measurements(o, g)
     ref = orc.relaxed(g, ys, np.ones(g.n_img), 3, "PKMA", lam=np.float32(lam),
-                      prior_grad=lambda v: io.rdp_gradient(v, shape, 2.0, 0.05, g.epps))
+                      prior_grad=lambda v: io.rdp_gradient(v, shape, 2.0, 0.05, g.epps, clamp=True))
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
     assert orc.rel_l2(ref, orc.relaxed(g, ys, np.ones(g.n_img), 3, "PKMA", lam=np.float32(lam))) > 1e-4
 
@@ -398,7 +403,7 @@ def test_builtin_preconditioned_matches_oracle(cuda, method, mode):
     extra = {"RDP": True, "RDP_gamma": 2.0, "beta": 0.05} if method == "MBSREM" else {}
     x = _run_builtin(o, method, 3, lam=lam, **extra)
     shape = (g.nx, g.ny, g.nz)
-    grad = (lambda v: io.rdp_gradient(v, shape, 2.0, 0.05, g.epps)) if method == "MBSREM" else None
+    grad = (lambda v: io.rdp_gradient(v, shape, 2.0, 0.05, g.epps, clamp=True)) if method == "MBSREM" else None
     ys = _subset_measurements(o, g)
     ref = orc.relaxed(g, ys, np.ones(g.n_img), 3, method, lam=np.float32(lam), prior_grad=grad, precond=mode)
     assert orc.rel_l2(x, ref) < 5e-5, orc.rel_l2(x, ref)
