@@ -292,18 +292,20 @@ __device__ __forceinline__ bool pre_loop_3d(const Grid &g, D3 s, D3 d, D3 diff, 
 template <int NB>
 __device__ __forceinline__ float tof_weights(const Tof &tof, float ddsign, float element, float D, float *w) {
     const float dX = element / 3.f;  // TRAPZ_BINS - 1
-    // the trapezoid points in units of sigma: a_tr = (D - c) / sigma - tr * beta (the last one at the element's
-    // end), and the normalisation sigma_coef * dX applied once to the weighted sum of the four Gaussians
-    const float beta = dX * ddsign * tof.sigma_inv;
-    const float aend = element * ddsign * tof.sigma_inv;
+    // the trapezoid points in units of sigma sqrt(2): a_tr = (D - c) / (sigma sqrt 2) - tr * beta (the last one
+    // at the element's end), each Gaussian exp(-a^2); the normalisation sigma_coef * dX applied once to the
+    // weighted sum of the four
+    const float si = tof.sigma_inv * 0.70710678f;
+    const float beta = dX * ddsign * si;
+    const float aend = element * ddsign * si;
     const float scale = tof.sigma_coef * dX;
     float sum = 0.f;
 #pragma unroll
     for (int to = 0; to < NB; ++to) {
-        const float a0 = (D - __ldg(tof.centers + to)) * tof.sigma_inv;
+        const float a0 = (D - __ldg(tof.centers + to)) * si;
         const float a1 = a0 - beta, a2 = fmaf(-2.f, beta, a0), a3 = a0 - aend;
-        const float e0 = __expf(a0 * (-0.5f * a0)), e1 = __expf(a1 * (-0.5f * a1));
-        const float e2 = __expf(a2 * (-0.5f * a2)), e3 = __expf(a3 * (-0.5f * a3));
+        const float e0 = __expf(-(a0 * a0)), e1 = __expf(-(a1 * a1));
+        const float e2 = __expf(-(a2 * a2)), e3 = __expf(-(a3 * a3));
         w[to] = ((e0 + e3) + 2.f * (e1 + e2)) * scale;
         sum += w[to];
     }
