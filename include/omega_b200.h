@@ -276,8 +276,11 @@ typedef struct omb_tuning {
                                         per-projection detector boxes staged in shared memory by TMA
                                         (applies with bdd_bp_zrun = 8 or 16; needs a row count that is a
                                         multiple of 4) */
-    int32_t siddon_bp_matrix;        /* 0, 1 (default 0): type-1 non-TOF backprojections of measurements
-                                        through a transposed system matrix kept on the handle (per subset:
+    int32_t siddon_bp_matrix;        /* 0, 1 (default 0): type-1, 2 and 3 non-TOF backprojections of
+                                        measurements through a transposed system matrix kept on the handle
+                                        (the Siddon or tube weights; types 2 / 3 also project forward
+                                        through a ray-major copy when fp_type == bp_type, and fall back to
+                                        the tracers when it does not fit in memory) (per subset:
                                         for every voxel the weights of the rays crossing it, 8 bytes a
                                         crossing), built by the first such call on a subset (that call
                                         synchronises its stream and must not be captured into a CUDA

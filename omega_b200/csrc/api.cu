@@ -327,6 +327,8 @@ static Frames one_frame_bp(const omb_handle *h, const float *y, float *img, int6
 
 // Ray-driven forward projection of a batch of frames (types 1 and 4).  With
 // BF16 reads the images are first rounded into the handle's BF16 copies.
+static int find_matrix(omb_handle *h, const RaySet &rs, const Orth *orth, cudaStream_t s, SysMat **out);
+
 static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cudaStream_t s) {
     Frames f = f_in;
     if (h->read_mode == OMB_READ_BF16 && f.n > 0) {
@@ -338,6 +340,14 @@ static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cud
         }
         f.img_in16 = h->d_img16;
         f.img_stride = h->n_img;
+    }
+    if ((h->desc.fp_type == 2 || h->desc.fp_type == 3) && h->desc.bp_type == h->desc.fp_type &&
+        h->tune.siddon_bp_matrix && h->tof.nbins == 1 && !f.img_in16 && f.img_in && f.meas_out) {
+        // the tube weights of the subset's system matrix (ray-major copy), built by its first call
+        SysMat *sm = nullptr;
+        const int fm = find_matrix(h, rs, &h->orth_bp, s, &sm);
+        if (fm < 0) return fm;
+        if (fm == OMB_OK && sm->rsent) return sysmat_forward(h->grid, *sm, f, rs.m_size, s);
     }
     if (h->desc.fp_type == 2 || h->desc.fp_type == 3) {
         if (f.img_in16) return set_error(OMB_ERR_UNSUPPORTED, "projector types 2 / 3 read FP32 images");
@@ -376,8 +386,57 @@ static int rays_forward(omb_handle *h, const RaySet &rs, const Frames &f_in, cud
 // frames into zeroed images; `sens` (zeroed) receives A^T 1 of the first
 // frame's rays.  f.meas == NULL backprojects ones, f.img == NULL keeps only
 // the sensitivity.
+// Backprojection of f's frames through the subset's transposed system matrix (types 1-3, non-TOF), built
+// by its first call; a build that does not fit in memory turns the matrix off for this handle and returns 1
+// (the caller takes the ray-driven path).
+static int find_matrix(omb_handle *h, const RaySet &rs, const Orth *orth, cudaStream_t s, SysMat **out) {
+    *out = nullptr;
+    for (auto &x : h->sysmats)
+        if (x.proj0 == rs.proj0 && x.m_size == rs.m_size && x.cur_subset == rs.cur_subset) *out = &x;
+    if (!*out) {
+        SysMat nm;
+        if (sysmat_build(h->grid, rs, h->desc.global_factor, nm, s, orth) != OMB_OK) {
+            if (orth && std::string(omb_last_error()).find("not enough device memory") != std::string::npos) {
+                h->tune.siddon_bp_matrix = 0;
+                return 1;
+            }
+            return -1;
+        }
+        h->sysmats.push_back(nm);
+        *out = &h->sysmats.back();
+    }
+    return OMB_OK;
+}
+
+static int matrix_backward(omb_handle *h, const RaySet &rs, const Frames &f, const Orth *orth, cudaStream_t s) {
+    SysMat *sm = nullptr;
+    const int fm = find_matrix(h, rs, orth, s, &sm);
+    if (fm != OMB_OK) return fm;
+    const int fb = f.n >= 8 ? 8 : (f.n >= 4 ? 4 : 1);
+    if (fb > 1 && (int64_t)fb * rs.m_size > h->ym_floats) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+            return set_error(OMB_ERR_INVALID, "the system-matrix backprojection scratch grows on a call outside "
+                                              "CUDA-graph capture (run one call first)");
+        float *p = nullptr;
+        if (cudaMalloc(&p, (size_t)fb * rs.m_size * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(OMB_ERR_CUDA, "allocating the system-matrix backprojection scratch failed");
+        }
+        if (h->d_ym) h->retired.push_back(h->d_ym);
+        h->d_ym = p;
+        h->ym_floats = (int64_t)fb * rs.m_size;
+    }
+    return sysmat_backward(h->grid, *sm, f, rs.m_size, h->d_ym, h->ym_floats, s);
+}
+
 static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, float *sens, cudaStream_t s) {
     Frames f = f_in;
+    if ((h->desc.bp_type == 2 || h->desc.bp_type == 3) && h->tune.siddon_bp_matrix && h->tof.nbins == 1 && !sens &&
+        f.meas && f.img) {
+        const int e = matrix_backward(h, rs, f, &h->orth_bp, s);
+        if (e != 1) return e;
+    }
     if (h->desc.bp_type == 2 || h->desc.bp_type == 3) {
         for (int fr = 0; fr < f.n; ++fr) {
             const int st = orth_backward(h->grid, rs, h->orth_bp, h->tof, h->desc.global_factor,
@@ -410,31 +469,7 @@ static int rays_backward(omb_handle *h, const RaySet &rs, const Frames &f_in, fl
     }
     if (h->tune.siddon_bp_matrix && h->tof.nbins == 1 && !sens && f.meas && f.img) {
         // the subset's transposed system matrix, built by its first call
-        SysMat *sm = nullptr;
-        for (auto &x : h->sysmats)
-            if (x.proj0 == rs.proj0 && x.m_size == rs.m_size && x.cur_subset == rs.cur_subset) sm = &x;
-        if (!sm) {
-            SysMat nm;
-            if (sysmat_build(h->grid, rs, h->desc.global_factor, nm, s) != OMB_OK) return -1;
-            h->sysmats.push_back(nm);
-            sm = &h->sysmats.back();
-        }
-        const int fb = f.n >= 8 ? 8 : (f.n >= 4 ? 4 : 1);
-        if (fb > 1 && (int64_t)fb * rs.m_size > h->ym_floats) {
-            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-            if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
-                return set_error(OMB_ERR_INVALID, "the system-matrix backprojection scratch grows on a call outside "
-                                                  "CUDA-graph capture (run one call first)");
-            float *p = nullptr;
-            if (cudaMalloc(&p, (size_t)fb * rs.m_size * sizeof(float)) != cudaSuccess) {
-                cudaGetLastError();
-                return set_error(OMB_ERR_CUDA, "allocating the system-matrix backprojection scratch failed");
-            }
-            if (h->d_ym) h->retired.push_back(h->d_ym);
-            h->d_ym = p;
-            h->ym_floats = (int64_t)fb * rs.m_size;
-        }
-        return sysmat_backward(h->grid, *sm, f, rs.m_size, h->d_ym, h->ym_floats, s);
+        return matrix_backward(h, rs, f, nullptr, s);
     }
     if (!sens && f.meas && f.img) attach_interleave(h, f, s);
     return siddon_backward(h->grid, rs, h->tof, h->desc.global_factor, f, sens, h->tune, s);
@@ -1070,6 +1105,9 @@ int omb_set_corrections(omb_handle *h, const float *meas_weights, int64_t n_weig
             h->retired.push_back(m.ent);
             h->retired.push_back(m.soff);
             h->retired.push_back(m.sent);
+            h->retired.push_back(m.rsoff);
+            h->retired.push_back(m.rsent);
+            h->retired.push_back(m.rcnt);
         }
         h->sysmats.clear();
     }
@@ -1268,6 +1306,21 @@ int omb_autotune(omb_handle *h, int32_t n_frames, int32_t repeats, omb_tuning *o
             }
         } else {
             cudaGetLastError();
+        }
+    }
+    // types 2 / 3 (non-TOF): the tube weights through the transposed system matrix when it fits and is faster
+    // (a build that does not fit turns the matrix off again)
+    if (e == cudaSuccess && st == OMB_OK && (h->desc.bp_type == 2 || h->desc.bp_type == 3) && h->desc.tof_bins == 1) {
+        h->tune = best;
+        h->tune.siddon_bp_matrix = 0;
+        const float b0 = timed(bwd);
+        h->tune.siddon_bp_matrix = 1;
+        const float b1 = timed(bwd);
+        if (b0 < 0.f || b1 < 0.f) st = -1;
+        else best.siddon_bp_matrix = h->tune.siddon_bp_matrix && b1 < b0 ? 1 : 0;
+        if (!best.siddon_bp_matrix) {
+            for (auto &x : h->sysmats) sysmat_free(x);
+            h->sysmats.clear();
         }
     }
     if (e == cudaSuccess && st == OMB_OK && h->desc.fp_type == 5) {

@@ -126,6 +126,12 @@ int orth_forward(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof,
                  cudaStream_t st);
 int orth_backward(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof, float gf, const float *y, float *img,
                   float *sens, cudaStream_t st);
+// The tube tracer's count and fill passes of the transposed system matrix (non-TOF; sysmat_build).
+// rcnt: each ray's entry count; rsoff / rsent (or NULL): the ray-major copy in slices of 32 rays.
+int orth_sm_count(const Grid &g, const RaySet &rs, const Orth &o, float gf, unsigned *cnt, unsigned *rcnt,
+                  cudaStream_t st);
+int orth_sm_fill(const Grid &g, const RaySet &rs, const Orth &o, float gf, unsigned long long *cursor, uint2 *ent,
+                 const int64_t *rsoff, uint2 *rsent, cudaStream_t st);
 
 // Multi-ray PET projections (rs.nr_xy x rs.nr_z rays per LOR), one frame.
 int multiray_forward(const Grid &g, const RaySet &rs, const Tof &tof, float gf, const float *img, float *y,
@@ -169,15 +175,23 @@ struct SysMat {
     // soff[slice] + 32 k + l; the voxel-major lists are released once it is built
     int64_t *soff = nullptr;
     uint2 *sent = nullptr;
+    // tube weights only: the ray-major copy for the forward projection (slices of 32 rays, entry k of ray l
+    // at rsoff[slice] + 32 k + l, (voxel, weight bits)) and each ray's entry count; NULL when it did not fit
+    int64_t *rsoff = nullptr;
+    uint2 *rsent = nullptr;
+    unsigned *rcnt = nullptr;
 };
-// Builds sm for the rays of rs (the walk and weights of the ray-driven backprojection); synchronises `st`
-// and refuses to run while `st` is captured into a CUDA graph.
-int sysmat_build(const Grid &g, const RaySet &rs, float gf, SysMat &sm, cudaStream_t st);
+// Builds sm for the rays of rs (the walk and weights of the ray-driven backprojection: the Siddon tracer, or
+// with `orth` the non-TOF tube tracer of projector types 2 / 3); synchronises `st` and refuses to run while
+// `st` is captured into a CUDA graph.
+int sysmat_build(const Grid &g, const RaySet &rs, float gf, SysMat &sm, cudaStream_t st, const Orth *orth = nullptr);
 void sysmat_free(SysMat &sm);
 // Backprojection of fr.n frames through sm (images overwritten); ym: ray-major scratch of at least
 // 8 * m floats (4 * m for 4..7 frames; unused for fewer).
 int sysmat_backward(const Grid &g, const SysMat &sm, const Frames &fr, int64_t m, float *ym, int64_t ym_floats,
                     cudaStream_t st);
+// Forward projection of fr.n frames through sm's ray-major copy (types 2 / 3; sm.rsent != NULL).
+int sysmat_forward(const Grid &g, const SysMat &sm, const Frames &fr, int64_t m, cudaStream_t st);
 
 // Detector-row filtering (filter.cu): out = the circular convolution (length nf) of each column of nr rows with
 // h; the measurement residual fp -= y; the dual step out = (p + sigma r) / denom (denom 1: no division).

@@ -473,6 +473,58 @@ __global__ void __launch_bounds__(kBlockO, 6) k_orth_bp(Grid g, RaySet rs, Orth 
     });
 }
 
+// The non-TOF tube weights of each ray (the backprojection's ele x scale) for the transposed system matrix:
+// the count of every voxel's entries, then the atomic fill (sysmat.cu sorts and slices the lists).
+__device__ __forceinline__ float orth_ray_scale(const Orth &o, const RaySet &rs, const Grid &g, const Ray &ray,
+                                                int64_t r, float gf) {
+    const float corr = (rs.w || rs.mu) ? ray_correction(g, rs, ray, r) : 1.f;
+    const double fx = (double)ray.d.x - ray.s.x, fy = (double)ray.d.y - ray.s.y, fz = (double)ray.d.z - ray.s.z;
+    const double L = sqrt(fx * fx + fy * fy + fz * fz);
+    const double r2 = (double)o.width * (double)o.width;
+    return (o.type == 3 ? (float)(1.0 / (L * (1.0 / 3.14159265358979323846) * r2)) : 1.f) * gf * corr;
+}
+
+__global__ void __launch_bounds__(kBlockO, 6) k_orth_sm_count(Grid g, RaySet rs, Orth o, float gf,
+                                                              unsigned *__restrict__ cnt, unsigned *__restrict__ rcnt) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rs.m_size) return;
+    const Ray ray = load_ray(rs, r);
+    const float scale = orth_ray_scale(o, rs, g, ray, r, gf);
+    const Tof tof{1, 0.f, 0.f, 0.f, nullptr};
+    float temp;
+    unsigned k = 0;
+    orth_trace<1>(g, o, ray, gf, tof, temp, [&](int64_t ind, float ele, const float *, float) {
+        const float le = ele * scale;
+        if (isnan(le) || le == 0.f) return;
+        atomicAdd(cnt + ind, 1u);
+        ++k;
+    });
+    rcnt[r] = k;
+}
+
+// rsent (or NULL): the ray-major copy in slices of 32 rays, entry k of ray l of slice s at rsoff[s] + 32 k + l
+__global__ void __launch_bounds__(kBlockO, 6) k_orth_sm_fill(Grid g, RaySet rs, Orth o, float gf,
+                                                             unsigned long long *__restrict__ cursor,
+                                                             uint2 *__restrict__ ent, const int64_t *__restrict__ rsoff,
+                                                             uint2 *__restrict__ rsent) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rs.m_size) return;
+    const Ray ray = load_ray(rs, r);
+    const float scale = orth_ray_scale(o, rs, g, ray, r, gf);
+    const Tof tof{1, 0.f, 0.f, 0.f, nullptr};
+    float temp;
+    uint2 *rd = rsent ? rsent + rsoff[r >> 5] + (r & 31) : nullptr;
+    int64_t k = 0;
+    orth_trace<1>(g, o, ray, gf, tof, temp, [&](int64_t ind, float ele, const float *, float) {
+        const float le = ele * scale;
+        if (isnan(le) || le == 0.f) return;
+        const unsigned long long pos = atomicAdd(cursor + ind, 1ull);
+        ent[pos] = make_uint2((unsigned)r, __float_as_uint(le));
+        if (rd) rd[32 * k] = make_uint2((unsigned)ind, __float_as_uint(le));
+        ++k;
+    });
+}
+
 template <int NB>
 int launch_fp(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof, float gf, const float *img, float *y,
               cudaStream_t st) {
@@ -506,6 +558,23 @@ int orth_forward(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof,
 #undef OMB_CASE
         default: return set_error(OMB_ERR_UNSUPPORTED, "TOF bin count above 16 is not built");
     }
+}
+
+int orth_sm_count(const Grid &g, const RaySet &rs, const Orth &o, float gf, unsigned *cnt, unsigned *rcnt,
+                  cudaStream_t st) {
+    if (rs.m_size <= 0) return OMB_OK;
+    k_orth_sm_count<<<(unsigned)((rs.m_size + kBlockO - 1) / kBlockO), kBlockO, 0, st>>>(g, rs, o, gf, cnt, rcnt);
+    OMB_LAUNCH_CHECK("tube system matrix count launch");
+    return OMB_OK;
+}
+
+int orth_sm_fill(const Grid &g, const RaySet &rs, const Orth &o, float gf, unsigned long long *cursor, uint2 *ent,
+                 const int64_t *rsoff, uint2 *rsent, cudaStream_t st) {
+    if (rs.m_size <= 0) return OMB_OK;
+    k_orth_sm_fill<<<(unsigned)((rs.m_size + kBlockO - 1) / kBlockO), kBlockO, 0, st>>>(g, rs, o, gf, cursor, ent,
+                                                                                        rsoff, rsent);
+    OMB_LAUNCH_CHECK("tube system matrix fill launch");
+    return OMB_OK;
 }
 
 int orth_backward(const Grid &g, const RaySet &rs, const Orth &o, const Tof &tof, float gf, const float *y, float *img,

@@ -14,7 +14,8 @@
 // sums taken in one fixed order (bit-identical call to call).  Frames are
 // gathered 8 (or 4) at a time from a ray-major copy of the measurements
 // (32 bytes a ray), so a crossing costs one 8-byte matrix read and one
-// 32-byte gather for 8 frames.
+// 32-byte gather for 8 frames.  Projector types 2 / 3 (non-TOF) build the
+// same structure from the tube tracer's weights.
 //
 // After the build the lists are re-laid in slices of 32 consecutive voxels
 // (one warp's voxels): entry k of every voxel of a slice side by side, so a
@@ -181,21 +182,57 @@ __global__ void __launch_bounds__(kBlock) k_sm_bp_sl(const int64_t *__restrict__
     }
 }
 
+// Forward projection through the ray-major slices: one thread per ray, y[r] = sum of w x[voxel] in the
+// tracer's order (the grid-stride loop keeps a warp on the 32 rays of one slice)
+__global__ void __launch_bounds__(kBlock) k_sm_fp_sl(const unsigned *__restrict__ rcnt,
+                                                     const int64_t *__restrict__ rsoff, const uint2 *__restrict__ rsent,
+                                                     const float *__restrict__ x, int64_t m, float *__restrict__ y) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += stride) {
+        const unsigned n = __ldg(rcnt + r);
+        const uint2 *e0 = rsent + __ldg(rsoff + (r >> 5)) + (r & 31);
+        float acc = 0.f;
+#pragma unroll 4
+        for (unsigned k = 0; k < n; ++k) {
+            const uint2 e = __ldg(e0 + (int64_t)k * 32);
+            acc = fmaf(__uint_as_float(e.y), __ldg(x + e.x), acc);
+        }
+        y[r] = acc;
+    }
+}
+
 }  // namespace
+
+int sysmat_forward(const Grid &g, const SysMat &sm, const Frames &fr, int64_t m, cudaStream_t st) {
+    (void)g;
+    if (!sm.rsent || !sm.rcnt) return set_error(OMB_ERR_INVALID, "system matrix has no forward copy");
+    for (int f = 0; f < fr.n; ++f) {
+        k_sm_fp_sl<<<grid_for(m, 8), kBlock, 0, st>>>(sm.rcnt, sm.rsoff, sm.rsent, fr.img_in + f * fr.img_stride, m,
+                                                      fr.meas_out + f * fr.meas_stride);
+        OMB_LAUNCH_CHECK("system matrix forward projection launch");
+    }
+    return OMB_OK;
+}
 
 void sysmat_free(SysMat &sm) {
     if (sm.off) cudaFree(sm.off);
     if (sm.ent) cudaFree(sm.ent);
     if (sm.soff) cudaFree(sm.soff);
     if (sm.sent) cudaFree(sm.sent);
+    if (sm.rsoff) cudaFree(sm.rsoff);
+    if (sm.rsent) cudaFree(sm.rsent);
+    if (sm.rcnt) cudaFree(sm.rcnt);
     sm.off = nullptr;
     sm.ent = nullptr;
     sm.soff = nullptr;
     sm.sent = nullptr;
+    sm.rsoff = nullptr;
+    sm.rsent = nullptr;
+    sm.rcnt = nullptr;
     sm.nnz = 0;
 }
 
-int sysmat_build(const Grid &g, const RaySet &rs, float gf, SysMat &sm, cudaStream_t st) {
+int sysmat_build(const Grid &g, const RaySet &rs, float gf, SysMat &sm, cudaStream_t st, const Orth *orth) {
     sysmat_free(sm);
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
@@ -206,27 +243,82 @@ int sysmat_build(const Grid &g, const RaySet &rs, float gf, SysMat &sm, cudaStre
     unsigned *cnt = nullptr;
     OMB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&cnt), (size_t)n_img * sizeof(unsigned), st));
     cudaMemsetAsync(cnt, 0, (size_t)n_img * sizeof(unsigned), st);
-    k_sm_count<<<grid_for(rs.m_size), kBlock, 0, st>>>(g, rs, gf, cnt);
+    unsigned *rcnt = nullptr;
+    if (orth) {
+        if (cudaMalloc(reinterpret_cast<void **>(&rcnt), (size_t)(rs.m_size > 0 ? rs.m_size : 1) * sizeof(unsigned)) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeAsync(cnt, st);
+            return set_error(OMB_ERR_CUDA, "not enough device memory for the system matrix (ray counts)");
+        }
+        sm.rcnt = rcnt;
+        const int ec = orth_sm_count(g, rs, *orth, gf, cnt, rcnt, st);
+        if (ec != OMB_OK) {
+            cudaFreeAsync(cnt, st);
+            sysmat_free(sm);
+            return ec;
+        }
+    } else {
+        k_sm_count<<<grid_for(rs.m_size), kBlock, 0, st>>>(g, rs, gf, cnt);
+    }
     std::vector<unsigned> hc((size_t)n_img);
     cudaMemcpyAsync(hc.data(), cnt, (size_t)n_img * sizeof(unsigned), cudaMemcpyDeviceToHost, st);
     cudaFreeAsync(cnt, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return set_error(OMB_ERR_CUDA, "system matrix count pass failed");
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        sysmat_free(sm);
+        return set_error(OMB_ERR_CUDA, "system matrix count pass failed");
+    }
     std::vector<int64_t> ho((size_t)n_img + 1);
     ho[0] = 0;
     for (int64_t v = 0; v < n_img; ++v) ho[v + 1] = ho[v] + hc[v];
     const int64_t nnz = ho[n_img];
+    std::vector<int64_t> hrs;
+    if (orth) {
+        // the ray-major copy's slice offsets (32 rays a slice, each slice as long as its longest ray)
+        std::vector<unsigned> hr((size_t)rs.m_size);
+        if (cudaMemcpy(hr.data(), rcnt, (size_t)rs.m_size * sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            sysmat_free(sm);
+            return set_error(OMB_ERR_CUDA, "system matrix ray counts could not be read");
+        }
+        const int64_t n_sl = (rs.m_size + 31) / 32;
+        hrs.assign((size_t)n_sl + 1, 0);
+        for (int64_t s_ = 0; s_ < n_sl; ++s_) {
+            unsigned mx = 0;
+            for (int64_t r = s_ * 32; r < rs.m_size && r < s_ * 32 + 32; ++r) mx = hr[r] > mx ? hr[r] : mx;
+            hrs[s_ + 1] = hrs[s_] + 32 * (int64_t)mx;
+        }
+        if (cudaMalloc(reinterpret_cast<void **>(&sm.rsoff), (size_t)(n_sl + 1) * sizeof(int64_t)) != cudaSuccess ||
+            cudaMalloc(reinterpret_cast<void **>(&sm.rsent), (size_t)(hrs[n_sl] > 0 ? hrs[n_sl] : 1) * sizeof(uint2)) !=
+                cudaSuccess) {
+            // no room for the forward copy: the forward projection keeps the tracer
+            cudaGetLastError();
+            if (sm.rsoff) cudaFree(sm.rsoff);
+            sm.rsoff = nullptr;
+            sm.rsent = nullptr;
+        } else {
+            cudaMemcpy(sm.rsoff, hrs.data(), (size_t)(n_sl + 1) * sizeof(int64_t), cudaMemcpyHostToDevice);
+        }
+    }
     if (cudaMalloc(reinterpret_cast<void **>(&sm.off), (size_t)(n_img + 1) * sizeof(int64_t)) != cudaSuccess ||
         cudaMalloc(reinterpret_cast<void **>(&sm.ent), (size_t)(nnz > 0 ? nnz : 1) * sizeof(uint2)) != cudaSuccess) {
         cudaGetLastError();
         sysmat_free(sm);
-        return set_error(OMB_ERR_CUDA, "not enough device memory for the type-1 system matrix (" +
+        return set_error(OMB_ERR_CUDA, "not enough device memory for the system matrix (" +
                                            std::to_string((double)nnz * 8.0 / 1e9) + " GB)");
     }
     cudaMemcpyAsync(sm.off, ho.data(), (size_t)(n_img + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st);
     unsigned long long *cursor = nullptr;
     OMB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&cursor), (size_t)n_img * sizeof(int64_t), st));
     cudaMemcpyAsync(cursor, sm.off, (size_t)n_img * sizeof(int64_t), cudaMemcpyDeviceToDevice, st);
-    k_sm_fill<<<grid_for(rs.m_size), kBlock, 0, st>>>(g, rs, gf, cursor, sm.ent);
+    if (orth) {
+        if (orth_sm_fill(g, rs, *orth, gf, cursor, sm.ent, sm.rsoff, sm.rsent, st) != OMB_OK) {
+            cudaFreeAsync(cursor, st);
+            sysmat_free(sm);
+            return -1;
+        }
+    } else {
+        k_sm_fill<<<grid_for(rs.m_size), kBlock, 0, st>>>(g, rs, gf, cursor, sm.ent);
+    }
     k_sm_sort<<<grid_for(n_img), kBlock, 0, st>>>(sm.off, sm.ent, n_img);
     cudaFreeAsync(cursor, st);
     const cudaError_t e = cudaStreamSynchronize(st);
