@@ -82,7 +82,7 @@ def parse_args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="cbct",
                    choices=["cbct", "cbct_small", "dynpet", "dynpet_small", "fanbeam64", "fanbeam64_small",
-                            "interp_tof", "interp_tof_small"])
+                            "interp_tof", "interp_tof_small", "tube", "tube_small"])
     p.add_argument("--frames", type=int, default=None)
     p.add_argument("--views", type=int, default=None,
                    help="cbct: number of projections (fewer than 360 only for short profiling captures)")
@@ -799,6 +799,135 @@ def run_dynpet(args, rank, world, dev):
     return line
 
 
+def tube_cpu_rate(o, image, seconds):
+    """The reference's own CPU projector with projector type 2 (FP64, OpenMP) on subset 0, else the FP64
+    restatement."""
+    from oracle import oracle as orc
+    g = orc.Geometry(o)
+    threads = os.cpu_count() or 1
+    use_ref = orc.ref_lib() is not None
+    rays = g.rays(0)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        if use_ref:
+            yy = orc.ref_orth(g, image, 0, True, 2, threads=threads)
+            orc.ref_orth(g, yy, 0, False, 2, threads=threads)
+        else:
+            yy = orc.orth_forward(g, image, 0)
+            orc.orth_backward(g, yy, 0)
+        done += rays
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    desc = "reference projectorType123Implementation4<double> with the orthogonal-distance tube (OpenMP)" \
+        if use_ref else "FP64 oracle restatement"
+    return done / el, threads if use_ref else 1, "reference" if use_ref else "port", \
+        f"subset 0 ({rays} rays) per FP+BP pair, {done // rays} pairs in {el:.1f} s; {desc}"
+
+
+def run_tube(args, rank, world, dev):
+    """Projector type 2 (orthogonal-distance tube, 4 mm) on the dynamic-PET
+    scanner, one frame: the 16 subsets projected forward, then back, each
+    through the resident system matrix of its tube weights (built by the
+    warm-up)."""
+    import torch
+    from omega_b200 import _native
+    small = args.workload == "tube_small"
+    o = dynamic_pet_options(small)
+    o.projector_type = 2
+    o.tube_width_z = o.tube_width_xy = 4.0
+    o.addProjector()
+    o.initProj()
+    h = o._handle
+    n = int(o.N[0])
+    S = int(o.subsets)
+    ms = [int(o.measurementCount(s)) for s in range(S)]
+    m = sum(ms)
+    img_host = dynamic_images(o, 1)[0]
+    x = torch.from_numpy(np.ascontiguousarray(img_host)).to(dev)
+    ys = [torch.empty(ms[s], device=dev) for s in range(S)]
+    back = torch.empty(n, device=dev)
+    sp = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    tuning = {"siddon_bp_matrix": 1}
+    if args.tuning:
+        tuning.update({k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))})
+    o.tuning = tuning
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def step(tm):
+        tm.mark()
+        for s in range(S):
+            _native.call("omb_forward_frames", h, s, 1, P(x), n, P(ys[s]), ms[s], sp)
+        tm.mark()
+        for s in range(S):
+            _native.call("omb_backward_frames", h, s, 1, P(ys[s]), ms[s], P(back), n, sp)
+        tm.mark()
+
+    tot, clk, wall = run_timed(args, world, dev, step, 2)
+    t_fp, t_bp = tot
+    total = t_fp + t_bp
+    h_in = torch.from_numpy(np.ascontiguousarray(img_host)).pin_memory()
+    h_out = torch.empty(n, dtype=torch.float32).pin_memory()
+
+    class _NoMarks:
+        def mark(self):
+            pass
+
+    def step_host():
+        x.copy_(h_in, non_blocking=True)
+        step(_NoMarks())
+        h_out.copy_(back, non_blocking=True)
+
+    e2e_total = e2e_time(args, world, dev, step_host)
+    if rank != 0:
+        return None
+    nnz = 0
+    for s in range(S):
+        v = ctypes.c_int64()
+        _native.call("omb_system_matrix_nnz", h, s, ctypes.byref(v))
+        nnz += v.value
+    K = args.steps
+    mean_fp, mean_bp = t_fp / K, t_bp / K
+    # algorithmic bytes through the matrix: 8 bytes a weight plus the 4-byte gather it drives, and the
+    # outputs once (FP: measurements; BP: one image a subset)
+    fp_bytes = 12 * nnz + 4 * m
+    bp_bytes = 12 * nnz + 4 * n * S
+    comp = (n + m) * 4
+    if mean_bp >= mean_fp:
+        rl = roofline("tube_bp", bp_bytes, mean_bp, (args.workload, "tube_bp"), comp)
+    else:
+        rl = roofline("tube_fp", fp_bytes, mean_fp, (args.workload, "tube_fp"), comp)
+    rl["model"] = "through the matrix: FP = 12 nnz + 4 m B; BP = 12 nnz + 4 N S B (nnz the tube weights)"
+    line = {
+        "metric": "proj+backproj rays/s", "value": m * K * world / total, "unit": "rays/s",
+        "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": 1e3 * total / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded phantom)",
+        "config": {"workload": ("PET, 384 crystals x 32 rings, 256x192x63 sinograms, 128x128x63 image, projector "
+                                "type 2 (orthogonal-distance tube, 4 mm), 16 subsets, through the resident system "
+                                "matrix") if not small else "tube small (8 rings) for profiling",
+                   "rays_per_step": m, "tube_weights": nnz, "subsets": S, "tuning": tuning,
+                   "parallelism": f"replicas x{world}", "l2": "256 MB L2 flush between steps"},
+        "fp_ms": 1e3 * mean_fp, "bp_ms": 1e3 * mean_bp,
+        "roofline": rl,
+        "e2e": {"value": m * K * world / e2e_total, "unit": "rays/s", "h2d_bytes_per_step": n * 4,
+                "d2h_bytes_per_step": n * 4},
+        "gpu_launches": 2 * S * K,
+        "clocks": clk,
+        "wall_s": wall,
+    }
+    if not args.no_baseline and world == 1:
+        try:
+            v, cores, kind, sample = tube_cpu_rate(o, img_host, 10.0)
+            line["cpu_baseline"] = {"value": v, "unit": "rays/s", "cores": cores, "kind": kind,
+                                    "sample": sample + f"; host CPU {cpu_model()}"}
+        except Exception as e:
+            line["cpu_baseline"] = {"error": str(e)}
+    return line
+
+
 # ---------------------------------------------------------------------------
 # our arm: 64 fan-beam CT slices of uneven sizes, one persistent launch per
 # direction (omb_batch_forward / omb_batch_backward)
@@ -1111,6 +1240,28 @@ def run_reference(args):
         sample = (f"slice 0 ({sizes[0][0]}^2 image, {sizes[0][1]} views, {rays} rays) per step; FP64 restatement of "
                   "the type-1 projector (the reference's CPU projector build here is PET-only)")
         workload = "64 fan-beam CT slices (same sizes as ours), FP+BP pair over slice 0"
+    elif args.workload.startswith("tube"):
+        o = dynamic_pet_options(args.workload == "tube_small")
+        o.projector_type = 2
+        o.tube_width_z = o.tube_width_xy = 4.0
+        o.addProjector()
+        img = dynamic_images(o, 1)[0]
+        g = orc.Geometry(o)
+        use_ref = orc.ref_lib() is not None
+        rays = g.rays(0)
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            if use_ref:
+                y = orc.ref_orth(g, img, 0, True, 2, threads=threads)
+                orc.ref_orth(g, y, 0, False, 2, threads=threads)
+            else:
+                y = orc.orth_forward(g, img, 0)
+                orc.orth_backward(g, y, 0)
+            if it >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        kind, cores = ("reference", threads) if use_ref else ("port", 1)
+        sample = f"subset 0 ({rays} rays) per step, projector type 2 (4 mm tube)"
+        workload = "PET tube projector type 2 (same geometry as ours), FP+BP pair over subset 0"
     else:
         o = dynamic_pet_options(args.workload == "dynpet_small")
         img = dynamic_images(o, 1)[0]
@@ -1160,17 +1311,20 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-    runs = {"cbct": run_cbct, "fanbeam": run_fanbeam, "dynpet": run_dynpet, "interp_tof": run_interp_tof}
+    runs = {"cbct": run_cbct, "fanbeam": run_fanbeam, "dynpet": run_dynpet, "interp_tof": run_interp_tof,
+            "tube": run_tube}
     run = next(f for k, f in runs.items() if args.workload.startswith(k))
     line = run(args, rank, world, dev)
     if args.workload == "cbct" and world == 1 and not args.no_legs:
         # the other projectors of the path, each timed the same way: improved
-        # Siddon (dynamic PET) and interpolation with TOF (precision workload)
+        # Siddon (dynamic PET), interpolation with TOF (precision workload) and
+        # the orthogonal-distance tube (type 2)
         import copy
 
         import torch
         legs = {}
-        for name, wl, fn in (("siddon_dynpet", "dynpet", run_dynpet), ("interp_tof", "interp_tof", run_interp_tof)):
+        for name, wl, fn in (("siddon_dynpet", "dynpet", run_dynpet), ("interp_tof", "interp_tof", run_interp_tof),
+                             ("tube", "tube", run_tube)):
             torch.cuda.empty_cache()
             a = copy.copy(args)
             a.workload = wl

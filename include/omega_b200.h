@@ -244,6 +244,14 @@ int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, floa
 int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, void *stream);
 
 /*
+ * Number of weights the handle's resident system matrix holds for `subset`
+ * (omb_tuning.siddon_bp_matrix; built by the subset's first projection
+ * through it), 0 when none is built.  Host only; no counterpart in the
+ * reference (its projectors hold no matrix).
+ */
+int omb_system_matrix_nnz(omb_handle *h, int32_t subset, int64_t *out_host);
+
+/*
  * Launch shapes of a handle's projector kernels.  omb_create sets the
  * defaults below; omb_autotune times the candidates on the handle's own
  * geometry and keeps the fastest; omb_set_tuning sets them directly.  The

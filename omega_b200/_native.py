@@ -328,6 +328,7 @@ EXPORTS = [
     ("omb_set_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Tuning)]),
     ("omb_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Tuning),
                                     ctypes.c_void_p]),
+    ("omb_system_matrix_nnz", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
     ("omb_intersection_count", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
                                               ctypes.c_void_p]),
     ("omb_batch_create", ctypes.c_int, [ctypes.POINTER(GeometryDesc), ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),

@@ -1016,6 +1016,18 @@ int omb_osem_subset_frames(omb_handle *h, int32_t subset, int32_t n_frames, floa
     return em_update_frames(images, image_stride, sens, work_img, h->n_img, h->n_img, n_frames, eps, s);
 }
 
+int omb_system_matrix_nnz(omb_handle *h, int32_t subset, int64_t *out_host) {
+    if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
+    if (!out_host) return set_error(OMB_ERR_INVALID, "output pointer is NULL");
+    RaySet rs{};
+    const int st = ray_set(h, subset, rs);
+    if (st != OMB_OK) return st;
+    *out_host = 0;
+    for (const auto &x : h->sysmats)
+        if (x.proj0 == rs.proj0 && x.m_size == rs.m_size && x.cur_subset == rs.cur_subset) *out_host = x.nnz;
+    return OMB_OK;
+}
+
 int omb_intersection_count(omb_handle *h, int32_t subset, int64_t *out_host, void *stream) {
     if (!h) return set_error(OMB_ERR_INVALID, "handle is NULL");
     if (!out_host) return set_error(OMB_ERR_INVALID, "output pointer is NULL");
