@@ -191,13 +191,21 @@ __global__ void __launch_bounds__(kBlock) k_sm_fp_sl(const unsigned *__restrict_
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += stride) {
         const unsigned n = __ldg(rcnt + r);
         const uint2 *e0 = rsent + __ldg(rsoff + (r >> 5)) + (r & 31);
-        float acc = 0.f;
+        // two partial sums (even and odd entries) keep more loads in flight; fixed order, so the result
+        // is the same call to call
+        float acc0 = 0.f, acc1 = 0.f;
+        unsigned k = 0;
 #pragma unroll 4
-        for (unsigned k = 0; k < n; ++k) {
-            const uint2 e = __ldg(e0 + (int64_t)k * 32);
-            acc = fmaf(__uint_as_float(e.y), __ldg(x + e.x), acc);
+        for (; k + 1 < n; k += 2) {
+            const uint2 ea = __ldg(e0 + (int64_t)k * 32), eb = __ldg(e0 + (int64_t)(k + 1) * 32);
+            acc0 = fmaf(__uint_as_float(ea.y), __ldg(x + ea.x), acc0);
+            acc1 = fmaf(__uint_as_float(eb.y), __ldg(x + eb.x), acc1);
         }
-        y[r] = acc;
+        if (k < n) {
+            const uint2 e = __ldg(e0 + (int64_t)k * 32);
+            acc0 = fmaf(__uint_as_float(e.y), __ldg(x + e.x), acc0);
+        }
+        y[r] = acc0 + acc1;
     }
 }
 
