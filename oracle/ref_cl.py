@@ -62,6 +62,10 @@ def _lib(variant, precision):
             L.refcl_tv_gradient_ex.argtypes = [_I, _I, _I, _P, _D, _D, _D, _D, _P, _P]
         if hasattr(L, "refcl_proxtv"):
             L.refcl_proxtv.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D]
+        if hasattr(L, "refcl_ggmrf"):
+            L.refcl_ggmrf.argtypes = [_I, _I, _I, _P, _P, _I, _D, _D, _D, _D, _D, _P]
+        if hasattr(L, "refcl_hyper"):
+            L.refcl_hyper.argtypes = [_I, _I, _I, _P, _P, _I, _D, _D, _D, _P]
         if hasattr(L, "refcl_rdp"):
             L.refcl_rdp.argtypes = [_I, _I, _I, _P, _D, _D, _D, _P]
         if hasattr(L, "refcl_proxtgv"):
@@ -328,4 +332,28 @@ def rdp_gradient(u, shape, gamma, epps, beta, images=True, precision="d", exact_
     e = exact_inputs
     _lib("aux_rdp" if images else "aux_rdp_buf", precision).refcl_rdp(
         nx, ny, nz, _dp(uu), _scalar(gamma, e), _scalar(epps, e), _scalar(beta, e), _dp(g))
+    return g
+
+
+def ggmrf_gradient(u, shape, weights, p, q, c, pqc, beta, precision="d", exact_inputs=False):
+    """GGMRFKernel of the reference (-DGGMRF, 3 x 3 x 3 window): beta * dGGMRF(u)."""
+    nx, ny, nz = shape
+    uu = np.ascontiguousarray(u, dtype=np.float64).ravel()
+    w = np.ascontiguousarray(weights, dtype=np.float64).ravel()
+    g = np.zeros(uu.size)
+    e = exact_inputs
+    _lib("aux_ggmrf", precision).refcl_ggmrf(nx, ny, nz, _dp(uu), _dp(w), w.size, _scalar(p, e), _scalar(q, e),
+                                             _scalar(c, e), _scalar(pqc, e), _scalar(beta, e), _dp(g))
+    return g
+
+
+def hyperbolic_gradient(u, shape, weights, delta, beta, epps=1e-8, precision="d", exact_inputs=False):
+    """hyperbolicKernel of the reference (-DHYPER, 3 x 3 x 3 window): beta * dHyperbolic(u)."""
+    nx, ny, nz = shape
+    uu = np.ascontiguousarray(u, dtype=np.float64).ravel()
+    w = np.ascontiguousarray(weights, dtype=np.float64).ravel()
+    g = np.zeros(uu.size)
+    e = exact_inputs
+    _lib("aux_hyper", precision).refcl_hyper(nx, ny, nz, _dp(uu), _dp(w), w.size, _scalar(delta, e),
+                                             _scalar(epps, e), _scalar(beta, e), _dp(g))
     return g

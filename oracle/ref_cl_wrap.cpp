@@ -332,6 +332,49 @@ REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, doub
 }
 #endif
 
+#ifdef GGMRF
+/* GGMRFKernel (auxKernels.cl:878-980) over the (2 SWINDOWX + 1)(2 SWINDOWY + 1)(2 SWINDOWZ + 1)
+ * neighbourhood: grad += beta * dGGMRF(u), weights w (nw values, centre left out) in the kernel's order.
+ * Each work item is its own work group here, so it fills its local cache itself. */
+REFCL_EXPORT int refcl_ggmrf(int nx, int ny, int nz, const double *u, const double *w, int nw, double p, double q,
+                             double c, double pqc, double beta, double *grad) {
+    const size_t N = (size_t)nx * ny * nz;
+    rvec uu = to_real(u, N), g = to_real(grad, N), ww = to_real(w, (size_t)nw);
+    const omb_tex tex = make_tex(uu, nx, ny, nz, 0, 0, 0);
+    const int3 Nn = make_int3(nx, ny, nz);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                GGMRFKernel(g.data(), &tex, ww.data(), Nn, (omb_real)p, (omb_real)q, (omb_real)c, (omb_real)pqc,
+                            (omb_real)beta);
+            }
+    from_real(g, grad);
+    return 0;
+}
+#endif
+
+#ifdef HYPER
+/* hyperbolicKernel (auxKernels.cl:1591-1688): grad += beta * dHyperbolic(u) with delta `sigma`. */
+REFCL_EXPORT int refcl_hyper(int nx, int ny, int nz, const double *u, const double *w, int nw, double sigma,
+                             double epps, double beta, double *grad) {
+    const size_t N = (size_t)nx * ny * nz;
+    rvec uu = to_real(u, N), g = to_real(grad, N), ww = to_real(w, (size_t)nw);
+    const omb_tex tex = make_tex(uu, nx, ny, nz, 0, 0, 0);
+    const int3 Nn = make_int3(nx, ny, nz);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                hyperbolicKernel(g.data(), &tex, Nn, Nn, (omb_real)sigma, (omb_real)epps, (omb_real)beta, ww.data());
+            }
+    from_real(g, grad);
+    return 0;
+}
+#endif
+
 #ifdef RDP
 /* RDPKernel (auxKernels.cl:650-875, the 6-neighbour form): grad += beta *
  * dRDP(u); built with USEIMAGES the image is read through the shim's

@@ -357,3 +357,22 @@ def test_rdp_pinned(images):
     ours = io.rdp_gradient(u, shape, 2.0, 0.3, 1e-8, clamp=images)
     assert np.abs(ours - theirs).max() <= 1e-14 * np.abs(theirs).max()
     assert orc.rel_l2(io.rdp_gradient(u, shape, 2.0, 0.3, 1e-8, clamp=not images), theirs) > 1e-2
+
+
+def test_ggmrf_and_hyperbolic_pinned():
+    """image_oracle.ggmrf_gradient and hyperbolic_gradient against
+    GGMRFKernel (-DGGMRF) and hyperbolicKernel (-DHYPER) compiled on the host
+    with a 3 x 3 x 3 window, the image read through the clamp-to-edge texture;
+    ties (rounded values) exercise GGMRF's d = 0 skip."""
+    from oracle import image_oracle as io
+    shape = (9, 8, 7)
+    rng = np.random.default_rng(72)
+    u = np.round(rng.uniform(0.5, 1.5, int(np.prod(shape))), 2)
+    w = rng.uniform(0.2, 1.0, 26)
+    p, q, c = 2.0, 1.5, 0.01
+    theirs = ref_cl.ggmrf_gradient(u, shape, w, p, q, c, (p - q) / c ** (p - q), 0.3, exact_inputs=True)
+    ours = io.ggmrf_gradient(u, shape, (1, 1, 1), w, p, q, c, 0.3)
+    assert np.abs(ours - theirs).max() <= 1e-13 * np.abs(theirs).max()
+    theirs = ref_cl.hyperbolic_gradient(u, shape, w, 0.7, 0.3, exact_inputs=True)
+    ours = io.hyperbolic_gradient(u, shape, (1, 1, 1), w, 0.7, 0.3)
+    assert np.abs(ours - theirs).max() <= 1e-13 * np.abs(theirs).max()
