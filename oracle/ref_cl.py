@@ -62,6 +62,8 @@ def _lib(variant, precision):
             L.refcl_tv_gradient_ex.argtypes = [_I, _I, _I, _P, _D, _D, _D, _D, _P, _P]
         if hasattr(L, "refcl_proxtv"):
             L.refcl_proxtv.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D]
+        if hasattr(L, "refcl_nlm"):
+            L.refcl_nlm.argtypes = [_I, _I, _I, _P, _P, _I, _D, _D, _D, _D, _D, _D, _D, _D, _P, _P]
         if hasattr(L, "refcl_ggmrf"):
             L.refcl_ggmrf.argtypes = [_I, _I, _I, _P, _P, _I, _D, _D, _D, _D, _D, _P]
         if hasattr(L, "refcl_hyper"):
@@ -356,4 +358,22 @@ def hyperbolic_gradient(u, shape, weights, delta, beta, epps=1e-8, precision="d"
     e = exact_inputs
     _lib("aux_hyper", precision).refcl_hyper(nx, ny, nz, _dp(uu), _dp(w), w.size, _scalar(delta, e),
                                              _scalar(epps, e), _scalar(beta, e), _dp(g))
+    return g
+
+
+def nlm_gradient(u, shape, gaussian, h, epps, beta, variant="nlm0", gamma=10.0, ggmrf=(2.0, 1.5, 0.001),
+                 adaptive_s=0.0, u_ref=None, precision="d", exact_inputs=False):
+    """The reference's NLM kernel built as `variant` (aux_<variant>: nlm0, nlm1, nlm3, nlm6, nlm0ar), search
+    and patch windows 3 x 3 x 3: beta * g(u)."""
+    nx, ny, nz = shape
+    uu = np.ascontiguousarray(u, dtype=np.float64).ravel()
+    gg = np.ascontiguousarray(gaussian, dtype=np.float64).ravel()
+    rr = np.ascontiguousarray(u_ref if u_ref is not None else uu, dtype=np.float64).ravel()
+    g = np.zeros(uu.size)
+    e = exact_inputs
+    p, q, c = ggmrf
+    _lib("aux_" + variant, precision).refcl_nlm(nx, ny, nz, _dp(uu), _dp(gg), gg.size, _scalar(h, e),
+                                                _scalar(epps, e), _scalar(beta, e), _scalar(gamma, e),
+                                                _scalar(p, e), _scalar(q, e), _scalar(c, e), _scalar(adaptive_s, e),
+                                                _dp(rr), _dp(g))
     return g

@@ -332,6 +332,52 @@ REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, doub
 }
 #endif
 
+#ifdef NLM_
+/* The NLM kernel (auxKernels.cl:297-620) in the variant the build selected (NLTYPE, NLMADAPTIVE, NLMREF),
+ * search window SWINDOW*, patch PWINDOW*, the images read through the clamp-to-edge texture:
+ * grad += beta * g(u).  gauss: the patch weights; uref: the reference image (NLMREF) or NULL. */
+REFCL_EXPORT int refcl_nlm(int nx, int ny, int nz, const double *u, const double *gauss, int ng, double h,
+                           double epps, double beta, double gamma, double p, double q, double c, double s_adapt,
+                           const double *uref, double *grad) {
+    const size_t N = (size_t)nx * ny * nz;
+    rvec uu = to_real(u, N), g = to_real(grad, N), gg = to_real(gauss, (size_t)ng);
+    const omb_tex tex = make_tex(uu, nx, ny, nz, 0, 0, 0);
+#ifdef NLMREF
+    rvec rr = to_real(uref, N);
+    const omb_tex texr = make_tex(rr, nx, ny, nz, 0, 0, 0);
+#else
+    (void)uref;
+#endif
+    (void)gamma;
+    (void)p;
+    (void)q;
+    (void)c;
+    (void)s_adapt;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                NLM(g.data(), &tex, gg.data(), nx, ny, nz, nx, ny, nz, (omb_real)h, (omb_real)epps, (omb_real)beta
+#if NLTYPE >= 3
+                    , (omb_real)gamma
+#endif
+#if NLTYPE == 6
+                    , (omb_real)p, (omb_real)q, (omb_real)c
+#endif
+#ifdef NLMADAPTIVE
+                    , (omb_real)s_adapt
+#endif
+#ifdef NLMREF
+                    , &texr
+#endif
+                );
+            }
+    from_real(g, grad);
+    return 0;
+}
+#endif
+
 #ifdef GGMRF
 /* GGMRFKernel (auxKernels.cl:878-980) over the (2 SWINDOWX + 1)(2 SWINDOWY + 1)(2 SWINDOWZ + 1)
  * neighbourhood: grad += beta * dGGMRF(u), weights w (nw values, centre left out) in the kernel's order.

@@ -376,3 +376,26 @@ def test_ggmrf_and_hyperbolic_pinned():
     theirs = ref_cl.hyperbolic_gradient(u, shape, w, 0.7, 0.3, exact_inputs=True)
     ours = io.hyperbolic_gradient(u, shape, (1, 1, 1), w, 0.7, 0.3)
     assert np.abs(ours - theirs).max() <= 1e-13 * np.abs(theirs).max()
+
+
+@pytest.mark.parametrize("variant,nl_type,extra", [("nlm0", 0, False), ("nlm1", 1, False), ("nlm3", 3, False),
+                                                   ("nlm6", 6, False), ("nlm0ar", 0, True)])
+def test_nlm_kernel_pinned(variant, nl_type, extra):
+    """image_oracle.nlm_gradient in its kernel mode (edges clamped) against
+    the reference's NLM kernel compiled on the host: NLM, NLTV, NLRD, NLGGMRF
+    and NLM with the adaptive weight and a reference image, search and patch
+    windows 3 x 3 x 3."""
+    from oracle import image_oracle as io
+    shape = (10, 9, 8)
+    rng = np.random.default_rng(73)
+    n = int(np.prod(shape))
+    u = rng.uniform(0.5, 1.5, n)
+    gauss = rng.uniform(0.1, 1.0, 27)
+    ref = rng.uniform(0.5, 1.5, n) if extra else None
+    s = 0.05 if extra else None
+    theirs = ref_cl.nlm_gradient(u, shape, gauss, 0.05, 1e-8, 0.3, variant=variant, gamma=2.0,
+                                 ggmrf=(2.0, 1.5, 0.01), adaptive_s=s or 0.0, u_ref=ref, exact_inputs=True)
+    ours = 0.3 * io.nlm_gradient(u, shape, gauss, (1, 1, 1), (1, 1, 1), 0.05, 1e-8, nl_type, gamma=2.0,
+                                 ggmrf=(2.0, 1.5, 0.01), u_ref=ref, adaptive_s=s)
+    assert np.count_nonzero(theirs) > n // 2
+    assert np.abs(ours - theirs).max() <= 1e-13 * np.abs(theirs).max()
