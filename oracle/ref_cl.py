@@ -62,6 +62,8 @@ def _lib(variant, precision):
             L.refcl_tv_gradient_ex.argtypes = [_I, _I, _I, _P, _D, _D, _D, _D, _P, _P]
         if hasattr(L, "refcl_proxtv"):
             L.refcl_proxtv.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D]
+        if hasattr(L, "refcl_psf"):
+            L.refcl_psf.argtypes = [_I, _I, _I, _P, _P, _I, _I, _I, _P]
         if hasattr(L, "refcl_nlm"):
             L.refcl_nlm.argtypes = [_I, _I, _I, _P, _P, _I, _D, _D, _D, _D, _D, _D, _D, _D, _P, _P]
         if hasattr(L, "refcl_ggmrf"):
@@ -377,3 +379,13 @@ def nlm_gradient(u, shape, gaussian, h, epps, beta, variant="nlm0", gamma=10.0, 
                                                 _scalar(p, e), _scalar(q, e), _scalar(c, e), _scalar(adaptive_s, e),
                                                 _dp(rr), _dp(g))
     return g
+
+
+def psf_convolve(x, shape, window, g, precision="d"):
+    """The reference's Convolution3D_f (-DPSF): the window applied at every voxel, faces mirrored."""
+    nx, ny, nz = shape
+    xx = np.ascontiguousarray(x, dtype=np.float64).ravel()
+    w = np.ascontiguousarray(window, dtype=np.float64).ravel()
+    out = np.zeros(xx.size)
+    _lib("aux_psf", precision).refcl_psf(nx, ny, nz, _dp(xx), _dp(w), int(g[0]), int(g[1]), int(g[2]), _dp(out))
+    return out

@@ -332,6 +332,30 @@ REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, doub
 }
 #endif
 
+#ifdef PSF
+/* Convolution3D_f (auxKernels.cl:190-245): out = the window (2 gx + 1)(2 gy + 1)(2 gz + 1) applied at every
+ * voxel with the image mirrored at its faces; the global size is the image size. */
+REFCL_EXPORT int refcl_psf(int nx, int ny, int nz, const double *in, const double *w, int gx, int gy, int gz,
+                           double *out) {
+    const size_t N = (size_t)nx * ny * nz;
+    const size_t nw = (size_t)(2 * gx + 1) * (2 * gy + 1) * (2 * gz + 1);
+    rvec ii = to_real(in, N), oo((size_t)N, (omb_real)0), ww = to_real(w, nw);
+#pragma omp parallel
+    {
+        gridDim = make_uint3((unsigned)nx, (unsigned)ny, (unsigned)nz);
+#pragma omp for schedule(static)
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    set_item((unsigned)i, (unsigned)j, (unsigned)k);
+                    Convolution3D_f(ii.data(), oo.data(), ww.data(), gx, gy, gz);
+                }
+    }
+    from_real(oo, out);
+    return 0;
+}
+#endif
+
 #ifdef NLM_
 /* The NLM kernel (auxKernels.cl:297-620) in the variant the build selected (NLTYPE, NLMADAPTIVE, NLMREF),
  * search window SWINDOW*, patch PWINDOW*, the images read through the clamp-to-edge texture:

@@ -399,3 +399,17 @@ def test_nlm_kernel_pinned(variant, nl_type, extra):
                                  ggmrf=(2.0, 1.5, 0.01), u_ref=ref, adaptive_s=s)
     assert np.count_nonzero(theirs) > n // 2
     assert np.abs(ours - theirs).max() <= 1e-13 * np.abs(theirs).max()
+
+
+@pytest.mark.parametrize("g", [(2, 3, 1), (1, 1, 1), (3, 2, 2)])
+def test_psf_pinned(g):
+    """image_oracle.psf_convolve against Convolution3D_f (-DPSF) compiled on
+    the host: the window applied at every voxel with the faces mirrored,
+    exactly, on an image smaller than some windows' reach in z."""
+    from oracle import image_oracle as io
+    shape = (13, 11, 9)
+    rng = np.random.default_rng(74)
+    x = rng.uniform(0.0, 2.0, int(np.prod(shape)))
+    w = rng.random((2 * g[0] + 1) * (2 * g[1] + 1) * (2 * g[2] + 1))
+    theirs = ref_cl.psf_convolve(x, shape, w, g)
+    assert np.abs(io.psf_convolve(x, shape, w, g) - theirs).max() <= 1e-14 * np.abs(theirs).max()
