@@ -381,6 +381,26 @@ def _grad_precond(xp, shape, diff_type, v1, v2):
     return np.minimum(v2, np.maximum(v1, f)).ravel(order='F')
 
 
+def poisson_update(kind, x, rhs, lam, eps, alpha, positivity=True):
+    """The image step after the backprojection (PoissonUpdate, auxKernels.cl:1994-2026): PKMA x_a = x - lam
+    rhs, x = (1 - alpha) x + alpha max(eps, x_a); MBSREM (MRAMLA too) x + lam rhs, max(eps, .), values >= alpha
+    (the bound U) set to alpha - eps; BSREM (RAMLA too) x + lam rhs x, max(eps, .)."""
+    x = np.asarray(x, dtype=np.float64)
+    if kind == "PKMA":
+        xa = x - lam * rhs
+    elif kind == "MBSREM":
+        xa = x + lam * rhs
+    else:
+        xa = x + lam * rhs * x
+    if positivity:
+        xa = np.maximum(eps, xa)
+    if kind == "PKMA":
+        return (1.0 - alpha) * x + alpha * xa
+    if kind == "MBSREM":
+        return np.where(xa >= alpha, alpha - eps, xa)
+    return xa
+
+
 def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None, backward=None, randoms=None,
             prior_grad=None, positivity=True, alpha=None, upper=10000.0, precond=0, ref=None, alpha_precond=None,
             grad_precond=None, curv_precond=False, meas_precond=False, auto_relax=False, relax_scaling=False,
@@ -509,20 +529,11 @@ def relaxed(geom: Geometry, y_subsets, x0, n_iter, kind, lam=None, forward=None,
                         lam[it] = np.float32(lam[it]) * np.float32(q / 1.5)
                 lm = float(lam[it])
             if kind == "PKMA":
-                a = float(alpha[it * S + s])
-                xa = x - lm * rhs
-                if positivity:
-                    xa = np.maximum(eps, xa)
-                x = (1.0 - a) * x + a * xa
+                x = poisson_update("PKMA", x, rhs, lm, eps, float(alpha[it * S + s]), positivity)
             elif kind in ("MRAMLA", "MBSREM"):
-                x = x + lm * rhs
-                if positivity:
-                    x = np.maximum(eps, x)
-                x = np.where(x >= upper, upper - eps, x)
+                x = poisson_update("MBSREM", x, rhs, lm, eps, upper, positivity)
             elif ramla:
-                x = x + lm * rhs * x
-                if positivity:
-                    x = np.maximum(eps, x)
+                x = poisson_update("BSREM", x, rhs, lm, eps, 0.0, positivity)
             else:
                 x = x + lm * x / sens[s] * (rhs - sens[s])
         if mapstep:

@@ -62,6 +62,8 @@ def _lib(variant, precision):
             L.refcl_tv_gradient_ex.argtypes = [_I, _I, _I, _P, _D, _D, _D, _D, _P, _P]
         if hasattr(L, "refcl_proxtv"):
             L.refcl_proxtv.argtypes = [_I, _I, _I, _P, _P, _P, _D, _D]
+        if hasattr(L, "refcl_poisson"):
+            L.refcl_poisson.argtypes = [_I, _P, _P, _D, _D, _D, _I]
         if hasattr(L, "refcl_psf"):
             L.refcl_psf.argtypes = [_I, _I, _I, _P, _P, _I, _I, _I, _P]
         if hasattr(L, "refcl_nlm"):
@@ -389,3 +391,13 @@ def psf_convolve(x, shape, window, g, precision="d"):
     out = np.zeros(xx.size)
     _lib("aux_psf", precision).refcl_psf(nx, ny, nz, _dp(xx), _dp(w), int(g[0]), int(g[1]), int(g[2]), _dp(out))
     return out
+
+
+def poisson_update(kind, x, rhs, lam, eps, alpha, positivity=True, precision="d", exact_inputs=False):
+    """PoissonUpdate of the reference built with -DPKMA / -DMBSREM / -DBSREM: the new image."""
+    xx = np.ascontiguousarray(x, dtype=np.float64).ravel().copy()
+    rr = np.ascontiguousarray(rhs, dtype=np.float64).ravel()
+    e = exact_inputs
+    _lib("aux_" + kind.lower(), precision).refcl_poisson(xx.size, _dp(xx), _dp(rr), _scalar(lam, e), _scalar(eps, e),
+                                                         _scalar(alpha, e), 1 if positivity else 0)
+    return xx

@@ -332,6 +332,22 @@ REFCL_EXPORT int refcl_tv_gradient(int nx, int ny, int nz, const double *u, doub
 }
 #endif
 
+#if defined(PKMA) || defined(MBSREM) || defined(BSREM)
+/* PoissonUpdate (auxKernels.cl:1994-2026) of the variant the build selected, over n voxels (a row). */
+REFCL_EXPORT int refcl_poisson(int n, double *im, const double *rhs, double lambda, double epps, double alpha,
+                               int positivity) {
+    rvec I = to_real(im, (size_t)n), R = to_real(rhs, (size_t)n);
+    const int3 Nn = make_int3(n, 1, 1);
+    for (int i = 0; i < n; ++i) {
+        set_item((unsigned)i, 0u, 0u);
+        PoissonUpdate(I.data(), R.data(), Nn, (omb_real)lambda, (omb_real)epps, (omb_real)alpha,
+                      (unsigned char)(positivity ? 1 : 0));
+    }
+    from_real(I, im);
+    return 0;
+}
+#endif
+
 #ifdef PSF
 /* Convolution3D_f (auxKernels.cl:190-245): out = the window (2 gx + 1)(2 gy + 1)(2 gz + 1) applied at every
  * voxel with the image mirrored at its faces; the global size is the image size. */

@@ -413,3 +413,20 @@ def test_psf_pinned(g):
     w = rng.random((2 * g[0] + 1) * (2 * g[1] + 1) * (2 * g[2] + 1))
     theirs = ref_cl.psf_convolve(x, shape, w, g)
     assert np.abs(io.psf_convolve(x, shape, w, g) - theirs).max() <= 1e-14 * np.abs(theirs).max()
+
+
+@pytest.mark.parametrize("kind", ["PKMA", "MBSREM", "BSREM"])
+@pytest.mark.parametrize("positivity", [True, False])
+def test_poisson_update_pinned(kind, positivity):
+    """oracle.poisson_update (the image step of the relaxed loops) against
+    PoissonUpdate compiled on the host with -DPKMA / -DMBSREM / -DBSREM, with
+    values that hit the positivity floor and, for MBSREM, the upper bound."""
+    rng = np.random.default_rng(75)
+    x = rng.uniform(0.0, 3.0, 500)
+    rhs = rng.normal(0.0, 2.0, 500)
+    alpha = {"PKMA": 0.7, "MBSREM": 2.5, "BSREM": 0.0}[kind]
+    theirs = ref_cl.poisson_update(kind, x, rhs, 0.6, 1e-5, alpha, positivity, exact_inputs=True)
+    ours = orc.poisson_update(kind, x, rhs, 0.6, 1e-5, alpha, positivity)
+    assert np.abs(ours - theirs).max() <= 1e-15 * np.abs(theirs).max()
+    if positivity:
+        assert np.any(theirs == 1e-5) or kind == "PKMA"
