@@ -278,12 +278,20 @@ __device__ __forceinline__ void bp_voxel_run(const float2 *__restrict__ pc, int 
             const int ma = min((int)lo, mmax), mb = min((int)hi, mmax);
             const float2 ea = pc[ma * STRIDE], eb = pc[mb * STRIDE];
             const float apu = fmaf(hi, eb.y, eb.x) - fmaf(lo, ea.y, ea.x);
-            if (apu != 0.f) {
+            if (SENS) {
+                if (apu != 0.f) {
+                    const float vz = fmaf((float)t, dz, vz0);
+                    const float q2 = fmaf(vz, vz, axy);
+                    const float ker = kscale * (q2 * rsqrtf(q2));
+                    temp[t] = fmaf(apu, ker, temp[t]);
+                    wsum[t] += ker;
+                }
+            } else {
+                // branch-free: with apu = 0 the multiply-add leaves the sum as it is (q2 >= axy > 0, so ker
+                // is finite)
                 const float vz = fmaf((float)t, dz, vz0);
                 const float q2 = fmaf(vz, vz, axy);
-                const float ker = kscale * (q2 * rsqrtf(q2));
-                temp[t] = fmaf(apu, ker, temp[t]);
-                if (SENS) wsum[t] += ker;
+                temp[t] = fmaf(apu, kscale * (q2 * rsqrtf(q2)), temp[t]);
             }
         }
     }
