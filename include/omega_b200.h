@@ -345,7 +345,9 @@ typedef enum omb_prior {
     OMB_PRIOR_GGMRF = 7,    /* options.GGMRF: omb_ggmrf_gradient over prior_g with ggmrf_weights and ggmrf[3] */
     OMB_PRIOR_HYPERBOLIC = 8,/* options.hyperbolic: omb_hyperbolic_gradient over prior_g with hyper_weights */
     OMB_PRIOR_WMEAN = 9,    /* options.weighted_mean, mean_type 1-6: omb_wmean_gradient over prior_g */
-    OMB_PRIOR_AD = 10       /* options.AD: omb_ad_gradient with ad_dt, ad_k, ad_niter, ad_flux, ad_diffusion */
+    OMB_PRIOR_AD = 10,      /* options.AD: omb_ad_gradient with ad_dt, ad_k, ad_niter, ad_flux, ad_diffusion */
+    OMB_PRIOR_LFILTER = 11, /* options.L: omb_lfilter_gradient over prior_g with lfilter_weights */
+    OMB_PRIOR_FMH = 12      /* options.FMH: omb_fmh_gradient over prior_g with fmh_weights */
 } omb_prior;
 
 typedef struct omb_recon_params {
@@ -453,6 +455,8 @@ typedef struct omb_recon_params {
                                  normalisation switch is mrp_no_norm (options.med_no_norm) */
     int32_t rdp_edge;         /* OMB_PRIOR_RDP: 1 neighbours outside the image clamped to the edge voxel (options.useImages,
                                  the reference's default), 0 read as 0 (see omb_rdp_gradient_ex) */
+    const float *lfilter_weights;/* OMB_PRIOR_LFILTER: device, options.a_L (one weight per rank of the window) */
+    const float *fmh_weights; /* OMB_PRIOR_FMH: device, options.fmh_weights ((2 Ndx + 1) x lines, column-major) */
 } omb_recon_params;
 
 /*
@@ -604,6 +608,34 @@ int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int3
  */
 int omb_mrp_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx, int32_t my,
                      int32_t mz, float epps, float beta, int32_t no_norm, void *stream);
+
+/*
+ * The neighbourhood of the L-filter and FMH priors is the reference's offsets
+ * grid (computeOffsets.m): columns over -m..m on every axis, m = Ndx, x
+ * fastest; 3 axes when Ndx = Ndy = Ndz (mx = my = mz here), 2 when Ndx = Ndy =
+ * 1 and Ndz = 0.  Other windows return OMB_ERR_UNSUPPORTED (the reference's
+ * grid does not follow them).  The image is mirrored at its faces
+ * (functions.hpp:216-260).
+ *
+ * L-filter prior gradient (L_filter, priors.h:84-97): s = sum over ranks r of
+ * a_l[r] times the window value of rank r (ascending); grad += beta * (u - s)
+ * / (s + epps) (no_norm: beta * (u - s)).  a_l (device) has one weight per
+ * window value; windows up to 125 values (m <= 2).
+ */
+int omb_lfilter_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx, int32_t my,
+                         int32_t mz, const float *a_l, float epps, float beta, int32_t no_norm, void *stream);
+
+/*
+ * FMH prior gradient (FMH, priors.h:54-82): the weighted means along 13 lines
+ * through the voxel (4 when nz = 1 or mz = 0; line ii = the grid columns
+ * m ii + e (c / m - ii), e = 0..2m, c the centre column) with the column ii
+ * of fmh_weights (device, (2m + 1) x lines, column-major), and the voxel's
+ * value; med = their median (the mean of the middle two of 14);
+ * grad += beta * (u - med) / (med + epps) (no_norm: beta * (u - med)).
+ * m <= 8.
+ */
+int omb_fmh_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx, int32_t my,
+                     int32_t mz, const float *fmh_weights, float epps, float beta, int32_t no_norm, void *stream);
 
 /*
  * Anisotropic-diffusion prior gradient (priors.h:226-237): grad += beta *

@@ -158,6 +158,8 @@ class ReconParams(ctypes.Structure):
         ("ad_flux", ctypes.c_int32),
         ("ad_diffusion", ctypes.c_int32),
         ("rdp_edge", ctypes.c_int32),
+        ("lfilter_weights", ctypes.c_void_p),
+        ("fmh_weights", ctypes.c_void_p),
     ]
 
 
@@ -182,6 +184,8 @@ OMB_PRIOR_GGMRF = 7
 OMB_PRIOR_HYPERBOLIC = 8
 OMB_PRIOR_WMEAN = 9
 OMB_PRIOR_AD = 10
+OMB_PRIOR_LFILTER = 11
+OMB_PRIOR_FMH = 12
 
 
 class Tuning(ctypes.Structure):
@@ -304,6 +308,14 @@ EXPORTS = [
     ("omb_mrp_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p]),
+    ("omb_lfilter_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                            ctypes.c_void_p]),
+    ("omb_fmh_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                        ctypes.c_void_p]),
     ("omb_nlm_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                         ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p, ctypes.c_float,

@@ -557,3 +557,139 @@ extern "C" int omb_wmean_gradient(const float *u, float *grad, int32_t nx, int32
     if (e != cudaSuccess) return set_error(OMB_ERR_CUDA, "weighted mean (types 4-6) launch failed");
     return OMB_OK;
 }
+
+namespace omb {
+
+// Neighbour column c of the offsets grid the L-filter and FMH index
+// (computeOffsets.m: ndgrid over -m..m on every axis, m = Ndx, x fastest;
+// d = 3 axes, or 2 when Ndx + Ndy + Ndz < 3) as an offset (i, j, k).
+__device__ __forceinline__ int3 nb_offset(int c, int m, int w, int d) {
+    return make_int3(c % w - m, (c / w) % w - m, d == 3 ? c / (w * w) - m : 0);
+}
+
+__device__ __forceinline__ float mirrored(const float *__restrict__ u, int x, int y, int z, int3 o, int nx, int ny,
+                                          int nz) {
+    return __ldg(u + mirror(x + o.x, nx) + (int64_t)mirror(y + o.y, ny) * nx +
+                 (int64_t)mirror(z + o.z, nz) * ((int64_t)nx * ny));
+}
+
+// L-filter prior (L_filter, priors.h:84-97): the w^d neighbourhood of the
+// image mirrored at its faces sorted ascending, its weighted sum with a_L
+// (a_L[r] weighs the value of rank r), grad += beta * (u - s) / (s + epps),
+// or beta * (u - s) with no_norm.  Each value takes the weight of its rank
+// (equal values share a rank range, and any split of it gives the same sum);
+// one thread per voxel, the window in local memory (at most 125 values).
+constexpr int kLfMax = 125;
+
+__global__ void k_lfilter_gradient(const float *__restrict__ u, float *__restrict__ grad, int nx, int ny, int nz, int m,
+                                   int d, const float *__restrict__ a, float epps, float beta, int no_norm) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const int w = 2 * m + 1;
+    const int ncol = d == 3 ? w * w * w : w * w;
+    float win[kLfMax];
+    for (int c = 0; c < ncol; ++c) win[c] = mirrored(u, x, y, z, nb_offset(c, m, w, d), nx, ny, nz);
+    float s = 0.f;
+    for (int h = 0; h < ncol; ++h) {
+        int rank = 0;
+        for (int l = 0; l < ncol; ++l) rank += (win[l] < win[h] || (win[l] == win[h] && l < h)) ? 1 : 0;
+        s = fmaf(__ldg(a + rank), win[h], s);
+    }
+    const int64_t n = x + (int64_t)y * nx + (int64_t)z * nx * ny;
+    const float dv = __ldg(u + n) - s;
+    grad[n] += no_norm ? dv * beta : dv / (s + epps) * beta;
+}
+
+// FMH prior (FMH, priors.h:54-82): nl lines through the voxel (13 in 3-D, 4
+// when Nz = 1 or Ndz = 0), line ii the offsets-grid columns
+// m ii + e (alku / m - ii), e = 0..2m, alku the centre column; each line's
+// weighted mean with the column ii of fmh_weights ((2m+1) x nl, column-major
+// as the reference loads it), the voxel's own value as value nl + 1, their
+// median (the mean of the middle two for an even count, af::median);
+// grad += beta * (u - med) / (med + epps), or beta * (u - med) with no_norm.
+constexpr int kFmhLines = 13;
+
+__global__ void k_fmh_gradient(const float *__restrict__ u, float *__restrict__ grad, int nx, int ny, int nz, int m,
+                               int d, int nl, const float *__restrict__ fw, float epps, float beta, int no_norm) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const int w = 2 * m + 1;
+    const int ncol = d == 3 ? w * w * w : w * w;
+    const int step0 = (ncol - 1) / 2 / m;
+    float v[kFmhLines + 1];
+    for (int ii = 0; ii < nl; ++ii) {
+        float acc = 0.f;
+        for (int e = 0; e < w; ++e)
+            acc = fmaf(__ldg(fw + e + ii * w), mirrored(u, x, y, z, nb_offset(m * ii + e * (step0 - ii), m, w, d), nx, ny, nz),
+                       acc);
+        v[ii] = acc;
+    }
+    const int64_t n = x + (int64_t)y * nx + (int64_t)z * nx * ny;
+    const float un = __ldg(u + n);
+    v[nl] = un;
+    const int nv = nl + 1;
+    for (int i = 1; i < nv; ++i) {
+        const float t = v[i];
+        int j = i - 1;
+        while (j >= 0 && v[j] > t) {
+            v[j + 1] = v[j];
+            --j;
+        }
+        v[j + 1] = t;
+    }
+    const float med = (nv & 1) ? v[nv / 2] : 0.5f * (v[nv / 2 - 1] + v[nv / 2]);
+    const float dv = un - med;
+    grad[n] += no_norm ? dv * beta : dv / (med + epps) * beta;
+}
+
+// the offsets grids the reference's computeOffsets.m lays out consistently:
+// Ndx = Ndy = Ndz (a cube, d = 3) or Ndx = Ndy = 1 with Ndz = 0 (d = 2)
+static int median_filter_grid(int32_t nx, int32_t ny, int32_t nz, int32_t mx, int32_t my, int32_t mz, int max_m,
+                              const char *what, int *d) {
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(OMB_ERR_INVALID, "image size must be positive");
+    if (nz > 65535) return set_error(OMB_ERR_UNSUPPORTED, "more than 65535 slices");
+    const bool cube = mx >= 1 && mx <= max_m && my == mx && mz == mx;
+    const bool square = mx == 1 && my == 1 && mz == 0;
+    if (!cube && !square) return set_error(OMB_ERR_UNSUPPORTED, what);
+    if (mx > nx || my > ny || mz > nz) return set_error(OMB_ERR_INVALID, "prior window larger than the image");
+    *d = cube ? 3 : 2;
+    return OMB_OK;
+}
+
+}  // namespace omb
+
+extern "C" int omb_lfilter_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx,
+                                    int32_t my, int32_t mz, const float *a_l, float epps, float beta, int32_t no_norm,
+                                    void *stream) {
+    using namespace omb;
+    if (!u || !grad || !a_l) return set_error(OMB_ERR_INVALID, "u/grad/a_L pointer is NULL");
+    int d = 0;
+    const int st = median_filter_grid(nx, ny, nz, mx, my, mz, 2, "L-filter windows: Ndx = Ndy = Ndz <= 2, or Ndx = Ndy = 1 with Ndz = 0", &d);
+    if (st != OMB_OK) return st;
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    k_lfilter_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, mx, d, a_l, epps, beta, no_norm);
+    OMB_LAUNCH_CHECK("L-filter gradient launch");
+    return OMB_OK;
+}
+
+extern "C" int omb_fmh_gradient(const float *u, float *grad, int32_t nx, int32_t ny, int32_t nz, int32_t mx,
+                                int32_t my, int32_t mz, const float *fmh_weights, float epps, float beta,
+                                int32_t no_norm, void *stream) {
+    using namespace omb;
+    if (!u || !grad || !fmh_weights) return set_error(OMB_ERR_INVALID, "u/grad/fmh_weights pointer is NULL");
+    int d = 0;
+    const int st = median_filter_grid(nx, ny, nz, mx, my, mz, 8, "FMH windows: Ndx = Ndy = Ndz <= 8, or Ndx = Ndy = 1 with Ndz = 0", &d);
+    if (st != OMB_OK) return st;
+    const int nl = (nz == 1 || mz == 0) ? 4 : kFmhLines;
+    dim3 block(32, 8);
+    dim3 grid((nx + 31) / 32, (ny + 7) / 8, nz);
+    k_fmh_gradient<<<grid, block, 0, (cudaStream_t)stream>>>(u, grad, nx, ny, nz, mx, d, nl, fmh_weights, epps, beta,
+                                                             no_norm);
+    OMB_LAUNCH_CHECK("FMH gradient launch");
+    return OMB_OK;
+}

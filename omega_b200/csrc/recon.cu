@@ -110,12 +110,16 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
         const bool sub_prior = alg == OMB_RECON_MBSREM || (pkma && p->prior != 0);
         const bool need_prior = osl || map || sub_prior;
         const bool no_sens = ramla || pkma || mb;
-        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_AD))
+        if (need_prior && (p->prior < OMB_PRIOR_RDP || p->prior > OMB_PRIOR_FMH))
             return set_error(OMB_ERR_INVALID, "unknown prior");
         if (need_prior && (p->prior == OMB_PRIOR_QUAD || p->prior == OMB_PRIOR_HUBER) && !p->prior_window)
             return set_error(OMB_ERR_INVALID, "the quadratic / Huber prior needs its window");
         if (need_prior && p->prior == OMB_PRIOR_WMEAN && !p->wmean_weights)
             return set_error(OMB_ERR_INVALID, "the weighted mean prior needs its weights");
+        if (need_prior && p->prior == OMB_PRIOR_LFILTER && !p->lfilter_weights)
+            return set_error(OMB_ERR_INVALID, "the L-filter prior needs its weights");
+        if (need_prior && p->prior == OMB_PRIOR_FMH && !p->fmh_weights)
+            return set_error(OMB_ERR_INVALID, "the FMH prior needs its weights");
         if (need_prior && p->prior == OMB_PRIOR_HYPERBOLIC && !p->hyper_weights)
             return set_error(OMB_ERR_INVALID, "the hyperbolic prior needs its weights");
         if (need_prior && p->prior == OMB_PRIOR_GGMRF && !p->ggmrf_weights)
@@ -267,6 +271,12 @@ extern "C" int omb_reconstruct(omb_handle *h, omb_recon_params *p, const float *
             if (p->prior == OMB_PRIOR_AD)
                 return omb_ad_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->ad_dt, p->ad_k, p->ad_niter, p->ad_flux,
                                        p->ad_diffusion, epps, p->beta, p->mrp_no_norm, stream);
+            if (p->prior == OMB_PRIOR_LFILTER)
+                return omb_lfilter_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1],
+                                            p->prior_g[2], p->lfilter_weights, epps, p->beta, p->mrp_no_norm, stream);
+            if (p->prior == OMB_PRIOR_FMH)
+                return omb_fmh_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1], p->prior_g[2],
+                                        p->fmh_weights, epps, p->beta, p->mrp_no_norm, stream);
             if (p->prior == OMB_PRIOR_MRP)
                 return omb_mrp_gradient(x_out, du.f(), g.nx, g.ny, g.nz, p->prior_g[0], p->prior_g[1], p->prior_g[2],
                                         epps, p->beta, p->mrp_no_norm, stream);

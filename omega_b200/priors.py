@@ -148,6 +148,143 @@ def weighted_mean_weights(options):
     return np.ascontiguousarray(w, dtype=np.float32)
 
 
+def _voxel_sizes(options):
+    """FOVa_x / Nx, FOVa_y / Ny, axial_fov / Nz in FP64 (the prepass's dx, dy, dz)."""
+    def one(v):
+        return float(np.ravel(v)[0])
+    return (one(options.FOVa_x) / one(options.Nx), one(options.FOVa_y) / one(options.Ny),
+            one(options.axial_fov) / one(options.Nz))
+
+
+def median_filter_window(options):
+    """(Ndx, Ndy, Ndz) of the L-filter / FMH, checked against the offsets grids
+    computeOffsets.m lays out consistently: Ndx = Ndy = Ndz, or Ndx = Ndy = 1
+    with Ndz = 0."""
+    nd = (int(options.Ndx), int(options.Ndy), int(options.Ndz))
+    if not ((nd[0] >= 1 and nd[0] == nd[1] == nd[2]) or nd == (1, 1, 0)):
+        raise ValueError('the L-filter and FMH need Ndx = Ndy = Ndz, or Ndx = Ndy = 1 with Ndz = 0')
+    return nd
+
+
+# the tabulated one-dimensional L-filter weights of lfilter_weights.m for 3, 9
+# and 25 window values (the first half and the centre; the rest mirrored)
+_LFILTER_1D = {
+    3: [0.15168, 0.69663],
+    9: [-0.01899, 0.02904, 0.06965, 0.23795, 0.36469],
+    25: [0.0055, 0.00335, -0.00427, -0.00101, -0.00008, 0.00065, 0.00314, 0.01064, 0.02907, 0.06499, 0.11835,
+         0.17195, 0.19541],
+}
+
+
+def lfilter_weights(options):
+    """The L-filter's weights a_L, float32, one per rank of the window:
+    options.a_L when given, else lfilter_weights.m.  One-dimensional
+    (oneD_weights): the tabulated sets for 3, 9 and 25 values, the Laplace
+    curve 0.5 exp(x / b) on linspace(-4, 0) mirrored and normalised for 67
+    values or more; the optimal weights for other counts below 67 come from
+    numerical integration and are not built (give options.a_L).  Otherwise
+    the distance weights: 0.5 exp(x / b), x = linspace(-1.5, 0, 3), over the
+    offset's distance (the centre alpha1(end) / min(dx, dy, dz); the axis
+    neighbours alpha1(2) / (d |l|); the diagonals alpha1(1) over the plane or
+    space diagonal, whose 3-D form is sqrt(sqrt(dx^2 + dy^2) + dz^2) as in the
+    reference), normalised to sum 1."""
+    a = np.asarray(getattr(options, 'a_L', np.empty(0)), dtype=np.float32).ravel(order='F')
+    ndx, ndy, ndz = median_filter_window(options)
+    N = (2 * ndx + 1) * (2 * ndy + 1) * (2 * ndz + 1)
+    if a.size:
+        if a.size != N:
+            raise ValueError('a_L must have (2 Ndx + 1)(2 Ndy + 1)(2 Ndz + 1) values')
+        return np.ascontiguousarray(a)
+    b = 1.0 / np.sqrt(2.0)
+    if bool(getattr(options, 'oneD_weights', False)):
+        if N in _LFILTER_1D:
+            h = np.asarray(_LFILTER_1D[N], dtype=np.float64)
+            alpha = np.concatenate([h, h[:-1][::-1]])
+        elif N >= 67:
+            h = 0.5 * np.exp(np.linspace(-4.0, 0.0, int(np.ceil(N / 2))) / b)
+            alpha = np.concatenate([h, h[:-1][::-1]])
+            alpha = alpha / np.sum(alpha)
+        else:
+            raise ValueError('one-dimensional L-filter weights for %d values need numerical integration; '
+                             'give options.a_L' % N)
+        return np.ascontiguousarray(alpha, dtype=np.float32)
+    dx, dy, dz = _voxel_sizes(options)
+    dxy = np.sqrt(dx ** 2 + dy ** 2)
+    dxz = np.sqrt(dx ** 2 + dz ** 2)
+    dyz = np.sqrt(dy ** 2 + dz ** 2)
+    dxyz = np.sqrt(np.sqrt(dy ** 2 + dx ** 2) + dz ** 2)
+    dmin = min(dx, dy, dz)
+    alpha1 = 0.5 * np.exp(np.linspace(-1.5, 0.0, min(1, ndx) + min(1, ndy) + 1) / b)
+    out = []
+    for lz in range(-ndz, ndz + 1):
+        for ly in range(-ndy, ndy + 1):
+            for lx in range(-ndx, ndx + 1):
+                if ndz == 0 or lz == 0:
+                    if ly == 0 and lx != 0:
+                        v = alpha1[1] / (dx * abs(lx))
+                    elif ly == 0 and lx == 0:
+                        v = alpha1[-1] / dmin
+                    elif lx == 0:
+                        v = alpha1[1] / (dy * abs(ly))
+                    else:
+                        v = alpha1[0] / dxy
+                elif lx == 0 and ly == 0:
+                    v = alpha1[1] / (dz * abs(lz))
+                elif lx == 0:
+                    v = alpha1[0] / dyz
+                elif ly == 0:
+                    v = alpha1[0] / dxz
+                else:
+                    v = alpha1[0] / dxyz
+                out.append(v)
+    alpha = np.asarray(out)
+    return np.ascontiguousarray(alpha / np.sum(alpha), dtype=np.float32)
+
+
+def fmh_weights(options):
+    """The FMH prior's line weights, float32, (2 Ndx + 1) x lines column-major
+    (the layout the reference loads): options.fmh_weights when given, else
+    fmhWeights.m: kerroin = fmh_center_weight^(1/4) FOVa_x / Nx; each line's
+    weights kerroin over the offset's length along the line, fmh_center_weight
+    at the centre, each column normalised to sum 1.  3-D (13 lines): columns
+    1-9 the lines with a z step (1, 3, 7, 9 the space diagonals; 2, 8 over the
+    x-z length; 4, 6 over the y-z length; 5 the z axis), 10-13 the in-plane
+    lines (10, 12 the plane diagonal, 11 x, 13 y); 2-D (Nz = 1 or Ndz = 0, 4
+    lines): the in-plane set.  The kernel takes column ii for its line ii,
+    as the reference does."""
+    ndx, ndy, ndz = median_filter_window(options)
+    nz = int(np.ravel(options.Nz)[0])
+    two_d = nz == 1 or ndz == 0
+    lines = 4 if two_d else 13
+    rows = 2 * ndx + 1
+    w = np.asarray(getattr(options, 'fmh_weights', np.empty(0)), dtype=np.float32)
+    if w.size:
+        if w.size != rows * lines:
+            raise ValueError('fmh_weights must be (2 Ndx + 1) x %d' % lines)
+        return np.ascontiguousarray(w.reshape((rows, lines), order='F') if w.ndim == 1 else w).ravel(order='F')
+    dx, dy, dz = _voxel_sizes(options)
+    cw = float(getattr(options, 'fmh_center_weight', 4.))
+    kerroin = cw ** 0.25 * dx
+
+    def col(n, length):
+        return np.asarray([cw if i == 0 else kerroin / length(i) for i in range(n, -n - 1, -1)])
+    planar = [lambda i: np.sqrt((dx * i) ** 2 + (dy * i) ** 2), lambda i: abs(dx * i),
+              lambda i: np.sqrt((dx * i) ** 2 + (dy * i) ** 2), lambda i: abs(dy * i)]
+    if two_d:
+        W = np.stack([col(ndx, f) for f in planar], axis=1)
+    else:
+        zl = {1: lambda i: np.sqrt(np.sqrt((dz * i) ** 2 + (dx * i) ** 2) ** 2 + (dy * i) ** 2),
+              2: lambda i: np.sqrt((dz * i) ** 2 + (dx * i) ** 2),
+              4: lambda i: np.sqrt((dz * i) ** 2 + (dy * i) ** 2),
+              5: lambda i: abs(dz * i)}
+        zl[3] = zl[7] = zl[9] = zl[1]
+        zl[8] = zl[2]
+        zl[6] = zl[4]
+        W = np.stack([col(ndz, zl[j]) for j in range(1, 10)] + [col(ndx, f) for f in planar], axis=1)
+    W = W / np.sum(W, axis=0)
+    return np.ascontiguousarray(W.astype(np.float32).ravel(order='F'))
+
+
 def tv_anatomical_tensor(ref, Nx, Ny, Nz, T):
     """The weighting tensor of anatomical TV type 1 (prepass.py:509-533,
     assembleS): per voxel B = I - (1 - gamma) nu nu^T, nu the unit vector of

@@ -230,6 +230,15 @@ class projectorClass:
     # reference): flux 1 exponential / 2 quadratic, diffusion 1 gradient /
     # 2 modified curvature, iterations, time step, conductance
     AD = False
+    # the L-filter and FMH priors (proj.py:95-96, 150-151 of the reference):
+    # their weights, or empty for the prepass's (lfilter_weights.m,
+    # fmhWeights.m); oneD_weights picks the L-filter's one-dimensional set
+    L = False
+    FMH = False
+    a_L = np.empty(0, dtype=np.float32)
+    fmh_weights = np.empty(0, dtype=np.float32)
+    oneD_weights = False
+    fmh_center_weight = 4.
     FluxType = 1
     DiffusionType = 2
     NiterAD = 1

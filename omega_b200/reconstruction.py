@@ -380,9 +380,6 @@ def reconstructions_main(options):
     if len(chosen) > 1:
         raise ValueError('Select one reconstruction method (' + ', '.join(list(_PET_METHODS) + ['PDHG']) + ')')
     method = chosen[0]
-    if bool(getattr(options, 'L', False)) or bool(getattr(options, 'FMH', False)):
-        # the reference's Python path has no weights for these filters (prepass.py:1021-1022)
-        raise ValueError('L-filter and FMH-filter are not yet implemented!')
     quad, huber = bool(getattr(options, 'Quad', False)), bool(getattr(options, 'Huber', False))
     nlm = bool(getattr(options, 'NLM', False))
     mrp = bool(getattr(options, 'MRP', False))
@@ -392,13 +389,14 @@ def reconstructions_main(options):
     wmean = bool(getattr(options, 'weighted_mean', False))
     apls = bool(getattr(options, 'APLS', False)) and not options.PDHG   # the APLS prior: TVKernel's APLS form
     ad = bool(getattr(options, 'AD', False))
+    lf, fmh = bool(getattr(options, 'L', False)), bool(getattr(options, 'FMH', False))
     n_priors = (int(bool(options.RDP)) + int(quad) + int(huber) + int(nlm) + int(mrp) + int(tvp) + int(ggmrf) +
-                int(hyper) + int(wmean) + int(apls) + int(ad))
+                int(hyper) + int(wmean) + int(apls) + int(ad) + int(lf) + int(fmh))
     prior = method in _PRIOR_METHODS or (method == 'PKMA' and n_priors > 0)
     if prior and n_priors != 1:
         raise ValueError(method + ' needs one prior: options.RDP, options.Quad, options.Huber, options.NLM, '
                                   'options.MRP, options.TV, options.APLS, options.GGMRF, options.hyperbolic, '
-                                  'options.weighted_mean or options.AD')
+                                  'options.weighted_mean, options.AD, options.L or options.FMH')
     if prior and ad:
         if int(getattr(options, 'NiterAD', 1)) < 1 or not float(getattr(options, 'KAD', 1.)) > 0:
             raise ValueError('options.AD needs NiterAD >= 1 and KAD > 0')
@@ -535,7 +533,9 @@ def reconstructions_main(options):
         p.pkma_relax = (1 if getattr(options, 'computeRelaxationParameters', False) else 0) | \
             (2 if getattr(options, 'relaxationScaling', False) else 0)
     if prior:
-        p.prior = (_native.OMB_PRIOR_AD if ad else
+        p.prior = (_native.OMB_PRIOR_LFILTER if lf else
+                   _native.OMB_PRIOR_FMH if fmh else
+                   _native.OMB_PRIOR_AD if ad else
                    _native.OMB_PRIOR_RDP if options.RDP else
                    (_native.OMB_PRIOR_NLM if nlm else
                     (_native.OMB_PRIOR_MRP if mrp else
@@ -553,6 +553,18 @@ def reconstructions_main(options):
             p.ad_flux = int(getattr(options, 'FluxType', 1))
             p.ad_diffusion = int(getattr(options, 'DiffusionType', 2))
             p.mrp_no_norm = 1 if getattr(options, 'med_no_norm', False) else 0
+        if lf or fmh:
+            # the L-filter (priors.h:84-97) and FMH (priors.h:54-82) over Ndx / Ndy / Ndz, with the
+            # MATLAB prepass's weights (lfilter_weights.m, fmhWeights.m) unless given
+            from . import priors
+            wl = torch.from_numpy(priors.lfilter_weights(options) if lf else priors.fmh_weights(options)).to(dev)
+            keep.append(wl)
+            if lf:
+                p.lfilter_weights = ctypes.c_void_p(wl.data_ptr())
+            else:
+                p.fmh_weights = ctypes.c_void_p(wl.data_ptr())
+            p.mrp_no_norm = 1 if getattr(options, 'med_no_norm', False) else 0
+            p.prior_g[0], p.prior_g[1], p.prior_g[2] = priors.median_filter_window(options)
         if wmean:
             from . import priors
             mt = int(getattr(options, 'mean_type', 4))

@@ -16,7 +16,10 @@ steps around the projectors, for the parity tests:
   epps), NLTV's squared sum from 0), which oracle/_ref exports and pins;
 * mrp_gradient: the median root prior (priors.h:4-25) on the symmetric
   padding; its median equals the reference CPU medianFilter3D (MRP.h),
-  which oracle/_ref exports.
+  which oracle/_ref exports;
+* lfilter_gradient / fmh_gradient: the L-filter and FMH priors (priors.h:
+  54-97) over the reference's offsets grid (computeOffsets.m) on the same
+  symmetric padding, with ArrayFire's sort / matmul / median written out.
 """
 import numpy as np
 
@@ -161,6 +164,62 @@ def mrp_gradient(u, shape, m, beta, epps, no_norm=False):
     med = np.median(np.stack(stack), axis=0)
     d = U - med
     return (beta * d if no_norm else d / (med + epps) * beta).ravel()
+
+
+def _offset_columns(u, shape, m):
+    """The window values of every voxel, one row per column of the offsets
+    grid (computeOffsets.m: ndgrid over -Ndx..Ndx on every axis, x fastest;
+    3 axes for Ndx = Ndy = Ndz, 2 for Ndx = Ndy = 1, Ndz = 0), on the image
+    padded symmetrically by (Ndx, Ndy, Ndz) (functions.hpp:216-260)."""
+    nx, ny, nz = shape
+    mx, my, mz = (int(v) for v in m)
+    assert (mx >= 1 and mx == my == mz) or (mx, my, mz) == (1, 1, 0)
+    d = 3 if mz else 2
+    w = 2 * mx + 1
+    U = np.asarray(u, dtype=np.float64).reshape((nz, ny, nx))
+    P = np.pad(U, ((mz, mz), (my, my), (mx, mx)), mode='symmetric')
+    rows = []
+    for c in range(w ** d):
+        i, j, k = c % w - mx, (c // w) % w - my, (c // (w * w) - mz if d == 3 else 0)
+        rows.append(P[mz + k:mz + k + nz, my + j:my + j + ny, mx + i:mx + i + nx].ravel())
+    return np.stack(rows)
+
+
+def lfilter_gradient(u, shape, m, a_l, beta, epps, no_norm=False):
+    """L-filter prior (priors.h:84-97): the window values sorted ascending per
+    voxel, their sum weighted by a_L, beta (u - s) / (s + epps) (no_norm:
+    beta (u - s))."""
+    V = np.sort(_offset_columns(u, shape, m), axis=0)
+    s = np.asarray(a_l, dtype=np.float64) @ V
+    d = np.asarray(u, dtype=np.float64).ravel() - s
+    return beta * d if no_norm else d / (s + epps) * beta
+
+
+def fmh_gradient(u, shape, m, fmh_w, beta, epps, no_norm=False):
+    """FMH prior (priors.h:54-82): for ii < luup (4 when Nz = 1 or Ndz = 0,
+    else 13) the offsets columns seq(Ndx ii, N - Ndx ii - 1, alku / Ndx - ii)
+    (alku the centre column, N the column count) weighted by column ii of
+    fmh_weights ((2 Ndx + 1) x luup, column-major); the centre value last;
+    the median of the luup + 1 values (numpy's median: the mean of the
+    middle two for an even count, as af::median); beta (u - med) / (med +
+    epps) (no_norm: beta (u - med))."""
+    nx, ny, nz = shape
+    mx, my, mz = (int(v) for v in m)
+    V = _offset_columns(u, shape, m)
+    N = V.shape[0]
+    alku = N // 2
+    luup = 4 if (nz == 1 or mz == 0) else 13
+    rows = 2 * mx + 1
+    W = np.asarray(fmh_w, dtype=np.float64).reshape((rows, luup), order='F')
+    vals = []
+    for ii in range(luup):
+        cols = list(range(mx * ii, N - mx * ii, alku // mx - ii))
+        assert len(cols) == rows
+        vals.append(W[:, ii] @ V[cols])
+    vals.append(V[alku])
+    med = np.median(np.stack(vals), axis=0)
+    d = np.asarray(u, dtype=np.float64).ravel() - med
+    return beta * d if no_norm else d / (med + epps) * beta
 
 
 def padded_symmetric(u, shape, m):

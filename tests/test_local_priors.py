@@ -294,17 +294,18 @@ def test_wmean46_oracle_follows_the_reference_steps():
 
 
 @pytest.mark.parametrize("flag", ["L", "FMH"])
-def test_l_filter_and_fmh_raise_as_the_reference(flag):
-    """The reference's Python path raises for the L-filter and FMH priors
-    (prepass.py:1021-1022: their weights are built only by the MATLAB
-    prepass); the built-in entry raises the same error before any launch."""
+def test_l_filter_and_fmh_count_as_priors(flag):
+    """The L-filter and FMH are priors of the MAP algorithms: one of them
+    with a second prior is refused before any launch, as any two priors are,
+    and so is a window the reference's offsets grid does not follow."""
     from conftest import make_options
     from omega_b200 import reconstruction as rec
     o = make_options("pet_mini")
     o.SinM = np.ones(int(o.Ndist) * int(o.Nang) * int(o.NSinos), np.float32)
     o.OSL_OSEM = True
     setattr(o, flag, True)
-    with pytest.raises(ValueError, match="not yet implemented"):
+    o.MRP = True
+    with pytest.raises(ValueError, match="needs one prior"):
         rec.reconstructions_main(o)
 
 
