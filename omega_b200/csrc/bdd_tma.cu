@@ -213,20 +213,23 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
                 const float *q1 = q + seg.o1, *q2 = q + seg.o2;
                 float R = fmaf(seg.w2, *q2, fmaf(seg.w1, *q1, seg.w0 * q[0]));
                 float S = 0.f;
-                float Cprev = (bz - (float)kc) * R;
+                // the row as an exact float: with bz >= 0 and at most one new
+                // row per column, (int)bz > kc is bz >= kc + 1, so no
+                // float-to-int conversion per column
+                float fkc = (float)kc;
+                float Cprev = (bz - fkc) * R;
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
                     bz = fmaf((float)(c + 1), w, zu);
-                    const int kn = (int)bz;
-                    if (kc < kn) {
+                    if (bz >= fkc + 1.f) {
                         S += R;
-                        ++kc;
+                        fkc += 1.f;
                         q += kBW;
                         q1 += kBW;
                         q2 += kBW;
                         R = fmaf(seg.w2, *q2, fmaf(seg.w1, *q1, seg.w0 * q[0]));
                     }
-                    const float C = fmaf(bz - (float)kc, R, S);
+                    const float C = fmaf(bz - fkc, R, S);
                     temp[c] = fmaf(C - Cprev, inv_area, temp[c]);
                     Cprev = C;
                 }
