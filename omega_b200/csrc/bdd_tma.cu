@@ -237,18 +237,21 @@ __global__ void k_bdd_fp_tma(const __grid_constant__ CUtensorMap map_img, const 
                 const float *q = sh.box[s] + (kc - o.y) * kBW + (i0 - o.x);
                 float R = fmaf(seg.w2, q[seg.o2], fmaf(seg.w1, q[seg.o1], seg.w0 * q[0]));
                 float S = 0.f;
-                float Cprev = (bz - (float)kc) * R;
+                // min((int)bz, zmax) > kc with bz in [0, nz] is bz >= kc + 1
+                // below the last row (the exact-float row as above)
+                float fkc = (float)kc;
+                const float fzmax = (float)zmax;
+                float Cprev = (bz - fkc) * R;
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
                     bz = fminf(fmaxf(fmaf((float)(c + 1), w, zu), 0.f), fz);
-                    const int kn = min((int)bz, zmax);
-                    if (kc < kn) {
+                    if (bz >= fkc + 1.f && fkc < fzmax) {
                         S += R;
-                        ++kc;
+                        fkc += 1.f;
                         q += kBW;
                         R = fmaf(seg.w2, q[seg.o2], fmaf(seg.w1, q[seg.o1], seg.w0 * q[0]));
                     }
-                    const float C = fmaf(bz - (float)kc, R, S);
+                    const float C = fmaf(bz - fkc, R, S);
                     temp[c] = fmaf(C - Cprev, inv_area, temp[c]);
                     Cprev = C;
                 }
